@@ -1,0 +1,170 @@
+/*
+ * jfb200.h — C ABI of the B200-native pseudo-spectral Galerkin Couette step.
+ *
+ * Plain C: device pointers, sizes and a CUDA stream handle (passed as void*,
+ * the value of a cudaStream_t; NULL = legacy default stream).  Every entry
+ * point returns an int status (JFB_OK == 0); jfb_last_error() returns a
+ * thread-local description of the last failure.  No C++ exceptions cross
+ * this boundary and no torch types appear in it.
+ *
+ * Each declaration cites the fnauman/jaxfun interface it replaces
+ * (file:line within that project).  Complex arrays are interleaved
+ * (re, im) float64 pairs (numpy/jax complex128 memory layout), C-ordered.
+ */
+#ifndef JFB200_H
+#define JFB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define JFB_OK 0
+#define JFB_ERR_ARG 1        /* invalid argument / unsupported shape         */
+#define JFB_ERR_CUDA 2       /* a CUDA runtime call failed                   */
+#define JFB_ERR_SINGULAR 3   /* zero or non-finite pivot (diamatrix.py:461)  */
+#define JFB_ERR_NONFINITE 4  /* non-finite value detected in the state       */
+#define JFB_ERR_STATE 5      /* call sequence error (e.g. no state set)      */
+
+/* ---- library ------------------------------------------------------------ */
+int jfb_version(void);
+const char* jfb_last_error(void);
+
+/* ---- jaxfun.la DIA matrices --------------------------------------------- */
+
+/* DiaMatrix.matvec(x, axis) / DiaMatrix.rmatvec(x, axis)
+ * (src/jaxfun/la/diamatrix.py:227-283, 285-348).
+ * Column-aligned DIA storage: data[d * n_cols + j] = A[j - offsets[d], j]
+ * (diamatrix.py:100-123).  x is viewed as (outer, m, inner) with the
+ * contracted axis in the middle; y as (outer, n, inner), where for
+ * transpose == 0 (matvec) m = n_cols, n = n_rows and for transpose == 1
+ * (rmatvec, x @ A) m = n_rows, n = n_cols.  is_complex selects interleaved
+ * complex128 x / y; data is always real float64.  offsets is a host array. */
+int jfb_dia_matvec(const double* data, const int64_t* offsets, int64_t n_diags,
+                   int64_t n_rows, int64_t n_cols, const double* x, double* y,
+                   int64_t outer, int64_t inner, int is_complex, int transpose,
+                   void* stream);
+
+/* Batched banded LU without pivoting (src/jaxfun/la/diamatrix.py:394-504,
+ * kernel 1936-1973; batched use in tpmatrix.py:1105-1149).
+ * band has shape (n_batch, p + q + 1, n) with band[b, p + off, j] =
+ * A_b[j - off, j]; it is factored in place (multipliers in the sub-diagonal
+ * rows, U in the rest).  Returns JFB_ERR_SINGULAR if any pivot is zero or
+ * non-finite (diamatrix.py:461-471); synchronises the stream to check. */
+int jfb_banded_lu_factor(double* band, int64_t n_batch, int64_t p, int64_t q,
+                         int64_t n, void* stream);
+
+/* TPMatricesWavenumberSolver.solve / solve_many / *_with_runtime_args
+ * (src/jaxfun/la/tpmatrix.py:1550-1677, batched recurrence 686-799).
+ * L: (n_F, n_L, n_P) unit-lower sub-diagonals with L_offsets (< 0);
+ * U: (n_F, n_U, n_P) with U_offsets (>= 0, containing 0).  Offsets are host
+ * arrays.  rhs / out are (n_rhs, outer, n_P, inner) with n_F = outer*inner:
+ * the polynomial axis sits between the Fourier axes exactly as in the
+ * reference tensor (Fourier index flattened C-order, tpmatrix.py:1335-1357).
+ * rhs and out may alias. */
+int jfb_wavenumber_solve(const double* L, const int64_t* L_offsets, int64_t n_L,
+                         const double* U, const int64_t* U_offsets, int64_t n_U,
+                         int64_t n_P, int64_t outer, int64_t inner, int64_t n_rhs,
+                         const double* rhs, double* out, int is_complex,
+                         void* stream);
+
+/* ---- KMM plane-Couette / channel step ----------------------------------- */
+
+#define JFB_FAMILY_CHEBYSHEV 0
+#define JFB_PRECISION_FP64 0
+#define JFB_PRECISION_MIXED 1
+#define JFB_NONLINEAR_ROTATIONAL 0
+
+/* Constructor arguments of KMM / PlaneCouetteFluctuationJax
+ * (examples/channelflow_kmm.py:107-230, examples/pcf_fluctuations_jax.py:35-75)
+ * restricted to the hot path: Chebyshev family, x unpadded, SBDF3 with an
+ * IMEXRK3 startup, rotational nonlinear form.  u_wall = 0 gives the plain
+ * KMM channel (no base flow). */
+typedef struct jfb_kmm_config {
+  int32_t nx, ny, nz;     /* N = (wall-normal orthogonal size, Fourier y, z) */
+  int32_t family;         /* JFB_FAMILY_CHEBYSHEV                           */
+  double x_lo, x_hi;      /* wall-normal domain                             */
+  double ly, lz;          /* periodic lengths of the y and z axes           */
+  double pad_y, pad_z;    /* dealiasing padding factors (1.5 = 3/2 rule)    */
+  double nu;              /* kinematic viscosity                            */
+  double dt;              /* fixed time step                                */
+  double u_wall;          /* base flow U_b(x) = u_wall * x                  */
+  int32_t precision;      /* JFB_PRECISION_FP64 or JFB_PRECISION_MIXED      */
+  int32_t nonlinear_form; /* JFB_NONLINEAR_ROTATIONAL                       */
+} jfb_kmm_config;
+
+/* Device pointers to a KMMState in the reference layout
+ * (examples/channelflow_kmm.py:50-101): u0 (nx-4, ny, nz) complex128 in the
+ * biharmonic basis; u1, u2, g (nx-2, ny, nz) complex128 in the Dirichlet
+ * basis; history levels as (Nu | u0, Ng | g) complex plus (Nv00 | v00,
+ * Nw00 | w00) float64 vectors of length nx-2. */
+typedef struct jfb_kmm_state {
+  void* u0;
+  void* u1;
+  void* u2;
+  void* g;
+  void* nonlinear_old[4];
+  void* nonlinear_older[4];
+  void* solution_old[4];
+  void* solution_older[4];
+  double history_steps;
+} jfb_kmm_state;
+
+typedef struct jfb_kmm_info {
+  int64_t n_pencils;          /* stored (ky, kz >= 0) spectral pencils      */
+  int64_t device_bytes;       /* device memory held by the plan             */
+  int64_t launches_per_step;  /* kernels launched per steady SBDF3 step     */
+  int64_t algorithmic_bytes;  /* stage-model HBM bytes per steady step      */
+  int32_t my, mz;             /* padded quadrature counts                   */
+} jfb_kmm_info;
+
+typedef struct jfb_kmm_plan jfb_kmm_plan;
+
+/* KMM.__init__ + _build_operators + lu_factor of Su/Sg/S00 and the three
+ * IMEXRK3 startup factor sets (channelflow_kmm.py:107-444).  Allocates the
+ * plan's device memory on the current device. */
+int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** plan);
+int jfb_kmm_destroy(jfb_kmm_plan* plan);
+int jfb_kmm_get_info(const jfb_kmm_plan* plan, jfb_kmm_info* info);
+
+/* Load / store the full KMMState (all history levels).  The plan keeps the
+ * real-field (Hermitian, kz >= 0) half of every spectrum; set_state reads the
+ * kz < nz/2 columns, get_state writes the full spectrum back using
+ * c(-ky, -kz) = conj(c(ky, kz)). */
+int jfb_kmm_set_state(jfb_kmm_plan* plan, const jfb_kmm_state* state,
+                      void* stream);
+int jfb_kmm_get_state(jfb_kmm_plan* plan, const jfb_kmm_state* state,
+                      void* stream);
+
+/* KMM.solve(state, steps) (channelflow_kmm.py:1231-1247): the IMEXRK3
+ * startup steps while history_steps < 2 (_step_sbdf3, :937-1014), then
+ * steady SBDF3 steps (_step_sbdf3_steady, :1016-1064), replayed from a CUDA
+ * graph.  steps == 1 is KMM.step. */
+int jfb_kmm_advance(jfb_kmm_plan* plan, int64_t steps, void* stream);
+
+/* KMM.convection(state) (channelflow_kmm.py:772-782) of the loaded state:
+ * writes the three dealiased TD coefficient fields H (nx-2, ny, nz) complex. */
+int jfb_kmm_convection(jfb_kmm_plan* plan, void* h0, void* h1, void* h2,
+                       void* stream);
+
+/* KMM.state_from_physical (channelflow_kmm.py:677-683) as used by
+ * PlaneCouetteFluctuationJax.initial_state (pcf_fluctuations_jax.py:77-97):
+ * u0, u1, u2 are real float64 samples (nx, ny, nz) on the Gauss-Chebyshev x
+ * nodes and the uniform y, z grids; loads TB/TD.forward of them (Nyquist
+ * masked), g = i ky u2 - i kz u1, and a zero history (history_steps = 0). */
+int jfb_kmm_state_from_physical(jfb_kmm_plan* plan, const double* u0,
+                                const double* u1, const double* u2, void* stream);
+
+/* PlaneCouetteFluctuationJax.diagnostics (pcf_fluctuations_jax.py:131-161) of
+ * the loaded state, written to the device array out[8] = (Epert, Etot, divL2,
+ * u_top, u_bot, wall_shear_top, wall_shear_bot, mean_shear).  Deterministic
+ * fixed-order reduction. */
+int jfb_kmm_diagnostics(jfb_kmm_plan* plan, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JFB200_H */

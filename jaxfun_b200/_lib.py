@@ -1,0 +1,152 @@
+"""ctypes binding of ``libjfb200.so`` (the C ABI declared in include/jfb200.h).
+
+The shared library is built in-tree by ``jaxfun_b200.build.build()``.  There is
+no fallback: importing a function from this module when the library is
+missing raises ``ImportError`` with the build command to run.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_double, c_int, c_int32, c_int64, c_void_p
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libjfb200.so")
+
+JFB_OK = 0
+JFB_ERR_ARG = 1
+JFB_ERR_CUDA = 2
+JFB_ERR_SINGULAR = 3
+JFB_ERR_NONFINITE = 4
+JFB_ERR_STATE = 5
+
+JFB_FAMILY_CHEBYSHEV = 0
+JFB_PRECISION_FP64 = 0
+JFB_PRECISION_MIXED = 1
+JFB_NONLINEAR_ROTATIONAL = 0
+
+
+class KMMConfig(ctypes.Structure):
+    """``jfb_kmm_config`` (include/jfb200.h)."""
+
+    _fields_ = [
+        ("nx", c_int32),
+        ("ny", c_int32),
+        ("nz", c_int32),
+        ("family", c_int32),
+        ("x_lo", c_double),
+        ("x_hi", c_double),
+        ("ly", c_double),
+        ("lz", c_double),
+        ("pad_y", c_double),
+        ("pad_z", c_double),
+        ("nu", c_double),
+        ("dt", c_double),
+        ("u_wall", c_double),
+        ("precision", c_int32),
+        ("nonlinear_form", c_int32),
+    ]
+
+
+class KMMStateC(ctypes.Structure):
+    """``jfb_kmm_state``: device pointers of a KMMState in the reference layout."""
+
+    _fields_ = [
+        ("u0", c_void_p),
+        ("u1", c_void_p),
+        ("u2", c_void_p),
+        ("g", c_void_p),
+        ("nonlinear_old", c_void_p * 4),
+        ("nonlinear_older", c_void_p * 4),
+        ("solution_old", c_void_p * 4),
+        ("solution_older", c_void_p * 4),
+        ("history_steps", c_double),
+    ]
+
+
+class KMMInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_pencils", c_int64),
+        ("device_bytes", c_int64),
+        ("launches_per_step", c_int64),
+        ("algorithmic_bytes", c_int64),
+        ("my", c_int32),
+        ("mz", c_int32),
+    ]
+
+
+# name -> (restype, argtypes); every symbol declared in include/jfb200.h
+SIGNATURES = {
+    "jfb_version": (c_int, []),
+    "jfb_last_error": (ctypes.c_char_p, []),
+    "jfb_dia_matvec": (
+        c_int,
+        [c_void_p, POINTER(c_int64), c_int64, c_int64, c_int64, c_void_p, c_void_p,
+         c_int64, c_int64, c_int, c_int, c_void_p],
+    ),
+    "jfb_banded_lu_factor": (
+        c_int, [c_void_p, c_int64, c_int64, c_int64, c_int64, c_void_p]
+    ),
+    "jfb_wavenumber_solve": (
+        c_int,
+        [c_void_p, POINTER(c_int64), c_int64, c_void_p, POINTER(c_int64), c_int64,
+         c_int64, c_int64, c_int64, c_int64, c_void_p, c_void_p, c_int, c_void_p],
+    ),
+    "jfb_kmm_create": (c_int, [POINTER(KMMConfig), POINTER(c_void_p)]),
+    "jfb_kmm_destroy": (c_int, [c_void_p]),
+    "jfb_kmm_get_info": (c_int, [c_void_p, POINTER(KMMInfo)]),
+    "jfb_kmm_set_state": (c_int, [c_void_p, POINTER(KMMStateC), c_void_p]),
+    "jfb_kmm_get_state": (c_int, [c_void_p, POINTER(KMMStateC), c_void_p]),
+    "jfb_kmm_advance": (c_int, [c_void_p, c_int64, c_void_p]),
+    "jfb_kmm_convection": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "jfb_kmm_state_from_physical": (
+        c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+    ),
+    "jfb_kmm_diagnostics": (c_int, [c_void_p, c_void_p, c_void_p]),
+}
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load (once) and return the shared library; raise if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with "
+            "`python -c 'import jaxfun_b200.build as b; b.build()'`"
+        )
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class JFBError(RuntimeError):
+    """A non-zero status returned by the C ABI."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"jfb status {status}: {msg}")
+        self.status = status
+
+
+def check(status: int) -> None:
+    if status != JFB_OK:
+        msg = load().jfb_last_error()
+        raise JFBError(status, msg.decode() if msg else "")
+
+
+def call(name: str, *args) -> None:
+    """Call a C-ABI function and raise ``JFBError`` on a non-zero status."""
+    check(getattr(load(), name)(*args))
+
+
+def int64_array(values) -> ctypes.Array:
+    vals = [int(v) for v in values]
+    return (c_int64 * max(1, len(vals)))(*vals)

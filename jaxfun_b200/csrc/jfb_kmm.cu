@@ -1,0 +1,866 @@
+// KMM plane-Couette plan: C-ABI entry points, device set-up (per-wavenumber
+// operator assembly, banded LU, packing), state conversion and the step
+// driver with CUDA-graph replay of steady SBDF3 steps.
+//
+// Reference: examples/channelflow_kmm.py (KMM), examples/pcf_fluctuations_jax.py
+// (PlaneCouetteFluctuationJax), src/jaxfun/integrators/sbdf3.py, imex_rk.py.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "jfb_common.cuh"
+#include "jfb_kmm.h"
+#include "jfb_kmm_kernels.cuh"
+
+namespace jfb {
+
+// IMEXRK3 (Spalart low-storage) tableau, integrators/imex_rk.py:96-125.
+static const double kRK3A[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+static const double kRK3B[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+static const double kSBDF3Implicit = 6.0 / 11.0;  // integrators/sbdf3.py:11-12
+
+// ---------------------------------------------------------------------------
+// set-up kernels
+// ---------------------------------------------------------------------------
+
+// band[m][p + off][j] = a0[m] X0[j-off, j] + a2[m] X2[j-off, j] + a4[m] X4[j-off, j]
+__global__ void assemble_band_kernel(const double* __restrict__ X0,
+                                     const double* __restrict__ X2,
+                                     const double* __restrict__ X4,
+                                     const double* __restrict__ coef, int n_modes, int n,
+                                     int p, int q, double* __restrict__ band) {
+  const int bw = p + q + 1;
+  const int64_t total = (int64_t)n_modes * bw * n;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int j = (int)(idx % n);
+    const int r = (int)((idx / n) % bw);
+    const int m = (int)(idx / ((int64_t)n * bw));
+    const int off = r - p;
+    const int i = j - off;
+    double v = 0.0;
+    if (i >= 0 && i < n) {
+      const size_t e = (size_t)i * n + j;
+      v = coef[3 * m] * X0[e] + coef[3 * m + 1] * X2[e];
+      if (X4) v += coef[3 * m + 2] * X4[e];
+    }
+    band[idx] = v;
+  }
+}
+
+// Factored band -> packed parity record (see packed_rec_size).
+__global__ void pack_factor_kernel(const double* __restrict__ band, int n_modes, int n,
+                                   int p, int q, double* __restrict__ out) {
+  const int m = blockIdx.x;
+  if (m >= n_modes) return;
+  const int bw = p + q + 1;
+  const double* B = band + (size_t)m * bw * n;
+  double* R = out + (size_t)m * packed_rec_size(n);
+  auto at = [&](int off, int col) { return B[(size_t)(p + off) * n + col]; };
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    R[2 * i] = (i >= 2 && p >= 2) ? at(-2, i - 2) : 0.0;      // L[i, i-2]
+    R[2 * i + 1] = (i >= 4 && p >= 4) ? at(-4, i - 4) : 0.0;  // L[i, i-4]
+  }
+  const int m0 = (n + 1) / 2, m1 = n / 2;
+  double* U0 = R + 2 * n;
+  double* U1 = U0 + m0 * (m0 + 1) / 2;
+  for (int par = 0; par < 2; ++par) {
+    const int mp = par ? m1 : m0;
+    double* Up = par ? U1 : U0;
+    const int tot = mp * (mp + 1) / 2;
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      // invert e -> (r, c) with e = c(c+1)/2 + r, r <= c
+      int c = (int)floor((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+      while (c * (c + 1) / 2 > e) --c;
+      while ((c + 1) * (c + 2) / 2 <= e) ++c;
+      const int r = e - c * (c + 1) / 2;
+      const int row = 2 * r + par, col = 2 * c + par;
+      const int off = col - row;
+      double v = (off <= q) ? at(off, col) : 0.0;
+      if (r == c) v = 1.0 / v;
+      Up[e] = v;
+    }
+  }
+}
+
+// Reference layout (n, Ny, Nz) complex -> half layout [i][ky][kz < Kz],
+// zeroing the y Nyquist row.
+__global__ void to_half_kernel(const c64* __restrict__ full, int n, int Ny, int Nz,
+                               c64* __restrict__ half) {
+  const int Kz = Nz / 2;
+  const int64_t total = (int64_t)n * Ny * Kz;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int kz = (int)(idx % Kz);
+    const int ky = (int)((idx / Kz) % Ny);
+    const int i = (int)(idx / ((int64_t)Kz * Ny));
+    half[idx] = (ky == Ny / 2) ? cmk(0.0, 0.0) : full[((size_t)i * Ny + ky) * Nz + kz];
+  }
+}
+
+// Half layout -> full reference layout using c(-ky, -kz) = conj(c(ky, kz));
+// the kz = Nz/2 column is zero.
+__global__ void to_full_kernel(const c64* __restrict__ half, int n, int Ny, int Nz,
+                               c64* __restrict__ full) {
+  const int Kz = Nz / 2;
+  const int64_t total = (int64_t)n * Ny * Nz;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int kz = (int)(idx % Nz);
+    const int ky = (int)((idx / Nz) % Ny);
+    const int i = (int)(idx / ((int64_t)Nz * Ny));
+    c64 v = cmk(0.0, 0.0);
+    if (kz < Kz) {
+      v = half[((size_t)i * Ny + ky) * Kz + kz];
+    } else if (kz > Kz) {
+      const int my = (Ny - ky) % Ny;
+      v = conjc(half[((size_t)i * Ny + my) * Kz + (Nz - kz)]);
+    }
+    full[idx] = v;
+  }
+}
+
+// Pack / unpack the two real mean-flow vectors into one complex vector.
+__global__ void means_in_kernel(const c64* __restrict__ u1, const c64* __restrict__ u2,
+                                int n, int Ny, int Nz, c64* __restrict__ vw) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    vw[i] = cmk(u1[(size_t)i * Ny * Nz].re, u2[(size_t)i * Ny * Nz].re);
+}
+__global__ void real_pair_in_kernel(const double* __restrict__ a,
+                                    const double* __restrict__ b, int n,
+                                    c64* __restrict__ vw) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    vw[i] = cmk(a ? a[i] : 0.0, b ? b[i] : 0.0);
+}
+__global__ void real_pair_out_kernel(const c64* __restrict__ vw, int n, double* a,
+                                     double* b) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (a) a[i] = vw[i].re;
+    if (b) b[i] = vw[i].im;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// plan
+// ---------------------------------------------------------------------------
+struct FactorSet {
+  double* su = nullptr;
+  double* sg = nullptr;
+  double* s00 = nullptr;
+};
+
+}  // namespace jfb
+
+struct jfb_kmm_plan {
+  jfb_kmm_config cfg;
+  jfb::HostOperators hop;
+  jfb::Dims d;
+  jfb::DevOps ops;
+  jfb::FFTPlan fy, fz;
+  int n_modes = 0, su_rec = 0, sg_rec = 0;
+  int KC = 0;
+  size_t smem_pencil = 0, smem_y = 0, smem_z = 0;
+  std::vector<void*> allocs;
+  int64_t device_bytes = 0;
+  jfb::FactorSet steady, startup[3];
+  jfb::c64 *U0[3], *G[3], *NU[3], *NG[3], *VW[3], *NVW[3];
+  jfb::c64 *NUst, *NGst, *NVWst;
+  jfb::c64 *U1S, *U2S;
+  jfb::c64 *X, *Y, *HZ, *HX, *HD;
+  jfb::c64 *twy, *twz, *twny, *twnz;
+  jfb::FFTPlan fny, fnz;  // unpadded y / z transforms (state_from_physical)
+  double *diag_partial = nullptr, *diag_mean = nullptr;
+  int diag_blocks = 0;
+  size_t smem_zf = 0, smem_diag = 0;
+  int64_t n = 0;       // ring counter: u^n lives in slot n % 3
+  int hist = 0;        // history_steps (0, 1, 2)
+  bool have_state = false;
+  bool have_H = false;     // HX holds H(u^n)
+  bool explicit_u12 = false;  // U1S/U2S hold the current u1, u2
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  cudaStream_t cap = nullptr;  // private stream used only to capture the graphs
+};
+
+namespace jfb {
+
+static int dalloc(jfb_kmm_plan* pl, void** ptr, size_t bytes) {
+  JFB_CHECK_CUDA(cudaMalloc(ptr, bytes));
+  JFB_CHECK_CUDA(cudaMemset(*ptr, 0, bytes));
+  pl->allocs.push_back(*ptr);
+  pl->device_bytes += (int64_t)bytes;
+  return JFB_OK;
+}
+
+template <typename T>
+static int upload(jfb_kmm_plan* pl, T** dst, const std::vector<T>& v) {
+  int st = dalloc(pl, (void**)dst, std::max<size_t>(1, v.size()) * sizeof(T));
+  if (st) return st;
+  if (!v.empty())
+    JFB_CHECK_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return JFB_OK;
+}
+
+static std::vector<c64> twiddles(int n) {
+  std::vector<c64> t(n);
+  for (int k = 0; k < n; ++k) {
+    const double a = -2.0 * M_PI * (double)k / (double)n;
+    t[k] = cmk(std::cos(a), std::sin(a));
+  }
+  return t;
+}
+
+// Build, factor and pack the per-wavenumber systems for implicit coefficient
+// gamma (tpmatrix.py:1900-2029 assembly, 1105-1149 batched LU).
+static int build_factor_set(jfb_kmm_plan* pl, double gamma, FactorSet& fs) {
+  const HostOperators& op = pl->hop;
+  const jfb_kmm_config& cfg = pl->cfg;
+  const Dims& d = pl->d;
+  const int nm = pl->n_modes;
+  int st;
+  double *dX0 = nullptr, *dX2 = nullptr, *dX4 = nullptr, *dcoef = nullptr, *dband = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(dX0);
+    cudaFree(dX2);
+    cudaFree(dX4);
+    cudaFree(dcoef);
+    cudaFree(dband);
+  };
+  for (int sys = 0; sys < 3; ++sys) {
+    // sys 0: Su (biharmonic basis), 1: Sg (Dirichlet), 2: S00 (1-D Dirichlet)
+    const bool bih = sys == 0;
+    const int n = bih ? d.nB : d.nD;
+    const std::vector<double>& X0 = bih ? op.XB0 : op.XD0;
+    const std::vector<double>& X2 = bih ? op.XB2 : op.XD2;
+    const int modes = (sys == 2) ? 1 : nm;
+    std::vector<double> coef((size_t)3 * modes);
+    if (sys == 2) {
+      coef[0] = 1.0;
+      coef[1] = -gamma * cfg.nu;
+      coef[2] = 0.0;
+    } else {
+      for (int a = 0; a < d.Ny / 2; ++a)
+        for (int b = 0; b < d.Kz; ++b)
+          mode_coefficients(op, cfg, a, b, gamma, bih, &coef[3 * (a * d.Kz + b)]);
+    }
+    // bandwidths from the nonzero structure of the x-matrices
+    int p = 0, q = 0;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        const double v = std::fabs(X0[(size_t)i * n + j]) + std::fabs(X2[(size_t)i * n + j]) +
+                         (bih ? std::fabs(op.XB4[(size_t)i * n + j]) : 0.0);
+        if (v != 0.0) {
+          if (j - i > q) q = j - i;
+          if (i - j > p) p = i - j;
+          JFB_REQUIRE(((j - i) & 1) == 0, "odd diagonal in a Shen operator");
+        }
+      }
+    JFB_REQUIRE(p <= 4, "unexpected lower bandwidth");
+    st = upload(pl, &dX0, X0);
+    if (st) return cleanup(), st;
+    st = upload(pl, &dX2, X2);
+    if (st) return cleanup(), st;
+    if (bih) {
+      st = upload(pl, &dX4, op.XB4);
+      if (st) return cleanup(), st;
+    }
+    st = upload(pl, &dcoef, coef);
+    if (st) return cleanup(), st;
+    const size_t band_elems = (size_t)modes * (p + q + 1) * n;
+    JFB_CHECK_CUDA(cudaMalloc((void**)&dband, band_elems * sizeof(double)));
+    assemble_band_kernel<<<1024, 256>>>(dX0, dX2, bih ? dX4 : nullptr, dcoef, modes, n, p,
+                                        q, dband);
+    JFB_CHECK_LAUNCH();
+    st = jfb_banded_lu_factor(dband, modes, p, q, n, nullptr);
+    if (st) return cleanup(), st;
+    double** dst = (sys == 0) ? &fs.su : (sys == 1) ? &fs.sg : &fs.s00;
+    st = dalloc(pl, (void**)dst, (size_t)modes * packed_rec_size(n) * sizeof(double));
+    if (st) return cleanup(), st;
+    pack_factor_kernel<<<modes, 128>>>(dband, modes, n, p, q, *dst);
+    JFB_CHECK_LAUNCH();
+    JFB_CHECK_CUDA(cudaDeviceSynchronize());
+    // the temporaries were registered as plan allocations by upload(): release them
+    for (void* ptr : {(void*)dX0, (void*)dX2, (void*)dX4, (void*)dcoef}) {
+      if (!ptr) continue;
+      for (size_t k = 0; k < pl->allocs.size(); ++k)
+        if (pl->allocs[k] == ptr) {
+          pl->allocs.erase(pl->allocs.begin() + k);
+          break;
+        }
+    }
+    pl->device_bytes -= (int64_t)(X0.size() + X2.size() + (bih ? op.XB4.size() : 0) +
+                                  coef.size()) *
+                        sizeof(double);
+    cleanup();
+    dX0 = dX2 = dX4 = dcoef = dband = nullptr;
+  }
+  return JFB_OK;
+}
+
+static PackedFactors packed(const jfb_kmm_plan* pl, const FactorSet& fs) {
+  PackedFactors f;
+  f.su = fs.su;
+  f.sg = fs.sg;
+  f.s00 = fs.s00;
+  f.su_rec = pl->su_rec;
+  f.sg_rec = pl->sg_rec;
+  return f;
+}
+
+static StageArgs blank_args() {
+  StageArgs a;
+  std::memset(&a, 0, sizeof(a));
+  return a;
+}
+
+static int launch_pencil(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s) {
+  const int blocks = pl->d.Ny * pl->d.nKb;
+  pencil_stage_kernel<<<blocks, kNW * 32, pl->smem_pencil, s>>>(pl->ops, pl->d, a);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+// y_backward -> z_cross -> y_forward: HX <- H(state whose x-physical fields are in X)
+static int launch_transforms(jfb_kmm_plan* pl, cudaStream_t s) {
+  const Dims& d = pl->d;
+  dim3 gy(d.Nx, 6, d.Kz / pl->KC);
+  y_backward_kernel<<<gy, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->X, pl->Y);
+  JFB_CHECK_LAUNCH();
+  const int zb = ceil_div((int64_t)d.Nx * d.My, kZRows);
+  z_cross_kernel<<<zb, 256, pl->smem_z, s>>>(pl->ops, d, pl->fz, pl->twz, pl->Y, pl->HZ);
+  JFB_CHECK_LAUNCH();
+  dim3 gf(d.Nx, 3, d.Kz / pl->KC);
+  y_forward_kernel<<<gf, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->HZ, pl->HX);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+static inline int slot(int64_t m) { return (int)(((m % 3) + 3) % 3); }
+
+// u1, u2 of the current state into U1S/U2S (reconstruction).
+static int ensure_explicit(jfb_kmm_plan* pl, cudaStream_t s) {
+  if (pl->explicit_u12) return JFB_OK;
+  StageArgs a = blank_args();
+  a.mode = kReconstruct;
+  const int c = slot(pl->n);
+  a.u0a = pl->U0[c];
+  a.ga = pl->G[c];
+  a.vwa = pl->VW[c];
+  a.X = pl->U1S;   // u1 out
+  a.Hd_out = pl->U2S;  // u2 out
+  int st = launch_pencil(pl, a, s);
+  if (st) return st;
+  pl->explicit_u12 = true;
+  return JFB_OK;
+}
+
+static int ensure_H(jfb_kmm_plan* pl, cudaStream_t s) {
+  if (pl->have_H) return JFB_OK;
+  int st = ensure_explicit(pl, s);
+  if (st) return st;
+  StageArgs a = blank_args();
+  a.mode = kPrologue;
+  const int c = slot(pl->n);
+  a.pu0 = pl->U0[c];
+  a.pu1 = pl->U1S;
+  a.pu2 = pl->U2S;
+  a.X = pl->X;
+  st = launch_pencil(pl, a, s);
+  if (st) return st;
+  st = launch_transforms(pl, s);
+  if (st) return st;
+  pl->have_H = true;
+  return JFB_OK;
+}
+
+// One steady SBDF3 step from ring position m (u^m in slot m % 3).
+static int steady_step(jfb_kmm_plan* pl, int64_t m, cudaStream_t s) {
+  StageArgs a = blank_args();
+  a.mode = kImplicit;
+  a.HX = pl->HX;
+  const int c = slot(m), o1 = slot(m - 1), o2 = slot(m - 2), nw = slot(m + 1);
+  a.c0 = 18.0 / 11.0;
+  a.c1 = -9.0 / 11.0;
+  a.c2 = 2.0 / 11.0;
+  a.cL = 0.0;
+  a.d0 = 18.0 / 11.0;
+  a.d1 = -18.0 / 11.0;
+  a.d2 = 6.0 / 11.0;
+  a.u0a = pl->U0[c];
+  a.u0b = pl->U0[o1];
+  a.u0c = pl->U0[o2];
+  a.ga = pl->G[c];
+  a.gb = pl->G[o1];
+  a.gc = pl->G[o2];
+  a.vwa = pl->VW[c];
+  a.vwb = pl->VW[o1];
+  a.vwc = pl->VW[o2];
+  a.Nup = pl->NU[o1];
+  a.Nuq = pl->NU[o2];
+  a.Ngp = pl->NG[o1];
+  a.Ngq = pl->NG[o2];
+  a.NVWp = pl->NVW[o1];
+  a.NVWq = pl->NVW[o2];
+  a.Nu_out = pl->NU[c];
+  a.Ng_out = pl->NG[c];
+  a.NVW_out = pl->NVW[c];
+  a.fac = packed(pl, pl->steady);
+  a.u0_out = pl->U0[nw];
+  a.g_out = pl->G[nw];
+  a.vw_out = pl->VW[nw];
+  a.X = pl->X;
+  int st = launch_pencil(pl, a, s);
+  if (st) return st;
+  return launch_transforms(pl, s);
+}
+
+// One IMEXRK3 startup step (_step_sbdf3 startup branch).
+static int startup_step(jfb_kmm_plan* pl, cudaStream_t s) {
+  const int64_t m = pl->n;
+  const int c = slot(m), nw = slot(m + 1);
+  for (int rk = 0; rk < 3; ++rk) {
+    StageArgs a = blank_args();
+    a.mode = kImplicit;
+    a.HX = pl->HX;
+    a.c0 = 1.0;
+    a.cL = (kRK3A[rk] + kRK3B[rk]) * pl->cfg.dt / 2.0;
+    a.d0 = kRK3A[rk];
+    a.d1 = kRK3B[rk];
+    const int src = (rk == 0) ? c : nw;
+    a.u0a = pl->U0[src];
+    a.ga = pl->G[src];
+    a.vwa = pl->VW[src];
+    if (rk == 1) {
+      a.Nup = pl->NU[c];
+      a.Ngp = pl->NG[c];
+      a.NVWp = pl->NVW[c];
+    } else if (rk == 2) {
+      a.Nup = pl->NUst;
+      a.Ngp = pl->NGst;
+      a.NVWp = pl->NVWst;
+    }
+    if (rk == 0) {
+      a.Nu_out = pl->NU[c];
+      a.Ng_out = pl->NG[c];
+      a.NVW_out = pl->NVW[c];
+    } else if (rk == 1) {
+      a.Nu_out = pl->NUst;
+      a.Ng_out = pl->NGst;
+      a.NVW_out = pl->NVWst;
+    }
+    a.fac = packed(pl, pl->startup[rk]);
+    a.u0_out = pl->U0[nw];
+    a.g_out = pl->G[nw];
+    a.vw_out = pl->VW[nw];
+    a.X = pl->X;
+    int st = launch_pencil(pl, a, s);
+    if (st) return st;
+    st = launch_transforms(pl, s);
+    if (st) return st;
+  }
+  return JFB_OK;
+}
+
+static void destroy_graphs(jfb_kmm_plan* pl) {
+  for (int k = 0; k < 3; ++k)
+    if (pl->graph[k]) {
+      cudaGraphExecDestroy(pl->graph[k]);
+      pl->graph[k] = nullptr;
+    }
+}
+
+}  // namespace jfb
+
+using namespace jfb;
+
+extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
+  JFB_REQUIRE(cfg && out, "null pointer");
+  *out = nullptr;
+  JFB_REQUIRE(cfg->family == JFB_FAMILY_CHEBYSHEV, "only the Chebyshev family is supported");
+  JFB_REQUIRE(cfg->nonlinear_form == JFB_NONLINEAR_ROTATIONAL,
+              "only the rotational nonlinear form is supported");
+  JFB_REQUIRE(cfg->precision == JFB_PRECISION_FP64, "precision not supported");
+  JFB_REQUIRE(cfg->nx >= 9 && cfg->nx <= 2 * 32 * kMaxRows, "nx out of range [9, 256]");
+  JFB_REQUIRE(cfg->ny >= 4 && cfg->ny % 2 == 0 && cfg->nz >= 4 && cfg->nz % 2 == 0,
+              "ny, nz must be even");
+  JFB_REQUIRE(cfg->dt > 0 && cfg->nu > 0, "dt and nu must be positive");
+  JFB_REQUIRE(cfg->x_hi > cfg->x_lo && cfg->ly > 0 && cfg->lz > 0, "bad domain");
+  jfb_kmm_plan* pl = new jfb_kmm_plan();
+  pl->cfg = *cfg;
+  int st = JFB_OK;
+  auto fail = [&](int code) {
+    jfb_kmm_destroy(pl);
+    return code;
+  };
+  build_host_operators(*cfg, pl->hop);
+  Dims& d = pl->d;
+  d.Nx = cfg->nx;
+  d.nB = cfg->nx - 4;
+  d.nD = cfg->nx - 2;
+  d.Ny = cfg->ny;
+  d.Nz = cfg->nz;
+  d.Kz = cfg->nz / 2;
+  d.P = d.Ny * d.Kz;
+  d.My = std::max(cfg->ny, (int)(cfg->pad_y * cfg->ny));
+  d.Mz = std::max(cfg->nz, (int)(cfg->pad_z * cfg->nz));
+  d.nKb = ceil_div(d.Kz, kNW);
+  d.dfx = pl->hop.dfx;
+  d.dfy = pl->hop.dfy;
+  d.dfz = pl->hop.dfz;
+  d.Myz = (2.0 * M_PI / d.dfy) * (2.0 * M_PI / d.dfz);
+  d.nu = cfg->nu;
+  d.dt = cfg->dt;
+  d.uwall = cfg->u_wall;
+  if (!make_fft_plan(d.My, pl->fy) || !make_fft_plan(d.Mz, pl->fz)) {
+    set_error("padded sizes must be of the form 2^a 3^b");
+    return fail(JFB_ERR_ARG);
+  }
+  if (d.Mz < d.Nz || d.My < d.Ny) {
+    set_error("padding must not truncate");
+    return fail(JFB_ERR_ARG);
+  }
+  // kz column chunk of the y transforms: two My x KC complex buffers <= 100 KB
+  pl->KC = d.Kz;
+  while ((size_t)2 * d.My * pl->KC * sizeof(c64) > 100 * 1024 && pl->KC % 2 == 0) pl->KC /= 2;
+  pl->smem_y = (size_t)2 * d.My * pl->KC * sizeof(c64);
+  pl->smem_z = (size_t)2 * d.Mz * kZRows * 3 * sizeof(c64);
+  pl->smem_pencil = (size_t)(6 * d.Nx * kLDW + kNW * 6 * d.Nx + d.Nx) * sizeof(c64);
+  pl->smem_zf = (size_t)2 * d.Nz * (kZRows / 2) * 3 * sizeof(c64);
+  pl->smem_diag = (size_t)kNW * 4 * d.Nx * sizeof(c64) + 2 * kNW * sizeof(double);
+  if (pl->smem_pencil > 227 * 1024 || pl->smem_y > 227 * 1024 || pl->smem_z > 227 * 1024) {
+    set_error("grid too large for the shared-memory tiling");
+    return fail(JFB_ERR_ARG);
+  }
+  cudaFuncSetAttribute(pencil_stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)pl->smem_pencil);
+  cudaFuncSetAttribute(y_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)pl->smem_y);
+  cudaFuncSetAttribute(y_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)pl->smem_y);
+  cudaFuncSetAttribute(z_cross_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)pl->smem_z);
+  cudaFuncSetAttribute(z_forward_real_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)pl->smem_zf);
+  cudaFuncSetAttribute(diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)pl->smem_diag);
+  JFB_CHECK_LAUNCH();
+
+  // constant operators
+  const HostOperators& op = pl->hop;
+  double* p;
+#define UP(field, vec)                       \
+  st = upload(pl, &p, vec);                  \
+  if (st) return fail(st);                   \
+  pl->ops.field = p;
+  UP(Q, op.Q);
+  UP(V, op.V);
+  UP(ns, op.ns);
+  UP(sB0, op.SB.s0);
+  UP(sB2, op.SB.s2);
+  UP(sB4, op.SB.s4);
+  UP(mlo, op.mlo);
+  UP(mdi, op.mdi);
+  UP(mhi, op.mhi);
+  UP(lul, op.lu_l);
+  UP(luu, op.lu_u);
+  UP(xphys, op.xphys);
+  UP(bl2, op.bl2);
+  UP(bl4, op.bl4);
+  UP(bu0, op.bu0);
+  UP(bu2, op.bu2);
+  UP(bu4, op.bu4);
+  UP(fejer, op.fejer);
+#undef UP
+  st = upload(pl, &pl->twy, twiddles(d.My));
+  if (st) return fail(st);
+  st = upload(pl, &pl->twz, twiddles(d.Mz));
+  if (st) return fail(st);
+  if (!make_fft_plan(d.Ny, pl->fny) || !make_fft_plan(d.Nz, pl->fnz)) {
+    set_error("ny, nz must be of the form 2^a 3^b");
+    return fail(JFB_ERR_ARG);
+  }
+  st = upload(pl, &pl->twny, twiddles(d.Ny));
+  if (st) return fail(st);
+  st = upload(pl, &pl->twnz, twiddles(d.Nz));
+  if (st) return fail(st);
+
+  // factors: steady SBDF3 and the three IMEXRK3 startup stages
+  pl->n_modes = (d.Ny / 2) * d.Kz;
+  pl->su_rec = packed_rec_size(d.nB);
+  pl->sg_rec = packed_rec_size(d.nD);
+  st = build_factor_set(pl, kSBDF3Implicit * cfg->dt, pl->steady);
+  if (st) return fail(st);
+  for (int rk = 0; rk < 3; ++rk) {
+    st = build_factor_set(pl, (kRK3A[rk] + kRK3B[rk]) * cfg->dt / 2.0, pl->startup[rk]);
+    if (st) return fail(st);
+  }
+
+  // state rings and work buffers
+  const size_t P = d.P;
+  auto cal = [&](c64** ptr, size_t elems) {
+    return dalloc(pl, (void**)ptr, std::max<size_t>(1, elems) * sizeof(c64));
+  };
+  for (int k = 0; k < 3; ++k) {
+    if ((st = cal(&pl->U0[k], (size_t)d.nB * P))) return fail(st);
+    if ((st = cal(&pl->G[k], (size_t)d.nD * P))) return fail(st);
+    if ((st = cal(&pl->NU[k], (size_t)d.nB * P))) return fail(st);
+    if ((st = cal(&pl->NG[k], (size_t)d.nD * P))) return fail(st);
+    if ((st = cal(&pl->VW[k], d.nD))) return fail(st);
+    if ((st = cal(&pl->NVW[k], d.nD))) return fail(st);
+  }
+  if ((st = cal(&pl->NUst, (size_t)d.nB * P))) return fail(st);
+  if ((st = cal(&pl->NGst, (size_t)d.nD * P))) return fail(st);
+  if ((st = cal(&pl->NVWst, d.nD))) return fail(st);
+  if ((st = cal(&pl->U1S, (size_t)d.nD * P))) return fail(st);
+  if ((st = cal(&pl->U2S, (size_t)d.nD * P))) return fail(st);
+  if ((st = cal(&pl->X, (size_t)6 * d.Nx * P))) return fail(st);
+  if ((st = cal(&pl->Y, (size_t)6 * d.Nx * d.My * d.Kz))) return fail(st);
+  if ((st = cal(&pl->HZ, (size_t)3 * d.Nx * d.My * d.Kz))) return fail(st);
+  if ((st = cal(&pl->HX, (size_t)3 * d.Nx * P))) return fail(st);
+  if ((st = cal(&pl->HD, (size_t)3 * d.nD * P))) return fail(st);
+  pl->diag_blocks = d.Ny * d.nKb;
+  if ((st = dalloc(pl, (void**)&pl->diag_partial, (size_t)2 * pl->diag_blocks * sizeof(double))))
+    return fail(st);
+  if ((st = dalloc(pl, (void**)&pl->diag_mean, (size_t)(8 + d.Nx) * sizeof(double))))
+    return fail(st);
+  JFB_CHECK_CUDA(cudaDeviceSynchronize());
+  *out = pl;
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_destroy(jfb_kmm_plan* pl) {
+  if (!pl) return JFB_OK;
+  destroy_graphs(pl);
+  if (pl->cap) cudaStreamDestroy(pl->cap);
+  for (void* ptr : pl->allocs) cudaFree(ptr);
+  delete pl;
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_get_info(const jfb_kmm_plan* pl, jfb_kmm_info* info) {
+  JFB_REQUIRE(pl && info, "null pointer");
+  const Dims& d = pl->d;
+  info->n_pencils = d.P;
+  info->device_bytes = pl->device_bytes;
+  info->launches_per_step = 4;
+  // stage model: 43 E_s + 18 E_m complex values, E_s = Nx Ny (Nz/2+1), E_m = Nx My (Nz/2+1)
+  const int64_t H = d.Nz / 2 + 1;
+  const int64_t Es = (int64_t)d.Nx * d.Ny * H, Em = (int64_t)d.Nx * d.My * H;
+  info->algorithmic_bytes = (43 * Es + 18 * Em) * 16;
+  info->my = d.My;
+  info->mz = d.Mz;
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_set_state(jfb_kmm_plan* pl, const jfb_kmm_state* s, void* stream) {
+  JFB_REQUIRE(pl && s && s->u0 && s->u1 && s->u2 && s->g, "null pointer");
+  JFB_REQUIRE(s->history_steps >= 0 && s->history_steps <= 2, "history_steps in [0, 2]");
+  cudaStream_t st = (cudaStream_t)stream;
+  const Dims& d = pl->d;
+  pl->n = 0;
+  const int c = slot(0), o1 = slot(-1), o2 = slot(-2);
+  const int blocks = 512;
+  auto half = [&](const void* full, int n, c64* dst) {
+    if (full) to_half_kernel<<<blocks, 256, 0, st>>>((const c64*)full, n, d.Ny, d.Nz, dst);
+    else cudaMemsetAsync(dst, 0, (size_t)n * d.P * sizeof(c64), st);
+  };
+  half(s->u0, d.nB, pl->U0[c]);
+  half(s->g, d.nD, pl->G[c]);
+  half(s->u1, d.nD, pl->U1S);
+  half(s->u2, d.nD, pl->U2S);
+  means_in_kernel<<<1, 128, 0, st>>>((const c64*)s->u1, (const c64*)s->u2, d.nD, d.Ny, d.Nz,
+                                     pl->VW[c]);
+  const int lv[2] = {o1, o2};
+  void* const* sol[2] = {s->solution_old, s->solution_older};
+  void* const* nl[2] = {s->nonlinear_old, s->nonlinear_older};
+  for (int k = 0; k < 2; ++k) {
+    half(sol[k][0], d.nB, pl->U0[lv[k]]);
+    half(sol[k][1], d.nD, pl->G[lv[k]]);
+    real_pair_in_kernel<<<1, 128, 0, st>>>((const double*)sol[k][2],
+                                           (const double*)sol[k][3], d.nD, pl->VW[lv[k]]);
+    half(nl[k][0], d.nB, pl->NU[lv[k]]);
+    half(nl[k][1], d.nD, pl->NG[lv[k]]);
+    real_pair_in_kernel<<<1, 128, 0, st>>>((const double*)nl[k][2], (const double*)nl[k][3],
+                                           d.nD, pl->NVW[lv[k]]);
+  }
+  JFB_CHECK_LAUNCH();
+  pl->hist = (int)s->history_steps;
+  pl->have_state = true;
+  pl->have_H = false;
+  pl->explicit_u12 = true;
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_get_state(jfb_kmm_plan* pl, const jfb_kmm_state* s, void* stream) {
+  JFB_REQUIRE(pl && s, "null pointer");
+  if (!pl->have_state) {
+    set_error("no state loaded");
+    return JFB_ERR_STATE;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const Dims& d = pl->d;
+  int rc = ensure_explicit(pl, st);
+  if (rc) return rc;
+  const int c = slot(pl->n), o1 = slot(pl->n - 1), o2 = slot(pl->n - 2);
+  const int blocks = 512;
+  auto full = [&](const c64* src, int n, void* dst) {
+    if (dst) to_full_kernel<<<blocks, 256, 0, st>>>(src, n, d.Ny, d.Nz, (c64*)dst);
+  };
+  full(pl->U0[c], d.nB, s->u0);
+  full(pl->G[c], d.nD, s->g);
+  full(pl->U1S, d.nD, s->u1);
+  full(pl->U2S, d.nD, s->u2);
+  const int lv[2] = {o1, o2};
+  void* const* sol[2] = {s->solution_old, s->solution_older};
+  void* const* nl[2] = {s->nonlinear_old, s->nonlinear_older};
+  for (int k = 0; k < 2; ++k) {
+    full(pl->U0[lv[k]], d.nB, sol[k][0]);
+    full(pl->G[lv[k]], d.nD, sol[k][1]);
+    real_pair_out_kernel<<<1, 128, 0, st>>>(pl->VW[lv[k]], d.nD, (double*)sol[k][2],
+                                            (double*)sol[k][3]);
+    full(pl->NU[lv[k]], d.nB, nl[k][0]);
+    full(pl->NG[lv[k]], d.nD, nl[k][1]);
+    real_pair_out_kernel<<<1, 128, 0, st>>>(pl->NVW[lv[k]], d.nD, (double*)nl[k][2],
+                                            (double*)nl[k][3]);
+  }
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_advance(jfb_kmm_plan* pl, int64_t steps, void* stream) {
+  JFB_REQUIRE(pl, "null pointer");
+  JFB_REQUIRE(steps >= 0, "steps must be >= 0");
+  if (!pl->have_state) {
+    set_error("no state loaded");
+    return JFB_ERR_STATE;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = ensure_H(pl, s);
+  if (st) return st;
+  while (steps > 0 && pl->hist < 2) {
+    st = startup_step(pl, s);
+    if (st) return st;
+    pl->n += 1;
+    pl->hist += 1;
+    pl->explicit_u12 = false;
+    --steps;
+  }
+  while (steps > 0) {
+    const int k = slot(pl->n);
+    if (!pl->graph[k]) {
+      // Capture one steady step for ring phase k on the private stream; the
+      // instantiated graph is then launched on the caller's stream (which
+      // may be the legacy default stream, where capture is not allowed).
+      if (!pl->cap) JFB_CHECK_CUDA(cudaStreamCreateWithFlags(&pl->cap, cudaStreamNonBlocking));
+      cudaGraph_t g;
+      JFB_CHECK_CUDA(cudaStreamBeginCapture(pl->cap, cudaStreamCaptureModeThreadLocal));
+      st = steady_step(pl, pl->n, pl->cap);
+      cudaError_t ec = cudaStreamEndCapture(pl->cap, &g);
+      if (st) return st;
+      JFB_CHECK_CUDA(ec);
+      JFB_CHECK_CUDA(cudaGraphInstantiate(&pl->graph[k], g, 0));
+      cudaGraphDestroy(g);
+    }
+    JFB_CHECK_CUDA(cudaGraphLaunch(pl->graph[k], s));
+    pl->n += 1;
+    pl->explicit_u12 = false;
+    --steps;
+  }
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_convection(jfb_kmm_plan* pl, void* h0, void* h1, void* h2,
+                                  void* stream) {
+  JFB_REQUIRE(pl && h0 && h1 && h2, "null pointer");
+  if (!pl->have_state) {
+    set_error("no state loaded");
+    return JFB_ERR_STATE;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = ensure_H(pl, s);
+  if (st) return st;
+  StageArgs a = blank_args();
+  a.mode = kHOnly;
+  a.HX = pl->HX;
+  a.Hd_out = pl->HD;
+  st = launch_pencil(pl, a, s);
+  if (st) return st;
+  const Dims& d = pl->d;
+  void* outs[3] = {h0, h1, h2};
+  for (int f = 0; f < 3; ++f)
+    to_full_kernel<<<512, 256, 0, s>>>(pl->HD + (size_t)f * d.nD * d.P, d.nD, d.Ny, d.Nz,
+                                       (c64*)outs[f]);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_state_from_physical(jfb_kmm_plan* pl, const double* u0,
+                                           const double* u1, const double* u2,
+                                           void* stream) {
+  JFB_REQUIRE(pl && u0 && u1 && u2, "null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  Dims d = pl->d;
+  const size_t P = d.P;
+  // z: real Nz -> Kz half spectrum (into HZ as [f][j][y][kz]), scaled 1/Nz
+  const int zb = ceil_div((int64_t)d.Nx * d.Ny, kZRows);
+  z_forward_real_kernel<<<zb, 256, pl->smem_zf, s>>>(d, pl->fnz, pl->twnz, u0, u1, u2,
+                                                     pl->HZ);
+  JFB_CHECK_LAUNCH();
+  // y: forward FFT of length Ny (no truncation), scaled 1/Ny
+  Dims dy = d;
+  dy.My = d.Ny;
+  int KC = d.Kz;
+  while ((size_t)2 * d.Ny * KC * sizeof(c64) > 100 * 1024 && KC % 2 == 0) KC /= 2;
+  dim3 gf(d.Nx, 3, d.Kz / KC);
+  y_forward_kernel<<<gf, 256, (size_t)2 * d.Ny * KC * sizeof(c64), s>>>(dy, pl->fny, KC,
+                                                                        pl->twny, pl->HZ,
+                                                                        pl->HX);
+  JFB_CHECK_LAUNCH();
+  // history reset and x: Shen forward transforms, g = i ky u2 - i kz u1
+  pl->n = 0;
+  for (int k = 0; k < 3; ++k) {
+    JFB_CHECK_CUDA(cudaMemsetAsync(pl->U0[k], 0, (size_t)d.nB * P * sizeof(c64), s));
+    JFB_CHECK_CUDA(cudaMemsetAsync(pl->G[k], 0, (size_t)d.nD * P * sizeof(c64), s));
+    JFB_CHECK_CUDA(cudaMemsetAsync(pl->NU[k], 0, (size_t)d.nB * P * sizeof(c64), s));
+    JFB_CHECK_CUDA(cudaMemsetAsync(pl->NG[k], 0, (size_t)d.nD * P * sizeof(c64), s));
+    JFB_CHECK_CUDA(cudaMemsetAsync(pl->VW[k], 0, (size_t)d.nD * sizeof(c64), s));
+    JFB_CHECK_CUDA(cudaMemsetAsync(pl->NVW[k], 0, (size_t)d.nD * sizeof(c64), s));
+  }
+  StageArgs a = blank_args();
+  a.mode = kFromPhys;
+  a.HX = pl->HX;
+  const int c = slot(0);
+  a.u0_out = pl->U0[c];
+  a.g_out = pl->G[c];
+  a.vw_out = pl->VW[c];
+  a.u1_out = pl->U1S;
+  a.u2_out = pl->U2S;
+  int st = launch_pencil(pl, a, s);
+  if (st) return st;
+  pl->hist = 0;
+  pl->have_state = true;
+  pl->have_H = false;
+  pl->explicit_u12 = true;
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_diagnostics(jfb_kmm_plan* pl, double* out, void* stream) {
+  JFB_REQUIRE(pl && out, "null pointer");
+  if (!pl->have_state) {
+    set_error("no state loaded");
+    return JFB_ERR_STATE;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = ensure_explicit(pl, s);
+  if (st) return st;
+  const Dims& d = pl->d;
+  const int c = slot(pl->n);
+  diag_kernel<<<pl->diag_blocks, kNW * 32, pl->smem_diag, s>>>(
+      pl->ops, d, pl->U0[c], pl->U1S, pl->U2S, pl->diag_partial, pl->diag_mean);
+  JFB_CHECK_LAUNCH();
+  diag_finish_kernel<<<1, 32, 0, s>>>(d, pl->diag_partial, pl->diag_blocks, pl->diag_mean,
+                                      pl->cfg.ly, pl->cfg.lz, pl->cfg.x_lo, pl->cfg.x_hi,
+                                      out);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}

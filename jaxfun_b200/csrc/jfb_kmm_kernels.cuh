@@ -1,0 +1,1013 @@
+// Device kernels of the KMM plane-Couette step (FP64 form).
+//
+// One steady SBDF3 step = four launches:
+//   pencil_stage  per (ky, kz>=0) pencil, along the wall-normal axis x:
+//                 x-forward of the dealiased nonlinear term, Shen projection,
+//                 coefficient-space KMM right-hand sides, SBDF3 (or IMEXRK3
+//                 stage) combination, the per-wavenumber banded solves,
+//                 velocity reconstruction, vorticity and the x-backward of the
+//                 six fields u, omega.
+//   y_backward    zero-padded inverse FFT along y (Ny -> My) of six fields.
+//   z_cross       inverse real FFT along z (Kz -> Mz), base flow, the
+//                 rotational product -(u x omega), forward real FFT (Mz -> Kz).
+//   y_forward     forward FFT along y (My -> Ny) with 3/2-rule truncation.
+// Spectral arrays are laid out [field][x][ky][kz] with kz in [0, Nz/2): the
+// real-field half spectrum (the Nyquist column kz = Nz/2 is masked to zero by
+// the reference, tensorproductspace.py:276-293, and is not stored).
+#pragma once
+
+#include "jfb_common.cuh"
+#include "jfb_fft.cuh"
+
+namespace jfb {
+
+constexpr int kNW = 8;         // pencils (warps) per pencil_stage block
+constexpr int kLDW = kNW + 1;  // padded pencil stride in shared memory
+constexpr int kMaxRows = 4;    // rows per lane in the column-oriented solves (n <= 256)
+
+struct DevOps {
+  const double* Q;   // [n][j] scalar-product quadrature (Nx x Nx)
+  const double* V;   // [j][n] Chebyshev Vandermonde (Nx x Nx)
+  const double* ns;  // norm^2 / df (Nx)
+  const double* sB0;
+  const double* sB2;
+  const double* sB4;  // biharmonic stencil diagonals (nB)
+  const double* mlo;
+  const double* mdi;
+  const double* mhi;  // Dirichlet mass tri-band (nD)
+  const double* lul;
+  const double* luu;    // its LU (nD)
+  const double* xphys;  // physical wall-normal nodes (Nx)
+  const double* bl2;
+  const double* bl4;
+  const double* bu0;
+  const double* bu2;
+  const double* bu4;     // biharmonic mass LU (nB)
+  const double* fejer;   // Fejer-I weights (Nx)
+};
+
+struct Dims {
+  int Nx, nB, nD, Ny, Nz, Kz, P, My, Mz, nKb;
+  double dfx, dfy, dfz, Myz, nu, dt, uwall;
+};
+
+struct PackedFactors {
+  const double* su;  // n_modes records of su_rec doubles
+  const double* sg;
+  const double* s00;  // one record (sg layout, n = nD)
+  int su_rec, sg_rec;
+};
+
+enum StageMode { kPrologue = 0, kImplicit = 1, kHOnly = 2, kReconstruct = 3, kFromPhys = 4 };
+
+struct StageArgs {
+  int mode;
+  const c64* HX;  // phase A input: 3 x [Nx][P]
+  double c0, c1, c2, cL, d0, d1, d2;
+  const c64 *u0a, *u0b, *u0c;
+  const c64 *ga, *gb, *gc;
+  const c64 *vwa, *vwb, *vwc;
+  const c64 *Nup, *Nuq, *Ngp, *Ngq, *NVWp, *NVWq;
+  c64 *Nu_out, *Ng_out, *NVW_out;
+  PackedFactors fac;
+  c64 *u0_out, *g_out, *vw_out;
+  const c64 *pu0, *pu1, *pu2;  // prologue: explicit fields
+  c64* X;                      // 6 x [Nx][P]
+  c64* Hd_out;                 // kHOnly: 3 x [nD][P]
+  c64 *u1_out, *u2_out;        // kFromPhys: tangential velocity (nD x P)
+};
+
+__host__ __device__ inline int packed_rec_size(int n) {
+  const int m0 = (n + 1) / 2, m1 = n / 2;
+  return 2 * n + m0 * (m0 + 1) / 2 + m1 * (m1 + 1) / 2;
+}
+
+// ---------------------------------------------------------------------------
+// Warp-level helpers (all lanes of the warp call them; arrays in smem).
+// ---------------------------------------------------------------------------
+
+// d = scale * chebder(c) on a length-L coefficient vector; in place allowed.
+// d_n = sum_{m > n, m - n odd} 2 m c_m, d_0 halved (Chebyshev.py:319-353).
+__device__ void chebder_warp(const c64* c, c64* d, int L, double scale, int lane) {
+  const int K = (L + 31) / 32;
+  const int lo = lane * K, hi = min(L, lo + K);
+  c64 se = cmk(0.0, 0.0), so = cmk(0.0, 0.0);
+  for (int m = lo; m < hi; ++m) {
+    const c64 e = (2.0 * m) * c[m];
+    if (m & 1) so = so + e; else se = se + e;
+  }
+  // inclusive suffix sums over lanes >= lane
+  c64 ie = se, io = so;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double er = __shfl_down_sync(0xffffffffu, ie.re, off);
+    const double ei = __shfl_down_sync(0xffffffffu, ie.im, off);
+    const double orr = __shfl_down_sync(0xffffffffu, io.re, off);
+    const double oi = __shfl_down_sync(0xffffffffu, io.im, off);
+    if (lane + off < 32) {
+      ie = ie + cmk(er, ei);
+      io = io + cmk(orr, oi);
+    }
+  }
+  c64 run_e = ie - se, run_o = io - so;  // sums over lanes > lane
+  __syncwarp();
+  for (int n = hi - 1; n >= lo; --n) {
+    const c64 cn = c[n];
+    c64 dn = (n & 1) ? run_e : run_o;
+    if (n == 0) dn = 0.5 * dn;
+    d[n] = scale * dn;
+    const c64 e = (2.0 * n) * cn;
+    if (n & 1) run_o = run_o + e; else run_e = run_e + e;
+  }
+  __syncwarp();
+}
+
+// out = S_B^T a  (length Nx from nB)
+__device__ __forceinline__ void apply_SBT(const DevOps& o, const Dims& d, const c64* a,
+                                          c64* out, int lane) {
+  for (int n = lane; n < d.Nx; n += 32) {
+    c64 v = cmk(0.0, 0.0);
+    if (n < d.nB) v = v + o.sB0[n] * a[n];
+    if (n >= 2 && n - 2 < d.nB) v = v + o.sB2[n - 2] * a[n - 2];
+    if (n >= 4 && n - 4 < d.nB) v = v + o.sB4[n - 4] * a[n - 4];
+    out[n] = v;
+  }
+  __syncwarp();
+}
+// out = S_D^T a  (length Nx from nD)
+__device__ __forceinline__ void apply_SDT(const Dims& d, const c64* a, c64* out, int lane) {
+  for (int n = lane; n < d.Nx; n += 32) {
+    c64 v = cmk(0.0, 0.0);
+    if (n < d.nD) v = a[n];
+    if (n >= 2 && n - 2 < d.nD) v = v - a[n - 2];
+    out[n] = v;
+  }
+  __syncwarp();
+}
+// out[i] = scale * (S_B (ns .* c))[i]   (length nB)
+__device__ __forceinline__ void apply_SB_ns(const DevOps& o, const Dims& d, const c64* c,
+                                            c64* out, double scale, int lane) {
+  for (int i = lane; i < d.nB; i += 32) {
+    c64 v = (o.sB0[i] * o.ns[i]) * c[i];
+    v = v + (o.sB2[i] * o.ns[i + 2]) * c[i + 2];
+    v = v + (o.sB4[i] * o.ns[i + 4]) * c[i + 4];
+    out[i] = scale * v;
+  }
+  __syncwarp();
+}
+// out[i] = scale * (S_D (ns .* c))[i]   (length nD)
+__device__ __forceinline__ void apply_SD_ns(const DevOps& o, const Dims& d, const c64* c,
+                                            c64* out, double scale, int lane) {
+  for (int i = lane; i < d.nD; i += 32) {
+    const c64 v = o.ns[i] * c[i] - o.ns[i + 2] * c[i + 2];
+    out[i] = scale * v;
+  }
+  __syncwarp();
+}
+
+// Tri-band (offsets -2, 0, 2) no-pivot LU solve of the Dirichlet mass matrix,
+// in place on `b` (length nD).  Two lanes (one per parity) per vector; `which`
+// selects the lane pair so several vectors can be solved concurrently.
+__device__ __forceinline__ void mass_solve_lane(const DevOps& o, const Dims& d, c64* b,
+                                                int par) {
+  for (int i = par + 2; i < d.nD; i += 2) b[i] = b[i] - o.lul[i] * b[i - 2];
+  int last = d.nD - 1;
+  if ((last & 1) != par) last -= 1;
+  for (int i = last; i >= 0; i -= 2) {
+    c64 v = b[i];
+    if (i + 2 < d.nD) v = v - o.mhi[i] * b[i + 2];
+    b[i] = (1.0 / o.luu[i]) * v;
+  }
+}
+
+// No-pivot LU solve of the biharmonic mass matrix (offsets -4..4), in place,
+// one lane per parity class.
+__device__ __forceinline__ void bmass_solve_lane(const DevOps& o, const Dims& d, c64* b,
+                                                 int par) {
+  for (int i = par; i < d.nB; i += 2) {
+    c64 v = b[i];
+    if (i >= 2) v = v - o.bl2[i] * b[i - 2];
+    if (i >= 4) v = v - o.bl4[i] * b[i - 4];
+    b[i] = v;
+  }
+  int last = d.nB - 1;
+  if ((last & 1) != par) last -= 1;
+  for (int i = last; i >= 0; i -= 2) {
+    c64 v = b[i];
+    if (i + 2 < d.nB) v = v - o.bu2[i] * b[i + 2];
+    if (i + 4 < d.nB) v = v - o.bu4[i] * b[i + 4];
+    b[i] = (1.0 / o.bu0[i]) * v;
+  }
+}
+
+// Forward elimination with the unit-lower factor of a packed record
+// (L[i, i-2], L[i, i-4]) for one parity; single lane.
+__device__ __forceinline__ void fwd_elim_lane(const double* rec, int n, c64* y, int par) {
+  for (int i = par; i < n; i += 2) {
+    c64 v = y[i];
+    if (i >= 2) v = v - rec[2 * i] * y[i - 2];
+    if (i >= 4) v = v - rec[2 * i + 1] * y[i - 4];
+    y[i] = v;
+  }
+}
+
+// Column-oriented back substitution of one parity class (size m, packed
+// column-major upper triangle with reciprocal diagonal) held in `y` at
+// indices 2 r + par.  All lanes participate.
+__device__ __forceinline__ void back_subst_warp(const double* __restrict__ Up, int m, c64* y,
+                                                int par, int lane) {
+  c64 yr[kMaxRows];
+#pragma unroll
+  for (int s = 0; s < kMaxRows; ++s) {
+    const int r = lane + 32 * s;
+    yr[s] = (r < m) ? y[2 * r + par] : cmk(0.0, 0.0);
+  }
+  for (int c = m - 1; c >= 0; --c) {
+    const int owner = c & 31, slot = c >> 5;
+    const int col = c * (c + 1) / 2;
+    c64 xc = cmk(0.0, 0.0);
+#pragma unroll
+    for (int s = 0; s < kMaxRows; ++s)
+      if (s == slot && lane == owner) {
+        xc = Up[col + c] * yr[s];
+        yr[s] = xc;
+      }
+    xc.re = __shfl_sync(0xffffffffu, xc.re, owner);
+    xc.im = __shfl_sync(0xffffffffu, xc.im, owner);
+#pragma unroll
+    for (int s = 0; s < kMaxRows; ++s) {
+      const int r = lane + 32 * s;
+      if (r < c) yr[s] = yr[s] - Up[col + r] * xc;
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < kMaxRows; ++s) {
+    const int r = lane + 32 * s;
+    if (r < m) y[2 * r + par] = yr[s];
+  }
+  __syncwarp();
+}
+
+// Solve a packed system of size n in place on y (both parities).
+__device__ __forceinline__ void packed_solve_warp(const double* __restrict__ rec, int n,
+                                                  c64* y, int lane) {
+  if (lane < 2) fwd_elim_lane(rec, n, y, lane);
+  __syncwarp();
+  const int m0 = (n + 1) / 2, m1 = n / 2;
+  const double* U0 = rec + 2 * n;
+  const double* U1 = U0 + m0 * (m0 + 1) / 2;
+  back_subst_warp(U0, m0, y, 0, lane);
+  back_subst_warp(U1, m1, y, 1, lane);
+}
+
+// Velocity reconstruction (channelflow_kmm.py:855-870): from u0 (TB, in A3)
+// and g (TD, in A4) form uo0 = S_B^T u0 (-> A5), f = P_TD(d/dx uo0),
+// u1 = i(ky f + kz g)/k^2 (-> A0), u2 = i(kz f - ky g)/k^2 (-> A1); the
+// ky = kz = 0 pencil takes the real mean-flow vectors (v00, w00) from vw.
+__device__ void reconstruct_warp(const DevOps& o, const Dims& d, const c64* A3,
+                                 const c64* A4, const c64* vw, bool mean_pencil,
+                                 double kyp, double kzp, c64* A0, c64* A1, c64* A2,
+                                 c64* A5, int lane) {
+  apply_SBT(o, d, A3, A5, lane);            // A5 = uo0 = S_B^T u0
+  chebder_warp(A5, A0, d.Nx, d.dfx, lane);   // A0 = d/dx uo0
+  apply_SD_ns(o, d, A0, A2, 1.0, lane);      // A2 = S_D(ns du)
+  if (lane < 2) mass_solve_lane(o, d, A2, lane);  // f = projection into TD
+  __syncwarp();
+  const double k2 = kyp * kyp + kzp * kzp;
+  const double inv = (k2 == 0.0) ? 1.0 : 1.0 / k2;
+  for (int i = lane; i < d.nD; i += 32) {
+    const c64 f = A2[i], g = A4[i];
+    c64 u1 = mul_i((kyp * inv) * f + (kzp * inv) * g);
+    c64 u2 = mul_i((kzp * inv) * f - (kyp * inv) * g);
+    if (mean_pencil) {
+      u1 = cmk(vw[i].re, 0.0);
+      u2 = cmk(vw[i].im, 0.0);
+    }
+    A0[i] = u1;
+    A1[i] = u2;
+  }
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// CTA-level small GEMMs against the x-transform matrices.
+// out[(f * R + r) * kLDW + w] = sum_k A[r * K + k] * in(f, k, w)
+// ---------------------------------------------------------------------------
+template <typename InFn>
+__device__ __forceinline__ void cta_gemm(const double* __restrict__ A, int R, int K, int NF,
+                                         InFn in, c64* out) {
+  const int C = NF * kNW;
+  const int G = blockDim.x / C;
+  const int t = threadIdx.x;
+  const int col = t % C, g = t / C;
+  if (g < G) {
+    const int f = col / kNW, w = col % kNW;
+    for (int r0 = g; r0 < R; r0 += 8 * G) {
+      c64 acc[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) acc[q] = cmk(0.0, 0.0);
+      for (int k = 0; k < K; ++k) {
+        const c64 x = in(f, k, w);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int r = r0 + q * G;
+          if (r < R) {
+            const double a = __ldg(A + (size_t)r * K + k);
+            acc[q] = cmk(acc[q].re + a * x.re, acc[q].im + a * x.im);
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int r = r0 + q * G;
+        if (r < R) out[(f * R + r) * kLDW + w] = acc[q];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pencil_stage: see file header.  Block = kNW warps, one pencil per warp.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, StageArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  c64* R1 = reinterpret_cast<c64*>(smem_raw);  // 6 * Nx * kLDW
+  c64* ARR = R1 + 6 * d.Nx * kLDW;              // kNW * 6 * Nx
+  c64* sVW = ARR + kNW * 6 * d.Nx;              // Nx
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int kyi = blockIdx.x / d.nKb;
+  const int kz0 = (blockIdx.x % d.nKb) * kNW;
+  const int p0 = kyi * d.Kz + kz0;
+  const int nvalid = min(kNW, d.Kz - kz0);
+  const int ky = (kyi < d.Ny / 2) ? kyi : kyi - d.Ny;
+  const bool nyq = (kyi == d.Ny / 2);
+  const int kz = kz0 + warp;
+  const bool active = (warp < nvalid) && !nyq;
+  const int p = p0 + warp;
+  const double kyp = ky * d.dfy, kzp = kz * d.dfz;
+  const double k2 = kyp * kyp + kzp * kzp;
+  const bool mean_pencil = active && ky == 0 && kz == 0;
+  const int mode_idx = (ky < 0 ? -ky : ky) * d.Kz + kz;
+  c64* A0 = ARR + (warp * 6 + 0) * d.Nx;
+  c64* A1 = A0 + d.Nx;
+  c64* A2 = A1 + d.Nx;
+  c64* A3 = A2 + d.Nx;
+  c64* A4 = A3 + d.Nx;
+  c64* A5 = A4 + d.Nx;
+  const size_t P = (size_t)d.P;
+
+  // ---------------- reconstruction only (u1, u2 of a stored state) --------
+  if (a.mode == kReconstruct) {
+    if (active) {
+      for (int i = lane; i < d.nB; i += 32) A3[i] = a.u0a[(size_t)i * P + p];
+      for (int i = lane; i < d.nD; i += 32) {
+        A4[i] = a.ga[(size_t)i * P + p];
+        if (mean_pencil) sVW[i] = a.vwa[i];
+      }
+      __syncwarp();
+      reconstruct_warp(o, d, A3, A4, sVW, mean_pencil, kyp, kzp, A0, A1, A2, A5, lane);
+      for (int i = lane; i < d.nD; i += 32) {
+        a.X[(size_t)i * P + p] = A0[i];
+        a.Hd_out[(size_t)i * P + p] = A1[i];
+      }
+    } else if (warp < nvalid) {
+      for (int i = lane; i < d.nD; i += 32) {
+        a.X[(size_t)i * P + p] = cmk(0.0, 0.0);
+        a.Hd_out[(size_t)i * P + p] = cmk(0.0, 0.0);
+      }
+    }
+    return;
+  }
+
+  // ---------------- phase A: nonlinear term of the current state ----------
+  if (a.mode != kPrologue) {
+    // cooperative load of the x-physical H fields into R1[0..2]
+    for (int idx = threadIdx.x; idx < 3 * d.Nx * kNW; idx += blockDim.x) {
+      const int w = idx % kNW, fi = idx / kNW;
+      c64 v = cmk(0.0, 0.0);
+      if (w < nvalid && !nyq) v = a.HX[(size_t)fi * P + p0 + w];
+      R1[fi * kLDW + w] = v;
+    }
+    __syncthreads();
+    // scalar products (T_n, H_f)_w for the 3 fields -> R1[3..5]
+    c64* sT = R1 + 3 * d.Nx * kLDW;
+    cta_gemm(o.Q, d.Nx, d.Nx, 3,
+             [&](int f, int k, int w) { return R1[(f * d.Nx + k) * kLDW + w]; }, sT);
+    __syncthreads();
+    if (a.mode == kFromPhys) {
+      // TB.forward(u0), TD.forward(u1), TD.forward(u2), mask, g = i ky u2 - i kz u1
+      // (channelflow_kmm.py:677-683)
+      if (active) {
+        for (int i = lane; i < d.nB; i += 32) {
+          const c64* t = sT + warp;
+          A0[i] = o.sB0[i] * t[i * kLDW] + o.sB2[i] * t[(i + 2) * kLDW] +
+                  o.sB4[i] * t[(i + 4) * kLDW];
+        }
+        for (int f = 1; f < 3; ++f) {
+          c64* out = (f == 1) ? A1 : A2;
+          for (int i = lane; i < d.nD; i += 32)
+            out[i] = sT[(f * d.Nx + i) * kLDW + warp] - sT[(f * d.Nx + i + 2) * kLDW + warp];
+        }
+        __syncwarp();
+        if (lane < 2) bmass_solve_lane(o, d, A0, lane);
+        else if (lane < 6) mass_solve_lane(o, d, (lane < 4) ? A1 : A2, lane & 1);
+        __syncwarp();
+        for (int i = lane; i < d.nB; i += 32) a.u0_out[(size_t)i * P + p] = A0[i];
+        for (int i = lane; i < d.nD; i += 32) {
+          const c64 u1 = A1[i], u2 = A2[i];
+          a.u1_out[(size_t)i * P + p] = u1;
+          a.u2_out[(size_t)i * P + p] = u2;
+          a.g_out[(size_t)i * P + p] = mul_i(kyp * u2 - kzp * u1);
+          if (mean_pencil) a.vw_out[i] = cmk(u1.re, u2.re);
+        }
+      } else if (warp < nvalid) {
+        for (int i = lane; i < d.nD; i += 32) {
+          if (i < d.nB) a.u0_out[(size_t)i * P + p] = cmk(0.0, 0.0);
+          a.u1_out[(size_t)i * P + p] = cmk(0.0, 0.0);
+          a.u2_out[(size_t)i * P + p] = cmk(0.0, 0.0);
+          a.g_out[(size_t)i * P + p] = cmk(0.0, 0.0);
+        }
+      }
+      return;
+    }
+    if (active) {
+      // S_D (T_n, H)_w -> A0..A2, then Dirichlet mass solves
+      for (int f = 0; f < 3; ++f) {
+        c64* out = (f == 0) ? A0 : (f == 1) ? A1 : A2;
+        for (int i = lane; i < d.nD; i += 32)
+          out[i] = sT[(f * d.Nx + i) * kLDW + warp] - sT[(f * d.Nx + i + 2) * kLDW + warp];
+      }
+      __syncwarp();
+      if (lane < 6) {
+        c64* b = (lane >> 1) == 0 ? A0 : (lane >> 1) == 1 ? A1 : A2;
+        mass_solve_lane(o, d, b, lane & 1);
+      }
+      __syncwarp();
+    }
+    if (a.mode == kHOnly) {
+      if (active)
+        for (int f = 0; f < 3; ++f) {
+          const c64* src = (f == 0) ? A0 : (f == 1) ? A1 : A2;
+          for (int i = lane; i < d.nD; i += 32) a.Hd_out[((size_t)f * d.nD + i) * P + p] = src[i];
+        }
+      else if (warp < nvalid)
+        for (int f = 0; f < 3; ++f)
+          for (int i = lane; i < d.nD; i += 32)
+            a.Hd_out[((size_t)f * d.nD + i) * P + p] = cmk(0.0, 0.0);
+      return;
+    }
+    if (active) {
+      // mean-flow nonlinear rows: -(M00 Re H1), -(M00 Re H2)  packed as re/im
+      if (mean_pencil) {
+        for (int i = lane; i < d.nD; i += 32) {
+          double v = o.mdi[i] * A1[i].re, w = o.mdi[i] * A2[i].re;
+          if (i >= 2) {
+            v += o.mlo[i] * A1[i - 2].re;
+            w += o.mlo[i] * A2[i - 2].re;
+          }
+          if (i + 2 < d.nD) {
+            v += o.mhi[i] * A1[i + 2].re;
+            w += o.mhi[i] * A2[i + 2].re;
+          }
+          sVW[i] = cmk(-v, -w);
+          if (a.NVW_out) a.NVW_out[i] = cmk(-v, -w);
+        }
+        __syncwarp();
+      }
+      // orthogonal coefficients Ho_f = S_D^T H_f : A3 <- Ho0, A4 <- Ho1, A5 <- Ho2
+      apply_SDT(d, A0, A3, lane);
+      apply_SDT(d, A1, A4, lane);
+      apply_SDT(d, A2, A5, lane);
+      // t = i ky Ho1 + i kz Ho2  -> A0 ;  Hg = i kz Ho1 - i ky Ho2 -> A1
+      for (int n = lane; n < d.Nx; n += 32) {
+        const c64 h1 = A4[n], h2 = A5[n];
+        A0[n] = mul_i(kyp * h1 + kzp * h2);
+        A1[n] = mul_i(kzp * h1 - kyp * h2);
+      }
+      __syncwarp();
+      chebder_warp(A0, A2, d.Nx, d.dfx, lane);  // A2 = d/dx t
+      for (int n = lane; n < d.Nx; n += 32) A2[n] = A2[n] + k2 * A3[n];  // Hu
+      __syncwarp();
+      // Nu = Myz S_B(ns Hu) -> A3 ; Ng = Myz S_D(ns Hg) -> A4
+      apply_SB_ns(o, d, A2, A3, d.Myz, lane);
+      apply_SD_ns(o, d, A1, A4, d.Myz, lane);
+      if (a.Nu_out)
+        for (int i = lane; i < d.nB; i += 32) a.Nu_out[(size_t)i * P + p] = A3[i];
+      if (a.Ng_out)
+        for (int i = lane; i < d.nD; i += 32) a.Ng_out[(size_t)i * P + p] = A4[i];
+
+      // ---- right-hand side of Su: Mu (c0 ua + c1 ub + c2 uc) + cL Lu ua + dt N ----
+      for (int i = lane; i < d.nB; i += 32) {
+        const size_t gi = (size_t)i * P + p;
+        c64 v = a.c0 * a.u0a[gi];
+        if (a.c1 != 0.0) v = v + a.c1 * a.u0b[gi];
+        if (a.c2 != 0.0) v = v + a.c2 * a.u0c[gi];
+        A0[i] = v;
+      }
+      __syncwarp();
+      apply_SBT(o, d, A0, A2, lane);            // A2 = S_B^T comb
+      chebder_warp(A2, A5, d.Nx, d.dfx, lane);   // A5 = D comb
+      chebder_warp(A5, A0, d.Nx, d.dfx, lane);   // A0 = D^2 comb
+      for (int n = lane; n < d.Nx; n += 32) A2[n] = A0[n] - k2 * A2[n];
+      __syncwarp();
+      if (a.cL != 0.0) {
+        // + cL nu (D^4 - 2 k2 D^2 + k2^2) S_B^T ua
+        for (int i = lane; i < d.nB; i += 32) A1[i] = a.u0a[(size_t)i * P + p];
+        __syncwarp();
+        apply_SBT(o, d, A1, A0, lane);           // A0 = w
+        chebder_warp(A0, A5, d.Nx, d.dfx, lane);
+        chebder_warp(A5, A1, d.Nx, d.dfx, lane);  // A1 = D^2 w
+        const double s = a.cL * d.nu;
+        for (int n = lane; n < d.Nx; n += 32)
+          A2[n] = A2[n] + s * (k2 * k2 * A0[n] - (2.0 * k2) * A1[n]);
+        __syncwarp();
+        chebder_warp(A1, A5, d.Nx, d.dfx, lane);
+        chebder_warp(A5, A0, d.Nx, d.dfx, lane);  // A0 = D^4 w
+        for (int n = lane; n < d.Nx; n += 32) A2[n] = A2[n] + s * A0[n];
+        __syncwarp();
+      }
+      apply_SB_ns(o, d, A2, A0, d.Myz, lane);  // A0 = mass rows (nB)
+      for (int i = lane; i < d.nB; i += 32) {
+        const size_t gi = (size_t)i * P + p;
+        c64 nl = a.d0 * A3[i];
+        if (a.d1 != 0.0) nl = nl + a.d1 * a.Nup[gi];
+        if (a.d2 != 0.0) nl = nl + a.d2 * a.Nuq[gi];
+        A3[i] = A0[i] + d.dt * nl;  // rhs_u
+      }
+      __syncwarp();
+
+      // ---- right-hand side of Sg: Mg comb_g + cL Lg ga + dt N ----
+      for (int i = lane; i < d.nD; i += 32) {
+        const size_t gi = (size_t)i * P + p;
+        c64 v = a.c0 * a.ga[gi];
+        if (a.c1 != 0.0) v = v + a.c1 * a.gb[gi];
+        if (a.c2 != 0.0) v = v + a.c2 * a.gc[gi];
+        A0[i] = v;
+      }
+      __syncwarp();
+      apply_SDT(d, A0, A2, lane);  // A2 = S_D^T comb
+      if (a.cL != 0.0) {
+        for (int i = lane; i < d.nD; i += 32) A1[i] = a.ga[(size_t)i * P + p];
+        __syncwarp();
+        apply_SDT(d, A1, A0, lane);  // A0 = w
+        chebder_warp(A0, A5, d.Nx, d.dfx, lane);
+        chebder_warp(A5, A1, d.Nx, d.dfx, lane);  // A1 = D^2 w
+        const double s = a.cL * d.nu;
+        for (int n = lane; n < d.Nx; n += 32) A2[n] = A2[n] + s * (A1[n] - k2 * A0[n]);
+        __syncwarp();
+      }
+      apply_SD_ns(o, d, A2, A0, d.Myz, lane);
+      for (int i = lane; i < d.nD; i += 32) {
+        const size_t gi = (size_t)i * P + p;
+        c64 nl = a.d0 * A4[i];
+        if (a.d1 != 0.0) nl = nl + a.d1 * a.Ngp[gi];
+        if (a.d2 != 0.0) nl = nl + a.d2 * a.Ngq[gi];
+        A4[i] = A0[i] + d.dt * nl;  // rhs_g
+      }
+      __syncwarp();
+
+      // ---- mean flow (ky = kz = 0): M00 comb + cL L00 + dt N  -> sVW ----
+      if (mean_pencil) {
+        for (int i = lane; i < d.nD; i += 32) {
+          c64 v = a.c0 * a.vwa[i];
+          if (a.c1 != 0.0) v = v + a.c1 * a.vwb[i];
+          if (a.c2 != 0.0) v = v + a.c2 * a.vwc[i];
+          A0[i] = v;
+        }
+        __syncwarp();
+        apply_SDT(d, A0, A2, lane);
+        if (a.cL != 0.0) {
+          for (int i = lane; i < d.nD; i += 32) A1[i] = a.vwa[i];
+          __syncwarp();
+          apply_SDT(d, A1, A0, lane);
+          chebder_warp(A0, A5, d.Nx, d.dfx, lane);
+          chebder_warp(A5, A1, d.Nx, d.dfx, lane);
+          for (int n = lane; n < d.Nx; n += 32) A2[n] = A2[n] + (a.cL * d.nu) * A1[n];
+          __syncwarp();
+        }
+        apply_SD_ns(o, d, A2, A0, 1.0, lane);
+        for (int i = lane; i < d.nD; i += 32) {
+          c64 nl = a.d0 * sVW[i];
+          if (a.d1 != 0.0) nl = nl + a.d1 * a.NVWp[i];
+          if (a.d2 != 0.0) nl = nl + a.d2 * a.NVWq[i];
+          sVW[i] = A0[i] + d.dt * nl;
+        }
+        __syncwarp();
+      }
+
+      // ---- solves ----
+      const double* rec_u = a.fac.su + (size_t)mode_idx * a.fac.su_rec;
+      const double* rec_g = a.fac.sg + (size_t)mode_idx * a.fac.sg_rec;
+      packed_solve_warp(rec_u, d.nB, A3, lane);
+      packed_solve_warp(rec_g, d.nD, A4, lane);
+      if (mean_pencil) {
+        packed_solve_warp(a.fac.s00, d.nD, sVW, lane);
+        for (int i = lane; i < d.nD; i += 32) a.vw_out[i] = sVW[i];
+        __syncwarp();
+      }
+      for (int i = lane; i < d.nB; i += 32) a.u0_out[(size_t)i * P + p] = A3[i];
+      for (int i = lane; i < d.nD; i += 32) a.g_out[(size_t)i * P + p] = A4[i];
+
+      reconstruct_warp(o, d, A3, A4, sVW, mean_pencil, kyp, kzp, A0, A1, A2, A5, lane);
+    }
+  } else if (active) {
+    // prologue: explicit u0, u1, u2
+    for (int i = lane; i < d.nB; i += 32) A3[i] = a.pu0[(size_t)i * P + p];
+    for (int i = lane; i < d.nD; i += 32) {
+      A0[i] = a.pu1[(size_t)i * P + p];
+      A1[i] = a.pu2[(size_t)i * P + p];
+    }
+    __syncwarp();
+    apply_SBT(o, d, A3, A5, lane);
+  }
+
+  // ---------------- phase B: u and omega in orthogonal coefficients -------
+  if (active) {
+    // A5 = uo0 (already), A0 <- uo1, A1 <- uo2 (in place, descending)
+    if (lane == 0) {
+      for (int n = d.Nx - 1; n >= 0; --n) {
+        c64 v = (n < d.nD) ? A0[n] : cmk(0.0, 0.0);
+        if (n >= 2) v = v - A0[n - 2];
+        A0[n] = v;
+      }
+    } else if (lane == 1) {
+      for (int n = d.Nx - 1; n >= 0; --n) {
+        c64 v = (n < d.nD) ? A1[n] : cmk(0.0, 0.0);
+        if (n >= 2) v = v - A1[n - 2];
+        A1[n] = v;
+      }
+    }
+    __syncwarp();
+    chebder_warp(A1, A3, d.Nx, d.dfx, lane);  // A3 = D uo2
+    chebder_warp(A0, A4, d.Nx, d.dfx, lane);  // A4 = D uo1
+    for (int n = lane; n < d.Nx; n += 32) {
+      const c64 u0 = A5[n], u1 = A0[n], u2 = A1[n];
+      A2[n] = mul_i(kyp * u2 - kzp * u1);        // omega_0
+      A3[n] = mul_i(kzp * u0) - A3[n];           // omega_1
+      A4[n] = A4[n] - mul_i(kyp * u0);           // omega_2
+    }
+    __syncwarp();
+  } else {
+    for (int n = lane; n < 6 * d.Nx; n += 32) A0[n] = cmk(0.0, 0.0);
+    __syncwarp();
+  }
+  __syncthreads();
+  // x-backward of the six fields: field order (u0, u1, u2, w0, w1, w2)
+  // lives in arrays (A5, A0, A1, A2, A3, A4).
+  cta_gemm(o.V, d.Nx, d.Nx, 6,
+           [&](int f, int k, int w) {
+             const int arr = (f == 0) ? 5 : f - 1;
+             return ARR[(w * 6 + arr) * d.Nx + k];
+           },
+           R1);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < 6 * d.Nx * kNW; idx += blockDim.x) {
+    const int w = idx % kNW, fi = idx / kNW;
+    if (w < nvalid) a.X[(size_t)fi * P + p0 + w] = R1[fi * kLDW + w];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// y_backward: per (x-plane, field): pad Ny -> My (middle zeros), inverse FFT.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) y_backward_kernel(Dims d, FFTPlan plan, int KC,
+                                                         const c64* __restrict__ tw,
+                                                         const c64* __restrict__ X,
+                                                         c64* __restrict__ Y) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  c64* A = reinterpret_cast<c64*>(smem_raw);
+  c64* B = A + d.My * KC;
+  const int j = blockIdx.x, f = blockIdx.y, kc0 = blockIdx.z * KC;
+  const c64* src = X + ((size_t)f * d.Nx + j) * d.P + kc0;
+  const int half = d.Ny / 2;
+  for (int idx = threadIdx.x; idx < d.My * KC; idx += blockDim.x) {
+    const int kz = idx % KC, r = idx / KC;
+    c64 v = cmk(0.0, 0.0);
+    if (r < half) v = src[r * d.Kz + kz];
+    else if (r >= d.My - half) v = src[(r - d.My + d.Ny) * d.Kz + kz];
+    A[idx] = v;
+  }
+  __syncthreads();
+  c64* res = fft_columns<double>(A, B, plan, KC, KC, tw, +1);
+  c64* dst = Y + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
+  for (int idx = threadIdx.x; idx < d.My * KC; idx += blockDim.x) {
+    const int kz = idx % KC, r = idx / KC;
+    dst[(size_t)r * d.Kz + kz] = res[idx];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z_cross: per group of 4 (x, y) rows.  Six half spectra -> three complex
+// inverse FFTs (two real fields packed per transform), base flow, the
+// product -(u x omega), then two packed forward transforms per row pair.
+// ---------------------------------------------------------------------------
+constexpr int kZRows = 4;
+
+__global__ void __launch_bounds__(256) z_cross_kernel(DevOps o, Dims d, FFTPlan plan,
+                                                      const c64* __restrict__ tw,
+                                                      const c64* __restrict__ Y,
+                                                      c64* __restrict__ HZ) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NC = kZRows * 3;  // packed columns
+  c64* A = reinterpret_cast<c64*>(smem_raw);
+  c64* B = A + d.Mz * NC;
+  const int row0 = blockIdx.x * kZRows;  // row = j * My + y
+  const int nrows = d.Nx * d.My;
+  const size_t plane = (size_t)d.Nx * d.My * d.Kz;
+  // build the Hermitian-extended packed spectra Z = A_f + i A_{f+1}
+  for (int idx = threadIdx.x; idx < d.Mz * NC; idx += blockDim.x) {
+    const int c = idx % NC, k = idx / NC;
+    const int rl = c / 3, pr = c % 3;
+    const int row = row0 + rl;
+    c64 z = cmk(0.0, 0.0);
+    if (row < nrows) {
+      const c64* fa = Y + (size_t)(2 * pr) * plane + (size_t)row * d.Kz;
+      const c64* fb = Y + (size_t)(2 * pr + 1) * plane + (size_t)row * d.Kz;
+      if (k == 0) {
+        z = cmk(fa[0].re, fb[0].re);
+      } else if (k < d.Kz) {
+        const c64 xa = fa[k], xb = fb[k];
+        z = cmk(xa.re - xb.im, xa.im + xb.re);
+      } else if (k > d.Mz - d.Kz) {
+        const int kk = d.Mz - k;
+        const c64 xa = fa[kk], xb = fb[kk];  // conj(xa) + i conj(xb)
+        z = cmk(xa.re + xb.im, -xa.im + xb.re);
+      }
+    }
+    A[k * NC + c] = z;
+  }
+  __syncthreads();
+  c64* phys = fft_columns<double>(A, B, plan, NC, NC, tw, +1);
+  c64* other = (phys == A) ? B : A;
+  // products: packed output columns per row pair q: [n0a+i n1a, n0b+i n1b, n2a+i n2b]
+  const int NCf = (kZRows / 2) * 3;
+  for (int idx = threadIdx.x; idx < d.Mz * kZRows; idx += blockDim.x) {
+    const int rl = idx % kZRows, n = idx / kZRows;
+    const int row = row0 + rl;
+    const int j = (row < nrows) ? row / d.My : 0;
+    const c64 z0 = phys[n * NC + rl * 3 + 0];
+    const c64 z1 = phys[n * NC + rl * 3 + 1];
+    const c64 z2 = phys[n * NC + rl * 3 + 2];
+    const double u0 = z0.re, u1 = z0.im + d.uwall * o.xphys[j], u2 = z1.re;
+    const double w0 = z1.im, w1 = z2.re, w2 = z2.im + d.uwall;
+    const double n0 = -(u1 * w2 - u2 * w1);
+    const double n1 = -(u2 * w0 - u0 * w2);
+    const double n2 = -(u0 * w1 - u1 * w0);
+    const int q = rl >> 1, ab = rl & 1;
+    other[n * NCf + q * 3 + ab] = cmk(n0, n1);
+    if (ab == 0) other[n * NCf + q * 3 + 2].re = n2;
+    else other[n * NCf + q * 3 + 2].im = n2;
+  }
+  __syncthreads();
+  c64* spec = fft_columns<double>(other, phys, plan, NCf, NCf, tw, -1);
+  const double scale = 1.0 / d.Mz;
+  for (int idx = threadIdx.x; idx < d.Kz * kZRows * 3; idx += blockDim.x) {
+    const int k = idx % d.Kz;
+    const int rf = idx / d.Kz;
+    const int f = rf % 3, rl = rf / 3;
+    const int row = row0 + rl;
+    if (row >= nrows) continue;
+    const int q = rl >> 1, ab = rl & 1;
+    const int col = (f < 2) ? q * 3 + ab : q * 3 + 2;
+    const c64 Zk = spec[k * NCf + col];
+    const c64 Zm = spec[((d.Mz - k) % d.Mz) * NCf + col];
+    // x + i y packed: X_k = (Z_k + conj Z_-k)/2, Y_k = (Z_k - conj Z_-k)/(2i)
+    c64 v;
+    const bool take_real = (f < 2) ? (f == 0) : (ab == 0);
+    if (take_real) v = cmk(0.5 * (Zk.re + Zm.re), 0.5 * (Zk.im - Zm.im));
+    else v = cmk(0.5 * (Zk.im + Zm.im), -0.5 * (Zk.re - Zm.re));
+    HZ[(size_t)f * plane + (size_t)row * d.Kz + k] = scale * v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// y_forward: per (x-plane, field): forward FFT My, scale 1/My, keep Ny modes.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) y_forward_kernel(Dims d, FFTPlan plan, int KC,
+                                                        const c64* __restrict__ tw,
+                                                        const c64* __restrict__ HZ,
+                                                        c64* __restrict__ HX) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  c64* A = reinterpret_cast<c64*>(smem_raw);
+  c64* B = A + d.My * KC;
+  const int j = blockIdx.x, f = blockIdx.y, kc0 = blockIdx.z * KC;
+  const c64* src = HZ + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
+  for (int idx = threadIdx.x; idx < d.My * KC; idx += blockDim.x) {
+    const int kz = idx % KC, r = idx / KC;
+    A[idx] = src[(size_t)r * d.Kz + kz];
+  }
+  __syncthreads();
+  c64* res = fft_columns<double>(A, B, plan, KC, KC, tw, -1);
+  const double scale = 1.0 / d.My;
+  const int half = d.Ny / 2;
+  c64* dst = HX + ((size_t)f * d.Nx + j) * d.P + kc0;
+  for (int idx = threadIdx.x; idx < d.Ny * KC; idx += blockDim.x) {
+    const int kz = idx % KC, r = idx / KC;
+    c64 v = cmk(0.0, 0.0);
+    if (r < half) v = res[r * KC + kz];
+    else if (r > half) v = res[(r - d.Ny + d.My) * KC + kz];  // r == half: Nyquist
+    dst[(size_t)r * d.Kz + kz] = scale * v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z_forward_real: three real physical fields (Nx, Ny, Nz) -> half spectra
+// along z, scaled 1/Nz (Fourier.forward, norm="forward").  Per 4 rows: two
+// fields packed per complex transform, third field packed across row pairs.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) z_forward_real_kernel(Dims d, FFTPlan plan,
+                                                             const c64* __restrict__ tw,
+                                                             const double* __restrict__ f0,
+                                                             const double* __restrict__ f1,
+                                                             const double* __restrict__ f2,
+                                                             c64* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int NCf = (kZRows / 2) * 3;
+  const int n = d.Nz;
+  c64* A = reinterpret_cast<c64*>(smem_raw);
+  c64* B = A + n * NCf;
+  const int row0 = blockIdx.x * kZRows;
+  const int nrows = d.Nx * d.Ny;
+  for (int idx = threadIdx.x; idx < n * kZRows; idx += blockDim.x) {
+    const int rl = idx % kZRows, z = idx / kZRows;
+    const int row = row0 + rl;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    if (row < nrows) {
+      const size_t e = (size_t)row * n + z;
+      a0 = f0[e];
+      a1 = f1[e];
+      a2 = f2[e];
+    }
+    const int q = rl >> 1, ab = rl & 1;
+    A[z * NCf + q * 3 + ab] = cmk(a0, a1);
+    if (ab == 0) A[z * NCf + q * 3 + 2].re = a2;
+    else A[z * NCf + q * 3 + 2].im = a2;
+  }
+  __syncthreads();
+  c64* spec = fft_columns<double>(A, B, plan, NCf, NCf, tw, -1);
+  const double scale = 1.0 / n;
+  const size_t plane = (size_t)d.Nx * d.Ny * d.Kz;
+  for (int idx = threadIdx.x; idx < d.Kz * kZRows * 3; idx += blockDim.x) {
+    const int k = idx % d.Kz;
+    const int rf = idx / d.Kz;
+    const int f = rf % 3, rl = rf / 3;
+    const int row = row0 + rl;
+    if (row >= nrows) continue;
+    const int q = rl >> 1, ab = rl & 1;
+    const int col = (f < 2) ? q * 3 + ab : q * 3 + 2;
+    const c64 Zk = spec[k * NCf + col];
+    const c64 Zm = spec[((n - k) % n) * NCf + col];
+    c64 v;
+    const bool take_real = (f < 2) ? (f == 0) : (ab == 0);
+    if (take_real) v = cmk(0.5 * (Zk.re + Zm.re), 0.5 * (Zk.im - Zm.im));
+    else v = cmk(0.5 * (Zk.im + Zm.im), -0.5 * (Zk.re - Zm.re));
+    out[(size_t)f * plane + (size_t)row * d.Kz + k] = scale * v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Diagnostics of PlaneCouetteFluctuationJax (pcf_fluctuations_jax.py:131-161)
+// from the spectral state.  y/z integrals use Parseval (exact for the
+// reference's uniform quadrature); x uses the Fejer-I weights of the Gauss
+// nodes.  Per block: partial sums of |u|^2 and |div u|^2; the mean pencil
+// writes its wall / base-flow terms.  diag_finish_kernel reduces in a fixed
+// order (deterministic).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) diag_kernel(DevOps o, Dims d, const c64* __restrict__ u0,
+                                                   const c64* __restrict__ u1,
+                                                   const c64* __restrict__ u2,
+                                                   double* __restrict__ partial,
+                                                   double* __restrict__ meanterms) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  c64* ARR = reinterpret_cast<c64*>(smem_raw);  // kNW * 4 * Nx
+  double* red = reinterpret_cast<double*>(ARR + kNW * 4 * d.Nx);  // kNW * 2
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int kyi = blockIdx.x / d.nKb;
+  const int kz = (blockIdx.x % d.nKb) * kNW + warp;
+  const int ky = (kyi < d.Ny / 2) ? kyi : kyi - d.Ny;
+  const bool active = kz < d.Kz && kyi != d.Ny / 2;
+  const int p = kyi * d.Kz + kz;
+  const size_t P = (size_t)d.P;
+  const double kyp = ky * d.dfy, kzp = kz * d.dfz;
+  c64* B0 = ARR + warp * 4 * d.Nx;  // uo0
+  c64* B1 = B0 + d.Nx;              // uo1
+  c64* B2 = B1 + d.Nx;              // uo2
+  c64* B3 = B2 + d.Nx;              // div
+  double e_u = 0.0, e_div = 0.0;
+  if (active) {
+    for (int i = lane; i < d.nD; i += 32) {
+      B1[i] = u1[(size_t)i * P + p];
+      B2[i] = u2[(size_t)i * P + p];
+      if (i < d.nB) B3[i] = u0[(size_t)i * P + p];
+    }
+    __syncwarp();
+    apply_SBT(o, d, B3, B0, lane);
+    if (lane == 0) {
+      for (int n = d.Nx - 1; n >= 0; --n) {
+        c64 v = (n < d.nD) ? B1[n] : cmk(0.0, 0.0);
+        if (n >= 2) v = v - B1[n - 2];
+        B1[n] = v;
+      }
+    } else if (lane == 1) {
+      for (int n = d.Nx - 1; n >= 0; --n) {
+        c64 v = (n < d.nD) ? B2[n] : cmk(0.0, 0.0);
+        if (n >= 2) v = v - B2[n - 2];
+        B2[n] = v;
+      }
+    }
+    __syncwarp();
+    chebder_warp(B0, B3, d.Nx, d.dfx, lane);
+    for (int n = lane; n < d.Nx; n += 32) B3[n] = B3[n] + mul_i(kyp * B1[n] + kzp * B2[n]);
+    __syncwarp();
+    const double mult = (kz == 0) ? 1.0 : 2.0;
+    for (int j = lane; j < d.Nx; j += 32) {
+      c64 v0 = cmk(0.0, 0.0), v1 = v0, v2 = v0, v3 = v0;
+      for (int n = 0; n < d.Nx; ++n) {
+        const double t = __ldg(o.V + (size_t)j * d.Nx + n);
+        v0 = v0 + t * B0[n];
+        v1 = v1 + t * B1[n];
+        v2 = v2 + t * B2[n];
+        v3 = v3 + t * B3[n];
+      }
+      const double w = o.fejer[j] * mult;
+      e_u += w * (v0.re * v0.re + v0.im * v0.im + v1.re * v1.re + v1.im * v1.im +
+                  v2.re * v2.re + v2.im * v2.im);
+      e_div += w * (v3.re * v3.re + v3.im * v3.im);
+      if (ky == 0 && kz == 0) {
+        // base-flow cross term 2 Ub Re(u1_00) + Ub^2 and the mean shear dv/dx
+        const double ub = d.uwall * o.xphys[j];
+        meanterms[8 + j] = o.fejer[j] * (2.0 * ub * v1.re + ub * ub);
+      }
+    }
+    if (ky == 0 && kz == 0) {
+      // wall values and wall derivatives of the mean streamwise velocity
+      chebder_warp(B1, B3, d.Nx, d.dfx, lane);
+      if (lane == 0) {
+        double top = 0.0, bot = 0.0, stop = 0.0, sbot = 0.0, shear = 0.0;
+        for (int n = 0; n < d.Nx; ++n) {
+          const double sgn = (n & 1) ? -1.0 : 1.0;
+          top += B1[n].re;
+          bot += sgn * B1[n].re;
+          const double n2 = (double)n * n;
+          stop += n2 * B1[n].re * d.dfx;
+          sbot += -sgn * n2 * B1[n].re * d.dfx;
+        }
+        for (int j = 0; j < d.Nx; ++j) {
+          double dv = 0.0;
+          for (int n = 0; n < d.Nx; ++n) dv += __ldg(o.V + (size_t)j * d.Nx + n) * B3[n].re;
+          shear += o.fejer[j] * dv;
+        }
+        meanterms[0] = top;
+        meanterms[1] = bot;
+        meanterms[2] = stop;
+        meanterms[3] = sbot;
+        meanterms[4] = shear;
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    e_u += __shfl_down_sync(0xffffffffu, e_u, off);
+    e_div += __shfl_down_sync(0xffffffffu, e_div, off);
+  }
+  if (lane == 0) {
+    red[2 * warp] = e_u;
+    red[2 * warp + 1] = e_div;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < kNW; ++w) {
+      a += red[2 * w];
+      b += red[2 * w + 1];
+    }
+    partial[2 * blockIdx.x] = a;
+    partial[2 * blockIdx.x + 1] = b;
+  }
+}
+
+// out = (Epert, Etot, divL2, u_top, u_bot, wall_shear_top, wall_shear_bot, mean_shear)
+__global__ void diag_finish_kernel(Dims d, const double* __restrict__ partial, int nblocks,
+                                   const double* __restrict__ meanterms, double ly, double lz,
+                                   double x_lo, double x_hi, double* __restrict__ out) {
+  const double lx = x_hi - x_lo;
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double eu = 0.0, ed = 0.0, base = 0.0;
+  for (int b = 0; b < nblocks; ++b) {
+    eu += partial[2 * b];
+    ed += partial[2 * b + 1];
+  }
+  for (int j = 0; j < d.Nx; ++j) base += meanterms[8 + j];
+  const double area = ly * lz;
+  out[0] = area * eu;
+  out[1] = area * (eu + base);
+  out[2] = sqrt(area * ed);
+  out[3] = meanterms[0] + d.uwall * x_hi;
+  out[4] = meanterms[1] + d.uwall * x_lo;
+  out[5] = meanterms[2] + d.uwall;
+  out[6] = meanterms[3] + d.uwall;
+  out[7] = (area * meanterms[4] + d.uwall * lx * area) / (lx * area);
+}
+
+}  // namespace jfb

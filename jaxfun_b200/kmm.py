@@ -1,0 +1,317 @@
+"""KMM / plane-Couette solver objects backed by the sm_100a step.
+
+Mirrors the reference's public API for the hot path:
+``examples/channelflow_kmm.py`` (``KMM``, ``KMMState``: ``step``, ``solve``,
+``convection``, ``zero_state``) and ``examples/pcf_fluctuations_jax.py``
+(``PlaneCouetteFluctuationJax``).  Arrays are torch tensors on a CUDA device in
+the reference layout (wall-normal axis first, full complex Fourier axes).
+All arithmetic runs in ``libjfb200.so``; there is no CPU path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, replace
+
+import torch
+
+from . import _lib
+
+_STEPPERS = {"IMEXRK222", "IMEXRK3", "CNAB2", "SBDF3"}
+
+
+@dataclass(frozen=True)
+class KMMState:
+    """Coefficient-space state with SBDF3 history (channelflow_kmm.py:50-101)."""
+
+    u: tuple
+    g: torch.Tensor
+    nonlinear_old: tuple | None = None
+    nonlinear_older: tuple | None = None
+    solution_old: tuple | None = None
+    solution_older: tuple | None = None
+    history_steps: float = 0.0
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("KMM state tensors must live on a CUDA device")
+    if not t.is_contiguous():
+        raise ValueError("KMM state tensors must be contiguous")
+    return t.data_ptr()
+
+
+class KMM:
+    """Velocity-vorticity KMM channel solver (channelflow_kmm.py:104-230).
+
+    Supported on the GPU path: Chebyshev family, wall-normal axis unpadded,
+    SBDF3 with IMEXRK3 startup, rotational nonlinear form.  The coefficient
+    path ("optimized" or "transform") only changes round-off in the reference
+    (tests/couette/test_pcf_fluctuations_jax.py:16-52), so both names select
+    the same coefficient-space kernels.
+    """
+
+    def __init__(
+        self,
+        N=(17, 16, 16),
+        domain=((-1.0, 1.0), (0.0, 4.0 * math.pi), (0.0, 2.0 * math.pi)),
+        nu: float = 1.0 / 600.0,
+        dt: float = 0.01,
+        family: str = "C",
+        padding_factor=(1.0, 1.5, 1.5),
+        dpdy: float = 0.0,
+        time_integrator: str | None = "SBDF3",
+        nonlinear_form: str = "rotational",
+        coefficient_path: str = "optimized",
+        solve_batching: str = "batched",
+        precision: str = "fp64",
+        device: str | torch.device = "cuda",
+        _u_wall: float = 0.0,
+    ) -> None:
+        self.N = tuple(int(n) for n in N)
+        self.domain = tuple(tuple(float(v) for v in d) for d in domain)
+        self.nu = float(nu)
+        self.dt = float(dt)
+        self.padding_factor = tuple(float(p) for p in padding_factor)
+        self.nonlinear_form = str(nonlinear_form).lower()
+        if self.nonlinear_form not in {"gradient", "rotational"}:
+            raise ValueError("nonlinear_form must be 'gradient' or 'rotational'")
+        self.coefficient_path = str(coefficient_path).lower()
+        if self.coefficient_path not in {"optimized", "transform"}:
+            raise ValueError("coefficient_path must be 'optimized' or 'transform'")
+        if str(solve_batching).lower() not in {"batched", "separate"}:
+            raise ValueError("solve_batching must be 'batched' or 'separate'")
+        if time_integrator is not None and time_integrator not in _STEPPERS:
+            raise ValueError(
+                "time_integrator must be one of "
+                "{'IMEXRK222', 'IMEXRK3', 'CNAB2', 'SBDF3'}"
+            )
+        unsupported = []
+        if time_integrator != "SBDF3":
+            unsupported.append(f"time_integrator={time_integrator!r}")
+        if self.nonlinear_form != "rotational":
+            unsupported.append(f"nonlinear_form={self.nonlinear_form!r}")
+        if not str(family).upper().startswith("C"):
+            unsupported.append(f"family={family!r}")
+        if self.padding_factor[0] != 1.0:
+            unsupported.append("wall-normal padding")
+        if float(dpdy) != 0.0:
+            unsupported.append("dpdy != 0")
+        if unsupported:
+            raise NotImplementedError(
+                "the B200 step supports SBDF3 / rotational / Chebyshev / unpadded x "
+                "only; requested " + ", ".join(unsupported)
+            )
+        self.time_integrator = "SBDF3"
+        self.family = "C"
+        self.precision = precision
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise ValueError("the B200 step runs on a CUDA device only")
+        self.dpdy = 0.0
+        Nx, Ny, Nz = self.N
+        self.shape_B = (Nx - 4, Ny, Nz)
+        self.shape_D = (Nx - 2, Ny, Nz)
+        cfg = _lib.KMMConfig()
+        cfg.nx, cfg.ny, cfg.nz = Nx, Ny, Nz
+        cfg.family = _lib.JFB_FAMILY_CHEBYSHEV
+        cfg.x_lo, cfg.x_hi = self.domain[0]
+        cfg.ly = self.domain[1][1] - self.domain[1][0]
+        cfg.lz = self.domain[2][1] - self.domain[2][0]
+        cfg.pad_y, cfg.pad_z = self.padding_factor[1], self.padding_factor[2]
+        cfg.nu = self.nu
+        cfg.dt = self.dt
+        cfg.u_wall = float(_u_wall)
+        cfg.precision = {
+            "fp64": _lib.JFB_PRECISION_FP64,
+            "mixed": _lib.JFB_PRECISION_MIXED,
+        }[precision]
+        cfg.nonlinear_form = _lib.JFB_NONLINEAR_ROTATIONAL
+        self._cfg = cfg
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.call("jfb_kmm_create", ctypes.byref(cfg), ctypes.byref(handle))
+        self._plan = handle
+        self._current = None  # the KMMState object the plan currently holds
+
+    # -- plumbing -------------------------------------------------------------
+    def __del__(self):
+        plan = getattr(self, "_plan", None)
+        if plan is not None and plan.value:
+            try:
+                _lib.load().jfb_kmm_destroy(plan)
+            except Exception:
+                pass
+            self._plan = None
+
+    def _stream(self) -> ctypes.c_void_p:
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def info(self) -> _lib.KMMInfo:
+        info = _lib.KMMInfo()
+        _lib.call("jfb_kmm_get_info", self._plan, ctypes.byref(info))
+        return info
+
+    def _c_state(self, st: KMMState) -> _lib.KMMStateC:
+        c = _lib.KMMStateC()
+        c.u0, c.u1, c.u2 = (_ptr(t) for t in st.u)
+        c.g = _ptr(st.g)
+        for name in ("nonlinear_old", "nonlinear_older", "solution_old", "solution_older"):
+            lv = getattr(st, name)
+            arr = getattr(c, name)
+            for k in range(4):
+                arr[k] = _ptr(lv[k]) if lv is not None else None
+        c.history_steps = float(st.history_steps)
+        return c
+
+    def _empty_state(self) -> KMMState:
+        dev = self.device
+        cd = torch.complex128
+
+        def lv():
+            return (
+                torch.empty(self.shape_B, dtype=cd, device=dev),
+                torch.empty(self.shape_D, dtype=cd, device=dev),
+                torch.empty(self.shape_D[0], dtype=torch.float64, device=dev),
+                torch.empty(self.shape_D[0], dtype=torch.float64, device=dev),
+            )
+
+        return KMMState(
+            u=(
+                torch.empty(self.shape_B, dtype=cd, device=dev),
+                torch.empty(self.shape_D, dtype=cd, device=dev),
+                torch.empty(self.shape_D, dtype=cd, device=dev),
+            ),
+            g=torch.empty(self.shape_D, dtype=cd, device=dev),
+            nonlinear_old=lv(),
+            nonlinear_older=lv(),
+            solution_old=lv(),
+            solution_older=lv(),
+        )
+
+    def _load(self, state: KMMState) -> None:
+        if state is self._current:
+            return
+        state = self._ensure_history(state)
+        c = self._c_state(state)
+        _lib.call("jfb_kmm_set_state", self._plan, ctypes.byref(c), self._stream())
+        self._current = state
+
+    def _fetch(self, history_steps: float) -> KMMState:
+        out = self._empty_state()
+        out = replace(out, history_steps=float(history_steps))
+        c = self._c_state(out)
+        _lib.call("jfb_kmm_get_state", self._plan, ctypes.byref(c), self._stream())
+        self._current = out
+        return out
+
+    def _ensure_history(self, state: KMMState) -> KMMState:
+        """Zero history levels for a fresh state (channelflow_kmm.py:609-654)."""
+        if state.solution_old is not None and state.nonlinear_old is not None:
+            return state
+        z = (
+            torch.zeros_like(state.u[0]),
+            torch.zeros_like(state.g),
+            torch.zeros(self.shape_D[0], dtype=torch.float64, device=self.device),
+            torch.zeros(self.shape_D[0], dtype=torch.float64, device=self.device),
+        )
+        return replace(
+            state,
+            nonlinear_old=z,
+            nonlinear_older=z,
+            solution_old=z,
+            solution_older=z,
+            history_steps=0.0,
+        )
+
+    # -- reference API ----------------------------------------------------------
+    def zero_state(self) -> KMMState:
+        dev, cd = self.device, torch.complex128
+        st = KMMState(
+            u=(
+                torch.zeros(self.shape_B, dtype=cd, device=dev),
+                torch.zeros(self.shape_D, dtype=cd, device=dev),
+                torch.zeros(self.shape_D, dtype=cd, device=dev),
+            ),
+            g=torch.zeros(self.shape_D, dtype=cd, device=dev),
+        )
+        return self._ensure_history(st)
+
+    def step(self, state: KMMState, dt=None, factor_args=None) -> KMMState:
+        """One SBDF3 step (IMEXRK3 startup while history_steps < 2)."""
+        return self.solve(state, 1)
+
+    def solve(self, state: KMMState, steps: int) -> KMMState:
+        """Advance ``steps`` steps (channelflow_kmm.py:1231-1247)."""
+        steps = int(steps)
+        self._load(state)
+        hist = float(self._current.history_steps)
+        _lib.call("jfb_kmm_advance", self._plan, steps, self._stream())
+        return self._fetch(min(2.0, hist + steps))
+
+    def advance_resident(self, steps: int) -> None:
+        """Advance the device-resident state without materialising it."""
+        _lib.call("jfb_kmm_advance", self._plan, int(steps), self._stream())
+        self._current = None
+
+    def convection(self, state: KMMState):
+        """Dealiased rotational convection in TD coefficients (channelflow_kmm.py:772-782)."""
+        self._load(state)
+        H = tuple(
+            torch.empty(self.shape_D, dtype=torch.complex128, device=self.device)
+            for _ in range(3)
+        )
+        _lib.call(
+            "jfb_kmm_convection", self._plan, H[0].data_ptr(), H[1].data_ptr(),
+            H[2].data_ptr(), self._stream(),
+        )
+        return H
+
+
+class PlaneCouetteFluctuation(KMM):
+    """Fluctuations about ``U_b = U_wall x`` (pcf_fluctuations_jax.py:29-75)."""
+
+    def __init__(
+        self,
+        N=(17, 16, 16),
+        domain=((-1.0, 1.0), (0.0, 4.0 * math.pi), (0.0, 2.0 * math.pi)),
+        Re: float = 600.0,
+        U_wall: float = 1.0,
+        dt: float = 0.01,
+        family: str = "C",
+        padding_factor=(1.0, 1.5, 1.5),
+        perturbation_amplitude: float = 0.05,
+        timestepper=None,
+        time_integrator: str | None = "SBDF3",
+        nonlinear_form: str = "rotational",
+        coefficient_path: str = "optimized",
+        solve_batching: str = "batched",
+        precision: str = "fp64",
+        device="cuda",
+    ) -> None:
+        self.Re = float(Re)
+        self.U_wall = float(U_wall)
+        self.perturbation_amplitude = float(perturbation_amplitude)
+        super().__init__(
+            N=N,
+            domain=domain,
+            nu=self.U_wall / self.Re,
+            dt=dt,
+            family=family,
+            padding_factor=padding_factor,
+            time_integrator=time_integrator,
+            nonlinear_form=nonlinear_form,
+            coefficient_path=coefficient_path,
+            solve_batching=solve_batching,
+            precision=precision,
+            device=device,
+            _u_wall=self.U_wall,
+        )
+        self.dUb_dx = self.U_wall
+
+
+# reference name
+PlaneCouetteFluctuationJax = PlaneCouetteFluctuation
