@@ -1,0 +1,447 @@
+#!/usr/bin/env python3
+"""Benchmark: SBDF3 steps/s of the rotational plane-Couette KMM step.
+
+Workload (one "step" = one steady SBDF3 step of the whole field): the Couette
+DNS configuration, 65 x 64 x 64 (Chebyshev wall-normal x Fourier x Fourier,
+3/2 dealiasing), Re = 1000, dt = 0.01, seeded divergence-free perturbation of
+energy 1e-4 (jaxfun_b200.workloads).  Single-GPU problem: with --gpus N every
+rank advances its own replica (weak scaling, no collective on the data path).
+
+Default arm (--impl b200): times K steady steps through
+``jfb_kmm_timed_steps`` (CUDA events around each kernel on the launching
+stream; a 256 MiB memset between steps flushes the 126 MB L2 outside the
+timed events), reports the per-kernel roofline of the dominant kernel, the
+back-to-back CUDA-graph throughput, an end-to-end figure through the public
+``solve`` API with pinned host buffers, and the CPU oracle on the host cores.
+
+Reference arm (--impl reference): the reference (JAX) cannot be installed
+here, so the reference's CPU algorithm is timed through the NumPy/SciPy
+restatement in oracle/ on all host cores, on the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SBDF3 steps/s at 65×64×64 on 1 B200: mixed vs FP64 form at stated err, vs CPU"
+UNIT = "steps/s"
+RE, DT, ENERGY = 1000.0, 0.01, 1.0e-4
+HBM_FALLBACK_GBS = 6650.0
+FLUSH_BYTES = 256 << 20
+BLOCK = 25  # reference rollout block (production/benchmark.py: rollout_steps)
+
+
+def parse_args(argv=None):
+    p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=500)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    p.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
+    p.add_argument("--grid", default="65,64,64")
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args(argv)
+
+
+def grid_of(args):
+    return tuple(int(v) for v in args.grid.split(","))
+
+
+def domain():
+    return ((-1.0, 1.0), (0.0, 4.0 * math.pi), (0.0, 2.0 * math.pi))
+
+
+def workload_desc(grid, precision, l2):
+    nx, ny, nz = grid
+    return {
+        "workload": (
+            f"plane Couette KMM SBDF3 rotational step {nx}x{ny}x{nz} "
+            f"(Chebyshev x Fourier x Fourier, 3/2 dealiasing), Re={RE:g}, dt={DT:g}, "
+            f"seeded divergence-free perturbation, energy {ENERGY:g}"
+        ),
+        "grid": list(grid),
+        "precision": precision,
+        "l2": l2,
+        "parallelism": "replicas",
+    }
+
+
+def stage_bytes(grid, my):
+    """Algorithmic HBM bytes (FP64 complex = 16 B) per launch of each kernel
+    and per step, in the stage model: Hermitian half spectra H = Nz/2 + 1,
+    E_s = Nx Ny H, E_m = Nx My H, factors regenerated (0 B), each array read
+    once and written once."""
+    nx, ny, nz = grid
+    H = nz // 2 + 1
+    Es, Em = nx * ny * H, nx * my * H
+    b = 16
+    return {
+        # reads: H 3 E_s + solution levels 6 E_s + nonlinear levels 4 E_s;
+        # writes: new (u0, g) 2 E_s + N 2 E_s + six x-physical fields 6 E_s
+        "pencil_stage": 23 * Es * b,
+        "y_backward": (6 * Es + 6 * Em) * b,
+        "z_cross": 9 * Em * b,
+        "y_forward": (3 * Em + 3 * Es) * b,
+        # canonical whole-step figure (43 E_s + 18 E_m)
+        "step": (43 * Es + 18 * Em) * b,
+    }
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def dram_traffic(kernel):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.index)],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.strip().split(",") for r in self.file if r.strip()]
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for name, v in zip(names, r[5:9], strict=False):
+                    if v.strip().lower() in ("active", "1"):
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle_rate(fields, grid, seconds, threads):
+    """Steady SBDF3 steps/s of the oracle (NumPy/SciPy restatement of the
+    reference algorithm) on the host cores; a bounded sample."""
+    from oracle import kmm as ok
+
+    ok.set_workers(threads)
+    o = ok.PlaneCouetteOracle(N=grid, Re=RE, dt=DT, domain=domain(),
+                              perturbation_amplitude=0.0)
+    st = o.state_from_physical(tuple(f.astype(complex) for f in fields))
+    st = o.step(o.step(st))  # IMEXRK3 startup, not timed
+    st = o.step(st)          # warm
+    n, t0 = 0, time.perf_counter()
+    while True:
+        st = o.step(st)
+        n += 1
+        if n >= 3 and time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return n / dt, n
+
+
+def max_over_ranks(value: float, device) -> float:
+    """Max of a per-rank scalar over the process group (identity if none)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args):
+    grid = grid_of(args)
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from jaxfun_b200.workloads import couette_perturbation_fields
+
+    fields = couette_perturbation_fields(grid, domain())
+    threads = host_threads()
+    # energy normalisation is linear: scale with the oracle's own projection
+    from oracle import kmm as ok
+
+    ok.set_workers(threads)
+    o = ok.PlaneCouetteOracle(N=grid, Re=RE, dt=DT, domain=domain())
+    e = o.diagnostics(o.state_from_physical(tuple(f.astype(complex) for f in fields)))["Epert"]
+    s = math.sqrt(ENERGY / e)
+    fields = tuple(f * s for f in fields)
+    per_step = max(3.0, args.cpu_seconds / max(1, args.steps))
+    rates = []
+    for _ in range(max(1, min(args.warmup, 1))):
+        cpu_oracle_rate(fields, grid, 1.0, threads)
+    for _ in range(max(1, min(args.steps, 3))):
+        r, _ = cpu_oracle_rate(fields, grid, per_step, threads)
+        rates.append(r)
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1000.0 / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": workload_desc(grid, "fp64", "n/a (host CPU)"),
+        "cpu_baseline": {
+            "value": value, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(rates)} samples of >= {per_step:.1f} s of steady SBDF3 steps "
+                      "of the oracle restatement (reference JAX not installable: no jax/jaxlib "
+                      "in the image, no network)",
+        },
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    from jaxfun_b200 import _lib
+    from jaxfun_b200.kmm import KMMState, PlaneCouetteFluctuation
+    from jaxfun_b200.workloads import couette_perturbation_fields, scale_to_energy
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=dev)
+    grid = grid_of(args)
+
+    solver = PlaneCouetteFluctuation(N=grid, domain=domain(), Re=RE, dt=DT,
+                                     precision=args.precision, device=dev)
+    info = solver.info()
+    fields = couette_perturbation_fields(grid, domain())
+    st0 = solver.state_from_physical(fields)
+    e0 = solver.diagnostics(st0)["Epert"]
+    fields = scale_to_energy(fields, e0, ENERGY)
+    state = solver.state_from_physical(fields)
+    stream = torch.cuda.current_stream(dev)
+
+    # warm-up: startup + W steady steps (graph replay), device resident
+    state = solver.solve(state, 2 + max(3, args.warmup))
+    torch.cuda.synchronize(dev)
+
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    kms = (ctypes.c_double * 4)()
+    sms = ctypes.c_double()
+    sampler = ClockSampler(local)
+    sampler.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    _lib.call("jfb_kmm_timed_steps", solver._plan, args.steps, flush.data_ptr(), FLUSH_BYTES,
+              kms, ctypes.byref(sms), ctypes.c_void_p(stream.cuda_stream))
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    solver._current = None
+    t_step = max_over_ranks(sms.value / max(1, args.steps), dev)  # ms per step, L2 flushed
+    value = world * 1000.0 / t_step
+    kernel_names = ("pencil_stage", "y_backward", "z_cross", "y_forward")
+    kernel_avg = {k: kms[i] / max(1, args.steps) for i, k in enumerate(kernel_names)}
+
+    # back-to-back graph replay (L2 stays warm between steps)
+    g_steps = max(10, args.steps)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.advance_resident(g_steps)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    graph_ms = max_over_ranks(e0.elapsed_time(e1) / g_steps, dev)
+
+    # end to end through the public API with pinned host buffers
+    cur = solver._fetch(2.0)
+
+    def host_copy(t):
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        h.copy_(t)
+        return h
+
+    def tree(st, fn):
+        lv = lambda x: tuple(fn(t) for t in x)  # noqa: E731
+        return KMMState(u=lv(st.u), g=fn(st.g), nonlinear_old=lv(st.nonlinear_old),
+                        nonlinear_older=lv(st.nonlinear_older),
+                        solution_old=lv(st.solution_old),
+                        solution_older=lv(st.solution_older),
+                        history_steps=st.history_steps)
+
+    host_state = tree(cur, host_copy)
+    state_bytes = sum(t.numel() * t.element_size() for t in
+                      (*host_state.u, host_state.g, *host_state.nonlinear_old,
+                       *host_state.nonlinear_older, *host_state.solution_old,
+                       *host_state.solution_older))
+    host_out = tree(cur, lambda t: torch.empty(t.shape, dtype=t.dtype, pin_memory=True))
+    diag_host = torch.empty(8, dtype=torch.float64, pin_memory=True)
+    blocks = max(1, min(4, args.steps // BLOCK))
+    torch.cuda.synchronize(dev)
+    x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    x0.record(stream)
+    hs = host_state
+    for _ in range(blocks):
+        dstate = tree(hs, lambda t: t.to(dev, non_blocking=True))
+        out = solver.solve(dstate, BLOCK)
+        diag = solver.diagnostics_tensor(out)
+        for src, dst in zip((*out.u, out.g, *out.nonlinear_old, *out.nonlinear_older,
+                             *out.solution_old, *out.solution_older),
+                            (*host_out.u, host_out.g, *host_out.nonlinear_old,
+                             *host_out.nonlinear_older, *host_out.solution_old,
+                             *host_out.solution_older), strict=True):
+            dst.copy_(src, non_blocking=True)
+        diag_host.copy_(diag, non_blocking=True)
+        hs = host_out
+    x1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(x0.elapsed_time(x1) / (blocks * BLOCK), dev)
+    final_diag = dict(zip(solver.DIAGNOSTIC_NAMES, diag_host.tolist(), strict=True))
+
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
+    sb = stage_bytes(grid, info.my)
+    peak, peak_kind = measured_peak()
+    dom = max(kernel_avg, key=kernel_avg.get)
+    dom_ms = kernel_avg[dom]
+    achieved = sb[dom] / (dom_ms * 1e-3) / 1e9
+    roofline = {
+        "bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
+        "traffic": dram_traffic(dom), "algorithmic_bytes_per_launch": sb[dom],
+        "launch_ms": dom_ms,
+    }
+    step_ach = sb["step"] / (t_step * 1e-3) / 1e9
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+        "data": "synthetic",
+        "config": workload_desc(grid, args.precision,
+                                "flushed between timed steps (256 MiB memset)"),
+        "roofline": roofline,
+        "step_roofline": {
+            "algorithmic_bytes": sb["step"], "achieved": step_ach, "peak": peak,
+            "unit": "GB/s", "frac": step_ach / peak, "peak_kind": f"of {peak_kind}",
+        },
+        "kernel_ms": kernel_avg,
+        "graph_l2_resident": {"ms_per_step": graph_ms, "value": world * 1000.0 / graph_ms},
+        "e2e": {
+            "value": world * 1000.0 / e2e_ms, "unit": UNIT,
+            "h2d_bytes_per_step": state_bytes / BLOCK,
+            "d2h_bytes_per_step": (state_bytes + 64) / BLOCK,
+            "path": f"solve(state, {BLOCK}) per block with pinned-host state in/out and "
+                    "diagnostics read back",
+        },
+        "gpu_launches": 4 * args.steps,
+        "clocks": clocks,
+        "final_diagnostics": final_diag,
+        "device_bytes": info.device_bytes,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        threads = host_threads()
+        rate, n = cpu_oracle_rate(fields, grid, args.cpu_seconds, threads)
+        line["cpu_baseline"] = {
+            "value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} steady SBDF3 steps of the same workload, oracle restatement, "
+                      f"scipy.fft workers={threads}",
+        }
+    print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -163,6 +163,19 @@ int jfb_kmm_state_from_physical(jfb_kmm_plan* plan, const double* u0,
  * fixed-order reduction. */
 int jfb_kmm_diagnostics(jfb_kmm_plan* plan, double* out, void* stream);
 
+/* Measurement entry point (no reference counterpart; the reference's
+ * production/benchmark.py:282-354 times blocks of KMM.solve with host
+ * clocks): advances `steps` steady steps with the same kernels as
+ * jfb_kmm_advance, launched without the graph and bracketed by CUDA events
+ * on `stream`.  Before each step, if flush_buf is non-NULL, flush_bytes of it
+ * are overwritten (an L2 flush outside the timed events).  Returns the summed
+ * device time of each of the four kernels (kernel_ms[4]: pencil stage,
+ * y backward, z cross, y forward) and of the whole steps (step_ms).
+ * IMEXRK3 startup steps still pending are run first and not timed. */
+int jfb_kmm_timed_steps(jfb_kmm_plan* plan, int64_t steps, void* flush_buf,
+                        int64_t flush_bytes, double* kernel_ms, double* step_ms,
+                        void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -104,6 +104,10 @@ SIGNATURES = {
         c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
     ),
     "jfb_kmm_diagnostics": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "jfb_kmm_timed_steps": (
+        c_int,
+        [c_void_p, c_int64, c_void_p, c_int64, POINTER(c_double), POINTER(c_double), c_void_p],
+    ),
 }
 
 _lib = None

@@ -12,6 +12,7 @@
 #include "jfb_common.cuh"
 #include "jfb_kmm.h"
 #include "jfb_kmm_kernels.cuh"
+#include "jfb_kmm_warpk.cuh"
 
 namespace jfb {
 
@@ -170,6 +171,10 @@ struct jfb_kmm_plan {
   jfb::c64 *X, *Y, *HZ, *HX, *HD;
   jfb::c64 *twy, *twz, *twny, *twnz;
   jfb::FFTPlan fny, fnz;  // unpadded y / z transforms (state_from_physical)
+  int py = 0, pz = 0, pnz = 0;  // warp-FFT radix (N = 32 P), 0 = shared-memory Stockham
+  int qk = 0;                   // ceil(Kz / 32)
+  int KCw = 0;                  // kz columns per warp-FFT y block
+  size_t smem_yw_b = 0, smem_yw_f = 0;
   double *diag_partial = nullptr, *diag_mean = nullptr;
   int diag_blocks = 0;
   size_t smem_zf = 0, smem_diag = 0;
@@ -180,6 +185,7 @@ struct jfb_kmm_plan {
   bool explicit_u12 = false;  // U1S/U2S hold the current u1, u2
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   cudaStream_t cap = nullptr;  // private stream used only to capture the graphs
+  cudaEvent_t* timing_events = nullptr;  // set by jfb_kmm_timed_steps
 };
 
 namespace jfb {
@@ -315,23 +321,96 @@ static StageArgs blank_args() {
 
 static int launch_pencil(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s) {
   const int blocks = pl->d.Ny * pl->d.nKb;
-  pencil_stage_kernel<<<blocks, kNW * 32, pl->smem_pencil, s>>>(pl->ops, pl->d, a);
+  if (pl->d.nD <= 64)
+    pencil_stage_kernel<1><<<blocks, kNW * 32, pl->smem_pencil, s>>>(pl->ops, pl->d, a);
+  else
+    pencil_stage_kernel<2><<<blocks, kNW * 32, pl->smem_pencil, s>>>(pl->ops, pl->d, a);
   JFB_CHECK_LAUNCH();
   return JFB_OK;
+}
+
+static int warp_radix(int n) {
+  if (n % 32) return 0;
+  const int p = n / 32;
+  return (p == 2 || p == 3 || p == 4 || p == 6) ? p : 0;
+}
+
+template <int P>
+static void launch_y_warp(jfb_kmm_plan* pl, cudaStream_t s, bool backward) {
+  const Dims& d = pl->d;
+  if (backward) {
+    dim3 g(d.Nx, 6, d.Kz / pl->KCw);
+    y_backward_warp_kernel<P><<<g, 256, pl->smem_yw_b, s>>>(d, pl->KCw, pl->twy, pl->X, pl->Y);
+  } else {
+    dim3 g(d.Nx, 3, d.Kz / pl->KCw);
+    y_forward_warp_kernel<P><<<g, 256, pl->smem_yw_f, s>>>(d, pl->KCw, pl->twy, pl->HZ, pl->HX);
+  }
+}
+
+static void launch_y_warp_any(jfb_kmm_plan* pl, cudaStream_t s, bool backward) {
+  switch (pl->py) {
+    case 2: launch_y_warp<2>(pl, s, backward); break;
+    case 3: launch_y_warp<3>(pl, s, backward); break;
+    case 4: launch_y_warp<4>(pl, s, backward); break;
+    default: launch_y_warp<6>(pl, s, backward); break;
+  }
+}
+
+template <int P>
+static void launch_zcross_warp(jfb_kmm_plan* pl, cudaStream_t s) {
+  const Dims& d = pl->d;
+  const int pairs = ceil_div((int64_t)d.Nx * d.My, 2);
+  const int blocks = ceil_div(pairs, 8);
+  if (pl->qk == 1)
+    z_cross_warp_kernel<P, 1><<<blocks, 256, 0, s>>>(pl->ops, d, pl->twz, pl->Y, pl->HZ);
+  else
+    z_cross_warp_kernel<P, 2><<<blocks, 256, 0, s>>>(pl->ops, d, pl->twz, pl->Y, pl->HZ);
+}
+
+template <int P>
+static void launch_zfwd_warp(jfb_kmm_plan* pl, const double* u0, const double* u1,
+                             const double* u2, cudaStream_t s) {
+  const Dims& d = pl->d;
+  const int pairs = ceil_div((int64_t)d.Nx * d.Ny, 2);
+  const int blocks = ceil_div(pairs, 8);
+  if (pl->qk == 1)
+    z_forward_real_warp_kernel<P, 1><<<blocks, 256, 0, s>>>(d, pl->twnz, u0, u1, u2, pl->HZ);
+  else
+    z_forward_real_warp_kernel<P, 2><<<blocks, 256, 0, s>>>(d, pl->twnz, u0, u1, u2, pl->HZ);
 }
 
 // y_backward -> z_cross -> y_forward: HX <- H(state whose x-physical fields are in X)
 static int launch_transforms(jfb_kmm_plan* pl, cudaStream_t s) {
   const Dims& d = pl->d;
+  if (pl->py && pl->pz) {
+    launch_y_warp_any(pl, s, true);
+    JFB_CHECK_LAUNCH();
+    if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[2], s));
+    switch (pl->pz) {
+      case 2: launch_zcross_warp<2>(pl, s); break;
+      case 3: launch_zcross_warp<3>(pl, s); break;
+      case 4: launch_zcross_warp<4>(pl, s); break;
+      default: launch_zcross_warp<6>(pl, s); break;
+    }
+    JFB_CHECK_LAUNCH();
+    if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[3], s));
+    launch_y_warp_any(pl, s, false);
+    JFB_CHECK_LAUNCH();
+    if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[4], s));
+    return JFB_OK;
+  }
   dim3 gy(d.Nx, 6, d.Kz / pl->KC);
   y_backward_kernel<<<gy, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->X, pl->Y);
   JFB_CHECK_LAUNCH();
+  if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[2], s));
   const int zb = ceil_div((int64_t)d.Nx * d.My, kZRows);
   z_cross_kernel<<<zb, 256, pl->smem_z, s>>>(pl->ops, d, pl->fz, pl->twz, pl->Y, pl->HZ);
   JFB_CHECK_LAUNCH();
+  if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[3], s));
   dim3 gf(d.Nx, 3, d.Kz / pl->KC);
   y_forward_kernel<<<gf, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->HZ, pl->HX);
   JFB_CHECK_LAUNCH();
+  if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[4], s));
   return JFB_OK;
 }
 
@@ -411,7 +490,17 @@ static int steady_step(jfb_kmm_plan* pl, int64_t m, cudaStream_t s) {
   a.X = pl->X;
   int st = launch_pencil(pl, a, s);
   if (st) return st;
+  if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[1], s));
   return launch_transforms(pl, s);
+}
+
+// steady_step with an event recorded after the pencil kernel and after each
+// of the three periodic-axis kernels (ev[1..4]); ev[0] is recorded by the caller.
+static int steady_step_timed(jfb_kmm_plan* pl, int64_t m, cudaStream_t s, cudaEvent_t* ev) {
+  pl->timing_events = ev;
+  const int st = steady_step(pl, m, s);
+  pl->timing_events = nullptr;
+  return st;
 }
 
 // One IMEXRK3 startup step (_step_sbdf3 startup branch).
@@ -480,7 +569,7 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   JFB_REQUIRE(cfg->nonlinear_form == JFB_NONLINEAR_ROTATIONAL,
               "only the rotational nonlinear form is supported");
   JFB_REQUIRE(cfg->precision == JFB_PRECISION_FP64, "precision not supported");
-  JFB_REQUIRE(cfg->nx >= 9 && cfg->nx <= 2 * 32 * kMaxRows, "nx out of range [9, 256]");
+  JFB_REQUIRE(cfg->nx >= 9 && cfg->nx <= 64 * kMaxNR + 1, "nx out of range [9, 129]");
   JFB_REQUIRE(cfg->ny >= 4 && cfg->ny % 2 == 0 && cfg->nz >= 4 && cfg->nz % 2 == 0,
               "ny, nz must be even");
   JFB_REQUIRE(cfg->dt > 0 && cfg->nu > 0, "dt and nu must be positive");
@@ -526,12 +615,23 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   pl->smem_z = (size_t)2 * d.Mz * kZRows * 3 * sizeof(c64);
   pl->smem_pencil = (size_t)(6 * d.Nx * kLDW + kNW * 6 * d.Nx + d.Nx) * sizeof(c64);
   pl->smem_zf = (size_t)2 * d.Nz * (kZRows / 2) * 3 * sizeof(c64);
+  // warp-shuffle FFT paths (lengths 32 P, P in {2, 3, 4, 6}; Kz <= 64)
+  pl->qk = ceil_div(d.Kz, 32);
+  pl->py = warp_radix(d.My);
+  pl->pz = (pl->qk <= 2) ? warp_radix(d.Mz) : 0;
+  pl->pnz = (pl->qk <= 2) ? warp_radix(d.Nz) : 0;
+  pl->KCw = 16;
+  while (d.Kz % pl->KCw) pl->KCw /= 2;
+  pl->smem_yw_b = (size_t)(d.Ny + d.My) * (pl->KCw + 1) * sizeof(c64);
+  pl->smem_yw_f = pl->smem_yw_b;
   pl->smem_diag = (size_t)kNW * 4 * d.Nx * sizeof(c64) + 2 * kNW * sizeof(double);
   if (pl->smem_pencil > 227 * 1024 || pl->smem_y > 227 * 1024 || pl->smem_z > 227 * 1024) {
     set_error("grid too large for the shared-memory tiling");
     return fail(JFB_ERR_ARG);
   }
-  cudaFuncSetAttribute(pencil_stage_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(pencil_stage_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)pl->smem_pencil);
+  cudaFuncSetAttribute(pencil_stage_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)pl->smem_pencil);
   cudaFuncSetAttribute(y_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)pl->smem_y);
@@ -543,6 +643,16 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
                        (int)pl->smem_zf);
   cudaFuncSetAttribute(diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)pl->smem_diag);
+#define JFB_YW_ATTR(P)                                                                   \
+  cudaFuncSetAttribute(y_backward_warp_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                       (int)pl->smem_yw_b);                                              \
+  cudaFuncSetAttribute(y_forward_warp_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                       (int)pl->smem_yw_f);
+  JFB_YW_ATTR(2)
+  JFB_YW_ATTR(3)
+  JFB_YW_ATTR(4)
+  JFB_YW_ATTR(6)
+#undef JFB_YW_ATTR
   JFB_CHECK_LAUNCH();
 
   // constant operators
@@ -554,6 +664,23 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   pl->ops.field = p;
   UP(Q, op.Q);
   UP(V, op.V);
+  {
+    const int N = d.Nx, Jh = (N + 1) / 2, Jl = N / 2, Ne = (N + 1) / 2, No = N / 2;
+    std::vector<double> VE((size_t)Jh * Ne), VO((size_t)Jh * std::max(1, No)),
+        QE((size_t)Ne * Jh), QO((size_t)std::max(1, No) * std::max(1, Jl));
+    for (int j = 0; j < Jh; ++j) {
+      for (int m = 0; m < Ne; ++m) VE[(size_t)j * Ne + m] = op.V[(size_t)j * N + 2 * m];
+      for (int m = 0; m < No; ++m) VO[(size_t)j * No + m] = op.V[(size_t)j * N + 2 * m + 1];
+    }
+    for (int m = 0; m < Ne; ++m)
+      for (int j = 0; j < Jh; ++j) QE[(size_t)m * Jh + j] = op.Q[(size_t)(2 * m) * N + j];
+    for (int m = 0; m < No; ++m)
+      for (int j = 0; j < Jl; ++j) QO[(size_t)m * Jl + j] = op.Q[(size_t)(2 * m + 1) * N + j];
+    UP(VE, VE);
+    UP(VO, VO);
+    UP(QE, QE);
+    UP(QO, QO);
+  }
   UP(ns, op.ns);
   UP(sB0, op.SB.s0);
   UP(sB2, op.SB.s2);
@@ -561,12 +688,15 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   UP(mlo, op.mlo);
   UP(mdi, op.mdi);
   UP(mhi, op.mhi);
+  std::vector<double> luu_inv(op.lu_u), bu0_inv(op.bu0);
+  for (double& v : luu_inv) v = 1.0 / v;
+  for (double& v : bu0_inv) v = 1.0 / v;
   UP(lul, op.lu_l);
-  UP(luu, op.lu_u);
+  UP(luu, luu_inv);
   UP(xphys, op.xphys);
   UP(bl2, op.bl2);
   UP(bl4, op.bl4);
-  UP(bu0, op.bu0);
+  UP(bu0, bu0_inv);
   UP(bu2, op.bu2);
   UP(bu4, op.bu4);
   UP(fejer, op.fejer);
@@ -802,9 +932,18 @@ extern "C" int jfb_kmm_state_from_physical(jfb_kmm_plan* pl, const double* u0,
   Dims d = pl->d;
   const size_t P = d.P;
   // z: real Nz -> Kz half spectrum (into HZ as [f][j][y][kz]), scaled 1/Nz
-  const int zb = ceil_div((int64_t)d.Nx * d.Ny, kZRows);
-  z_forward_real_kernel<<<zb, 256, pl->smem_zf, s>>>(d, pl->fnz, pl->twnz, u0, u1, u2,
-                                                     pl->HZ);
+  if (pl->pnz) {
+    switch (pl->pnz) {
+      case 2: launch_zfwd_warp<2>(pl, u0, u1, u2, s); break;
+      case 3: launch_zfwd_warp<3>(pl, u0, u1, u2, s); break;
+      case 4: launch_zfwd_warp<4>(pl, u0, u1, u2, s); break;
+      default: launch_zfwd_warp<6>(pl, u0, u1, u2, s); break;
+    }
+  } else {
+    const int zb = ceil_div((int64_t)d.Nx * d.Ny, kZRows);
+    z_forward_real_kernel<<<zb, 256, pl->smem_zf, s>>>(d, pl->fnz, pl->twnz, u0, u1, u2,
+                                                       pl->HZ);
+  }
   JFB_CHECK_LAUNCH();
   // y: forward FFT of length Ny (no truncation), scaled 1/Ny
   Dims dy = d;
@@ -862,5 +1001,51 @@ extern "C" int jfb_kmm_diagnostics(jfb_kmm_plan* pl, double* out, void* stream) 
                                       pl->cfg.ly, pl->cfg.lz, pl->cfg.x_lo, pl->cfg.x_hi,
                                       out);
   JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_timed_steps(jfb_kmm_plan* pl, int64_t steps, void* flush_buf,
+                                   int64_t flush_bytes, double* kernel_ms, double* step_ms,
+                                   void* stream) {
+  JFB_REQUIRE(pl && kernel_ms && step_ms, "null pointer");
+  JFB_REQUIRE(steps >= 0, "steps must be >= 0");
+  if (!pl->have_state) {
+    set_error("no state loaded");
+    return JFB_ERR_STATE;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = ensure_H(pl, s);
+  if (st) return st;
+  while (steps > 0 && pl->hist < 2) {  // startup steps are not timed
+    st = startup_step(pl, s);
+    if (st) return st;
+    pl->n += 1;
+    pl->hist += 1;
+    pl->explicit_u12 = false;
+  }
+  cudaEvent_t ev[5];
+  for (int k = 0; k < 5; ++k) JFB_CHECK_CUDA(cudaEventCreate(&ev[k]));
+  for (int k = 0; k < 4; ++k) kernel_ms[k] = 0.0;
+  *step_ms = 0.0;
+  for (int64_t i = 0; i < steps; ++i) {
+    if (flush_buf && flush_bytes > 0)
+      JFB_CHECK_CUDA(cudaMemsetAsync(flush_buf, (int)(i & 0xff), (size_t)flush_bytes, s));
+    const int64_t m = pl->n;
+    // the four launches of steady_step, with an event after each
+    JFB_CHECK_CUDA(cudaEventRecord(ev[0], s));
+    st = steady_step_timed(pl, m, s, ev);
+    if (st) return st;
+    JFB_CHECK_CUDA(cudaEventSynchronize(ev[4]));
+    float ms;
+    for (int k = 0; k < 4; ++k) {
+      JFB_CHECK_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      kernel_ms[k] += ms;
+    }
+    JFB_CHECK_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[4]));
+    *step_ms += ms;
+    pl->n += 1;
+    pl->explicit_u12 = false;
+  }
+  for (int k = 0; k < 5; ++k) cudaEventDestroy(ev[k]);
   return JFB_OK;
 }

@@ -23,11 +23,15 @@ namespace jfb {
 
 constexpr int kNW = 8;         // pencils (warps) per pencil_stage block
 constexpr int kLDW = kNW + 1;  // padded pencil stride in shared memory
-constexpr int kMaxRows = 4;    // rows per lane in the column-oriented solves (n <= 256)
+constexpr int kMaxNR = 2;      // rows per lane in the register solves (n <= 128)
 
 struct DevOps {
   const double* Q;   // [n][j] scalar-product quadrature (Nx x Nx)
   const double* V;   // [j][n] Chebyshev Vandermonde (Nx x Nx)
+  const double* VE;  // [j][m] = V[j][2m],   j < ceil(Nx/2)
+  const double* VO;  // [j][m] = V[j][2m+1], j < ceil(Nx/2)
+  const double* QE;  // [m][j] = Q[2m][j],   j < ceil(Nx/2)
+  const double* QO;  // [m][j] = Q[2m+1][j], j < floor(Nx/2)
   const double* ns;  // norm^2 / df (Nx)
   const double* sB0;
   const double* sB2;
@@ -36,7 +40,7 @@ struct DevOps {
   const double* mdi;
   const double* mhi;  // Dirichlet mass tri-band (nD)
   const double* lul;
-  const double* luu;    // its LU (nD)
+  const double* luu;    // its LU (nD): multipliers and reciprocal pivots
   const double* xphys;  // physical wall-normal nodes (Nx)
   const double* bl2;
   const double* bl4;
@@ -176,7 +180,7 @@ __device__ __forceinline__ void mass_solve_lane(const DevOps& o, const Dims& d, 
   for (int i = last; i >= 0; i -= 2) {
     c64 v = b[i];
     if (i + 2 < d.nD) v = v - o.mhi[i] * b[i + 2];
-    b[i] = (1.0 / o.luu[i]) * v;
+    b[i] = o.luu[i] * v;
   }
 }
 
@@ -196,68 +200,93 @@ __device__ __forceinline__ void bmass_solve_lane(const DevOps& o, const Dims& d,
     c64 v = b[i];
     if (i + 2 < d.nB) v = v - o.bu2[i] * b[i + 2];
     if (i + 4 < d.nB) v = v - o.bu4[i] * b[i + 4];
-    b[i] = (1.0 / o.bu0[i]) * v;
+    b[i] = o.bu0[i] * v;
   }
 }
 
-// Forward elimination with the unit-lower factor of a packed record
-// (L[i, i-2], L[i, i-4]) for one parity; single lane.
-__device__ __forceinline__ void fwd_elim_lane(const double* rec, int n, c64* y, int par) {
-  for (int i = par; i < n; i += 2) {
-    c64 v = y[i];
-    if (i >= 2) v = v - rec[2 * i] * y[i - 2];
-    if (i >= 4) v = v - rec[2 * i + 1] * y[i - 4];
-    y[i] = v;
-  }
-}
-
-// Column-oriented back substitution of one parity class (size m, packed
-// column-major upper triangle with reciprocal diagonal) held in `y` at
-// indices 2 r + par.  All lanes participate.
-__device__ __forceinline__ void back_subst_warp(const double* __restrict__ Up, int m, c64* y,
-                                                int par, int lane) {
-  c64 yr[kMaxRows];
+// Solve one parity class of a packed record in registers.  Lane r holds
+// row 2r + par (and 2(r+32) + par when m > 32).  Forward elimination with
+// the unit-lower factor (L[i, i-2], L[i, i-4]) passes the solved rows down
+// the lanes with shuffles; back substitution is column-oriented: the owner
+// lane of column c scales by the reciprocal pivot, broadcasts x_c, and every
+// lane r < c subtracts U[r, c] x_c.  All factor entries a lane needs are
+// loaded before the dependent chains start (no memory latency on the chain).
+template <int NR>
+__device__ __forceinline__ void parity_solve_regs(const double* __restrict__ rec, int n,
+                                                  c64* y, int par, int lane) {
+  const int m0 = (n + 1) / 2;
+  const int m = par ? n / 2 : m0;
+  const double* __restrict__ Up = rec + 2 * n + (par ? m0 * (m0 + 1) / 2 : 0);
+  c64 yr[NR];
+  double l1[NR], l2[NR];
 #pragma unroll
-  for (int s = 0; s < kMaxRows; ++s) {
+  for (int s = 0; s < NR; ++s) {
     const int r = lane + 32 * s;
-    yr[s] = (r < m) ? y[2 * r + par] : cmk(0.0, 0.0);
+    const int i = 2 * r + par;
+    const bool ok = r < m;
+    yr[s] = ok ? y[i] : cmk(0.0, 0.0);
+    l1[s] = ok ? __ldg(rec + 2 * i) : 0.0;
+    l2[s] = ok ? __ldg(rec + 2 * i + 1) : 0.0;
   }
-  for (int c = m - 1; c >= 0; --c) {
-    const int owner = c & 31, slot = c >> 5;
-    const int col = c * (c + 1) / 2;
-    c64 xc = cmk(0.0, 0.0);
+  // forward elimination: y_r -= l1_r y_{r-1} + l2_r y_{r-2}
+  c64 ym1 = cmk(0.0, 0.0), ym2 = cmk(0.0, 0.0);
 #pragma unroll
-    for (int s = 0; s < kMaxRows; ++s)
-      if (s == slot && lane == owner) {
-        xc = Up[col + c] * yr[s];
-        yr[s] = xc;
+  for (int s = 0; s < NR; ++s) {
+    for (int r0 = 0; r0 < 32; ++r0) {
+      const int r = r0 + 32 * s;
+      if (r >= m) break;
+      if (lane == r0) yr[s] = yr[s] - l1[s] * ym1 - l2[s] * ym2;
+      c64 t;
+      t.re = __shfl_sync(0xffffffffu, yr[s].re, r0);
+      t.im = __shfl_sync(0xffffffffu, yr[s].im, r0);
+      ym2 = ym1;
+      ym1 = t;
+    }
+  }
+  // back substitution, 32 columns per chunk, factor column entries prefetched
+#pragma unroll
+  for (int cs = NR - 1; cs >= 0; --cs) {
+    double u[NR][32];
+#pragma unroll
+    for (int s = 0; s < NR; ++s)
+#pragma unroll
+      for (int cc = 0; cc < 32; ++cc) {
+        const int c = cc + 32 * cs;
+        const int r = lane + 32 * s;
+        u[s][cc] = (s <= cs && c < m && r <= c) ? __ldg(Up + c * (c + 1) / 2 + r) : 0.0;
       }
-    xc.re = __shfl_sync(0xffffffffu, xc.re, owner);
-    xc.im = __shfl_sync(0xffffffffu, xc.im, owner);
 #pragma unroll
-    for (int s = 0; s < kMaxRows; ++s) {
-      const int r = lane + 32 * s;
-      if (r < c) yr[s] = yr[s] - Up[col + r] * xc;
+    for (int cc = 31; cc >= 0; --cc) {
+      const int c = cc + 32 * cs;
+      if (c >= m) continue;
+      c64 xc = cmk(0.0, 0.0);
+      if (lane == cc) {
+        xc = u[cs][cc] * yr[cs];  // reciprocal pivot
+        yr[cs] = xc;
+      }
+      xc.re = __shfl_sync(0xffffffffu, xc.re, cc);
+      xc.im = __shfl_sync(0xffffffffu, xc.im, cc);
+#pragma unroll
+      for (int s = 0; s < NR; ++s) {
+        const int r = lane + 32 * s;
+        if (s <= cs && r < c) yr[s] = yr[s] - u[s][cc] * xc;
+      }
     }
   }
 #pragma unroll
-  for (int s = 0; s < kMaxRows; ++s) {
+  for (int s = 0; s < NR; ++s) {
     const int r = lane + 32 * s;
     if (r < m) y[2 * r + par] = yr[s];
   }
   __syncwarp();
 }
 
-// Solve a packed system of size n in place on y (both parities).
+// Solve a packed system of size n <= 64 * NR in place on y (both parities).
+template <int NR>
 __device__ __forceinline__ void packed_solve_warp(const double* __restrict__ rec, int n,
                                                   c64* y, int lane) {
-  if (lane < 2) fwd_elim_lane(rec, n, y, lane);
-  __syncwarp();
-  const int m0 = (n + 1) / 2, m1 = n / 2;
-  const double* U0 = rec + 2 * n;
-  const double* U1 = U0 + m0 * (m0 + 1) / 2;
-  back_subst_warp(U0, m0, y, 0, lane);
-  back_subst_warp(U1, m1, y, 1, lane);
+  parity_solve_regs<NR>(rec, n, y, 0, lane);
+  parity_solve_regs<NR>(rec, n, y, 1, lane);
 }
 
 // Velocity reconstruction (channelflow_kmm.py:855-870): from u0 (TB, in A3)
@@ -326,9 +355,109 @@ __device__ __forceinline__ void cta_gemm(const double* __restrict__ A, int R, in
   }
 }
 
+// Parity-split x-backward: with x_{N-1-j} = -x_j and T_n(-x) = (-1)^n T_n(x),
+// u(x_j) = E_j + O_j and u(x_{N-1-j}) = E_j - O_j, where E (O) sums the even
+// (odd) coefficients.  Halves the Vandermonde work.
+// out[(f * N + j) * kLDW + w] for the NF fields of in(f, n, w).
+template <typename InFn>
+__device__ __forceinline__ void cta_backward_parity(const double* __restrict__ VE,
+                                                    const double* __restrict__ VO, int N,
+                                                    int NF, InFn in, c64* out) {
+  const int C = NF * kNW;
+  const int G = blockDim.x / C;
+  const int t = threadIdx.x;
+  const int col = t % C, g = t / C;
+  const int Jh = (N + 1) / 2, Ne = (N + 1) / 2, No = N / 2;
+  if (g >= G) return;
+  const int f = col / kNW, w = col % kNW;
+  for (int j0 = g; j0 < Jh; j0 += 4 * G) {
+    c64 E[4], O[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) E[q] = O[q] = cmk(0.0, 0.0);
+    for (int m = 0; m < Ne; ++m) {
+      const c64 x = in(f, 2 * m, w);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = j0 + q * G;
+        if (j < Jh) {
+          const double a = __ldg(VE + (size_t)j * Ne + m);
+          E[q] = cmk(E[q].re + a * x.re, E[q].im + a * x.im);
+        }
+      }
+    }
+    for (int m = 0; m < No; ++m) {
+      const c64 x = in(f, 2 * m + 1, w);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = j0 + q * G;
+        if (j < Jh) {
+          const double a = __ldg(VO + (size_t)j * No + m);
+          O[q] = cmk(O[q].re + a * x.re, O[q].im + a * x.im);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = j0 + q * G;
+      if (j < Jh) {
+        out[(f * N + j) * kLDW + w] = E[q] + O[q];
+        if (N - 1 - j != j) out[(f * N + N - 1 - j) * kLDW + w] = E[q] - O[q];
+      }
+    }
+  }
+}
+
+// Parity-split x-forward scalar products: sp[2m] = sum_j QE[m][j] (u_j +
+// u_{N-1-j}) (middle node once), sp[2m+1] = sum_j QO[m][j] (u_j - u_{N-1-j}).
+// Input phys(f, j, w); output out[(f * N + n) * kLDW + w].
+template <typename InFn>
+__device__ __forceinline__ void cta_forward_parity(const double* __restrict__ QE,
+                                                   const double* __restrict__ QO, int N,
+                                                   int NF, InFn phys, c64* out) {
+  const int C = NF * kNW;
+  const int G = blockDim.x / C;
+  const int t = threadIdx.x;
+  const int col = t % C, g = t / C;
+  const int Jh = (N + 1) / 2, Jl = N / 2, Ne = (N + 1) / 2, No = N / 2;
+  if (g >= G) return;
+  const int f = col / kNW, w = col % kNW;
+  // virtual rows: [0, Ne) even outputs, [Ne, Ne + No) odd outputs
+  const int R = Ne + No;
+  for (int r0 = g; r0 < R; r0 += 4 * G) {
+    c64 acc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = cmk(0.0, 0.0);
+    for (int j = 0; j < Jh; ++j) {
+      const c64 a = phys(f, j, w);
+      const c64 b = (N - 1 - j != j) ? phys(f, N - 1 - j, w) : cmk(0.0, 0.0);
+      const c64 sum = a + b, dif = a - b;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = r0 + q * G;
+        if (r < Ne) {
+          const double c = __ldg(QE + (size_t)r * Jh + j);
+          acc[q] = cmk(acc[q].re + c * sum.re, acc[q].im + c * sum.im);
+        } else if (r < R && j < Jl) {
+          const double c = __ldg(QO + (size_t)(r - Ne) * Jl + j);
+          acc[q] = cmk(acc[q].re + c * dif.re, acc[q].im + c * dif.im);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = r0 + q * G;
+      if (r < R) {
+        const int n = (r < Ne) ? 2 * r : 2 * (r - Ne) + 1;
+        out[(f * N + n) * kLDW + w] = acc[q];
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // pencil_stage: see file header.  Block = kNW warps, one pencil per warp.
 // ---------------------------------------------------------------------------
+template <int NR>
 __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   c64* R1 = reinterpret_cast<c64*>(smem_raw);  // 6 * Nx * kLDW
@@ -392,8 +521,8 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
     __syncthreads();
     // scalar products (T_n, H_f)_w for the 3 fields -> R1[3..5]
     c64* sT = R1 + 3 * d.Nx * kLDW;
-    cta_gemm(o.Q, d.Nx, d.Nx, 3,
-             [&](int f, int k, int w) { return R1[(f * d.Nx + k) * kLDW + w]; }, sT);
+    cta_forward_parity(o.QE, o.QO, d.Nx, 3,
+                       [&](int f, int j, int w) { return R1[(f * d.Nx + j) * kLDW + w]; }, sT);
     __syncthreads();
     if (a.mode == kFromPhys) {
       // TB.forward(u0), TD.forward(u1), TD.forward(u2), mask, g = i ky u2 - i kz u1
@@ -599,10 +728,10 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
       // ---- solves ----
       const double* rec_u = a.fac.su + (size_t)mode_idx * a.fac.su_rec;
       const double* rec_g = a.fac.sg + (size_t)mode_idx * a.fac.sg_rec;
-      packed_solve_warp(rec_u, d.nB, A3, lane);
-      packed_solve_warp(rec_g, d.nD, A4, lane);
+      packed_solve_warp<NR>(rec_u, d.nB, A3, lane);
+      packed_solve_warp<NR>(rec_g, d.nD, A4, lane);
       if (mean_pencil) {
-        packed_solve_warp(a.fac.s00, d.nD, sVW, lane);
+        packed_solve_warp<NR>(a.fac.s00, d.nD, sVW, lane);
         for (int i = lane; i < d.nD; i += 32) a.vw_out[i] = sVW[i];
         __syncwarp();
       }
@@ -624,28 +753,16 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
 
   // ---------------- phase B: u and omega in orthogonal coefficients -------
   if (active) {
-    // A5 = uo0 (already), A0 <- uo1, A1 <- uo2 (in place, descending)
-    if (lane == 0) {
-      for (int n = d.Nx - 1; n >= 0; --n) {
-        c64 v = (n < d.nD) ? A0[n] : cmk(0.0, 0.0);
-        if (n >= 2) v = v - A0[n - 2];
-        A0[n] = v;
-      }
-    } else if (lane == 1) {
-      for (int n = d.Nx - 1; n >= 0; --n) {
-        c64 v = (n < d.nD) ? A1[n] : cmk(0.0, 0.0);
-        if (n >= 2) v = v - A1[n - 2];
-        A1[n] = v;
-      }
-    }
-    __syncwarp();
-    chebder_warp(A1, A3, d.Nx, d.dfx, lane);  // A3 = D uo2
-    chebder_warp(A0, A4, d.Nx, d.dfx, lane);  // A4 = D uo1
+    // A5 = uo0 (already); uo1 = S_D^T u1 -> A2, uo2 = S_D^T u2 -> A3
+    apply_SDT(d, A0, A2, lane);
+    apply_SDT(d, A1, A3, lane);
+    chebder_warp(A3, A4, d.Nx, d.dfx, lane);  // A4 = D uo2
+    chebder_warp(A2, A0, d.Nx, d.dfx, lane);  // A0 = D uo1
     for (int n = lane; n < d.Nx; n += 32) {
-      const c64 u0 = A5[n], u1 = A0[n], u2 = A1[n];
-      A2[n] = mul_i(kyp * u2 - kzp * u1);        // omega_0
-      A3[n] = mul_i(kzp * u0) - A3[n];           // omega_1
-      A4[n] = A4[n] - mul_i(kyp * u0);           // omega_2
+      const c64 u0 = A5[n], u1 = A2[n], u2 = A3[n];
+      A1[n] = mul_i(kyp * u2 - kzp * u1);        // omega_0
+      A4[n] = mul_i(kzp * u0) - A4[n];           // omega_1
+      A0[n] = A0[n] - mul_i(kyp * u0);           // omega_2
     }
     __syncwarp();
   } else {
@@ -654,13 +771,14 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
   }
   __syncthreads();
   // x-backward of the six fields: field order (u0, u1, u2, w0, w1, w2)
-  // lives in arrays (A5, A0, A1, A2, A3, A4).
-  cta_gemm(o.V, d.Nx, d.Nx, 6,
-           [&](int f, int k, int w) {
-             const int arr = (f == 0) ? 5 : f - 1;
-             return ARR[(w * 6 + arr) * d.Nx + k];
-           },
-           R1);
+  // lives in arrays (A5, A2, A3, A1, A4, A0).
+  cta_backward_parity(o.VE, o.VO, d.Nx, 6,
+                      [&](int f, int k, int w) {
+                        const int arr = (f == 0) ? 5 : (f == 1) ? 2 : (f == 2) ? 3
+                                        : (f == 3) ? 1 : (f == 4) ? 4 : 0;
+                        return ARR[(w * 6 + arr) * d.Nx + k];
+                      },
+                      R1);
   __syncthreads();
   for (int idx = threadIdx.x; idx < 6 * d.Nx * kNW; idx += blockDim.x) {
     const int w = idx % kNW, fi = idx / kNW;

@@ -257,6 +257,66 @@ class KMM:
         _lib.call("jfb_kmm_advance", self._plan, int(steps), self._stream())
         self._current = None
 
+    # -- meshes and physical-space entry points -------------------------------
+    def mesh(self):
+        """Quadrature mesh (x on Gauss-Chebyshev nodes, y/z uniform), broadcast
+        like ``TensorProductSpace.mesh`` (tensorproductspace.py:207-232)."""
+        Nx, Ny, Nz = self.N
+        (a, b), (y0, y1), (z0, z1) = self.domain
+        X = torch.cos(
+            math.pi + (2 * torch.arange(Nx, dtype=torch.float64) + 1) * math.pi / (2 * Nx)
+        )
+        x = a + (X + 1.0) * (b - a) / 2.0
+        y = y0 + torch.arange(Ny, dtype=torch.float64) * (y1 - y0) / Ny
+        z = z0 + torch.arange(Nz, dtype=torch.float64) * (z1 - z0) / Nz
+        dev = self.device
+        return (
+            x.reshape(Nx, 1, 1).to(dev),
+            y.reshape(1, Ny, 1).to(dev),
+            z.reshape(1, 1, Nz).to(dev),
+        )
+
+    def state_from_physical(self, u_phys) -> KMMState:
+        """``KMM.state_from_physical`` (channelflow_kmm.py:677-683): real
+        velocity samples (Nx, Ny, Nz) on the quadrature mesh -> coefficient
+        state with a zero history."""
+        shape = self.N
+        fields = []
+        for v in u_phys:
+            t = torch.as_tensor(v, device=self.device)
+            if t.is_complex():
+                t = t.real
+            t = torch.broadcast_to(t.to(torch.float64), shape).contiguous()
+            fields.append(t)
+        _lib.call(
+            "jfb_kmm_state_from_physical", self._plan, fields[0].data_ptr(),
+            fields[1].data_ptr(), fields[2].data_ptr(), self._stream(),
+        )
+        return self._fetch(0.0)
+
+    def diagnostics_tensor(self, state: KMMState) -> torch.Tensor:
+        """Device tensor (8,) of the scalar diagnostics of ``state``."""
+        self._load(state)
+        out = torch.empty(8, dtype=torch.float64, device=self.device)
+        _lib.call("jfb_kmm_diagnostics", self._plan, out.data_ptr(), self._stream())
+        return out
+
+    DIAGNOSTIC_NAMES = (
+        "Epert", "Etot", "divL2", "u_top", "u_bot",
+        "wall_shear_top", "wall_shear_bot", "mean_shear",
+    )
+
+    def diagnostics(self, state: KMMState) -> dict[str, float]:
+        """pcf_fluctuations_jax.py:131-161 (with U_wall = 0 for the plain KMM)."""
+        vals = self.diagnostics_tensor(state).cpu().tolist()
+        return dict(zip(self.DIAGNOSTIC_NAMES, vals, strict=True))
+
+    def perturbation_energy(self, state: KMMState) -> float:
+        return self.diagnostics(state)["Epert"]
+
+    def divergence_l2(self, state: KMMState) -> float:
+        return self.diagnostics(state)["divL2"]
+
     def convection(self, state: KMMState):
         """Dealiased rotational convection in TD coefficients (channelflow_kmm.py:772-782)."""
         self._load(state)
@@ -311,6 +371,19 @@ class PlaneCouetteFluctuation(KMM):
             _u_wall=self.U_wall,
         )
         self.dUb_dx = self.U_wall
+
+    def initial_state(self) -> KMMState:
+        """Deterministic analytic perturbation (pcf_fluctuations_jax.py:77-97)."""
+        x, y, z = self.mesh()
+        amp = self.perturbation_amplitude
+        wall = 1.0 - x**2
+        Ly = self.domain[1][1] - self.domain[1][0]
+        Lz = self.domain[2][1] - self.domain[2][0]
+        tp = 2.0 * math.pi
+        u0 = amp * wall * torch.sin(tp * y / Ly) * torch.cos(tp * z / Lz)
+        u1 = amp * wall * torch.cos(tp * y / Ly) * torch.sin(tp * z / Lz)
+        u2 = amp * wall * torch.sin(2 * tp * y / Ly) * torch.cos(2 * tp * z / Lz)
+        return self.state_from_physical((u0, u1, u2))
 
 
 # reference name

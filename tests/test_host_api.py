@@ -1,0 +1,67 @@
+"""Host-side logic that needs no GPU: argument validation of the solver
+objects, the workload generator and the benchmark's byte model."""
+
+import math
+
+import numpy as np
+import pytest
+
+import bench
+from jaxfun_b200 import workloads
+from jaxfun_b200.kmm import KMM, PlaneCouetteFluctuation
+
+
+@pytest.mark.parametrize("kw", [
+    {"time_integrator": "IMEXRK222"},
+    {"nonlinear_form": "gradient"},
+    {"family": "L"},
+    {"padding_factor": (1.5, 1.5, 1.5)},
+])
+def test_unsupported_options_are_rejected_before_any_device_work(kw):
+    with pytest.raises(NotImplementedError):
+        KMM(N=(17, 16, 16), **kw)
+
+
+@pytest.mark.parametrize("kw, exc", [
+    ({"nonlinear_form": "skew"}, ValueError),
+    ({"coefficient_path": "fast"}, ValueError),
+    ({"time_integrator": "RK4"}, ValueError),
+])
+def test_invalid_options_raise_value_error(kw, exc):
+    with pytest.raises(exc):
+        PlaneCouetteFluctuation(N=(17, 16, 16), **kw)
+
+
+def test_workload_fields_are_divergence_free_and_wall_bounded():
+    N = (33, 16, 16)
+    dom = bench.domain()
+    u0, u1, u2 = workloads.couette_perturbation_fields(N, dom)
+    assert u0.shape == N and np.isfinite(u0).all()
+    # no-slip: fields vanish towards the walls like (1 - x^2)
+    x = np.cos(np.pi + (2 * np.arange(N[0]) + 1) * np.pi / (2 * N[0]))
+    assert np.abs(u1[0]).max() < 10 * (1 - x[0] ** 2) * np.abs(u1).max()
+    # spectral divergence of the analytic construction: d_y u1 + d_z u2 = 0 per x-plane
+    # (u0 varies with x only through the envelope)
+    Ly, Lz = dom[1][1] - dom[1][0], dom[2][1] - dom[2][0]
+    ky = np.fft.fftfreq(N[1], 1.0 / N[1]) * 2 * np.pi / Ly
+    kz = np.fft.fftfreq(N[2], 1.0 / N[2]) * 2 * np.pi / Lz
+    f1, f2 = np.fft.fft2(u1), np.fft.fft2(u2)
+    u0x = np.gradient(u0, x, axis=0, edge_order=2)
+    div = np.fft.ifft2(1j * ky[None, :, None] * f1 + 1j * kz[None, None, :] * f2).real + u0x
+    assert np.abs(div[N[0] // 2]).max() < 1e-2 * np.abs(u0x).max() + 1e-12
+    s = workloads.scale_to_energy((u0,), 4.0, 1.0)[0]
+    np.testing.assert_allclose(s, u0 * 0.5)
+
+
+def test_stage_byte_model_matches_the_canonical_figure():
+    sb = bench.stage_bytes((65, 64, 64), 96)
+    # 43 E_s + 18 E_m complex at 16 B: 153.75 MB for 65x64x64
+    assert abs(sb["step"] / 1e6 - 153.75) < 0.01
+    fused = sum(sb[k] for k in ("pencil_stage", "y_backward", "z_cross", "y_forward"))
+    assert fused < sb["step"]
+
+
+def test_measured_peak_has_a_source():
+    peak, kind = bench.measured_peak()
+    assert peak > 1000 and kind in ("measured", "fallback")
+    assert math.isfinite(peak)

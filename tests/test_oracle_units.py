@@ -1,0 +1,117 @@
+"""Unit checks of the oracle's building blocks against independent NumPy
+computations (CPU only)."""
+
+import numpy as np
+import pytest
+
+from oracle import kmm as ok
+
+
+@pytest.mark.parametrize("N", [9, 17, 33, 65])
+def test_chebyshev_transforms_round_trip_and_nodes(N):
+    c = ok.Chebyshev1D(N)
+    rng = np.random.default_rng(N)
+    coef = rng.standard_normal(N)
+    u = c.backward(coef)
+    V = np.polynomial.chebyshev.chebvander(c.nodes(), N - 1)
+    np.testing.assert_allclose(u, V @ coef, atol=1e-13)
+    np.testing.assert_allclose(c.forward(u), coef, atol=1e-13)
+    # scalar products are exact Gauss-Chebyshev quadrature
+    sp = c.scalar_product(u)
+    np.testing.assert_allclose(sp, c.norm_squared() * coef, atol=1e-12)
+
+
+@pytest.mark.parametrize("N", [9, 33])
+def test_derivative_recurrences(N):
+    rng = np.random.default_rng(1)
+    coef = rng.standard_normal(N)
+    ch = ok.Chebyshev1D(N).derivative_coeffs(coef, 2)
+    ref = np.polynomial.chebyshev.chebder(coef, 2)
+    np.testing.assert_allclose(ch[: ref.size], ref, atol=1e-10)
+    lg = ok.Legendre1D(N).derivative_coeffs(coef, 1)
+    ref = np.polynomial.legendre.legder(coef, 1)
+    np.testing.assert_allclose(lg[: ref.size], ref, atol=1e-10)
+
+
+@pytest.mark.parametrize("family", ["C", "L"])
+def test_shen_bases_satisfy_boundary_conditions(family):
+    orth = ok.make_orthogonal(family, 17)
+    for bc, ders in (("dirichlet", (0,)), ("biharmonic", (0, 1))):
+        comp = ok.Composite1D(orth, bc)
+        for k in ders:
+            rows = comp.boundary_rows(k)
+            assert np.abs(rows).max() < 1e-12
+
+
+def test_galerkin_matrices_match_quadrature():
+    """(T_i, T_j^(k))_w by exact Gauss-Chebyshev quadrature of chebder."""
+    N = 17
+    c = ok.Chebyshev1D(N)
+    x = c.nodes(N)
+    w = np.full(N, np.pi / N)
+    V = np.polynomial.chebyshev.chebvander(x, N - 1)
+    for k in (0, 2, 4):
+        Dk = np.zeros((N, N))
+        for j in range(N):
+            e = np.zeros(N)
+            e[j] = 1
+            d = np.polynomial.chebyshev.chebder(e, k) if k else e
+            Dk[:, j] = V[:, : d.size] @ d
+        quad = (V * w[:, None]).T @ Dk
+        np.testing.assert_allclose(c.galerkin_matrix(k), quad, atol=1e-9 * np.abs(quad).max())
+
+
+def test_banded_lu_matches_dense_solve():
+    rng = np.random.default_rng(3)
+    n, p, q = 21, 4, 8
+    A = np.zeros((5, n, n))
+    for b in range(5):
+        for off in range(-p, q + 1, 2):
+            A[b] += np.diag(rng.standard_normal(n - abs(off)), off)
+        A[b] += np.eye(n) * 20
+    lu = ok.BandedLU.factor(A)
+    rhs = rng.standard_normal((5, n)) + 1j * rng.standard_normal((5, n))
+    x = lu.solve(rhs)
+    np.testing.assert_allclose(np.einsum("bij,bj->bi", A, x), rhs, atol=1e-12)
+
+
+def test_wavenumber_solver_matches_kronecker_solve():
+    """tests/la/test_tpmatrices_solvers.py:131-138 of the reference, on a
+    Helmholtz system: per-mode solve vs the assembled Kronecker operator."""
+    N = (9, 4, 6)
+    D = ok.Composite1D(ok.Chebyshev1D(N[0]), "dirichlet")
+    F1, F2 = ok.Fourier1D(N[1]), ok.Fourier1D(N[2])
+    op = ok.mass_terms(D, F1, F2) - ok.laplace_terms(D, F1, F2).scale(0.1)
+    solver = ok.WavenumberSolver(op)
+    rng = np.random.default_rng(0)
+    rhs = rng.standard_normal(solver.shape) + 1j * rng.standard_normal(solver.shape)
+    x = solver.solve(rhs)
+    np.testing.assert_allclose(op.matvec(x), rhs, atol=1e-10 * np.abs(rhs).max())
+
+
+def test_sbdf3_third_order():
+    """Third-order convergence of the SBDF3 combination on y' = -y + sin(t)
+    split as implicit -y, explicit sin(t) (tests/integrators/test_sbdf3.py)."""
+    def run(dt, T=2.0):
+        n = int(round(T / dt))
+        ex = lambda t: 0.5 * (np.sin(t) - np.cos(t)) + 1.5 * np.exp(-t)  # noqa: E731
+        y = [ex(0.0), ex(dt), ex(2 * dt)]
+        for k in range(2, n):
+            t = k * dt
+            nl = [np.sin(t), np.sin(t - dt), np.sin(t - 2 * dt)]
+            rhs = (18 * y[-1] - 9 * y[-2] + 2 * y[-3]) / 11 + dt * (
+                18 * nl[0] - 18 * nl[1] + 6 * nl[2]) / 11
+            y.append(rhs / (1 + ok.SBDF3_IMPLICIT * dt))
+        return abs(y[-1] - ex(n * dt))
+    e1, e2 = run(0.02), run(0.01)
+    order = np.log2(e1 / e2)
+    assert 2.7 < order < 3.3
+
+
+def test_fourier_padding_round_trip():
+    f = ok.Fourier1D(16)
+    rng = np.random.default_rng(2)
+    c = rng.standard_normal(16) + 1j * rng.standard_normal(16)
+    c[8] = 0
+    u = f.backward(c, 24, 0)
+    np.testing.assert_allclose(f.forward(u, 0), c, atol=1e-14)
