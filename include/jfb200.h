@@ -56,6 +56,23 @@ int jfb_dia_matvec(const double* data, const int64_t* offsets, int64_t n_diags,
 int jfb_banded_lu_factor(double* band, int64_t n_batch, int64_t p, int64_t q,
                          int64_t n, void* stream);
 
+/* Allocation-free variant of jfb_banded_lu_factor (no counterpart in the
+ * reference).  For callers that cannot allocate device memory: code running
+ * during CUDA stream capture, inside an XLA custom call or under another
+ * framework's memory pool.  It factors the same batch in place with the same
+ * arithmetic but keeps the per-matrix pivot status in a fixed device array of
+ * the library (256 KiB per GPU, held until exit), so it calls no allocator.
+ * n_batch must not exceed JFB_NOALLOC_LU_MAX_BATCH (else JFB_ERR_ARG).  On a
+ * zero or non-finite pivot it returns JFB_ERR_SINGULAR and, if
+ * first_singular is non-NULL, the lowest singular matrix index there (-1 when
+ * none).  Synchronises `stream`.  The first call on a device looks up the
+ * array's device address, so make it before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU (different streams or
+ * threads) race. */
+#define JFB_NOALLOC_LU_MAX_BATCH 65536
+int jfb_banded_lu_factor_noalloc(double* band, int64_t n_batch, int64_t p, int64_t q,
+                                 int64_t n, int32_t* first_singular, void* stream);
+
 /* TPMatricesWavenumberSolver.solve / solve_many / *_with_runtime_args
  * (src/jaxfun/la/tpmatrix.py:1550-1677, batched recurrence 686-799).
  * L: (n_F, n_L, n_P) unit-lower sub-diagonals with L_offsets (< 0);

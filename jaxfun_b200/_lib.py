@@ -88,6 +88,9 @@ SIGNATURES = {
     "jfb_banded_lu_factor": (
         c_int, [c_void_p, c_int64, c_int64, c_int64, c_int64, c_void_p]
     ),
+    "jfb_banded_lu_factor_noalloc": (
+        c_int, [c_void_p, c_int64, c_int64, c_int64, c_int64, POINTER(c_int32), c_void_p]
+    ),
     "jfb_wavenumber_solve": (
         c_int,
         [c_void_p, POINTER(c_int64), c_int64, c_void_p, POINTER(c_int64), c_int64,

@@ -5,6 +5,7 @@
 //   DiaMatrix storage / matvec / rmatvec   src/jaxfun/la/diamatrix.py:100-348
 //   no-pivot banded LU kernel              src/jaxfun/la/diamatrix.py:1936-1973
 //   batched wavenumber solve               src/jaxfun/la/tpmatrix.py:686-799
+#include <climits>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -295,5 +296,125 @@ extern "C" int jfb_wavenumber_solve(const double* L, const int64_t* L_offsets, i
         L, lt, U, ut, main_idx, (int)n_P, outer, inner, n_rhs, out, out);
   }
   JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+// ===========================================================================
+// Allocation-free variant of the batched banded LU.
+//
+// Some callers cannot call cudaMalloc at all: code that runs while a stream
+// is being captured into a CUDA graph, kernels launched from a host callback,
+// or hosts whose device memory is fully owned by another framework's pool
+// (an XLA custom call, for example).  jfb_banded_lu_factor above allocates its
+// pivot-status word with cudaMallocAsync; this entry point keeps the pivot
+// status of every matrix in a fixed file-scope device array instead, so it
+// allocates nothing.  The array holds JFB_NOALLOC_LU_MAX_BATCH per-matrix
+// flags plus one slot for the index of the first singular matrix; every GPU
+// that loads the library holds it (256 KiB) until the process exits.
+// ===========================================================================
+
+static __device__ __align__(256) int g_noalloc_lu_status[JFB_NOALLOC_LU_MAX_BATCH + 1];
+
+namespace jfb {
+
+// Zero the per-matrix flags of this call and reset the first-singular slot.
+__global__ void noalloc_lu_clear_kernel(int* status, int64_t n_batch) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_batch;
+       i += (int64_t)gridDim.x * blockDim.x)
+    status[i] = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) status[JFB_NOALLOC_LU_MAX_BATCH] = INT_MAX;
+}
+
+// Same elimination as banded_lu_kernel (one warp per matrix, identical
+// operation order); a zero or non-finite pivot sets status[b].
+__global__ void noalloc_lu_kernel(double* __restrict__ band, int64_t n_batch, int p, int q,
+                                  int n, int* __restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  const int64_t b = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (b >= n_batch) return;
+  double* A = band + b * (int64_t)(p + q + 1) * n;
+  auto at = [&](int row, int col) -> double& { return A[(int64_t)row * n + col]; };
+  const int c = p;
+  for (int k = 0; k < n; ++k) {
+    const double pivot = at(c, k);
+    if (lane == 0 && (!(fabs(pivot) > 0.0) || !isfinite(pivot))) status[b] = 1;
+    for (int s = 1; s <= p; ++s) {
+      if (k + s >= n) break;
+      const double f = at(c - s, k) / pivot;
+      __syncwarp();
+      if (lane == 0) at(c - s, k) = f;
+      for (int u = 1 + lane; u <= q; u += 32) {
+        const int j = k + u;
+        if (j < n) at(c + u - s, j) -= f * at(c + u, j);
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Lowest index of a singular matrix into the last slot.
+__global__ void noalloc_lu_first_kernel(int* status, int64_t n_batch) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_batch;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (status[i]) atomicMin(&status[JFB_NOALLOC_LU_MAX_BATCH], (int)i);
+}
+
+// Device address of the status array, looked up once per device with that
+// device current (the host-side symbol is only a stand-in, not a device
+// address, so it must never be passed to a kernel).
+static int noalloc_status_address(int** out) {
+  static std::mutex mu;
+  static int* addr[128] = {nullptr};
+  int dev = 0;
+  JFB_CHECK_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) {
+    set_error("device ordinal out of range");
+    return JFB_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    int* p = nullptr;
+    JFB_CHECK_CUDA(cudaGetSymbolAddress((void**)&p, g_noalloc_lu_status));
+    addr[dev] = p;
+  }
+  *out = addr[dev];
+  return JFB_OK;
+}
+
+}  // namespace jfb
+
+extern "C" int jfb_banded_lu_factor_noalloc(double* band, int64_t n_batch, int64_t p,
+                                            int64_t q, int64_t n, int32_t* first_singular,
+                                            void* stream) {
+  JFB_REQUIRE(band, "null pointer");
+  JFB_REQUIRE(n_batch > 0 && p >= 0 && q >= 0 && n > 0, "bad shape");
+  if (n_batch > JFB_NOALLOC_LU_MAX_BATCH) {
+    set_error("n_batch exceeds JFB_NOALLOC_LU_MAX_BATCH (65536) of the allocation-free LU");
+    return JFB_ERR_ARG;
+  }
+  int* status = nullptr;
+  int st = noalloc_status_address(&status);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int cblocks = (int)std::min<int64_t>((n_batch + 255) / 256, 1024);
+  noalloc_lu_clear_kernel<<<cblocks, 256, 0, s>>>(status, n_batch);
+  JFB_CHECK_LAUNCH();
+  const int threads = 128;
+  const int blocks = (int)((n_batch * 32 + threads - 1) / threads);
+  noalloc_lu_kernel<<<blocks, threads, 0, s>>>(band, n_batch, (int)p, (int)q, (int)n, status);
+  JFB_CHECK_LAUNCH();
+  noalloc_lu_first_kernel<<<cblocks, 256, 0, s>>>(status, n_batch);
+  JFB_CHECK_LAUNCH();
+  int first = INT_MAX;
+  JFB_CHECK_CUDA(cudaMemcpyAsync(&first, status + JFB_NOALLOC_LU_MAX_BATCH, sizeof(int),
+                                 cudaMemcpyDeviceToHost, s));
+  JFB_CHECK_CUDA(cudaStreamSynchronize(s));
+  if (first_singular) *first_singular = (first == INT_MAX) ? -1 : first;
+  if (first != INT_MAX) {
+    set_error("Matrix " + std::to_string(first) +
+              " of the batch is singular or has a zero/non-finite pivot in LU "
+              "factorisation without pivoting");
+    return JFB_ERR_SINGULAR;
+  }
   return JFB_OK;
 }
