@@ -454,6 +454,109 @@ __device__ __forceinline__ void cta_forward_parity(const double* __restrict__ QE
   }
 }
 
+// FP64 tensor-core product D = A B + C for one 8x8x4 tile (mma.sync m8n8k4
+// f64).  Fragments: a = A[lane / 4][lane % 4], b = B[lane % 4][lane / 4],
+// c/d = C[lane / 4][2 (lane % 4) + {0, 1}].
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+// Parity-split x-backward on the FP64 tensor cores.  Columns of the product
+// are (pencil w, field f, re/im) with re/im the lowest bit, so each lane's
+// accumulator pair is one complex output value.  E (even coefficients) and O
+// (odd) tiles share an output tile; u(x_j) = E + O, u(x_{N-1-j}) = E - O.
+// coef(w, f, n) returns the orthogonal coefficient n of field f of pencil w.
+template <typename CoefFn>
+__device__ __forceinline__ void cta_backward_dmma(const double* __restrict__ VE,
+                                                  const double* __restrict__ VO, int N,
+                                                  int NF, CoefFn coef, c64* out) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int Jh = (N + 1) / 2, Ne = (N + 1) / 2, No = N / 2;
+  const int mt = (Jh + 7) / 8, nt = (NF * kNW * 2) / 8;
+  const int g = lane >> 2, t4 = lane & 3;
+  for (int tile = warp; tile < mt * nt; tile += nwarps) {
+    const int m0 = (tile / nt) * 8, n0 = (tile % nt) * 8;
+    // B column owned by this lane for the b fragment: n0 + g
+    const int colb = n0 + g;
+    const int wb = colb / (2 * NF), fb = (colb / 2) % NF, rib = colb & 1;
+    const int ja = m0 + g;  // A row of the a fragment
+    double e0 = 0.0, e1 = 0.0, o0 = 0.0, o1 = 0.0;
+    for (int k0 = 0; k0 < Ne; k0 += 4) {
+      const int k = k0 + t4;
+      const double a = (ja < Jh && k < Ne) ? __ldg(VE + (size_t)ja * Ne + k) : 0.0;
+      double b = 0.0;
+      if (k < Ne) {
+        const c64 v = coef(wb, fb, 2 * k);
+        b = rib ? v.im : v.re;
+      }
+      dmma_8x8x4(e0, e1, a, b);
+    }
+    for (int k0 = 0; k0 < No; k0 += 4) {
+      const int k = k0 + t4;
+      const double a = (ja < Jh && k < No) ? __ldg(VO + (size_t)ja * No + k) : 0.0;
+      double b = 0.0;
+      if (k < No) {
+        const c64 v = coef(wb, fb, 2 * k + 1);
+        b = rib ? v.im : v.re;
+      }
+      dmma_8x8x4(o0, o1, a, b);
+    }
+    const int j = m0 + g;
+    const int colc = n0 + 2 * t4;  // even column: re, next: im
+    const int wc = colc / (2 * NF), fc = (colc / 2) % NF;
+    if (j < Jh) {
+      out[(fc * N + j) * kLDW + wc] = cmk(e0 + o0, e1 + o1);
+      if (N - 1 - j != j) out[(fc * N + N - 1 - j) * kLDW + wc] = cmk(e0 - o0, e1 - o1);
+    }
+  }
+}
+
+// Parity-split x-forward scalar products on the FP64 tensor cores:
+// sp[2m] = sum_j QE[m][j] (u_j + u_{N-1-j}), sp[2m+1] = sum_j QO[m][j] (u_j -
+// u_{N-1-j}); phys(f, j, w) returns the sample of field f of pencil w at x_j.
+template <typename PhysFn>
+__device__ __forceinline__ void cta_forward_dmma(const double* __restrict__ QE,
+                                                 const double* __restrict__ QO, int N, int NF,
+                                                 PhysFn phys, c64* out) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int Jh = (N + 1) / 2, Jl = N / 2, Ne = (N + 1) / 2, No = N / 2;
+  const int mte = (Ne + 7) / 8, mto = (No + 7) / 8, nt = (NF * kNW * 2) / 8;
+  const int g = lane >> 2, t4 = lane & 3;
+  for (int tile = warp; tile < (mte + mto) * nt; tile += nwarps) {
+    const int mi = tile / nt;
+    const bool odd = mi >= mte;
+    const int m0 = (odd ? mi - mte : mi) * 8, n0 = (tile % nt) * 8;
+    const int M = odd ? No : Ne, K = odd ? Jl : Jh;
+    const double* A = odd ? QO : QE;
+    const int colb = n0 + g;
+    const int wb = colb / (2 * NF), fb = (colb / 2) % NF, rib = colb & 1;
+    const int ma = m0 + g;
+    double d0 = 0.0, d1 = 0.0;
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      const int k = k0 + t4;
+      const double a = (ma < M && k < K) ? __ldg(A + (size_t)ma * K + k) : 0.0;
+      double b = 0.0;
+      if (k < K) {
+        const c64 u = phys(fb, k, wb);
+        const c64 v = (N - 1 - k != k) ? phys(fb, N - 1 - k, wb) : cmk(0.0, 0.0);
+        const c64 c = odd ? u - v : u + v;
+        b = rib ? c.im : c.re;
+      }
+      dmma_8x8x4(d0, d1, a, b);
+    }
+    const int m = m0 + g;
+    const int colc = n0 + 2 * t4;
+    const int wc = colc / (2 * NF), fc = (colc / 2) % NF;
+    if (m < M) {
+      const int n = odd ? 2 * m + 1 : 2 * m;
+      out[(fc * N + n) * kLDW + wc] = cmk(d0, d1);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // pencil_stage: see file header.  Block = kNW warps, one pencil per warp.
 // ---------------------------------------------------------------------------
@@ -521,8 +624,8 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
     __syncthreads();
     // scalar products (T_n, H_f)_w for the 3 fields -> R1[3..5]
     c64* sT = R1 + 3 * d.Nx * kLDW;
-    cta_forward_parity(o.QE, o.QO, d.Nx, 3,
-                       [&](int f, int j, int w) { return R1[(f * d.Nx + j) * kLDW + w]; }, sT);
+    cta_forward_dmma(o.QE, o.QO, d.Nx, 3,
+                     [&](int f, int j, int w) { return R1[(f * d.Nx + j) * kLDW + w]; }, sT);
     __syncthreads();
     if (a.mode == kFromPhys) {
       // TB.forward(u0), TD.forward(u1), TD.forward(u2), mask, g = i ky u2 - i kz u1
@@ -772,13 +875,13 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
   __syncthreads();
   // x-backward of the six fields: field order (u0, u1, u2, w0, w1, w2)
   // lives in arrays (A5, A2, A3, A1, A4, A0).
-  cta_backward_parity(o.VE, o.VO, d.Nx, 6,
-                      [&](int f, int k, int w) {
-                        const int arr = (f == 0) ? 5 : (f == 1) ? 2 : (f == 2) ? 3
-                                        : (f == 3) ? 1 : (f == 4) ? 4 : 0;
-                        return ARR[(w * 6 + arr) * d.Nx + k];
-                      },
-                      R1);
+  cta_backward_dmma(o.VE, o.VO, d.Nx, 6,
+                    [&](int w, int f, int n) {
+                      const int arr = (f == 0) ? 5 : (f == 1) ? 2 : (f == 2) ? 3
+                                      : (f == 3) ? 1 : (f == 4) ? 4 : 0;
+                      return ARR[(w * 6 + arr) * d.Nx + n];
+                    },
+                    R1);
   __syncthreads();
   for (int idx = threadIdx.x; idx < 6 * d.Nx * kNW; idx += blockDim.x) {
     const int w = idx % kNW, fi = idx / kNW;
