@@ -5,6 +5,7 @@
 // Reference: examples/channelflow_kmm.py (KMM), examples/pcf_fluctuations_jax.py
 // (PlaneCouetteFluctuationJax), src/jaxfun/integrators/sbdf3.py, imex_rk.py.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -13,6 +14,7 @@
 #include "jfb_kmm.h"
 #include "jfb_kmm_kernels.cuh"
 #include "jfb_kmm_warpk.cuh"
+#include "jfb_kmm_gemm.cuh"
 
 namespace jfb {
 
@@ -81,6 +83,41 @@ __global__ void pack_factor_kernel(const double* __restrict__ band, int n_modes,
       double v = (off <= q) ? at(off, col) : 0.0;
       if (r == c) v = 1.0 / v;
       Up[e] = v;
+    }
+  }
+}
+
+// Factored band -> record of the tensor-core pencil stage: the L pairs as in
+// pack_factor_kernel, then per parity class the INVERSE of the upper factor,
+// packed column-major (entry (r, c), r <= c, at c (c + 1) / 2 + r).  Column c
+// is U^-1 e_c by back substitution (diamatrix.py:1936-1973 gives U).
+constexpr int kMaxHalfInv = 64;
+__global__ void pack_factor_inv_kernel(const double* __restrict__ band, int n_modes, int n,
+                                       int p, int q, double* __restrict__ out) {
+  const int mode = blockIdx.x;
+  if (mode >= n_modes) return;
+  const int bw = p + q + 1;
+  const double* B = band + (size_t)mode * bw * n;
+  double* R = out + (size_t)mode * packed_rec_size(n);
+  auto at = [&](int off, int col) { return B[(size_t)(p + off) * n + col]; };
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    R[2 * i] = (i >= 2 && p >= 2) ? at(-2, i - 2) : 0.0;
+    R[2 * i + 1] = (i >= 4 && p >= 4) ? at(-4, i - 4) : 0.0;
+  }
+  const int m0 = (n + 1) / 2, m1 = n / 2;
+  for (int par = 0; par < 2; ++par) {
+    const int mp = par ? m1 : m0;
+    double* X = R + 2 * n + (par ? m0 * (m0 + 1) / 2 : 0);
+    auto U = [&](int r, int k) { return at(2 * (k - r), 2 * k + par); };
+    for (int c = threadIdx.x; c < mp; c += blockDim.x) {
+      double x[kMaxHalfInv];
+      x[c] = 1.0 / U(c, c);
+      for (int r = c - 1; r >= 0; --r) {
+        double s = 0.0;
+        for (int k = r + 1; k <= c && 2 * (k - r) <= q; ++k) s += U(r, k) * x[k];
+        x[r] = -s / U(r, r);
+      }
+      for (int r = 0; r <= c; ++r) X[c * (c + 1) / 2 + r] = x[r];
     }
   }
 }
@@ -186,6 +223,9 @@ struct jfb_kmm_plan {
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   cudaStream_t cap = nullptr;  // private stream used only to capture the graphs
   cudaEvent_t* timing_events = nullptr;  // set by jfb_kmm_timed_steps
+  bool gemm = false;       // tensor-core pencil stage (pencil_gemm_kernel)
+  jfb::GemmOps gops;
+  size_t smem_gemm = 0;
 };
 
 namespace jfb {
@@ -282,7 +322,12 @@ static int build_factor_set(jfb_kmm_plan* pl, double gamma, FactorSet& fs) {
     double** dst = (sys == 0) ? &fs.su : (sys == 1) ? &fs.sg : &fs.s00;
     st = dalloc(pl, (void**)dst, (size_t)modes * packed_rec_size(n) * sizeof(double));
     if (st) return cleanup(), st;
-    pack_factor_kernel<<<modes, 128>>>(dband, modes, n, p, q, *dst);
+    if (pl->gemm) {
+      JFB_REQUIRE(n <= 2 * kMaxHalfInv, "system too large for the inverse-factor records");
+      pack_factor_inv_kernel<<<modes, 64>>>(dband, modes, n, p, q, *dst);
+    } else {
+      pack_factor_kernel<<<modes, 128>>>(dband, modes, n, p, q, *dst);
+    }
     JFB_CHECK_LAUNCH();
     JFB_CHECK_CUDA(cudaDeviceSynchronize());
     // the temporaries were registered as plan allocations by upload(): release them
@@ -325,6 +370,52 @@ static int launch_pencil(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s) {
     pencil_stage_kernel<1><<<blocks, kNW * 32, pl->smem_pencil, s>>>(pl->ops, pl->d, a);
   else
     pencil_stage_kernel<2><<<blocks, kNW * 32, pl->smem_pencil, s>>>(pl->ops, pl->d, a);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+// One implicit stage (mode kImplicit): the tensor-core pencil stage when the
+// plan has it, else the warp-per-pencil kernel.
+static int launch_implicit(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s) {
+  if (!pl->gemm) return launch_pencil(pl, a, s);
+  GemmStageArgs g;
+  g.HX = a.HX;
+  g.c0 = a.c0;
+  g.c1 = a.c1;
+  g.c2 = a.c2;
+  g.d0 = a.d0;
+  g.d1 = a.d1;
+  g.d2 = a.d2;
+  g.slin = a.cL * pl->d.nu;
+  g.u0a = a.u0a;
+  g.u0b = a.u0b;
+  g.u0c = a.u0c;
+  g.ga = a.ga;
+  g.gb = a.gb;
+  g.gc = a.gc;
+  g.vwa = a.vwa;
+  g.vwb = a.vwb;
+  g.vwc = a.vwc;
+  g.Nup = a.Nup;
+  g.Nuq = a.Nuq;
+  g.Ngp = a.Ngp;
+  g.Ngq = a.Ngq;
+  g.NVWp = a.NVWp;
+  g.NVWq = a.NVWq;
+  g.Nu_out = a.Nu_out;
+  g.Ng_out = a.Ng_out;
+  g.NVW_out = a.NVW_out;
+  g.su = a.fac.su;
+  g.sg = a.fac.sg;
+  g.s00 = a.fac.s00;
+  g.su_rec = a.fac.su_rec;
+  g.sg_rec = a.fac.sg_rec;
+  g.u0_out = a.u0_out;
+  g.g_out = a.g_out;
+  g.vw_out = a.vw_out;
+  g.X = a.X;
+  const int blocks = (pl->d.Ny / 2) * ceil_div(pl->d.Kz, 8);
+  pencil_gemm_kernel<<<blocks, 256, pl->smem_gemm, s>>>(pl->d, pl->ops, pl->gops, g);
   JFB_CHECK_LAUNCH();
   return JFB_OK;
 }
@@ -488,7 +579,7 @@ static int steady_step(jfb_kmm_plan* pl, int64_t m, cudaStream_t s) {
   a.g_out = pl->G[nw];
   a.vw_out = pl->VW[nw];
   a.X = pl->X;
-  int st = launch_pencil(pl, a, s);
+  int st = launch_implicit(pl, a, s);
   if (st) return st;
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[1], s));
   return launch_transforms(pl, s);
@@ -542,7 +633,7 @@ static int startup_step(jfb_kmm_plan* pl, cudaStream_t s) {
     a.g_out = pl->G[nw];
     a.vw_out = pl->VW[nw];
     a.X = pl->X;
-    int st = launch_pencil(pl, a, s);
+    int st = launch_implicit(pl, a, s);
     if (st) return st;
     st = launch_transforms(pl, s);
     if (st) return st;
@@ -713,6 +804,70 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   if (st) return fail(st);
   st = upload(pl, &pl->twnz, twiddles(d.Nz));
   if (st) return fail(st);
+
+  // tensor-core pencil stage: folded x-operators and its shared-memory plan
+  // (JFB200_PENCIL=warp selects the warp-per-pencil kernel instead)
+  {
+    const int N = d.Nx, Jh = (N + 1) / 2, Jl = N / 2;
+    const int nBe = (d.nB + 1) / 2, nBo = d.nB / 2, nDe = (d.nD + 1) / 2, nDo = d.nD / 2;
+    GemmOps& G = pl->gops;
+    std::memset(&G, 0, sizeof(G));
+    G.oHNE = 0;
+    G.oHNO = round4(N);
+    G.oHGE = G.oHNO + round4(N);
+    G.oHGO = G.oHGE + round4(Jh);
+    G.oMUE = G.oHGO + round4(Jl);
+    G.oMUO = G.oMUE + round4(3 * nBe);
+    G.oMGE = G.oMUO + round4(3 * nBo);
+    G.oMGO = G.oMGE + round4(2 * nDe);
+    G.oRU = G.oMGO + round4(2 * nDo);
+    G.oRG = G.oRU + d.nB;
+    G.rows = G.oRG + d.nD;
+    G.oUE = 0;
+    G.oUO = round4(nBe);
+    G.oGE = G.oUO + round4(nBo);
+    G.oGO = G.oGE + round4(nDe);
+    G.oMean = G.rows * kGLd;
+    const size_t smem = ((size_t)G.rows * kGLd + 2 * N + 4 * d.nD) * sizeof(double);
+    const char* env = std::getenv("JFB200_PENCIL");
+    const bool want = !(env && std::string(env) == "warp");
+    pl->gemm = want && smem <= 227 * 1024 && G.oGO + round4(nDo) <= G.oRU && d.nD <= 256 &&
+               (d.nD + 1) / 2 <= kMaxHalfInv;
+    if (pl->gemm) {
+      GemmHost gh;
+      std::string err;
+      if (!build_gemm_operators(pl->hop, gh, err)) {
+        set_error(err);
+        return fail(JFB_ERR_ARG);
+      }
+      double* fr;
+      int* kr;
+      if ((st = upload(pl, &fr, gh.frag))) return fail(st);
+      if ((st = upload(pl, &kr, gh.krange))) return fail(st);
+      G.frag = fr;
+      G.krange = kr;
+      double* r3;
+      double* x2;
+      if ((st = upload(pl, &r3, gh.R3))) return fail(st);
+      if ((st = upload(pl, &x2, gh.X2D))) return fail(st);
+      G.R3 = r3;
+      G.X2D = x2;
+      for (int k = 0; k < gNumSub; ++k) G.sub[k] = SubDesc{gh.off[k], gh.mt[k], gh.kt[k], gh.kr[k]};
+      G.Jh = gh.Jh;
+      G.Jl = gh.Jl;
+      G.nBe = gh.nBe;
+      G.nBo = gh.nBo;
+      G.nDe = gh.nDe;
+      G.nDo = gh.nDo;
+      G.kt_mu_lin[0] = ceil_div(2 * nBe, 4);
+      G.kt_mu_lin[1] = ceil_div(2 * nBo, 4);
+      G.kt_mg_lin[0] = ceil_div(nDe, 4);
+      G.kt_mg_lin[1] = ceil_div(nDo, 4);
+      pl->smem_gemm = smem;
+      JFB_CHECK_CUDA(cudaFuncSetAttribute(pencil_gemm_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+  }
 
   // factors: steady SBDF3 and the three IMEXRK3 startup stages
   pl->n_modes = (d.Ny / 2) * d.Kz;

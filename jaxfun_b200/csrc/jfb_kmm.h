@@ -1,6 +1,7 @@
 // Internal declarations of the KMM plane-Couette plan (not part of the C ABI).
 #pragma once
 
+#include <string>
 #include <vector>
 
 #include "../../include/jfb200.h"
@@ -29,7 +30,31 @@ struct HostOperators {
   std::vector<double> fejer;  // Fejer-I weights on the Gauss nodes / df
 };
 
+// Parity-split x-operators of the step in mma.sync m8n8k4 fragment order.
+// Sub-matrix ids (rows x columns in the half spaces; E/O = symmetric /
+// antisymmetric physical half, e/o = even / odd coefficient half):
+//   Nu/Ng right-hand sides   gNuE, gNuO, gNgE, gNgO   (physical -> coefficient)
+//   mass rows of Su / Sg     gMuE, gMuO, gMgE, gMgO   (coefficient -> coefficient)
+//   velocity / vorticity     gA0Ee ... gB1Oo          (coefficient -> physical)
+enum GemmSub {
+  gNuE, gNuO, gNgE, gNgO, gMuE, gMuO, gMgE, gMgO,
+  gA0Ee, gP2Ee, gP1Oe, gP1Eo, gA0Oo, gP2Oo, gB1Ee, gB2Oe, gB2Eo, gB1Oo,
+  gNumSub
+};
+
+struct GemmHost {
+  int Jh = 0, Jl = 0, nBe = 0, nBo = 0, nDe = 0, nDo = 0;
+  std::vector<double> frag;   // fragment-tiled sub-matrices
+  std::vector<int> krange;    // per sub-matrix and row tile: [first k tile, end k tile)
+  int off[gNumSub], mt[gNumSub], kt[gNumSub], kr[gNumSub];
+  std::vector<double> R3;     // S_D Q (nD x N): mean-flow nonlinear rows
+  std::vector<double> X2D;    // (T_i, phi_j'')_w of the Dirichlet basis (nD x nD)
+};
+
 Stencil make_stencil(int N, bool biharmonic);
+// Builds GemmHost from the 1-D operators; returns false (with a message) if a
+// parity property the split relies on does not hold.
+bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& err);
 void build_host_operators(const jfb_kmm_config& cfg, HostOperators& op);
 void mode_coefficients(const HostOperators& op, const jfb_kmm_config& cfg, int ky,
                        int kz, double gamma, bool biharmonic, double out[3]);

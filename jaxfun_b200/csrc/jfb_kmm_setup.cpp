@@ -14,6 +14,8 @@
 #include <cmath>
 #include <cstdint>
 #include <stdexcept>
+#include <algorithm>
+#include <string>
 
 namespace jfb {
 
@@ -238,6 +240,249 @@ void mode_coefficients(const HostOperators& op, const jfb_kmm_config& cfg, int k
     out[1] = -gamma * nu * My * Mz;
     out[2] = 0.0;
   }
+}
+
+
+// ---------------------------------------------------------------------------
+// Folded x-operators of the step (long double products, rounded once).
+//
+// Every per-pencil map of the step along x is linear with (ky, kz)-dependent
+// scalar weights, so the Shen projections, chebder recurrences and mass
+// solves fold into fixed matrices shared by all pencils:
+//   Pi = S_D^T M_D^-1 S_D Q      physical -> orthogonal coefficients of P_TD
+//   Nu = Myz [R1 (i ky H1 + i kz H2) + k^2 R0 H0],  R0 = S_B W Pi, R1 = S_B W D Pi
+//   Ng = Myz R2 (i kz H1 - i ky H2),                R2 = S_D W Pi
+//        (channelflow_kmm.py:784-829, coefficient path)
+//   u0 = A0 u0,  u1 = i (ky P1 u0 + kz B1 g) / k^2,  u2 = i (kz P1 u0 - ky B1 g) / k^2
+//   w0 = B1 g,   w1 = i kz A0 u0 - i (kz P2 u0 - ky B2 g) / k^2,
+//   w2 = i (ky P2 u0 + kz B2 g) / k^2 - i ky A0 u0      (channelflow_kmm.py:699-714, 831-870)
+// with A0 = V S_B^T, B1 = V S_D^T, B2 = V D S_D^T, F = M_D^-1 S_D W D S_B^T,
+// P1 = B1 F, P2 = B2 F, W = diag(norm^2 / df).  Gauss nodes are mirror
+// symmetric and T_n has parity n, so each matrix splits into a symmetric and
+// an antisymmetric half of half the size.
+// ---------------------------------------------------------------------------
+namespace {
+using LD = long double;
+struct LMat {
+  int r = 0, c = 0;
+  std::vector<LD> v;
+  LMat(int r_, int c_) : r(r_), c(c_), v((size_t)r_ * c_, 0.0L) {}
+  LD& operator()(int i, int j) { return v[(size_t)i * c + j]; }
+  LD operator()(int i, int j) const { return v[(size_t)i * c + j]; }
+};
+LMat mul(const LMat& A, const LMat& B) {
+  LMat C(A.r, B.c);
+  for (int i = 0; i < A.r; ++i)
+    for (int k = 0; k < A.c; ++k) {
+      const LD a = A(i, k);
+      if (a == 0.0L) continue;
+      for (int j = 0; j < B.c; ++j) C(i, j) += a * B(k, j);
+    }
+  return C;
+}
+LMat transpose(const LMat& A) {
+  LMat T(A.c, A.r);
+  for (int i = 0; i < A.r; ++i)
+    for (int j = 0; j < A.c; ++j) T(j, i) = A(i, j);
+  return T;
+}
+// Gauss-Jordan inverse with partial pivoting (small SPD mass matrix).
+LMat inverse(const LMat& A) {
+  const int n = A.r;
+  LMat M = A, I(n, n);
+  for (int i = 0; i < n; ++i) I(i, i) = 1.0L;
+  for (int k = 0; k < n; ++k) {
+    int piv = k;
+    for (int i = k + 1; i < n; ++i)
+      if (std::fabs((double)M(i, k)) > std::fabs((double)M(piv, k))) piv = i;
+    if (piv != k)
+      for (int j = 0; j < n; ++j) {
+        std::swap(M(k, j), M(piv, j));
+        std::swap(I(k, j), I(piv, j));
+      }
+    const LD inv = 1.0L / M(k, k);
+    for (int j = 0; j < n; ++j) {
+      M(k, j) *= inv;
+      I(k, j) *= inv;
+    }
+    for (int i = 0; i < n; ++i) {
+      if (i == k) continue;
+      const LD f = M(i, k);
+      if (f == 0.0L) continue;
+      for (int j = 0; j < n; ++j) {
+        M(i, j) -= f * M(k, j);
+        I(i, j) -= f * I(k, j);
+      }
+    }
+  }
+  return I;
+}
+LMat from_dense(const std::vector<double>& a, int r, int c) {
+  LMat M(r, c);
+  for (size_t k = 0; k < a.size(); ++k) M.v[k] = a[k];
+  return M;
+}
+// max |M[i][N-1-j] - sign_i M[i][j]| relative to the largest entry of row i
+// (rows of a physical-input matrix) is tiny for every row.
+bool rows_mirror(const LMat& M, int sign_even_row) {
+  const int N = M.c;
+  for (int i = 0; i < M.r; ++i) {
+    const LD s = (i % 2 == 0) ? sign_even_row : -sign_even_row;
+    LD big = 0, bad = 0;
+    for (int j = 0; j < N; ++j) big = std::max(big, std::fabs(M(i, j)));
+    for (int j = 0; j < N; ++j) bad = std::max(bad, std::fabs(M(i, N - 1 - j) - s * M(i, j)));
+    if (bad > 1e-13L * (big + 1e-300L)) return false;
+  }
+  return true;
+}
+bool cols_mirror(const LMat& M, int sign_even_col) {
+  const int N = M.r;
+  for (int c = 0; c < M.c; ++c) {
+    const LD s = (c % 2 == 0) ? sign_even_col : -sign_even_col;
+    LD big = 0, bad = 0;
+    for (int j = 0; j < N; ++j) big = std::max(big, std::fabs(M(j, c)));
+    for (int j = 0; j < N; ++j) bad = std::max(bad, std::fabs(M(N - 1 - j, c) - s * M(j, c)));
+    if (bad > 1e-13L * (big + 1e-300L)) return false;
+  }
+  return true;
+}
+}  // namespace
+
+bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& err) {
+  const int N = op.N, nB = op.nB, nD = op.nD;
+  const LD pi = std::acos(-1.0L);
+  const LD dfx = op.dfx;
+  LMat V(N, N), Q(N, N), D(N, N), W(N, N), SB(nB, N), SD(nD, N);
+  for (int j = 0; j < N; ++j) {
+    const LD th = pi + (2.0L * j + 1.0L) * pi / (2.0L * N);
+    for (int n = 0; n < N; ++n) V(j, n) = std::cos((LD)n * th);
+  }
+  for (int n = 0; n < N; ++n)
+    for (int j = 0; j < N; ++j) Q(n, j) = V(j, n) * (pi / N) / dfx;
+  for (int i = 0; i < N; ++i)
+    for (int j = i + 1; j < N; j += 2) D(i, j) = dfx * (LD)((i == 0) ? j : 2 * j);
+  for (int n = 0; n < N; ++n) W(n, n) = ((n == 0) ? pi : pi / 2.0L) / dfx;
+  for (int i = 0; i < nB; ++i) {
+    const LD n = i;
+    SB(i, i) = 1.0L;
+    SB(i, i + 2) = 2.0L * (-n - 2.0L) / (n + 3.0L);
+    SB(i, i + 4) = (n + 1.0L) / (n + 3.0L);
+  }
+  for (int i = 0; i < nD; ++i) {
+    SD(i, i) = 1.0L;
+    SD(i, i + 2) = -1.0L;
+  }
+  const LMat SBt = transpose(SB), SDt = transpose(SD);
+  const LMat WD = mul(W, D);
+  const LMat MDi = inverse(mul(mul(SD, W), SDt));
+  const LMat Pi = mul(mul(mul(SDt, MDi), SD), Q);
+  const LMat R0 = mul(mul(SB, W), Pi);
+  const LMat R1 = mul(mul(SB, WD), Pi);
+  const LMat R2 = mul(mul(SD, W), Pi);
+  const LMat R3 = mul(SD, Q);
+  const LMat F = mul(mul(mul(MDi, SD), WD), SBt);
+  const LMat A0 = mul(V, SBt);
+  const LMat B1 = mul(V, SDt);
+  const LMat B2 = mul(mul(V, D), SDt);
+  const LMat P1 = mul(B1, F);
+  const LMat P2 = mul(B2, F);
+  const LMat K0 = from_dense(op.XB0, nB, nB), K2 = from_dense(op.XB2, nB, nB),
+             K4 = from_dense(op.XB4, nB, nB);
+  const LMat X0D = from_dense(op.XD0, nD, nD), X2D = from_dense(op.XD2, nD, nD);
+
+  if (!rows_mirror(R0, +1) || !rows_mirror(R1, -1) || !rows_mirror(R2, +1) ||
+      !cols_mirror(A0, +1) || !cols_mirror(B1, +1) || !cols_mirror(B2, -1) ||
+      !cols_mirror(P1, -1) || !cols_mirror(P2, +1)) {
+    err = "x-operators lack the mirror parity of the Gauss nodes";
+    return false;
+  }
+  for (int i = 0; i < nB; ++i)
+    for (int j = 0; j < nB; ++j)
+      if ((i - j) % 2 != 0 && (K0(i, j) != 0 || K2(i, j) != 0 || K4(i, j) != 0)) {
+        err = "biharmonic Galerkin matrices couple odd offsets";
+        return false;
+      }
+
+  const int Jh = (N + 1) / 2, Jl = N / 2;
+  const int nBe = (nB + 1) / 2, nBo = nB / 2, nDe = (nD + 1) / 2, nDo = nD / 2;
+  gh.Jh = Jh;
+  gh.Jl = Jl;
+  gh.nBe = nBe;
+  gh.nBo = nBo;
+  gh.nDe = nDe;
+  gh.nDo = nDo;
+  gh.frag.clear();
+  gh.krange.clear();
+  auto add = [&](int id, int R, int K, auto val) {
+    const int MT = (R + 7) / 8, KT = (K + 3) / 4;
+    gh.off[id] = (int)gh.frag.size();
+    gh.mt[id] = MT;
+    gh.kt[id] = KT;
+    gh.kr[id] = (int)gh.krange.size();
+    gh.frag.resize(gh.frag.size() + (size_t)MT * KT * 32, 0.0);
+    for (int mt = 0; mt < MT; ++mt) {
+      int kb = KT, ke = 0;
+      for (int kt = 0; kt < KT; ++kt)
+        for (int lane = 0; lane < 32; ++lane) {
+          const int r = mt * 8 + lane / 4, k = kt * 4 + lane % 4;
+          const double v = (r < R && k < K) ? (double)val(r, k) : 0.0;
+          gh.frag[gh.off[id] + ((size_t)mt * KT + kt) * 32 + lane] = v;
+          if (v != 0.0) {
+            kb = std::min(kb, kt);
+            ke = std::max(ke, kt + 1);
+          }
+        }
+      if (ke == 0) kb = 0;
+      gh.krange.push_back(kb);
+      gh.krange.push_back(ke);
+    }
+  };
+  // right-hand sides: B rows [d(h12); s(k2 h0)] (E) and [s(h12); d(k2 h0)] (O)
+  add(gNuE, nBe, Jl + Jh, [&](int r, int k) { return k < Jl ? R1(2 * r, k) : R0(2 * r, k - Jl); });
+  add(gNuO, nBo, Jh + Jl,
+      [&](int r, int k) { return k < Jh ? R1(2 * r + 1, k) : R0(2 * r + 1, k - Jh); });
+  add(gNgE, nDe, Jh, [&](int r, int k) { return R2(2 * r, k); });
+  add(gNgO, nDo, Jl, [&](int r, int k) { return R2(2 * r + 1, k); });
+  // mass rows: B rows [v1; v2; v3] against [X2_B | X0_B | X4_B], [w1; w2] against [X0_D | X2_D]
+  auto mu = [&](int par, int nh) {
+    return [&, par, nh](int r, int k) {
+      const int seg = k / nh, c = 2 * (k % nh) + par, i = 2 * r + par;
+      return seg == 0 ? K2(i, c) : seg == 1 ? K0(i, c) : K4(i, c);
+    };
+  };
+  add(gMuE, nBe, 3 * nBe, mu(0, nBe));
+  add(gMuO, nBo, 3 * nBo, mu(1, nBo));
+  auto mg = [&](int par, int nh) {
+    return [&, par, nh](int r, int k) {
+      const int seg = k / nh, c = 2 * (k % nh) + par, i = 2 * r + par;
+      return seg == 0 ? X0D(i, c) : X2D(i, c);
+    };
+  };
+  add(gMgE, nDe, 2 * nDe, mg(0, nDe));
+  add(gMgO, nDo, 2 * nDo, mg(1, nDo));
+  // velocity / vorticity halves: rows j < Jh (antisymmetric halves zero for j >= Jl)
+  auto ph = [&](const LMat& M, int par, bool anti) {
+    return [&, par, anti](int j, int k) -> LD {
+      if (anti && j >= Jl) return 0.0L;
+      return M(j, 2 * k + par);
+    };
+  };
+  add(gA0Ee, Jh, nBe, ph(A0, 0, false));
+  add(gP2Ee, Jh, nBe, ph(P2, 0, false));
+  add(gP1Oe, Jh, nBe, ph(P1, 0, true));
+  add(gP1Eo, Jh, nBo, ph(P1, 1, false));
+  add(gA0Oo, Jh, nBo, ph(A0, 1, true));
+  add(gP2Oo, Jh, nBo, ph(P2, 1, true));
+  add(gB1Ee, Jh, nDe, ph(B1, 0, false));
+  add(gB2Oe, Jh, nDe, ph(B2, 0, true));
+  add(gB2Eo, Jh, nDo, ph(B2, 1, false));
+  add(gB1Oo, Jh, nDo, ph(B1, 1, true));
+
+  gh.R3.assign((size_t)nD * N, 0.0);
+  for (int i = 0; i < nD; ++i)
+    for (int j = 0; j < N; ++j) gh.R3[(size_t)i * N + j] = (double)R3(i, j);
+  gh.X2D = op.XD2;
+  return true;
 }
 
 }  // namespace jfb
