@@ -7,10 +7,11 @@ DNS configuration, 65 x 64 x 64 (Chebyshev wall-normal x Fourier x Fourier,
 energy 1e-4 (jaxfun_b200.workloads).  Single-GPU problem: with --gpus N every
 rank advances its own replica (weak scaling, no collective on the data path).
 
-Default arm (--impl b200): times K steady steps through
-``jfb_kmm_timed_steps`` (CUDA events around each kernel on the launching
-stream; a 256 MiB memset between steps flushes the 126 MB L2 outside the
-timed events), reports the per-kernel roofline of the dominant kernel, the
+Default arm (--impl b200): times K steady steps, each one CUDA-graph launch
+bracketed by CUDA events on the launching stream (a 256 MiB memset before
+each step flushes the 126 MB L2 outside the events); a second, untimed pass
+through ``jfb_kmm_timed_steps`` gives per-kernel times (events around every
+launch); reports the per-kernel roofline of the dominant kernel, the
 back-to-back CUDA-graph throughput, an end-to-end figure through the public
 ``solve`` API with pinned host buffers, and the CPU oracle on the host cores.
 
@@ -303,24 +304,42 @@ def main(argv=None):
     torch.cuda.synchronize(dev)
 
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
-    kms = (ctypes.c_double * 4)()
-    sms = ctypes.c_double()
+    # timed region: K steady steps, each one CUDA-graph launch (the production
+    # path) bracketed by events; a 256 MiB memset before each step flushes the
+    # 126 MB L2 outside the events
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     sampler = ClockSampler(local)
     sampler.start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
-    _lib.call("jfb_kmm_timed_steps", solver._plan, args.steps, flush.data_ptr(), FLUSH_BYTES,
-              kms, ctypes.byref(sms), ctypes.c_void_p(stream.cuda_stream))
+    for i in range(args.steps):
+        flush.fill_(i & 0xFF)
+        starts[i].record(stream)
+        solver.advance_resident(1)
+        ends[i].record(stream)
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
     clocks = sampler.stop()
     solver._current = None
-    t_step = max_over_ranks(sms.value / max(1, args.steps), dev)  # ms per step, L2 flushed
+    step_ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends, strict=True))
+    t_step = max_over_ranks(step_ms / max(1, args.steps), dev)  # ms per step, L2 flushed
     value = world * 1000.0 / t_step
+
+    # per-kernel breakdown (diagnostic, outside the timed region): events
+    # around each kernel launch, L2 flushed before each step; every interval
+    # also holds one kernel launch latency
+    kms = (ctypes.c_double * 4)()
+    sms = ctypes.c_double()
+    kb_steps = min(args.steps, 50)
+    _lib.call("jfb_kmm_timed_steps", solver._plan, kb_steps, flush.data_ptr(), FLUSH_BYTES,
+              kms, ctypes.byref(sms), ctypes.c_void_p(stream.cuda_stream))
+    torch.cuda.synchronize(dev)
+    solver._current = None
     kernel_names = ("pencil_stage", "y_backward", "z_cross", "y_forward")
-    kernel_avg = {k: kms[i] / max(1, args.steps) for i, k in enumerate(kernel_names)}
+    kernel_avg = {k: kms[i] / kb_steps for i, k in enumerate(kernel_names)}
 
     # back-to-back graph replay (L2 stays warm between steps)
     g_steps = max(10, args.steps)

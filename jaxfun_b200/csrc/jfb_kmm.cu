@@ -4,6 +4,7 @@
 //
 // Reference: examples/channelflow_kmm.py (KMM), examples/pcf_fluctuations_jax.py
 // (PlaneCouetteFluctuationJax), src/jaxfun/integrators/sbdf3.py, imex_rk.py.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -415,7 +416,7 @@ static int launch_implicit(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s)
   g.vw_out = a.vw_out;
   g.X = a.X;
   const int blocks = (pl->d.Ny / 2) * ceil_div(pl->d.Kz, 8);
-  pencil_gemm_kernel<<<blocks, 256, pl->smem_gemm, s>>>(pl->d, pl->ops, pl->gops, g);
+  pencil_gemm_kernel<<<blocks, kGThreads, pl->smem_gemm, s>>>(pl->d, pl->ops, pl->gops, g);
   JFB_CHECK_LAUNCH();
   return JFB_OK;
 }
@@ -808,50 +809,77 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   // tensor-core pencil stage: folded x-operators and its shared-memory plan
   // (JFB200_PENCIL=warp selects the warp-per-pencil kernel instead)
   {
-    const int N = d.Nx, Jh = (N + 1) / 2, Jl = N / 2;
+    const int N = d.Nx, Jl = N / 2;
     const int nBe = (d.nB + 1) / 2, nBo = d.nB / 2, nDe = (d.nD + 1) / 2, nDo = d.nD / 2;
     GemmOps& G = pl->gops;
     std::memset(&G, 0, sizeof(G));
-    G.oHNE = 0;
-    G.oHNO = round4(N);
-    G.oHGE = G.oHNO + round4(N);
-    G.oHGO = G.oHGE + round4(Jh);
-    G.oMUE = G.oHGO + round4(Jl);
+    // operand rows: three x-sample blocks (round4(N) + 4 rows each), the
+    // mass-row inputs (three segments per parity), the right-hand sides
+    const int hb = round4(N) + 4;
+    G.oH[0] = 0;
+    G.oH[1] = hb;
+    G.oH[2] = 2 * hb;
+    G.oMUE = 3 * hb;
     G.oMUO = G.oMUE + round4(3 * nBe);
     G.oMGE = G.oMUO + round4(3 * nBo);
-    G.oMGO = G.oMGE + round4(2 * nDe);
-    G.oRU = G.oMGO + round4(2 * nDo);
+    G.oMGO = G.oMGE + round4(3 * nDe);
+    G.oRU = G.oMGO + round4(3 * nDo);
     G.oRG = G.oRU + d.nB;
     G.rows = G.oRG + d.nD;
+    // velocity operands and the staged velocity operators reuse dead rows
     G.oUE = 0;
     G.oUO = round4(nBe);
     G.oGE = G.oUO + round4(nBo);
     G.oGO = G.oGE + round4(nDe);
+    G.oVel = G.oGO + round4(nDo);
     G.oMean = G.rows * kGLd;
-    const size_t smem = ((size_t)G.rows * kGLd + 2 * N + 4 * d.nD) * sizeof(double);
+    G.oMid = G.oMean + 2 * N + 6 * d.nD;
+    const size_t smem = ((size_t)G.oMid + 5 * 2 * kGW) * sizeof(double);
     const char* env = std::getenv("JFB200_PENCIL");
     const bool want = !(env && std::string(env) == "warp");
-    pl->gemm = want && smem <= 227 * 1024 && G.oGO + round4(nDo) <= G.oRU && d.nD <= 256 &&
-               (d.nD + 1) / 2 <= kMaxHalfInv;
+    pl->gemm = want && smem <= 227 * 1024 && (d.nD + 1) / 2 <= kMaxM && Jl <= kMaxM;
+    GemmHost gh;
     if (pl->gemm) {
-      GemmHost gh;
       std::string err;
       if (!build_gemm_operators(pl->hop, gh, err)) {
         set_error(err);
         return fail(JFB_ERR_ARG);
       }
-      double* fr;
-      int* kr;
-      if ((st = upload(pl, &fr, gh.frag))) return fail(st);
+      // unrolled k ranges and the staged velocity operators must fit
+      bool fits = (size_t)G.oVel * kGLd + (gh.frag.size() - gh.off[gA0Ee]) <=
+                  (size_t)G.oRU * kGLd;
+      for (int k = 0; k < gNumSub && fits; ++k)
+        for (int mt = 0; mt < gh.mt[k]; ++mt) {
+          const int span = gh.krange[gh.kr[k] + 2 * mt + 1] - gh.krange[gh.kr[k] + 2 * mt];
+          if ((k <= gNgO && span > kKtN) || (k >= gMuE && k <= gMgO && span > kKtM)) fits = false;
+        }
+      pl->gemm = fits;  // otherwise the warp-per-pencil kernel handles this size
+    }
+    if (pl->gemm) {
+      // kReplicas copies of the operators: CTA b reads copy b % kReplicas, so
+      // the CTAs that all read every operator line do not queue on the same
+      // L2 slices
+      constexpr int kReplicas = 16;
+      std::vector<double> rep((size_t)kReplicas * gh.frag.size());
+      for (int r = 0; r < kReplicas; ++r)
+        std::copy(gh.frag.begin(), gh.frag.end(), rep.begin() + (size_t)r * gh.frag.size());
+      double *fr, *r3, *x2, *md;
+      int *kr, *stw;
+      if ((st = upload(pl, &fr, rep))) return fail(st);
       if ((st = upload(pl, &kr, gh.krange))) return fail(st);
-      G.frag = fr;
-      G.krange = kr;
-      double* r3;
-      double* x2;
       if ((st = upload(pl, &r3, gh.R3))) return fail(st);
       if ((st = upload(pl, &x2, gh.X2D))) return fail(st);
+      if ((st = upload(pl, &md, gh.mid))) return fail(st);
+      if ((st = dalloc(pl, (void**)&stw, sizeof(int)))) return fail(st);
+      G.frag = fr;
+      G.krange = kr;
       G.R3 = r3;
       G.X2D = x2;
+      G.mid = md;
+      G.status = stw;
+      G.mid_stride = gh.mid_stride;
+      G.nfrag = (int)gh.frag.size();
+      G.nrep = kReplicas;
       for (int k = 0; k < gNumSub; ++k) G.sub[k] = SubDesc{gh.off[k], gh.mt[k], gh.kt[k], gh.kr[k]};
       G.Jh = gh.Jh;
       G.Jl = gh.Jl;

@@ -49,6 +49,10 @@ struct GemmHost {
   int off[gNumSub], mt[gNumSub], kt[gNumSub], kr[gNumSub];
   std::vector<double> R3;     // S_D Q (nD x N): mean-flow nonlinear rows
   std::vector<double> X2D;    // (T_i, phi_j'')_w of the Dirichlet basis (nD x nD)
+  // middle Gauss node of an odd N: rows of A0 (even cols), P2 (even), P1 (odd),
+  // B1 (even), B2 (odd), each padded to mid_stride
+  std::vector<double> mid;
+  int mid_stride = 0;
 };
 
 Stencil make_stencil(int N, bool biharmonic);

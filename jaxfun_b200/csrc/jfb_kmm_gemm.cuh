@@ -19,7 +19,12 @@
 // Operand layout: a sub-matrix of R x K is stored as 8x4 tiles in fragment
 // order (one double per lane, coalesced); B operands live in shared memory
 // as rows of 16 complex values (32 real columns, re/im interleaved) with a
-// 36-double stride so that fragment loads are bank-conflict free.
+// 36-double stride so that fragment loads are bank-conflict free.  Inputs are
+// staged with 16-byte cp.async copies (thousands of 128-byte bulk copies per
+// CTA proved slow: each is one copy-engine operation); the velocity operators
+// arrive in one bulk copy into rows that are dead by then.  Every CTA reads
+// all operators, so the plan keeps several copies and CTA b reads copy
+// b % nrep, spreading those L2 lines.
 #pragma once
 
 #include "jfb_kmm.h"
@@ -27,26 +32,38 @@
 
 namespace jfb {
 
-constexpr int kGW = 16;   // pencils per CTA
-constexpr int kGLd = 36;  // doubles per shared row: 2 kGW + 4
+constexpr int kGW = 16;         // pencils per CTA
+constexpr int kGLd = 36;        // doubles per shared row: 2 kGW + 4
+constexpr int kGThreads = 512;  // 16 warps
+constexpr int kGWarps = kGThreads / 32;
 
 struct SubDesc {
   int off, mt, kt, kr;
 };
 
 struct GemmOps {
-  const double* frag;
+  const double* frag;   // nrep copies of the fragment-tiled operators
   const int* krange;
-  const double* R3;   // S_D Q (nD x Nx)
-  const double* X2D;  // nD x nD
+  const double* R3;     // S_D Q (nD x Nx)
+  const double* X2D;    // nD x nD
+  const double* mid;    // middle-node rows (odd Nx), 5 x mid_stride
+  int* status;          // device status word (nonzero: a bounded wait gave up)
   SubDesc sub[gNumSub];
   int Jh, Jl, nBe, nBo, nDe, nDo;
   int kt_mu_lin[2], kt_mg_lin[2];  // k-tile limits when the stage has no linear term
-  // shared-memory row offsets
-  int oHNE, oHNO, oHGE, oHGO, oMUE, oMUO, oMGE, oMGO, oRU, oRG, oUE, oUO, oGE, oGO;
-  int rows;     // total rows of kGLd doubles
+  // shared-memory row offsets (rows of kGLd doubles)
+  int oH[3], oMUE, oMUO, oMGE, oMGO, oRU, oRG, oUE, oUO, oGE, oGO, oVel, rows;
   int oMean;    // first double of the mean-flow scratch
+  int oMid;     // first double of the middle-node scratch (5 x 2 kGW doubles)
+  int nfrag;    // doubles in one copy of frag; the velocity sub-matrices are its tail
+  int nrep;     // copies of frag (CTA b reads copy b % nrep)
+  int mid_stride;
 };
+
+// Largest k-tile ranges of the pipelined products (checked on the host).
+constexpr int kKtN = 20;   // Nu / Ng products
+constexpr int kKtM = 24;   // mass-row products
+constexpr int kMaxM = 32;  // rows per parity class of Su / Sg
 
 struct GemmStageArgs {
   const c64* HX;
@@ -62,20 +79,104 @@ struct GemmStageArgs {
 
 __host__ __device__ inline int round4(int x) { return (x + 3) & ~3; }
 
-// acc[nt] += A(sub, mt) * B(rows of Bs, columns 8 nt .. 8 nt + 7), k tiles [kb, ke)
-template <int NT>
-__device__ __forceinline__ void gemm_acc(const GemmOps& G, int id, int mt, int kb, int ke,
-                                         const double* __restrict__ Bs, int ncol0, int lane,
+// Read-only (non-coherent) load of one complex value.
+__device__ __forceinline__ c64 ldg_c(const c64* p) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  return cmk(v.x, v.y);
+}
+
+// ---------------------------------------------------------------------------
+// asynchronous copies
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+// L2 prefetch of [ptr, ptr + bytes) in whole 16-byte units.
+__device__ __forceinline__ void prefetch_l2(const void* ptr, size_t bytes) {
+  uintptr_t a = reinterpret_cast<uintptr_t>(ptr);
+  const uintptr_t lo = a & ~(uintptr_t)15, hi = (a + bytes + 15) & ~(uintptr_t)15;
+  for (uintptr_t x = lo; x < hi; x += 32768) {
+    const uint32_t n = (uint32_t)min((uintptr_t)32768, hi - x);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(x), "r"(n) : "memory");
+  }
+}
+// 16-byte asynchronous global -> shared copy (L2 only), and its completion.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// Bulk global -> shared copy (no multicast) completing on `bar`.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for phase `parity` of `bar` for at most ~2^27 cycles (tens of ms).
+// On time-out the status word gets `code`, the wait is repeated once with
+// the same limit (the copy in flight targets this CTA's shared memory), and
+// false is returned.
+__device__ __noinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* status, int code) {
+  for (int round = 0; round < 2; ++round) {
+    const long long t0 = clock64();
+    while (clock64() - t0 < (1ll << 27))
+      if (mbar_try(bar, parity)) return round == 0;
+    if (round == 0 && status) atomicExch(status, code);
+  }
+  return false;
+}
+
+// acc[nt] += A(rows of one 8-row tile) * B(Bs rows, columns 8 nt ..), k tiles
+// [kb, ke) with ke - kb <= KMAX; A fragments are loaded in chunks of 8 k tiles,
+// the next chunk in flight while the current one is multiplied.
+template <int NT, int KMAX>
+__device__ __forceinline__ void gemm_acc(const double* __restrict__ A, int kb, int ke,
+                                         const double* __restrict__ Bs, int lane,
                                          double (&acc)[NT][2]) {
-  const SubDesc s = G.sub[id];
-  const double* __restrict__ A = G.frag + s.off + (size_t)mt * s.kt * 32 + lane;
+  constexpr int CH = 8, NC = (KMAX + CH - 1) / CH;
   const int g = lane >> 2, t4 = lane & 3;
-  const double* __restrict__ b = Bs + t4 * kGLd + ncol0 + g;
-#pragma unroll 4
-  for (int kt = kb; kt < ke; ++kt) {
-    const double a = __ldg(A + kt * 32);
+  const double* __restrict__ b = Bs + t4 * kGLd + g;
+  double af[2][CH];
 #pragma unroll
-    for (int nt = 0; nt < NT; ++nt) dmma_8x8x4(acc[nt][0], acc[nt][1], a, b[kt * 4 * kGLd + nt * 8]);
+  for (int k = 0; k < CH; ++k) af[0][k] = (kb + k < ke) ? __ldg(A + (kb + k) * 32 + lane) : 0.0;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    if (c + 1 < NC) {
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        const int kk = kb + (c + 1) * CH + k;
+        af[(c + 1) & 1][k] = (kk < ke) ? __ldg(A + kk * 32 + lane) : 0.0;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < CH; ++k) {
+      const int kk = kb + c * CH + k;
+      if (kk < ke) {
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+          dmma_8x8x4(acc[nt][0], acc[nt][1], af[c & 1][k], b[kk * 4 * kGLd + nt * 8]);
+      }
+    }
   }
 }
 
@@ -84,18 +185,158 @@ __device__ __forceinline__ int2 sub_krange(const GemmOps& G, int id, int mt) {
   return make_int2(kr[0], kr[1]);
 }
 
-__global__ void __launch_bounds__(256, 1) pencil_gemm_kernel(Dims d, DevOps o, GemmOps G,
-                                                             GemmStageArgs a) {
-  extern __shared__ __align__(16) double sm[];
+// u, omega (f[0..5]) of one pencil from the symmetric or antisymmetric
+// halves of A0 u0, P1 u0, P2 u0, B1 g, B2 g; for ky = kz = 0 the g slot
+// carries the mean flow v + i w.
+__device__ __forceinline__ void velocity_fields(double ky, double kz, c64 av, c64 b1, c64 b2,
+                                                c64 c1, c64 c2, c64 (&f)[6]) {
+  const double k2 = ky * ky + kz * kz;
+  f[0] = av;
+  if (k2 == 0.0) {
+    f[1] = cmk(c1.re, 0.0);
+    f[2] = cmk(c1.im, 0.0);
+    f[3] = cmk(0.0, 0.0);
+    f[4] = cmk(-c2.im, 0.0);
+    f[5] = cmk(c2.re, 0.0);
+  } else {
+    const double inv = 1.0 / k2;
+    f[1] = mul_i((ky * inv) * b1 + (kz * inv) * c1);
+    f[2] = mul_i((kz * inv) * b1 - (ky * inv) * c1);
+    f[3] = c1;
+    f[4] = mul_i(kz * av) - mul_i((kz * inv) * b2 - (ky * inv) * c2);
+    f[5] = mul_i((ky * inv) * b2 + (kz * inv) * c2) - mul_i(ky * av);
+  }
+}
+
+// Forward elimination with the unit lower factor of one parity class, in
+// place on y[r * stride] (r < m): y_r -= L[i, i-2] y_{r-1} + L[i, i-4] y_{r-2},
+// i = 2 r + par; the multipliers (rec[2 i], rec[2 i + 1]) are loaded eight
+// rows ahead of their use.
+__device__ __forceinline__ void forward_elim(const double* __restrict__ rec, int par, int m,
+                                             c64* y, int stride) {
+  constexpr int CH = 8, NC = kMaxM / CH;
+  double l1[2][CH], l2[2][CH];
+#pragma unroll
+  for (int k = 0; k < CH; ++k) {
+    const int i = 2 * k + par;
+    l1[0][k] = (k < m) ? __ldg(rec + 2 * i) : 0.0;
+    l2[0][k] = (k < m) ? __ldg(rec + 2 * i + 1) : 0.0;
+  }
+  c64 y1 = cmk(0.0, 0.0), y2 = y1;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    if (c + 1 < NC) {
+#pragma unroll
+      for (int k = 0; k < CH; ++k) {
+        const int r = (c + 1) * CH + k, i = 2 * r + par;
+        l1[(c + 1) & 1][k] = (r < m) ? __ldg(rec + 2 * i) : 0.0;
+        l2[(c + 1) & 1][k] = (r < m) ? __ldg(rec + 2 * i + 1) : 0.0;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < CH; ++k) {
+      const int r = c * CH + k;
+      if (r < m) {
+        c64 v = y[r * stride];
+        v = v - l1[c & 1][k] * y1;
+        v = v - l2[c & 1][k] * y2;
+        y[r * stride] = v;
+        y2 = y1;
+        y1 = v;
+      }
+    }
+  }
+}
+
+// Named barrier over `count` threads.
+__device__ __forceinline__ void bar_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// Mean-flow system of the ky = kz = 0 pencil (channelflow_kmm.py mean rows)
+// on kMeanThreads threads t: N = -(S_D Q Re H1, S_D Q Re H2), rhs = M00 comb
+// + slin X2D vwa + dt (d0 N + d1 N' + d2 N''), S00 solve (forward
+// elimination, then the inverse upper factor).  Leaves (v, w) in vwx.
+constexpr int kMeanThreads = 192;
+__device__ void mean_flow(const Dims& d, const DevOps& o, const GemmOps& G,
+                          const GemmStageArgs& a, const double* hm, c64* nvw, c64* vw,
+                          c64* vwx, int t) {
+  const int N = d.Nx, nD = d.nD, Jl = N / 2;
+  for (int e = t; e < 2 * nD; e += kMeanThreads) {
+    const int i = e >> 1, f = e & 1;
+    const double* __restrict__ r3 = G.R3 + (size_t)i * N;
+    const double* h = hm + f * N;
+    const double sg = (i & 1) ? -1.0 : 1.0;  // rows of S_D Q have the parity of i
+    double a0 = 0.0, a1 = 0.0;
+#pragma unroll 8
+    for (int j = 0; j + 1 < Jl; j += 2) {
+      a0 += __ldg(r3 + j) * (h[j] + sg * h[N - 1 - j]);
+      a1 += __ldg(r3 + j + 1) * (h[j + 1] + sg * h[N - 2 - j]);
+    }
+    if (Jl & 1) a0 += __ldg(r3 + Jl - 1) * (h[Jl - 1] + sg * h[N - Jl]);
+    if ((N & 1) && !(i & 1)) a1 += __ldg(r3 + Jl) * h[Jl];
+    reinterpret_cast<double*>(nvw)[e] = -(a0 + a1);
+  }
+  bar_sync(1, kMeanThreads);
+  for (int i = t; i < nD; i += kMeanThreads) {
+    auto comb = [&](int k) {
+      c64 v = a.c0 * ldg_c(a.vwa + k);
+      if (a.c1 != 0.0) v = v + a.c1 * ldg_c(a.vwb + k);
+      if (a.c2 != 0.0) v = v + a.c2 * ldg_c(a.vwc + k);
+      return v;
+    };
+    c64 r = o.mdi[i] * comb(i);
+    if (i >= 2) r = r + o.mlo[i] * comb(i - 2);
+    if (i + 2 < nD) r = r + o.mhi[i] * comb(i + 2);
+    if (a.slin != 0.0) {
+      c64 s = cmk(0.0, 0.0);
+#pragma unroll 8
+      for (int k = 0; k < nD; ++k) s = s + __ldg(G.X2D + (size_t)i * nD + k) * ldg_c(a.vwa + k);
+      r = r + a.slin * s;
+    }
+    c64 nl = a.d0 * nvw[i];
+    if (a.d1 != 0.0) nl = nl + a.d1 * ldg_c(a.NVWp + i);
+    if (a.d2 != 0.0) nl = nl + a.d2 * ldg_c(a.NVWq + i);
+    if (a.NVW_out) a.NVW_out[i] = nvw[i];
+    vw[i] = r + d.dt * nl;
+  }
+  bar_sync(1, kMeanThreads);
+  if (t < 2) forward_elim(a.s00, t, t ? nD / 2 : (nD + 1) / 2, vw + t, 2);
+  bar_sync(1, kMeanThreads);
+  for (int i = t; i < nD; i += kMeanThreads) {
+    const int m0 = (nD + 1) / 2, par = i & 1, r = i >> 1;
+    const int m = par ? nD / 2 : m0;
+    const double* tri = a.s00 + 2 * nD + (par ? m0 * (m0 + 1) / 2 : 0);
+    double u[kMaxM];
+#pragma unroll
+    for (int c = 0; c < kMaxM; ++c) u[c] = (c >= r && c < m) ? __ldg(tri + c * (c + 1) / 2 + r) : 0.0;
+    c64 xv = cmk(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < kMaxM; ++c)
+      if (c >= r && c < m) xv = xv + u[c] * vw[2 * c + par];
+    vwx[i] = xv;
+    a.vw_out[i] = xv;
+  }
+}
+
+__global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOps o, GemmOps G,
+                                                                   GemmStageArgs a) {
+  extern __shared__ __align__(128) double sm[];
   __shared__ int s_p[kGW], s_mode[kGW];
   __shared__ double s_ky[kGW], s_kz[kGW];
+  __shared__ __align__(8) uint64_t s_bar;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t4 = lane & 3;
   const int nKc = (d.Kz + 7) / 8;
   const int kyi = blockIdx.x / nKc, kz0 = (blockIdx.x % nKc) * 8;
+  const int nkz = min(8, d.Kz - kz0);  // valid kz columns per side
   const bool mean_cta = (kyi == 0 && kz0 == 0);
   const int N = d.Nx, Jh = G.Jh, Jl = G.Jl;
   const size_t P = (size_t)d.P;
+  const double* __restrict__ frag = G.frag + (size_t)(blockIdx.x % G.nrep) * G.nfrag;
+  c64* rowc = reinterpret_cast<c64*>(sm);  // row r, pencil w: rowc[r * LC + w]
+  const int LC = kGLd / 2;
+  const double sl = a.slin;
 
   if (tid < kGW) {
     const int side = tid >> 3, kz = kz0 + (tid & 7);
@@ -112,21 +353,91 @@ __global__ void __launch_bounds__(256, 1) pencil_gemm_kernel(Dims d, DevOps o, G
     s_mode[tid] = mode;
     s_ky[tid] = kyp;
     s_kz[tid] = kzp;
+  } else if (tid == 32) {
+    mbar_init(&s_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  } else if (tid == 64) {
+    // factor records of this tile's wavenumbers (consecutive modes) into L2
+    const size_t m0 = (size_t)kyi * d.Kz + kz0;
+    prefetch_l2(a.su + m0 * a.su_rec, (size_t)nkz * a.su_rec * sizeof(double));
+    prefetch_l2(a.sg + m0 * a.sg_rec, (size_t)nkz * a.sg_rec * sizeof(double));
+  } else if (tid == 96) {
+    // this CTA's share of its operator copy
+    const int users = (gridDim.x + G.nrep - 1) / G.nrep, slot = blockIdx.x / G.nrep;
+    const int chunk = (G.nfrag + users - 1) / users;
+    const int b0 = min(G.nfrag, slot * chunk), b1 = min(G.nfrag, b0 + chunk);
+    if (b1 > b0) prefetch_l2(frag + b0, (size_t)(b1 - b0) * sizeof(double));
+  } else if (tid == 128 && mean_cta) {
+    prefetch_l2(G.R3, (size_t)d.nD * d.Nx * sizeof(double));
+    prefetch_l2(a.s00, (size_t)a.sg_rec * sizeof(double));
+    if (sl != 0.0) prefetch_l2(G.X2D, (size_t)d.nD * d.nD * sizeof(double));
   }
   __syncthreads();
 
   // ------------------------------------------------------------------ A --
-  c64* rowc = reinterpret_cast<c64*>(sm);  // row r, pencil w: rowc[r * kGLd / 2 + w]
-  const int LC = kGLd / 2;
-  for (int idx = tid; idx < Jh * kGW; idx += blockDim.x) {
-    const int j = idx / kGW, w = idx % kGW;
-    const int p = s_p[w];
-    const int jm = N - 1 - j;
+  // 16-byte asynchronous copies of this tile's values straight into the
+  // operand rows (all threads, no registers): H_f row j -> block f row j; u0
+  // levels a, b, c -> segments 0, 1, 2 of the parity half of the mass operand
+  // (row i -> i / 2), likewise g.  Column = pencil (8 +ky then 8 -ky).
+  const bool has_b = (a.c1 != 0.0), has_c = (a.c2 != 0.0);
+  const int sides = (kyi == 0) ? 1 : 2;
+  {
+    const int lv = 1 + has_b + has_c;
+    const int nrow = 3 * N + (d.nB + d.nD) * lv;
+    const int per_row = sides * nkz;
+    for (int e = tid; e < nrow * per_row; e += kGThreads) {
+      const int r = e / per_row, c = e % per_row;
+      const int side = c / nkz, kz = c % nkz;
+      const c64* src;
+      int dst_row;
+      if (r < 3 * N) {
+        const int f = r / N, j = r % N;
+        src = a.HX + ((size_t)f * N + j) * P;
+        dst_row = G.oH[f] + j;
+      } else if (r < 3 * N + d.nB * lv) {
+        const int q = r - 3 * N, lvl = q / d.nB, i = q % d.nB;
+        const int l = (lvl == 0) ? 0 : (lvl == 1 && has_b) ? 1 : 2;
+        src = ((l == 0) ? a.u0a : (l == 1) ? a.u0b : a.u0c) + (size_t)i * P;
+        const int nh = (i & 1) ? G.nBo : G.nBe;
+        dst_row = ((i & 1) ? G.oMUO : G.oMUE) + l * nh + (i >> 1);
+      } else {
+        const int q = r - 3 * N - d.nB * lv, lvl = q / d.nD, i = q % d.nD;
+        const int l = (lvl == 0) ? 0 : (lvl == 1 && has_b) ? 1 : 2;
+        src = ((l == 0) ? a.ga : (l == 1) ? a.gb : a.gc) + (size_t)i * P;
+        const int nh = (i & 1) ? G.nDo : G.nDe;
+        dst_row = ((i & 1) ? G.oMGO : G.oMGE) + l * nh + (i >> 1);
+      }
+      const int kyrow = side ? d.Ny - kyi : kyi;
+      cp_async16(rowc + (size_t)dst_row * LC + side * 8 + kz, src + (size_t)kyrow * d.Kz + kz0 + kz);
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+  }
+  __syncthreads();
+
+  // in-place transform: mirror sums / differences, (i ky, i kz, k^2) weights
+  double* mean = sm + G.oMean;  // mean-flow scratch
+  // [0, 2N): Re H1, Re H2 of the mean pencil; [2N, 2N + 2 nD): N (v, w);
+  // [2N + 2nD, 2N + 4nD): rhs / forward-eliminated rhs; [2N + 4nD, 2N + 6nD): solution
+  c64* m_nvw = reinterpret_cast<c64*>(mean + 2 * N);
+  c64* m_vw = reinterpret_cast<c64*>(mean + 2 * N + 2 * d.nD);
+  c64* m_x = reinterpret_cast<c64*>(mean + 2 * N + 4 * d.nD);
+  for (int idx = tid; idx < Jh * kGW; idx += kGThreads) {
+    const int j = idx / kGW, w = idx % kGW, jm = N - 1 - j;
+    const bool ok = s_p[w] >= 0;
     c64 h[2][3];
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
-      h[0][f] = (p >= 0) ? a.HX[((size_t)f * N + j) * P + p] : cmk(0.0, 0.0);
-      h[1][f] = (p >= 0 && jm != j) ? a.HX[((size_t)f * N + jm) * P + p] : cmk(0.0, 0.0);
+      h[0][f] = ok ? rowc[(G.oH[f] + j) * LC + w] : cmk(0.0, 0.0);
+      h[1][f] = (ok && jm != j) ? rowc[(G.oH[f] + jm) * LC + w] : cmk(0.0, 0.0);
+    }
+    if (mean_cta && w == 0) {
+      mean[j] = h[0][1].re;
+      mean[N + j] = h[0][2].re;
+      if (jm != j) {
+        mean[jm] = h[1][1].re;
+        mean[N + jm] = h[1][2].re;
+      }
     }
     const double ky = s_ky[w], kz = s_kz[w], k2 = ky * ky + kz * kz;
     c64 h12[2], k2h0[2], hg[2];
@@ -136,73 +447,64 @@ __global__ void __launch_bounds__(256, 1) pencil_gemm_kernel(Dims d, DevOps o, G
       k2h0[s] = k2 * h[s][0];
       hg[s] = mul_i(kz * h[s][1] - ky * h[s][2]);
     }
-    if (j < Jl) {
-      rowc[(G.oHNE + j) * LC + w] = h12[0] - h12[1];
-      rowc[(G.oHNE + Jl + j) * LC + w] = k2h0[0] + k2h0[1];
-      rowc[(G.oHNO + j) * LC + w] = h12[0] + h12[1];
-      rowc[(G.oHNO + Jh + j) * LC + w] = k2h0[0] - k2h0[1];
-      rowc[(G.oHGE + j) * LC + w] = hg[0] + hg[1];
-      rowc[(G.oHGO + j) * LC + w] = hg[0] - hg[1];
+    if (jm != j) {
+      rowc[(G.oH[0] + j) * LC + w] = h12[0] - h12[1];
+      rowc[(G.oH[0] + jm) * LC + w] = k2h0[0] + k2h0[1];
+      rowc[(G.oH[1] + j) * LC + w] = h12[0] + h12[1];
+      rowc[(G.oH[1] + jm) * LC + w] = k2h0[0] - k2h0[1];
+      rowc[(G.oH[2] + j) * LC + w] = hg[0] + hg[1];
+      rowc[(G.oH[2] + jm) * LC + w] = hg[0] - hg[1];
     } else {  // middle node (odd N): sums only
-      rowc[(G.oHNE + Jl + j) * LC + w] = k2h0[0];
-      rowc[(G.oHNO + j) * LC + w] = h12[0];
-      rowc[(G.oHGE + j) * LC + w] = hg[0];
+      rowc[(G.oH[0] + j) * LC + w] = k2h0[0];
+      rowc[(G.oH[1] + j) * LC + w] = h12[0];
+      rowc[(G.oH[2] + j) * LC + w] = hg[0];
     }
   }
-  // mass-row inputs by parity: [v1; v2; v3] (u) and [w1; w2] (g)
-  const double sl = a.slin;
-  for (int idx = tid; idx < d.nD * kGW; idx += blockDim.x) {
+  // mass-row inputs: u levels (a, b, c) -> (v1, v2, v3), g levels -> (w1, w2)
+  for (int idx = tid; idx < d.nD * kGW; idx += kGThreads) {
     const int i = idx / kGW, w = idx % kGW;
-    const int p = s_p[w];
+    const bool ok = s_p[w] >= 0;
     const double ky = s_ky[w], kz = s_kz[w], k2 = ky * ky + kz * kz;
     const int par = i & 1, m = i >> 1;
     if (i < d.nB) {
-      c64 ua = cmk(0.0, 0.0), comb = ua;
-      if (p >= 0) {
-        const size_t gi = (size_t)i * P + p;
-        ua = a.u0a[gi];
-        comb = a.c0 * ua;
-        if (a.c1 != 0.0) comb = comb + a.c1 * a.u0b[gi];
-        if (a.c2 != 0.0) comb = comb + a.c2 * a.u0c[gi];
-      }
       const int nh = par ? G.nBo : G.nBe;
-      const int base = par ? G.oMUO : G.oMUE;
-      rowc[(base + m) * LC + w] = comb - (2.0 * sl * k2) * ua;
-      rowc[(base + nh + m) * LC + w] = (sl * k2 * k2) * ua - k2 * comb;
-      rowc[(base + 2 * nh + m) * LC + w] = sl * ua;
-    }
-    c64 ga = cmk(0.0, 0.0), comb = ga;
-    if (p >= 0) {
-      const size_t gi = (size_t)i * P + p;
-      ga = a.ga[gi];
-      comb = a.c0 * ga;
-      if (a.c1 != 0.0) comb = comb + a.c1 * a.gb[gi];
-      if (a.c2 != 0.0) comb = comb + a.c2 * a.gc[gi];
+      c64* x = rowc + (size_t)((par ? G.oMUO : G.oMUE) + m) * LC + w;
+      c64 ua = cmk(0.0, 0.0), cu = ua;
+      if (ok) {
+        ua = x[0];
+        cu = a.c0 * ua;
+        if (has_b) cu = cu + a.c1 * x[nh * LC];
+        if (has_c) cu = cu + a.c2 * x[2 * nh * LC];
+      }
+      x[0] = cu - (2.0 * sl * k2) * ua;
+      x[nh * LC] = (sl * k2 * k2) * ua - k2 * cu;
+      x[2 * nh * LC] = sl * ua;
     }
     const int nh = par ? G.nDo : G.nDe;
-    const int base = par ? G.oMGO : G.oMGE;
-    rowc[(base + m) * LC + w] = comb - (sl * k2) * ga;
-    rowc[(base + nh + m) * LC + w] = sl * ga;
+    c64* x = rowc + (size_t)((par ? G.oMGO : G.oMGE) + m) * LC + w;
+    c64 ga = cmk(0.0, 0.0), cg = ga;
+    if (ok) {
+      ga = x[0];
+      cg = a.c0 * ga;
+      if (has_b) cg = cg + a.c1 * x[nh * LC];
+      if (has_c) cg = cg + a.c2 * x[2 * nh * LC];
+    }
+    x[0] = cg - (sl * k2) * ga;
+    x[nh * LC] = sl * ga;
   }
-  // zero the k padding of the B operands
+  // zero the k padding of the operands (rows past the data of each product)
   {
-    const int pads[8][2] = {{G.oHNE + N, round4(N) - N},         {G.oHNO + N, round4(N) - N},
-                            {G.oHGE + Jh, round4(Jh) - Jh},      {G.oHGO + Jl, round4(Jl) - Jl},
+    const int hb = round4(N) + 4;
+    const int pads[7][2] = {{G.oH[0] + N, hb - N},
+                            {G.oH[1] + N, hb - N},
+                            {G.oH[2] + N, hb - N},
                             {G.oMUE + 3 * G.nBe, round4(3 * G.nBe) - 3 * G.nBe},
                             {G.oMUO + 3 * G.nBo, round4(3 * G.nBo) - 3 * G.nBo},
-                            {G.oMGE + 2 * G.nDe, round4(2 * G.nDe) - 2 * G.nDe},
-                            {G.oMGO + 2 * G.nDo, round4(2 * G.nDo) - 2 * G.nDo}};
-    for (int q = 0; q < 8; ++q)
-      for (int e = tid; e < pads[q][1] * kGLd; e += blockDim.x) sm[pads[q][0] * kGLd + e] = 0.0;
-  }
-  double* mean = sm + G.oMean;  // mean-flow scratch
-  // [0, 2N): Re H1, Re H2 of the mean pencil; [2N, 2N + 2 nD): NVW (v, w);
-  // [2N + 2nD, 2N + 4nD): rhs / solution (v, w)
-  if (mean_cta) {
-    for (int j = tid; j < N; j += blockDim.x) {
-      mean[j] = a.HX[((size_t)1 * N + j) * P].re;
-      mean[N + j] = a.HX[((size_t)2 * N + j) * P].re;
-    }
+                            {G.oMGE + 2 * G.nDe, round4(3 * G.nDe) - 2 * G.nDe},
+                            {G.oMGO + 2 * G.nDo, round4(3 * G.nDo) - 2 * G.nDo}};
+    __syncthreads();  // the g transform above reads segment 2 before it is cleared
+    for (int q = 0; q < 7; ++q)
+      for (int e = tid; e < pads[q][1] * kGLd; e += kGThreads) sm[pads[q][0] * kGLd + e] = 0.0;
   }
   __syncthreads();
 
@@ -212,7 +514,7 @@ __global__ void __launch_bounds__(256, 1) pencil_gemm_kernel(Dims d, DevOps o, G
     const int nTask = nNu + G.sub[gNgE].mt + G.sub[gNgO].mt;
     const bool lin = (sl != 0.0);
     const double Myz = d.Myz, dt = d.dt;
-    for (int task = warp; task < nTask; task += 8) {
+    for (int task = warp; task < nTask; task += kGWarps) {
       const bool isNu = task < nNu;
       int mt = isNu ? task : task - nNu;
       int half = 0;
@@ -223,38 +525,46 @@ __global__ void __launch_bounds__(256, 1) pencil_gemm_kernel(Dims d, DevOps o, G
       }
       const int idN = isNu ? (half ? gNuO : gNuE) : (half ? gNgO : gNgE);
       const int idM = isNu ? (half ? gMuO : gMuE) : (half ? gMgO : gMgE);
-      const int oBN = isNu ? (half ? G.oHNO : G.oHNE) : (half ? G.oHGO : G.oHGE);
+      const int oBN = isNu ? G.oH[half] : G.oH[2] + (half ? Jh : 0);
       const int oBM = isNu ? (half ? G.oMUO : G.oMUE) : (half ? G.oMGO : G.oMGE);
+      const int nh = isNu ? (half ? G.nBo : G.nBe) : (half ? G.nDo : G.nDe);
+      const int r = mt * 8 + g;
+      const int i = 2 * r + half;
+      // history terms of the epilogue, loaded ahead of the products
+      const c64* Np = isNu ? a.Nup : a.Ngp;
+      const c64* Nq = isNu ? a.Nuq : a.Ngq;
+      c64 hp[4], hq[4];
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int p = s_p[nt * 4 + t4];
+        const bool ok = p >= 0 && r < nh;
+        const size_t gi = (size_t)i * P + (ok ? p : 0);
+        hp[nt] = (ok && a.d1 != 0.0) ? ldg_c(Np + gi) : cmk(0.0, 0.0);
+        hq[nt] = (ok && a.d2 != 0.0) ? ldg_c(Nq + gi) : cmk(0.0, 0.0);
+      }
       double accN[4][2], accM[4][2];
 #pragma unroll
       for (int nt = 0; nt < 4; ++nt) accN[nt][0] = accN[nt][1] = accM[nt][0] = accM[nt][1] = 0.0;
-      int2 kr = sub_krange(G, idN, mt);
-      gemm_acc<4>(G, idN, mt, kr.x, kr.y, sm + (size_t)oBN * kGLd, 0, lane, accN);
-      kr = sub_krange(G, idM, mt);
-      int ke = kr.y;
-      if (!lin) ke = min(ke, isNu ? G.kt_mu_lin[half] : G.kt_mg_lin[half]);
-      gemm_acc<4>(G, idM, mt, kr.x, ke, sm + (size_t)oBM * kGLd, 0, lane, accM);
-      // epilogue: row r of this half, pencils 4 nt + t4
-      const int nh = isNu ? (half ? G.nBo : G.nBe) : (half ? G.nDo : G.nDe);
-      const int r = mt * 8 + g;
+      const SubDesc sN = G.sub[idN], sM = G.sub[idM];
+      const int2 krN = sub_krange(G, idN, mt);
+      int2 krM = sub_krange(G, idM, mt);
+      if (!lin) krM.y = min(krM.y, isNu ? G.kt_mu_lin[half] : G.kt_mg_lin[half]);
+      gemm_acc<4, kKtN>(frag + sN.off + (size_t)mt * sN.kt * 32, krN.x, krN.y,
+                        sm + (size_t)oBN * kGLd, lane, accN);
+      gemm_acc<4, kKtM>(frag + sM.off + (size_t)mt * sM.kt * 32, krM.x, max(krM.x, krM.y),
+                        sm + (size_t)oBM * kGLd, lane, accM);
       if (r < nh) {
-        const int i = 2 * r + half;
         const int oR = isNu ? G.oRU + half * G.nBe : G.oRG + half * G.nDe;
         c64* Nout = isNu ? a.Nu_out : a.Ng_out;
-        const c64* Np = isNu ? a.Nup : a.Ngp;
-        const c64* Nq = isNu ? a.Nuq : a.Ngq;
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
           const int w = nt * 4 + t4;
           const int p = s_p[w];
           c64 rhs = cmk(0.0, 0.0);
           if (p >= 0) {
-            const size_t gi = (size_t)i * P + p;
             const c64 nl0 = cmk(Myz * accN[nt][0], Myz * accN[nt][1]);
-            if (Nout) Nout[gi] = nl0;
-            c64 nl = a.d0 * nl0;
-            if (a.d1 != 0.0) nl = nl + a.d1 * Np[gi];
-            if (a.d2 != 0.0) nl = nl + a.d2 * Nq[gi];
+            if (Nout) Nout[(size_t)i * P + p] = nl0;
+            const c64 nl = a.d0 * nl0 + a.d1 * hp[nt] + a.d2 * hq[nt];
             rhs = cmk(Myz * accM[nt][0], Myz * accM[nt][1]) + dt * nl;
           }
           rowc[(oR + r) * LC + w] = rhs;
@@ -265,7 +575,16 @@ __global__ void __launch_bounds__(256, 1) pencil_gemm_kernel(Dims d, DevOps o, G
   __syncthreads();
 
   // ------------------------------------------------------------------ C --
-  // C1: forward elimination, one thread per (pencil, system, parity), in place
+  // stage the velocity operators (tail of the operator copy) into dead rows
+  if (tid == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    const int voff = G.sub[gA0Ee].off;
+    const uint32_t bytes = (uint32_t)(G.nfrag - voff) * sizeof(double);
+    mbar_arrive_expect(&s_bar, bytes);
+    bulk_g2s(sm + (size_t)G.oVel * kGLd, frag + voff, bytes, &s_bar);
+  }
+  // C1: forward elimination, one thread per (pencil, system, parity), in place;
+  // warps 2..7 of the mean CTA solve the mean-flow system meanwhile
   if (tid < 4 * kGW) {
     const int w = tid & 15, sys = (tid >> 4) & 1, par = tid >> 5;
     const int p = s_p[w];
@@ -274,75 +593,55 @@ __global__ void __launch_bounds__(256, 1) pencil_gemm_kernel(Dims d, DevOps o, G
       const int m = par ? n / 2 : (n + 1) / 2;
       const double* __restrict__ rec =
           sys ? a.sg + (size_t)s_mode[w] * a.sg_rec : a.su + (size_t)s_mode[w] * a.su_rec;
-      c64* y = rowc + (size_t)(sys ? G.oRG + par * G.nDe : G.oRU + par * G.nBe) * LC + w;
-      c64 y1 = cmk(0.0, 0.0), y2 = y1;
-#pragma unroll 4
-      for (int r = 0; r < m; ++r) {
-        const int i = 2 * r + par;
-        const double l1 = __ldg(rec + 2 * i), l2 = __ldg(rec + 2 * i + 1);
-        c64 v = y[r * LC];
-        v = v - l1 * y1;
-        v = v - l2 * y2;
-        y[r * LC] = v;
-        y2 = y1;
-        y1 = v;
-      }
+      forward_elim(rec, par, m,
+                   rowc + (size_t)(sys ? G.oRG + par * G.nDe : G.oRU + par * G.nBe) * LC + w, LC);
     }
+  } else if (tid < 4 * kGW + kMeanThreads) {
+    if (mean_cta) mean_flow(d, o, G, a, mean, m_nvw, m_vw, m_x, tid - 4 * kGW);
   } else {
-    // zero the k padding of the velocity operands (they alias dead B rows)
+    const int t2 = tid - 4 * kGW - kMeanThreads, n2 = kGThreads - 4 * kGW - kMeanThreads;
+    // zero the k padding of the velocity operands (they alias dead rows)
     const int pads[4][2] = {{G.oUE + G.nBe, round4(G.nBe) - G.nBe},
                             {G.oUO + G.nBo, round4(G.nBo) - G.nBo},
                             {G.oGE + G.nDe, round4(G.nDe) - G.nDe},
                             {G.oGO + G.nDo, round4(G.nDo) - G.nDo}};
     for (int q = 0; q < 4; ++q)
-      for (int e = tid - 4 * kGW; e < pads[q][1] * kGLd; e += blockDim.x - 4 * kGW)
-        sm[pads[q][0] * kGLd + e] = 0.0;
-    if (mean_cta) {
-      // mean-flow nonlinear rows -(S_D Q Re H1), -(S_D Q Re H2)
-      for (int e = tid - 4 * kGW; e < 2 * d.nD; e += blockDim.x - 4 * kGW) {
-        const int i = e >> 1, f = e & 1;
-        const double* __restrict__ r3 = G.R3 + (size_t)i * N;
-        const double* hm = mean + f * N;
-        double s = 0.0;
-        for (int j = 0; j < N; ++j) s += __ldg(r3 + j) * hm[j];
-        mean[2 * N + 2 * i + f] = -s;
-      }
-    }
+      for (int e = t2; e < pads[q][1] * kGLd; e += n2) sm[pads[q][0] * kGLd + e] = 0.0;
   }
   __syncthreads();
-  // C2: x = U^-1 y for both pencils of a wavenumber, one warp per (pair, system, parity)
-  for (int task = warp; task < 4 * (kGW / 2); task += 8) {
+  // C2: x = U^-1 y for both pencils of a wavenumber; one warp per (pair,
+  // system, parity), lane = row
+  for (int task = warp; task < 4 * (kGW / 2); task += kGWarps) {
     const int ms = task & 7, sys = (task >> 3) & 1, par = task >> 4;
-    const int w0 = ms, w1 = ms + 8;
-    if (s_p[w0] < 0) continue;
+    if (s_p[ms] < 0) continue;
     const int n = sys ? d.nD : d.nB;
     const int m0 = (n + 1) / 2, m = par ? n / 2 : m0;
-    const double* __restrict__ tri = (sys ? a.sg + (size_t)s_mode[w0] * a.sg_rec
-                                          : a.su + (size_t)s_mode[w0] * a.su_rec) +
-                                     2 * n + (par ? m0 * (m0 + 1) / 2 : 0);
+    const double* tri =
+        (sys ? a.sg + (size_t)s_mode[ms] * a.sg_rec : a.su + (size_t)s_mode[ms] * a.su_rec) + 2 * n +
+        (par ? m0 * (m0 + 1) / 2 : 0);
+    double u[kMaxM];
+#pragma unroll
+    for (int c = 0; c < kMaxM; ++c)
+      u[c] = (c < m && lane <= c) ? __ldg(tri + c * (c + 1) / 2 + lane) : 0.0;
+    const int w0 = ms, w1 = ms + 8;
     const c64* y = rowc + (size_t)(sys ? G.oRG + par * G.nDe : G.oRU + par * G.nBe) * LC;
     c64* x = rowc + (size_t)(sys ? (par ? G.oGO : G.oGE) : (par ? G.oUO : G.oUE)) * LC;
-    for (int r0 = 0; r0 < m; r0 += 32) {
-      const int r = r0 + lane;
-      c64 s0 = cmk(0.0, 0.0), s1 = s0;
-#pragma unroll 4
-      for (int c = r0; c < m; ++c) {
-        const c64 ya = y[c * LC + w0], yb = y[c * LC + w1];
-        if (r <= c && r < m) {
-          const double u = __ldg(tri + c * (c + 1) / 2 + r);
-          s0 = s0 + u * ya;
-          s1 = s1 + u * yb;
-        }
+    c64 s0 = cmk(0.0, 0.0), s1 = s0;
+#pragma unroll
+    for (int c = 0; c < kMaxM; ++c) {
+      if (c < m) {
+        s0 = s0 + u[c] * y[c * LC + w0];
+        s1 = s1 + u[c] * y[c * LC + w1];
       }
-      if (r < m) {
-        x[r * LC + w0] = s0;
-        x[r * LC + w1] = (s_p[w1] >= 0) ? s1 : cmk(0.0, 0.0);
-      }
+    }
+    if (lane < m) {
+      x[lane * LC + w0] = s0;
+      x[lane * LC + w1] = (s_p[w1] >= 0) ? s1 : cmk(0.0, 0.0);
     }
   }
   __syncthreads();
   // C3: solved coefficients to global memory (coalesced along pencils)
-  for (int idx = tid; idx < d.nD * kGW; idx += blockDim.x) {
+  for (int idx = tid; idx < d.nD * kGW; idx += kGThreads) {
     const int i = idx / kGW, w = idx % kGW;
     const int p = s_p[w];
     if (p < 0) continue;
@@ -351,186 +650,97 @@ __global__ void __launch_bounds__(256, 1) pencil_gemm_kernel(Dims d, DevOps o, G
     a.g_out[(size_t)i * P + p] = rowc[((par ? G.oGO : G.oGE) + m) * LC + w];
   }
   if (mean_cta) {
-    // C4: mean flow: rhs = M00 comb + slin X2D vwa + dt (d0 N + d1 N' + d2 N''),
-    // then the S00 solve; (v, w) replaces g in the velocity operand of pencil 0
-    c64* vw = reinterpret_cast<c64*>(mean + 2 * N + 2 * d.nD);  // nD complex
-    const c64* nvw = reinterpret_cast<const c64*>(mean + 2 * N);
+    // the mean flow (v + i w) replaces g in the velocity operand of pencil 0
     __syncthreads();
-    for (int i = tid; i < d.nD; i += blockDim.x) {
-      auto comb = [&](int k) {
-        c64 v = a.c0 * a.vwa[k];
-        if (a.c1 != 0.0) v = v + a.c1 * a.vwb[k];
-        if (a.c2 != 0.0) v = v + a.c2 * a.vwc[k];
-        return v;
-      };
-      c64 r = o.mdi[i] * comb(i);
-      if (i >= 2) r = r + o.mlo[i] * comb(i - 2);
-      if (i + 2 < d.nD) r = r + o.mhi[i] * comb(i + 2);
-      if (sl != 0.0) {
-        c64 s = cmk(0.0, 0.0);
-        for (int k = 0; k < d.nD; ++k) s = s + __ldg(G.X2D + (size_t)i * d.nD + k) * a.vwa[k];
-        r = r + sl * s;
-      }
-      c64 nl = a.d0 * nvw[i];
-      if (a.d1 != 0.0) nl = nl + a.d1 * a.NVWp[i];
-      if (a.d2 != 0.0) nl = nl + a.d2 * a.NVWq[i];
-      if (a.NVW_out) a.NVW_out[i] = nvw[i];
-      vw[i] = r + d.dt * nl;
-    }
-    __syncthreads();
-    if (tid < 2) {
-      const int par = tid, n = d.nD, m = par ? n / 2 : (n + 1) / 2;
-      c64 y1 = cmk(0.0, 0.0), y2 = y1;
-      for (int r = 0; r < m; ++r) {
-        const int i = 2 * r + par;
-        c64 v = vw[i] - a.s00[2 * i] * y1;
-        v = v - a.s00[2 * i + 1] * y2;
-        vw[i] = v;
-        y2 = y1;
-        y1 = v;
-      }
-    }
-    __syncthreads();
-    c64 xv = cmk(0.0, 0.0);
-    const int i = tid;
-    if (i < d.nD) {
-      const int n = d.nD, m0 = (n + 1) / 2, par = i & 1, r = i >> 1;
-      const int m = par ? n / 2 : m0;
-      const double* tri = a.s00 + 2 * n + (par ? m0 * (m0 + 1) / 2 : 0);
-      for (int c = r; c < m; ++c) xv = xv + tri[c * (c + 1) / 2 + r] * vw[2 * c + par];
-    }
-    __syncthreads();
-    if (i < d.nD) {
-      a.vw_out[i] = xv;
-      const int par = i & 1, r = i >> 1;
-      rowc[((par ? G.oGO : G.oGE) + r) * LC + 0] = xv;
-    }
+    for (int i = tid; i < d.nD; i += kGThreads)
+      rowc[(((i & 1) ? G.oGO : G.oGE) + (i >> 1)) * LC + 0] = m_x[i];
   }
+  mbar_wait_bounded(&s_bar, 0, G.status, 2);
   __syncthreads();
 
   // ------------------------------------------------------------------ D --
   {
     const int MTv = G.sub[gA0Ee].mt;
-    for (int task = warp; task < 2 * MTv; task += 8) {
-      const int jt = task >> 1, ncol0 = (task & 1) * 16;
+    const double* vs = sm + (size_t)G.oVel * kGLd - G.sub[gA0Ee].off + lane;
+    for (int task = warp; task < 4 * MTv; task += kGWarps) {
+      const int jt = task >> 2, ncol0 = (task & 3) * 8;
       // accumulators: 0 aE, 1 b1E, 2 b2E, 3 c1E, 4 c2E, 5 aO, 6 b1O, 7 b2O, 8 c1O, 9 c2O
-      double acc[10][2][2];
+      double acc[10][2];
 #pragma unroll
-      for (int q = 0; q < 10; ++q)
-#pragma unroll
-        for (int nt = 0; nt < 2; ++nt) acc[q][nt][0] = acc[q][nt][1] = 0.0;
-      {
-        const double* __restrict__ Bs = sm + (size_t)G.oUE * kGLd + t4 * kGLd + ncol0 + g;
-        const double* __restrict__ A0 = G.frag + G.sub[gA0Ee].off + (size_t)jt * G.sub[gA0Ee].kt * 32 + lane;
-        const double* __restrict__ A1 = G.frag + G.sub[gP2Ee].off + (size_t)jt * G.sub[gP2Ee].kt * 32 + lane;
-        const double* __restrict__ A2 = G.frag + G.sub[gP1Oe].off + (size_t)jt * G.sub[gP1Oe].kt * 32 + lane;
-        const int KT = G.sub[gA0Ee].kt;
-#pragma unroll 2
-        for (int kt = 0; kt < KT; ++kt) {
-          const double a0 = __ldg(A0 + kt * 32), a1 = __ldg(A1 + kt * 32), a2 = __ldg(A2 + kt * 32);
-#pragma unroll
-          for (int nt = 0; nt < 2; ++nt) {
-            const double b = Bs[kt * 4 * kGLd + nt * 8];
-            dmma_8x8x4(acc[0][nt][0], acc[0][nt][1], a0, b);
-            dmma_8x8x4(acc[2][nt][0], acc[2][nt][1], a1, b);
-            dmma_8x8x4(acc[6][nt][0], acc[6][nt][1], a2, b);
-          }
+      for (int q = 0; q < 10; ++q) acc[q][0] = acc[q][1] = 0.0;
+      auto group3 = [&](int oB, int s0, int s1, int s2, int q0, int q1, int q2) {
+        const double* __restrict__ Bs = sm + (size_t)oB * kGLd + t4 * kGLd + ncol0 + g;
+        const SubDesc d0 = G.sub[s0], d1 = G.sub[s1], d2 = G.sub[s2];
+        const double* A0 = vs + d0.off + jt * d0.kt * 32;
+        const double* A1 = vs + d1.off + jt * d1.kt * 32;
+        const double* A2 = vs + d2.off + jt * d2.kt * 32;
+#pragma unroll 4
+        for (int kt = 0; kt < d0.kt; ++kt) {
+          const double b = Bs[kt * 4 * kGLd];
+          dmma_8x8x4(acc[q0][0], acc[q0][1], A0[kt * 32], b);
+          dmma_8x8x4(acc[q1][0], acc[q1][1], A1[kt * 32], b);
+          dmma_8x8x4(acc[q2][0], acc[q2][1], A2[kt * 32], b);
         }
-      }
-      {
-        const double* __restrict__ Bs = sm + (size_t)G.oUO * kGLd + t4 * kGLd + ncol0 + g;
-        const double* __restrict__ A0 = G.frag + G.sub[gP1Eo].off + (size_t)jt * G.sub[gP1Eo].kt * 32 + lane;
-        const double* __restrict__ A1 = G.frag + G.sub[gA0Oo].off + (size_t)jt * G.sub[gA0Oo].kt * 32 + lane;
-        const double* __restrict__ A2 = G.frag + G.sub[gP2Oo].off + (size_t)jt * G.sub[gP2Oo].kt * 32 + lane;
-        const int KT = G.sub[gP1Eo].kt;
-#pragma unroll 2
-        for (int kt = 0; kt < KT; ++kt) {
-          const double a0 = __ldg(A0 + kt * 32), a1 = __ldg(A1 + kt * 32), a2 = __ldg(A2 + kt * 32);
-#pragma unroll
-          for (int nt = 0; nt < 2; ++nt) {
-            const double b = Bs[kt * 4 * kGLd + nt * 8];
-            dmma_8x8x4(acc[1][nt][0], acc[1][nt][1], a0, b);
-            dmma_8x8x4(acc[5][nt][0], acc[5][nt][1], a1, b);
-            dmma_8x8x4(acc[7][nt][0], acc[7][nt][1], a2, b);
-          }
+      };
+      auto group2 = [&](int oB, int s0, int s1, int q0, int q1) {
+        const double* __restrict__ Bs = sm + (size_t)oB * kGLd + t4 * kGLd + ncol0 + g;
+        const SubDesc d0 = G.sub[s0], d1 = G.sub[s1];
+        const double* A0 = vs + d0.off + jt * d0.kt * 32;
+        const double* A1 = vs + d1.off + jt * d1.kt * 32;
+#pragma unroll 4
+        for (int kt = 0; kt < d0.kt; ++kt) {
+          const double b = Bs[kt * 4 * kGLd];
+          dmma_8x8x4(acc[q0][0], acc[q0][1], A0[kt * 32], b);
+          dmma_8x8x4(acc[q1][0], acc[q1][1], A1[kt * 32], b);
         }
-      }
-      {
-        const double* __restrict__ Bs = sm + (size_t)G.oGE * kGLd + t4 * kGLd + ncol0 + g;
-        const double* __restrict__ A0 = G.frag + G.sub[gB1Ee].off + (size_t)jt * G.sub[gB1Ee].kt * 32 + lane;
-        const double* __restrict__ A1 = G.frag + G.sub[gB2Oe].off + (size_t)jt * G.sub[gB2Oe].kt * 32 + lane;
-        const int KT = G.sub[gB1Ee].kt;
-#pragma unroll 2
-        for (int kt = 0; kt < KT; ++kt) {
-          const double a0 = __ldg(A0 + kt * 32), a1 = __ldg(A1 + kt * 32);
-#pragma unroll
-          for (int nt = 0; nt < 2; ++nt) {
-            const double b = Bs[kt * 4 * kGLd + nt * 8];
-            dmma_8x8x4(acc[3][nt][0], acc[3][nt][1], a0, b);
-            dmma_8x8x4(acc[9][nt][0], acc[9][nt][1], a1, b);
-          }
-        }
-      }
-      {
-        const double* __restrict__ Bs = sm + (size_t)G.oGO * kGLd + t4 * kGLd + ncol0 + g;
-        const double* __restrict__ A0 = G.frag + G.sub[gB2Eo].off + (size_t)jt * G.sub[gB2Eo].kt * 32 + lane;
-        const double* __restrict__ A1 = G.frag + G.sub[gB1Oo].off + (size_t)jt * G.sub[gB1Oo].kt * 32 + lane;
-        const int KT = G.sub[gB2Eo].kt;
-#pragma unroll 2
-        for (int kt = 0; kt < KT; ++kt) {
-          const double a0 = __ldg(A0 + kt * 32), a1 = __ldg(A1 + kt * 32);
-#pragma unroll
-          for (int nt = 0; nt < 2; ++nt) {
-            const double b = Bs[kt * 4 * kGLd + nt * 8];
-            dmma_8x8x4(acc[4][nt][0], acc[4][nt][1], a0, b);
-            dmma_8x8x4(acc[8][nt][0], acc[8][nt][1], a1, b);
-          }
-        }
-      }
-      // epilogue: six fields at x_j and x_{N-1-j}
+      };
+      group3(G.oUE, gA0Ee, gP2Ee, gP1Oe, 0, 2, 6);
+      group3(G.oUO, gP1Eo, gA0Oo, gP2Oo, 1, 5, 7);
+      group2(G.oGE, gB1Ee, gB2Oe, 3, 9);
+      group2(G.oGO, gB2Eo, gB1Oo, 4, 8);
+      // epilogue: six fields at x_j and x_{N-1-j}, j < Jl
       const int j = jt * 8 + g;
-      if (j < Jh) {
+      const int w = (ncol0 >> 1) + t4;
+      const int p = s_p[w];
+      if (j < Jl && p >= 0) {
         const int jm = N - 1 - j;
+        c64 fe[6], fo[6];
+        velocity_fields(s_ky[w], s_kz[w], cmk(acc[0][0], acc[0][1]), cmk(acc[1][0], acc[1][1]),
+                        cmk(acc[2][0], acc[2][1]), cmk(acc[3][0], acc[3][1]),
+                        cmk(acc[4][0], acc[4][1]), fe);
+        velocity_fields(s_ky[w], s_kz[w], cmk(acc[5][0], acc[5][1]), cmk(acc[6][0], acc[6][1]),
+                        cmk(acc[7][0], acc[7][1]), cmk(acc[8][0], acc[8][1]),
+                        cmk(acc[9][0], acc[9][1]), fo);
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-          const int w = (ncol0 >> 1) + nt * 4 + t4;
-          const int p = s_p[w];
-          if (p < 0) continue;
-          const double ky = s_ky[w], kz = s_kz[w], k2 = ky * ky + kz * kz;
-          const bool meanp = (k2 == 0.0);
-          const double inv = meanp ? 0.0 : 1.0 / k2;
-          c64 f[2][6];
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int q = 5 * h;
-            const c64 av = cmk(acc[q + 0][nt][0], acc[q + 0][nt][1]);
-            const c64 b1 = cmk(acc[q + 1][nt][0], acc[q + 1][nt][1]);
-            const c64 b2 = cmk(acc[q + 2][nt][0], acc[q + 2][nt][1]);
-            const c64 c1 = cmk(acc[q + 3][nt][0], acc[q + 3][nt][1]);
-            const c64 c2 = cmk(acc[q + 4][nt][0], acc[q + 4][nt][1]);
-            f[h][0] = av;
-            if (meanp) {  // c1, c2 hold (B1, B2) (v + i w) of the mean flow
-              f[h][1] = cmk(c1.re, 0.0);
-              f[h][2] = cmk(c1.im, 0.0);
-              f[h][3] = cmk(0.0, 0.0);
-              f[h][4] = cmk(-c2.im, 0.0);
-              f[h][5] = cmk(c2.re, 0.0);
-            } else {
-              f[h][1] = mul_i((ky * inv) * b1 + (kz * inv) * c1);
-              f[h][2] = mul_i((kz * inv) * b1 - (ky * inv) * c1);
-              f[h][3] = c1;
-              f[h][4] = mul_i(kz * av) - mul_i((kz * inv) * b2 - (ky * inv) * c2);
-              f[h][5] = mul_i((ky * inv) * b2 + (kz * inv) * c2) - mul_i(ky * av);
-            }
-          }
-#pragma unroll
-          for (int q = 0; q < 6; ++q) {
-            c64* X = a.X + (size_t)q * N * P + p;
-            X[(size_t)j * P] = f[0][q] + f[1][q];
-            if (jm != j) X[(size_t)jm * P] = f[0][q] - f[1][q];
-          }
+        for (int q = 0; q < 6; ++q) {
+          c64* X = a.X + (size_t)q * N * P + p;
+          X[(size_t)j * P] = fe[q] + fo[q];
+          X[(size_t)jm * P] = fe[q] - fo[q];
         }
       }
+    }
+  }
+  if (Jh > Jl) {
+    // middle Gauss node (odd N): symmetric halves only, one dot product per
+    // (operator, pencil, re/im) thread
+    double* md = sm + G.oMid;
+    if (tid < 5 * 2 * kGW) {
+      const int col = tid % (2 * kGW), op = tid / (2 * kGW);
+      const int oB = (op <= 1) ? G.oUE : (op == 2) ? G.oUO : (op == 3) ? G.oGE : G.oGO;
+      const int K = (op <= 1) ? G.nBe : (op == 2) ? G.nBo : (op == 3) ? G.nDe : G.nDo;
+      const double* row = G.mid + op * G.mid_stride;
+      double s = 0.0;
+      for (int k = 0; k < K; ++k) s += __ldg(row + k) * sm[(size_t)(oB + k) * kGLd + col];
+      md[tid] = s;
+    }
+    __syncthreads();
+    if (tid < kGW && s_p[tid] >= 0) {
+      const int w = tid;
+      auto val = [&](int op) { return cmk(md[op * 2 * kGW + 2 * w], md[op * 2 * kGW + 2 * w + 1]); };
+      c64 f[6];
+      velocity_fields(s_ky[w], s_kz[w], val(0), val(2), val(1), val(3), val(4), f);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) a.X[(size_t)q * N * P + (size_t)Jl * P + s_p[w]] = f[q];
     }
   }
 }

@@ -390,7 +390,7 @@ bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& er
              K4 = from_dense(op.XB4, nB, nB);
   const LMat X0D = from_dense(op.XD0, nD, nD), X2D = from_dense(op.XD2, nD, nD);
 
-  if (!rows_mirror(R0, +1) || !rows_mirror(R1, -1) || !rows_mirror(R2, +1) ||
+  if (!rows_mirror(R0, +1) || !rows_mirror(R1, -1) || !rows_mirror(R2, +1) || !rows_mirror(R3, +1) ||
       !cols_mirror(A0, +1) || !cols_mirror(B1, +1) || !cols_mirror(B2, -1) ||
       !cols_mirror(P1, -1) || !cols_mirror(P2, +1)) {
     err = "x-operators lack the mirror parity of the Gauss nodes";
@@ -437,12 +437,17 @@ bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& er
       gh.krange.push_back(ke);
     }
   };
-  // right-hand sides: B rows [d(h12); s(k2 h0)] (E) and [s(h12); d(k2 h0)] (O)
-  add(gNuE, nBe, Jl + Jh, [&](int r, int k) { return k < Jl ? R1(2 * r, k) : R0(2 * r, k - Jl); });
-  add(gNuO, nBo, Jh + Jl,
-      [&](int r, int k) { return k < Jh ? R1(2 * r + 1, k) : R0(2 * r + 1, k - Jh); });
+  // right-hand sides.  The B operands are the three x-sample blocks after an
+  // in-place mirror transform: block 0 row j < Jl holds d(h12)_j and row
+  // N-1-j holds s(k2 h0)_j; block 1 row j holds s(h12)_j, row N-1-j d(k2 h0)_j;
+  // block 2 row j holds s(hg)_j, row N-1-j d(hg)_j (j = Jl, the middle node of
+  // an odd N, holds the sums).  Columns follow that row order.
+  add(gNuE, nBe, N,
+      [&](int r, int k) { return k < Jl ? R1(2 * r, k) : R0(2 * r, N - 1 - k); });
+  add(gNuO, nBo, N,
+      [&](int r, int k) { return k < Jh ? R1(2 * r + 1, k) : R0(2 * r + 1, N - 1 - k); });
   add(gNgE, nDe, Jh, [&](int r, int k) { return R2(2 * r, k); });
-  add(gNgO, nDo, Jl, [&](int r, int k) { return R2(2 * r + 1, k); });
+  add(gNgO, nDo, Jl, [&](int r, int k) { return R2(2 * r + 1, Jl - 1 - k); });
   // mass rows: B rows [v1; v2; v3] against [X2_B | X0_B | X4_B], [w1; w2] against [X0_D | X2_D]
   auto mu = [&](int par, int nh) {
     return [&, par, nh](int r, int k) {
@@ -460,23 +465,33 @@ bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& er
   };
   add(gMgE, nDe, 2 * nDe, mg(0, nDe));
   add(gMgO, nDo, 2 * nDo, mg(1, nDo));
-  // velocity / vorticity halves: rows j < Jh (antisymmetric halves zero for j >= Jl)
-  auto ph = [&](const LMat& M, int par, bool anti) {
-    return [&, par, anti](int j, int k) -> LD {
-      if (anti && j >= Jl) return 0.0L;
-      return M(j, 2 * k + par);
-    };
+  // velocity / vorticity halves: rows j < Jl; the middle node of an odd N
+  // (symmetric half only) is kept apart in `mid`
+  auto ph = [&](const LMat& M, int par) {
+    return [&, par](int j, int k) -> LD { return M(j, 2 * k + par); };
   };
-  add(gA0Ee, Jh, nBe, ph(A0, 0, false));
-  add(gP2Ee, Jh, nBe, ph(P2, 0, false));
-  add(gP1Oe, Jh, nBe, ph(P1, 0, true));
-  add(gP1Eo, Jh, nBo, ph(P1, 1, false));
-  add(gA0Oo, Jh, nBo, ph(A0, 1, true));
-  add(gP2Oo, Jh, nBo, ph(P2, 1, true));
-  add(gB1Ee, Jh, nDe, ph(B1, 0, false));
-  add(gB2Oe, Jh, nDe, ph(B2, 0, true));
-  add(gB2Eo, Jh, nDo, ph(B2, 1, false));
-  add(gB1Oo, Jh, nDo, ph(B1, 1, true));
+  add(gA0Ee, Jl, nBe, ph(A0, 0));
+  add(gP2Ee, Jl, nBe, ph(P2, 0));
+  add(gP1Oe, Jl, nBe, ph(P1, 0));
+  add(gP1Eo, Jl, nBo, ph(P1, 1));
+  add(gA0Oo, Jl, nBo, ph(A0, 1));
+  add(gP2Oo, Jl, nBo, ph(P2, 1));
+  add(gB1Ee, Jl, nDe, ph(B1, 0));
+  add(gB2Oe, Jl, nDe, ph(B2, 0));
+  add(gB2Eo, Jl, nDo, ph(B2, 1));
+  add(gB1Oo, Jl, nDo, ph(B1, 1));
+  gh.mid_stride = std::max(std::max(nBe, nBo), std::max(nDe, nDo));
+  gh.mid.assign((size_t)5 * gh.mid_stride, 0.0);
+  if (N % 2 == 1) {
+    const int j = Jl;
+    for (int k = 0; k < nBe; ++k) {
+      gh.mid[0 * gh.mid_stride + k] = (double)A0(j, 2 * k);
+      gh.mid[1 * gh.mid_stride + k] = (double)P2(j, 2 * k);
+    }
+    for (int k = 0; k < nBo; ++k) gh.mid[2 * gh.mid_stride + k] = (double)P1(j, 2 * k + 1);
+    for (int k = 0; k < nDe; ++k) gh.mid[3 * gh.mid_stride + k] = (double)B1(j, 2 * k);
+    for (int k = 0; k < nDo; ++k) gh.mid[4 * gh.mid_stride + k] = (double)B2(j, 2 * k + 1);
+  }
 
   gh.R3.assign((size_t)nD * N, 0.0);
   for (int i = 0; i < nD; ++i)
