@@ -95,6 +95,8 @@ def stage_bytes(grid, my):
         "y_backward": (6 * Es + 6 * Em) * b,
         "z_cross": 9 * Em * b,
         "y_forward": (3 * Em + 3 * Es) * b,
+        # fused plane transforms: reads X (6 E_s), writes HX (3 E_s)
+        "plane_transforms": 9 * Es * b,
         # canonical whole-step figure (43 E_s + 18 E_m)
         "step": (43 * Es + 18 * Em) * b,
     }
@@ -338,7 +340,10 @@ def main(argv=None):
               kms, ctypes.byref(sms), ctypes.c_void_p(stream.cuda_stream))
     torch.cuda.synchronize(dev)
     solver._current = None
-    kernel_names = ("pencil_stage", "y_backward", "z_cross", "y_forward")
+    if info.launches_per_step == 2:  # pencil stage + fused plane transforms
+        kernel_names = ("pencil_stage", "plane_transforms")
+    else:
+        kernel_names = ("pencil_stage", "y_backward", "z_cross", "y_forward")
     kernel_avg = {k: kms[i] / kb_steps for i, k in enumerate(kernel_names)}
 
     # back-to-back graph replay (L2 stays warm between steps)

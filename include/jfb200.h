@@ -186,8 +186,10 @@ int jfb_kmm_diagnostics(jfb_kmm_plan* plan, double* out, void* stream);
  * jfb_kmm_advance, launched without the graph and bracketed by CUDA events
  * on `stream`.  Before each step, if flush_buf is non-NULL, flush_bytes of it
  * are overwritten (an L2 flush outside the timed events).  Returns the summed
- * device time of each of the four kernels (kernel_ms[4]: pencil stage,
- * y backward, z cross, y forward) and of the whole steps (step_ms).
+ * device time of each kernel slot (kernel_ms[4]: pencil stage, y backward,
+ * z cross, y forward; when the plan fuses the periodic-axis transforms into
+ * one launch, jfb_kmm_info.launches_per_step == 2, slot 1 holds that launch
+ * and slots 2-3 are zero) and of the whole steps (step_ms).
  * IMEXRK3 startup steps still pending are run first and not timed. */
 int jfb_kmm_timed_steps(jfb_kmm_plan* plan, int64_t steps, void* flush_buf,
                         int64_t flush_bytes, double* kernel_ms, double* step_ms,

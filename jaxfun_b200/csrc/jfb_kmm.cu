@@ -208,6 +208,8 @@ struct jfb_kmm_plan {
   jfb::c64 *U1S, *U2S;
   jfb::c64 *X, *Y, *HZ, *HX, *HD;
   jfb::c64 *twy, *twz, *twny, *twnz;
+  jfb::c32 *twy32 = nullptr, *twz32 = nullptr;  // mixed form: float twiddles
+  bool mixed = false;  // X, Y, HZ, HX of the step in complex64
   jfb::FFTPlan fny, fnz;  // unpadded y / z transforms (state_from_physical)
   int py = 0, pz = 0, pnz = 0;  // warp-FFT radix (N = 32 P), 0 = shared-memory Stockham
   int qk = 0;                   // ceil(Kz / 32)
@@ -225,11 +227,30 @@ struct jfb_kmm_plan {
   cudaStream_t cap = nullptr;  // private stream used only to capture the graphs
   cudaEvent_t* timing_events = nullptr;  // set by jfb_kmm_timed_steps
   bool gemm = false;       // tensor-core pencil stage (pencil_gemm_kernel)
+  bool plane = false;      // fused periodic-axis transforms (plane_cross_kernel)
+  size_t smem_plane = 0;
   jfb::GemmOps gops;
   size_t smem_gemm = 0;
 };
 
 namespace jfb {
+
+// Dynamic shared memory limit of a kernel: the device's opt-in maximum less
+// its static shared memory.  The
+// attribute is process-wide per kernel, so a per-plan value would let the
+// last plan built shrink the limit under an earlier plan's launches.
+static cudaError_t allow_smem(const void* fn) {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa;
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             optin - (int)fa.sharedSizeBytes);
+  return e;
+}
 
 static int dalloc(jfb_kmm_plan* pl, void** ptr, size_t bytes) {
   JFB_CHECK_CUDA(cudaMalloc(ptr, bytes));
@@ -378,7 +399,11 @@ static int launch_pencil(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s) {
 // One implicit stage (mode kImplicit): the tensor-core pencil stage when the
 // plan has it, else the warp-per-pencil kernel.
 static int launch_implicit(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s) {
-  if (!pl->gemm) return launch_pencil(pl, a, s);
+  if (!pl->gemm) {
+    StageArgs b = a;
+    b.x32 = pl->mixed ? 1 : 0;
+    return launch_pencil(pl, b, s);
+  }
   GemmStageArgs g;
   g.HX = a.HX;
   g.c0 = a.c0;
@@ -415,6 +440,7 @@ static int launch_implicit(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s)
   g.g_out = a.g_out;
   g.vw_out = a.vw_out;
   g.X = a.X;
+  g.x32 = pl->mixed ? 1 : 0;
   const int blocks = (pl->d.Ny / 2) * ceil_div(pl->d.Kz, 8);
   pencil_gemm_kernel<<<blocks, kGThreads, pl->smem_gemm, s>>>(pl->d, pl->ops, pl->gops, g);
   JFB_CHECK_LAUNCH();
@@ -427,36 +453,55 @@ static int warp_radix(int n) {
   return (p == 2 || p == 3 || p == 4 || p == 6) ? p : 0;
 }
 
-template <int P>
+// Step transform buffers and twiddles in the plan's transform precision.
+template <typename T> struct Tx;
+template <> struct Tx<double> {
+  static const c64* twy(const jfb_kmm_plan* pl) { return pl->twy; }
+  static const c64* twz(const jfb_kmm_plan* pl) { return pl->twz; }
+};
+template <> struct Tx<float> {
+  static const c32* twy(const jfb_kmm_plan* pl) { return pl->twy32; }
+  static const c32* twz(const jfb_kmm_plan* pl) { return pl->twz32; }
+};
+template <typename T> static cpx<T>* buf(void* p) { return reinterpret_cast<cpx<T>*>(p); }
+
+template <int P, typename T>
 static void launch_y_warp(jfb_kmm_plan* pl, cudaStream_t s, bool backward) {
   const Dims& d = pl->d;
+  const size_t sm = backward ? pl->smem_yw_b : pl->smem_yw_f;
+  const size_t smT = sm / sizeof(c64) * sizeof(cpx<T>);
   if (backward) {
     dim3 g(d.Nx, 6, d.Kz / pl->KCw);
-    y_backward_warp_kernel<P><<<g, 256, pl->smem_yw_b, s>>>(d, pl->KCw, pl->twy, pl->X, pl->Y);
+    y_backward_warp_kernel<P, T><<<g, 256, smT, s>>>(d, pl->KCw, Tx<T>::twy(pl), buf<T>(pl->X),
+                                                       buf<T>(pl->Y));
   } else {
     dim3 g(d.Nx, 3, d.Kz / pl->KCw);
-    y_forward_warp_kernel<P><<<g, 256, pl->smem_yw_f, s>>>(d, pl->KCw, pl->twy, pl->HZ, pl->HX);
+    y_forward_warp_kernel<P, T><<<g, 256, smT, s>>>(d, pl->KCw, Tx<T>::twy(pl), buf<T>(pl->HZ),
+                                                      buf<T>(pl->HX), pl->ops.xphys);
   }
 }
 
+template <typename T>
 static void launch_y_warp_any(jfb_kmm_plan* pl, cudaStream_t s, bool backward) {
   switch (pl->py) {
-    case 2: launch_y_warp<2>(pl, s, backward); break;
-    case 3: launch_y_warp<3>(pl, s, backward); break;
-    case 4: launch_y_warp<4>(pl, s, backward); break;
-    default: launch_y_warp<6>(pl, s, backward); break;
+    case 2: launch_y_warp<2, T>(pl, s, backward); break;
+    case 3: launch_y_warp<3, T>(pl, s, backward); break;
+    case 4: launch_y_warp<4, T>(pl, s, backward); break;
+    default: launch_y_warp<6, T>(pl, s, backward); break;
   }
 }
 
-template <int P>
+template <int P, typename T>
 static void launch_zcross_warp(jfb_kmm_plan* pl, cudaStream_t s) {
   const Dims& d = pl->d;
   const int pairs = ceil_div((int64_t)d.Nx * d.My, 2);
   const int blocks = ceil_div(pairs, 8);
   if (pl->qk == 1)
-    z_cross_warp_kernel<P, 1><<<blocks, 256, 0, s>>>(pl->ops, d, pl->twz, pl->Y, pl->HZ);
+    z_cross_warp_kernel<P, 1, T><<<blocks, 256, 0, s>>>(pl->ops, d, Tx<T>::twz(pl), buf<T>(pl->Y),
+                                                      buf<T>(pl->HZ));
   else
-    z_cross_warp_kernel<P, 2><<<blocks, 256, 0, s>>>(pl->ops, d, pl->twz, pl->Y, pl->HZ);
+    z_cross_warp_kernel<P, 2, T><<<blocks, 256, 0, s>>>(pl->ops, d, Tx<T>::twz(pl), buf<T>(pl->Y),
+                                                      buf<T>(pl->HZ));
 }
 
 template <int P>
@@ -471,39 +516,67 @@ static void launch_zfwd_warp(jfb_kmm_plan* pl, const double* u0, const double* u
     z_forward_real_warp_kernel<P, 2><<<blocks, 256, 0, s>>>(d, pl->twnz, u0, u1, u2, pl->HZ);
 }
 
+template <int PY, int PZ, typename T>
+static void launch_plane(jfb_kmm_plan* pl, cudaStream_t s) {
+  plane_cross_kernel<PY, PZ, 1, T><<<2 * pl->d.Nx, kPlaneThreads,
+                                     plane_smem_bytes(pl->d.My, pl->d.Kz, sizeof(cpx<T>)), s>>>(
+      pl->ops, pl->d, Tx<T>::twy(pl), Tx<T>::twz(pl), buf<T>(pl->X), buf<T>(pl->HX));
+}
+
 // y_backward -> z_cross -> y_forward: HX <- H(state whose x-physical fields are in X)
-static int launch_transforms(jfb_kmm_plan* pl, cudaStream_t s) {
+template <typename T>
+static int launch_transforms_t(jfb_kmm_plan* pl, cudaStream_t s) {
   const Dims& d = pl->d;
+  if (pl->plane) {
+    const int key = pl->py * 10 + pl->pz;
+    if (key == 22) launch_plane<2, 2, T>(pl, s);
+    else if (key == 23) launch_plane<2, 3, T>(pl, s);
+    else if (key == 32) launch_plane<3, 2, T>(pl, s);
+    else launch_plane<3, 3, T>(pl, s);
+    JFB_CHECK_LAUNCH();
+    if (pl->timing_events)
+      for (int k = 2; k <= 4; ++k) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[k], s));
+    return JFB_OK;
+  }
   if (pl->py && pl->pz) {
-    launch_y_warp_any(pl, s, true);
+    launch_y_warp_any<T>(pl, s, true);
     JFB_CHECK_LAUNCH();
     if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[2], s));
     switch (pl->pz) {
-      case 2: launch_zcross_warp<2>(pl, s); break;
-      case 3: launch_zcross_warp<3>(pl, s); break;
-      case 4: launch_zcross_warp<4>(pl, s); break;
-      default: launch_zcross_warp<6>(pl, s); break;
+      case 2: launch_zcross_warp<2, T>(pl, s); break;
+      case 3: launch_zcross_warp<3, T>(pl, s); break;
+      case 4: launch_zcross_warp<4, T>(pl, s); break;
+      default: launch_zcross_warp<6, T>(pl, s); break;
     }
     JFB_CHECK_LAUNCH();
     if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[3], s));
-    launch_y_warp_any(pl, s, false);
+    launch_y_warp_any<T>(pl, s, false);
     JFB_CHECK_LAUNCH();
     if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[4], s));
     return JFB_OK;
   }
   dim3 gy(d.Nx, 6, d.Kz / pl->KC);
-  y_backward_kernel<<<gy, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->X, pl->Y);
+  const size_t smy = pl->smem_y / sizeof(c64) * sizeof(cpx<T>);
+  const size_t smz = pl->smem_z / sizeof(c64) * sizeof(cpx<T>);
+  y_backward_kernel<T><<<gy, 256, smy, s>>>(d, pl->fy, pl->KC, Tx<T>::twy(pl), buf<T>(pl->X),
+                                            buf<T>(pl->Y));
   JFB_CHECK_LAUNCH();
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[2], s));
   const int zb = ceil_div((int64_t)d.Nx * d.My, kZRows);
-  z_cross_kernel<<<zb, 256, pl->smem_z, s>>>(pl->ops, d, pl->fz, pl->twz, pl->Y, pl->HZ);
+  z_cross_kernel<T><<<zb, 256, smz, s>>>(pl->ops, d, pl->fz, Tx<T>::twz(pl), buf<T>(pl->Y),
+                                         buf<T>(pl->HZ));
   JFB_CHECK_LAUNCH();
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[3], s));
   dim3 gf(d.Nx, 3, d.Kz / pl->KC);
-  y_forward_kernel<<<gf, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->HZ, pl->HX);
+  y_forward_kernel<T><<<gf, 256, smy, s>>>(d, pl->fy, pl->KC, Tx<T>::twy(pl), buf<T>(pl->HZ),
+                                           buf<T>(pl->HX), pl->ops.xphys);
   JFB_CHECK_LAUNCH();
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[4], s));
   return JFB_OK;
+}
+
+static int launch_transforms(jfb_kmm_plan* pl, cudaStream_t s) {
+  return pl->mixed ? launch_transforms_t<float>(pl, s) : launch_transforms_t<double>(pl, s);
 }
 
 static inline int slot(int64_t m) { return (int)(((m % 3) + 3) % 3); }
@@ -531,6 +604,7 @@ static int ensure_H(jfb_kmm_plan* pl, cudaStream_t s) {
   if (st) return st;
   StageArgs a = blank_args();
   a.mode = kPrologue;
+  a.x32 = pl->mixed ? 1 : 0;
   const int c = slot(pl->n);
   a.pu0 = pl->U0[c];
   a.pu1 = pl->U1S;
@@ -660,7 +734,8 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   JFB_REQUIRE(cfg->family == JFB_FAMILY_CHEBYSHEV, "only the Chebyshev family is supported");
   JFB_REQUIRE(cfg->nonlinear_form == JFB_NONLINEAR_ROTATIONAL,
               "only the rotational nonlinear form is supported");
-  JFB_REQUIRE(cfg->precision == JFB_PRECISION_FP64, "precision not supported");
+  JFB_REQUIRE(cfg->precision == JFB_PRECISION_FP64 || cfg->precision == JFB_PRECISION_MIXED,
+              "precision must be JFB_PRECISION_FP64 or JFB_PRECISION_MIXED");
   JFB_REQUIRE(cfg->nx >= 9 && cfg->nx <= 64 * kMaxNR + 1, "nx out of range [9, 129]");
   JFB_REQUIRE(cfg->ny >= 4 && cfg->ny % 2 == 0 && cfg->nz >= 4 && cfg->nz % 2 == 0,
               "ny, nz must be even");
@@ -716,30 +791,50 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   while (d.Kz % pl->KCw) pl->KCw /= 2;
   pl->smem_yw_b = (size_t)(d.Ny + d.My) * (pl->KCw + 1) * sizeof(c64);
   pl->smem_yw_f = pl->smem_yw_b;
+  // fused plane transforms: warp-FFT lengths 64 or 96 on both periodic axes,
+  // Kz even and <= 32, and the plane buffers within one CTA pair
+  pl->mixed = cfg->precision == JFB_PRECISION_MIXED;
+  pl->smem_plane = plane_smem_bytes(d.My, d.Kz, pl->mixed ? sizeof(c32) : sizeof(c64));
+  pl->plane = (pl->py == 2 || pl->py == 3) && (pl->pz == 2 || pl->pz == 3) && d.Kz % 2 == 0 &&
+              d.Kz <= 32 && pl->smem_plane <= 227 * 1024;
+  {
+    const char* ev = std::getenv("JFB200_TRANSFORMS");
+    if (ev && std::string(ev) == "split") pl->plane = false;
+  }
+  if (pl->plane) {
+    auto attr = [&](const void* fn) { return allow_smem(fn); };
+    if (attr((const void*)plane_cross_kernel<2, 2, 1, double>) != cudaSuccess ||
+        attr((const void*)plane_cross_kernel<2, 3, 1, double>) != cudaSuccess ||
+        attr((const void*)plane_cross_kernel<3, 2, 1, double>) != cudaSuccess ||
+        attr((const void*)plane_cross_kernel<3, 3, 1, double>) != cudaSuccess ||
+        attr((const void*)plane_cross_kernel<2, 2, 1, float>) != cudaSuccess ||
+        attr((const void*)plane_cross_kernel<2, 3, 1, float>) != cudaSuccess ||
+        attr((const void*)plane_cross_kernel<3, 2, 1, float>) != cudaSuccess ||
+        attr((const void*)plane_cross_kernel<3, 3, 1, float>) != cudaSuccess) {
+      set_error("cannot configure the plane transform kernel");
+      return fail(JFB_ERR_CUDA);
+    }
+  }
   pl->smem_diag = (size_t)kNW * 4 * d.Nx * sizeof(c64) + 2 * kNW * sizeof(double);
   if (pl->smem_pencil > 227 * 1024 || pl->smem_y > 227 * 1024 || pl->smem_z > 227 * 1024) {
     set_error("grid too large for the shared-memory tiling");
     return fail(JFB_ERR_ARG);
   }
-  cudaFuncSetAttribute(pencil_stage_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)pl->smem_pencil);
-  cudaFuncSetAttribute(pencil_stage_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)pl->smem_pencil);
-  cudaFuncSetAttribute(y_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)pl->smem_y);
-  cudaFuncSetAttribute(y_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)pl->smem_y);
-  cudaFuncSetAttribute(z_cross_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)pl->smem_z);
-  cudaFuncSetAttribute(z_forward_real_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)pl->smem_zf);
-  cudaFuncSetAttribute(diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)pl->smem_diag);
+  allow_smem((const void*)pencil_stage_kernel<1>);
+  allow_smem((const void*)pencil_stage_kernel<2>);
+  for (const void* fn : {(const void*)y_backward_kernel<double>, (const void*)y_forward_kernel<double>,
+                         (const void*)y_backward_kernel<float>, (const void*)y_forward_kernel<float>})
+    allow_smem(fn);
+  for (const void* fn : {(const void*)z_cross_kernel<double>, (const void*)z_cross_kernel<float>})
+    allow_smem(fn);
+  allow_smem((const void*)z_forward_real_kernel);
+  allow_smem((const void*)diag_kernel);
 #define JFB_YW_ATTR(P)                                                                   \
-  cudaFuncSetAttribute(y_backward_warp_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                       (int)pl->smem_yw_b);                                              \
-  cudaFuncSetAttribute(y_forward_warp_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                       (int)pl->smem_yw_f);
+  for (const void* fn : {(const void*)y_backward_warp_kernel<P, double>,                  \
+                         (const void*)y_forward_warp_kernel<P, double>,                   \
+                         (const void*)y_backward_warp_kernel<P, float>,                   \
+                         (const void*)y_forward_warp_kernel<P, float>})                   \
+    allow_smem(fn);
   JFB_YW_ATTR(2)
   JFB_YW_ATTR(3)
   JFB_YW_ATTR(4)
@@ -797,6 +892,15 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   if (st) return fail(st);
   st = upload(pl, &pl->twz, twiddles(d.Mz));
   if (st) return fail(st);
+  if (pl->mixed) {
+    auto narrow = [](const std::vector<c64>& t) {
+      std::vector<c32> o(t.size());
+      for (size_t k = 0; k < t.size(); ++k) o[k] = cmk((float)t[k].re, (float)t[k].im);
+      return o;
+    };
+    if ((st = upload(pl, &pl->twy32, narrow(twiddles(d.My))))) return fail(st);
+    if ((st = upload(pl, &pl->twz32, narrow(twiddles(d.Mz))))) return fail(st);
+  }
   if (!make_fft_plan(d.Ny, pl->fny) || !make_fft_plan(d.Nz, pl->fnz)) {
     set_error("ny, nz must be of the form 2^a 3^b");
     return fail(JFB_ERR_ARG);
@@ -892,8 +996,7 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
       G.kt_mg_lin[0] = ceil_div(nDe, 4);
       G.kt_mg_lin[1] = ceil_div(nDo, 4);
       pl->smem_gemm = smem;
-      JFB_CHECK_CUDA(cudaFuncSetAttribute(pencil_gemm_kernel,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      JFB_CHECK_CUDA(allow_smem((const void*)pencil_gemm_kernel));
     }
   }
 
@@ -926,8 +1029,11 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   if ((st = cal(&pl->NVWst, d.nD))) return fail(st);
   if ((st = cal(&pl->U1S, (size_t)d.nD * P))) return fail(st);
   if ((st = cal(&pl->U2S, (size_t)d.nD * P))) return fail(st);
-  if ((st = cal(&pl->X, (size_t)6 * d.Nx * P))) return fail(st);
-  if ((st = cal(&pl->Y, (size_t)6 * d.Nx * d.My * d.Kz))) return fail(st);
+  // X and Y exist only for the step: half size in the mixed form (complex64);
+  // HZ and HX also serve the FP64 state_from_physical path
+  const size_t xs = pl->mixed ? 2 : 1;
+  if ((st = cal(&pl->X, ((size_t)6 * d.Nx * P + xs - 1) / xs))) return fail(st);
+  if ((st = cal(&pl->Y, ((size_t)6 * d.Nx * d.My * d.Kz + xs - 1) / xs))) return fail(st);
   if ((st = cal(&pl->HZ, (size_t)3 * d.Nx * d.My * d.Kz))) return fail(st);
   if ((st = cal(&pl->HX, (size_t)3 * d.Nx * P))) return fail(st);
   if ((st = cal(&pl->HD, (size_t)3 * d.nD * P))) return fail(st);
@@ -955,7 +1061,7 @@ extern "C" int jfb_kmm_get_info(const jfb_kmm_plan* pl, jfb_kmm_info* info) {
   const Dims& d = pl->d;
   info->n_pencils = d.P;
   info->device_bytes = pl->device_bytes;
-  info->launches_per_step = 4;
+  info->launches_per_step = pl->plane ? 2 : 4;
   // stage model: 43 E_s + 18 E_m complex values, E_s = Nx Ny (Nz/2+1), E_m = Nx My (Nz/2+1)
   const int64_t H = d.Nz / 2 + 1;
   const int64_t Es = (int64_t)d.Nx * d.Ny * H, Em = (int64_t)d.Nx * d.My * H;
@@ -1094,6 +1200,7 @@ extern "C" int jfb_kmm_convection(jfb_kmm_plan* pl, void* h0, void* h1, void* h2
   if (st) return st;
   StageArgs a = blank_args();
   a.mode = kHOnly;
+  a.x32 = pl->mixed ? 1 : 0;
   a.HX = pl->HX;
   a.Hd_out = pl->HD;
   st = launch_pencil(pl, a, s);
@@ -1134,9 +1241,9 @@ extern "C" int jfb_kmm_state_from_physical(jfb_kmm_plan* pl, const double* u0,
   int KC = d.Kz;
   while ((size_t)2 * d.Ny * KC * sizeof(c64) > 100 * 1024 && KC % 2 == 0) KC /= 2;
   dim3 gf(d.Nx, 3, d.Kz / KC);
-  y_forward_kernel<<<gf, 256, (size_t)2 * d.Ny * KC * sizeof(c64), s>>>(dy, pl->fny, KC,
+  y_forward_kernel<double><<<gf, 256, (size_t)2 * d.Ny * KC * sizeof(c64), s>>>(dy, pl->fny, KC,
                                                                         pl->twny, pl->HZ,
-                                                                        pl->HX);
+                                                                        pl->HX, nullptr);
   JFB_CHECK_LAUNCH();
   // history reset and x: Shen forward transforms, g = i ky u2 - i kz u1
   pl->n = 0;

@@ -75,6 +75,7 @@ struct GemmStageArgs {
   int su_rec, sg_rec;
   c64 *u0_out, *g_out, *vw_out;
   c64* X;
+  int x32;  // HX and X hold complex64 values (mixed form)
 };
 
 __host__ __device__ inline int round4(int x) { return (x + 3) & ~3; }
@@ -103,6 +104,10 @@ __device__ __forceinline__ void prefetch_l2(const void* ptr, size_t bytes) {
 // 16-byte asynchronous global -> shared copy (L2 only), and its completion.
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem)), "l"(gmem)
                : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
@@ -408,7 +413,12 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
         dst_row = ((i & 1) ? G.oMGO : G.oMGE) + l * nh + (i >> 1);
       }
       const int kyrow = side ? d.Ny - kyi : kyi;
-      cp_async16(rowc + (size_t)dst_row * LC + side * 8 + kz, src + (size_t)kyrow * d.Kz + kz0 + kz);
+      const size_t so = (size_t)kyrow * d.Kz + kz0 + kz;
+      if (a.x32 && r < 3 * N)  // complex64 sample: lands in the first half of the slot
+        cp_async8(rowc + (size_t)dst_row * LC + side * 8 + kz,
+                  reinterpret_cast<const c32*>(a.HX) + (src - a.HX) + so);
+      else
+        cp_async16(rowc + (size_t)dst_row * LC + side * 8 + kz, src + so);
     }
     cp_async_commit();
     cp_async_wait_all();
@@ -426,10 +436,16 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     const int j = idx / kGW, w = idx % kGW, jm = N - 1 - j;
     const bool ok = s_p[w] >= 0;
     c64 h[2][3];
+    auto slot = [&](int row) {
+      const c64* q = rowc + (size_t)row * LC + w;
+      if (!a.x32) return *q;
+      const c32 v = *reinterpret_cast<const c32*>(q);
+      return cmk((double)v.re, (double)v.im);
+    };
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
-      h[0][f] = ok ? rowc[(G.oH[f] + j) * LC + w] : cmk(0.0, 0.0);
-      h[1][f] = (ok && jm != j) ? rowc[(G.oH[f] + jm) * LC + w] : cmk(0.0, 0.0);
+      h[0][f] = ok ? slot(G.oH[f] + j) : cmk(0.0, 0.0);
+      h[1][f] = (ok && jm != j) ? slot(G.oH[f] + jm) : cmk(0.0, 0.0);
     }
     if (mean_cta && w == 0) {
       mean[j] = h[0][1].re;
@@ -713,9 +729,17 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
                         cmk(acc[9][0], acc[9][1]), fo);
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
-          c64* X = a.X + (size_t)q * N * P + p;
-          X[(size_t)j * P] = fe[q] + fo[q];
-          X[(size_t)jm * P] = fe[q] - fo[q];
+          const c64 vp = fe[q] + fo[q], vm = fe[q] - fo[q];
+          const size_t e = (size_t)q * N * P + p;
+          if (a.x32) {
+            c32* X = reinterpret_cast<c32*>(a.X) + e;
+            X[(size_t)j * P] = cmk((float)vp.re, (float)vp.im);
+            X[(size_t)jm * P] = cmk((float)vm.re, (float)vm.im);
+          } else {
+            c64* X = a.X + e;
+            X[(size_t)j * P] = vp;
+            X[(size_t)jm * P] = vm;
+          }
         }
       }
     }
@@ -740,7 +764,11 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
       c64 f[6];
       velocity_fields(s_ky[w], s_kz[w], val(0), val(2), val(1), val(3), val(4), f);
 #pragma unroll
-      for (int q = 0; q < 6; ++q) a.X[(size_t)q * N * P + (size_t)Jl * P + s_p[w]] = f[q];
+      for (int q = 0; q < 6; ++q) {
+        const size_t e = (size_t)q * N * P + (size_t)Jl * P + s_p[w];
+        if (a.x32) reinterpret_cast<c32*>(a.X)[e] = cmk((float)f[q].re, (float)f[q].im);
+        else a.X[e] = f[q];
+      }
     }
   }
 }

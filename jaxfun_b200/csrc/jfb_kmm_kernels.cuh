@@ -79,6 +79,7 @@ struct StageArgs {
   c64* X;                      // 6 x [Nx][P]
   c64* Hd_out;                 // kHOnly: 3 x [nD][P]
   c64 *u1_out, *u2_out;        // kFromPhys: tangential velocity (nD x P)
+  int x32;  // HX (read, step modes) and X (written by the x-backward) hold complex64
 };
 
 __host__ __device__ inline int packed_rec_size(int n) {
@@ -618,7 +619,15 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
     for (int idx = threadIdx.x; idx < 3 * d.Nx * kNW; idx += blockDim.x) {
       const int w = idx % kNW, fi = idx / kNW;
       c64 v = cmk(0.0, 0.0);
-      if (w < nvalid && !nyq) v = a.HX[(size_t)fi * P + p0 + w];
+      if (w < nvalid && !nyq) {
+        const size_t e = (size_t)fi * P + p0 + w;
+        if (a.x32 && a.mode != kFromPhys) {
+          const c32 h = reinterpret_cast<const c32*>(a.HX)[e];
+          v = cmk((double)h.re, (double)h.im);
+        } else {
+          v = a.HX[e];
+        }
+      }
       R1[fi * kLDW + w] = v;
     }
     __syncthreads();
@@ -885,33 +894,39 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
   __syncthreads();
   for (int idx = threadIdx.x; idx < 6 * d.Nx * kNW; idx += blockDim.x) {
     const int w = idx % kNW, fi = idx / kNW;
-    if (w < nvalid) a.X[(size_t)fi * P + p0 + w] = R1[fi * kLDW + w];
+    if (w < nvalid) {
+      const size_t e = (size_t)fi * P + p0 + w;
+      const c64 v = R1[fi * kLDW + w];
+      if (a.x32) reinterpret_cast<c32*>(a.X)[e] = cmk((float)v.re, (float)v.im);
+      else a.X[e] = v;
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // y_backward: per (x-plane, field): pad Ny -> My (middle zeros), inverse FFT.
 // ---------------------------------------------------------------------------
+template <typename T>
 __global__ void __launch_bounds__(256) y_backward_kernel(Dims d, FFTPlan plan, int KC,
-                                                         const c64* __restrict__ tw,
-                                                         const c64* __restrict__ X,
-                                                         c64* __restrict__ Y) {
+                                                         const cpx<T>* __restrict__ tw,
+                                                         const cpx<T>* __restrict__ X,
+                                                         cpx<T>* __restrict__ Y) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  c64* A = reinterpret_cast<c64*>(smem_raw);
-  c64* B = A + d.My * KC;
+  cpx<T>* A = reinterpret_cast<cpx<T>*>(smem_raw);
+  cpx<T>* B = A + d.My * KC;
   const int j = blockIdx.x, f = blockIdx.y, kc0 = blockIdx.z * KC;
-  const c64* src = X + ((size_t)f * d.Nx + j) * d.P + kc0;
+  const cpx<T>* src = X + ((size_t)f * d.Nx + j) * d.P + kc0;
   const int half = d.Ny / 2;
   for (int idx = threadIdx.x; idx < d.My * KC; idx += blockDim.x) {
     const int kz = idx % KC, r = idx / KC;
-    c64 v = cmk(0.0, 0.0);
+    cpx<T> v = cmk(T(0), T(0));
     if (r < half) v = src[r * d.Kz + kz];
     else if (r >= d.My - half) v = src[(r - d.My + d.Ny) * d.Kz + kz];
     A[idx] = v;
   }
   __syncthreads();
-  c64* res = fft_columns<double>(A, B, plan, KC, KC, tw, +1);
-  c64* dst = Y + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
+  cpx<T>* res = fft_columns<T>(A, B, plan, KC, KC, tw, +1);
+  cpx<T>* dst = Y + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
   for (int idx = threadIdx.x; idx < d.My * KC; idx += blockDim.x) {
     const int kz = idx % KC, r = idx / KC;
     dst[(size_t)r * d.Kz + kz] = res[idx];
@@ -925,14 +940,29 @@ __global__ void __launch_bounds__(256) y_backward_kernel(Dims d, FFTPlan plan, i
 // ---------------------------------------------------------------------------
 constexpr int kZRows = 4;
 
+// -(u x omega) of the perturbation (u, omega) about the base flow U_b e_y,
+// U_wall e_z, expanded so that no O(1) base-flow value is added to a
+// perturbation value before the products (FP32 keeps the perturbation's
+// digits): -(u' x w') - U_b e_y x w' - U_wall u' x e_z.  The remaining
+// base-flow self term -U_b U_wall e_x is constant in (y, z) and is added to
+// the (ky, kz) = (0, 0) mode after the forward transforms.
+template <typename T>
+__device__ __forceinline__ void rotational_product(T u0, T u1, T u2, T w0, T w1, T w2, T ub, T uw,
+                                                   T& n0, T& n1, T& n2) {
+  n0 = -((u1 * w2 - u2 * w1) + uw * u1 + ub * w2);
+  n1 = -((u2 * w0 - u0 * w2) - uw * u0);
+  n2 = -((u0 * w1 - u1 * w0) - ub * w0);
+}
+
+template <typename T>
 __global__ void __launch_bounds__(256) z_cross_kernel(DevOps o, Dims d, FFTPlan plan,
-                                                      const c64* __restrict__ tw,
-                                                      const c64* __restrict__ Y,
-                                                      c64* __restrict__ HZ) {
+                                                      const cpx<T>* __restrict__ tw,
+                                                      const cpx<T>* __restrict__ Y,
+                                                      cpx<T>* __restrict__ HZ) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int NC = kZRows * 3;  // packed columns
-  c64* A = reinterpret_cast<c64*>(smem_raw);
-  c64* B = A + d.Mz * NC;
+  cpx<T>* A = reinterpret_cast<cpx<T>*>(smem_raw);
+  cpx<T>* B = A + d.Mz * NC;
   const int row0 = blockIdx.x * kZRows;  // row = j * My + y
   const int nrows = d.Nx * d.My;
   const size_t plane = (size_t)d.Nx * d.My * d.Kz;
@@ -941,48 +971,46 @@ __global__ void __launch_bounds__(256) z_cross_kernel(DevOps o, Dims d, FFTPlan 
     const int c = idx % NC, k = idx / NC;
     const int rl = c / 3, pr = c % 3;
     const int row = row0 + rl;
-    c64 z = cmk(0.0, 0.0);
+    cpx<T> z = cmk(T(0), T(0));
     if (row < nrows) {
-      const c64* fa = Y + (size_t)(2 * pr) * plane + (size_t)row * d.Kz;
-      const c64* fb = Y + (size_t)(2 * pr + 1) * plane + (size_t)row * d.Kz;
+      const cpx<T>* fa = Y + (size_t)(2 * pr) * plane + (size_t)row * d.Kz;
+      const cpx<T>* fb = Y + (size_t)(2 * pr + 1) * plane + (size_t)row * d.Kz;
       if (k == 0) {
         z = cmk(fa[0].re, fb[0].re);
       } else if (k < d.Kz) {
-        const c64 xa = fa[k], xb = fb[k];
+        const cpx<T> xa = fa[k], xb = fb[k];
         z = cmk(xa.re - xb.im, xa.im + xb.re);
       } else if (k > d.Mz - d.Kz) {
         const int kk = d.Mz - k;
-        const c64 xa = fa[kk], xb = fb[kk];  // conj(xa) + i conj(xb)
+        const cpx<T> xa = fa[kk], xb = fb[kk];  // conj(xa) + i conj(xb)
         z = cmk(xa.re + xb.im, -xa.im + xb.re);
       }
     }
     A[k * NC + c] = z;
   }
   __syncthreads();
-  c64* phys = fft_columns<double>(A, B, plan, NC, NC, tw, +1);
-  c64* other = (phys == A) ? B : A;
+  cpx<T>* phys = fft_columns<T>(A, B, plan, NC, NC, tw, +1);
+  cpx<T>* other = (phys == A) ? B : A;
   // products: packed output columns per row pair q: [n0a+i n1a, n0b+i n1b, n2a+i n2b]
   const int NCf = (kZRows / 2) * 3;
   for (int idx = threadIdx.x; idx < d.Mz * kZRows; idx += blockDim.x) {
     const int rl = idx % kZRows, n = idx / kZRows;
     const int row = row0 + rl;
     const int j = (row < nrows) ? row / d.My : 0;
-    const c64 z0 = phys[n * NC + rl * 3 + 0];
-    const c64 z1 = phys[n * NC + rl * 3 + 1];
-    const c64 z2 = phys[n * NC + rl * 3 + 2];
-    const double u0 = z0.re, u1 = z0.im + d.uwall * o.xphys[j], u2 = z1.re;
-    const double w0 = z1.im, w1 = z2.re, w2 = z2.im + d.uwall;
-    const double n0 = -(u1 * w2 - u2 * w1);
-    const double n1 = -(u2 * w0 - u0 * w2);
-    const double n2 = -(u0 * w1 - u1 * w0);
+    const cpx<T> z0 = phys[n * NC + rl * 3 + 0];
+    const cpx<T> z1 = phys[n * NC + rl * 3 + 1];
+    const cpx<T> z2 = phys[n * NC + rl * 3 + 2];
+    T n0, n1, n2;
+    rotational_product(z0.re, z0.im, z1.re, z1.im, z2.re, z2.im, T(d.uwall * o.xphys[j]),
+                       T(d.uwall), n0, n1, n2);
     const int q = rl >> 1, ab = rl & 1;
     other[n * NCf + q * 3 + ab] = cmk(n0, n1);
     if (ab == 0) other[n * NCf + q * 3 + 2].re = n2;
     else other[n * NCf + q * 3 + 2].im = n2;
   }
   __syncthreads();
-  c64* spec = fft_columns<double>(other, phys, plan, NCf, NCf, tw, -1);
-  const double scale = 1.0 / d.Mz;
+  cpx<T>* spec = fft_columns<T>(other, phys, plan, NCf, NCf, tw, -1);
+  const T scale = T(1.0 / d.Mz);
   for (int idx = threadIdx.x; idx < d.Kz * kZRows * 3; idx += blockDim.x) {
     const int k = idx % d.Kz;
     const int rf = idx / d.Kz;
@@ -991,13 +1019,14 @@ __global__ void __launch_bounds__(256) z_cross_kernel(DevOps o, Dims d, FFTPlan 
     if (row >= nrows) continue;
     const int q = rl >> 1, ab = rl & 1;
     const int col = (f < 2) ? q * 3 + ab : q * 3 + 2;
-    const c64 Zk = spec[k * NCf + col];
-    const c64 Zm = spec[((d.Mz - k) % d.Mz) * NCf + col];
+    const cpx<T> Zk = spec[k * NCf + col];
+    const cpx<T> Zm = spec[((d.Mz - k) % d.Mz) * NCf + col];
     // x + i y packed: X_k = (Z_k + conj Z_-k)/2, Y_k = (Z_k - conj Z_-k)/(2i)
-    c64 v;
+    cpx<T> v;
     const bool take_real = (f < 2) ? (f == 0) : (ab == 0);
-    if (take_real) v = cmk(0.5 * (Zk.re + Zm.re), 0.5 * (Zk.im - Zm.im));
-    else v = cmk(0.5 * (Zk.im + Zm.im), -0.5 * (Zk.re - Zm.re));
+    const T h = T(0.5);
+    if (take_real) v = cmk(h * (Zk.re + Zm.re), h * (Zk.im - Zm.im));
+    else v = cmk(h * (Zk.im + Zm.im), -h * (Zk.re - Zm.re));
     HZ[(size_t)f * plane + (size_t)row * d.Kz + k] = scale * v;
   }
 }
@@ -1005,27 +1034,34 @@ __global__ void __launch_bounds__(256) z_cross_kernel(DevOps o, Dims d, FFTPlan 
 // ---------------------------------------------------------------------------
 // y_forward: per (x-plane, field): forward FFT My, scale 1/My, keep Ny modes.
 // ---------------------------------------------------------------------------
+template <typename T>
 __global__ void __launch_bounds__(256) y_forward_kernel(Dims d, FFTPlan plan, int KC,
-                                                        const c64* __restrict__ tw,
-                                                        const c64* __restrict__ HZ,
-                                                        c64* __restrict__ HX) {
+                                                        const cpx<T>* __restrict__ tw,
+                                                        const cpx<T>* __restrict__ HZ,
+                                                        cpx<T>* __restrict__ HX,
+                                                        const double* __restrict__ xb) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  c64* A = reinterpret_cast<c64*>(smem_raw);
-  c64* B = A + d.My * KC;
+  cpx<T>* A = reinterpret_cast<cpx<T>*>(smem_raw);
+  cpx<T>* B = A + d.My * KC;
   const int j = blockIdx.x, f = blockIdx.y, kc0 = blockIdx.z * KC;
-  const c64* src = HZ + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
+  const cpx<T>* src = HZ + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
   for (int idx = threadIdx.x; idx < d.My * KC; idx += blockDim.x) {
     const int kz = idx % KC, r = idx / KC;
     A[idx] = src[(size_t)r * d.Kz + kz];
   }
   __syncthreads();
-  c64* res = fft_columns<double>(A, B, plan, KC, KC, tw, -1);
-  const double scale = 1.0 / d.My;
+  cpx<T>* res = fft_columns<T>(A, B, plan, KC, KC, tw, -1);
+  const T scale = T(1.0 / d.My);
   const int half = d.Ny / 2;
-  c64* dst = HX + ((size_t)f * d.Nx + j) * d.P + kc0;
+  if (xb && f == 0 && kc0 == 0 && threadIdx.x == 0) {
+    // base-flow self term -U_b U_wall e_x: its (ky, kz) = (0, 0) mode
+    res[0].re += T(-d.uwall * xb[j] * d.uwall * d.My);
+  }
+  __syncthreads();
+  cpx<T>* dst = HX + ((size_t)f * d.Nx + j) * d.P + kc0;
   for (int idx = threadIdx.x; idx < d.Ny * KC; idx += blockDim.x) {
     const int kz = idx % KC, r = idx / KC;
-    c64 v = cmk(0.0, 0.0);
+    cpx<T> v = cmk(T(0), T(0));
     if (r < half) v = res[r * KC + kz];
     else if (r > half) v = res[(r - d.Ny + d.My) * KC + kz];  // r == half: Nyquist
     dst[(size_t)r * d.Kz + kz] = scale * v;

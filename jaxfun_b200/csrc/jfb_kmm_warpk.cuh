@@ -2,6 +2,8 @@
 // (used when the transform lengths are 32 P with P in {2, 3, 4, 6}).
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "jfb_kmm_kernels.cuh"
 #include "jfb_warpfft.cuh"
 
@@ -13,43 +15,43 @@ namespace jfb {
 // (zero padding Ny -> My in the middle of the spectrum), and the padded
 // plane is written back with coalesced rows.
 // ---------------------------------------------------------------------------
-template <int P>
+template <int P, typename T>
 __global__ void __launch_bounds__(256) y_backward_warp_kernel(Dims d, int KC,
-                                                              const c64* __restrict__ tw,
-                                                              const c64* __restrict__ X,
-                                                              c64* __restrict__ Y) {
+                                                              const cpx<T>* __restrict__ tw,
+                                                              const cpx<T>* __restrict__ X,
+                                                              cpx<T>* __restrict__ Y) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ld = KC + 1;
-  c64* in = reinterpret_cast<c64*>(smem_raw);  // Ny x ld
-  c64* out = in + d.Ny * ld;                   // My x ld
+  cpx<T>* in = reinterpret_cast<cpx<T>*>(smem_raw);  // Ny x ld
+  cpx<T>* out = in + d.Ny * ld;                   // My x ld
   const int j = blockIdx.x, f = blockIdx.y, kc0 = blockIdx.z * KC;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const c64* src = X + ((size_t)f * d.Nx + j) * d.P + kc0;
+  const cpx<T>* src = X + ((size_t)f * d.Nx + j) * d.P + kc0;
   for (int idx = threadIdx.x; idx < d.Ny * KC; idx += blockDim.x) {
     const int c = idx % KC, r = idx / KC;
     in[r * ld + c] = src[(size_t)r * d.Kz + c];
   }
-  WarpTw<P, double> w;
-  load_warp_tw<P, double>(w, tw, lane);
+  WarpTw<P, T> w;
+  load_warp_tw<P, T>(w, tw, lane);
   __syncthreads();
   const int half = d.Ny / 2;
   for (int c = warp; c < KC; c += blockDim.x / 32) {
-    c64 v[P];
+    cpx<T> v[P];
 #pragma unroll
     for (int r = 0; r < P; ++r) {
       const int k = 32 * r + lane;
-      c64 z = cmk(0.0, 0.0);
+      cpx<T> z = cmk(T(0), T(0));
       if (k < half) z = in[k * ld + c];
       else if (k >= d.My - half) z = in[(k - d.My + d.Ny) * ld + c];
       v[r] = z;
     }
-    warp_fft_inverse<P, double>(v, w, lane);
+    warp_fft_inverse<P, T>(v, w, lane);
     const int br = bitrev5(lane);
 #pragma unroll
     for (int k1 = 0; k1 < P; ++k1) out[(k1 + P * br) * ld + c] = v[k1];
   }
   __syncthreads();
-  c64* dst = Y + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
+  cpx<T>* dst = Y + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
   for (int idx = threadIdx.x; idx < d.My * KC; idx += blockDim.x) {
     const int c = idx % KC, r = idx / KC;
     dst[(size_t)r * d.Kz + c] = out[r * ld + c];
@@ -60,43 +62,49 @@ __global__ void __launch_bounds__(256) y_backward_warp_kernel(Dims d, int KC,
 // y_forward: per (x-plane, field, kz chunk): forward FFT My along y, keep the
 // Ny retained modes (Nyquist zeroed), scale 1/My.
 // ---------------------------------------------------------------------------
-template <int P>
+template <int P, typename T>
 __global__ void __launch_bounds__(256) y_forward_warp_kernel(Dims d, int KC,
-                                                             const c64* __restrict__ tw,
-                                                             const c64* __restrict__ HZ,
-                                                             c64* __restrict__ HX) {
+                                                             const cpx<T>* __restrict__ tw,
+                                                             const cpx<T>* __restrict__ HZ,
+                                                             cpx<T>* __restrict__ HX,
+                                                             const double* __restrict__ xb) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ld = KC + 1;
-  c64* in = reinterpret_cast<c64*>(smem_raw);  // My x ld
-  c64* out = in + d.My * ld;                   // Ny x ld
+  cpx<T>* in = reinterpret_cast<cpx<T>*>(smem_raw);  // My x ld
+  cpx<T>* out = in + d.My * ld;                   // Ny x ld
   const int j = blockIdx.x, f = blockIdx.y, kc0 = blockIdx.z * KC;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const c64* src = HZ + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
+  const cpx<T>* src = HZ + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
   for (int idx = threadIdx.x; idx < d.My * KC; idx += blockDim.x) {
     const int c = idx % KC, r = idx / KC;
     in[r * ld + c] = src[(size_t)r * d.Kz + c];
   }
-  WarpTw<P, double> w;
-  load_warp_tw<P, double>(w, tw, lane);
+  WarpTw<P, T> w;
+  load_warp_tw<P, T>(w, tw, lane);
   __syncthreads();
   const int half = d.Ny / 2;
-  const double scale = 1.0 / d.My;
+  const T scale = T(1.0 / d.My);
   const int br = bitrev5(lane);
   for (int c = warp; c < KC; c += blockDim.x / 32) {
-    c64 v[P];
+    cpx<T> v[P];
 #pragma unroll
     for (int n1 = 0; n1 < P; ++n1) v[n1] = in[(n1 + P * br) * ld + c];
-    warp_fft_forward<P, double>(v, w, lane);
+    warp_fft_forward<P, T>(v, w, lane);
 #pragma unroll
     for (int k1 = 0; k1 < P; ++k1) {
       const int k = 32 * k1 + lane;
       if (k < half) out[k * ld + c] = scale * v[k1];
       else if (k > d.My - half) out[(k - d.My + d.Ny) * ld + c] = scale * v[k1];
-      else if (k == d.My - half) out[half * ld + c] = cmk(0.0, 0.0);  // Nyquist
+      else if (k == d.My - half) out[half * ld + c] = cmk(T(0), T(0));  // Nyquist
     }
   }
   __syncthreads();
-  c64* dst = HX + ((size_t)f * d.Nx + j) * d.P + kc0;
+  if (xb && f == 0 && kc0 == 0 && threadIdx.x == 0) {
+    // base-flow self term -U_b U_wall e_x: its (ky, kz) = (0, 0) mode
+    out[0].re += T(-d.uwall * xb[j] * d.uwall);
+  }
+  __syncthreads();
+  cpx<T>* dst = HX + ((size_t)f * d.Nx + j) * d.P + kc0;
   for (int idx = threadIdx.x; idx < d.Ny * KC; idx += blockDim.x) {
     const int c = idx % KC, r = idx / KC;
     dst[(size_t)r * d.Kz + c] = out[r * ld + c];
@@ -106,14 +114,14 @@ __global__ void __launch_bounds__(256) y_forward_warp_kernel(Dims d, int KC,
 // Hermitian-extended packed spectrum Z = A + i B of two real fields whose
 // half spectra (k < Kz) are held as A[q], B[q] at lane l (k = 32 q + l).
 // Z[r] at lane l is Z_(32 r + l) of the length-N = 32 P transform.
-template <int P, int QK>
-__device__ __forceinline__ void build_packed(const c64 (&A)[QK], const c64 (&B)[QK], int Kz,
-                                             int lane, c64 (&Z)[P]) {
+template <int P, int QK, typename T>
+__device__ __forceinline__ void build_packed(const cpx<T> (&A)[QK], const cpx<T> (&B)[QK], int Kz,
+                                             int lane, cpx<T> (&Z)[P]) {
   constexpr int N = 32 * P;
 #pragma unroll
   for (int r = 0; r < P; ++r) {
     const int k = 32 * r + lane;
-    c64 z = cmk(0.0, 0.0);
+    cpx<T> z = cmk(T(0), T(0));
     if (r < QK && k < Kz) {
       z = (k == 0) ? cmk(A[r].re, B[r].re) : cmk(A[r].re - B[r].im, A[r].im + B[r].re);
     }
@@ -121,7 +129,7 @@ __device__ __forceinline__ void build_packed(const c64 (&A)[QK], const c64 (&B)[
     constexpr int dummy = 0;
     (void)dummy;
     const int q1 = P - r - 1, q0 = P - r;
-    c64 a1 = cmk(0.0, 0.0), b1 = a1, a0 = a1, b0 = a1;
+    cpx<T> a1 = cmk(T(0), T(0)), b1 = a1, a0 = a1, b0 = a1;
 #pragma unroll
     for (int q = 0; q < QK; ++q) {
       if (q == q1) {
@@ -136,8 +144,8 @@ __device__ __forceinline__ void build_packed(const c64 (&A)[QK], const c64 (&B)[
     if (k > N - Kz) {
       const int kk = N - k;
       if (kk < Kz) {
-        const c64 a = (lane != 0) ? a1 : a0;
-        const c64 b = (lane != 0) ? b1 : b0;
+        const cpx<T> a = (lane != 0) ? a1 : a0;
+        const cpx<T> b = (lane != 0) ? b1 : b0;
         z = cmk(a.re + b.im, b.re - a.im);
       }
     }
@@ -148,82 +156,80 @@ __device__ __forceinline__ void build_packed(const c64 (&A)[QK], const c64 (&B)[
 // From a natural-order forward transform F of z = x + i y, the half spectra
 // X_k, Y_k at k = 32 q + lane (q < QK): X = (F_k + conj F_{N-k}) / 2,
 // Y = (F_k - conj F_{N-k}) / (2 i).
-template <int P, int QK>
-__device__ __forceinline__ void unpack_pair(const c64 (&F)[P], int lane, c64 (&Xo)[QK],
-                                            c64 (&Yo)[QK]) {
+template <int P, int QK, typename T>
+__device__ __forceinline__ void unpack_pair(const cpx<T> (&F)[P], int lane, cpx<T> (&Xo)[QK],
+                                            cpx<T> (&Yo)[QK]) {
 #pragma unroll
   for (int q = 0; q < QK; ++q) {
-    const c64 m1 = shfl_c(F[(P - q - 1 + P) % P], (32 - lane) & 31);
-    const c64 m0 = shfl_c(F[(P - q) % P], 0);
-    const c64 Zm = (lane != 0) ? m1 : m0;
-    const c64 Zk = F[q];
-    Xo[q] = cmk(0.5 * (Zk.re + Zm.re), 0.5 * (Zk.im - Zm.im));
-    Yo[q] = cmk(0.5 * (Zk.im + Zm.im), -0.5 * (Zk.re - Zm.re));
+    const cpx<T> m1 = shfl_c(F[(P - q - 1 + P) % P], (32 - lane) & 31);
+    const cpx<T> m0 = shfl_c(F[(P - q) % P], 0);
+    const cpx<T> Zm = (lane != 0) ? m1 : m0;
+    const cpx<T> Zk = F[q];
+    const T h = T(0.5);
+    Xo[q] = cmk(h * (Zk.re + Zm.re), h * (Zk.im - Zm.im));
+    Yo[q] = cmk(h * (Zk.im + Zm.im), -h * (Zk.re - Zm.re));
   }
 }
 
 // ---------------------------------------------------------------------------
 // z_cross: one warp per pair of (x, y) rows, everything in registers.
 // ---------------------------------------------------------------------------
-template <int P, int QK>
+template <int P, int QK, typename T>
 __global__ void __launch_bounds__(256) z_cross_warp_kernel(DevOps o, Dims d,
-                                                           const c64* __restrict__ tw,
-                                                           const c64* __restrict__ Y,
-                                                           c64* __restrict__ HZ) {
+                                                           const cpx<T>* __restrict__ tw,
+                                                           const cpx<T>* __restrict__ Y,
+                                                           cpx<T>* __restrict__ HZ) {
   const int lane = threadIdx.x & 31;
   const int pair = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   const int nrows = d.Nx * d.My;
   const int rowa = 2 * pair;
   if (rowa >= nrows) return;
   const bool hasb = rowa + 1 < nrows;
-  WarpTw<P, double> w;
-  load_warp_tw<P, double>(w, tw, lane);
+  WarpTw<P, T> w;
+  load_warp_tw<P, T>(w, tw, lane);
   const size_t plane = (size_t)d.Nx * d.My * d.Kz;
-  double nrm[2][3][P];  // products n0, n1, n2 per row, scrambled layout
+  T nrm[2][3][P];  // products n0, n1, n2 per row, scrambled layout
 #pragma unroll
   for (int rb = 0; rb < 2; ++rb) {
     const int row = rowa + rb;
     const bool ok = rb == 0 || hasb;
-    c64 ph[3][P];
+    cpx<T> ph[3][P];
 #pragma unroll
     for (int pr = 0; pr < 3; ++pr) {
-      c64 A[QK], B[QK];
+      cpx<T> A[QK], B[QK];
 #pragma unroll
       for (int q = 0; q < QK; ++q) {
         const int k = 32 * q + lane;
         const bool in = ok && k < d.Kz;
-        A[q] = in ? Y[(size_t)(2 * pr) * plane + (size_t)row * d.Kz + k] : cmk(0.0, 0.0);
-        B[q] = in ? Y[(size_t)(2 * pr + 1) * plane + (size_t)row * d.Kz + k] : cmk(0.0, 0.0);
+        A[q] = in ? Y[(size_t)(2 * pr) * plane + (size_t)row * d.Kz + k] : cmk(T(0), T(0));
+        B[q] = in ? Y[(size_t)(2 * pr + 1) * plane + (size_t)row * d.Kz + k] : cmk(T(0), T(0));
       }
-      build_packed<P, QK>(A, B, d.Kz, lane, ph[pr]);
-      warp_fft_inverse<P, double>(ph[pr], w, lane);
+      build_packed<P, QK, T>(A, B, d.Kz, lane, ph[pr]);
+      warp_fft_inverse<P, T>(ph[pr], w, lane);
     }
     const int j = (ok ? row : rowa) / d.My;
-    const double ub = d.uwall * o.xphys[j];
+    const T ub = T(d.uwall * o.xphys[j]), uw = T(d.uwall);
 #pragma unroll
     for (int r = 0; r < P; ++r) {
-      const double u0 = ph[0][r].re, u1 = ph[0][r].im + ub, u2 = ph[1][r].re;
-      const double w0 = ph[1][r].im, w1 = ph[2][r].re, w2 = ph[2][r].im + d.uwall;
-      nrm[rb][0][r] = -(u1 * w2 - u2 * w1);
-      nrm[rb][1][r] = -(u2 * w0 - u0 * w2);
-      nrm[rb][2][r] = -(u0 * w1 - u1 * w0);
+      rotational_product(ph[0][r].re, ph[0][r].im, ph[1][r].re, ph[1][r].im, ph[2][r].re,
+                         ph[2][r].im, ub, uw, nrm[rb][0][r], nrm[rb][1][r], nrm[rb][2][r]);
     }
   }
-  c64 F0[P], F1[P], F2[P];
+  cpx<T> F0[P], F1[P], F2[P];
 #pragma unroll
   for (int r = 0; r < P; ++r) {
     F0[r] = cmk(nrm[0][0][r], nrm[0][1][r]);
     F1[r] = cmk(nrm[1][0][r], nrm[1][1][r]);
     F2[r] = cmk(nrm[0][2][r], nrm[1][2][r]);
   }
-  warp_fft_forward<P, double>(F0, w, lane);
-  warp_fft_forward<P, double>(F1, w, lane);
-  warp_fft_forward<P, double>(F2, w, lane);
-  c64 xa0[QK], xa1[QK], xb0[QK], xb1[QK], x2a[QK], x2b[QK];
-  unpack_pair<P, QK>(F0, lane, xa0, xa1);
-  unpack_pair<P, QK>(F1, lane, xb0, xb1);
-  unpack_pair<P, QK>(F2, lane, x2a, x2b);
-  const double scale = 1.0 / (32 * P);
+  warp_fft_forward<P, T>(F0, w, lane);
+  warp_fft_forward<P, T>(F1, w, lane);
+  warp_fft_forward<P, T>(F2, w, lane);
+  cpx<T> xa0[QK], xa1[QK], xb0[QK], xb1[QK], x2a[QK], x2b[QK];
+  unpack_pair<P, QK, T>(F0, lane, xa0, xa1);
+  unpack_pair<P, QK, T>(F1, lane, xb0, xb1);
+  unpack_pair<P, QK, T>(F2, lane, x2a, x2b);
+  const T scale = T(1.0 / (32 * P));
 #pragma unroll
   for (int q = 0; q < QK; ++q) {
     const int k = 32 * q + lane;
@@ -271,9 +277,9 @@ __global__ void __launch_bounds__(256) z_forward_real_warp_kernel(
   warp_fft_forward<P, double>(F1, w, lane);
   warp_fft_forward<P, double>(F2, w, lane);
   c64 xa0[QK], xa1[QK], xb0[QK], xb1[QK], x2a[QK], x2b[QK];
-  unpack_pair<P, QK>(F0, lane, xa0, xa1);
-  unpack_pair<P, QK>(F1, lane, xb0, xb1);
-  unpack_pair<P, QK>(F2, lane, x2a, x2b);
+  unpack_pair<P, QK, double>(F0, lane, xa0, xa1);
+  unpack_pair<P, QK, double>(F1, lane, xb0, xb1);
+  unpack_pair<P, QK, double>(F2, lane, x2a, x2b);
   const size_t plane = (size_t)d.Nx * d.Ny * d.Kz;
   const double scale = 1.0 / N;
 #pragma unroll
@@ -289,6 +295,175 @@ __global__ void __launch_bounds__(256) z_forward_real_warp_kernel(
       out[(size_t)2 * plane + (size_t)(rowa + 1) * d.Kz + k] = scale * x2b[q];
     }
   }
+}
+
+
+// ---------------------------------------------------------------------------
+// plane_cross: y_backward -> z_cross -> y_forward of one x-plane in one
+// launch, on a cluster of two CTAs (distributed shared memory, no
+// multicast).  CTA `rank` owns kz columns [rank Kz/2, (rank+1) Kz/2) for the
+// y transforms and padded rows [rank My/2, (rank+1) My/2) for the z stage:
+//   1. inverse y FFT (Ny -> My, zero padded) of the six fields of its
+//      columns into Ys[f][y][col] (own shared memory);
+//   2. per pair of its rows: the six half spectra along z, half of them read
+//      from the peer's Ys, inverse real z FFTs, base flow, -(u x omega),
+//      forward real z FFTs -> Hs[f][row][kz] (own shared memory, kz XOR
+//      swizzled by row when Kz is a multiple of 8);
+//   3. forward y FFT (My -> Ny, truncation, Nyquist zeroed) of the three
+//      fields of its columns, rows read from both CTAs' Hs, into HX.
+// Cluster barriers separate the stages and keep each CTA's shared memory
+// alive until the peer has finished reading it.
+// ---------------------------------------------------------------------------
+constexpr int kPlaneThreads = 512;
+
+__host__ __device__ inline size_t plane_smem_bytes(int My, int Kz, size_t elem) {
+  return (size_t)6 * My * (Kz / 2 + 1) * elem + (size_t)3 * (My / 2) * Kz * elem;
+}
+
+template <int PY, int PZ, int QK, typename T>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
+    plane_cross_kernel(DevOps o, Dims d, const cpx<T>* __restrict__ twy,
+                       const cpx<T>* __restrict__ twz, const cpx<T>* __restrict__ X,
+                       cpx<T>* __restrict__ HX) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int MY = 32 * PY, MH = MY / 2, MZ = 32 * PZ;
+  const int rank = (int)cluster.block_rank();
+  const int j = blockIdx.x >> 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int NW = kPlaneThreads / 32;
+  const int Kz = d.Kz, KH = Kz / 2, LDZ = KH + 1;
+  const bool swz = (Kz & 7) == 0;
+  cpx<T>* Ys = reinterpret_cast<cpx<T>*>(smem_raw);  // [6][MY][LDZ]
+  cpx<T>* Hs = Ys + (size_t)6 * MY * LDZ;              // [3][MH][Kz]
+  const cpx<T>* Ypeer = cluster.map_shared_rank(Ys, rank ^ 1);
+  const cpx<T>* Hpeer = cluster.map_shared_rank(Hs, rank ^ 1);
+  const size_t P = (size_t)d.P;
+  const int half = d.Ny / 2;
+  const int br = bitrev5(lane);
+
+  // 1. inverse y transforms of this CTA's columns
+  {
+    WarpTw<PY, T> w;
+    load_warp_tw<PY, T>(w, twy, lane);
+    for (int t = warp; t < 6 * KH; t += NW) {
+      const int f = t / KH, cl = t % KH, kz = rank * KH + cl;
+      const cpx<T>* src = X + ((size_t)f * d.Nx + j) * P + kz;
+      cpx<T> v[PY];
+#pragma unroll
+      for (int r = 0; r < PY; ++r) {
+        const int k = 32 * r + lane;
+        cpx<T> z = cmk(T(0), T(0));
+        if (k < half) z = src[(size_t)k * Kz];
+        else if (k >= MY - half) z = src[(size_t)(k - MY + d.Ny) * Kz];
+        v[r] = z;
+      }
+      warp_fft_inverse<PY, T>(v, w, lane);
+#pragma unroll
+      for (int k1 = 0; k1 < PY; ++k1) Ys[((size_t)f * MY + k1 + PY * br) * LDZ + cl] = v[k1];
+    }
+  }
+  cluster.sync();
+
+  // 2. z stage on this CTA's rows, two rows per warp
+  {
+    WarpTw<PZ, T> w;
+    load_warp_tw<PZ, T>(w, twz, lane);
+    const T ub = T(d.uwall * o.xphys[j]), uw = T(d.uwall);
+    const T scale = T(1.0 / MZ);
+    for (int pair = warp; pair < MH / 2; pair += NW) {
+      T nrm[2][3][PZ];
+#pragma unroll
+      for (int rb = 0; rb < 2; ++rb) {
+        const int y = rank * MH + 2 * pair + rb;
+        cpx<T> ph[3][PZ];
+#pragma unroll
+        for (int pr = 0; pr < 3; ++pr) {
+          cpx<T> A[QK], B[QK];
+#pragma unroll
+          for (int q = 0; q < QK; ++q) {
+            const int kz = 32 * q + lane;
+            A[q] = B[q] = cmk(T(0), T(0));
+            if (kz < Kz) {
+              const int own = kz / KH, cl = kz - own * KH;
+              const cpx<T>* base = (own == rank) ? Ys : Ypeer;
+              A[q] = base[((size_t)(2 * pr) * MY + y) * LDZ + cl];
+              B[q] = base[((size_t)(2 * pr + 1) * MY + y) * LDZ + cl];
+            }
+          }
+          build_packed<PZ, QK, T>(A, B, Kz, lane, ph[pr]);
+          warp_fft_inverse<PZ, T>(ph[pr], w, lane);
+        }
+#pragma unroll
+        for (int r = 0; r < PZ; ++r) {
+          rotational_product(ph[0][r].re, ph[0][r].im, ph[1][r].re, ph[1][r].im, ph[2][r].re,
+                             ph[2][r].im, ub, uw, nrm[rb][0][r], nrm[rb][1][r], nrm[rb][2][r]);
+        }
+      }
+      cpx<T> F0[PZ], F1[PZ], F2[PZ];
+#pragma unroll
+      for (int r = 0; r < PZ; ++r) {
+        F0[r] = cmk(nrm[0][0][r], nrm[0][1][r]);
+        F1[r] = cmk(nrm[1][0][r], nrm[1][1][r]);
+        F2[r] = cmk(nrm[0][2][r], nrm[1][2][r]);
+      }
+      warp_fft_forward<PZ, T>(F0, w, lane);
+      warp_fft_forward<PZ, T>(F1, w, lane);
+      warp_fft_forward<PZ, T>(F2, w, lane);
+      cpx<T> xa0[QK], xa1[QK], xb0[QK], xb1[QK], x2a[QK], x2b[QK];
+      unpack_pair<PZ, QK, T>(F0, lane, xa0, xa1);
+      unpack_pair<PZ, QK, T>(F1, lane, xb0, xb1);
+      unpack_pair<PZ, QK, T>(F2, lane, x2a, x2b);
+      const int ya = 2 * pair, yb = ya + 1;  // local rows
+#pragma unroll
+      for (int q = 0; q < QK; ++q) {
+        const int kz = 32 * q + lane;
+        if (kz >= Kz) continue;
+        const int ca = swz ? (kz ^ (ya & 7)) : kz, cb = swz ? (kz ^ (yb & 7)) : kz;
+        Hs[((size_t)0 * MH + ya) * Kz + ca] = scale * xa0[q];
+        Hs[((size_t)1 * MH + ya) * Kz + ca] = scale * xa1[q];
+        Hs[((size_t)2 * MH + ya) * Kz + ca] = scale * x2a[q];
+        Hs[((size_t)0 * MH + yb) * Kz + cb] = scale * xb0[q];
+        Hs[((size_t)1 * MH + yb) * Kz + cb] = scale * xb1[q];
+        Hs[((size_t)2 * MH + yb) * Kz + cb] = scale * x2b[q];
+      }
+    }
+  }
+  cluster.sync();
+
+  // 3. forward y transforms of this CTA's columns
+  {
+    WarpTw<PY, T> w;
+    load_warp_tw<PY, T>(w, twy, lane);
+    const T scale = T(1.0 / MY);
+    for (int t = warp; t < 3 * KH; t += NW) {
+      const int f = t / KH, cl = t % KH, kz = rank * KH + cl;
+      cpx<T> v[PY];
+#pragma unroll
+      for (int n1 = 0; n1 < PY; ++n1) {
+        const int y = n1 + PY * br;
+        const int own = y / MH, yl = y - own * MH;
+        const cpx<T>* base = (own == rank) ? Hs : Hpeer;
+        v[n1] = base[((size_t)f * MH + yl) * Kz + (swz ? (kz ^ (yl & 7)) : kz)];
+      }
+      warp_fft_forward<PY, T>(v, w, lane);
+      cpx<T>* dst = HX + ((size_t)f * d.Nx + j) * P + kz;
+#pragma unroll
+      for (int k1 = 0; k1 < PY; ++k1) {
+        const int k = 32 * k1 + lane;
+        if (k < half) {
+          cpx<T> val = scale * v[k1];
+          if (f == 0 && kz == 0 && k == 0) val.re += T(-d.uwall * o.xphys[j] * d.uwall);
+          dst[(size_t)k * Kz] = val;
+        } else if (k > MY - half) {
+          dst[(size_t)(k - MY + d.Ny) * Kz] = scale * v[k1];
+        }
+        else if (k == MY - half) dst[(size_t)half * Kz] = cmk(T(0), T(0));  // Nyquist
+      }
+    }
+  }
+  cluster.sync();
 }
 
 }  // namespace jfb

@@ -169,3 +169,71 @@ def test_tensor_core_and_warp_pencil_kernels_agree(cuda, N, monkeypatch):
     a, b = g1.solve(s0, 12), g2.solve(s0, 12)
     for x, y in zip((*a.u, a.g), (*b.u, b.g), strict=True):
         assert rel(x, y.cpu().numpy()) < 1e-12
+
+
+@pytest.mark.parametrize("N", [(65, 64, 64), (33, 64, 64)])
+def test_fused_and_split_periodic_transforms_agree(cuda, N, monkeypatch):
+    """The one-launch plane transforms (CTA pair per x-plane) and the three
+    separate transform launches give the same steps."""
+    g1 = PlaneCouetteFluctuation(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02,
+                                 device=cuda)
+    assert g1.info().launches_per_step == 2
+    monkeypatch.setenv("JFB200_TRANSFORMS", "split")
+    g2 = PlaneCouetteFluctuation(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02,
+                                 device=cuda)
+    assert g2.info().launches_per_step == 4
+    s0 = g1.initial_state()
+    a, b = g1.solve(s0, 12), g2.solve(s0, 12)
+    for x, y in zip((*a.u, a.g), (*b.u, b.g), strict=True):
+        assert rel(x, y.cpu().numpy()) < 1e-12
+
+
+def test_plans_of_different_sizes_and_precisions_coexist(cuda):
+    """Building a smaller or mixed-precision plan after a larger one must not
+    break the larger plan's launches (kernel attributes are process-wide)."""
+    big = PlaneCouetteFluctuation(N=(65, 64, 64), Re=400.0, dt=1e-3, perturbation_amplitude=0.02,
+                                  device=cuda)
+    ref = big.solve(big.initial_state(), 3)
+    PlaneCouetteFluctuation(N=(33, 32, 32), precision="mixed", device=cuda)
+    PlaneCouetteFluctuation(N=(17, 16, 16), device=cuda)
+    again = big.solve(big.initial_state(), 3)
+    for x, y in zip((*again.u, again.g), (*ref.u, ref.g), strict=True):
+        assert torch.equal(x, y)
+
+
+def _seeded_pair(N, cuda):
+    import math
+
+    from jaxfun_b200.workloads import couette_perturbation_fields, scale_to_energy
+    dom = ((-1.0, 1.0), (0.0, 4.0 * math.pi), (0.0, 2.0 * math.pi))
+    g64 = PlaneCouetteFluctuation(N=N, domain=dom, Re=1000.0, dt=0.01, device=cuda)
+    g32 = PlaneCouetteFluctuation(N=N, domain=dom, Re=1000.0, dt=0.01, precision="mixed",
+                                  device=cuda)
+    f = couette_perturbation_fields(N, dom)
+    f = scale_to_energy(f, g64.diagnostics(g64.state_from_physical(f))["Epert"], 1e-4)
+    return g64, g32, g64.state_from_physical(f), g32.state_from_physical(f)
+
+
+def test_mixed_form_tracks_fp64(cuda):
+    """Mixed form (complex64 transforms and products, FP64 Shen operators and
+    solves) against the FP64 form on the seeded 65x64x64 Couette workload.
+    Measured: <= 3.3e-7 per field after 100 steps, <= 1.6e-6 after 1000."""
+    g64, g32, s64, s32 = _seeded_pair((65, 64, 64), cuda)
+    for x, y in zip((*s32.u, s32.g), (*s64.u, s64.g), strict=True):
+        assert torch.equal(x, y)  # the projection of the initial field is FP64 in both
+    done = 0
+    for n, tol in ((100, 1e-6), (1000, 5e-6)):
+        s64, s32 = g64.solve(s64, n - done), g32.solve(s32, n - done)
+        done = n
+        for x, y in zip((*s32.u, s32.g), (*s64.u, s64.g), strict=True):
+            assert rel(x, y.cpu().numpy()) < tol, n
+
+
+@pytest.mark.parametrize("N", [(17, 16, 16), (33, 32, 32)])
+def test_mixed_form_against_oracle(cuda, N):
+    o = PlaneCouetteOracle(N=N, Re=400.0, dt=1e-3, perturbation_amplitude=0.05)
+    g = PlaneCouetteFluctuation(N=N, Re=400.0, dt=1e-3, perturbation_amplitude=0.05,
+                                precision="mixed", device=cuda)
+    st, gs = o.solve(o.initial_state(), 6), g.solve(g.initial_state(), 6)
+    for a, b in zip((*gs.u, gs.g), (*st.u, st.g), strict=True):
+        assert rel(a, b) < 1e-6
