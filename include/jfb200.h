@@ -195,6 +195,55 @@ int jfb_kmm_timed_steps(jfb_kmm_plan* plan, int64_t steps, void* flush_buf,
                         int64_t flush_bytes, double* kernel_ms, double* step_ms,
                         void* stream);
 
+/* ---- plane-Couette MHD (vector potential, conducting walls) ------------- */
+
+/* Device pointers to an MHDState (examples/pcf_mhd_jax.py:34-66): the flow
+ * KMMState and the vector potential A in the Dirichlet basis, three
+ * (nx-2, ny, nz) complex128 components per level, with its SBDF3 history
+ * (the mass rows of the EMF and the two previous A levels). */
+typedef struct jfb_mhd_state {
+  jfb_kmm_state flow;
+  void* A[3];
+  void* nonlinear_A_old[3];
+  void* nonlinear_A_older[3];
+  void* A_old[3];
+  void* A_older[3];
+} jfb_mhd_state;
+
+/* PlaneCouetteMHDJax.__init__ + _build_A_operators (pcf_mhd_jax.py:76-143):
+ * the flow plan of jfb_kmm_create plus the A systems MA - gamma LA with
+ * eta = u_wall / rm (steady SBDF3 and the three IMEXRK3 startup stages).
+ * FP64 only (JFB_ERR_ARG for JFB_PRECISION_MIXED).  All other jfb_kmm_*
+ * entry points accept the plan; jfb_kmm_advance / jfb_kmm_timed_steps then
+ * advance the coupled flow + A system (_step_sbdf3_mhd, pcf_mhd_jax.py:
+ * 563-715; Lorentz force in the momentum nonlinear term, EMF in the A
+ * equation) and jfb_kmm_convection returns H with the Lorentz force. */
+int jfb_mhd_create(const jfb_kmm_config* cfg, double rm, jfb_kmm_plan** plan);
+
+/* Load / store the full MHDState; the flow part as jfb_kmm_set_state /
+ * jfb_kmm_get_state.  NULL A-history pointers load zeros (get: skipped). */
+int jfb_mhd_set_state(jfb_kmm_plan* plan, const jfb_mhd_state* state, void* stream);
+int jfb_mhd_get_state(jfb_kmm_plan* plan, const jfb_mhd_state* state, void* stream);
+
+/* _A_state_from_physical (pcf_mhd_jax.py:210-215): TD.forward (Nyquist
+ * masked) of real float64 samples (nx, ny, nz) of the three components of A,
+ * written to a0, a1, a2 ((nx-2, ny, nz) complex128).  The loaded state is
+ * unchanged. */
+int jfb_mhd_potential_from_physical(jfb_kmm_plan* plan, const double* ax, const double* ay,
+                                    const double* az, void* a0, void* a1, void* a2,
+                                    void* stream);
+
+/* _mhd_convection (pcf_mhd_jax.py:339-357) of the loaded state: H (the TD
+ * forward of -(u_t x omega_t) - J x B) and HA (the TD forward of
+ * (u + U_b e_y) x B), six (nx-2, ny, nz) complex128 fields. */
+int jfb_mhd_convection(jfb_kmm_plan* plan, void* h0, void* h1, void* h2, void* ha0,
+                       void* ha1, void* ha2, void* stream);
+
+/* PlaneCouetteMHDJax.diagnostics (pcf_mhd_jax.py:776-790) of the loaded
+ * state: device array out[10] = the eight values of jfb_kmm_diagnostics,
+ * then divB_L2 and Emag. */
+int jfb_mhd_diagnostics(jfb_kmm_plan* plan, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

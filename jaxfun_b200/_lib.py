@@ -65,6 +65,19 @@ class KMMStateC(ctypes.Structure):
     ]
 
 
+class MHDStateC(ctypes.Structure):
+    """``jfb_mhd_state``: device pointers of an MHDState in the reference layout."""
+
+    _fields_ = [
+        ("flow", KMMStateC),
+        ("A", c_void_p * 3),
+        ("nonlinear_A_old", c_void_p * 3),
+        ("nonlinear_A_older", c_void_p * 3),
+        ("A_old", c_void_p * 3),
+        ("A_older", c_void_p * 3),
+    ]
+
+
 class KMMInfo(ctypes.Structure):
     _fields_ = [
         ("n_pencils", c_int64),
@@ -111,6 +124,16 @@ SIGNATURES = {
         c_int,
         [c_void_p, c_int64, c_void_p, c_int64, POINTER(c_double), POINTER(c_double), c_void_p],
     ),
+    "jfb_mhd_create": (c_int, [POINTER(KMMConfig), c_double, POINTER(c_void_p)]),
+    "jfb_mhd_set_state": (c_int, [c_void_p, POINTER(MHDStateC), c_void_p]),
+    "jfb_mhd_get_state": (c_int, [c_void_p, POINTER(MHDStateC), c_void_p]),
+    "jfb_mhd_potential_from_physical": (
+        c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+    ),
+    "jfb_mhd_convection": (
+        c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
+    ),
+    "jfb_mhd_diagnostics": (c_int, [c_void_p, c_void_p, c_void_p]),
 }
 
 _lib = None

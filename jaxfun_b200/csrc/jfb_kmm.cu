@@ -16,6 +16,7 @@
 #include "jfb_kmm_kernels.cuh"
 #include "jfb_kmm_warpk.cuh"
 #include "jfb_kmm_gemm.cuh"
+#include "jfb_kmm_mhd.cuh"
 
 namespace jfb {
 
@@ -231,6 +232,14 @@ struct jfb_kmm_plan {
   size_t smem_plane = 0;
   jfb::GemmOps gops;
   size_t smem_gemm = 0;
+  // MHD (vector potential A, three Dirichlet components per level)
+  bool mhd = false;
+  double eta = 0.0;
+  jfb::MhdOps mops;
+  double *sa_steady = nullptr, *sa_startup[3] = {nullptr, nullptr, nullptr};
+  jfb::c64 *AR[3], *NA[3], *NAst;
+  size_t smem_mhd = 0, smem_zm = 0;
+  double* mdiag_partial = nullptr;
 };
 
 namespace jfb {
@@ -280,9 +289,14 @@ static std::vector<c64> twiddles(int n) {
 
 // Build, factor and pack the per-wavenumber systems for implicit coefficient
 // gamma (tpmatrix.py:1900-2029 assembly, 1105-1149 batched LU).
-static int build_factor_set(jfb_kmm_plan* pl, double gamma, FactorSet& fs) {
+// Systems sys_first..sys_last (0: Su, 1: Sg, 2: S00) with diffusivity nu;
+// inv selects the explicit inverse-factor records (always used by the
+// tensor-core pencil stage and the A solves).
+static int build_factor_set(jfb_kmm_plan* pl, double gamma, FactorSet& fs, double nu,
+                            int sys_first, int sys_last, bool inv) {
   const HostOperators& op = pl->hop;
-  const jfb_kmm_config& cfg = pl->cfg;
+  jfb_kmm_config cfg = pl->cfg;
+  cfg.nu = nu;
   const Dims& d = pl->d;
   const int nm = pl->n_modes;
   int st;
@@ -294,7 +308,7 @@ static int build_factor_set(jfb_kmm_plan* pl, double gamma, FactorSet& fs) {
     cudaFree(dcoef);
     cudaFree(dband);
   };
-  for (int sys = 0; sys < 3; ++sys) {
+  for (int sys = sys_first; sys <= sys_last; ++sys) {
     // sys 0: Su (biharmonic basis), 1: Sg (Dirichlet), 2: S00 (1-D Dirichlet)
     const bool bih = sys == 0;
     const int n = bih ? d.nB : d.nD;
@@ -344,7 +358,7 @@ static int build_factor_set(jfb_kmm_plan* pl, double gamma, FactorSet& fs) {
     double** dst = (sys == 0) ? &fs.su : (sys == 1) ? &fs.sg : &fs.s00;
     st = dalloc(pl, (void**)dst, (size_t)modes * packed_rec_size(n) * sizeof(double));
     if (st) return cleanup(), st;
-    if (pl->gemm) {
+    if (inv) {
       JFB_REQUIRE(n <= 2 * kMaxHalfInv, "system too large for the inverse-factor records");
       pack_factor_inv_kernel<<<modes, 64>>>(dband, modes, n, p, q, *dst);
     } else {
@@ -575,8 +589,51 @@ static int launch_transforms_t(jfb_kmm_plan* pl, cudaStream_t s) {
   return JFB_OK;
 }
 
+// The coupled MHD step: twelve fields (u, omega, b, j) backward in y, the z
+// stage with the Lorentz force and the EMF, six fields (n, emf) forward in y.
+static int launch_transforms_mhd(jfb_kmm_plan* pl, cudaStream_t s) {
+  const Dims& d = pl->d;
+  dim3 gy(d.Nx, 12, d.Kz / pl->KC);
+  y_backward_kernel<double><<<gy, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->X, pl->Y);
+  JFB_CHECK_LAUNCH();
+  if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[2], s));
+  const int zb = ceil_div((int64_t)d.Nx * d.My, kZRows);
+  z_cross_mhd_kernel<<<zb, 256, pl->smem_zm, s>>>(pl->ops, d, pl->fz, pl->twz, pl->Y, pl->HZ);
+  JFB_CHECK_LAUNCH();
+  if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[3], s));
+  dim3 gf(d.Nx, 6, d.Kz / pl->KC);
+  y_forward_kernel<double><<<gf, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->HZ, pl->HX,
+                                                       pl->ops.xphys);
+  JFB_CHECK_LAUNCH();
+  if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[4], s));
+  return JFB_OK;
+}
+
 static int launch_transforms(jfb_kmm_plan* pl, cudaStream_t s) {
+  if (pl->mhd) return launch_transforms_mhd(pl, s);
   return pl->mixed ? launch_transforms_t<float>(pl, s) : launch_transforms_t<double>(pl, s);
+}
+
+static MhdArgs blank_mhd() {
+  MhdArgs a;
+  std::memset(&a, 0, sizeof(a));
+  return a;
+}
+
+static int launch_mhd(jfb_kmm_plan* pl, const MhdArgs& a, cudaStream_t s) {
+  const int blocks = (pl->d.Ny / 2) * ceil_div(pl->d.Kz, 8);
+  mhd_a_kernel<<<blocks, kMhdThreads, pl->smem_mhd, s>>>(pl->d, pl->ops, pl->mops, a);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+// x-physical b and j of A (ring slot c) into X fields 6..11.
+static int mhd_fields(jfb_kmm_plan* pl, int c, cudaStream_t s) {
+  MhdArgs m = blank_mhd();
+  m.mode = kMhdFields;
+  m.Aa = pl->AR[c];
+  m.XB = pl->X + (size_t)6 * pl->d.Nx * pl->d.P;
+  return launch_mhd(pl, m, s);
 }
 
 static inline int slot(int64_t m) { return (int)(((m % 3) + 3) % 3); }
@@ -612,6 +669,7 @@ static int ensure_H(jfb_kmm_plan* pl, cudaStream_t s) {
   a.X = pl->X;
   st = launch_pencil(pl, a, s);
   if (st) return st;
+  if (pl->mhd && (st = mhd_fields(pl, c, s))) return st;
   st = launch_transforms(pl, s);
   if (st) return st;
   pl->have_H = true;
@@ -656,6 +714,28 @@ static int steady_step(jfb_kmm_plan* pl, int64_t m, cudaStream_t s) {
   a.X = pl->X;
   int st = launch_implicit(pl, a, s);
   if (st) return st;
+  if (pl->mhd) {
+    MhdArgs m = blank_mhd();
+    m.mode = kMhdStep;
+    m.HXA = pl->HX + (size_t)3 * pl->d.Nx * pl->d.P;
+    m.c0 = a.c0;
+    m.c1 = a.c1;
+    m.c2 = a.c2;
+    m.d0 = a.d0;
+    m.d1 = a.d1;
+    m.d2 = a.d2;
+    m.Aa = pl->AR[c];
+    m.Ab = pl->AR[o1];
+    m.Ac = pl->AR[o2];
+    m.NAp = pl->NA[o1];
+    m.NAq = pl->NA[o2];
+    m.NA_out = pl->NA[c];
+    m.sa = pl->sa_steady;
+    m.sa_rec = pl->sg_rec;
+    m.A_out = pl->AR[nw];
+    m.XB = pl->X + (size_t)6 * pl->d.Nx * pl->d.P;
+    if ((st = launch_mhd(pl, m, s))) return st;
+  }
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[1], s));
   return launch_transforms(pl, s);
 }
@@ -710,6 +790,25 @@ static int startup_step(jfb_kmm_plan* pl, cudaStream_t s) {
     a.X = pl->X;
     int st = launch_implicit(pl, a, s);
     if (st) return st;
+    if (pl->mhd) {
+      MhdArgs m = blank_mhd();
+      m.mode = kMhdStep;
+      m.HXA = pl->HX + (size_t)3 * pl->d.Nx * pl->d.P;
+      m.c0 = 1.0;
+      m.slin = a.cL * pl->eta;
+      m.d0 = kRK3A[rk];
+      m.d1 = kRK3B[rk];
+      m.Aa = pl->AR[src];
+      if (rk == 1) m.NAp = pl->NA[c];
+      else if (rk == 2) m.NAp = pl->NAst;
+      if (rk == 0) m.NA_out = pl->NA[c];
+      else if (rk == 1) m.NA_out = pl->NAst;
+      m.sa = pl->sa_startup[rk];
+      m.sa_rec = pl->sg_rec;
+      m.A_out = pl->AR[nw];
+      m.XB = pl->X + (size_t)6 * pl->d.Nx * pl->d.P;
+      if ((st = launch_mhd(pl, m, s))) return st;
+    }
     st = launch_transforms(pl, s);
     if (st) return st;
   }
@@ -728,7 +827,7 @@ static void destroy_graphs(jfb_kmm_plan* pl) {
 
 using namespace jfb;
 
-extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
+static int create_plan(const jfb_kmm_config* cfg, bool mhd, double rm, jfb_kmm_plan** out) {
   JFB_REQUIRE(cfg && out, "null pointer");
   *out = nullptr;
   JFB_REQUIRE(cfg->family == JFB_FAMILY_CHEBYSHEV, "only the Chebyshev family is supported");
@@ -743,6 +842,8 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   JFB_REQUIRE(cfg->x_hi > cfg->x_lo && cfg->ly > 0 && cfg->lz > 0, "bad domain");
   jfb_kmm_plan* pl = new jfb_kmm_plan();
   pl->cfg = *cfg;
+  pl->mhd = mhd;
+  pl->eta = mhd ? cfg->u_wall / rm : 0.0;
   int st = JFB_OK;
   auto fail = [&](int code) {
     jfb_kmm_destroy(pl);
@@ -800,6 +901,21 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   {
     const char* ev = std::getenv("JFB200_TRANSFORMS");
     if (ev && std::string(ev) == "split") pl->plane = false;
+  }
+  if (pl->mhd) {
+    // the coupled step transforms twelve fields with the shared-memory kernels
+    pl->plane = false;
+    pl->smem_mhd = mhd_smem_bytes(d.nD);
+    pl->smem_zm = (size_t)2 * d.Mz * kZRows * 6 * sizeof(c64);
+    if (pl->smem_mhd > 227 * 1024 || pl->smem_zm > 227 * 1024) {
+      set_error("grid too large for the MHD shared-memory tiling");
+      return fail(JFB_ERR_ARG);
+    }
+    if (allow_smem((const void*)mhd_a_kernel) != cudaSuccess ||
+        allow_smem((const void*)z_cross_mhd_kernel) != cudaSuccess) {
+      set_error("cannot configure the MHD kernels");
+      return fail(JFB_ERR_CUDA);
+    }
   }
   if (pl->plane) {
     auto attr = [&](const void* fn) { return allow_smem(fn); };
@@ -1000,15 +1116,54 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
     }
   }
 
+  if (pl->mhd) {
+    GemmHost gh;
+    std::string err;
+    if (!build_gemm_operators(pl->hop, gh, err)) {
+      set_error(err);
+      return fail(JFB_ERR_ARG);
+    }
+    MhdOps& M = pl->mops;
+    double* q;
+#define UPM(field, vec)                    \
+    if ((st = upload(pl, &q, vec))) return fail(st); \
+    M.field = q;
+    UPM(R3, gh.R3);
+    UPM(X2D, gh.X2D);
+    UPM(B1, gh.B1);
+    UPM(B2, gh.B2);
+    UPM(C1, gh.C1);
+    UPM(C2, gh.C2);
+#undef UPM
+    M.Jh = (d.Nx + 1) / 2;
+    M.Jl = d.Nx / 2;
+    M.nDe = (d.nD + 1) / 2;
+    M.nDo = d.nD / 2;
+  }
+
   // factors: steady SBDF3 and the three IMEXRK3 startup stages
   pl->n_modes = (d.Ny / 2) * d.Kz;
   pl->su_rec = packed_rec_size(d.nB);
   pl->sg_rec = packed_rec_size(d.nD);
-  st = build_factor_set(pl, kSBDF3Implicit * cfg->dt, pl->steady);
+  st = build_factor_set(pl, kSBDF3Implicit * cfg->dt, pl->steady, cfg->nu, 0, 2, pl->gemm);
   if (st) return fail(st);
   for (int rk = 0; rk < 3; ++rk) {
-    st = build_factor_set(pl, (kRK3A[rk] + kRK3B[rk]) * cfg->dt / 2.0, pl->startup[rk]);
+    st = build_factor_set(pl, (kRK3A[rk] + kRK3B[rk]) * cfg->dt / 2.0, pl->startup[rk],
+                          cfg->nu, 0, 2, pl->gemm);
     if (st) return fail(st);
+  }
+  if (pl->mhd) {
+    // SA = MA - gamma LA: the Sg structure with diffusivity eta
+    FactorSet fs;
+    st = build_factor_set(pl, kSBDF3Implicit * cfg->dt, fs, pl->eta, 1, 1, true);
+    if (st) return fail(st);
+    pl->sa_steady = fs.sg;
+    for (int rk = 0; rk < 3; ++rk) {
+      FactorSet fr;
+      st = build_factor_set(pl, (kRK3A[rk] + kRK3B[rk]) * cfg->dt / 2.0, fr, pl->eta, 1, 1, true);
+      if (st) return fail(st);
+      pl->sa_startup[rk] = fr.sg;
+    }
   }
 
   // state rings and work buffers
@@ -1031,20 +1186,45 @@ extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
   if ((st = cal(&pl->U2S, (size_t)d.nD * P))) return fail(st);
   // X and Y exist only for the step: half size in the mixed form (complex64);
   // HZ and HX also serve the FP64 state_from_physical path
+  // (the coupled MHD step: twelve x-physical fields u, omega, b, j and six
+  // nonlinear fields n, emf)
   const size_t xs = pl->mixed ? 2 : 1;
-  if ((st = cal(&pl->X, ((size_t)6 * d.Nx * P + xs - 1) / xs))) return fail(st);
-  if ((st = cal(&pl->Y, ((size_t)6 * d.Nx * d.My * d.Kz + xs - 1) / xs))) return fail(st);
-  if ((st = cal(&pl->HZ, (size_t)3 * d.Nx * d.My * d.Kz))) return fail(st);
-  if ((st = cal(&pl->HX, (size_t)3 * d.Nx * P))) return fail(st);
+  const size_t nxf = pl->mhd ? 12 : 6, nhf = pl->mhd ? 6 : 3;
+  if ((st = cal(&pl->X, (nxf * d.Nx * P + xs - 1) / xs))) return fail(st);
+  if ((st = cal(&pl->Y, (nxf * d.Nx * d.My * d.Kz + xs - 1) / xs))) return fail(st);
+  if ((st = cal(&pl->HZ, nhf * d.Nx * d.My * d.Kz))) return fail(st);
+  if ((st = cal(&pl->HX, nhf * d.Nx * P))) return fail(st);
+  if (pl->mhd) {
+    for (int k = 0; k < 3; ++k) {
+      if ((st = cal(&pl->AR[k], (size_t)3 * d.nD * P))) return fail(st);
+      if ((st = cal(&pl->NA[k], (size_t)3 * d.nD * P))) return fail(st);
+    }
+    if ((st = cal(&pl->NAst, (size_t)3 * d.nD * P))) return fail(st);
+  }
   if ((st = cal(&pl->HD, (size_t)3 * d.nD * P))) return fail(st);
   pl->diag_blocks = d.Ny * d.nKb;
   if ((st = dalloc(pl, (void**)&pl->diag_partial, (size_t)2 * pl->diag_blocks * sizeof(double))))
     return fail(st);
   if ((st = dalloc(pl, (void**)&pl->diag_mean, (size_t)(8 + d.Nx) * sizeof(double))))
     return fail(st);
+  if (pl->mhd &&
+      (st = dalloc(pl, (void**)&pl->mdiag_partial, (size_t)2 * pl->diag_blocks * sizeof(double))))
+    return fail(st);
   JFB_CHECK_CUDA(cudaDeviceSynchronize());
   *out = pl;
   return JFB_OK;
+}
+
+extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
+  return create_plan(cfg, false, 0.0, out);
+}
+
+extern "C" int jfb_mhd_create(const jfb_kmm_config* cfg, double rm, jfb_kmm_plan** out) {
+  JFB_REQUIRE(cfg && out, "null pointer");
+  *out = nullptr;
+  JFB_REQUIRE(rm > 0.0 && std::isfinite(rm), "rm must be positive");
+  JFB_REQUIRE(cfg->precision == JFB_PRECISION_FP64, "the MHD step runs in FP64 only");
+  return create_plan(cfg, true, rm, out);
 }
 
 extern "C" int jfb_kmm_destroy(jfb_kmm_plan* pl) {
@@ -1061,7 +1241,7 @@ extern "C" int jfb_kmm_get_info(const jfb_kmm_plan* pl, jfb_kmm_info* info) {
   const Dims& d = pl->d;
   info->n_pencils = d.P;
   info->device_bytes = pl->device_bytes;
-  info->launches_per_step = pl->plane ? 2 : 4;
+  info->launches_per_step = pl->mhd ? 5 : pl->plane ? 2 : 4;
   // stage model: 43 E_s + 18 E_m complex values, E_s = Nx Ny (Nz/2+1), E_m = Nx My (Nz/2+1)
   const int64_t H = d.Nz / 2 + 1;
   const int64_t Es = (int64_t)d.Nx * d.Ny * H, Em = (int64_t)d.Nx * d.My * H;
@@ -1254,6 +1434,10 @@ extern "C" int jfb_kmm_state_from_physical(jfb_kmm_plan* pl, const double* u0,
     JFB_CHECK_CUDA(cudaMemsetAsync(pl->NG[k], 0, (size_t)d.nD * P * sizeof(c64), s));
     JFB_CHECK_CUDA(cudaMemsetAsync(pl->VW[k], 0, (size_t)d.nD * sizeof(c64), s));
     JFB_CHECK_CUDA(cudaMemsetAsync(pl->NVW[k], 0, (size_t)d.nD * sizeof(c64), s));
+    if (pl->mhd) {
+      JFB_CHECK_CUDA(cudaMemsetAsync(pl->AR[k], 0, (size_t)3 * d.nD * P * sizeof(c64), s));
+      JFB_CHECK_CUDA(cudaMemsetAsync(pl->NA[k], 0, (size_t)3 * d.nD * P * sizeof(c64), s));
+    }
   }
   StageArgs a = blank_args();
   a.mode = kFromPhys;
@@ -1337,5 +1521,144 @@ extern "C" int jfb_kmm_timed_steps(jfb_kmm_plan* pl, int64_t steps, void* flush_
     pl->explicit_u12 = false;
   }
   for (int k = 0; k < 5; ++k) cudaEventDestroy(ev[k]);
+  return JFB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// MHD entry points
+// ---------------------------------------------------------------------------
+
+extern "C" int jfb_mhd_set_state(jfb_kmm_plan* pl, const jfb_mhd_state* s, void* stream) {
+  JFB_REQUIRE(pl && s, "null pointer");
+  JFB_REQUIRE(pl->mhd, "not an MHD plan");
+  JFB_REQUIRE(s->A[0] && s->A[1] && s->A[2], "null pointer");
+  int st = jfb_kmm_set_state(pl, &s->flow, stream);
+  if (st) return st;
+  cudaStream_t cs = (cudaStream_t)stream;
+  const Dims& d = pl->d;
+  const size_t comp = (size_t)d.nD * d.P;
+  auto half3 = [&](void* const* full, c64* dst) {
+    for (int k = 0; k < 3; ++k) {
+      if (full && full[k])
+        to_half_kernel<<<512, 256, 0, cs>>>((const c64*)full[k], d.nD, d.Ny, d.Nz, dst + k * comp);
+      else
+        cudaMemsetAsync(dst + k * comp, 0, comp * sizeof(c64), cs);
+    }
+  };
+  half3(s->A, pl->AR[slot(0)]);
+  half3(s->A_old, pl->AR[slot(-1)]);
+  half3(s->A_older, pl->AR[slot(-2)]);
+  half3(s->nonlinear_A_old, pl->NA[slot(-1)]);
+  half3(s->nonlinear_A_older, pl->NA[slot(-2)]);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+extern "C" int jfb_mhd_get_state(jfb_kmm_plan* pl, const jfb_mhd_state* s, void* stream) {
+  JFB_REQUIRE(pl && s, "null pointer");
+  JFB_REQUIRE(pl->mhd, "not an MHD plan");
+  int st = jfb_kmm_get_state(pl, &s->flow, stream);
+  if (st) return st;
+  cudaStream_t cs = (cudaStream_t)stream;
+  const Dims& d = pl->d;
+  const size_t comp = (size_t)d.nD * d.P;
+  auto full3 = [&](const c64* src, void* const* dst) {
+    for (int k = 0; k < 3; ++k)
+      if (dst[k])
+        to_full_kernel<<<512, 256, 0, cs>>>(src + k * comp, d.nD, d.Ny, d.Nz, (c64*)dst[k]);
+  };
+  full3(pl->AR[slot(pl->n)], s->A);
+  full3(pl->AR[slot(pl->n - 1)], s->A_old);
+  full3(pl->AR[slot(pl->n - 2)], s->A_older);
+  full3(pl->NA[slot(pl->n - 1)], s->nonlinear_A_old);
+  full3(pl->NA[slot(pl->n - 2)], s->nonlinear_A_older);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+extern "C" int jfb_mhd_potential_from_physical(jfb_kmm_plan* pl, const double* ax,
+                                               const double* ay, const double* az, void* a0,
+                                               void* a1, void* a2, void* stream) {
+  JFB_REQUIRE(pl && ax && ay && az && a0 && a1 && a2, "null pointer");
+  JFB_REQUIRE(pl->mhd, "not an MHD plan");
+  cudaStream_t s = (cudaStream_t)stream;
+  Dims d = pl->d;
+  // z then y forward transforms of the three samples into HX (as in
+  // jfb_kmm_state_from_physical); HX then no longer holds the state's H
+  if (pl->pnz) {
+    switch (pl->pnz) {
+      case 2: launch_zfwd_warp<2>(pl, ax, ay, az, s); break;
+      case 3: launch_zfwd_warp<3>(pl, ax, ay, az, s); break;
+      case 4: launch_zfwd_warp<4>(pl, ax, ay, az, s); break;
+      default: launch_zfwd_warp<6>(pl, ax, ay, az, s); break;
+    }
+  } else {
+    const int zb = ceil_div((int64_t)d.Nx * d.Ny, kZRows);
+    z_forward_real_kernel<<<zb, 256, pl->smem_zf, s>>>(d, pl->fnz, pl->twnz, ax, ay, az, pl->HZ);
+  }
+  JFB_CHECK_LAUNCH();
+  Dims dy = d;
+  dy.My = d.Ny;
+  int KC = d.Kz;
+  while ((size_t)2 * d.Ny * KC * sizeof(c64) > 100 * 1024 && KC % 2 == 0) KC /= 2;
+  dim3 gf(d.Nx, 3, d.Kz / KC);
+  y_forward_kernel<double><<<gf, 256, (size_t)2 * d.Ny * KC * sizeof(c64), s>>>(
+      dy, pl->fny, KC, pl->twny, pl->HZ, pl->HX, nullptr);
+  JFB_CHECK_LAUNCH();
+  pl->have_H = false;
+  MhdArgs m = blank_mhd();
+  m.mode = kMhdFromPhys;
+  m.HXA = pl->HX;
+  m.A_out = pl->HD;
+  int st = launch_mhd(pl, m, s);
+  if (st) return st;
+  void* outs[3] = {a0, a1, a2};
+  for (int k = 0; k < 3; ++k)
+    to_full_kernel<<<512, 256, 0, s>>>(pl->HD + (size_t)k * d.nD * d.P, d.nD, d.Ny, d.Nz,
+                                       (c64*)outs[k]);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+extern "C" int jfb_mhd_convection(jfb_kmm_plan* pl, void* h0, void* h1, void* h2, void* ha0,
+                                  void* ha1, void* ha2, void* stream) {
+  JFB_REQUIRE(pl && h0 && h1 && h2 && ha0 && ha1 && ha2, "null pointer");
+  JFB_REQUIRE(pl->mhd, "not an MHD plan");
+  if (!pl->have_state) {
+    set_error("no state loaded");
+    return JFB_ERR_STATE;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = ensure_H(pl, s);
+  if (st) return st;
+  const Dims& d = pl->d;
+  void* outs[6] = {h0, h1, h2, ha0, ha1, ha2};
+  for (int half = 0; half < 2; ++half) {
+    StageArgs a = blank_args();
+    a.mode = kHOnly;
+    a.HX = pl->HX + (size_t)half * 3 * d.Nx * d.P;
+    a.Hd_out = pl->HD;
+    if ((st = launch_pencil(pl, a, s))) return st;
+    for (int f = 0; f < 3; ++f)
+      to_full_kernel<<<512, 256, 0, s>>>(pl->HD + (size_t)f * d.nD * d.P, d.nD, d.Ny, d.Nz,
+                                         (c64*)outs[3 * half + f]);
+    JFB_CHECK_LAUNCH();
+  }
+  return JFB_OK;
+}
+
+extern "C" int jfb_mhd_diagnostics(jfb_kmm_plan* pl, double* out, void* stream) {
+  JFB_REQUIRE(pl && out, "null pointer");
+  JFB_REQUIRE(pl->mhd, "not an MHD plan");
+  int st = jfb_kmm_diagnostics(pl, out, stream);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const Dims& d = pl->d;
+  mhd_diag_kernel<<<pl->diag_blocks, kNW * 32, 0, s>>>(pl->ops, d, pl->mops, pl->AR[slot(pl->n)],
+                                                       pl->mdiag_partial);
+  JFB_CHECK_LAUNCH();
+  mhd_diag_finish_kernel<<<1, 32, 0, s>>>(pl->mdiag_partial, pl->diag_blocks, pl->cfg.ly,
+                                          pl->cfg.lz, out + 8);
+  JFB_CHECK_LAUNCH();
   return JFB_OK;
 }

@@ -53,6 +53,10 @@ struct GemmHost {
   // B1 (even), B2 (odd), each padded to mid_stride
   std::vector<double> mid;
   int mid_stride = 0;
+  // MHD: x-physical values (N x nD, row-major) of a Dirichlet-basis field and
+  // of TD projections of its derivatives: B1 = V S_D^T, B2 = V D S_D^T,
+  // C1 = V S_D^T M_D^-1 S_D W D S_D^T, C2 = V S_D^T M_D^-1 S_D W D^2 S_D^T
+  std::vector<double> B1, B2, C1, C2;
 };
 
 Stencil make_stencil(int N, bool biharmonic);

@@ -493,6 +493,20 @@ bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& er
     for (int k = 0; k < nDo; ++k) gh.mid[4 * gh.mid_stride + k] = (double)B2(j, 2 * k + 1);
   }
 
+  {
+    const LMat WD2 = mul(WD, D);
+    const LMat C1 = mul(mul(mul(mul(V, SDt), MDi), mul(SD, WD)), SDt);
+    const LMat C2 = mul(mul(mul(mul(V, SDt), MDi), mul(SD, WD2)), SDt);
+    auto dense = [&](const LMat& M) {
+      std::vector<double> o((size_t)M.r * M.c);
+      for (size_t k = 0; k < o.size(); ++k) o[k] = (double)M.v[k];
+      return o;
+    };
+    gh.B1 = dense(B1);
+    gh.B2 = dense(B2);
+    gh.C1 = dense(C1);
+    gh.C2 = dense(C2);
+  }
   gh.R3.assign((size_t)nD * N, 0.0);
   for (int i = 0; i < nD; ++i)
     for (int j = 0; j < N; ++j) gh.R3[(size_t)i * N + j] = (double)R3(i, j);

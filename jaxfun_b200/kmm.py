@@ -133,9 +133,12 @@ class KMM:
         self._cfg = cfg
         handle = ctypes.c_void_p()
         with torch.cuda.device(self.device):
-            _lib.call("jfb_kmm_create", ctypes.byref(cfg), ctypes.byref(handle))
+            self._create_plan(cfg, handle)
         self._plan = handle
-        self._current = None  # the KMMState object the plan currently holds
+        self._current = None  # the state object the plan currently holds
+
+    def _create_plan(self, cfg: _lib.KMMConfig, handle: ctypes.c_void_p) -> None:
+        _lib.call("jfb_kmm_create", ctypes.byref(cfg), ctypes.byref(handle))
 
     # -- plumbing -------------------------------------------------------------
     def __del__(self):

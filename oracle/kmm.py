@@ -1327,3 +1327,234 @@ class PlaneCouetteOracle(KMMOracle):
             "wall_shear_bot": float(np.real(np.mean(sh[0]))),
             "mean_shear": float(np.real(self.TD.integrate(dvdx + self.dUb_dx))) / vol,
         }
+
+
+# ---------------------------------------------------------------------------
+# MHD: plane Couette with a magnetic vector potential (examples/pcf_mhd_jax.py)
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class MHDState:
+    """pcf_mhd_jax.py:34-66: flow state, A in TD^3, and the A histories."""
+
+    flow: KMMState
+    A: tuple
+    nonlinear_A_old: tuple | None = None
+    nonlinear_A_older: tuple | None = None
+    A_old: tuple | None = None
+    A_older: tuple | None = None
+
+
+class PlaneCouetteMHDOracle(PlaneCouetteOracle):
+    """PlaneCouetteMHDJax (pcf_mhd_jax.py:69-789), conducting walls: A in
+    TD^3, B = curl A in (TD, TC, TC), J = curl B in (TC, TD, TD)."""
+
+    def __init__(self, N=(17, 16, 16), Re=600.0, Rm=None, U_wall=1.0, dt=0.01,
+                 perturbation_amplitude=0.05, magnetic_amplitude=0.05, **kw):
+        self.Rm = float(Re if Rm is None else Rm)
+        self.eta = float(U_wall) / self.Rm
+        self.magnetic_amplitude = float(magnetic_amplitude)
+        super().__init__(N=N, Re=Re, U_wall=U_wall, dt=dt,
+                         perturbation_amplitude=perturbation_amplitude, **kw)
+        self._build_A_operators()
+
+    # pcf_mhd_jax.py:116-139
+    def _build_A_operators(self):
+        TDs = (self.D0, self.F1, self.F2)
+        self.MA = mass_terms(*TDs)
+        self.LA = laplace_terms(*TDs).scale(self.eta)
+
+        def factor(gamma):
+            return WavenumberSolver(self.MA - self.LA.scale(gamma))
+
+        if self.time_integrator == "SBDF3":
+            self.SA = factor(self.dt * SBDF3_IMPLICIT)
+            self.SA_startup = [
+                factor((IMEXRK3_A[rk] + IMEXRK3_B[rk]) * self.dt / 2.0) for rk in range(3)
+            ]
+        elif self.time_integrator == "IMEXRK3":
+            self.SA_startup = [
+                factor((IMEXRK3_A[rk] + IMEXRK3_B[rk]) * self.dt / 2.0) for rk in range(3)
+            ]
+        else:
+            raise NotImplementedError("MHD oracle: SBDF3 or IMEXRK3")
+
+    @property
+    def b_spaces(self):
+        return (self.TD, self.TC, self.TC)
+
+    @property
+    def j_spaces(self):
+        return (self.TC, self.TD, self.TD)
+
+    def _A_mass_rhs(self, A):
+        return tuple(self.MA.matvec(a) for a in A)
+
+    def _A_eta_lap(self, A):
+        return tuple(self.LA.matvec(a) for a in A)
+
+    def _A_solve(self, solver, rhs):
+        return tuple(self.TD.mask_nyquist(solver.solve(self.TD.mask_nyquist(r))) for r in rhs)
+
+    def _curl(self, F, spaces_in, spaces_out):
+        """pcf_mhd_jax.py:249-291: projected curl without a physical round trip."""
+        FO = tuple(sp.to_orthogonal(f) for sp, f in zip(spaces_in, F, strict=True))
+        d = lambda sp, f, k: sp.differentiate_orthogonal_coeffs(f, k)  # noqa: E731
+        S = spaces_in
+        cx = d(S[2], FO[2], (0, 1, 0)) - d(S[1], FO[1], (0, 0, 1))
+        cy = d(S[0], FO[0], (0, 0, 1)) - d(S[2], FO[2], (1, 0, 0))
+        cz = d(S[1], FO[1], (1, 0, 0)) - d(S[0], FO[0], (0, 1, 0))
+        return tuple(
+            sp.mask_nyquist(sp.project_from_orthogonal(c))
+            for sp, c in zip(spaces_out, (cx, cy, cz), strict=True)
+        )
+
+    def update_B_from_A(self, A):
+        return self._curl(A, (self.TD, self.TD, self.TD), self.b_spaces)
+
+    def update_J_from_B(self, B):
+        return self._curl(B, self.b_spaces, self.j_spaces)
+
+    def _backward_vec(self, F, spaces, padded):
+        counts = self.pad_counts if padded else self.counts
+        return tuple(sp.backward(f, counts) for sp, f in zip(spaces, F, strict=True))
+
+    @staticmethod
+    def _cross(a, b):
+        return (a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0])
+
+    def mhd_convection(self, state: MHDState):
+        """pcf_mhd_jax.py:331-346: H = TD[-(u_t x w_t) - J x B], HA = TD[(u + U_b) x B]."""
+        flow = state.flow
+        n = self.convection_physical(flow.u)
+        up = self.backward_velocity(flow.u, padded=True)
+        B = self.update_B_from_A(state.A)
+        J = self.update_J_from_B(B)
+        bp = self._backward_vec(B, self.b_spaces, True)
+        jp = self._backward_vec(J, self.j_spaces, True)
+        lorentz = self._cross(jp, bp)
+        n = tuple(ni - li for ni, li in zip(n, lorentz, strict=True))
+        H = tuple(self.TD.mask_nyquist(self.TD.forward(v)) for v in n)
+        utot = (up[0], up[1] + self.Ubp, up[2])
+        emf = self._cross(utot, bp)
+        HA = tuple(self.TD.mask_nyquist(self.TD.forward(v)) for v in emf)
+        return H, HA
+
+    def initial_state(self) -> MHDState:
+        """pcf_mhd_jax.py:232-247."""
+        flow = super().initial_state()
+        x, y, z = self.X
+        amp = self.magnetic_amplitude
+        shape = self.counts
+        ax = np.zeros(shape)
+        if amp != 0.0:
+            Ly = self.domain[1][1] - self.domain[1][0]
+            Lz = self.domain[2][1] - self.domain[2][0]
+            ky, kz = 2.0 * np.pi / Ly, 2.0 * np.pi / Lz
+            ax = np.broadcast_to(
+                amp * (1.0 - x**2) * (1.0 / kz) * np.sin(ky * y) * np.sin(kz * z), shape)
+        A = tuple(self.TD.mask_nyquist(self.TD.forward(np.asarray(a, dtype=complex)))
+                  for a in (ax, np.zeros(shape), np.zeros(shape)))
+        return self._reset_mhd_history(MHDState(flow=flow, A=A))
+
+    def _reset_mhd_history(self, state: MHDState) -> MHDState:
+        zero = tuple(np.zeros_like(a) for a in state.A)
+        return replace(state, flow=self._reset_history(state.flow), nonlinear_A_old=zero,
+                       nonlinear_A_older=zero, A_old=zero, A_older=zero)
+
+    def step_imexrk3_mhd(self, state: MHDState, factors, SA) -> MHDState:
+        """pcf_mhd_jax.py:487-560 (coupled Spalart IMEXRK3)."""
+        dt = self.dt
+        flow_stage, A_stage = state.flow, state.A
+        prev = (np.zeros_like(state.flow.u[0]), np.zeros_like(state.flow.g),
+                np.zeros(state.flow.u[1].shape[0]), np.zeros(state.flow.u[2].shape[0]))
+        prev_A = tuple(np.zeros_like(a) for a in state.A)
+        for rk in range(3):
+            H, HA = self.mhd_convection(MHDState(flow=flow_stage, A=A_stage))
+            cur = self.nonlinear_rhs(H)
+            cur_A = self._A_mass_rhs(HA)
+            a, b = IMEXRK3_A[rk], IMEXRK3_B[rk]
+            gamma = (a + b) * dt / 2.0
+            u_stage, g_stage = flow_stage.u, flow_stage.g
+            v = np.real(u_stage[1][:, 0, 0])
+            w = np.real(u_stage[2][:, 0, 0])
+            rhs_u = self.Mu.matvec(u_stage[0]) + gamma * self.Lu.matvec(u_stage[0])
+            rhs_g = self.Mg.matvec(g_stage) + gamma * self.Lg.matvec(g_stage)
+            rhs_v = self.M00 @ v + gamma * (self.L00 @ v)
+            rhs_w = self.M00 @ w + gamma * (self.L00 @ w)
+            rhs_u = rhs_u + dt * (a * cur[0] + b * prev[0])
+            rhs_g = rhs_g + dt * (a * cur[1] + b * prev[1])
+            rhs_v = rhs_v + dt * (a * cur[2] + b * prev[2])
+            rhs_w = rhs_w + dt * (a * cur[3] + b * prev[3])
+            mA, lA = self._A_mass_rhs(A_stage), self._A_eta_lap(A_stage)
+            rhs_A = [mA[i] + gamma * lA[i] + dt * (a * cur_A[i] + b * prev_A[i]) for i in range(3)]
+            u0, g, v00, w00 = self._solve_all(factors[rk], rhs_u, rhs_g, rhs_v, rhs_w)
+            flow_stage = replace(flow_stage, u=self.reconstruct(u0, g, v00, w00), g=g)
+            A_stage = self._A_solve(SA[rk], rhs_A)
+            prev, prev_A = cur, cur_A
+        return replace(state, flow=replace(state.flow, u=flow_stage.u, g=flow_stage.g), A=A_stage)
+
+    def step_sbdf3_mhd(self, state: MHDState) -> MHDState:
+        """pcf_mhd_jax.py:562-715 (IMEXRK3 startup, then steady SBDF3)."""
+        dt = self.dt
+        flow = state.flow
+        cur_p = self.primary(flow)
+        H, HA = self.mhd_convection(state)
+        cur_n = self.nonlinear_rhs(H)
+        cur_nA = self._A_mass_rhs(HA)
+        if flow.history_steps < 2:
+            adv = self.step_imexrk3_mhd(state, self.startup, self.SA_startup)
+        else:
+            def comb(m0, m1, m2, n0, n1, n2):
+                return (18.0 * m0 - 9.0 * m1 + 2.0 * m2) / 11.0 + dt * (
+                    18.0 * n0 - 18.0 * n1 + 6.0 * n2) / 11.0  # sbdf3.py:15-41
+            rhs = [comb(*t) for t in zip(
+                self.mass_rows(cur_p), self.mass_rows(flow.solution_old),
+                self.mass_rows(flow.solution_older), cur_n, flow.nonlinear_old,
+                flow.nonlinear_older, strict=True)]
+            rhs_A = [comb(*t) for t in zip(
+                self._A_mass_rhs(state.A), self._A_mass_rhs(state.A_old),
+                self._A_mass_rhs(state.A_older), cur_nA, state.nonlinear_A_old,
+                state.nonlinear_A_older, strict=True)]
+            u0, g, v00, w00 = self._solve_all(self.steady, *rhs)
+            adv = replace(state, flow=replace(flow, u=self.reconstruct(u0, g, v00, w00), g=g),
+                          A=self._A_solve(self.SA, rhs_A))
+        new_flow = replace(
+            adv.flow, nonlinear_old=cur_n, nonlinear_older=flow.nonlinear_old,
+            solution_old=cur_p, solution_older=flow.solution_old,
+            history_steps=min(2.0, flow.history_steps + 1.0))
+        return replace(adv, flow=new_flow, nonlinear_A_old=cur_nA,
+                       nonlinear_A_older=state.nonlinear_A_old, A_old=state.A,
+                       A_older=state.A_old)
+
+    def step(self, state: MHDState) -> MHDState:
+        if self.time_integrator == "SBDF3":
+            return self.step_sbdf3_mhd(state)
+        return self.step_imexrk3_mhd(state, self.startup, self.SA_startup)
+
+    def solve(self, state: MHDState, steps: int) -> MHDState:
+        for _ in range(int(steps)):
+            state = self.step(state)
+        return state
+
+    def magnetic_divergence_l2(self, state: MHDState) -> float:
+        """pcf_mhd_jax.py:736-744."""
+        B = self.update_B_from_A(state.A)
+        S = self.b_spaces
+        divb = (S[0].backward_primitive(B[0], (1, 0, 0))
+                + S[1].backward_primitive(B[1], (0, 1, 0))
+                + S[2].backward_primitive(B[2], (0, 0, 1)))
+        return float(np.sqrt(np.real(self.TC.integrate(np.conj(divb) * divb))))
+
+    def diagnostics(self, state: MHDState) -> dict[str, float]:
+        """pcf_mhd_jax.py:752-765."""
+        out = super().diagnostics(state.flow)
+        B = self.update_B_from_A(state.A)
+        bp = self._backward_vec(B, self.b_spaces, False)
+        emag = 0.0
+        for bi, sp in zip(bp, self.b_spaces, strict=True):
+            emag += float(np.real(sp.integrate(np.conj(bi) * bi)))
+        out["divB_L2"] = self.magnetic_divergence_l2(state)
+        out["Emag"] = emag
+        return out

@@ -20,5 +20,8 @@ int main(void) {
   printf("jfb_kmm_info %zu\n", sizeof(jfb_kmm_info));
   F(jfb_kmm_info, n_pencils); F(jfb_kmm_info, algorithmic_bytes); F(jfb_kmm_info, my);
   F(jfb_kmm_info, mz);
+  printf("jfb_mhd_state %zu\n", sizeof(jfb_mhd_state));
+  F(jfb_mhd_state, flow); F(jfb_mhd_state, A); F(jfb_mhd_state, nonlinear_A_old);
+  F(jfb_mhd_state, nonlinear_A_older); F(jfb_mhd_state, A_old); F(jfb_mhd_state, A_older);
   return 0;
 }

@@ -47,6 +47,24 @@ REFERENCE = {
         "state_checksum": {"element_count": 3056123, "l2_norm": 5.062610681087452,
                            "real_sum": -7.830872524041756},
     },
+    "benchmark_mhd_sbdf3_rotational_65x64x64": {
+        "source": "benchmark-results/mhd-sbdf3-rotational-65x64x64-r1.json "
+                  "(timing.final_diagnostics; solver built by "
+                  "production/benchmark_pcf_refactor.py: PlaneCouetteMHDJax, "
+                  "velocity amplitude 0.02, magnetic amplitude 0.005)",
+        "solver": {"N": [65, 64, 64], "family": "C", "dt": 1.0e-3,
+                   "perturbation_amplitude": 0.02, "magnetic_amplitude": 0.005,
+                   "Re": 400.0, "Rm": 400.0,
+                   "time_integrator": "SBDF3", "nonlinear_form": "rotational",
+                   "coefficient_path": "optimized", "padding_factor": [1.0, 1.5, 1.5]},
+        "steps": 325,
+        "diagnostics": {"Emag": 0.0006539729631867507, "Epert": 0.03186034627195483,
+                        "Etot": 52.669153697981685, "divB_L2": 3.2078792579026027e-18,
+                        "divL2": 7.275547313434249e-17, "mean_shear": 1.0,
+                        "u_bot": -1.0, "u_top": 1.0,
+                        "wall_shear_bot": 1.0000166621379911,
+                        "wall_shear_top": 1.0000166621379911},
+    },
 }
 
 

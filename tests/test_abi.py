@@ -23,7 +23,7 @@ def declared_functions():
 def test_header_declares_the_abi():
     names = declared_functions()
     assert "jfb_kmm_advance" in names and "jfb_wavenumber_solve" in names
-    assert len(names) >= 14
+    assert len(names) >= 20
 
 
 def test_library_exports_every_declared_symbol():
@@ -63,10 +63,24 @@ def c_layout(tmp_path_factory):
 
 @pytest.mark.parametrize("cname, cls", [("jfb_kmm_config", _lib.KMMConfig),
                                         ("jfb_kmm_state", _lib.KMMStateC),
-                                        ("jfb_kmm_info", _lib.KMMInfo)])
+                                        ("jfb_kmm_info", _lib.KMMInfo),
+                                        ("jfb_mhd_state", _lib.MHDStateC)])
 def test_struct_layouts_match_c(c_layout, cname, cls):
     assert int(c_layout[cname]) == ctypes.sizeof(cls)
     for key, off in c_layout.items():
         if key.startswith(cname + "."):
             field = key.split(".", 1)[1]
             assert getattr(cls, field).offset == int(off), key
+
+
+def test_mhd_argument_errors_are_reported_without_a_gpu():
+    lib = _lib.load()
+    cfg = _lib.KMMConfig()
+    cfg.nx, cfg.ny, cfg.nz = 17, 16, 16
+    cfg.precision = _lib.JFB_PRECISION_MIXED
+    h = ctypes.c_void_p()
+    assert lib.jfb_mhd_create(ctypes.byref(cfg), 400.0, ctypes.byref(h)) == _lib.JFB_ERR_ARG
+    assert b"FP64" in lib.jfb_last_error()
+    cfg.precision = _lib.JFB_PRECISION_FP64
+    assert lib.jfb_mhd_create(ctypes.byref(cfg), -1.0, ctypes.byref(h)) == _lib.JFB_ERR_ARG
+    assert b"rm" in lib.jfb_last_error()

@@ -6,7 +6,7 @@ import os
 import numpy as np
 import pytest
 
-from oracle.kmm import PlaneCouetteOracle
+from oracle.kmm import PlaneCouetteMHDOracle, PlaneCouetteOracle
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = json.load(open(os.path.join(HERE, "golden", "reference_goldens.json")))
@@ -50,6 +50,22 @@ def test_benchmark_325_steps_golden():
     cs = spec["state_checksum"]
     assert count == cs["element_count"]
     assert np.isclose(l2, cs["l2_norm"], rtol=1e-10)
+
+
+@pytest.mark.slow
+def test_mhd_benchmark_325_steps_golden():
+    """benchmark-results/mhd-sbdf3-rotational-65x64x64-r1.json of the
+    reference: the coupled flow + vector-potential step, 325 SBDF3 rotational
+    steps (about 10 minutes)."""
+    spec = GOLD["benchmark_mhd_sbdf3_rotational_65x64x64"]
+    s = spec["solver"]
+    o = PlaneCouetteMHDOracle(N=tuple(s["N"]), Re=s["Re"], Rm=s["Rm"], dt=s["dt"],
+                              perturbation_amplitude=s["perturbation_amplitude"],
+                              magnetic_amplitude=s["magnetic_amplitude"])
+    d = o.diagnostics(o.solve(o.initial_state(), spec["steps"]))
+    for key in ("Emag", "Epert", "Etot", "wall_shear_top", "wall_shear_bot", "u_top", "u_bot"):
+        assert np.isclose(d[key], spec["diagnostics"][key], rtol=1e-10, atol=1e-14), key
+    assert d["divB_L2"] < 1e-15 and d["divL2"] < 1e-15
 
 
 def test_oracle_matches_committed_fixture():

@@ -115,3 +115,41 @@ def test_fourier_padding_round_trip():
     c[8] = 0
     u = f.backward(c, 24, 0)
     np.testing.assert_allclose(f.forward(u, 0), c, atol=1e-14)
+
+
+def test_mhd_initial_magnetic_energy_is_analytic():
+    """A_x = a (1 - x^2) sin(ky y) sin(kz z) / kz gives B = curl A =
+    (0, a (1 - x^2) sin(ky y) cos(kz z), -a (ky / kz) (1 - x^2) cos(ky y) sin(kz z)),
+    so Emag = a^2 (16/15) (Ly Lz / 4) (1 + (ky/kz)^2) exactly (1 - x^2 lies in
+    the Dirichlet space)."""
+    a = 0.2
+    o = ok.PlaneCouetteMHDOracle(N=(17, 16, 16), Re=400.0, dt=1e-3, magnetic_amplitude=a)
+    d = o.diagnostics(o.initial_state())
+    Ly, Lz = 4.0 * np.pi, 2.0 * np.pi
+    ky, kz = 2.0 * np.pi / Ly, 2.0 * np.pi / Lz
+    exact = a * a * (16.0 / 15.0) * (Ly * Lz / 4.0) * (1.0 + (ky / kz) ** 2)
+    assert abs(d["Emag"] - exact) < 1e-13 * exact
+    assert d["divB_L2"] < 1e-15
+
+
+def test_mhd_without_field_is_the_hydro_step():
+    """magnetic_amplitude = 0: A stays zero, the flow follows the hydro oracle."""
+    kw = dict(N=(17, 16, 16), Re=400.0, dt=1e-3, perturbation_amplitude=0.05)
+    m = ok.PlaneCouetteMHDOracle(magnetic_amplitude=0.0, **kw)
+    h = ok.PlaneCouetteOracle(**kw)
+    sm, sh = m.solve(m.initial_state(), 4), h.solve(h.initial_state(), 4)
+    for x, y in zip((*sm.flow.u, sm.flow.g), (*sh.u, sh.g), strict=True):
+        np.testing.assert_allclose(x, y, rtol=0, atol=1e-16)
+    assert all(np.abs(A).max() == 0.0 for A in sm.A)
+
+
+def test_mhd_field_stays_solenoidal_and_couples():
+    """B = curl A keeps div B at round-off through startup and steady steps,
+    and the Lorentz force changes the flow."""
+    kw = dict(N=(17, 16, 16), Re=400.0, dt=1e-3, perturbation_amplitude=0.05)
+    m = ok.PlaneCouetteMHDOracle(magnetic_amplitude=0.5, **kw)
+    st = m.solve(m.initial_state(), 5)
+    assert m.magnetic_divergence_l2(st) < 1e-14
+    h = ok.PlaneCouetteOracle(**kw)
+    sh = h.solve(h.initial_state(), 5)
+    assert np.linalg.norm(st.flow.u[0] - sh.u[0]) > 1e-8 * np.linalg.norm(sh.u[0])
