@@ -195,6 +195,29 @@ int jfb_kmm_timed_steps(jfb_kmm_plan* plan, int64_t steps, void* flush_buf,
                         int64_t flush_bytes, double* kernel_ms, double* step_ms,
                         void* stream);
 
+/* perturbation_gain + jax.value_and_grad of it (examples/
+ * pcf_minimal_seed_jax.py:111-150): runs `steps` steps from `init` (its
+ * u0, u1, u2, g; history_steps must be 0, history pointers are ignored) and
+ * writes gain = E(T) / E(0) (perturbation energies) to *gain_out (host).  If
+ * grad is non-NULL, writes d gain / d init in jax.grad's convention (the
+ * directional derivative along d is Re sum(grad * d) over the leaves) to
+ * grad->u0, u1, u2, g (full-spectrum reference layout; the Hermitian
+ * representative) and zeros to any history pointers given.  The gradient is
+ * the hand-written discrete adjoint of the FP64 step (transposed transforms,
+ * transposed banded solves, linearised rotational product) over a reverse
+ * sweep that recomputes `checkpoint` steps at a time from stored states.
+ * FP64 flow plans only.  The plan's loaded state is consumed. */
+int jfb_kmm_gain_gradient(jfb_kmm_plan* plan, const jfb_kmm_state* init, int64_t steps,
+                          int64_t checkpoint, double* gain_out, const jfb_kmm_state* grad,
+                          void* stream);
+
+/* jax.grad(perturbation_energy)(state) (pcf_minimal_seed_jax.py:125-137
+ * uses it for the fixed-energy tangent): writes the gradient of
+ * E = sum_f int |u_f|^2 with respect to u0, u1, u2 (jax.grad convention,
+ * full-spectrum layout) and zeros to grad->g if given.  Loads `state`. */
+int jfb_kmm_energy_gradient(jfb_kmm_plan* plan, const jfb_kmm_state* state,
+                            const jfb_kmm_state* grad, void* stream);
+
 /* ---- plane-Couette MHD (vector potential, conducting walls) ------------- */
 
 /* Device pointers to an MHDState (examples/pcf_mhd_jax.py:34-66): the flow

@@ -124,6 +124,14 @@ SIGNATURES = {
         c_int,
         [c_void_p, c_int64, c_void_p, c_int64, POINTER(c_double), POINTER(c_double), c_void_p],
     ),
+    "jfb_kmm_gain_gradient": (
+        c_int,
+        [c_void_p, POINTER(KMMStateC), c_int64, c_int64, POINTER(c_double),
+         POINTER(KMMStateC), c_void_p],
+    ),
+    "jfb_kmm_energy_gradient": (
+        c_int, [c_void_p, POINTER(KMMStateC), POINTER(KMMStateC), c_void_p]
+    ),
     "jfb_mhd_create": (c_int, [POINTER(KMMConfig), c_double, POINTER(c_void_p)]),
     "jfb_mhd_set_state": (c_int, [c_void_p, POINTER(MHDStateC), c_void_p]),
     "jfb_mhd_get_state": (c_int, [c_void_p, POINTER(MHDStateC), c_void_p]),

@@ -17,6 +17,7 @@
 #include "jfb_kmm_warpk.cuh"
 #include "jfb_kmm_gemm.cuh"
 #include "jfb_kmm_mhd.cuh"
+#include "jfb_kmm_adjoint.cuh"
 
 namespace jfb {
 
@@ -188,6 +189,16 @@ struct FactorSet {
   double* su = nullptr;
   double* sg = nullptr;
   double* s00 = nullptr;
+  // factored bands kept for the transposed solves of the adjoint (Su, Sg, S00)
+  double* band[3] = {nullptr, nullptr, nullptr};
+  int bp[3] = {0, 0, 0}, bq[3] = {0, 0, 0};
+};
+
+// Real x-matrices of the adjoint (row-major, forward orientation).
+struct AdjOps {
+  double *A0 = nullptr, *F = nullptr, *R0 = nullptr, *R1 = nullptr, *R2 = nullptr,
+         *R3 = nullptr, *B1 = nullptr, *B2 = nullptr, *GB = nullptr, *GD = nullptr,
+         *XB0 = nullptr, *XB2 = nullptr, *XB4 = nullptr, *XD0 = nullptr, *XD2 = nullptr;
 };
 
 }  // namespace jfb
@@ -240,6 +251,11 @@ struct jfb_kmm_plan {
   jfb::c64 *AR[3], *NA[3], *NAst;
   size_t smem_mhd = 0, smem_zm = 0;
   double* mdiag_partial = nullptr;
+  // adjoint: operators and kept factor bands, built on first use
+  bool adj_ready = false;
+  jfb::AdjOps aops;
+  jfb::FactorSet adj_steady, adj_startup[3];
+  size_t smem_za = 0;
 };
 
 namespace jfb {
@@ -291,9 +307,10 @@ static std::vector<c64> twiddles(int n) {
 // gamma (tpmatrix.py:1900-2029 assembly, 1105-1149 batched LU).
 // Systems sys_first..sys_last (0: Su, 1: Sg, 2: S00) with diffusivity nu;
 // inv selects the explicit inverse-factor records (always used by the
-// tensor-core pencil stage and the A solves).
+// tensor-core pencil stage and the A solves); keep_band keeps the factored
+// band instead of packing it (the adjoint's transposed solves).
 static int build_factor_set(jfb_kmm_plan* pl, double gamma, FactorSet& fs, double nu,
-                            int sys_first, int sys_last, bool inv) {
+                            int sys_first, int sys_last, bool inv, bool keep_band = false) {
   const HostOperators& op = pl->hop;
   jfb_kmm_config cfg = pl->cfg;
   cfg.nu = nu;
@@ -355,6 +372,29 @@ static int build_factor_set(jfb_kmm_plan* pl, double gamma, FactorSet& fs, doubl
     JFB_CHECK_LAUNCH();
     st = jfb_banded_lu_factor(dband, modes, p, q, n, nullptr);
     if (st) return cleanup(), st;
+    if (keep_band) {
+      fs.band[sys] = dband;
+      fs.bp[sys] = p;
+      fs.bq[sys] = q;
+      pl->allocs.push_back(dband);
+      pl->device_bytes += (int64_t)(band_elems * sizeof(double));
+      dband = nullptr;
+      JFB_CHECK_CUDA(cudaDeviceSynchronize());
+      for (void* ptr : {(void*)dX0, (void*)dX2, (void*)dX4, (void*)dcoef}) {
+        if (!ptr) continue;
+        for (size_t k = 0; k < pl->allocs.size(); ++k)
+          if (pl->allocs[k] == ptr) {
+            pl->allocs.erase(pl->allocs.begin() + k);
+            break;
+          }
+      }
+      pl->device_bytes -= (int64_t)(X0.size() + X2.size() + (bih ? op.XB4.size() : 0) +
+                                    coef.size()) *
+                          sizeof(double);
+      cleanup();
+      dX0 = dX2 = dX4 = dcoef = nullptr;
+      continue;
+    }
     double** dst = (sys == 0) ? &fs.su : (sys == 1) ? &fs.sg : &fs.s00;
     st = dalloc(pl, (void**)dst, (size_t)modes * packed_rec_size(n) * sizeof(double));
     if (st) return cleanup(), st;
@@ -750,7 +790,9 @@ static int steady_step_timed(jfb_kmm_plan* pl, int64_t m, cudaStream_t s, cudaEv
 }
 
 // One IMEXRK3 startup step (_step_sbdf3 startup branch).
-static int startup_step(jfb_kmm_plan* pl, cudaStream_t s) {
+// rec (optional): receives the stage states after stages 0 and 1 as
+// (u0, g, vw) of stage 1 then of stage 2 (the adjoint's linearisation points).
+static int startup_step(jfb_kmm_plan* pl, cudaStream_t s, c64* const* rec = nullptr) {
   const int64_t m = pl->n;
   const int c = slot(m), nw = slot(m + 1);
   for (int rk = 0; rk < 3; ++rk) {
@@ -808,6 +850,15 @@ static int startup_step(jfb_kmm_plan* pl, cudaStream_t s) {
       m.A_out = pl->AR[nw];
       m.XB = pl->X + (size_t)6 * pl->d.Nx * pl->d.P;
       if ((st = launch_mhd(pl, m, s))) return st;
+    }
+    if (rec && rk < 2) {
+      const size_t P = pl->d.P;
+      JFB_CHECK_CUDA(cudaMemcpyAsync(rec[3 * rk], pl->U0[nw], (size_t)pl->d.nB * P * sizeof(c64),
+                                     cudaMemcpyDeviceToDevice, s));
+      JFB_CHECK_CUDA(cudaMemcpyAsync(rec[3 * rk + 1], pl->G[nw], (size_t)pl->d.nD * P * sizeof(c64),
+                                     cudaMemcpyDeviceToDevice, s));
+      JFB_CHECK_CUDA(cudaMemcpyAsync(rec[3 * rk + 2], pl->VW[nw], (size_t)pl->d.nD * sizeof(c64),
+                                     cudaMemcpyDeviceToDevice, s));
     }
     st = launch_transforms(pl, s);
     if (st) return st;
@@ -1660,5 +1711,635 @@ extern "C" int jfb_mhd_diagnostics(jfb_kmm_plan* pl, double* out, void* stream) 
   mhd_diag_finish_kernel<<<1, 32, 0, s>>>(pl->mdiag_partial, pl->diag_blocks, pl->cfg.ly,
                                           pl->cfg.lz, out + 8);
   JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint of the FP64 step: gain E(T)/E(0) and its gradient with respect to
+// the initial state (perturbation_gain / gain_and_projected_gradient,
+// examples/pcf_minimal_seed_jax.py:111-150, the gradient that jax.grad takes
+// through KMM.solve).  State s = (u0, g, v00, w00) as in KMM.primary; the
+// explicit initial leaves (u0, u1, u2, g) enter the first nonlinear term
+// directly.  Reverse sweep over recomputed segments of `checkpoint` steps.
+// ---------------------------------------------------------------------------
+
+namespace jfb {
+
+struct AState {
+  c64 *u = nullptr, *g = nullptr, *v = nullptr, *w = nullptr;  // v, w: mean column only
+};
+
+struct AdjRun {
+  std::vector<void*> mem;
+  c64 *XF, *YF, *AH, *AW, *HZ6, *AX, *U1w, *U2w, *EU[3];
+  AState S[4], Nn[4], MU, Z, NZ[3];
+  int K = 0;
+  c64 *TU0, *TG, *TVW;          // states of the segment being reversed, K + 1 slots
+  c64* rec[2][6];               // stage states of the two startup steps
+  c64 *IU0, *IU1, *IU2, *IG;    // explicit initial leaves
+  std::vector<c64*> ck;         // checkpoints: rings + HX
+  size_t ck_elems = 0;
+  ~AdjRun() {
+    for (void* p : mem) cudaFree(p);
+  }
+  int alloc(c64** p, size_t elems) {
+    JFB_CHECK_CUDA(cudaMalloc((void**)p, std::max<size_t>(1, elems) * sizeof(c64)));
+    JFB_CHECK_CUDA(cudaMemset(*p, 0, std::max<size_t>(1, elems) * sizeof(c64)));
+    mem.push_back(*p);
+    return JFB_OK;
+  }
+};
+
+static int adj_prepare(jfb_kmm_plan* pl) {
+  if (pl->adj_ready) return JFB_OK;
+  const Dims& d = pl->d;
+  GemmHost gh;
+  std::string err;
+  if (!build_gemm_operators(pl->hop, gh, err)) {
+    set_error(err);
+    return JFB_ERR_ARG;
+  }
+  AdjOps& A = pl->aops;
+  const HostOperators& op = pl->hop;
+  int st;
+#define UPA(field, vec) \
+  if ((st = upload(pl, &A.field, vec))) return st;
+  UPA(A0, gh.A0);
+  UPA(F, gh.F);
+  UPA(R0, gh.R0);
+  UPA(R1, gh.R1);
+  UPA(R2, gh.R2);
+  UPA(R3, gh.R3);
+  UPA(B1, gh.B1);
+  UPA(B2, gh.B2);
+  UPA(GB, gh.GB);
+  UPA(GD, gh.GD);
+  UPA(XB0, op.XB0);
+  UPA(XB2, op.XB2);
+  UPA(XB4, op.XB4);
+  UPA(XD0, op.XD0);
+  UPA(XD2, op.XD2);
+#undef UPA
+  const double nu = pl->cfg.nu, dt = pl->cfg.dt;
+  if ((st = build_factor_set(pl, kSBDF3Implicit * dt, pl->adj_steady, nu, 0, 2, false, true)))
+    return st;
+  for (int rk = 0; rk < 3; ++rk)
+    if ((st = build_factor_set(pl, (kRK3A[rk] + kRK3B[rk]) * dt / 2.0, pl->adj_startup[rk], nu,
+                               0, 2, false, true)))
+      return st;
+  pl->smem_za = (size_t)2 * d.Mz * kZRows * 5 * sizeof(c64);
+  if (pl->smem_za > 227 * 1024) {
+    set_error("grid too large for the adjoint z stage");
+    return JFB_ERR_ARG;
+  }
+  JFB_CHECK_CUDA(allow_smem((const void*)z_adjoint_kernel));
+  pl->adj_ready = true;
+  return JFB_OK;
+}
+
+// -- term lists ---------------------------------------------------------------
+static PTermList tlist(c64* dst, int rows, bool acc) {
+  PTermList L;
+  std::memset(&L, 0, sizeof(L));
+  L.dst = dst;
+  L.dst_rows = rows;
+  L.accumulate = acc ? 1 : 0;
+  return L;
+}
+
+static void term(PTermList& L, const c64* src, const double* mat, int src_rows, int trans,
+                 double cre, double cim, int a = 0, int b = 0, int c = 0, int sel = 0,
+                 int realpart = 0) {
+  if (cre == 0.0 && cim == 0.0) return;
+  PTerm& T = L.t[L.n++];
+  T.src = src;
+  T.mat = mat;
+  T.src_rows = src_rows;
+  T.trans = trans;
+  T.cre = cre;
+  T.cim = cim;
+  T.a = a;
+  T.b = b;
+  T.c = c;
+  T.sel = sel;
+  T.realpart = realpart;
+}
+
+static int run(jfb_kmm_plan* pl, const PTermList& L, cudaStream_t s) {
+  JFB_REQUIRE(L.n <= kMaxTerms, "term list too long");
+  dim3 g(ceil_div(pl->d.P, 32), ceil_div(L.dst_rows, 8));
+  pencil_terms_kernel<<<g, 256, 0, s>>>(pl->d, L);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+#define JFB_RUN(L) \
+  if ((st = run(pl, L, s))) return st;
+
+// explicit adjoint (a_u0, a_u1, a_u2) = pro^H (adjoint of the six x-physical
+// fields u, omega of the prologue map)
+static int adj_pro(jfb_kmm_plan* pl, AdjRun& R, cudaStream_t s) {
+  const Dims& d = pl->d;
+  const AdjOps& A = pl->aops;
+  const size_t f = (size_t)d.Nx * d.P;
+  const c64* X = R.AX;
+  const int N = d.Nx;
+  int st;
+  PTermList L = tlist(R.EU[0], d.nB, false);
+  term(L, X + 0 * f, A.A0, N, 1, 1, 0);
+  term(L, X + 4 * f, A.A0, N, 1, 0, -1, 0, 1);  // -i kz
+  term(L, X + 5 * f, A.A0, N, 1, 0, 1, 1, 0);   // +i ky
+  JFB_RUN(L);
+  L = tlist(R.EU[1], d.nD, false);
+  term(L, X + 1 * f, A.B1, N, 1, 1, 0);
+  term(L, X + 3 * f, A.B1, N, 1, 0, 1, 0, 1);  // +i kz
+  term(L, X + 5 * f, A.B2, N, 1, 1, 0);
+  JFB_RUN(L);
+  L = tlist(R.EU[2], d.nD, false);
+  term(L, X + 2 * f, A.B1, N, 1, 1, 0);
+  term(L, X + 3 * f, A.B1, N, 1, 0, -1, 1, 0);  // -i ky
+  term(L, X + 4 * f, A.B2, N, 1, -1, 0);
+  JFB_RUN(L);
+  return JFB_OK;
+}
+
+// dst (+)= recon^H (EU): reconstruct_velocity (channelflow_kmm.py:855-870)
+static int adj_recon(jfb_kmm_plan* pl, AdjRun& R, const AState& dst, bool acc, cudaStream_t s) {
+  const Dims& d = pl->d;
+  const AdjOps& A = pl->aops;
+  int st;
+  PTermList L = tlist(dst.u, d.nB, acc);
+  term(L, R.EU[0], nullptr, d.nB, 0, 1, 0);
+  term(L, R.EU[1], A.F, d.nD, 1, 0, -1, 1, 0, -1);  // -i ky / k^2
+  term(L, R.EU[2], A.F, d.nD, 1, 0, -1, 0, 1, -1);  // -i kz / k^2
+  JFB_RUN(L);
+  L = tlist(dst.g, d.nD, acc);
+  term(L, R.EU[1], nullptr, d.nD, 0, 0, -1, 0, 1, -1);  // -i kz / k^2
+  term(L, R.EU[2], nullptr, d.nD, 0, 0, 1, 1, 0, -1);   // +i ky / k^2
+  JFB_RUN(L);
+  L = tlist(dst.v, d.nD, acc);
+  term(L, R.EU[1], nullptr, d.nD, 0, 1, 0, 0, 0, 0, 2, 1);
+  JFB_RUN(L);
+  L = tlist(dst.w, d.nD, acc);
+  term(L, R.EU[2], nullptr, d.nD, 0, 1, 0, 0, 0, 0, 2, 1);
+  JFB_RUN(L);
+  return JFB_OK;
+}
+
+// AH = R_n^H mu: adjoint of the nonlinear rows (channelflow_kmm.py:810-829)
+static int adj_rows(jfb_kmm_plan* pl, AdjRun& R, const AState& mu, cudaStream_t s) {
+  const Dims& d = pl->d;
+  const AdjOps& A = pl->aops;
+  const size_t f = (size_t)d.Nx * d.P;
+  const double myz = d.Myz;
+  int st;
+  PTermList L = tlist(R.AH, d.Nx, false);
+  term(L, mu.u, A.R0, d.nB, 1, myz, 0, 0, 0, 1);  // Myz k^2
+  JFB_RUN(L);
+  L = tlist(R.AH + f, d.Nx, false);
+  term(L, mu.u, A.R1, d.nB, 1, 0, -myz, 1, 0);  // -i ky Myz
+  term(L, mu.g, A.R2, d.nD, 1, 0, -myz, 0, 1);  // -i kz Myz
+  term(L, mu.v, A.R3, d.nD, 1, -1, 0, 0, 0, 0, 2, 1);
+  JFB_RUN(L);
+  L = tlist(R.AH + 2 * f, d.Nx, false);
+  term(L, mu.u, A.R1, d.nB, 1, 0, -myz, 0, 1);  // -i kz Myz
+  term(L, mu.g, A.R2, d.nD, 1, 0, myz, 1, 0);   // +i ky Myz
+  term(L, mu.w, A.R3, d.nD, 1, -1, 0, 0, 0, 0, 2, 1);
+  JFB_RUN(L);
+  return JFB_OK;
+}
+
+// dst += cm (M + gamma L)^T mu, gl = gamma nu (mass rows channelflow_kmm.py:261-409)
+static int adj_mass(jfb_kmm_plan* pl, const AState& mu, double cm, double gl, const AState& dst,
+                    cudaStream_t s) {
+  const Dims& d = pl->d;
+  const AdjOps& A = pl->aops;
+  const double m = cm * d.Myz;
+  int st;
+  PTermList L = tlist(dst.u, d.nB, true);
+  term(L, mu.u, A.XB0, d.nB, 1, -m, 0, 0, 0, 1);
+  term(L, mu.u, A.XB0, d.nB, 1, m * gl, 0, 0, 0, 2);
+  term(L, mu.u, A.XB2, d.nB, 1, m, 0);
+  term(L, mu.u, A.XB2, d.nB, 1, -2.0 * m * gl, 0, 0, 0, 1);
+  term(L, mu.u, A.XB4, d.nB, 1, m * gl, 0);
+  JFB_RUN(L);
+  L = tlist(dst.g, d.nD, true);
+  term(L, mu.g, A.XD0, d.nD, 1, m, 0);
+  term(L, mu.g, A.XD0, d.nD, 1, -m * gl, 0, 0, 0, 1);
+  term(L, mu.g, A.XD2, d.nD, 1, m * gl, 0);
+  JFB_RUN(L);
+  for (int k = 0; k < 2; ++k) {
+    c64* out = k ? dst.w : dst.v;
+    const c64* in = k ? mu.w : mu.v;
+    L = tlist(out, d.nD, true);
+    term(L, in, A.XD0, d.nD, 1, cm, 0, 0, 0, 0, 2);
+    term(L, in, A.XD2, d.nD, 1, cm * gl, 0, 0, 0, 0, 2);
+    JFB_RUN(L);
+  }
+  return JFB_OK;
+}
+
+// dst = S^-T src with the kept factor bands
+static int adj_solve(jfb_kmm_plan* pl, const FactorSet& fs, const AState& src, const AState& dst,
+                     cudaStream_t s) {
+  const Dims& d = pl->d;
+  const int blocks = ceil_div(d.P, 128);
+  band_solve_t_kernel<<<blocks, 128, 0, s>>>(d, fs.band[0], fs.bp[0], fs.bq[0], d.nB, 0, src.u, dst.u);
+  band_solve_t_kernel<<<blocks, 128, 0, s>>>(d, fs.band[1], fs.bp[1], fs.bq[1], d.nD, 0, src.g, dst.g);
+  band_solve_t_kernel<<<1, 32, 0, s>>>(d, fs.band[2], fs.bp[2], fs.bq[2], d.nD, 1, src.v, dst.v);
+  band_solve_t_kernel<<<1, 32, 0, s>>>(d, fs.band[2], fs.bp[2], fs.bq[2], d.nD, 1, src.w, dst.w);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+static void astate_axpy(const jfb_kmm_plan* pl, const AState& y, const AState& x, double a,
+                        cudaStream_t s) {
+  const Dims& d = pl->d;
+  const size_t P = d.P;
+  axpy_kernel<<<256, 256, 0, s>>>(y.u, x.u, a, (size_t)d.nB * P);
+  axpy_kernel<<<256, 256, 0, s>>>(y.g, x.g, a, (size_t)d.nD * P);
+  axpy_kernel<<<64, 256, 0, s>>>(y.v, x.v, a, (size_t)d.nD * P);
+  axpy_kernel<<<64, 256, 0, s>>>(y.w, x.w, a, (size_t)d.nD * P);
+}
+
+static int astate_zero(const jfb_kmm_plan* pl, const AState& y, cudaStream_t s) {
+  const Dims& d = pl->d;
+  const size_t P = d.P;
+  JFB_CHECK_CUDA(cudaMemsetAsync(y.u, 0, (size_t)d.nB * P * sizeof(c64), s));
+  JFB_CHECK_CUDA(cudaMemsetAsync(y.g, 0, (size_t)d.nD * P * sizeof(c64), s));
+  JFB_CHECK_CUDA(cudaMemsetAsync(y.v, 0, (size_t)d.nD * P * sizeof(c64), s));
+  JFB_CHECK_CUDA(cudaMemsetAsync(y.w, 0, (size_t)d.nD * P * sizeof(c64), s));
+  return JFB_OK;
+}
+
+// EU = J^H mu at a linearisation point: the state (u0, g, vw) or, with u1
+// and u2 given, the explicit velocity (u0, u1, u2).
+static int adj_nonlinear(jfb_kmm_plan* pl, AdjRun& R, const c64* u0, const c64* g, const c64* vw,
+                         const c64* u1, const c64* u2, const AState& mu, cudaStream_t s) {
+  const Dims& d = pl->d;
+  int st;
+  if (!u1) {
+    StageArgs a = blank_args();
+    a.mode = kReconstruct;
+    a.u0a = u0;
+    a.ga = g;
+    a.vwa = vw;
+    a.X = R.U1w;
+    a.Hd_out = R.U2w;
+    if ((st = launch_pencil(pl, a, s))) return st;
+    u1 = R.U1w;
+    u2 = R.U2w;
+  }
+  StageArgs a = blank_args();
+  a.mode = kPrologue;
+  a.pu0 = u0;
+  a.pu1 = u1;
+  a.pu2 = u2;
+  a.X = R.XF;
+  if ((st = launch_pencil(pl, a, s))) return st;
+  dim3 gy6(d.Nx, 6, d.Kz / pl->KC), gy3(d.Nx, 3, d.Kz / pl->KC);
+  y_backward_kernel<double><<<gy6, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, R.XF, R.YF);
+  JFB_CHECK_LAUNCH();
+  if ((st = adj_rows(pl, R, mu, s))) return st;
+  y_backward_kernel<double><<<gy3, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, R.AH, R.AW);
+  JFB_CHECK_LAUNCH();
+  const int zb = ceil_div((int64_t)d.Nx * d.My, kZRows);
+  z_adjoint_kernel<<<zb, 256, pl->smem_za, s>>>(pl->ops, d, pl->fz, pl->twz, R.YF, R.AW, R.HZ6);
+  JFB_CHECK_LAUNCH();
+  y_forward_kernel<double><<<gy6, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, R.HZ6, R.AX,
+                                                        nullptr);
+  JFB_CHECK_LAUNCH();
+  return adj_pro(pl, R, s);
+}
+
+// EU (+)= scale G u (gradient of the perturbation energy, 2 Ly Lz G u)
+static int adj_energy(jfb_kmm_plan* pl, AdjRun& R, const c64* u0, const c64* u1, const c64* u2,
+                      double scale, bool acc, cudaStream_t s) {
+  const Dims& d = pl->d;
+  const AdjOps& A = pl->aops;
+  int st;
+  PTermList L = tlist(R.EU[0], d.nB, acc);
+  term(L, u0, A.GB, d.nB, 0, scale, 0);
+  JFB_RUN(L);
+  L = tlist(R.EU[1], d.nD, acc);
+  term(L, u1, A.GD, d.nD, 0, scale, 0);
+  JFB_RUN(L);
+  L = tlist(R.EU[2], d.nD, acc);
+  term(L, u2, A.GD, d.nD, 0, scale, 0);
+  JFB_RUN(L);
+  return JFB_OK;
+}
+
+static int perturbation_energy(jfb_kmm_plan* pl, double* dev8, cudaStream_t s, double* out) {
+  int st = jfb_kmm_diagnostics(pl, dev8, s);
+  if (st) return st;
+  JFB_CHECK_CUDA(cudaMemcpyAsync(out, dev8, sizeof(double), cudaMemcpyDeviceToHost, s));
+  JFB_CHECK_CUDA(cudaStreamSynchronize(s));
+  return JFB_OK;
+}
+
+// rings + HX of the plan <-> checkpoint buffer
+static int checkpoint_io(jfb_kmm_plan* pl, c64* buf, bool save, cudaStream_t s) {
+  const Dims& d = pl->d;
+  const size_t P = d.P;
+  size_t off = 0;
+  auto io = [&](c64* arr, size_t n) -> int {
+    if (save)
+      JFB_CHECK_CUDA(cudaMemcpyAsync(buf + off, arr, n * sizeof(c64), cudaMemcpyDeviceToDevice, s));
+    else
+      JFB_CHECK_CUDA(cudaMemcpyAsync(arr, buf + off, n * sizeof(c64), cudaMemcpyDeviceToDevice, s));
+    off += n;
+    return JFB_OK;
+  };
+  int st;
+  for (int k = 0; k < 3; ++k) {
+    if ((st = io(pl->U0[k], (size_t)d.nB * P))) return st;
+    if ((st = io(pl->G[k], (size_t)d.nD * P))) return st;
+    if ((st = io(pl->VW[k], d.nD))) return st;
+    if ((st = io(pl->NU[k], (size_t)d.nB * P))) return st;
+    if ((st = io(pl->NG[k], (size_t)d.nD * P))) return st;
+    if ((st = io(pl->NVW[k], d.nD))) return st;
+  }
+  return io(pl->HX, (size_t)3 * d.Nx * P);
+}
+
+static size_t checkpoint_elems(const jfb_kmm_plan* pl) {
+  const Dims& d = pl->d;
+  const size_t P = d.P;
+  return 3 * (2 * (size_t)d.nB * P + 2 * (size_t)d.nD * P + 2 * (size_t)d.nD) +
+         (size_t)3 * d.Nx * P;
+}
+
+// One forward step from ring position pl->n (startup while hist < 2),
+// recording the startup stage states when rec is given.
+static int forward_step(jfb_kmm_plan* pl, cudaStream_t s, c64* const* rec) {
+  int st = (pl->hist < 2) ? startup_step(pl, s, rec) : steady_step(pl, pl->n, s);
+  if (st) return st;
+  pl->n += 1;
+  if (pl->hist < 2) pl->hist += 1;
+  pl->explicit_u12 = false;
+  return JFB_OK;
+}
+
+static int record_state(jfb_kmm_plan* pl, AdjRun& R, int slot_idx, cudaStream_t s) {
+  const Dims& d = pl->d;
+  const size_t P = d.P;
+  const int c = slot(pl->n);
+  JFB_CHECK_CUDA(cudaMemcpyAsync(R.TU0 + (size_t)slot_idx * d.nB * P, pl->U0[c],
+                                 (size_t)d.nB * P * sizeof(c64), cudaMemcpyDeviceToDevice, s));
+  JFB_CHECK_CUDA(cudaMemcpyAsync(R.TG + (size_t)slot_idx * d.nD * P, pl->G[c],
+                                 (size_t)d.nD * P * sizeof(c64), cudaMemcpyDeviceToDevice, s));
+  JFB_CHECK_CUDA(cudaMemcpyAsync(R.TVW + (size_t)slot_idx * d.nD, pl->VW[c], (size_t)d.nD * sizeof(c64),
+                                 cudaMemcpyDeviceToDevice, s));
+  return JFB_OK;
+}
+
+}  // namespace jfb
+
+extern "C" int jfb_kmm_gain_gradient(jfb_kmm_plan* pl, const jfb_kmm_state* init, int64_t steps,
+                                     int64_t checkpoint, double* gain_out,
+                                     const jfb_kmm_state* grad, void* stream) {
+  JFB_REQUIRE(pl && init && gain_out, "null pointer");
+  JFB_REQUIRE(!pl->mhd && !pl->mixed, "the adjoint runs on FP64 flow plans");
+  JFB_REQUIRE(steps >= 1, "steps must be >= 1");
+  JFB_REQUIRE(init->history_steps == 0.0, "the initial state must have history_steps == 0");
+  cudaStream_t s = (cudaStream_t)stream;
+  const Dims& d = pl->d;
+  const size_t P = d.P, nBP = (size_t)d.nB * P, nDP = (size_t)d.nD * P;
+  const int64_t T = steps;
+  const int K = (int)std::max<int64_t>(1, std::min<int64_t>(checkpoint > 0 ? checkpoint : T, T));
+  int st = adj_prepare(pl);
+  if (st) return st;
+  // the initial state with a zero history
+  jfb_kmm_state z = *init;
+  for (int k = 0; k < 4; ++k)
+    z.nonlinear_old[k] = z.nonlinear_older[k] = z.solution_old[k] = z.solution_older[k] = nullptr;
+  if ((st = jfb_kmm_set_state(pl, &z, stream))) return st;
+
+  AdjRun R;
+  const size_t f = (size_t)d.Nx * P, fm = (size_t)d.Nx * d.My * d.Kz;
+#define AL(p, n) \
+  if ((st = R.alloc(&(p), (n)))) return st;
+  AL(R.XF, 6 * f);
+  AL(R.YF, 6 * fm);
+  AL(R.AH, 3 * f);
+  AL(R.AW, 3 * fm);
+  AL(R.HZ6, 6 * fm);
+  AL(R.AX, 6 * f);
+  AL(R.U1w, nDP);
+  AL(R.U2w, nDP);
+  AL(R.EU[0], nBP);
+  AL(R.EU[1], nDP);
+  AL(R.EU[2], nDP);
+  auto alloc_state = [&](AState& a) -> int {
+    int e;
+    if ((e = R.alloc(&a.u, nBP))) return e;
+    if ((e = R.alloc(&a.g, nDP))) return e;
+    if ((e = R.alloc(&a.v, nDP))) return e;
+    return R.alloc(&a.w, nDP);
+  };
+  for (int k = 0; k < 4; ++k) {
+    if ((st = alloc_state(R.S[k]))) return st;
+    if ((st = alloc_state(R.Nn[k]))) return st;
+  }
+  if ((st = alloc_state(R.MU))) return st;
+  if ((st = alloc_state(R.Z))) return st;
+  for (int k = 0; k < 3; ++k)
+    if ((st = alloc_state(R.NZ[k]))) return st;
+  AL(R.TU0, (size_t)(K + 1) * nBP);
+  AL(R.TG, (size_t)(K + 1) * nDP);
+  AL(R.TVW, (size_t)(K + 1) * d.nD);
+  for (int n = 0; n < 2; ++n)
+    for (int z1 = 0; z1 < 2; ++z1) {
+      AL(R.rec[n][3 * z1], nBP);
+      AL(R.rec[n][3 * z1 + 1], nDP);
+      AL(R.rec[n][3 * z1 + 2], (size_t)d.nD);
+    }
+  AL(R.IU0, nBP);
+  AL(R.IU1, nDP);
+  AL(R.IU2, nDP);
+  AL(R.IG, nDP);
+  const int nck = (int)((T + K - 1) / K);
+  R.ck_elems = checkpoint_elems(pl);
+  R.ck.resize(nck);
+  for (int k = 0; k < nck; ++k) AL(R.ck[k], R.ck_elems);
+  double* dev8 = nullptr;
+  JFB_CHECK_CUDA(cudaMalloc((void**)&dev8, 10 * sizeof(double)));
+  R.mem.push_back(dev8);
+#undef AL
+
+  // explicit initial leaves and E(0)
+  const int c0 = slot(0);
+  JFB_CHECK_CUDA(cudaMemcpyAsync(R.IU0, pl->U0[c0], nBP * sizeof(c64), cudaMemcpyDeviceToDevice, s));
+  JFB_CHECK_CUDA(cudaMemcpyAsync(R.IG, pl->G[c0], nDP * sizeof(c64), cudaMemcpyDeviceToDevice, s));
+  JFB_CHECK_CUDA(cudaMemcpyAsync(R.IU1, pl->U1S, nDP * sizeof(c64), cudaMemcpyDeviceToDevice, s));
+  JFB_CHECK_CUDA(cudaMemcpyAsync(R.IU2, pl->U2S, nDP * sizeof(c64), cudaMemcpyDeviceToDevice, s));
+  double E0 = 0.0, ET = 0.0;
+  if ((st = perturbation_energy(pl, dev8, s, &E0))) return st;
+  JFB_REQUIRE(std::isfinite(E0) && E0 > 0.0, "initial energy must be positive");
+  if ((st = ensure_H(pl, s))) return st;
+
+  // forward sweep with checkpoints
+  for (int64_t m = 0; m < T; ++m) {
+    if (m % K == 0) {
+      if ((st = checkpoint_io(pl, R.ck[m / K], true, s))) return st;
+    }
+    if ((st = forward_step(pl, s, nullptr))) return st;
+  }
+  if ((st = perturbation_energy(pl, dev8, s, &ET))) return st;
+  const double gain = ET / E0;
+  *gain_out = gain;
+  if (!grad) return JFB_OK;
+
+  // terminal adjoint: grad of E(T) / E(0) through the reconstruction of u(T)
+  const double area = pl->cfg.ly * pl->cfg.lz;
+  for (int k = 0; k < 4; ++k) {
+    if ((st = astate_zero(pl, R.S[k], s))) return st;
+    if ((st = astate_zero(pl, R.Nn[k], s))) return st;
+  }
+  {
+    const int cT = slot(pl->n);
+    if ((st = adj_energy(pl, R, pl->U0[cT], pl->U1S, pl->U2S, 2.0 * area / E0, false, s)))
+      return st;
+    if ((st = adj_recon(pl, R, R.S[T % 4], false, s))) return st;
+  }
+  const double dt = pl->cfg.dt;
+  const double cS[3] = {18.0 / 11.0, -9.0 / 11.0, 2.0 / 11.0};
+  const double dS[3] = {18.0 / 11.0, -18.0 / 11.0, 6.0 / 11.0};
+  auto ring = [](int64_t i) { return (int)(((i % 4) + 4) % 4); };
+  for (int seg = nck - 1; seg >= 0; --seg) {
+    const int64_t a = (int64_t)seg * K, b = std::min<int64_t>(T, a + K);
+    // recompute s_a .. s_b
+    if ((st = checkpoint_io(pl, R.ck[seg], false, s))) return st;
+    pl->n = a;
+    pl->hist = (int)std::min<int64_t>(2, a);
+    pl->have_H = true;
+    pl->explicit_u12 = false;
+    if ((st = record_state(pl, R, 0, s))) return st;
+    for (int64_t m = a; m < b; ++m) {
+      c64* const* rec = (m < 2) ? R.rec[m] : nullptr;
+      if ((st = forward_step(pl, s, rec))) return st;
+      if ((st = record_state(pl, R, (int)(m + 1 - a), s))) return st;
+    }
+    auto su0 = [&](int64_t m) { return R.TU0 + (size_t)(m - a) * nBP; };
+    auto sg = [&](int64_t m) { return R.TG + (size_t)(m - a) * nDP; };
+    auto svw = [&](int64_t m) { return R.TVW + (size_t)(m - a) * d.nD; };
+    for (int64_t n = b - 1; n >= a; --n) {
+      // the nonlinear term of s_{n+1} is complete: fold it into its state adjoint
+      if (n + 1 <= T - 1) {
+        if ((st = adj_nonlinear(pl, R, su0(n + 1), sg(n + 1), svw(n + 1), nullptr, nullptr,
+                                R.Nn[ring(n + 1)], s)))
+          return st;
+        if ((st = adj_recon(pl, R, R.S[ring(n + 1)], true, s))) return st;
+      }
+      if (n >= 2) {
+        if ((st = adj_solve(pl, pl->adj_steady, R.S[ring(n + 1)], R.MU, s))) return st;
+        for (int l = 0; l < 3; ++l) {
+          if ((st = adj_mass(pl, R.MU, cS[l], 0.0, R.S[ring(n - l)], s))) return st;
+          astate_axpy(pl, R.Nn[ring(n - l)], R.MU, dt * dS[l], s);
+        }
+      } else {
+        // IMEXRK3 startup step from s_n: stage states z0 = s_n, z1, z2 (rec)
+        JFB_CHECK_CUDA(cudaMemcpyAsync(R.Z.u, R.S[ring(n + 1)].u, nBP * sizeof(c64),
+                                       cudaMemcpyDeviceToDevice, s));
+        JFB_CHECK_CUDA(cudaMemcpyAsync(R.Z.g, R.S[ring(n + 1)].g, nDP * sizeof(c64),
+                                       cudaMemcpyDeviceToDevice, s));
+        JFB_CHECK_CUDA(cudaMemcpyAsync(R.Z.v, R.S[ring(n + 1)].v, nDP * sizeof(c64),
+                                       cudaMemcpyDeviceToDevice, s));
+        JFB_CHECK_CUDA(cudaMemcpyAsync(R.Z.w, R.S[ring(n + 1)].w, nDP * sizeof(c64),
+                                       cudaMemcpyDeviceToDevice, s));
+        for (int k = 0; k < 3; ++k)
+          if ((st = astate_zero(pl, R.NZ[k], s))) return st;
+        for (int rk = 2; rk >= 0; --rk) {
+          const double gl = (kRK3A[rk] + kRK3B[rk]) * dt / 2.0 * pl->cfg.nu;
+          if ((st = adj_solve(pl, pl->adj_startup[rk], R.Z, R.MU, s))) return st;
+          if ((st = astate_zero(pl, R.Z, s))) return st;
+          if ((st = adj_mass(pl, R.MU, 1.0, gl, R.Z, s))) return st;
+          astate_axpy(pl, R.NZ[rk], R.MU, dt * kRK3A[rk], s);
+          if (rk > 0) astate_axpy(pl, R.NZ[rk - 1], R.MU, dt * kRK3B[rk], s);
+          if (rk > 0) {
+            // the stage state's own nonlinear term is complete
+            c64* const* z = R.rec[n] + 3 * (rk - 1);
+            if ((st = adj_nonlinear(pl, R, z[0], z[1], z[2], nullptr, nullptr, R.NZ[rk], s)))
+              return st;
+            if ((st = adj_recon(pl, R, R.Z, true, s))) return st;
+          }
+        }
+        astate_axpy(pl, R.S[ring(n)], R.Z, 1.0, s);
+        astate_axpy(pl, R.Nn[ring(n)], R.NZ[0], 1.0, s);
+      }
+      // index n + 1 is finished; its ring slot serves index n - 3 next
+      if ((st = astate_zero(pl, R.S[ring(n + 1)], s))) return st;
+      if ((st = astate_zero(pl, R.Nn[ring(n + 1)], s))) return st;
+    }
+  }
+  // explicit leaves: the first nonlinear term (explicit velocity) ...
+  if ((st = adj_nonlinear(pl, R, R.IU0, R.IG, nullptr, R.IU1, R.IU2, R.Nn[ring(0)], s))) return st;
+  // ... minus gain * grad E(0) / E(0) ...
+  if ((st = adj_energy(pl, R, R.IU0, R.IU1, R.IU2, -2.0 * area * gain / E0, true, s))) return st;
+  // ... plus the primary-state adjoint: u0, g, and the means of u1, u2
+  const AState& S0 = R.S[ring(0)];
+  axpy_kernel<<<256, 256, 0, s>>>(R.EU[0], S0.u, 1.0, nBP);
+  {
+    PTermList L = tlist(R.EU[1], d.nD, true);
+    term(L, S0.v, nullptr, d.nD, 0, 1, 0, 0, 0, 0, 2, 1);
+    if ((st = run(pl, L, s))) return st;
+    L = tlist(R.EU[2], d.nD, true);
+    term(L, S0.w, nullptr, d.nD, 0, 1, 0, 0, 0, 0, 2, 1);
+    if ((st = run(pl, L, s))) return st;
+  }
+  JFB_CHECK_LAUNCH();
+  // jax.grad convention (directional derivative Re sum(g d)): conjugate
+  const c64* outs_half[4] = {R.EU[0], R.EU[1], R.EU[2], S0.g};
+  void* outs[4] = {grad->u0, grad->u1, grad->u2, grad->g};
+  const int rows[4] = {d.nB, d.nD, d.nD, d.nD};
+  for (int k = 0; k < 4; ++k) {
+    if (!outs[k]) continue;
+    to_full_kernel<<<512, 256, 0, s>>>(outs_half[k], rows[k], d.Ny, d.Nz, (c64*)outs[k]);
+    conj_kernel<<<512, 256, 0, s>>>((c64*)outs[k], (size_t)rows[k] * d.Ny * d.Nz);
+  }
+  for (int k = 0; k < 4; ++k) {
+    void* const lv[4] = {grad->nonlinear_old[k], grad->nonlinear_older[k], grad->solution_old[k],
+                         grad->solution_older[k]};
+    const size_t bytes = (k < 2) ? (size_t)rows[k == 0 ? 0 : 3] * d.Ny * d.Nz * sizeof(c64)
+                                 : (size_t)d.nD * sizeof(double);
+    for (void* p : lv)
+      if (p) JFB_CHECK_CUDA(cudaMemsetAsync(p, 0, bytes, s));
+  }
+  JFB_CHECK_LAUNCH();
+  JFB_CHECK_CUDA(cudaStreamSynchronize(s));
+  pl->have_state = false;  // the plan's state was consumed by the sweep
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_energy_gradient(jfb_kmm_plan* pl, const jfb_kmm_state* state,
+                                       const jfb_kmm_state* grad, void* stream) {
+  JFB_REQUIRE(pl && state && grad && grad->u0 && grad->u1 && grad->u2, "null pointer");
+  JFB_REQUIRE(!pl->mhd, "flow plans only");
+  int st = adj_prepare(pl);
+  if (st) return st;
+  jfb_kmm_state z = *state;
+  for (int k = 0; k < 4; ++k)
+    z.nonlinear_old[k] = z.nonlinear_older[k] = z.solution_old[k] = z.solution_older[k] = nullptr;
+  z.history_steps = 0.0;
+  if ((st = jfb_kmm_set_state(pl, &z, stream))) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const Dims& d = pl->d;
+  AdjRun R;
+  const size_t P = d.P;
+  if ((st = R.alloc(&R.EU[0], (size_t)d.nB * P))) return st;
+  if ((st = R.alloc(&R.EU[1], (size_t)d.nD * P))) return st;
+  if ((st = R.alloc(&R.EU[2], (size_t)d.nD * P))) return st;
+  const double area = pl->cfg.ly * pl->cfg.lz;
+  if ((st = adj_energy(pl, R, pl->U0[slot(0)], pl->U1S, pl->U2S, 2.0 * area, false, s))) return st;
+  void* outs[3] = {grad->u0, grad->u1, grad->u2};
+  const int rows[3] = {d.nB, d.nD, d.nD};
+  for (int k = 0; k < 3; ++k) {
+    to_full_kernel<<<512, 256, 0, s>>>(R.EU[k], rows[k], d.Ny, d.Nz, (c64*)outs[k]);
+    conj_kernel<<<512, 256, 0, s>>>((c64*)outs[k], (size_t)rows[k] * d.Ny * d.Nz);
+  }
+  if (grad->g) JFB_CHECK_CUDA(cudaMemsetAsync(grad->g, 0, (size_t)d.nD * d.Ny * d.Nz * sizeof(c64), s));
+  JFB_CHECK_LAUNCH();
+  JFB_CHECK_CUDA(cudaStreamSynchronize(s));
   return JFB_OK;
 }

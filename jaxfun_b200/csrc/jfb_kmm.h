@@ -57,6 +57,13 @@ struct GemmHost {
   // of TD projections of its derivatives: B1 = V S_D^T, B2 = V D S_D^T,
   // C1 = V S_D^T M_D^-1 S_D W D S_D^T, C2 = V S_D^T M_D^-1 S_D W D^2 S_D^T
   std::vector<double> B1, B2, C1, C2;
+  // Adjoint of the step: A0 = V S_B^T (N x nB), F = M_D^-1 S_D W D S_B^T
+  // (nD x nB, the TD projection of d/dx of a TB field), the nonlinear-row
+  // operators R0 = S_B W Pi, R1 = S_B W D Pi (nB x N), R2 = S_D W Pi (nD x N)
+  // with Pi = S_D^T M_D^-1 S_D Q, and the energy Gram matrices
+  // GB = A0^T diag(w) A0 (nB x nB), GD = B1^T diag(w) B1 (nD x nD), w the
+  // Fejer weights.  All row-major.
+  std::vector<double> A0, F, R0, R1, R2, GB, GD;
 };
 
 Stencil make_stencil(int N, bool biharmonic);

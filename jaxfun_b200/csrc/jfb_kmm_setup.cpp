@@ -506,6 +506,15 @@ bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& er
     gh.B2 = dense(B2);
     gh.C1 = dense(C1);
     gh.C2 = dense(C2);
+    gh.A0 = dense(A0);
+    gh.F = dense(F);
+    gh.R0 = dense(R0);
+    gh.R1 = dense(R1);
+    gh.R2 = dense(R2);
+    LMat Wf(N, N);
+    for (int j = 0; j < N; ++j) Wf(j, j) = (LD)op.fejer[j];
+    gh.GB = dense(mul(mul(transpose(A0), Wf), A0));
+    gh.GD = dense(mul(mul(transpose(B1), Wf), B1));
   }
   gh.R3.assign((size_t)nD * N, 0.0);
   for (int i = 0; i < nD; ++i)
