@@ -60,6 +60,10 @@ def parse_args(argv=None):
     p.add_argument("--grid", default="65,64,64")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true",
+                   help="skip the adjoint / minimal-seed block")
+    p.add_argument("--adjoint-steps", type=int, default=200)
+    p.add_argument("--ascent-iterations", type=int, default=20)
     return p.parse_args(argv)
 
 
@@ -469,9 +473,71 @@ def main(argv=None):
             out[f"after_{n}_steps"] = errs
         return out
 
+    def adjoint_block():
+        """The adjoint / minimal-seed workload: gain E(T)/E(0) over
+        --adjoint-steps FP64 SBDF3 steps of the same Couette problem, its
+        gradient by the hand-written adjoint (recompute checkpoint every 20
+        steps), central FD (eps 1e-6) along 8 seeded divergence-free
+        directions (seeds 200..207), then --ascent-iterations projected-gradient
+        ascent iterations at fixed initial energy 1e-4."""
+        from jaxfun_b200 import minimal_seed as ms
+
+        T, ck = args.adjoint_steps, 20
+        g64 = PlaneCouetteFluctuation(N=grid, domain=domain(), Re=RE, dt=DT, device=dev)
+        e0 = g64.diagnostics(g64.state_from_physical(fields0))["Epert"]
+        x0 = ms._primary(g64.state_from_physical(scale_to_energy(fields0, e0, ENERGY)))
+        ms.gain_and_gradient(g64, x0, 4, checkpoint=2)  # operators and bands, untimed
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        gain_f, _ = ms.gain_and_gradient(g64, x0, T, checkpoint=ck, with_gradient=False)
+        torch.cuda.synchronize(dev)
+        t1 = time.perf_counter()
+        gain, grad = ms.gain_and_gradient(g64, x0, T, checkpoint=ck)
+        torch.cuda.synchronize(dev)
+        t2 = time.perf_counter()
+        fd = []
+        for m in range(8):
+            f = couette_perturbation_fields(grid, domain(), seeds=(200 + m, 300 + m))
+            d = ms._primary(g64.state_from_physical(f))
+            d = ms.tree_scale(d, ms.tree_l2_norm(x0) / ms.tree_l2_norm(d))
+            eps = 1e-6
+            jp = ms.perturbation_gain(g64, ms.tree_add_scaled(x0, d, eps), T)
+            jm = ms.perturbation_gain(g64, ms.tree_add_scaled(x0, d, -eps), T)
+            fdv = (jp - jm) / (2 * eps)
+            adj = ms.jax_complex_directional_derivative(grad, d)
+            fd.append({"seed": 200 + m, "adjoint": adj, "fd": fdv,
+                       "rel_err": abs(adj - fdv) / max(abs(fdv), 1e-300)})
+        t3 = time.perf_counter()
+        _, hist = ms.minimal_seed_ascent(g64, x0, target_energy=ENERGY, steps=T,
+                                         iterations=args.ascent_iterations, step_size=1.0,
+                                         checkpoint=ck)
+        torch.cuda.synchronize(dev)
+        t4 = time.perf_counter()
+        return {
+            "workload": f"{T} FP64 SBDF3 steps (2 IMEXRK3 startup) of the Couette workload, "
+                        f"gain E(T)/E(0), checkpoint every {ck} steps",
+            "gain": gain,
+            "forward_s": t1 - t0,
+            "gain_and_gradient_s": t2 - t1,
+            "gradient_over_forward": (t2 - t1) / max(t1 - t0, 1e-12),
+            "fd_check": {"eps": 1e-6, "directions": fd,
+                         "max_rel_err": max(r["rel_err"] for r in fd)},
+            "fd_s": t3 - t2,
+            "ascent": {
+                "iterations": len(hist),
+                "accepted": sum(1 for h in hist if h.accepted),
+                "gain_first": hist[0].gain if hist else None,
+                "gain_last": hist[-1].gain if hist else None,
+                "gains": [h.gain for h in hist],
+                "seconds": t4 - t3,
+            },
+            "reference_jax_grad": "unavailable: jax is not installed on this host",
+        }
+
     forms = ("mixed", "fp64") if args.precision == "both" else (args.precision,)
     results = {p: measure(p) for p in forms}
     err = mixed_error() if "mixed" in forms and rank == 0 else None
+    adj = adjoint_block() if (rank == 0 and world == 1 and not args.no_adjoint) else None
 
     if rank != 0:
         if world > 1:
@@ -506,6 +572,8 @@ def main(argv=None):
                                      "kernel_ms", "graph_l2_resident", "e2e", "gpu_launches")}
     if err is not None:
         line["mixed_vs_fp64_rel_l2"] = err
+    if adj is not None:
+        line["adjoint"] = adj
     if world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         rate, n = cpu_oracle_rate(fields, grid, args.cpu_seconds, threads)
