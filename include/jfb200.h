@@ -233,15 +233,29 @@ typedef struct jfb_mhd_state {
   void* A_older[3];
 } jfb_mhd_state;
 
+/* Magnetic parameters.  PlaneCouetteMHDJax (pcf_mhd_jax.py:76-115):
+ * eta = U_wall / Rm, omega = 0, b0 = 0.  PlaneCouetteMRIShearpyJax
+ * (pcf_mhd_mri_shearpy_jax.py:36-97, 149-176): eta = 1 / Rm, the rotation
+ * rate omega (Coriolis term -2 omega e_z x u in the momentum nonlinear term)
+ * and the imposed uniform field b0 (added to B in the Lorentz force and the
+ * EMF); its base flow U_b = -shear_rate x is jfb_kmm_config.u_wall =
+ * -shear_rate with nu = 1 / Re. */
+typedef struct jfb_mhd_params {
+  double eta;    /* magnetic diffusivity                     */
+  double omega;  /* rotation rate of the frame               */
+  double b0[3];  /* imposed uniform magnetic field (x, y, z) */
+} jfb_mhd_params;
+
 /* PlaneCouetteMHDJax.__init__ + _build_A_operators (pcf_mhd_jax.py:76-143):
- * the flow plan of jfb_kmm_create plus the A systems MA - gamma LA with
- * eta = u_wall / rm (steady SBDF3 and the three IMEXRK3 startup stages).
- * FP64 only (JFB_ERR_ARG for JFB_PRECISION_MIXED).  All other jfb_kmm_*
- * entry points accept the plan; jfb_kmm_advance / jfb_kmm_timed_steps then
- * advance the coupled flow + A system (_step_sbdf3_mhd, pcf_mhd_jax.py:
- * 563-715; Lorentz force in the momentum nonlinear term, EMF in the A
- * equation) and jfb_kmm_convection returns H with the Lorentz force. */
-int jfb_mhd_create(const jfb_kmm_config* cfg, double rm, jfb_kmm_plan** plan);
+ * the flow plan of jfb_kmm_create plus the A systems MA - gamma eta LA
+ * (steady SBDF3 and the three IMEXRK3 startup stages).  FP64 only
+ * (JFB_ERR_ARG for JFB_PRECISION_MIXED).  All other jfb_kmm_* entry points
+ * accept the plan; jfb_kmm_advance / jfb_kmm_timed_steps then advance the
+ * coupled flow + A system (_step_sbdf3_mhd, pcf_mhd_jax.py:563-715; Lorentz
+ * force in the momentum nonlinear term, EMF in the A equation) and
+ * jfb_kmm_convection returns H with the Lorentz force. */
+int jfb_mhd_create(const jfb_kmm_config* cfg, const jfb_mhd_params* params,
+                   jfb_kmm_plan** plan);
 
 /* Load / store the full MHDState; the flow part as jfb_kmm_set_state /
  * jfb_kmm_get_state.  NULL A-history pointers load zeros (get: skipped). */
@@ -266,6 +280,20 @@ int jfb_mhd_convection(jfb_kmm_plan* plan, void* h0, void* h1, void* h2, void* h
  * state: device array out[10] = the eight values of jfb_kmm_diagnostics,
  * then divB_L2 and Emag. */
 int jfb_mhd_diagnostics(jfb_kmm_plan* plan, double* out, void* stream);
+
+/* ---- ensembles ------------------------------------------------------------ */
+
+/* Independent members (flow or MHD plans, any sizes; no reference counterpart:
+ * the reference runs members one solver at a time) advanced together.  Each
+ * steady step is one CUDA graph holding every member's step on its own
+ * stream, so members of uneven wall-normal size run concurrently.  Members
+ * keep their own states (jfb_kmm_set_state / jfb_mhd_set_state, get_state);
+ * all must share the step phase and history count when advanced.  Destroy
+ * the ensemble before its members. */
+typedef struct jfb_ensemble jfb_ensemble;
+int jfb_ensemble_create(jfb_kmm_plan* const* plans, int32_t n, jfb_ensemble** ensemble);
+int jfb_ensemble_advance(jfb_ensemble* ensemble, int64_t steps, void* stream);
+int jfb_ensemble_destroy(jfb_ensemble* ensemble);
 
 #ifdef __cplusplus
 }

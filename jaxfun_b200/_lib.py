@@ -78,6 +78,16 @@ class MHDStateC(ctypes.Structure):
     ]
 
 
+class MHDParams(ctypes.Structure):
+    """``jfb_mhd_params``."""
+
+    _fields_ = [
+        ("eta", c_double),
+        ("omega", c_double),
+        ("b0", c_double * 3),
+    ]
+
+
 class KMMInfo(ctypes.Structure):
     _fields_ = [
         ("n_pencils", c_int64),
@@ -132,7 +142,10 @@ SIGNATURES = {
     "jfb_kmm_energy_gradient": (
         c_int, [c_void_p, POINTER(KMMStateC), POINTER(KMMStateC), c_void_p]
     ),
-    "jfb_mhd_create": (c_int, [POINTER(KMMConfig), c_double, POINTER(c_void_p)]),
+    "jfb_mhd_create": (c_int, [POINTER(KMMConfig), POINTER(MHDParams), POINTER(c_void_p)]),
+    "jfb_ensemble_create": (c_int, [POINTER(c_void_p), c_int32, POINTER(c_void_p)]),
+    "jfb_ensemble_advance": (c_int, [c_void_p, c_int64, c_void_p]),
+    "jfb_ensemble_destroy": (c_int, [c_void_p]),
     "jfb_mhd_set_state": (c_int, [c_void_p, POINTER(MHDStateC), c_void_p]),
     "jfb_mhd_get_state": (c_int, [c_void_p, POINTER(MHDStateC), c_void_p]),
     "jfb_mhd_potential_from_physical": (

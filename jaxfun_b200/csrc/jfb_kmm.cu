@@ -246,6 +246,7 @@ struct jfb_kmm_plan {
   // MHD (vector potential A, three Dirichlet components per level)
   bool mhd = false;
   double eta = 0.0;
+  jfb::MhdPhys mphys = {0.0, 0.0, 0.0, 0.0};
   jfb::MhdOps mops;
   double *sa_steady = nullptr, *sa_startup[3] = {nullptr, nullptr, nullptr};
   jfb::c64 *AR[3], *NA[3], *NAst;
@@ -638,7 +639,8 @@ static int launch_transforms_mhd(jfb_kmm_plan* pl, cudaStream_t s) {
   JFB_CHECK_LAUNCH();
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[2], s));
   const int zb = ceil_div((int64_t)d.Nx * d.My, kZRows);
-  z_cross_mhd_kernel<<<zb, 256, pl->smem_zm, s>>>(pl->ops, d, pl->fz, pl->twz, pl->Y, pl->HZ);
+  z_cross_mhd_kernel<<<zb, 256, pl->smem_zm, s>>>(pl->ops, d, pl->mphys, pl->fz, pl->twz, pl->Y,
+                                                  pl->HZ);
   JFB_CHECK_LAUNCH();
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[3], s));
   dim3 gf(d.Nx, 6, d.Kz / pl->KC);
@@ -878,7 +880,8 @@ static void destroy_graphs(jfb_kmm_plan* pl) {
 
 using namespace jfb;
 
-static int create_plan(const jfb_kmm_config* cfg, bool mhd, double rm, jfb_kmm_plan** out) {
+static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
+                       jfb_kmm_plan** out) {
   JFB_REQUIRE(cfg && out, "null pointer");
   *out = nullptr;
   JFB_REQUIRE(cfg->family == JFB_FAMILY_CHEBYSHEV, "only the Chebyshev family is supported");
@@ -893,8 +896,11 @@ static int create_plan(const jfb_kmm_config* cfg, bool mhd, double rm, jfb_kmm_p
   JFB_REQUIRE(cfg->x_hi > cfg->x_lo && cfg->ly > 0 && cfg->lz > 0, "bad domain");
   jfb_kmm_plan* pl = new jfb_kmm_plan();
   pl->cfg = *cfg;
-  pl->mhd = mhd;
-  pl->eta = mhd ? cfg->u_wall / rm : 0.0;
+  pl->mhd = mhd != nullptr;
+  if (mhd) {
+    pl->eta = mhd->eta;
+    pl->mphys = MhdPhys{mhd->b0[0], mhd->b0[1], mhd->b0[2], 2.0 * mhd->omega};
+  }
   int st = JFB_OK;
   auto fail = [&](int code) {
     jfb_kmm_destroy(pl);
@@ -1267,15 +1273,19 @@ static int create_plan(const jfb_kmm_config* cfg, bool mhd, double rm, jfb_kmm_p
 }
 
 extern "C" int jfb_kmm_create(const jfb_kmm_config* cfg, jfb_kmm_plan** out) {
-  return create_plan(cfg, false, 0.0, out);
+  return create_plan(cfg, nullptr, out);
 }
 
-extern "C" int jfb_mhd_create(const jfb_kmm_config* cfg, double rm, jfb_kmm_plan** out) {
-  JFB_REQUIRE(cfg && out, "null pointer");
+extern "C" int jfb_mhd_create(const jfb_kmm_config* cfg, const jfb_mhd_params* prm,
+                              jfb_kmm_plan** out) {
+  JFB_REQUIRE(cfg && prm && out, "null pointer");
   *out = nullptr;
-  JFB_REQUIRE(rm > 0.0 && std::isfinite(rm), "rm must be positive");
+  JFB_REQUIRE(prm->eta > 0.0 && std::isfinite(prm->eta), "eta must be positive");
+  JFB_REQUIRE(std::isfinite(prm->omega) && std::isfinite(prm->b0[0]) &&
+                  std::isfinite(prm->b0[1]) && std::isfinite(prm->b0[2]),
+              "omega and b0 must be finite");
   JFB_REQUIRE(cfg->precision == JFB_PRECISION_FP64, "the MHD step runs in FP64 only");
-  return create_plan(cfg, true, rm, out);
+  return create_plan(cfg, prm, out);
 }
 
 extern "C" int jfb_kmm_destroy(jfb_kmm_plan* pl) {
@@ -2341,5 +2351,118 @@ extern "C" int jfb_kmm_energy_gradient(jfb_kmm_plan* pl, const jfb_kmm_state* st
   if (grad->g) JFB_CHECK_CUDA(cudaMemsetAsync(grad->g, 0, (size_t)d.nD * d.Ny * d.Nz * sizeof(c64), s));
   JFB_CHECK_LAUNCH();
   JFB_CHECK_CUDA(cudaStreamSynchronize(s));
+  return JFB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Ensembles: independent members (any mix of flow / MHD plans and sizes)
+// advanced together, one CUDA graph per steady step holding every member's
+// step on its own stream (fork / join inside the capture), so members of
+// uneven wall-normal size run concurrently.
+// ---------------------------------------------------------------------------
+
+struct jfb_ensemble {
+  std::vector<jfb_kmm_plan*> m;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> join;
+  cudaStream_t cap = nullptr;
+  cudaEvent_t fork = nullptr;
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+};
+
+extern "C" int jfb_ensemble_destroy(jfb_ensemble* e) {
+  if (!e) return JFB_OK;
+  for (auto& g : e->graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (cudaStream_t s : e->streams) cudaStreamDestroy(s);
+  for (cudaEvent_t ev : e->join) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->cap) cudaStreamDestroy(e->cap);
+  delete e;
+  return JFB_OK;
+}
+
+extern "C" int jfb_ensemble_create(jfb_kmm_plan* const* plans, int32_t n, jfb_ensemble** out) {
+  JFB_REQUIRE(plans && out && n >= 1, "null pointer or empty ensemble");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) JFB_REQUIRE(plans[i], "null member plan");
+  jfb_ensemble* e = new jfb_ensemble();
+  e->m.assign(plans, plans + n);
+  auto fail = [&](cudaError_t err) {
+    set_error(std::string("CUDA error: ") + cudaGetErrorString(err));
+    jfb_ensemble_destroy(e);
+    return JFB_ERR_CUDA;
+  };
+  cudaError_t err;
+  if ((err = cudaStreamCreateWithFlags(&e->cap, cudaStreamNonBlocking)) != cudaSuccess) return fail(err);
+  if ((err = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming)) != cudaSuccess) return fail(err);
+  e->streams.resize(n, nullptr);
+  e->join.resize(n, nullptr);
+  for (int i = 0; i < n; ++i) {
+    if ((err = cudaStreamCreateWithFlags(&e->streams[i], cudaStreamNonBlocking)) != cudaSuccess)
+      return fail(err);
+    if ((err = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming)) != cudaSuccess)
+      return fail(err);
+  }
+  *out = e;
+  return JFB_OK;
+}
+
+extern "C" int jfb_ensemble_advance(jfb_ensemble* e, int64_t steps, void* stream) {
+  JFB_REQUIRE(e, "null pointer");
+  JFB_REQUIRE(steps >= 0, "steps must be >= 0");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int n = (int)e->m.size();
+  for (jfb_kmm_plan* pl : e->m) {
+    if (!pl->have_state) {
+      set_error("an ensemble member has no state loaded");
+      return JFB_ERR_STATE;
+    }
+    if (slot(pl->n) != slot(e->m[0]->n) || pl->hist != e->m[0]->hist) {
+      set_error("ensemble members must share the step phase and history count");
+      return JFB_ERR_STATE;
+    }
+  }
+  int st;
+  for (jfb_kmm_plan* pl : e->m)
+    if ((st = ensure_H(pl, s))) return st;
+  while (steps > 0 && e->m[0]->hist < 2) {
+    for (jfb_kmm_plan* pl : e->m) {
+      if ((st = startup_step(pl, s))) return st;
+      pl->n += 1;
+      pl->hist += 1;
+      pl->explicit_u12 = false;
+    }
+    --steps;
+  }
+  while (steps > 0) {
+    const int k = slot(e->m[0]->n);
+    if (!e->graph[k]) {
+      cudaGraph_t g;
+      JFB_CHECK_CUDA(cudaStreamBeginCapture(e->cap, cudaStreamCaptureModeThreadLocal));
+      int rc = JFB_OK;
+      cudaError_t ce = cudaEventRecord(e->fork, e->cap);
+      for (int i = 0; i < n && rc == JFB_OK && ce == cudaSuccess; ++i) {
+        ce = cudaStreamWaitEvent(e->streams[i], e->fork, 0);
+        if (ce != cudaSuccess) break;
+        rc = steady_step(e->m[i], e->m[i]->n, e->streams[i]);
+        if (rc) break;
+        ce = cudaEventRecord(e->join[i], e->streams[i]);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->cap, e->join[i], 0);
+      }
+      cudaError_t ec = cudaStreamEndCapture(e->cap, &g);
+      if (rc) return rc;
+      JFB_CHECK_CUDA(ce);
+      JFB_CHECK_CUDA(ec);
+      JFB_CHECK_CUDA(cudaGraphInstantiate(&e->graph[k], g, 0));
+      cudaGraphDestroy(g);
+    }
+    JFB_CHECK_CUDA(cudaGraphLaunch(e->graph[k], s));
+    for (jfb_kmm_plan* pl : e->m) {
+      pl->n += 1;
+      pl->explicit_u12 = false;
+    }
+    --steps;
+  }
   return JFB_OK;
 }

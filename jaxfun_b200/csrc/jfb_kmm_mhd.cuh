@@ -47,6 +47,14 @@ struct MhdOps {
 
 enum MhdMode { kMhdStep = 0, kMhdFields = 1, kMhdFromPhys = 2 };
 
+// Imposed uniform field B0 (added to b in the Lorentz force and the EMF) and
+// the Coriolis term of a rotating frame, n += -2 Omega e_z x u
+// (pcf_mhd_mri_shearpy_jax.py:149-176).
+struct MhdPhys {
+  double b0x, b0y, b0z;
+  double two_omega;
+};
+
 struct MhdArgs {
   int mode;
   const c64* HXA;  // EMF (kMhdStep) or physical samples (kMhdFromPhys): 3 x [Nx][P]
@@ -298,10 +306,12 @@ __global__ void __launch_bounds__(kMhdThreads, 1) mhd_a_kernel(Dims d, DevOps o,
 // spectra (u, omega, b, j) -> six packed complex inverse FFTs, the products
 //   n = -(u_t x omega_t) - j x b,   emf = (u + U_b e_y) x b
 // (_mhd_convection, pcf_mhd_jax.py:339-357; the flow part in the split form
-// of rotational_product, whose constant base-flow term the y stage adds),
-// then three packed forward transforms: HZ fields (n_x, n_y, n_z, e_x, e_y, e_z).
+// of rotational_product, whose constant base-flow term the y stage adds; b
+// includes the imposed field and n the Coriolis term of MhdPhys), then three
+// packed forward transforms: HZ fields (n_x, n_y, n_z, e_x, e_y, e_z).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) z_cross_mhd_kernel(DevOps o, Dims d, FFTPlan plan,
+__global__ void __launch_bounds__(256) z_cross_mhd_kernel(DevOps o, Dims d, MhdPhys ph,
+                                                          FFTPlan plan,
                                                           const c64* __restrict__ tw,
                                                           const c64* __restrict__ Y,
                                                           c64* __restrict__ HZ) {
@@ -344,11 +354,13 @@ __global__ void __launch_bounds__(256) z_cross_mhd_kernel(DevOps o, Dims d, FFTP
     const c64* z = phys + n * NC + rl * 6;
     const double u0 = z[0].re, u1 = z[0].im, u2 = z[1].re;
     const double w0 = z[1].im, w1 = z[2].re, w2 = z[2].im;
-    const double b0 = z[3].re, b1 = z[3].im, b2 = z[4].re;
+    const double b0 = z[3].re + ph.b0x, b1 = z[3].im + ph.b0y, b2 = z[4].re + ph.b0z;
     const double j0 = z[4].im, j1 = z[5].re, j2 = z[5].im;
     const double ub = d.uwall * o.xphys[j];
     double n0, n1, n2;
     rotational_product(u0, u1, u2, w0, w1, w2, ub, d.uwall, n0, n1, n2);
+    n0 -= ph.two_omega * u1;
+    n1 += ph.two_omega * u0;
     n0 -= j1 * b2 - j2 * b1;
     n1 -= j2 * b0 - j0 * b2;
     n2 -= j0 * b1 - j1 * b0;

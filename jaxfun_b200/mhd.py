@@ -78,8 +78,17 @@ class PlaneCouetteMHD(PlaneCouetteFluctuation):
             device=device,
         )
 
+    # imposed field and rotation rate (PlaneCouetteMRIShearpy sets them)
+    background_b = (0.0, 0.0, 0.0)
+    omega = 0.0
+
     def _create_plan(self, cfg: _lib.KMMConfig, handle: ctypes.c_void_p) -> None:
-        _lib.call("jfb_mhd_create", ctypes.byref(cfg), self.Rm, ctypes.byref(handle))
+        prm = _lib.MHDParams()
+        prm.eta = self.eta
+        prm.omega = float(self.omega)
+        for k in range(3):
+            prm.b0[k] = float(self.background_b[k])
+        _lib.call("jfb_mhd_create", ctypes.byref(cfg), ctypes.byref(prm), ctypes.byref(handle))
 
     # -- plumbing -------------------------------------------------------------
     def _c_mhd_state(self, st: MHDState) -> _lib.MHDStateC:
@@ -213,5 +222,134 @@ class PlaneCouetteMHD(PlaneCouetteFluctuation):
         return out[:3], out[3:]
 
 
-# reference name
+class PlaneCouetteMRIShearpy(PlaneCouetteMHD):
+    """Rotating-shear plane-Couette MHD (pcf_mhd_mri_shearpy_jax.py:30-176):
+    base flow U_b = -shear_rate x, Coriolis -2 omega e_z x u, imposed uniform
+    field ``background_b`` in the Lorentz force and the EMF, nu = 1/Re,
+    eta = 1/Rm.  The channel-mode seed of ``initial_state`` follows
+    pcf_mhd_mri_shearpy_jax.py:99-147 (magnetic_seed "ax_yz" or
+    "sinusoidal_bz_x")."""
+
+    def __init__(
+        self,
+        N=(17, 16, 16),
+        domain=((-1.0, 1.0), (0.0, 4.0 * math.pi), (0.0, 2.0 * math.pi)),
+        Re: float = 400.0,
+        Rm: float | None = None,
+        omega: float = 1.0,
+        shear_rate: float = 1.0,
+        background_b=(0.0, 0.0, 0.025),
+        dt: float = 0.01,
+        family: str = "C",
+        padding_factor=(1.0, 1.5, 1.5),
+        perturbation_amplitude: float = 0.05,
+        magnetic_amplitude: float = 0.0,
+        magnetic_seed: str = "ax_yz",
+        time_integrator: str | None = "SBDF3",
+        nonlinear_form: str = "rotational",
+        coefficient_path: str = "transform",
+        solve_batching: str = "batched",
+        device="cuda",
+    ) -> None:
+        from .kmm import KMM
+
+        self.omega = float(omega)
+        self.shear_rate = float(shear_rate)
+        self.background_b = tuple(float(v) for v in background_b)
+        if magnetic_seed not in {"ax_yz", "sinusoidal_bz_x"}:
+            raise ValueError("magnetic_seed must be one of {ax_yz, sinusoidal_bz_x}")
+        self.magnetic_seed = magnetic_seed
+        self.Re = float(Re)
+        self.U_wall = 1.0
+        self.Rm = float(Re if Rm is None else Rm)
+        self.eta = 1.0 / self.Rm
+        self.magnetic_amplitude = float(magnetic_amplitude)
+        self.perturbation_amplitude = float(perturbation_amplitude)
+        KMM.__init__(
+            self, N=N, domain=domain, nu=1.0 / self.Re, dt=dt, family=family,
+            padding_factor=padding_factor, time_integrator=time_integrator,
+            nonlinear_form=nonlinear_form, coefficient_path=coefficient_path,
+            solve_batching=solve_batching, precision="fp64", device=device,
+            _u_wall=-self.shear_rate,
+        )
+        self.dUb_dx = -self.shear_rate
+
+    def initial_state(self) -> MHDState:
+        """The shearpy MRI channel-mode seed (pcf_mhd_mri_shearpy_jax.py:99-147)."""
+        x, y, z = self.mesh()
+        (a, b) = self.domain[0]
+        xc, hw = 0.5 * (a + b), 0.5 * (b - a)
+        wall = 1.0 - ((x - xc) / hw) ** 2
+        amp = self.perturbation_amplitude
+        Ly = self.domain[1][1] - self.domain[1][0]
+        Lz = self.domain[2][1] - self.domain[2][0]
+        ky, kz = 2.0 * math.pi / Ly, 2.0 * math.pi / Lz
+        shape = self.N
+        zero = torch.zeros(shape, dtype=torch.float64, device=self.device)
+        u0, u1, u2 = zero, zero, zero
+        if amp != 0.0:
+            for h in (1, 2, 3):
+                u0 = u0 + amp * wall * torch.cos(h * kz * z)
+                u1 = u1 + amp * wall * torch.sin(h * kz * z)
+            u0 = u0 + 0.1 * amp * wall * torch.sin(ky * y) * torch.cos(kz * z)
+            u1 = u1 + 0.1 * amp * wall * torch.cos(ky * y) * torch.sin(kz * z)
+            u2 = u2 + 0.1 * amp * wall * torch.sin(2.0 * ky * y) * torch.cos(2.0 * kz * z)
+        flow = self.state_from_physical((u0, u1, u2))
+        mag = self.magnetic_amplitude
+        ax, ay, az = zero, zero, zero
+        if mag != 0.0 and self.magnetic_seed == "ax_yz":
+            ax = mag * wall * (1.0 / kz) * torch.sin(ky * y) * torch.sin(kz * z)
+        elif mag != 0.0:
+            xi = (x - xc) / hw
+            ay = ay - (mag * hw / math.pi) * (torch.cos(math.pi * xi) + 1.0)
+        A = self._A_state_from_physical((ax, ay, az))
+        return self._ensure_mhd_history(MHDState(flow=flow, A=A))
+
+
+class Ensemble:
+    """Independent solvers (flow or MHD, any sizes) advanced together: one
+    CUDA graph per step with every member on its own stream
+    (``jfb_ensemble_*``).  ``solve(states, steps)`` takes and returns one state
+    per member."""
+
+    def __init__(self, members) -> None:
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*(m._plan.value for m in self.members))
+        handle = ctypes.c_void_p()
+        _lib.call("jfb_ensemble_create", arr, len(self.members), ctypes.byref(handle))
+        self._handle = handle
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.load().jfb_ensemble_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
+
+    def load(self, states) -> None:
+        for m, st in zip(self.members, states, strict=True):
+            m._load(st)
+
+    def advance_resident(self, steps: int) -> None:
+        stream = self.members[0]._stream()
+        _lib.call("jfb_ensemble_advance", self._handle, int(steps), stream)
+        for m in self.members:
+            m._current = None
+
+    def solve(self, states, steps: int):
+        self.load(states)
+        hist = [float(m._current.flow.history_steps if isinstance(m._current, MHDState)
+                      else m._current.history_steps) for m in self.members]
+        self.advance_resident(steps)
+        out = []
+        for m, h in zip(self.members, hist, strict=True):
+            h = min(2.0, h + int(steps))
+            out.append(m._fetch_mhd(h) if isinstance(m, PlaneCouetteMHD) else m._fetch(h))
+        return out
+
+
+# reference names
 PlaneCouetteMHDJax = PlaneCouetteMHD
+PlaneCouetteMRIShearpyJax = PlaneCouetteMRIShearpy

@@ -1424,14 +1424,23 @@ class PlaneCouetteMHDOracle(PlaneCouetteOracle):
     def _cross(a, b):
         return (a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0])
 
+    # imposed field and rotation (zero here; PlaneCouetteMRIOracle sets them)
+    background_b = (0.0, 0.0, 0.0)
+    omega = 0.0
+
     def mhd_convection(self, state: MHDState):
-        """pcf_mhd_jax.py:331-346: H = TD[-(u_t x w_t) - J x B], HA = TD[(u + U_b) x B]."""
+        """pcf_mhd_jax.py:331-346: H = TD[-(u_t x w_t) - J x B], HA = TD[(u + U_b) x B];
+        with pcf_mhd_mri_shearpy_jax.py:149-176, B includes the imposed field
+        and H the Coriolis term -2 omega e_z x u."""
         flow = state.flow
         n = self.convection_physical(flow.u)
         up = self.backward_velocity(flow.u, padded=True)
+        if self.omega != 0.0:
+            n = (n[0] - 2.0 * self.omega * up[1], n[1] + 2.0 * self.omega * up[0], n[2])
         B = self.update_B_from_A(state.A)
         J = self.update_J_from_B(B)
         bp = self._backward_vec(B, self.b_spaces, True)
+        bp = tuple(b + b0 for b, b0 in zip(bp, self.background_b, strict=True))
         jp = self._backward_vec(J, self.j_spaces, True)
         lorentz = self._cross(jp, bp)
         n = tuple(ni - li for ni, li in zip(n, lorentz, strict=True))
@@ -1558,3 +1567,24 @@ class PlaneCouetteMHDOracle(PlaneCouetteOracle):
         out["divB_L2"] = self.magnetic_divergence_l2(state)
         out["Emag"] = emag
         return out
+
+
+class PlaneCouetteMRIOracle(PlaneCouetteMHDOracle):
+    """PlaneCouetteMRIShearpyJax's dynamics (pcf_mhd_mri_shearpy_jax.py:36-176):
+    nu = 1/Re, eta = 1/Rm (U_wall = 1 in the parent), base flow
+    U_b = -shear_rate x, Coriolis -2 omega e_z x u, imposed field B0.  The
+    initial state is the parent's (tests load their own states)."""
+
+    def __init__(self, N=(17, 16, 16), Re=400.0, Rm=None, omega=1.0, shear_rate=1.0,
+                 background_b=(0.0, 0.0, 0.025), dt=0.01, perturbation_amplitude=0.05,
+                 magnetic_amplitude=0.0, **kw):
+        super().__init__(N=N, Re=Re, Rm=Rm, U_wall=1.0, dt=dt,
+                         perturbation_amplitude=perturbation_amplitude,
+                         magnetic_amplitude=magnetic_amplitude, **kw)
+        self.omega = float(omega)
+        self.shear_rate = float(shear_rate)
+        self.background_b = tuple(float(v) for v in background_b)
+        self.U_wall = -self.shear_rate
+        self.Ub = -self.shear_rate * self.X[0]
+        self.Ubp = -self.shear_rate * self.Xp[0]
+        self.dUb_dx = -self.shear_rate

@@ -23,5 +23,7 @@ int main(void) {
   printf("jfb_mhd_state %zu\n", sizeof(jfb_mhd_state));
   F(jfb_mhd_state, flow); F(jfb_mhd_state, A); F(jfb_mhd_state, nonlinear_A_old);
   F(jfb_mhd_state, nonlinear_A_older); F(jfb_mhd_state, A_old); F(jfb_mhd_state, A_older);
+  printf("jfb_mhd_params %zu\n", sizeof(jfb_mhd_params));
+  F(jfb_mhd_params, eta); F(jfb_mhd_params, omega); F(jfb_mhd_params, b0);
   return 0;
 }

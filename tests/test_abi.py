@@ -64,7 +64,8 @@ def c_layout(tmp_path_factory):
 @pytest.mark.parametrize("cname, cls", [("jfb_kmm_config", _lib.KMMConfig),
                                         ("jfb_kmm_state", _lib.KMMStateC),
                                         ("jfb_kmm_info", _lib.KMMInfo),
-                                        ("jfb_mhd_state", _lib.MHDStateC)])
+                                        ("jfb_mhd_state", _lib.MHDStateC),
+                                        ("jfb_mhd_params", _lib.MHDParams)])
 def test_struct_layouts_match_c(c_layout, cname, cls):
     assert int(c_layout[cname]) == ctypes.sizeof(cls)
     for key, off in c_layout.items():
@@ -79,8 +80,12 @@ def test_mhd_argument_errors_are_reported_without_a_gpu():
     cfg.nx, cfg.ny, cfg.nz = 17, 16, 16
     cfg.precision = _lib.JFB_PRECISION_MIXED
     h = ctypes.c_void_p()
-    assert lib.jfb_mhd_create(ctypes.byref(cfg), 400.0, ctypes.byref(h)) == _lib.JFB_ERR_ARG
+    prm = _lib.MHDParams()
+    prm.eta = 1.0 / 400.0
+    assert lib.jfb_mhd_create(ctypes.byref(cfg), ctypes.byref(prm), ctypes.byref(h)) == _lib.JFB_ERR_ARG
     assert b"FP64" in lib.jfb_last_error()
     cfg.precision = _lib.JFB_PRECISION_FP64
-    assert lib.jfb_mhd_create(ctypes.byref(cfg), -1.0, ctypes.byref(h)) == _lib.JFB_ERR_ARG
-    assert b"rm" in lib.jfb_last_error()
+    prm.eta = -1.0
+    assert lib.jfb_mhd_create(ctypes.byref(cfg), ctypes.byref(prm), ctypes.byref(h)) == _lib.JFB_ERR_ARG
+    assert b"eta" in lib.jfb_last_error()
+    assert lib.jfb_ensemble_create(None, 0, ctypes.byref(h)) == _lib.JFB_ERR_ARG

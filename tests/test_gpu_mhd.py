@@ -172,3 +172,56 @@ def test_reference_mhd_benchmark_golden(cuda):
         ref = spec["diagnostics"][key]
         assert abs(d[key] - ref) <= 1e-10 * abs(ref) + 1e-14, key
     assert d["divB_L2"] < 1e-15 and d["divL2"] < 1e-15
+
+
+def test_rotating_shear_variant_matches_oracle(cuda):
+    """PlaneCouetteMRIShearpyJax dynamics: U_b = -S x, Coriolis, imposed B0,
+    eta = 1/Rm != nu (pcf_mhd_mri_shearpy_jax.py:36-176)."""
+    from jaxfun_b200.mhd import PlaneCouetteMRIShearpy
+    from oracle.kmm import PlaneCouetteMRIOracle
+
+    kw = dict(N=(17, 16, 16), Re=400.0, Rm=250.0, omega=0.5, shear_rate=1.5,
+              background_b=(0.01, 0.02, 0.1), dt=1e-3, magnetic_amplitude=0.2)
+    o = PlaneCouetteMRIOracle(**kw)
+    g = PlaneCouetteMRIShearpy(device=cuda, **kw)
+    st = o.initial_state()
+    gs = to_dev(st, cuda)
+    done = 0
+    for n in (1, 2, 3, 6):
+        st = o.solve(st, n - done)
+        gs = g.solve(gs, n - done)
+        done = n
+        for a, b in zip((*gs.flow.u, gs.flow.g), (*st.flow.u, st.flow.g), strict=True):
+            assert rel(a, b) < 1e-12, n
+        sc = a_scale(st.A)
+        for a, b in zip(gs.A, st.A, strict=True):
+            assert rel(a, b, floor=sc) < 1e-12, n
+    do, dg = o.diagnostics(st), g.diagnostics(gs)
+    for k in ("Epert", "Etot", "u_top", "u_bot", "wall_shear_top", "Emag"):
+        assert abs(dg[k] - do[k]) <= 1e-12 * max(1.0, abs(do[k])), k
+
+
+def test_ensemble_of_uneven_members_equals_separate_runs(cuda):
+    """Members of uneven wall-normal size (and a flow-only member) advanced
+    as one graph per step give bitwise the results of separate runs."""
+    from jaxfun_b200.kmm import PlaneCouetteFluctuation
+    from jaxfun_b200.mhd import Ensemble
+
+    def members():
+        return [PlaneCouetteMHD(N=(17, 16, 16), dt=1e-3, magnetic_amplitude=0.1, device=cuda),
+                PlaneCouetteMHD(N=(25, 16, 16), dt=1e-3, magnetic_amplitude=0.1, device=cuda),
+                PlaneCouetteMHD(N=(33, 16, 16), dt=1e-3, magnetic_amplitude=0.1, device=cuda),
+                PlaneCouetteFluctuation(N=(33, 16, 16), dt=1e-3, device=cuda)]
+
+    sep = members()
+    ref = [m.solve(m.initial_state(), 7) for m in sep]
+    ens_m = members()
+    ens = Ensemble(ens_m)
+    out = ens.solve([m.initial_state() for m in ens_m], 7)
+    for a, b in zip(out, ref, strict=True):
+        if isinstance(a, MHDState):
+            la, lb = (*a.flow.u, a.flow.g, *a.A), (*b.flow.u, b.flow.g, *b.A)
+        else:
+            la, lb = (*a.u, a.g), (*b.u, b.g)
+        for x, y in zip(la, lb, strict=True):
+            assert torch.equal(x, y)
