@@ -64,6 +64,9 @@ def parse_args(argv=None):
                    help="skip the adjoint / minimal-seed block")
     p.add_argument("--adjoint-steps", type=int, default=200)
     p.add_argument("--ascent-iterations", type=int, default=20)
+    p.add_argument("--no-ensemble", action="store_true",
+                   help="skip the MHD ensemble block")
+    p.add_argument("--ensemble-members", type=int, default=32)
     return p.parse_args(argv)
 
 
@@ -534,10 +537,63 @@ def main(argv=None):
             "reference_jax_grad": "unavailable: jax is not installed on this host",
         }
 
+    def ensemble_block():
+        """The batched MHD ensemble workload: --ensemble-members members with
+        wall-normal sizes cycling 33, 49, 65 x 64 x 64 Fourier modes, Re = Rm
+        = 1000, imposed field B0 = 0.1 e_z, base flow U_b = x, seeded
+        divergence-free perturbations of u and b (energies 1e-4 each), FP64;
+        one CUDA graph per ensemble step with every member on its own stream."""
+        from jaxfun_b200.mhd import Ensemble, MHDState, PlaneCouetteMRIShearpy
+
+        sizes = (33, 49, 65)
+        members, states = [], []
+        for m in range(args.ensemble_members):
+            N = (sizes[m % 3], grid[1], grid[2])
+            sv = PlaneCouetteMRIShearpy(N=N, domain=domain(), Re=RE, Rm=RE, omega=0.0,
+                                        shear_rate=-1.0, background_b=(0.0, 0.0, 0.1),
+                                        dt=DT, device=dev)
+            fu = couette_perturbation_fields(N, domain(), seeds=(100 + m, 1100 + m))
+            e_u = sv.diagnostics(sv.state_from_physical(fu))["Epert"]
+            flow = sv.state_from_physical(scale_to_energy(fu, e_u, ENERGY))
+            fa = couette_perturbation_fields(N, domain(), seeds=(2100 + m, 3100 + m))
+            A = sv._A_state_from_physical(fa)
+            e_b = sv.diagnostics(MHDState(flow=flow, A=A))["Emag"]
+            A = tuple(a * math.sqrt(ENERGY / e_b) for a in A)
+            members.append(sv)
+            states.append(MHDState(flow=flow, A=A))
+        ens = Ensemble(members)
+        ens.load(states)
+        ens.advance_resident(2 + max(3, args.warmup))
+        torch.cuda.synchronize(dev)
+        K = max(10, min(args.steps, 100))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ens.advance_resident(K)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms_step = e0.elapsed_time(e1) / K
+        launches = sum(m.info().launches_per_step for m in members)
+        diags = [m.diagnostics(m._fetch_mhd(2.0)) for m in members[:3]]
+        return {
+            "workload": f"{len(members)} MHD members, N cycling {sizes} x {grid[1]} x {grid[2]}, "
+                        "Re = Rm = 1000, B0 = 0.1 e_z, u and b perturbation energies 1e-4",
+            "members": len(members),
+            "dtype": "f64",
+            "ms_per_ensemble_step": ms_step,
+            "member_steps_per_s": len(members) * 1000.0 / ms_step,
+            "steps": K,
+            "gpu_launches_per_step": launches,
+            "launch": "one CUDA graph per ensemble step, one stream per member",
+            "l2": "not flushed: the ensemble's state exceeds L2",
+            "device_bytes": sum(m.info().device_bytes for m in members),
+            "sample_diagnostics": [{k: d[k] for k in ("Epert", "Emag", "divB_L2")} for d in diags],
+        }
+
     forms = ("mixed", "fp64") if args.precision == "both" else (args.precision,)
     results = {p: measure(p) for p in forms}
     err = mixed_error() if "mixed" in forms and rank == 0 else None
     adj = adjoint_block() if (rank == 0 and world == 1 and not args.no_adjoint) else None
+    ensb = ensemble_block() if (rank == 0 and world == 1 and not args.no_ensemble) else None
 
     if rank != 0:
         if world > 1:
@@ -574,6 +630,8 @@ def main(argv=None):
         line["mixed_vs_fp64_rel_l2"] = err
     if adj is not None:
         line["adjoint"] = adj
+    if ensb is not None:
+        line["mhd_ensemble"] = ensb
     if world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         rate, n = cpu_oracle_rate(fields, grid, args.cpu_seconds, threads)
