@@ -457,6 +457,7 @@ static int launch_implicit(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s)
   if (!pl->gemm) {
     StageArgs b = a;
     b.x32 = pl->mixed ? 1 : 0;
+    b.Xlin = pl->mixed ? reinterpret_cast<const c32*>(pl->X) : nullptr;
     return launch_pencil(pl, b, s);
   }
   GemmStageArgs g;
@@ -496,6 +497,7 @@ static int launch_implicit(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s)
   g.vw_out = a.vw_out;
   g.X = a.X;
   g.x32 = pl->mixed ? 1 : 0;
+  g.Xlin = pl->mixed ? reinterpret_cast<const c32*>(pl->X) : nullptr;
   const int blocks = (pl->d.Ny / 2) * ceil_div(pl->d.Kz, 8);
   pencil_gemm_kernel<<<blocks, kGThreads, pl->smem_gemm, s>>>(pl->d, pl->ops, pl->gops, g);
   JFB_CHECK_LAUNCH();
@@ -506,6 +508,16 @@ static int warp_radix(int n) {
   if (n % 32) return 0;
   const int p = n / 32;
   return (p == 2 || p == 3 || p == 4 || p == 6) ? p : 0;
+}
+
+// Dimensions handed to the periodic-axis kernels: in the complex64 form the
+// base flow is left out of the transforms (the pencil kernels add its terms,
+// linear in the perturbation, in FP64 at the x nodes).
+template <typename T>
+static Dims tdims(const jfb_kmm_plan* pl) {
+  Dims d = pl->d;
+  if (sizeof(T) == sizeof(float)) d.uwall = 0.0;
+  return d;
 }
 
 // Step transform buffers and twiddles in the plan's transform precision.
@@ -522,7 +534,7 @@ template <typename T> static cpx<T>* buf(void* p) { return reinterpret_cast<cpx<
 
 template <int P, typename T>
 static void launch_y_warp(jfb_kmm_plan* pl, cudaStream_t s, bool backward) {
-  const Dims& d = pl->d;
+  const Dims d = tdims<T>(pl);
   const size_t sm = backward ? pl->smem_yw_b : pl->smem_yw_f;
   const size_t smT = sm / sizeof(c64) * sizeof(cpx<T>);
   if (backward) {
@@ -548,7 +560,7 @@ static void launch_y_warp_any(jfb_kmm_plan* pl, cudaStream_t s, bool backward) {
 
 template <int P, typename T>
 static void launch_zcross_warp(jfb_kmm_plan* pl, cudaStream_t s) {
-  const Dims& d = pl->d;
+  const Dims d = tdims<T>(pl);
   const int pairs = ceil_div((int64_t)d.Nx * d.My, 2);
   const int blocks = ceil_div(pairs, 8);
   if (pl->qk == 1)
@@ -575,13 +587,13 @@ template <int PY, int PZ, typename T>
 static void launch_plane(jfb_kmm_plan* pl, cudaStream_t s) {
   plane_cross_kernel<PY, PZ, 1, T><<<2 * pl->d.Nx, kPlaneThreads,
                                      plane_smem_bytes(pl->d.My, pl->d.Kz, sizeof(cpx<T>)), s>>>(
-      pl->ops, pl->d, Tx<T>::twy(pl), Tx<T>::twz(pl), buf<T>(pl->X), buf<T>(pl->HX));
+      pl->ops, tdims<T>(pl), Tx<T>::twy(pl), Tx<T>::twz(pl), buf<T>(pl->X), buf<T>(pl->HX));
 }
 
 // y_backward -> z_cross -> y_forward: HX <- H(state whose x-physical fields are in X)
 template <typename T>
 static int launch_transforms_t(jfb_kmm_plan* pl, cudaStream_t s) {
-  const Dims& d = pl->d;
+  const Dims d = tdims<T>(pl);
   if (pl->plane) {
     const int key = pl->py * 10 + pl->pz;
     if (key == 22) launch_plane<2, 2, T>(pl, s);
@@ -1442,6 +1454,7 @@ extern "C" int jfb_kmm_convection(jfb_kmm_plan* pl, void* h0, void* h1, void* h2
   StageArgs a = blank_args();
   a.mode = kHOnly;
   a.x32 = pl->mixed ? 1 : 0;
+  a.Xlin = pl->mixed ? reinterpret_cast<const c32*>(pl->X) : nullptr;
   a.HX = pl->HX;
   a.Hd_out = pl->HD;
   st = launch_pencil(pl, a, s);

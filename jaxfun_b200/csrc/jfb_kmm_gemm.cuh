@@ -76,7 +76,29 @@ struct GemmStageArgs {
   c64 *u0_out, *g_out, *vw_out;
   c64* X;
   int x32;  // HX and X hold complex64 values (mixed form)
+  // mixed form: x-physical u, omega (complex64) of the state whose nonlinear
+  // term is in HX; the FP32 transforms carry only -(u' x omega') and the
+  // base-flow terms, linear in u', omega', are added here in FP64
+  const c32* Xlin;
 };
+
+// Base-flow part of the rotational term at one x node (pcf_fluctuations_jax.py:
+// 108-112 with U_b = U_wall x): -U_b e_y x omega' - U_wall u' x e_z, plus the
+// constant -U_b U_wall e_x on the mean pencil.  f = field order u0, u1, u2,
+// omega0, omega1, omega2 of X.
+__device__ __forceinline__ void add_base_flow_terms(const c32* __restrict__ X, size_t P, int N,
+                                                    int j, size_t p, double ub, double uw,
+                                                    c64 (&h)[3]) {
+  auto ld = [&](int f) {
+    const c32 v = X[((size_t)f * N + j) * P + p];
+    return cmk((double)v.re, (double)v.im);
+  };
+  const c64 u0 = ld(0), u1 = ld(1), w0 = ld(3), w2 = ld(5);
+  h[0] = h[0] - uw * u1 - ub * w2;
+  h[1] = h[1] + uw * u0;
+  h[2] = h[2] + ub * w0;
+  if (p == 0) h[0].re -= ub * uw;
+}
 
 __host__ __device__ inline int round4(int x) { return (x + 3) & ~3; }
 
@@ -446,6 +468,11 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     for (int f = 0; f < 3; ++f) {
       h[0][f] = ok ? slot(G.oH[f] + j) : cmk(0.0, 0.0);
       h[1][f] = (ok && jm != j) ? slot(G.oH[f] + jm) : cmk(0.0, 0.0);
+    }
+    if (a.Xlin && ok) {
+      add_base_flow_terms(a.Xlin, P, N, j, s_p[w], d.uwall * o.xphys[j], d.uwall, h[0]);
+      if (jm != j)
+        add_base_flow_terms(a.Xlin, P, N, jm, s_p[w], d.uwall * o.xphys[jm], d.uwall, h[1]);
     }
     if (mean_cta && w == 0) {
       mean[j] = h[0][1].re;

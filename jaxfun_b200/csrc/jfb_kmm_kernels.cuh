@@ -80,6 +80,7 @@ struct StageArgs {
   c64* Hd_out;                 // kHOnly: 3 x [nD][P]
   c64 *u1_out, *u2_out;        // kFromPhys: tangential velocity (nD x P)
   int x32;  // HX (read, step modes) and X (written by the x-backward) hold complex64
+  const c32* Xlin;  // mixed form: u, omega of HX's state; FP64 base-flow terms added here
 };
 
 __host__ __device__ inline int packed_rec_size(int n) {
@@ -626,6 +627,24 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
           v = cmk((double)h.re, (double)h.im);
         } else {
           v = a.HX[e];
+        }
+        if (a.Xlin && a.mode != kFromPhys) {
+          // base-flow terms of the rotational product in FP64 (the complex64
+          // transforms carry -(u' x omega') only)
+          const int f = fi / d.Nx, j = fi % d.Nx;
+          const double uw = d.uwall, ub = d.uwall * o.xphys[j];
+          auto ld = [&](int g) {
+            const c32 x = a.Xlin[((size_t)g * d.Nx + j) * P + p0 + w];
+            return cmk((double)x.re, (double)x.im);
+          };
+          if (f == 0) {
+            v = v - uw * ld(1) - ub * ld(5);
+            if (p0 + w == 0) v.re -= ub * uw;
+          } else if (f == 1) {
+            v = v + uw * ld(0);
+          } else {
+            v = v + ub * ld(3);
+          }
         }
       }
       R1[fi * kLDW + w] = v;
