@@ -189,6 +189,7 @@ struct FactorSet {
   double* su = nullptr;
   double* sg = nullptr;
   double* s00 = nullptr;
+  double* s00inv = nullptr;  // explicit inverse of the mean-flow system (tensor-core stage)
   // factored bands kept for the transposed solves of the adjoint (Su, Sg, S00)
   double* band[3] = {nullptr, nullptr, nullptr};
   int bp[3] = {0, 0, 0}, bq[3] = {0, 0, 0};
@@ -396,6 +397,39 @@ static int build_factor_set(jfb_kmm_plan* pl, double gamma, FactorSet& fs, doubl
       dX0 = dX2 = dX4 = dcoef = nullptr;
       continue;
     }
+    if (sys == 2 && inv) {
+      // dense S00 = X0 - gamma nu X2 inverted in long double (Gauss-Jordan,
+      // partial pivoting); rows of one parity stay within that parity
+      const int nn = n;
+      std::vector<long double> Aa((size_t)nn * 2 * nn, 0.0L);
+      for (int i = 0; i < nn; ++i) {
+        for (int j = 0; j < nn; ++j)
+          Aa[(size_t)i * 2 * nn + j] = (long double)coef[0] * X0[(size_t)i * nn + j] +
+                                       (long double)coef[1] * X2[(size_t)i * nn + j];
+        Aa[(size_t)i * 2 * nn + nn + i] = 1.0L;
+      }
+      for (int c = 0; c < nn; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < nn; ++r)
+          if (std::fabs(Aa[(size_t)r * 2 * nn + c]) > std::fabs(Aa[(size_t)piv * 2 * nn + c])) piv = r;
+        JFB_REQUIRE(Aa[(size_t)piv * 2 * nn + c] != 0.0L, "singular mean-flow system");
+        if (piv != c)
+          for (int k = 0; k < 2 * nn; ++k) std::swap(Aa[(size_t)c * 2 * nn + k], Aa[(size_t)piv * 2 * nn + k]);
+        const long double inv_p = 1.0L / Aa[(size_t)c * 2 * nn + c];
+        for (int k = 0; k < 2 * nn; ++k) Aa[(size_t)c * 2 * nn + k] *= inv_p;
+        for (int r = 0; r < nn; ++r) {
+          if (r == c) continue;
+          const long double f = Aa[(size_t)r * 2 * nn + c];
+          if (f == 0.0L) continue;
+          for (int k = 0; k < 2 * nn; ++k) Aa[(size_t)r * 2 * nn + k] -= f * Aa[(size_t)c * 2 * nn + k];
+        }
+      }
+      std::vector<double> Si((size_t)nn * nn);
+      for (int i = 0; i < nn; ++i)
+        for (int j = 0; j < nn; ++j) Si[(size_t)i * nn + j] = (double)Aa[(size_t)i * 2 * nn + nn + j];
+      st = upload(pl, &fs.s00inv, Si);
+      if (st) return cleanup(), st;
+    }
     double** dst = (sys == 0) ? &fs.su : (sys == 1) ? &fs.sg : &fs.s00;
     st = dalloc(pl, (void**)dst, (size_t)modes * packed_rec_size(n) * sizeof(double));
     if (st) return cleanup(), st;
@@ -430,6 +464,7 @@ static PackedFactors packed(const jfb_kmm_plan* pl, const FactorSet& fs) {
   f.su = fs.su;
   f.sg = fs.sg;
   f.s00 = fs.s00;
+  f.s00inv = fs.s00inv;
   f.su_rec = pl->su_rec;
   f.sg_rec = pl->sg_rec;
   return f;
@@ -490,6 +525,7 @@ static int launch_implicit(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s)
   g.su = a.fac.su;
   g.sg = a.fac.sg;
   g.s00 = a.fac.s00;
+  g.s00inv = a.fac.s00inv;
   g.su_rec = a.fac.su_rec;
   g.sg_rec = a.fac.sg_rec;
   g.u0_out = a.u0_out;

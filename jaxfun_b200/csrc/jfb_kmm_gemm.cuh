@@ -72,6 +72,7 @@ struct GemmStageArgs {
   const c64 *Nup, *Nuq, *Ngp, *Ngq, *NVWp, *NVWq;
   c64 *Nu_out, *Ng_out, *NVW_out;
   const double *su, *sg, *s00;  // records: L pairs, then inverse upper triangles
+  const double* s00inv;         // mean-flow system inverse (nD x nD, row-major)
   int su_rec, sg_rec;
   c64 *u0_out, *g_out, *vw_out;
   c64* X;
@@ -86,18 +87,14 @@ struct GemmStageArgs {
 // 108-112 with U_b = U_wall x): -U_b e_y x omega' - U_wall u' x e_z, plus the
 // constant -U_b U_wall e_x on the mean pencil.  f = field order u0, u1, u2,
 // omega0, omega1, omega2 of X.
-__device__ __forceinline__ void add_base_flow_terms(const c32* __restrict__ X, size_t P, int N,
-                                                    int j, size_t p, double ub, double uw,
-                                                    c64 (&h)[3]) {
-  auto ld = [&](int f) {
-    const c32 v = X[((size_t)f * N + j) * P + p];
-    return cmk((double)v.re, (double)v.im);
-  };
-  const c64 u0 = ld(0), u1 = ld(1), w0 = ld(3), w2 = ld(5);
-  h[0] = h[0] - uw * u1 - ub * w2;
-  h[1] = h[1] + uw * u0;
-  h[2] = h[2] + ub * w0;
-  if (p == 0) h[0].re -= ub * uw;
+// x = (u0, u1, omega0, omega2) at the node.
+__device__ __forceinline__ void add_base_flow_terms(const c32 (&x)[4], bool mean, double ub,
+                                                    double uw, c64 (&h)[3]) {
+  auto c = [&](int k) { return cmk((double)x[k].re, (double)x[k].im); };
+  h[0] = h[0] - uw * c(1) - ub * c(3);
+  h[1] = h[1] + uw * c(0);
+  h[2] = h[2] + ub * c(2);
+  if (mean) h[0].re -= ub * uw;
 }
 
 __host__ __device__ inline int round4(int x) { return (x + 3) & ~3; }
@@ -328,19 +325,20 @@ __device__ void mean_flow(const Dims& d, const DevOps& o, const GemmOps& G,
     vw[i] = r + d.dt * nl;
   }
   bar_sync(1, kMeanThreads);
-  if (t < 2) forward_elim(a.s00, t, t ? nD / 2 : (nD + 1) / 2, vw + t, 2);
-  bar_sync(1, kMeanThreads);
+  // S00^-1 rhs: rows of parity p couple only to columns of parity p (a
+  // sequential elimination on two threads would sit on the kernel's
+  // critical path; the inverse makes it one product per row)
   for (int i = t; i < nD; i += kMeanThreads) {
-    const int m0 = (nD + 1) / 2, par = i & 1, r = i >> 1;
-    const int m = par ? nD / 2 : m0;
-    const double* tri = a.s00 + 2 * nD + (par ? m0 * (m0 + 1) / 2 : 0);
-    double u[kMaxM];
-#pragma unroll
-    for (int c = 0; c < kMaxM; ++c) u[c] = (c >= r && c < m) ? __ldg(tri + c * (c + 1) / 2 + r) : 0.0;
-    c64 xv = cmk(0.0, 0.0);
-#pragma unroll
-    for (int c = 0; c < kMaxM; ++c)
-      if (c >= r && c < m) xv = xv + u[c] * vw[2 * c + par];
+    const double* __restrict__ row = a.s00inv + (size_t)i * nD;
+    c64 x0 = cmk(0.0, 0.0), x1 = x0;
+    int k = i & 1;
+#pragma unroll 4
+    for (; k + 2 < nD; k += 4) {
+      x0 = x0 + __ldg(row + k) * vw[k];
+      x1 = x1 + __ldg(row + k + 2) * vw[k + 2];
+    }
+    if (k < nD) x0 = x0 + __ldg(row + k) * vw[k];
+    const c64 xv = x0 + x1;
     vwx[i] = xv;
     a.vw_out[i] = xv;
   }
@@ -396,7 +394,7 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     if (b1 > b0) prefetch_l2(frag + b0, (size_t)(b1 - b0) * sizeof(double));
   } else if (tid == 128 && mean_cta) {
     prefetch_l2(G.R3, (size_t)d.nD * d.Nx * sizeof(double));
-    prefetch_l2(a.s00, (size_t)a.sg_rec * sizeof(double));
+    prefetch_l2(a.s00inv, (size_t)d.nD * d.nD * sizeof(double));
     if (sl != 0.0) prefetch_l2(G.X2D, (size_t)d.nD * d.nD * sizeof(double));
   }
   __syncthreads();
@@ -408,39 +406,65 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
   // (row i -> i / 2), likewise g.  Column = pencil (8 +ky then 8 -ky).
   const bool has_b = (a.c1 != 0.0), has_c = (a.c2 != 0.0);
   const int sides = (kyi == 0) ? 1 : 2;
+  c32 xl[2][2][4];  // mixed form: (u0, u1, omega0, omega2) at rows j, N-1-j of two items
   {
     const int lv = 1 + has_b + has_c;
     const int nrow = 3 * N + (d.nB + d.nD) * lv;
-    const int per_row = sides * nkz;
-    for (int e = tid; e < nrow * per_row; e += kGThreads) {
-      const int r = e / per_row, c = e % per_row;
-      const int side = c / nkz, kz = c % nkz;
+    // one half-warp per row (lane & 15 = pencil column), so that the row's
+    // source and destination are formed once per row, not per element
+    const int hw = tid >> 4, c = tid & 15;
+    const int side = c >> 3, kz = c & 7;  // nkz <= 8 columns per side
+    const bool col_ok = side < sides && kz < nkz;
+    const size_t so = (size_t)(side ? d.Ny - kyi : kyi) * d.Kz + kz0 + kz;
+    for (int r = hw; r < nrow; r += kGThreads / 16) {
+      if (!col_ok) continue;
       const c64* src;
       int dst_row;
       if (r < 3 * N) {
-        const int f = r / N, j = r % N;
-        src = a.HX + ((size_t)f * N + j) * P;
+        const int f = r >= 2 * N ? 2 : r >= N ? 1 : 0, j = r - f * N;
         dst_row = G.oH[f] + j;
+        const size_t e = ((size_t)f * N + j) * P + so;
+        if (a.x32)  // complex64 sample: lands in the first half of the slot
+          cp_async8(rowc + (size_t)dst_row * LC + side * 8 + kz,
+                    reinterpret_cast<const c32*>(a.HX) + e);
+        else
+          cp_async16(rowc + (size_t)dst_row * LC + side * 8 + kz, a.HX + e);
+        continue;
       } else if (r < 3 * N + d.nB * lv) {
-        const int q = r - 3 * N, lvl = q / d.nB, i = q % d.nB;
+        int q = r - 3 * N, lvl = 0;
+        while (q >= d.nB) { q -= d.nB; ++lvl; }
+        const int i = q;
         const int l = (lvl == 0) ? 0 : (lvl == 1 && has_b) ? 1 : 2;
         src = ((l == 0) ? a.u0a : (l == 1) ? a.u0b : a.u0c) + (size_t)i * P;
         const int nh = (i & 1) ? G.nBo : G.nBe;
         dst_row = ((i & 1) ? G.oMUO : G.oMUE) + l * nh + (i >> 1);
       } else {
-        const int q = r - 3 * N - d.nB * lv, lvl = q / d.nD, i = q % d.nD;
+        int q = r - 3 * N - d.nB * lv, lvl = 0;
+        while (q >= d.nD) { q -= d.nD; ++lvl; }
+        const int i = q;
         const int l = (lvl == 0) ? 0 : (lvl == 1 && has_b) ? 1 : 2;
         src = ((l == 0) ? a.ga : (l == 1) ? a.gb : a.gc) + (size_t)i * P;
         const int nh = (i & 1) ? G.nDo : G.nDe;
         dst_row = ((i & 1) ? G.oMGO : G.oMGE) + l * nh + (i >> 1);
       }
-      const int kyrow = side ? d.Ny - kyi : kyi;
-      const size_t so = (size_t)kyrow * d.Kz + kz0 + kz;
-      if (a.x32 && r < 3 * N)  // complex64 sample: lands in the first half of the slot
-        cp_async8(rowc + (size_t)dst_row * LC + side * 8 + kz,
-                  reinterpret_cast<const c32*>(a.HX) + (src - a.HX) + so);
-      else
-        cp_async16(rowc + (size_t)dst_row * LC + side * 8 + kz, src + so);
+      cp_async16(rowc + (size_t)dst_row * LC + side * 8 + kz, src + so);
+    }
+    // mixed form: this thread's base-flow samples, loaded while the copies fly
+    if (a.Xlin) {
+#pragma unroll
+      for (int it = 0; it < 2; ++it) {
+        const int idx = tid + it * kGThreads;
+        if (idx >= Jh * kGW) continue;
+        const int j = idx / kGW, w = idx % kGW, p = s_p[w];
+        if (p < 0) continue;
+        const int rows[2] = {j, N - 1 - j};
+        const int fs[4] = {0, 1, 3, 5};
+#pragma unroll
+        for (int s2 = 0; s2 < 2; ++s2)
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            xl[it][s2][k] = a.Xlin[((size_t)fs[k] * N + rows[s2]) * P + p];
+      }
     }
     cp_async_commit();
     cp_async_wait_all();
@@ -454,7 +478,11 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
   c64* m_nvw = reinterpret_cast<c64*>(mean + 2 * N);
   c64* m_vw = reinterpret_cast<c64*>(mean + 2 * N + 2 * d.nD);
   c64* m_x = reinterpret_cast<c64*>(mean + 2 * N + 4 * d.nD);
-  for (int idx = tid; idx < Jh * kGW; idx += kGThreads) {
+  // (Jh * kGW <= 2 * kGThreads: the tensor-core path runs for Nx <= 65)
+#pragma unroll
+  for (int it = 0; it < 2; ++it) {
+    const int idx = tid + it * kGThreads;
+    if (idx >= Jh * kGW) break;
     const int j = idx / kGW, w = idx % kGW, jm = N - 1 - j;
     const bool ok = s_p[w] >= 0;
     c64 h[2][3];
@@ -470,9 +498,9 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
       h[1][f] = (ok && jm != j) ? slot(G.oH[f] + jm) : cmk(0.0, 0.0);
     }
     if (a.Xlin && ok) {
-      add_base_flow_terms(a.Xlin, P, N, j, s_p[w], d.uwall * o.xphys[j], d.uwall, h[0]);
-      if (jm != j)
-        add_base_flow_terms(a.Xlin, P, N, jm, s_p[w], d.uwall * o.xphys[jm], d.uwall, h[1]);
+      const bool mean = s_p[w] == 0;
+      add_base_flow_terms(xl[it][0], mean, d.uwall * o.xphys[j], d.uwall, h[0]);
+      if (jm != j) add_base_flow_terms(xl[it][1], mean, d.uwall * o.xphys[jm], d.uwall, h[1]);
     }
     if (mean_cta && w == 0) {
       mean[j] = h[0][1].re;

@@ -59,6 +59,7 @@ struct PackedFactors {
   const double* su;  // n_modes records of su_rec doubles
   const double* sg;
   const double* s00;  // one record (sg layout, n = nD)
+  const double* s00inv;  // the explicit inverse of the mean-flow system (nD x nD)
   int su_rec, sg_rec;
 };
 
