@@ -343,8 +343,41 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
   const int half = d.Ny / 2;
   const int br = bitrev5(lane);
 
-  // 1. inverse y transforms of this CTA's columns
-  {
+  // 1. inverse y transforms of this CTA's columns (complex64: staged row
+  //    by row, coalesced along kz, into Ys in padded order, then one column
+  //    per warp in place; FP64: gathered per column straight from X)
+  if constexpr (sizeof(T) == 4) {
+    // half-warp per row (KH <= 16 columns), no per-element index division
+    const int hw = threadIdx.x >> 4, cl = threadIdx.x & 15;
+    if (cl < KH) {
+#pragma unroll 1
+      for (int f = 0; f < 6; ++f) {
+        const cpx<T>* src = X + ((size_t)f * d.Nx + j) * P + rank * KH + cl;
+        cpx<T>* dst = Ys + (size_t)f * MY * LDZ + cl;
+        for (int r = hw; r < d.Ny; r += kPlaneThreads / 16) {
+          if (r == half) continue;  // Nyquist row: zero, below
+          const int k = (r < half) ? r : r - d.Ny + MY;  // padded row
+          dst[(size_t)k * LDZ] = src[(size_t)r * Kz];
+        }
+        for (int k = half + hw; k <= MY - half; k += kPlaneThreads / 16)
+          dst[(size_t)k * LDZ] = cmk(T(0), T(0));
+      }
+    }
+    __syncthreads();
+    WarpTw<PY, T> w;
+    load_warp_tw<PY, T>(w, twy, lane);
+    for (int t = warp; t < 6 * KH; t += NW) {
+      const int f = t / KH, cl = t % KH;
+      cpx<T>* col = Ys + (size_t)f * MY * LDZ + cl;
+      cpx<T> v[PY];
+#pragma unroll
+      for (int r = 0; r < PY; ++r) v[r] = col[(size_t)(32 * r + lane) * LDZ];
+      __syncwarp();
+      warp_fft_inverse<PY, T>(v, w, lane);
+#pragma unroll
+      for (int k1 = 0; k1 < PY; ++k1) col[(size_t)(k1 + PY * br) * LDZ] = v[k1];
+    }
+  } else {
     WarpTw<PY, T> w;
     load_warp_tw<PY, T>(w, twy, lane);
     for (int t = warp; t < 6 * KH; t += NW) {
@@ -386,7 +419,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
             const int kz = 32 * q + lane;
             A[q] = B[q] = cmk(T(0), T(0));
             if (kz < Kz) {
-              const int own = kz / KH, cl = kz - own * KH;
+              const int own = kz >= KH, cl = kz - own * KH;
               const cpx<T>* base = (own == rank) ? Ys : Ypeer;
               A[q] = base[((size_t)(2 * pr) * MY + y) * LDZ + cl];
               B[q] = base[((size_t)(2 * pr + 1) * MY + y) * LDZ + cl];
@@ -432,8 +465,41 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
   }
   cluster.sync();
 
-  // 3. forward y transforms of this CTA's columns
-  {
+  // 3. forward y transforms of this CTA's columns (complex64: into Ys,
+  //    free once the peer has passed the barrier above, then row-wise
+  //    coalesced stores; FP64: stored per column)
+  if constexpr (sizeof(T) == 4) {
+    WarpTw<PY, T> w;
+    load_warp_tw<PY, T>(w, twy, lane);
+    const T scale = T(1.0 / MY);
+    for (int t = warp; t < 3 * KH; t += NW) {
+      const int f = t / KH, cl = t % KH, kz = rank * KH + cl;
+      cpx<T> v[PY];
+#pragma unroll
+      for (int n1 = 0; n1 < PY; ++n1) {
+        const int y = n1 + PY * br;
+        const int own = y / MH, yl = y - own * MH;
+        const cpx<T>* base = (own == rank) ? Hs : Hpeer;
+        v[n1] = base[((size_t)f * MH + yl) * Kz + (swz ? (kz ^ (yl & 7)) : kz)];
+      }
+      warp_fft_forward<PY, T>(v, w, lane);
+      cpx<T>* col = Ys + (size_t)f * MY * LDZ + cl;
+#pragma unroll
+      for (int k1 = 0; k1 < PY; ++k1) col[(size_t)(32 * k1 + lane) * LDZ] = scale * v[k1];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 3 * d.Ny * KH; e += kPlaneThreads) {
+      const int cl = e % KH, rf = e / KH, r = rf % d.Ny, f = rf / d.Ny;
+      const int kz = rank * KH + cl;
+      cpx<T> val = cmk(T(0), T(0));  // r == half: Nyquist row
+      if (r != half) {
+        const int k = (r < half) ? r : r - d.Ny + MY;
+        val = Ys[((size_t)f * MY + k) * LDZ + cl];
+        if (f == 0 && kz == 0 && r == 0) val.re += T(-d.uwall * o.xphys[j] * d.uwall);
+      }
+      HX[((size_t)f * d.Nx + j) * P + (size_t)r * Kz + kz] = val;
+    }
+  } else {
     WarpTw<PY, T> w;
     load_warp_tw<PY, T>(w, twy, lane);
     const T scale = T(1.0 / MY);
