@@ -281,6 +281,48 @@ int jfb_mhd_convection(jfb_kmm_plan* plan, void* h0, void* h1, void* h2, void* h
  * then divB_L2 and Emag. */
 int jfb_mhd_diagnostics(jfb_kmm_plan* plan, double* out, void* stream);
 
+/* ---- tensor-product spaces ------------------------------------------------ */
+
+#define JFB_BASIS_ORTHOGONAL 0  /* Chebyshev T_k                              */
+#define JFB_BASIS_DIRICHLET 1   /* T_k - T_{k+2} (Composite, u(+-1) = 0)      */
+#define JFB_BASIS_BIHARMONIC 2  /* u(+-1) = u'(+-1) = 0 (Composite)           */
+
+/* TensorProduct(Chebyshev-family x axis, Fourier[, Fourier])
+ * (src/jaxfun/galerkin/tensorproductspace.py:104-293): n[0] Gauss-Chebyshev
+ * points on [x_lo, x_hi], n[1] (and n[2]) Fourier modes on periods l[0]
+ * (l[1]), padding factors pad[] for the padded backward / forward
+ * (get_dealiased: max(N, int(pad N)) points). */
+typedef struct jfb_tps_config {
+  int32_t ndim;   /* 2: (x, y), 3: (x, y, z) */
+  int32_t basis;  /* JFB_BASIS_*             */
+  int32_t n[3];
+  double x_lo, x_hi;
+  double l[2];
+  double pad[2];
+} jfb_tps_config;
+
+typedef struct jfb_tps jfb_tps;
+int jfb_tps_create(const jfb_tps_config* cfg, jfb_tps** tps);
+int jfb_tps_destroy(jfb_tps* tps);
+/* out4 = (basis dofs nb, quadrature points N, padded counts m1, m2). */
+int jfb_tps_get_sizes(const jfb_tps* tps, int32_t* out4);
+
+/* TensorProductSpace.backward (tensorproductspace.py:253-293, 553-594):
+ * coeffs (nb, n1[, n2]) complex128 -> phys (N, m1[, m2]) complex128, m = n
+ * unpadded or the padded counts when padded != 0 (Fourier.py:128-150). */
+int jfb_tps_backward(jfb_tps* tps, const void* coeffs, void* phys, int padded, void* stream);
+
+/* kind 0: TensorProductSpace.forward (tensorproductspace.py:529-551; the L2
+ * projection along x, Fourier.forward scaled 1/M and truncated, Nyquist kept);
+ * kind 1: scalar_product (per-axis scalar products, Fourier weight 2 pi / df).
+ * phys (N, m1[, m2]) -> coeffs (nb, n1[, n2]). */
+int jfb_tps_forward(jfb_tps* tps, const void* phys, void* coeffs, int padded, int kind,
+                    void* stream);
+
+/* Galerkin x-matrix (phi_i, phi_j^(order))_w, order 0 or 2, dense row-major
+ * nb x nb on the host (the 1-D mass / stiffness of inner.py, domain-scaled). */
+int jfb_tps_galerkin(const jfb_tps* tps, int order, double* out);
+
 /* ---- ensembles ------------------------------------------------------------ */
 
 /* Independent members (flow or MHD plans, any sizes; no reference counterpart:

@@ -25,6 +25,9 @@ JFB_FAMILY_CHEBYSHEV = 0
 JFB_PRECISION_FP64 = 0
 JFB_PRECISION_MIXED = 1
 JFB_NONLINEAR_ROTATIONAL = 0
+JFB_BASIS_ORTHOGONAL = 0
+JFB_BASIS_DIRICHLET = 1
+JFB_BASIS_BIHARMONIC = 2
 
 
 class KMMConfig(ctypes.Structure):
@@ -88,6 +91,20 @@ class MHDParams(ctypes.Structure):
     ]
 
 
+class TPSConfig(ctypes.Structure):
+    """``jfb_tps_config``."""
+
+    _fields_ = [
+        ("ndim", c_int32),
+        ("basis", c_int32),
+        ("n", c_int32 * 3),
+        ("x_lo", c_double),
+        ("x_hi", c_double),
+        ("l", c_double * 2),
+        ("pad", c_double * 2),
+    ]
+
+
 class KMMInfo(ctypes.Structure):
     _fields_ = [
         ("n_pencils", c_int64),
@@ -143,6 +160,12 @@ SIGNATURES = {
         c_int, [c_void_p, POINTER(KMMStateC), POINTER(KMMStateC), c_void_p]
     ),
     "jfb_mhd_create": (c_int, [POINTER(KMMConfig), POINTER(MHDParams), POINTER(c_void_p)]),
+    "jfb_tps_create": (c_int, [POINTER(TPSConfig), POINTER(c_void_p)]),
+    "jfb_tps_destroy": (c_int, [c_void_p]),
+    "jfb_tps_get_sizes": (c_int, [c_void_p, POINTER(c_int32)]),
+    "jfb_tps_backward": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "jfb_tps_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]),
+    "jfb_tps_galerkin": (c_int, [c_void_p, c_int, POINTER(c_double)]),
     "jfb_ensemble_create": (c_int, [POINTER(c_void_p), c_int32, POINTER(c_void_p)]),
     "jfb_ensemble_advance": (c_int, [c_void_p, c_int64, c_void_p]),
     "jfb_ensemble_destroy": (c_int, [c_void_p]),

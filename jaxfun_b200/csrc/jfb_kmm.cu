@@ -2515,3 +2515,5 @@ extern "C" int jfb_ensemble_advance(jfb_ensemble* e, int64_t steps, void* stream
   }
   return JFB_OK;
 }
+
+#include "jfb_tps.cuh"

@@ -66,6 +66,17 @@ struct GemmHost {
   std::vector<double> A0, F, R0, R1, R2, GB, GD;
 };
 
+// x-axis operators of a standalone tensor-product space (row-major):
+// backward B = V S^T (N x nb), forward (L2 projection) F = M^-1 S Q (nb x N),
+// scalar product Sq = S Q (nb x N), Galerkin G0 = (phi_i, phi_j)_w and
+// G2 = (phi_i, phi_j'')_w (nb x nb, domain-scaled).  basis: 0 orthogonal
+// Chebyshev, 1 Dirichlet (T_k - T_{k+2}), 2 biharmonic.
+struct TpsX {
+  int N = 0, nb = 0;
+  std::vector<double> B, F, Sq, G0, G2;
+};
+void build_tps_x_operators(const HostOperators& op, int basis, TpsX& t);
+
 Stencil make_stencil(int N, bool biharmonic);
 // Builds GemmHost from the 1-D operators; returns false (with a message) if a
 // parity property the split relies on does not hold.

@@ -1059,7 +1059,8 @@ __global__ void __launch_bounds__(256) y_forward_kernel(Dims d, FFTPlan plan, in
                                                         const cpx<T>* __restrict__ tw,
                                                         const cpx<T>* __restrict__ HZ,
                                                         cpx<T>* __restrict__ HX,
-                                                        const double* __restrict__ xb) {
+                                                        const double* __restrict__ xb,
+                                                        int keep_nyq = 0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cpx<T>* A = reinterpret_cast<cpx<T>*>(smem_raw);
   cpx<T>* B = A + d.My * KC;
@@ -1083,7 +1084,8 @@ __global__ void __launch_bounds__(256) y_forward_kernel(Dims d, FFTPlan plan, in
     const int kz = idx % KC, r = idx / KC;
     cpx<T> v = cmk(T(0), T(0));
     if (r < half) v = res[r * KC + kz];
-    else if (r > half) v = res[(r - d.Ny + d.My) * KC + kz];  // r == half: Nyquist
+    else if (r > half) v = res[(r - d.Ny + d.My) * KC + kz];
+    else if (keep_nyq) v = res[(d.My - half) * KC + kz];  // the -Ny/2 mode (else masked)
     dst[(size_t)r * d.Kz + kz] = scale * v;
   }
 }

@@ -523,4 +523,48 @@ bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& er
   return true;
 }
 
+
+void build_tps_x_operators(const HostOperators& op, int basis, TpsX& t) {
+  const int N = op.N;
+  const int nb = basis == 0 ? N : basis == 1 ? N - 2 : N - 4;
+  LMat V = from_dense(op.V, N, N), Q = from_dense(op.Q, N, N), W(N, N), S(nb, N);
+  for (int n = 0; n < N; ++n) W(n, n) = (LD)op.ns[n];
+  if (basis == 0) {
+    for (int i = 0; i < N; ++i) S(i, i) = 1.0L;
+  } else {
+    const Stencil& st = basis == 1 ? op.SD : op.SB;
+    for (int i = 0; i < nb; ++i) {
+      S(i, i) = st.s0[i];
+      S(i, i + 2) = st.s2[i];
+      if (basis == 2) S(i, i + 4) = st.s4[i];
+    }
+  }
+  const LMat St = transpose(S);
+  const LMat Minv = inverse(mul(mul(S, W), St));
+  auto dense = [](const LMat& M) {
+    std::vector<double> o((size_t)M.r * M.c);
+    for (size_t k = 0; k < o.size(); ++k) o[k] = (double)M.v[k];
+    return o;
+  };
+  t.N = N;
+  t.nb = nb;
+  t.B = dense(mul(V, St));
+  t.Sq = dense(mul(S, Q));
+  t.F = dense(mul(Minv, mul(S, Q)));
+  if (basis == 0) {
+    // (T_i, T_j^(k))_w with the df^(k-1) domain scaling
+    std::vector<double> T0 = chebyshev_galerkin(N, 0), T2 = chebyshev_galerkin(N, 2);
+    for (double& v : T0) v /= op.dfx;
+    for (double& v : T2) v *= op.dfx;
+    t.G0 = T0;
+    t.G2 = T2;
+  } else if (basis == 1) {
+    t.G0 = op.XD0;
+    t.G2 = op.XD2;
+  } else {
+    t.G0 = op.XB0;
+    t.G2 = op.XB2;
+  }
+}
+
 }  // namespace jfb

@@ -1,0 +1,305 @@
+// Standalone tensor-product transforms: TensorProductSpace.backward / forward /
+// scalar_product (src/jaxfun/galerkin/tensorproductspace.py:253-551) for a
+// Chebyshev axis (orthogonal, Dirichlet or biharmonic basis) times one or two
+// Fourier axes, on full complex spectra in the reference layout, with the 3/2
+// padding of the Fourier axes (Fourier.py:128-184: zero padding in the middle,
+// unnormalised inverse, forward scaled 1/M and truncated to the modes
+// wavenumbers() keeps, Nyquist included).
+//
+//   x axis:       dense real operator per axis-0 line (x_apply_kernel)
+//   middle axis:  y_backward_kernel / y_forward_kernel (shared with the step)
+//   last axis:    fft_rows_kernel (contiguous lines, shared-memory Stockham)
+//
+// Included at the end of jfb_kmm.cu (one translation unit with the step).
+#pragma once
+
+#include "jfb_kmm_kernels.cuh"
+
+namespace jfb {
+
+// out[i][m] = sum_k A[i][k] in[k][m], A real (rows x cols), m < M contiguous.
+__global__ void __launch_bounds__(256) x_apply_kernel(const double* __restrict__ A, int rows,
+                                                      int cols, const c64* __restrict__ in,
+                                                      c64* __restrict__ out, int64_t M) {
+  const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (m >= M || i >= rows) return;
+  const double* a = A + (size_t)i * cols;
+  c64 s0 = cmk(0.0, 0.0), s1 = s0;
+  int k = 0;
+  for (; k + 1 < cols; k += 2) {
+    s0 = s0 + __ldg(a + k) * in[(size_t)k * M + m];
+    s1 = s1 + __ldg(a + k + 1) * in[(size_t)(k + 1) * M + m];
+  }
+  if (k < cols) s0 = s0 + __ldg(a + k) * in[(size_t)k * M + m];
+  out[(size_t)i * M + m] = s0 + s1;
+}
+
+// Complex FFT along contiguous lines: `lines` rows of length nin -> nout.
+// Inverse (sign +1, transform length nout): pad nin -> nout in the middle,
+// unnormalised.  Forward (sign -1, transform length nin): scaled 1/nin,
+// truncated to nout modes in FFT order (k < nout/2 and the last nout/2 of
+// the spectrum, the -nout/2 mode included).  kTpsRows lines per block.
+constexpr int kTpsRows = 8;
+__global__ void __launch_bounds__(256) fft_rows_kernel(FFTPlan plan, const c64* __restrict__ tw,
+                                                       int sign, const c64* __restrict__ in,
+                                                       c64* __restrict__ out, int64_t lines,
+                                                       int nin, int nout) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = plan.n;
+  c64* A = reinterpret_cast<c64*>(smem_raw);
+  c64* B = A + (size_t)n * kTpsRows;
+  const int64_t l0 = blockIdx.x * (int64_t)kTpsRows;
+  for (int idx = threadIdx.x; idx < n * kTpsRows; idx += blockDim.x) {
+    const int c = idx % kTpsRows, k = idx / kTpsRows;
+    const int64_t line = l0 + c;
+    c64 v = cmk(0.0, 0.0);
+    if (line < lines) {
+      if (sign > 0) {
+        const int h = nin / 2;
+        if (k < h) v = in[line * nin + k];
+        else if (k >= n - (nin - h)) v = in[line * nin + (k - n + nin)];
+      } else {
+        v = in[line * nin + k];
+      }
+    }
+    A[k * kTpsRows + c] = v;
+  }
+  __syncthreads();
+  c64* res = fft_columns<double>(A, B, plan, kTpsRows, kTpsRows, tw, sign);
+  const double scale = sign > 0 ? 1.0 : 1.0 / n;
+  const int h = nout / 2;
+  for (int idx = threadIdx.x; idx < nout * kTpsRows; idx += blockDim.x) {
+    const int c = idx % kTpsRows, k = idx / kTpsRows;
+    const int64_t line = l0 + c;
+    if (line >= lines) continue;
+    int src = k;
+    if (sign < 0 && k >= h) src = k - nout + n;
+    out[line * nout + k] = scale * res[src * kTpsRows + c];
+  }
+}
+
+__global__ void tps_scale_kernel(c64* __restrict__ y, double a, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    y[i] = a * y[i];
+}
+
+}  // namespace jfb
+
+struct jfb_tps {
+  jfb_tps_config cfg;
+  int nb = 0, N = 0;
+  int n1 = 1, n2 = 1, m1 = 1, m2 = 1;  // Fourier modes and padded counts
+  double *B = nullptr, *F = nullptr, *Sq = nullptr;
+  std::vector<double> G0, G2;
+  c64 *tw1n = nullptr, *tw1m = nullptr, *tw2n = nullptr, *tw2m = nullptr;
+  FFTPlan f1n, f1m, f2n, f2m;
+  c64 *w0 = nullptr, *w1 = nullptr;  // work buffers
+  std::vector<void*> allocs;
+};
+
+extern "C" int jfb_tps_destroy(jfb_tps* t) {
+  if (!t) return JFB_OK;
+  for (void* p : t->allocs) cudaFree(p);
+  delete t;
+  return JFB_OK;
+}
+
+extern "C" int jfb_tps_create(const jfb_tps_config* cfg, jfb_tps** out) {
+  JFB_REQUIRE(cfg && out, "null pointer");
+  *out = nullptr;
+  JFB_REQUIRE(cfg->ndim == 2 || cfg->ndim == 3, "ndim must be 2 or 3");
+  JFB_REQUIRE(cfg->basis >= 0 && cfg->basis <= 2, "unknown basis");
+  JFB_REQUIRE(cfg->n[0] >= 8 && cfg->n[0] <= 513, "n[0] out of range [8, 513]");
+  for (int a = 1; a < cfg->ndim; ++a)
+    JFB_REQUIRE(cfg->n[a] >= 2 && cfg->n[a] % 2 == 0, "Fourier sizes must be even");
+  JFB_REQUIRE(cfg->x_hi > cfg->x_lo, "bad domain");
+  jfb_tps* t = new jfb_tps();
+  t->cfg = *cfg;
+  auto fail = [&](int code) {
+    jfb_tps_destroy(t);
+    return code;
+  };
+  jfb_kmm_config kc;
+  std::memset(&kc, 0, sizeof(kc));
+  kc.nx = cfg->n[0];
+  kc.ny = 4;
+  kc.nz = 4;
+  kc.x_lo = cfg->x_lo;
+  kc.x_hi = cfg->x_hi;
+  kc.ly = kc.lz = 2.0 * M_PI;
+  HostOperators op;
+  build_host_operators(kc, op);
+  TpsX x;
+  build_tps_x_operators(op, cfg->basis, x);
+  t->N = x.N;
+  t->nb = x.nb;
+  t->G0 = x.G0;
+  t->G2 = x.G2;
+  t->n1 = cfg->n[1];
+  t->n2 = cfg->ndim == 3 ? cfg->n[2] : 1;
+  t->m1 = std::max(t->n1, (int)(cfg->pad[0] * t->n1));
+  t->m2 = cfg->ndim == 3 ? std::max(t->n2, (int)(cfg->pad[1] * t->n2)) : 1;
+  if (!make_fft_plan(t->n1, t->f1n) || !make_fft_plan(t->m1, t->f1m) ||
+      (cfg->ndim == 3 && (!make_fft_plan(t->n2, t->f2n) || !make_fft_plan(t->m2, t->f2m)))) {
+    set_error("Fourier sizes (and padded sizes) must be of the form 2^a 3^b");
+    return fail(JFB_ERR_ARG);
+  }
+  auto up = [&](auto** dst, const auto& v) -> int {
+    using E = typename std::decay_t<decltype(v)>::value_type;
+    cudaError_t e = cudaMalloc((void**)dst, std::max<size_t>(1, v.size()) * sizeof(E));
+    if (e != cudaSuccess) {
+      set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      return JFB_ERR_CUDA;
+    }
+    t->allocs.push_back(*dst);
+    e = cudaMemcpy(*dst, v.data(), v.size() * sizeof(E), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      set_error(std::string("cudaMemcpy: ") + cudaGetErrorString(e));
+      return JFB_ERR_CUDA;
+    }
+    return JFB_OK;
+  };
+  int st;
+  if ((st = up(&t->B, x.B)) || (st = up(&t->F, x.F)) || (st = up(&t->Sq, x.Sq))) return fail(st);
+  if ((st = up(&t->tw1n, twiddles(t->n1))) || (st = up(&t->tw1m, twiddles(t->m1))))
+    return fail(st);
+  if (cfg->ndim == 3 &&
+      ((st = up(&t->tw2n, twiddles(t->n2))) || (st = up(&t->tw2m, twiddles(t->m2)))))
+    return fail(st);
+  const size_t big = (size_t)std::max(t->N, t->nb) * t->m1 * t->m2;
+  for (c64** w : {&t->w0, &t->w1}) {
+    cudaError_t e = cudaMalloc((void**)w, big * sizeof(c64));
+    if (e != cudaSuccess) {
+      set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      return fail(JFB_ERR_CUDA);
+    }
+    t->allocs.push_back(*w);
+  }
+  if (allow_smem((const void*)y_backward_kernel<double>) != cudaSuccess ||
+      allow_smem((const void*)y_forward_kernel<double>) != cudaSuccess ||
+      allow_smem((const void*)fft_rows_kernel) != cudaSuccess) {
+    set_error("cannot configure the transform kernels");
+    return fail(JFB_ERR_CUDA);
+  }
+  *out = t;
+  return JFB_OK;
+}
+
+namespace jfb {
+
+static int tps_x(const double* A, int rows, int cols, const c64* in, c64* out, int64_t M,
+                 cudaStream_t s) {
+  dim3 g((unsigned)((M + 255) / 256), rows);
+  x_apply_kernel<<<g, 256, 0, s>>>(A, rows, cols, in, out, M);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+// middle axis of an array (rows, len, inner): the y kernels with Kz = inner
+static int tps_y(jfb_tps* t, int sign, int rows, int inner, const c64* in, c64* out,
+                 bool padded, cudaStream_t s) {
+  Dims d;
+  std::memset(&d, 0, sizeof(d));
+  d.Nx = rows;
+  d.Ny = t->n1;
+  d.Kz = inner;
+  d.P = t->n1 * inner;
+  d.My = padded ? t->m1 : t->n1;
+  const FFTPlan& plan = padded ? t->f1m : t->f1n;
+  const c64* tw = padded ? t->tw1m : t->tw1n;
+  int KC = inner;
+  while ((size_t)2 * d.My * KC * sizeof(c64) > 96 * 1024 && KC % 2 == 0) KC /= 2;
+  JFB_REQUIRE((size_t)2 * d.My * KC * sizeof(c64) <= 200 * 1024, "Fourier axis too long");
+  dim3 g(rows, 1, inner / KC);
+  const size_t sm = (size_t)2 * d.My * KC * sizeof(c64);
+  if (sign > 0) y_backward_kernel<double><<<g, 256, sm, s>>>(d, plan, KC, tw, in, out);
+  else y_forward_kernel<double><<<g, 256, sm, s>>>(d, plan, KC, tw, in, out, nullptr, 1);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+static int tps_z(jfb_tps* t, int sign, int64_t lines, const c64* in, c64* out, bool padded,
+                 cudaStream_t s) {
+  const int n = t->n2, m = padded ? t->m2 : t->n2;
+  const FFTPlan& plan = padded ? t->f2m : t->f2n;
+  const c64* tw = padded ? t->tw2m : t->tw2n;
+  const size_t sm = (size_t)2 * m * kTpsRows * sizeof(c64);
+  JFB_REQUIRE(sm <= 200 * 1024, "Fourier axis too long");
+  const int blocks = (int)((lines + kTpsRows - 1) / kTpsRows);
+  if (sign > 0) fft_rows_kernel<<<blocks, 256, sm, s>>>(plan, tw, +1, in, out, lines, n, m);
+  else fft_rows_kernel<<<blocks, 256, sm, s>>>(plan, tw, -1, in, out, lines, m, n);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+}  // namespace jfb
+
+extern "C" int jfb_tps_backward(jfb_tps* t, const void* coeffs, void* phys, int padded,
+                                void* stream) {
+  JFB_REQUIRE(t && coeffs && phys, "null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  const bool pad = padded != 0;
+  const int m1 = pad ? t->m1 : t->n1;
+  int st;
+  if (t->cfg.ndim == 2) {
+    // x: (nb, n1) -> (N, n1); y: -> (N, m1)
+    if ((st = tps_x(t->B, t->N, t->nb, (const c64*)coeffs, t->w0, t->n1, s))) return st;
+    return tps_y(t, +1, t->N, 1, t->w0, (c64*)phys, pad, s);
+  }
+  if ((st = tps_x(t->B, t->N, t->nb, (const c64*)coeffs, t->w0, (int64_t)t->n1 * t->n2, s)))
+    return st;
+  if ((st = tps_y(t, +1, t->N, t->n2, t->w0, t->w1, pad, s))) return st;
+  return tps_z(t, +1, (int64_t)t->N * m1, t->w1, (c64*)phys, pad, s);
+}
+
+extern "C" int jfb_tps_forward(jfb_tps* t, const void* phys, void* coeffs, int padded, int kind,
+                               void* stream) {
+  JFB_REQUIRE(t && phys && coeffs, "null pointer");
+  JFB_REQUIRE(kind == 0 || kind == 1, "kind must be 0 (forward) or 1 (scalar product)");
+  cudaStream_t s = (cudaStream_t)stream;
+  const bool pad = padded != 0;
+  const int m1 = pad ? t->m1 : t->n1;
+  const double* X = kind ? t->Sq : t->F;
+  int st;
+  if (t->cfg.ndim == 2) {
+    if ((st = tps_y(t, -1, t->N, 1, (const c64*)phys, t->w0, pad, s))) return st;
+    if ((st = tps_x(X, t->nb, t->N, t->w0, (c64*)coeffs, t->n1, s))) return st;
+  } else {
+    if ((st = tps_z(t, -1, (int64_t)t->N * m1, (const c64*)phys, t->w0, pad, s))) return st;
+    if ((st = tps_y(t, -1, t->N, t->n2, t->w0, t->w1, pad, s))) return st;
+    if ((st = tps_x(X, t->nb, t->N, t->w1, (c64*)coeffs, (int64_t)t->n1 * t->n2, s))) return st;
+  }
+  if (kind == 1) {
+    // scalar products carry the Fourier weight 2 pi / df per periodic axis
+    // (Fourier.py:152-167); the forward transform does not
+    double w = 1.0;
+    for (int a = 0; a + 1 < t->cfg.ndim; ++a) {
+      const double L = t->cfg.l[a];
+      const double df = std::fabs(L - 2.0 * M_PI) < 1e-12 ? 1.0 : 2.0 * M_PI / L;
+      w *= 2.0 * M_PI / df;
+    }
+    const size_t n = (size_t)t->nb * t->n1 * t->n2;
+    tps_scale_kernel<<<256, 256, 0, s>>>((c64*)coeffs, w, n);
+    JFB_CHECK_LAUNCH();
+  }
+  return JFB_OK;
+}
+
+extern "C" int jfb_tps_galerkin(const jfb_tps* t, int order, double* out) {
+  JFB_REQUIRE(t && out, "null pointer");
+  JFB_REQUIRE(order == 0 || order == 2, "order must be 0 or 2");
+  const std::vector<double>& G = order ? t->G2 : t->G0;
+  std::copy(G.begin(), G.end(), out);
+  return JFB_OK;
+}
+
+extern "C" int jfb_tps_get_sizes(const jfb_tps* t, int32_t* out4) {
+  JFB_REQUIRE(t && out4, "null pointer");
+  out4[0] = t->nb;
+  out4[1] = t->N;
+  out4[2] = t->m1;
+  out4[3] = t->m2;
+  return JFB_OK;
+}

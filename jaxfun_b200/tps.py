@@ -1,0 +1,161 @@
+"""Tensor-product spaces (Chebyshev-family x Fourier [x Fourier]) and the
+2-D Helmholtz solver, backed by ``libjfb200.so``.
+
+``TensorProductSpace`` mirrors ``jaxfun.galerkin.TensorProductSpace``
+(tensorproductspace.py:104-594) for the spaces of the hot path: ``backward``,
+``forward``, ``scalar_product`` (padded or not) on full complex spectra in the
+reference layout.  ``Helmholtz2D`` is the Shen-Galerkin solver of
+``-lap u + alpha u = f`` (la/solvers.py:22-61 with the per-wavenumber banded
+solve of tpmatrix.py:1550-1677): scalar products of f, one banded solve per
+Fourier mode, backward transform.  All arithmetic runs on the GPU; there is no
+CPU path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .la import DiaMatrix, TPMatrices, TPMatrix, tpmats_wavenumber_factor
+
+_BASES = {"C": _lib.JFB_BASIS_ORTHOGONAL, "D": _lib.JFB_BASIS_DIRICHLET,
+          "B": _lib.JFB_BASIS_BIHARMONIC}
+
+
+def _stream(dev) -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+
+class TensorProductSpace:
+    """``TensorProduct(x_space, Fourier[, Fourier])``.
+
+    basis: "C" (orthogonal Chebyshev), "D" (Dirichlet), "B" (biharmonic);
+    N = (x points, Fourier modes...); domain = ((x_lo, x_hi), (y0, y1)[, (z0, z1)]);
+    padding_factor as in ``get_dealiased`` (the x entry is ignored).
+    """
+
+    def __init__(self, basis: str, N, domain, padding_factor=None, device="cuda"):
+        self.N = tuple(int(n) for n in N)
+        self.ndim = len(self.N)
+        if self.ndim not in (2, 3):
+            raise ValueError("2-D or 3-D spaces only")
+        if basis not in _BASES:
+            raise ValueError("basis must be 'C', 'D' or 'B'")
+        self.basis = basis
+        self.domain = tuple(tuple(float(v) for v in d) for d in domain)
+        pad = tuple(padding_factor) if padding_factor is not None else (1.0,) * self.ndim
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise ValueError("the transforms run on a CUDA device only")
+        cfg = _lib.TPSConfig()
+        cfg.ndim = self.ndim
+        cfg.basis = _BASES[basis]
+        for a in range(3):
+            cfg.n[a] = self.N[a] if a < self.ndim else 1
+        cfg.x_lo, cfg.x_hi = self.domain[0]
+        for a in range(self.ndim - 1):
+            cfg.l[a] = self.domain[a + 1][1] - self.domain[a + 1][0]
+            cfg.pad[a] = float(pad[a + 1])
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.call("jfb_tps_create", ctypes.byref(cfg), ctypes.byref(h))
+        self._h = h
+        sizes = (ctypes.c_int32 * 4)()
+        _lib.call("jfb_tps_get_sizes", h, sizes)
+        self.num_dofs = (sizes[0],) + self.N[1:]
+        self.padded_counts = (sizes[1], sizes[2]) + ((sizes[3],) if self.ndim == 3 else ())
+        self.counts = self.N
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.load().jfb_tps_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def _check(self, t: torch.Tensor, shape) -> torch.Tensor:
+        if not t.is_cuda:
+            raise ValueError("arrays must live on a CUDA device")
+        if tuple(t.shape) != tuple(shape):
+            raise ValueError(f"expected shape {tuple(shape)}, received {tuple(t.shape)}")
+        return t.to(torch.complex128).contiguous()
+
+    def backward(self, c: torch.Tensor, padded: bool = False) -> torch.Tensor:
+        c = self._check(c, self.num_dofs)
+        shape = self.padded_counts if padded else self.counts
+        out = torch.empty(shape, dtype=torch.complex128, device=self.device)
+        _lib.call("jfb_tps_backward", self._h, c.data_ptr(), out.data_ptr(), int(padded),
+                  _stream(self.device))
+        return out
+
+    def _fwd(self, u: torch.Tensor, padded: bool, kind: int) -> torch.Tensor:
+        u = self._check(u, self.padded_counts if padded else self.counts)
+        out = torch.empty(self.num_dofs, dtype=torch.complex128, device=self.device)
+        _lib.call("jfb_tps_forward", self._h, u.data_ptr(), out.data_ptr(), int(padded), kind,
+                  _stream(self.device))
+        return out
+
+    def forward(self, u: torch.Tensor, padded: bool = False) -> torch.Tensor:
+        return self._fwd(u, padded, 0)
+
+    def scalar_product(self, u: torch.Tensor, padded: bool = False) -> torch.Tensor:
+        return self._fwd(u, padded, 1)
+
+    def galerkin(self, order: int) -> np.ndarray:
+        """Dense (phi_i, phi_j^(order))_w along x (host array)."""
+        nb = self.num_dofs[0]
+        out = (ctypes.c_double * (nb * nb))()
+        _lib.call("jfb_tps_galerkin", self._h, int(order), out)
+        return np.frombuffer(out, dtype=np.float64).reshape(nb, nb).copy()
+
+    def wavenumbers(self, axis: int) -> torch.Tensor:
+        """Physical Fourier wavenumbers (FFT order) along a periodic axis."""
+        n = self.N[axis]
+        L = self.domain[axis][1] - self.domain[axis][0]
+        k = torch.fft.fftfreq(n, d=1.0 / n, dtype=torch.float64)
+        return (k * (2.0 * math.pi / L)).to(self.device)
+
+
+class Helmholtz2D:
+    """``-lap u + alpha u = f`` on Chebyshev-Dirichlet (x) x Fourier (y)
+    (la/solvers.py:22-61): scalar products of f, one banded Galerkin solve
+    per Fourier mode (``TPMatricesWavenumberSolver``), backward transform."""
+
+    def __init__(self, N=(64, 64), domain=((-1.0, 1.0), (0.0, 2.0 * math.pi)),
+                 alpha: float = 1.0, device="cuda"):
+        self.TD = TensorProductSpace("D", N, domain, device=device)
+        self.TC = TensorProductSpace("C", N, domain, device=device)
+        self.device = self.TD.device
+        G0, G2 = self.TD.galerkin(0), self.TD.galerkin(2)
+        k = self.TD.wavenumbers(1)
+        M = int(N[1])
+        dev = self.device
+        ident = DiaMatrix(torch.ones((1, M), dtype=torch.float64, device=dev), [0], (M, M))
+        kk = DiaMatrix((k * k + alpha).reshape(1, M), [0], (M, M))
+
+        def dia(a):  # every structurally nonzero diagonal, however small
+            n = a.shape[0]
+            offs = [k for k in range(-(n - 1), n) if np.any(np.diagonal(a, k) != 0.0)]
+            return DiaMatrix.from_dense(torch.from_numpy(a).to(dev), offsets=offs)
+
+        A = TPMatrices([TPMatrix([dia(-G2), ident]), TPMatrix([dia(G0), kk])])
+        self.solver = tpmats_wavenumber_factor(A)
+        # the Fourier mass 2 pi / df = L of the scalar product is not in A
+        self._fourier_mass = domain[1][1] - domain[1][0]
+
+    def solve_coefficients(self, f_phys: torch.Tensor) -> torch.Tensor:
+        """Dirichlet x Fourier coefficients of u from samples of f."""
+        rhs = self.TD.scalar_product(f_phys) / self._fourier_mass
+        return self.solver.solve(rhs)
+
+    def __call__(self, f_hat: torch.Tensor) -> torch.Tensor:
+        """f given by orthogonal Chebyshev x Fourier coefficients: backward,
+        scalar products, per-mode solves, backward; returns u on the mesh."""
+        f_phys = self.TC.backward(f_hat)
+        return self.TD.backward(self.solve_coefficients(f_phys))

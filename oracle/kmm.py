@@ -1588,3 +1588,45 @@ class PlaneCouetteMRIOracle(PlaneCouetteMHDOracle):
         self.Ub = -self.shear_rate * self.X[0]
         self.Ubp = -self.shear_rate * self.Xp[0]
         self.dUb_dx = -self.shear_rate
+
+
+# ---------------------------------------------------------------------------
+# 2-D Helmholtz: -lap u + alpha u = f on Chebyshev-Dirichlet (x) x Fourier (y)
+# (la/solvers.py:22-61; the pipeline of the 2-D Helmholtz benchmark case)
+# ---------------------------------------------------------------------------
+
+
+def helmholtz2d_forcing(N=(64, 64), seed=1) -> np.ndarray:
+    """Seeded orthogonal-Chebyshev x Fourier coefficients of f:
+    (a + i b)/sqrt(2) (1 + j)^-2 (1 + |k|)^-2, a, b ~ N(0, 1) (PCG64), made
+    Hermitian in k (a real f) with the Nyquist mode zero."""
+    Nx, Ny = N
+    rng = np.random.Generator(np.random.PCG64(seed))
+    a = rng.standard_normal((Nx, Ny))
+    b = rng.standard_normal((Nx, Ny))
+    j = np.arange(Nx)[:, None]
+    k = np.fft.fftfreq(Ny, 1.0 / Ny)[None, :]
+    c = (a + 1j * b) / np.sqrt(2.0) * (1.0 + j) ** -2 * (1.0 + np.abs(k)) ** -2
+    c[:, Ny // 2] = 0.0
+    kk = (-np.arange(Ny)) % Ny
+    return 0.5 * (c + np.conj(c[:, kk]))
+
+
+def helmholtz2d_solve(f_hat: np.ndarray, domain=((-1.0, 1.0), (0.0, 2.0 * math.pi)),
+                      alpha: float = 1.0):
+    """Reference FP64 solution: f = TC.backward(f_hat); per Fourier mode the
+    Galerkin system (-(phi_i, phi_j'') + (k^2 + alpha)(phi_i, phi_j)) u = (phi_i, f)
+    solved densely; returns (Dirichlet x Fourier coefficients, u on the mesh)."""
+    Nx, Ny = f_hat.shape
+    orth = make_orthogonal("C", Nx, domain[0])
+    D = Composite1D(orth, "dirichlet")
+    F = Fourier1D(Ny, domain[1])
+    f = F.backward(orth.backward(f_hat, None, 0), None, 1)
+    rhs = D.scalar_product(F.forward(f, 1), 0)
+    G0, G2 = D.galerkin_matrix(0), D.galerkin_matrix(2)
+    k = F.wavenumbers() * F.df
+    u_hat = np.empty_like(rhs)
+    for m in range(Ny):
+        u_hat[:, m] = np.linalg.solve(-G2 + (k[m] ** 2 + alpha) * G0, rhs[:, m])
+    u = F.backward(D.backward(u_hat, None, 0), None, 1)
+    return u_hat, u

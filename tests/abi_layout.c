@@ -25,5 +25,8 @@ int main(void) {
   F(jfb_mhd_state, nonlinear_A_older); F(jfb_mhd_state, A_old); F(jfb_mhd_state, A_older);
   printf("jfb_mhd_params %zu\n", sizeof(jfb_mhd_params));
   F(jfb_mhd_params, eta); F(jfb_mhd_params, omega); F(jfb_mhd_params, b0);
+  printf("jfb_tps_config %zu\n", sizeof(jfb_tps_config));
+  F(jfb_tps_config, ndim); F(jfb_tps_config, n); F(jfb_tps_config, x_lo);
+  F(jfb_tps_config, l); F(jfb_tps_config, pad);
   return 0;
 }

@@ -65,7 +65,8 @@ def c_layout(tmp_path_factory):
                                         ("jfb_kmm_state", _lib.KMMStateC),
                                         ("jfb_kmm_info", _lib.KMMInfo),
                                         ("jfb_mhd_state", _lib.MHDStateC),
-                                        ("jfb_mhd_params", _lib.MHDParams)])
+                                        ("jfb_mhd_params", _lib.MHDParams),
+                                        ("jfb_tps_config", _lib.TPSConfig)])
 def test_struct_layouts_match_c(c_layout, cname, cls):
     assert int(c_layout[cname]) == ctypes.sizeof(cls)
     for key, off in c_layout.items():
