@@ -67,6 +67,8 @@ def parse_args(argv=None):
     p.add_argument("--no-ensemble", action="store_true",
                    help="skip the MHD ensemble block")
     p.add_argument("--ensemble-members", type=int, default=32)
+    p.add_argument("--no-helmholtz", action="store_true",
+                   help="skip the 2-D Helmholtz block")
     return p.parse_args(argv)
 
 
@@ -589,11 +591,70 @@ def main(argv=None):
             "sample_diagnostics": [{k: d[k] for k in ("Epert", "Emag", "divB_L2")} for d in diags],
         }
 
+    def helmholtz_block():
+        """The 2-D Helmholtz case: -lap u + u = f on 64 Chebyshev-Dirichlet x
+        64 Fourier modes, seeded forcing; one solve = backward of f, scalar
+        products, per-mode banded solves, backward of u.  Accuracy from a
+        manufactured solution (f built from random coefficients of u with
+        numpy's Chebyshev derivative), time per solve with CUDA events."""
+        import numpy as np
+        from numpy.polynomial import chebyshev as npc
+
+        from jaxfun_b200.tps import Helmholtz2D
+        from jaxfun_b200.workloads import helmholtz2d_forcing
+
+        N = (64, 64)
+        h = Helmholtz2D(N, device=dev)
+        f_hat = torch.from_numpy(helmholtz2d_forcing(N, seed=1)).to(dev)
+        rng = np.random.default_rng(2)
+        uh = rng.standard_normal((N[0] - 2, N[1])) + 1j * rng.standard_normal((N[0] - 2, N[1]))
+        uh[:, N[1] // 2] = 0
+        uo = np.zeros((N[0], N[1]), dtype=complex)
+        uo[:-2] += uh
+        uo[2:] -= uh
+        d2 = np.zeros_like(uo)
+        d2[: N[0] - 2] = npc.chebder(uo, 2, axis=0)
+        k = np.fft.fftfreq(N[1], 1.0 / N[1])
+        fm = -d2 + (k[None, :] ** 2 + 1.0) * uo
+        got = h.solve_coefficients(h.TC.backward(torch.from_numpy(fm).to(dev))).cpu().numpy()
+        err = float(np.linalg.norm(got - uh) / np.linalg.norm(uh))
+        for _ in range(5):
+            h(f_hat)
+        torch.cuda.synchronize(dev)
+        K = 200
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            u = h(f_hat)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        us = e0.elapsed_time(e1) * 1000.0 / K
+        out = {
+            "workload": "-lap u + u = f, 64 Chebyshev-Dirichlet x 64 Fourier, seeded forcing",
+            "us_per_solve": us,
+            "solves": K,
+            "manufactured_rel_l2": err,
+            "u_max": float(u.abs().max()),
+        }
+        if not args.no_cpu_baseline:
+            from oracle import kmm as ok
+
+            fh = helmholtz2d_forcing(N, seed=1)
+            t0 = time.perf_counter()
+            n = 0
+            while time.perf_counter() - t0 < 2.0:
+                ok.helmholtz2d_solve(fh)
+                n += 1
+            out["cpu_baseline"] = {"us_per_solve": (time.perf_counter() - t0) * 1e6 / n,
+                                   "kind": "port", "cores": 1, "sample": f"{n} oracle solves"}
+        return out
+
     forms = ("mixed", "fp64") if args.precision == "both" else (args.precision,)
     results = {p: measure(p) for p in forms}
     err = mixed_error() if "mixed" in forms and rank == 0 else None
     adj = adjoint_block() if (rank == 0 and world == 1 and not args.no_adjoint) else None
     ensb = ensemble_block() if (rank == 0 and world == 1 and not args.no_ensemble) else None
+    helm = helmholtz_block() if (rank == 0 and world == 1 and not args.no_helmholtz) else None
 
     if rank != 0:
         if world > 1:
@@ -632,6 +693,8 @@ def main(argv=None):
         line["adjoint"] = adj
     if ensb is not None:
         line["mhd_ensemble"] = ensb
+    if helm is not None:
+        line["helmholtz2d"] = helm
     if world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         rate, n = cpu_oracle_rate(fields, grid, args.cpu_seconds, threads)

@@ -72,3 +72,20 @@ def scale_to_energy(fields, energy_now: float, target: float):
     """Scale physical fields linearly so the projected energy equals target."""
     s = math.sqrt(target / energy_now)
     return tuple(f * s for f in fields)
+
+
+def helmholtz2d_forcing(N=(64, 64), seed=1) -> np.ndarray:
+    """Seeded forcing of the 2-D Helmholtz case: orthogonal Chebyshev x
+    Fourier coefficients (a + i b)/sqrt(2) (1 + j)^-2 (1 + |k|)^-2 with
+    a, b ~ N(0, 1) (numpy PCG64), made Hermitian in k (a real f), Nyquist
+    mode zero."""
+    Nx, Ny = N
+    rng = np.random.Generator(np.random.PCG64(seed))
+    a = rng.standard_normal((Nx, Ny))
+    b = rng.standard_normal((Nx, Ny))
+    j = np.arange(Nx)[:, None]
+    k = np.fft.fftfreq(Ny, 1.0 / Ny)[None, :]
+    c = (a + 1j * b) / np.sqrt(2.0) * (1.0 + j) ** -2 * (1.0 + np.abs(k)) ** -2
+    c[:, Ny // 2] = 0.0
+    kk = (-np.arange(Ny)) % Ny
+    return 0.5 * (c + np.conj(c[:, kk]))
