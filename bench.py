@@ -69,6 +69,8 @@ def parse_args(argv=None):
     p.add_argument("--ensemble-members", type=int, default=32)
     p.add_argument("--no-helmholtz", action="store_true",
                    help="skip the 2-D Helmholtz block")
+    p.add_argument("--no-sizes", action="store_true",
+                   help="skip the 97^3 / 129^3 mixed-vs-FP64 block")
     return p.parse_args(argv)
 
 
@@ -649,12 +651,58 @@ def main(argv=None):
                                    "kind": "port", "cores": 1, "sample": f"{n} oracle solves"}
         return out
 
+    def sizes_block():
+        """The same Couette workload at 97^3 and 129^3 (wall-normal points x
+        Fourier modes): steady steps/s of both forms (graph replay, CUDA
+        events) and the per-field relative L2 distance of the mixed form to
+        the FP64 form after 100 and 1000 steps."""
+        out = {}
+        for n in (97, 129):
+            grid_n = (n, n - 1, n - 1)
+            f0 = couette_perturbation_fields(grid_n, domain())
+            rec = {}
+            states = {}
+            for prec in ("fp64", "mixed"):
+                sv = PlaneCouetteFluctuation(N=grid_n, domain=domain(), Re=RE, dt=DT,
+                                             precision=prec, device=dev)
+                if prec == "fp64":
+                    e0 = sv.diagnostics(sv.state_from_physical(f0))["Epert"]
+                    fields_n = scale_to_energy(f0, e0, ENERGY)
+                st = sv.state_from_physical(fields_n)
+                st = sv.solve(st, 5)
+                torch.cuda.synchronize(dev)
+                K = 20
+                e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0_.record(stream)
+                sv.advance_resident(K)
+                e1_.record(stream)
+                torch.cuda.synchronize(dev)
+                ms = e0_.elapsed_time(e1_) / K
+                rec[prec] = {"ms_per_step": ms, "steps_per_s": 1000.0 / ms,
+                             "launches_per_step": sv.info().launches_per_step}
+                states[prec] = (sv, sv.state_from_physical(fields_n))
+            (g64, a), (g32, b) = states["fp64"], states["mixed"]
+            done = 0
+            for m in (100, 1000):
+                a, b = g64.solve(a, m - done), g32.solve(b, m - done)
+                done = m
+                errs = {}
+                for name, x, y in zip(("u0", "u1", "u2", "g"), (*b.u, b.g), (*a.u, a.g), strict=True):
+                    errs[name] = float(torch.linalg.norm(x - y) / torch.linalg.norm(y))
+                num = sum(float(torch.linalg.norm(x - y)) ** 2 for x, y in zip((*b.u, b.g), (*a.u, a.g)))
+                den = sum(float(torch.linalg.norm(y)) ** 2 for y in (*a.u, a.g))
+                errs["state"] = math.sqrt(num / den)
+                rec[f"mixed_vs_fp64_after_{m}_steps"] = errs
+            out[f"{n}x{n - 1}x{n - 1}"] = rec
+        return out
+
     forms = ("mixed", "fp64") if args.precision == "both" else (args.precision,)
     results = {p: measure(p) for p in forms}
     err = mixed_error() if "mixed" in forms and rank == 0 else None
     adj = adjoint_block() if (rank == 0 and world == 1 and not args.no_adjoint) else None
     ensb = ensemble_block() if (rank == 0 and world == 1 and not args.no_ensemble) else None
     helm = helmholtz_block() if (rank == 0 and world == 1 and not args.no_helmholtz) else None
+    sizes = sizes_block() if (rank == 0 and world == 1 and not args.no_sizes) else None
 
     if rank != 0:
         if world > 1:
@@ -695,6 +743,8 @@ def main(argv=None):
         line["mhd_ensemble"] = ensb
     if helm is not None:
         line["helmholtz2d"] = helm
+    if sizes is not None:
+        line["larger_grids"] = sizes
     if world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         rate, n = cpu_oracle_rate(fields, grid, args.cpu_seconds, threads)

@@ -303,7 +303,10 @@ class TPMatricesWavenumberSolver:
         cplx = rhs.is_complex()
         r = rhs.to(torch.complex128 if cplx else torch.float64).contiguous()
         out = torch.empty_like(r)
-        lo, uo = _lib.int64_array(self.L_offsets), _lib.int64_array(self.U_offsets)
+        if not hasattr(self, "_offset_arrays"):
+            self._offset_arrays = (_lib.int64_array(self.L_offsets),
+                                   _lib.int64_array(self.U_offsets))
+        lo, uo = self._offset_arrays
         L = L.contiguous()
         U = U.contiguous()
         _lib.call("jfb_wavenumber_solve", L.data_ptr() if L.numel() else None, lo,
