@@ -117,12 +117,25 @@ __device__ __forceinline__ void warp_fft_inverse(cpx<T> (&v)[P], const WarpTw<P,
   for (int s = 0; s < 5; ++s) {
     const int h = 16 >> s;
     const bool bottom = (lane & h) != 0;
-    cpx<T> tws = w.stage[s];
-    tws.im = -tws.im;
+    // FP32: top lanes v + p, bottom lanes (p - v) conj(w), formed as
+    // (p + sg v) t with (sg, t) = (1, 1) on top, (-1, conj(w)) below
+    if constexpr (sizeof(T) == 4) {
+      const T sg = bottom ? T(-1) : T(1);
+      const cpx<T> t = bottom ? cmk(w.stage[s].re, -w.stage[s].im) : cmk(T(1), T(0));
 #pragma unroll
-    for (int r = 0; r < P; ++r) {
-      const cpx<T> p = shfl_xor_c(v[r], h);
-      v[r] = bottom ? (p - v[r]) * tws : v[r] + p;
+      for (int r = 0; r < P; ++r) {
+        const cpx<T> p = shfl_xor_c(v[r], h);
+        const cpx<T> d = cmk(p.re + sg * v[r].re, p.im + sg * v[r].im);
+        v[r] = d * t;  // t = 1 on the top lanes: exact
+      }
+    } else {  // FP64: fewer live temporaries (register pressure of its callers)
+      cpx<T> tws = w.stage[s];
+      tws.im = -tws.im;
+#pragma unroll
+      for (int r = 0; r < P; ++r) {
+        const cpx<T> p = shfl_xor_c(v[r], h);
+        v[r] = bottom ? (p - v[r]) * tws : v[r] + p;
+      }
     }
   }
 }
@@ -136,10 +149,22 @@ __device__ __forceinline__ void warp_fft_forward(cpx<T> (&v)[P], const WarpTw<P,
     const int h = 16 >> s;
     const bool bottom = (lane & h) != 0;
     const cpx<T> tws = w.stage[s];
+    if constexpr (sizeof(T) == 4) {
+      const T sg = bottom ? T(-1) : T(1);
 #pragma unroll
-    for (int r = 0; r < P; ++r) {
-      const cpx<T> p = shfl_xor_c(v[r], h);
-      v[r] = bottom ? p - v[r] * tws : v[r] + p * tws;
+      for (int r = 0; r < P; ++r) {
+        // top lanes: v + p w; bottom lanes: p - v w -- one product per value
+        const cpx<T> p = shfl_xor_c(v[r], h);
+        const cpx<T> a = bottom ? p : v[r];
+        const cpx<T> m = (bottom ? v[r] : p) * tws;
+        v[r] = cmk(a.re + sg * m.re, a.im + sg * m.im);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < P; ++r) {
+        const cpx<T> p = shfl_xor_c(v[r], h);
+        v[r] = bottom ? p - v[r] * tws : v[r] + p * tws;
+      }
     }
   }
 #pragma unroll
