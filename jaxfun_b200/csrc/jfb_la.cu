@@ -188,6 +188,121 @@ __global__ void wavenumber_solve_kernel(const double* __restrict__ L, OffsetTabl
   }
 }
 
+// Same solve, one warp per (rhs r, Fourier mode f) for factors with many
+// diagonals (dense upper triangles of Chebyshev stiffness matrices): the
+// system's vector lives in shared memory, the lanes split the sum over the
+// diagonals of each row (the factor entries of the next row are loaded while
+// the current row is reduced), lane 0 writes the row.  Rows stay sequential.
+template <typename V>
+__global__ void wavenumber_solve_warp_kernel(const double* __restrict__ L, OffsetTable loff,
+                                             const double* __restrict__ U, OffsetTable uoff,
+                                             int main_idx, int n_P, int64_t outer,
+                                             int64_t inner, int64_t n_rhs, V* __restrict__ x_all) {
+  extern __shared__ double wsm[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double* xr = wsm + (size_t)wib * 2 * n_P;
+  double* xi = xr + n_P;
+  const int64_t n_F = outer * inner;
+  const int64_t gid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (gid >= n_F * n_rhs) return;
+  const int64_t t = gid % inner;
+  const int64_t o = (gid / inner) % outer;
+  const int64_t r = gid / n_F;
+  const int64_t f = o * inner + t;
+  const int64_t base = (r * outer + o) * (int64_t)n_P * inner + t;
+  const double* Lf = L + f * (int64_t)loff.n * n_P;
+  const double* Uf = U + f * (int64_t)uoff.n * n_P;
+  V* x = x_all + base;
+  constexpr bool kCplx = sizeof(V) != sizeof(double);
+  for (int i = lane; i < n_P; i += 32) {
+    if constexpr (kCplx) {
+      const V v = x[(int64_t)i * inner];
+      xr[i] = v.re;
+      xi[i] = v.im;
+    } else {
+      xr[i] = x[(int64_t)i * inner];
+      xi[i] = 0.0;
+    }
+  }
+  __syncwarp();
+  auto reduce = [&](double& a, double& b) {
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, m);
+      b += __shfl_xor_sync(0xffffffffu, b, m);
+    }
+  };
+  // factor entry of row i on this lane's first diagonal (0 when out of range)
+  auto lval = [&](int i) {
+    if (lane >= loff.n) return 0.0;
+    const int j = i + loff.off[lane];
+    return (j >= 0) ? Lf[(int64_t)lane * n_P + j] : 0.0;
+  };
+  auto uval = [&](int i) {
+    if (lane >= uoff.n || uoff.off[lane] == 0) return 0.0;
+    const int j = i + uoff.off[lane];
+    return (j < n_P) ? Uf[(int64_t)lane * n_P + j] : 0.0;
+  };
+  double lnext = lval(0);
+  for (int i = 0; i < n_P; ++i) {
+    const double lc = lnext;
+    if (i + 1 < n_P) lnext = lval(i + 1);
+    double ar = 0.0, ai = 0.0;
+    if (lane < loff.n) {
+      const int j = i + loff.off[lane];
+      if (j >= 0) {
+        ar = lc * xr[j];
+        ai = lc * xi[j];
+      }
+    }
+    for (int d = lane + 32; d < loff.n; d += 32) {
+      const int j = i + loff.off[d];
+      if (j < 0) continue;
+      const double l = Lf[(int64_t)d * n_P + j];
+      ar += l * xr[j];
+      ai += l * xi[j];
+    }
+    reduce(ar, ai);
+    if (lane == 0) {
+      xr[i] -= ar;
+      xi[i] -= ai;
+    }
+    __syncwarp();
+  }
+  double unext = uval(n_P - 1);
+  for (int i = n_P - 1; i >= 0; --i) {
+    const double uc = unext;
+    if (i > 0) unext = uval(i - 1);
+    double ar = 0.0, ai = 0.0;
+    if (lane < uoff.n && uoff.off[lane] != 0) {
+      const int j = i + uoff.off[lane];
+      if (j < n_P) {
+        ar = uc * xr[j];
+        ai = uc * xi[j];
+      }
+    }
+    for (int d = lane + 32; d < uoff.n; d += 32) {
+      const int sft = uoff.off[d];
+      const int j = i + sft;
+      if (sft == 0 || j >= n_P) continue;
+      const double u = Uf[(int64_t)d * n_P + j];
+      ar += u * xr[j];
+      ai += u * xi[j];
+    }
+    reduce(ar, ai);
+    if (lane == 0) {
+      const double diag = Uf[(int64_t)main_idx * n_P + i];
+      xr[i] = (xr[i] - ar) / diag;
+      xi[i] = (xi[i] - ai) / diag;
+    }
+    __syncwarp();
+  }
+  for (int i = lane; i < n_P; i += 32) {
+    if constexpr (kCplx) x[(int64_t)i * inner] = cmk(xr[i], xi[i]);
+    else x[(int64_t)i * inner] = xr[i];
+  }
+}
+
 static int fill_offsets(OffsetTable& t, const int64_t* offs, int64_t n) {
   if (n < 0 || n > kMaxOffsets) {
     set_error("too many DIA offsets (max 512)");
@@ -286,6 +401,19 @@ extern "C" int jfb_wavenumber_solve(const double* L, const int64_t* L_offsets, i
   }
   const int64_t total = n_rhs * outer * inner;
   const int threads = 128;
+  if (lt.n + ut.n > 8) {  // wide factors: a warp per system
+    const int64_t wblocks = (total * 32 + threads - 1) / threads;
+    const size_t sm = (size_t)(threads / 32) * 2 * n_P * sizeof(double);
+    JFB_REQUIRE(sm <= 48 * 1024, "n_P too large for the warp solve (max 768)");
+    if (is_complex)
+      wavenumber_solve_warp_kernel<c64><<<(unsigned)wblocks, threads, sm, s>>>(
+          L, lt, U, ut, main_idx, (int)n_P, outer, inner, n_rhs, (c64*)out);
+    else
+      wavenumber_solve_warp_kernel<double><<<(unsigned)wblocks, threads, sm, s>>>(
+          L, lt, U, ut, main_idx, (int)n_P, outer, inner, n_rhs, out);
+    JFB_CHECK_LAUNCH();
+    return JFB_OK;
+  }
   const int blocks = (int)((total + threads - 1) / threads);
   if (is_complex) {
     wavenumber_solve_kernel<c64><<<blocks, threads, 0, s>>>(

@@ -78,3 +78,18 @@ def test_helmholtz2d_manufactured_solution(cuda):
     h = Helmholtz2D((Nx, Ny), device=cuda)
     f_phys = h.TC.backward(torch.from_numpy(f_hat).to(cuda))
     assert rel(h.solve_coefficients(f_phys), uh) < 1e-11
+
+
+def test_helmholtz2d_graph_replay_matches_eager(cuda):
+    f_hat = torch.from_numpy(ok.helmholtz2d_forcing((64, 64), seed=3)).to(cuda)
+    h = Helmholtz2D((64, 64), device=cuda)
+    eager = h(f_hat)
+    g, f_in, u_out = h.graphed(f_hat)
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(u_out, eager)
+    f2 = torch.from_numpy(ok.helmholtz2d_forcing((64, 64), seed=4)).to(cuda)
+    f_in.copy_(f2)
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(u_out, h(f2))
