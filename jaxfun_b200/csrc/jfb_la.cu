@@ -188,16 +188,21 @@ __global__ void wavenumber_solve_kernel(const double* __restrict__ L, OffsetTabl
   }
 }
 
-// Same solve, one warp per (rhs r, Fourier mode f) for factors with many
-// diagonals (dense upper triangles of Chebyshev stiffness matrices): the
-// system's vector lives in shared memory, the lanes split the sum over the
-// diagonals of each row (the factor entries of the next row are loaded while
-// the current row is reduced), lane 0 writes the row.  Rows stay sequential.
+// Same solve, one warp per (rhs r, Fourier mode f), for factors with many
+// diagonals (the dense upper triangles of Chebyshev stiffness matrices).
+// Column-oriented substitution on the system's vector in shared memory: once
+// x_c is final, lane t applies the column-c entry of diagonal t to that
+// diagonal's row (distinct diagonals hit distinct rows, so the updates of one
+// column are independent).  The dependent chain is one shared read, (for U)
+// a division and one update per column; the factor entries of the next
+// column are loaded while the current one is applied.  Reads rhs, writes out
+// (in place allowed: a warp reads its whole vector before it writes).
 template <typename V>
 __global__ void wavenumber_solve_warp_kernel(const double* __restrict__ L, OffsetTable loff,
                                              const double* __restrict__ U, OffsetTable uoff,
                                              int main_idx, int n_P, int64_t outer,
-                                             int64_t inner, int64_t n_rhs, V* __restrict__ x_all) {
+                                             int64_t inner, int64_t n_rhs, const V* rhs,
+                                             V* out) {
   extern __shared__ double wsm[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double* xr = wsm + (size_t)wib * 2 * n_P;
@@ -212,94 +217,67 @@ __global__ void wavenumber_solve_warp_kernel(const double* __restrict__ L, Offse
   const int64_t base = (r * outer + o) * (int64_t)n_P * inner + t;
   const double* Lf = L + f * (int64_t)loff.n * n_P;
   const double* Uf = U + f * (int64_t)uoff.n * n_P;
-  V* x = x_all + base;
   constexpr bool kCplx = sizeof(V) != sizeof(double);
   for (int i = lane; i < n_P; i += 32) {
     if constexpr (kCplx) {
-      const V v = x[(int64_t)i * inner];
+      const V v = rhs[base + (int64_t)i * inner];
       xr[i] = v.re;
       xi[i] = v.im;
     } else {
-      xr[i] = x[(int64_t)i * inner];
+      xr[i] = rhs[base + (int64_t)i * inner];
       xi[i] = 0.0;
     }
   }
   __syncwarp();
-  auto reduce = [&](double& a, double& b) {
-#pragma unroll
-    for (int m = 16; m > 0; m >>= 1) {
-      a += __shfl_xor_sync(0xffffffffu, a, m);
-      b += __shfl_xor_sync(0xffffffffu, b, m);
-    }
-  };
-  // factor entry of row i on this lane's first diagonal (0 when out of range)
-  auto lval = [&](int i) {
-    if (lane >= loff.n) return 0.0;
-    const int j = i + loff.off[lane];
-    return (j >= 0) ? Lf[(int64_t)lane * n_P + j] : 0.0;
-  };
-  auto uval = [&](int i) {
-    if (lane >= uoff.n || uoff.off[lane] == 0) return 0.0;
-    const int j = i + uoff.off[lane];
-    return (j < n_P) ? Uf[(int64_t)lane * n_P + j] : 0.0;
-  };
-  double lnext = lval(0);
-  for (int i = 0; i < n_P; ++i) {
-    const double lc = lnext;
-    if (i + 1 < n_P) lnext = lval(i + 1);
-    double ar = 0.0, ai = 0.0;
-    if (lane < loff.n) {
-      const int j = i + loff.off[lane];
-      if (j >= 0) {
-        ar = lc * xr[j];
-        ai = lc * xi[j];
-      }
+  // forward: L[i, i + s] (s < 0) sits at column c = i + s, Lf[d * n_P + c]
+  const int lrow = (lane < loff.n) ? -loff.off[lane] : n_P;  // row = c + lrow
+  double lnext = (lrow < n_P) ? Lf[(int64_t)lane * n_P] : 0.0;
+  for (int c = 0; c < n_P; ++c) {
+    const double l = lnext;
+    if (c + 1 + lrow < n_P) lnext = Lf[(int64_t)lane * n_P + c + 1];
+    const double yr = xr[c], yi = xi[c];
+    if (c + lrow < n_P) {
+      xr[c + lrow] -= l * yr;
+      xi[c + lrow] -= l * yi;
     }
     for (int d = lane + 32; d < loff.n; d += 32) {
-      const int j = i + loff.off[d];
-      if (j < 0) continue;
-      const double l = Lf[(int64_t)d * n_P + j];
-      ar += l * xr[j];
-      ai += l * xi[j];
-    }
-    reduce(ar, ai);
-    if (lane == 0) {
-      xr[i] -= ar;
-      xi[i] -= ai;
+      const int i = c - loff.off[d];
+      if (i >= n_P) continue;
+      const double ld = Lf[(int64_t)d * n_P + c];
+      xr[i] -= ld * yr;
+      xi[i] -= ld * yi;
     }
     __syncwarp();
   }
-  double unext = uval(n_P - 1);
-  for (int i = n_P - 1; i >= 0; --i) {
-    const double uc = unext;
-    if (i > 0) unext = uval(i - 1);
-    double ar = 0.0, ai = 0.0;
-    if (lane < uoff.n && uoff.off[lane] != 0) {
-      const int j = i + uoff.off[lane];
-      if (j < n_P) {
-        ar = uc * xr[j];
-        ai = uc * xi[j];
-      }
+  // backward: U[i, i + s] (s > 0) sits at column c = i + s, Uf[d * n_P + c]
+  const int urow = (lane < uoff.n && uoff.off[lane] != 0) ? uoff.off[lane] : -1;  // row = c - urow
+  const double* Ud = Uf + (int64_t)main_idx * n_P;
+  double unext = (urow > 0 && n_P - 1 - urow >= 0) ? Uf[(int64_t)lane * n_P + n_P - 1] : 0.0;
+  double dnext = Ud[n_P - 1];
+  for (int c = n_P - 1; c >= 0; --c) {
+    const double u = unext, dg = dnext;
+    if (c > 0) {
+      dnext = Ud[c - 1];
+      if (urow > 0 && c - 1 - urow >= 0) unext = Uf[(int64_t)lane * n_P + c - 1];
+    }
+    const double x_r = xr[c] / dg, x_i = xi[c] / dg;
+    if (lane == (c & 31)) {
+      if constexpr (kCplx) out[base + (int64_t)c * inner] = cmk(x_r, x_i);
+      else out[base + (int64_t)c * inner] = x_r;
+    }
+    if (urow > 0 && c - urow >= 0) {
+      xr[c - urow] -= u * x_r;
+      xi[c - urow] -= u * x_i;
     }
     for (int d = lane + 32; d < uoff.n; d += 32) {
       const int sft = uoff.off[d];
-      const int j = i + sft;
-      if (sft == 0 || j >= n_P) continue;
-      const double u = Uf[(int64_t)d * n_P + j];
-      ar += u * xr[j];
-      ai += u * xi[j];
-    }
-    reduce(ar, ai);
-    if (lane == 0) {
-      const double diag = Uf[(int64_t)main_idx * n_P + i];
-      xr[i] = (xr[i] - ar) / diag;
-      xi[i] = (xi[i] - ai) / diag;
+      const int i = c - sft;
+      if (sft == 0 || i < 0) continue;
+      const double ud = Uf[(int64_t)d * n_P + c];
+      xr[i] -= ud * x_r;
+      xi[i] -= ud * x_i;
     }
     __syncwarp();
-  }
-  for (int i = lane; i < n_P; i += 32) {
-    if constexpr (kCplx) x[(int64_t)i * inner] = cmk(xr[i], xi[i]);
-    else x[(int64_t)i * inner] = xr[i];
   }
 }
 
@@ -394,25 +372,30 @@ extern "C" int jfb_wavenumber_solve(const double* L, const int64_t* L_offsets, i
   for (int d = 0; d < lt.n; ++d) JFB_REQUIRE(lt.off[d] < 0, "L offsets must be < 0");
   JFB_REQUIRE(main_idx >= 0, "U offsets must contain the main diagonal");
   cudaStream_t s = (cudaStream_t)stream;
-  if (rhs != out) {
-    const int64_t elems = n_rhs * outer * n_P * inner * (is_complex ? 2 : 1);
-    JFB_CHECK_CUDA(cudaMemcpyAsync(out, rhs, elems * sizeof(double),
-                                   cudaMemcpyDeviceToDevice, s));
-  }
   const int64_t total = n_rhs * outer * inner;
   const int threads = 128;
-  if (lt.n + ut.n > 8) {  // wide factors: a warp per system
+  if (lt.n + ut.n > 8) {  // wide factors: a warp per system, rhs read in place
+    // the column updates of one step write one row per diagonal
+    for (int a = 0; a < ut.n; ++a)
+      for (int b = a + 1; b < ut.n; ++b) JFB_REQUIRE(ut.off[a] != ut.off[b], "repeated U offset");
+    for (int a = 0; a < lt.n; ++a)
+      for (int b = a + 1; b < lt.n; ++b) JFB_REQUIRE(lt.off[a] != lt.off[b], "repeated L offset");
     const int64_t wblocks = (total * 32 + threads - 1) / threads;
     const size_t sm = (size_t)(threads / 32) * 2 * n_P * sizeof(double);
     JFB_REQUIRE(sm <= 48 * 1024, "n_P too large for the warp solve (max 768)");
     if (is_complex)
       wavenumber_solve_warp_kernel<c64><<<(unsigned)wblocks, threads, sm, s>>>(
-          L, lt, U, ut, main_idx, (int)n_P, outer, inner, n_rhs, (c64*)out);
+          L, lt, U, ut, main_idx, (int)n_P, outer, inner, n_rhs, (const c64*)rhs, (c64*)out);
     else
       wavenumber_solve_warp_kernel<double><<<(unsigned)wblocks, threads, sm, s>>>(
-          L, lt, U, ut, main_idx, (int)n_P, outer, inner, n_rhs, out);
+          L, lt, U, ut, main_idx, (int)n_P, outer, inner, n_rhs, rhs, out);
     JFB_CHECK_LAUNCH();
     return JFB_OK;
+  }
+  if (rhs != out) {
+    const int64_t elems = n_rhs * outer * n_P * inner * (is_complex ? 2 : 1);
+    JFB_CHECK_CUDA(cudaMemcpyAsync(out, rhs, elems * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, s));
   }
   const int blocks = (int)((total + threads - 1) / threads);
   if (is_complex) {

@@ -51,6 +51,24 @@ def test_dia_solve_matches_oracle_lu(cuda):
     np.testing.assert_allclose(x, ref, rtol=0, atol=1e-13 * np.abs(ref).max())
 
 
+@pytest.mark.parametrize("cplx", [False, True])
+def test_wide_factor_solve_matches_dense(cuda, cplx):
+    """More than 32 diagonals on each side of the diagonal: the warp-per-system
+    solve with its second pass over the diagonals (real and complex, several
+    right-hand sides)."""
+    rng = np.random.default_rng(3)
+    n = 90
+    offsets = tuple(range(-40, 0, 1)) + tuple(range(0, 70, 2))
+    a = dense_dia(n, n, offsets, rng) * 0.05 + 4 * np.eye(n)
+    A = DiaMatrix.from_dense(torch.from_numpy(a).to(cuda), offsets)
+    b = rng.standard_normal((n, 5))
+    if cplx:
+        b = b + 1j * rng.standard_normal((n, 5))
+    x = A.solve(torch.from_numpy(b).to(cuda), 0).cpu().numpy()
+    ref = np.linalg.solve(a, b)
+    np.testing.assert_allclose(x, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+
+
 def test_singular_pivot_is_reported(cuda):
     a = np.eye(6)
     a[3, 3] = 0.0
