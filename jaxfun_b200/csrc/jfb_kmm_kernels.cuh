@@ -24,6 +24,8 @@ namespace jfb {
 constexpr int kNW = 8;         // pencils (warps) per pencil_stage block
 constexpr int kLDW = kNW + 1;  // padded pencil stride in shared memory
 constexpr int kMaxNR = 2;      // rows per lane in the register solves (n <= 128)
+constexpr int kSolveChunk = 16;  // back-substitution columns per prefetch
+constexpr int kLoadBatch = 4;    // staged loads per thread in flight
 
 struct DevOps {
   const double* Q;   // [n][j] scalar-product quadrature (Nx x Nx)
@@ -214,8 +216,11 @@ __device__ __forceinline__ void bmass_solve_lane(const DevOps& o, const Dims& d,
 // lane of column c scales by the reciprocal pivot, broadcasts x_c, and every
 // lane r < c subtracts U[r, c] x_c.  All factor entries a lane needs are
 // loaded before the dependent chains start (no memory latency on the chain).
+// Not inlined: the solve is long straight-line code (fully unrolled columns)
+// and its call sites (Su, Sg, S00, two parities each) share one copy in the
+// instruction cache.
 template <int NR>
-__device__ __forceinline__ void parity_solve_regs(const double* __restrict__ rec, int n,
+__device__ __noinline__ void parity_solve_regs(const double* __restrict__ rec, int n,
                                                   c64* y, int par, int lane) {
   const int m0 = (n + 1) / 2;
   const int m = par ? n / 2 : m0;
@@ -246,33 +251,36 @@ __device__ __forceinline__ void parity_solve_regs(const double* __restrict__ rec
       ym1 = t;
     }
   }
-  // back substitution, 32 columns per chunk, factor column entries prefetched
-#pragma unroll
-  for (int cs = NR - 1; cs >= 0; --cs) {
-    double u[NR][32];
+  // back substitution, kSolveChunk columns per chunk, the chunk's factor
+  // column entries prefetched
+  for (int ch = (m + kSolveChunk - 1) / kSolveChunk - 1; ch >= 0; --ch) {
+    double u[NR][kSolveChunk];
 #pragma unroll
     for (int s = 0; s < NR; ++s)
 #pragma unroll
-      for (int cc = 0; cc < 32; ++cc) {
-        const int c = cc + 32 * cs;
+      for (int cc = 0; cc < kSolveChunk; ++cc) {
+        const int c = cc + kSolveChunk * ch;
         const int r = lane + 32 * s;
-        u[s][cc] = (s <= cs && c < m && r <= c) ? __ldg(Up + c * (c + 1) / 2 + r) : 0.0;
+        u[s][cc] = (c < m && r <= c) ? __ldg(Up + c * (c + 1) / 2 + r) : 0.0;
       }
 #pragma unroll
-    for (int cc = 31; cc >= 0; --cc) {
-      const int c = cc + 32 * cs;
+    for (int cc = kSolveChunk - 1; cc >= 0; --cc) {
+      const int c = cc + kSolveChunk * ch;
       if (c >= m) continue;
+      const int own = c & 31, os = c >> 5;  // lane and slot of row c
       c64 xc = cmk(0.0, 0.0);
-      if (lane == cc) {
-        xc = u[cs][cc] * yr[cs];  // reciprocal pivot
-        yr[cs] = xc;
-      }
-      xc.re = __shfl_sync(0xffffffffu, xc.re, cc);
-      xc.im = __shfl_sync(0xffffffffu, xc.im, cc);
+#pragma unroll
+      for (int s = 0; s < NR; ++s)
+        if (s == os && lane == own) {
+          xc = u[s][cc] * yr[s];  // reciprocal pivot
+          yr[s] = xc;
+        }
+      xc.re = __shfl_sync(0xffffffffu, xc.re, own);
+      xc.im = __shfl_sync(0xffffffffu, xc.im, own);
 #pragma unroll
       for (int s = 0; s < NR; ++s) {
         const int r = lane + 32 * s;
-        if (s <= cs && r < c) yr[s] = yr[s] - u[s][cc] * xc;
+        if (r < c) yr[s] = yr[s] - u[s][cc] * xc;
       }
     }
   }
@@ -290,6 +298,62 @@ __device__ __forceinline__ void packed_solve_warp(const double* __restrict__ rec
                                                   c64* y, int lane) {
   parity_solve_regs<NR>(rec, n, y, 0, lane);
   parity_solve_regs<NR>(rec, n, y, 1, lane);
+}
+
+// Rows i = lane + 32 t of one pencil (n <= 128: the host limits Nx to 129),
+// all global loads of the warp issued before the arithmetic.
+// out[i] = c0 x[i] + c1 y[i] + c2 z[i]  (the y, z terms only when c1, c2 != 0)
+__device__ __forceinline__ void comb_rows(c64* out, const c64* x, const c64* y, const c64* z,
+                                          double c0, double c1, double c2, int n, size_t P,
+                                          int p, int lane) {
+  c64 vx[4], vy[4], vz[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int i = lane + 32 * t;
+    const size_t gi = (size_t)i * P + p;
+    vx[t] = vy[t] = vz[t] = cmk(0.0, 0.0);
+    if (i < n) {
+      vx[t] = x[gi];
+      if (c1 != 0.0) vy[t] = y[gi];
+      if (c2 != 0.0) vz[t] = z[gi];
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int i = lane + 32 * t;
+    if (i < n) {
+      c64 v = c0 * vx[t];
+      if (c1 != 0.0) v = v + c1 * vy[t];
+      if (c2 != 0.0) v = v + c2 * vz[t];
+      out[i] = v;
+    }
+  }
+}
+// acc[i] = mass[i] + dt (d0 acc[i] + d1 q1[i] + d2 q2[i])  (q terms when d1, d2 != 0)
+__device__ __forceinline__ void rhs_rows(c64* acc, const c64* mass, const c64* q1,
+                                         const c64* q2, double d0, double d1, double d2,
+                                         double dt, int n, size_t P, int p, int lane) {
+  c64 v1[4], v2[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int i = lane + 32 * t;
+    const size_t gi = (size_t)i * P + p;
+    v1[t] = v2[t] = cmk(0.0, 0.0);
+    if (i < n) {
+      if (d1 != 0.0) v1[t] = q1[gi];
+      if (d2 != 0.0) v2[t] = q2[gi];
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int i = lane + 32 * t;
+    if (i < n) {
+      c64 nl = d0 * acc[i];
+      if (d1 != 0.0) nl = nl + d1 * v1[t];
+      if (d2 != 0.0) nl = nl + d2 * v2[t];
+      acc[i] = mass[i] + dt * nl;
+    }
+  }
 }
 
 // Velocity reconstruction (channelflow_kmm.py:855-870): from u0 (TB, in A3)
@@ -457,6 +521,15 @@ __device__ __forceinline__ void cta_forward_parity(const double* __restrict__ QE
   }
 }
 
+constexpr int kDmmaChunk = 8;  // k steps whose operands are loaded together
+constexpr int kDmmaGroup = 6;  // column tiles sharing one operator fragment load
+// doubles per B-operand row of the x-backward: 6 fields x kNW pencils x re/im,
+// + 4 so that the four rows of a fragment fall in distinct bank halves
+constexpr int kLDB = 2 * 6 * kNW + 4;
+// doubles per B-operand row of the x-forward (3 fields): consecutive rows
+// fall in opposite bank halves
+constexpr int kLDF = 2 * 3 * kNW + 8;
+
 // FP64 tensor-core product D = A B + C for one 8x8x4 tile (mma.sync m8n8k4
 // f64).  Fragments: a = A[lane / 4][lane % 4], b = B[lane % 4][lane / 4],
 // c/d = C[lane / 4][2 (lane % 4) + {0, 1}].
@@ -471,91 +544,130 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 // are (pencil w, field f, re/im) with re/im the lowest bit, so each lane's
 // accumulator pair is one complex output value.  E (even coefficients) and O
 // (odd) tiles share an output tile; u(x_j) = E + O, u(x_{N-1-j}) = E - O.
-// coef(w, f, n) returns the orthogonal coefficient n of field f of pencil w.
-template <typename CoefFn>
+// The B operand sits in shared memory as rows Bs[n * kLDB + c], n the
+// orthogonal coefficient, c = (w NF + f) 2 + re/im, so the fragment of a
+// k step is one 8-byte load per lane from four rows (two wavefronts).
+// Output: out[(f N + j) ldo + w].  A warp's unit of work is one 8-row tile of
+// the operator against up to kDmmaGroup column tiles: each operator fragment
+// (read from L2, shared by all CTAs) is loaded once per unit.
 __device__ __forceinline__ void cta_backward_dmma(const double* __restrict__ VE,
                                                   const double* __restrict__ VO, int N,
-                                                  int NF, CoefFn coef, c64* out) {
+                                                  int NF, const double* Bs, c64* out,
+                                                  int ldo) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   const int Jh = (N + 1) / 2, Ne = (N + 1) / 2, No = N / 2;
   const int mt = (Jh + 7) / 8, nt = (NF * kNW * 2) / 8;
+  const int ng = (nt + kDmmaGroup - 1) / kDmmaGroup;
   const int g = lane >> 2, t4 = lane & 3;
-  for (int tile = warp; tile < mt * nt; tile += nwarps) {
-    const int m0 = (tile / nt) * 8, n0 = (tile % nt) * 8;
-    // B column owned by this lane for the b fragment: n0 + g
-    const int colb = n0 + g;
-    const int wb = colb / (2 * NF), fb = (colb / 2) % NF, rib = colb & 1;
+  for (int unit = warp; unit < mt * ng; unit += nwarps) {
+    const int m0 = (unit / ng) * 8, nb = (unit % ng) * kDmmaGroup;
+    const int nq = min(kDmmaGroup, nt - nb);
     const int ja = m0 + g;  // A row of the a fragment
-    double e0 = 0.0, e1 = 0.0, o0 = 0.0, o1 = 0.0;
-    for (int k0 = 0; k0 < Ne; k0 += 4) {
-      const int k = k0 + t4;
-      const double a = (ja < Jh && k < Ne) ? __ldg(VE + (size_t)ja * Ne + k) : 0.0;
-      double b = 0.0;
-      if (k < Ne) {
-        const c64 v = coef(wb, fb, 2 * k);
-        b = rib ? v.im : v.re;
+    double e0[kDmmaGroup], e1[kDmmaGroup], o0[kDmmaGroup], o1[kDmmaGroup];
+#pragma unroll
+    for (int q = 0; q < kDmmaGroup; ++q) e0[q] = e1[q] = o0[q] = o1[q] = 0.0;
+#pragma unroll
+    for (int par = 0; par < 2; ++par) {
+      const int K = par ? No : Ne;
+      const double* A = par ? VO : VE;
+      for (int kb = 0; kb < K; kb += 4 * kDmmaChunk) {
+        double av[kDmmaChunk];
+#pragma unroll
+        for (int u = 0; u < kDmmaChunk; ++u) {
+          const int k = kb + 4 * u + t4;
+          av[u] = (ja < Jh && k < K) ? __ldg(A + (size_t)ja * K + k) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < kDmmaGroup; ++q) {
+          if (q >= nq) break;
+          const double* brow = Bs + (nb + q) * 8 + g + par * kLDB;  // + 2 k kLDB
+          double bv[kDmmaChunk];
+#pragma unroll
+          for (int u = 0; u < kDmmaChunk; ++u) {
+            const int k = kb + 4 * u + t4;
+            bv[u] = (k < K) ? brow[2 * k * kLDB] : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < kDmmaChunk; ++u)
+            if (kb + 4 * u < K) {
+              if (par) dmma_8x8x4(o0[q], o1[q], av[u], bv[u]);
+              else dmma_8x8x4(e0[q], e1[q], av[u], bv[u]);
+            }
+        }
       }
-      dmma_8x8x4(e0, e1, a, b);
-    }
-    for (int k0 = 0; k0 < No; k0 += 4) {
-      const int k = k0 + t4;
-      const double a = (ja < Jh && k < No) ? __ldg(VO + (size_t)ja * No + k) : 0.0;
-      double b = 0.0;
-      if (k < No) {
-        const c64 v = coef(wb, fb, 2 * k + 1);
-        b = rib ? v.im : v.re;
-      }
-      dmma_8x8x4(o0, o1, a, b);
     }
     const int j = m0 + g;
-    const int colc = n0 + 2 * t4;  // even column: re, next: im
-    const int wc = colc / (2 * NF), fc = (colc / 2) % NF;
-    if (j < Jh) {
-      out[(fc * N + j) * kLDW + wc] = cmk(e0 + o0, e1 + o1);
-      if (N - 1 - j != j) out[(fc * N + N - 1 - j) * kLDW + wc] = cmk(e0 - o0, e1 - o1);
+#pragma unroll
+    for (int q = 0; q < kDmmaGroup; ++q) {
+      if (q >= nq) break;
+      const int colc = (nb + q) * 8 + 2 * t4;  // even column: re, next: im
+      const int wc = colc / (2 * NF), fc = (colc / 2) % NF;
+      if (j < Jh) {
+        out[(fc * N + j) * ldo + wc] = cmk(e0[q] + o0[q], e1[q] + o1[q]);
+        if (N - 1 - j != j) out[(fc * N + N - 1 - j) * ldo + wc] = cmk(e0[q] - o0[q], e1[q] - o1[q]);
+      }
     }
   }
 }
 
 // Parity-split x-forward scalar products on the FP64 tensor cores:
 // sp[2m] = sum_j QE[m][j] (u_j + u_{N-1-j}), sp[2m+1] = sum_j QO[m][j] (u_j -
-// u_{N-1-j}); phys(f, j, w) returns the sample of field f of pencil w at x_j.
-template <typename PhysFn>
+// u_{N-1-j}).  The mirror sums (Se, ceil(N/2) rows) and differences (So,
+// floor(N/2) rows) sit in shared memory as rows of kLDF doubles, column
+// c = (w NF + f) 2 + re/im.  Output: out[(f N + n) kLDW + w].  Units of
+// work as in cta_backward_dmma.
 __device__ __forceinline__ void cta_forward_dmma(const double* __restrict__ QE,
                                                  const double* __restrict__ QO, int N, int NF,
-                                                 PhysFn phys, c64* out) {
+                                                 const double* Se, const double* So, c64* out) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   const int Jh = (N + 1) / 2, Jl = N / 2, Ne = (N + 1) / 2, No = N / 2;
   const int mte = (Ne + 7) / 8, mto = (No + 7) / 8, nt = (NF * kNW * 2) / 8;
+  const int ng = (nt + kDmmaGroup - 1) / kDmmaGroup;
   const int g = lane >> 2, t4 = lane & 3;
-  for (int tile = warp; tile < (mte + mto) * nt; tile += nwarps) {
-    const int mi = tile / nt;
+  for (int unit = warp; unit < (mte + mto) * ng; unit += nwarps) {
+    const int mi = unit / ng, nb = (unit % ng) * kDmmaGroup;
+    const int nq = min(kDmmaGroup, nt - nb);
     const bool odd = mi >= mte;
-    const int m0 = (odd ? mi - mte : mi) * 8, n0 = (tile % nt) * 8;
+    const int m0 = (odd ? mi - mte : mi) * 8;
     const int M = odd ? No : Ne, K = odd ? Jl : Jh;
     const double* A = odd ? QO : QE;
-    const int colb = n0 + g;
-    const int wb = colb / (2 * NF), fb = (colb / 2) % NF, rib = colb & 1;
+    const double* B = odd ? So : Se;
     const int ma = m0 + g;
-    double d0 = 0.0, d1 = 0.0;
-    for (int k0 = 0; k0 < K; k0 += 4) {
-      const int k = k0 + t4;
-      const double a = (ma < M && k < K) ? __ldg(A + (size_t)ma * K + k) : 0.0;
-      double b = 0.0;
-      if (k < K) {
-        const c64 u = phys(fb, k, wb);
-        const c64 v = (N - 1 - k != k) ? phys(fb, N - 1 - k, wb) : cmk(0.0, 0.0);
-        const c64 c = odd ? u - v : u + v;
-        b = rib ? c.im : c.re;
+    double d0[kDmmaGroup], d1[kDmmaGroup];
+#pragma unroll
+    for (int q = 0; q < kDmmaGroup; ++q) d0[q] = d1[q] = 0.0;
+    for (int kb = 0; kb < K; kb += 4 * kDmmaChunk) {
+      double av[kDmmaChunk];
+#pragma unroll
+      for (int u = 0; u < kDmmaChunk; ++u) {
+        const int k = kb + 4 * u + t4;
+        av[u] = (ma < M && k < K) ? __ldg(A + (size_t)ma * K + k) : 0.0;
       }
-      dmma_8x8x4(d0, d1, a, b);
+#pragma unroll
+      for (int q = 0; q < kDmmaGroup; ++q) {
+        if (q >= nq) break;
+        const double* brow = B + (nb + q) * 8 + g;
+        double bv[kDmmaChunk];
+#pragma unroll
+        for (int u = 0; u < kDmmaChunk; ++u) {
+          const int k = kb + 4 * u + t4;
+          bv[u] = (k < K) ? brow[k * kLDF] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < kDmmaChunk; ++u)
+          if (kb + 4 * u < K) dmma_8x8x4(d0[q], d1[q], av[u], bv[u]);
+      }
     }
     const int m = m0 + g;
-    const int colc = n0 + 2 * t4;
-    const int wc = colc / (2 * NF), fc = (colc / 2) % NF;
-    if (m < M) {
-      const int n = odd ? 2 * m + 1 : 2 * m;
-      out[(fc * N + n) * kLDW + wc] = cmk(d0, d1);
+#pragma unroll
+    for (int q = 0; q < kDmmaGroup; ++q) {
+      if (q >= nq) break;
+      const int colc = (nb + q) * 8 + 2 * t4;
+      const int wc = colc / (2 * NF), fc = (colc / 2) % NF;
+      if (m < M) {
+        const int n = odd ? 2 * m + 1 : 2 * m;
+        out[(fc * N + n) * kLDW + wc] = cmk(d0[q], d1[q]);
+      }
     }
   }
 }
@@ -564,7 +676,7 @@ __device__ __forceinline__ void cta_forward_dmma(const double* __restrict__ QE,
 // pencil_stage: see file header.  Block = kNW warps, one pencil per warp.
 // ---------------------------------------------------------------------------
 template <int NR>
-__global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, StageArgs a) {
+__global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   c64* R1 = reinterpret_cast<c64*>(smem_raw);  // 6 * Nx * kLDW
   c64* ARR = R1 + 6 * d.Nx * kLDW;              // kNW * 6 * Nx
@@ -617,8 +729,9 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
 
   // ---------------- phase A: nonlinear term of the current state ----------
   if (a.mode != kPrologue) {
-    // cooperative load of the x-physical H fields into R1[0..2]
-    for (int idx = threadIdx.x; idx < 3 * d.Nx * kNW; idx += blockDim.x) {
+    // cooperative load of the x-physical H fields into R1[0..2], kLoadBatch
+    // values per thread in flight
+    auto load_h = [&](int idx) {
       const int w = idx % kNW, fi = idx / kNW;
       c64 v = cmk(0.0, 0.0);
       if (w < nvalid && !nyq) {
@@ -648,13 +761,47 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
           }
         }
       }
-      R1[fi * kLDW + w] = v;
+      return v;
+    };
+    const int nload = 3 * d.Nx * kNW;
+    for (int i0 = threadIdx.x; i0 < nload; i0 += kLoadBatch * blockDim.x) {
+      c64 v[kLoadBatch];
+#pragma unroll
+      for (int u = 0; u < kLoadBatch; ++u) {
+        const int idx = i0 + u * blockDim.x;
+        v[u] = (idx < nload) ? load_h(idx) : cmk(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < kLoadBatch; ++u) {
+        const int idx = i0 + u * blockDim.x;
+        if (idx < nload) R1[(idx / kNW) * kLDW + idx % kNW] = v[u];
+      }
+    }
+    __syncthreads();
+    // mirror sums / differences of the samples as B-operand rows in ARR
+    // (free until the per-pencil work starts)
+    {
+      const int Jh = (d.Nx + 1) / 2, Jl = d.Nx / 2;
+      double* Se = reinterpret_cast<double*>(ARR);
+      double* So = Se + (size_t)Jh * kLDF;
+      for (int idx = threadIdx.x; idx < Jh * 3 * kNW; idx += blockDim.x) {
+        const int wf = idx % (3 * kNW), k = idx / (3 * kNW);
+        const int w = wf / 3, f = wf % 3;
+        const c64 x = R1[(f * d.Nx + k) * kLDW + w];
+        const c64 y = (d.Nx - 1 - k != k) ? R1[(f * d.Nx + d.Nx - 1 - k) * kLDW + w] : cmk(0.0, 0.0);
+        const c64 sm = x + y;
+        *reinterpret_cast<double2*>(Se + (size_t)k * kLDF + 2 * wf) = make_double2(sm.re, sm.im);
+        if (k < Jl) {
+          const c64 df = x - y;
+          *reinterpret_cast<double2*>(So + (size_t)k * kLDF + 2 * wf) = make_double2(df.re, df.im);
+        }
+      }
     }
     __syncthreads();
     // scalar products (T_n, H_f)_w for the 3 fields -> R1[3..5]
     c64* sT = R1 + 3 * d.Nx * kLDW;
-    cta_forward_dmma(o.QE, o.QO, d.Nx, 3,
-                     [&](int f, int j, int w) { return R1[(f * d.Nx + j) * kLDW + w]; }, sT);
+    cta_forward_dmma(o.QE, o.QO, d.Nx, 3, reinterpret_cast<const double*>(ARR),
+                     reinterpret_cast<const double*>(ARR) + (size_t)((d.Nx + 1) / 2) * kLDF, sT);
     __syncthreads();
     if (a.mode == kFromPhys) {
       // TB.forward(u0), TD.forward(u1), TD.forward(u2), mask, g = i ky u2 - i kz u1
@@ -759,13 +906,7 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
         for (int i = lane; i < d.nD; i += 32) a.Ng_out[(size_t)i * P + p] = A4[i];
 
       // ---- right-hand side of Su: Mu (c0 ua + c1 ub + c2 uc) + cL Lu ua + dt N ----
-      for (int i = lane; i < d.nB; i += 32) {
-        const size_t gi = (size_t)i * P + p;
-        c64 v = a.c0 * a.u0a[gi];
-        if (a.c1 != 0.0) v = v + a.c1 * a.u0b[gi];
-        if (a.c2 != 0.0) v = v + a.c2 * a.u0c[gi];
-        A0[i] = v;
-      }
+      comb_rows(A0, a.u0a, a.u0b, a.u0c, a.c0, a.c1, a.c2, d.nB, P, p, lane);
       __syncwarp();
       apply_SBT(o, d, A0, A2, lane);            // A2 = S_B^T comb
       chebder_warp(A2, A5, d.Nx, d.dfx, lane);   // A5 = D comb
@@ -789,23 +930,11 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
         __syncwarp();
       }
       apply_SB_ns(o, d, A2, A0, d.Myz, lane);  // A0 = mass rows (nB)
-      for (int i = lane; i < d.nB; i += 32) {
-        const size_t gi = (size_t)i * P + p;
-        c64 nl = a.d0 * A3[i];
-        if (a.d1 != 0.0) nl = nl + a.d1 * a.Nup[gi];
-        if (a.d2 != 0.0) nl = nl + a.d2 * a.Nuq[gi];
-        A3[i] = A0[i] + d.dt * nl;  // rhs_u
-      }
+      rhs_rows(A3, A0, a.Nup, a.Nuq, a.d0, a.d1, a.d2, d.dt, d.nB, P, p, lane);  // rhs_u
       __syncwarp();
 
       // ---- right-hand side of Sg: Mg comb_g + cL Lg ga + dt N ----
-      for (int i = lane; i < d.nD; i += 32) {
-        const size_t gi = (size_t)i * P + p;
-        c64 v = a.c0 * a.ga[gi];
-        if (a.c1 != 0.0) v = v + a.c1 * a.gb[gi];
-        if (a.c2 != 0.0) v = v + a.c2 * a.gc[gi];
-        A0[i] = v;
-      }
+      comb_rows(A0, a.ga, a.gb, a.gc, a.c0, a.c1, a.c2, d.nD, P, p, lane);
       __syncwarp();
       apply_SDT(d, A0, A2, lane);  // A2 = S_D^T comb
       if (a.cL != 0.0) {
@@ -819,13 +948,7 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
         __syncwarp();
       }
       apply_SD_ns(o, d, A2, A0, d.Myz, lane);
-      for (int i = lane; i < d.nD; i += 32) {
-        const size_t gi = (size_t)i * P + p;
-        c64 nl = a.d0 * A4[i];
-        if (a.d1 != 0.0) nl = nl + a.d1 * a.Ngp[gi];
-        if (a.d2 != 0.0) nl = nl + a.d2 * a.Ngq[gi];
-        A4[i] = A0[i] + d.dt * nl;  // rhs_g
-      }
+      rhs_rows(A4, A0, a.Ngp, a.Ngq, a.d0, a.d1, a.d2, d.dt, d.nD, P, p, lane);  // rhs_g
       __syncwarp();
 
       // ---- mean flow (ky = kz = 0): M00 comb + cL L00 + dt N  -> sVW ----
@@ -902,21 +1025,25 @@ __global__ void __launch_bounds__(256) pencil_stage_kernel(DevOps o, Dims d, Sta
     __syncwarp();
   }
   __syncthreads();
-  // x-backward of the six fields: field order (u0, u1, u2, w0, w1, w2)
-  // lives in arrays (A5, A2, A3, A1, A4, A0).
-  cta_backward_dmma(o.VE, o.VO, d.Nx, 6,
-                    [&](int w, int f, int n) {
-                      const int arr = (f == 0) ? 5 : (f == 1) ? 2 : (f == 2) ? 3
-                                      : (f == 3) ? 1 : (f == 4) ? 4 : 0;
-                      return ARR[(w * 6 + arr) * d.Nx + n];
-                    },
-                    R1);
+  // x-backward of the six fields: field order (u0, u1, u2, w0, w1, w2) lives
+  // in arrays (A5, A2, A3, A1, A4, A0).  Their B-operand rows go into R1 (dead
+  // by now), the product into ARR (dead once the rows are built).
+  double* Bs = reinterpret_cast<double*>(R1);
+  for (int idx = threadIdx.x; idx < d.Nx * 6 * kNW; idx += blockDim.x) {
+    const int n = idx % d.Nx, wf = idx / d.Nx;
+    const int w = wf / 6, f = wf % 6;
+    const int arr = (f == 0) ? 5 : (f == 1) ? 2 : (f == 2) ? 3 : (f == 3) ? 1 : (f == 4) ? 4 : 0;
+    const c64 v = ARR[(w * 6 + arr) * d.Nx + n];
+    *reinterpret_cast<double2*>(Bs + (size_t)n * kLDB + 2 * wf) = make_double2(v.re, v.im);
+  }
+  __syncthreads();
+  cta_backward_dmma(o.VE, o.VO, d.Nx, 6, Bs, ARR, kNW);
   __syncthreads();
   for (int idx = threadIdx.x; idx < 6 * d.Nx * kNW; idx += blockDim.x) {
     const int w = idx % kNW, fi = idx / kNW;
     if (w < nvalid) {
       const size_t e = (size_t)fi * P + p0 + w;
-      const c64 v = R1[fi * kLDW + w];
+      const c64 v = ARR[fi * kNW + w];
       if (a.x32) reinterpret_cast<c32*>(a.X)[e] = cmk((float)v.re, (float)v.im);
       else a.X[e] = v;
     }

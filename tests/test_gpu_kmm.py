@@ -238,3 +238,22 @@ def test_mixed_form_against_oracle(cuda, N):
     st, gs = o.solve(o.initial_state(), 6), g.solve(g.initial_state(), 6)
     for a, b in zip((*gs.u, gs.g), (*st.u, st.g), strict=True):
         assert rel(a, b) < 1e-7
+
+
+@pytest.mark.parametrize("N, precision", [((97, 16, 16), "fp64"), ((129, 12, 12), "fp64"),
+                                          ((97, 16, 16), "mixed")])
+def test_wide_wall_normal_grids_match_oracle(cuda, N, precision):
+    """Nx above the tensor-core tiling (97, 129): the warp-per-pencil stage
+    with two register rows per lane in its solves, against the oracle.  The
+    mixed form is held to its complex64 transform round-off."""
+    o = PlaneCouetteOracle(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02)
+    g = PlaneCouetteFluctuation(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02,
+                                precision=precision, device=cuda)
+    st = o.initial_state()
+    gs = g._ensure_history(to_dev(st, cuda))
+    for _ in range(4):
+        st = o.step(st)
+    gs = g.solve(gs, 4)
+    tol = 1e-12 if precision == "fp64" else 1e-6
+    for a, b in zip((*gs.u, gs.g), (*st.u, st.g), strict=True):
+        assert rel(a, b) < tol
