@@ -1250,11 +1250,12 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   pl->n_modes = (d.Ny / 2) * d.Kz;
   pl->su_rec = packed_rec_size(d.nB);
   pl->sg_rec = packed_rec_size(d.nD);
-  st = build_factor_set(pl, kSBDF3Implicit * cfg->dt, pl->steady, cfg->nu, 0, 2, pl->gemm);
+  // records with the explicit inverses of the upper factors (both pencil kernels)
+  st = build_factor_set(pl, kSBDF3Implicit * cfg->dt, pl->steady, cfg->nu, 0, 2, true);
   if (st) return fail(st);
   for (int rk = 0; rk < 3; ++rk) {
     st = build_factor_set(pl, (kRK3A[rk] + kRK3B[rk]) * cfg->dt / 2.0, pl->startup[rk],
-                          cfg->nu, 0, 2, pl->gemm);
+                          cfg->nu, 0, 2, true);
     if (st) return fail(st);
   }
   if (pl->mhd) {

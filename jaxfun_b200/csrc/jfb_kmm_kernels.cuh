@@ -212,19 +212,18 @@ __device__ __forceinline__ void bmass_solve_lane(const DevOps& o, const Dims& d,
 // Solve one parity class of a packed record in registers.  Lane r holds
 // row 2r + par (and 2(r+32) + par when m > 32).  Forward elimination with
 // the unit-lower factor (L[i, i-2], L[i, i-4]) passes the solved rows down
-// the lanes with shuffles; back substitution is column-oriented: the owner
-// lane of column c scales by the reciprocal pivot, broadcasts x_c, and every
-// lane r < c subtracts U[r, c] x_c.  All factor entries a lane needs are
-// loaded before the dependent chains start (no memory latency on the chain).
-// Not inlined: the solve is long straight-line code (fully unrolled columns)
-// and its call sites (Su, Sg, S00, two parities each) share one copy in the
-// instruction cache.
+// the lanes with shuffles; then x = U^-1 y with the record's explicit inverse
+// of the parity's upper factor (column-major packed, entry (r, c), r <= c, at
+// c (c + 1) / 2 + r): y_c is broadcast and every lane r <= c accumulates
+// U^-1[r, c] y_c, kSolveChunk columns of the inverse loaded at a time.  Not
+// inlined: the call sites (Su, Sg, S00, two parities each) share one copy in
+// the instruction cache.
 template <int NR>
-__device__ __noinline__ void parity_solve_regs(const double* __restrict__ rec, int n,
-                                                  c64* y, int par, int lane) {
+__device__ __noinline__ void parity_solve_regs(const double* __restrict__ rec, int n, c64* y,
+                                               int par, int lane) {
   const int m0 = (n + 1) / 2;
   const int m = par ? n / 2 : m0;
-  const double* __restrict__ Up = rec + 2 * n + (par ? m0 * (m0 + 1) / 2 : 0);
+  const double* __restrict__ Ui = rec + 2 * n + (par ? m0 * (m0 + 1) / 2 : 0);
   c64 yr[NR];
   double l1[NR], l2[NR];
 #pragma unroll
@@ -251,9 +250,11 @@ __device__ __noinline__ void parity_solve_regs(const double* __restrict__ rec, i
       ym1 = t;
     }
   }
-  // back substitution, kSolveChunk columns per chunk, the chunk's factor
-  // column entries prefetched
-  for (int ch = (m + kSolveChunk - 1) / kSolveChunk - 1; ch >= 0; --ch) {
+  // x = U^-1 y
+  c64 acc[NR];
+#pragma unroll
+  for (int s = 0; s < NR; ++s) acc[s] = cmk(0.0, 0.0);
+  for (int ch = 0; ch * kSolveChunk < m; ++ch) {
     double u[NR][kSolveChunk];
 #pragma unroll
     for (int s = 0; s < NR; ++s)
@@ -261,33 +262,28 @@ __device__ __noinline__ void parity_solve_regs(const double* __restrict__ rec, i
       for (int cc = 0; cc < kSolveChunk; ++cc) {
         const int c = cc + kSolveChunk * ch;
         const int r = lane + 32 * s;
-        u[s][cc] = (c < m && r <= c) ? __ldg(Up + c * (c + 1) / 2 + r) : 0.0;
+        u[s][cc] = (c < m && r <= c) ? __ldg(Ui + c * (c + 1) / 2 + r) : 0.0;
       }
 #pragma unroll
-    for (int cc = kSolveChunk - 1; cc >= 0; --cc) {
+    for (int cc = 0; cc < kSolveChunk; ++cc) {
       const int c = cc + kSolveChunk * ch;
-      if (c >= m) continue;
+      if (c >= m) break;
       const int own = c & 31, os = c >> 5;  // lane and slot of row c
-      c64 xc = cmk(0.0, 0.0);
+      c64 v = yr[0];
 #pragma unroll
-      for (int s = 0; s < NR; ++s)
-        if (s == os && lane == own) {
-          xc = u[s][cc] * yr[s];  // reciprocal pivot
-          yr[s] = xc;
-        }
-      xc.re = __shfl_sync(0xffffffffu, xc.re, own);
-      xc.im = __shfl_sync(0xffffffffu, xc.im, own);
+      for (int s = 1; s < NR; ++s)
+        if (s == os) v = yr[s];
+      c64 yc;
+      yc.re = __shfl_sync(0xffffffffu, v.re, own);
+      yc.im = __shfl_sync(0xffffffffu, v.im, own);
 #pragma unroll
-      for (int s = 0; s < NR; ++s) {
-        const int r = lane + 32 * s;
-        if (r < c) yr[s] = yr[s] - u[s][cc] * xc;
-      }
+      for (int s = 0; s < NR; ++s) acc[s] = acc[s] + u[s][cc] * yc;
     }
   }
 #pragma unroll
   for (int s = 0; s < NR; ++s) {
     const int r = lane + 32 * s;
-    if (r < m) y[2 * r + par] = yr[s];
+    if (r < m) y[2 * r + par] = acc[s];
   }
   __syncwarp();
 }
