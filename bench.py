@@ -133,15 +133,16 @@ def measured_peak():
         return HBM_FALLBACK_GBS, "fallback"
 
 
-def dram_traffic(kernel, precision):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summaries."""
+def dram_traffic(kernel, precision, grid):
+    """Per-launch DRAM bytes of `kernel` on `grid` from the committed ncu
+    summaries (null when that kernel and grid were not captured)."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
             t = json.load(f)
     except (OSError, ValueError):
         return None
-    return t.get(f"{kernel}/{precision}", t.get(kernel) if precision == "fp64" else None)
+    return t.get("x".join(str(n) for n in grid), {}).get(f"{kernel}/{precision}")
 
 
 class ClockSampler:
@@ -435,7 +436,7 @@ def main(argv=None):
             "roofline": {
                 "bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
-                "traffic": dram_traffic(dom, precision),
+                "traffic": dram_traffic(dom, precision, grid),
                 "algorithmic_bytes_per_launch": sb[dom], "launch_ms": dom_ms,
             },
             "step_roofline": {
@@ -689,8 +690,19 @@ def main(argv=None):
                 e1_.record(stream)
                 torch.cuda.synchronize(dev)
                 ms = e0_.elapsed_time(e1_) / K
+                # per-kernel split (events around each launch, L2 not flushed)
+                kms = (ctypes.c_double * 4)()
+                sms = ctypes.c_double()
+                _lib.call("jfb_kmm_timed_steps", sv._plan, K, None, 0, kms, ctypes.byref(sms),
+                          ctypes.c_void_p(stream.cuda_stream))
+                torch.cuda.synchronize(dev)
+                sv._current = None
+                lps = sv.info().launches_per_step
+                names = (("pencil_stage", "plane_transforms") if lps == 2 else
+                         ("pencil_stage", "y_backward", "z_cross", "y_forward"))
                 rec[prec] = {"ms_per_step": ms, "steps_per_s": 1000.0 / ms,
-                             "launches_per_step": sv.info().launches_per_step}
+                             "launches_per_step": lps,
+                             "kernel_us": {k: kms[i] * 1000.0 / K for i, k in enumerate(names)}}
                 states[prec] = (sv, sv.state_from_physical(fields_n))
             (g64, a), (g32, b) = states["fp64"], states["mixed"]
             done = 0
