@@ -323,6 +323,23 @@ int jfb_tps_forward(jfb_tps* tps, const void* phys, void* coeffs, int padded, in
  * nb x nb on the host (the 1-D mass / stiffness of inner.py, domain-scaled). */
 int jfb_tps_galerkin(const jfb_tps* tps, int order, double* out);
 
+/* The 2-D Helmholtz solve -lap u + alpha u = f of la/solvers.py:22-61 as one
+ * launch: orthogonal-Chebyshev x Fourier coefficients f_hat (N, n1) ->
+ * backward of tc, scalar products of td divided by fourier_mass, the
+ * per-wavenumber banded solve with the no-pivot LU factors (L, U) of
+ * TPMatricesWavenumberSolver (tpmatrix.py:1550-1677; DIA data (n1, n_diag,
+ * N - 2), L offsets < 0, U offsets >= 0 with 0), backward of td -> u (N, n1)
+ * complex128.  tc: 2-D, JFB_BASIS_ORTHOGONAL; td: 2-D, JFB_BASIS_DIRICHLET,
+ * same sizes.  One cluster of 8 CTAs holds the whole problem in distributed
+ * shared memory (per CTA 16 (2 N c + N q + 2 n1 ceil(N/8)) + 8 N (N - 2)
+ * bytes, c = ceil(n1/8), q = c rounded up to 1 mod 4): JFB_ERR_ARG when that
+ * exceeds a CTA's shared memory (use the separate transforms and
+ * jfb_wavenumber_solve then). */
+int jfb_helmholtz2d_solve(const jfb_tps* tc, const jfb_tps* td, const double* L,
+                          const int64_t* L_offsets, int64_t n_L, const double* U,
+                          const int64_t* U_offsets, int64_t n_U, double fourier_mass,
+                          const void* f_hat, void* u, void* stream);
+
 /* ---- ensembles ------------------------------------------------------------ */
 
 /* Independent members (flow or MHD plans, any sizes; no reference counterpart:

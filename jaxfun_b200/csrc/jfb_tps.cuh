@@ -85,6 +85,232 @@ __global__ void tps_scale_kernel(c64* __restrict__ y, double a, size_t n) {
     y[i] = a * y[i];
 }
 
+
+// ---------------------------------------------------------------------------
+// 2-D Helmholtz solve in one launch (la/solvers.py:22-61 with the per-
+// wavenumber solve of tpmatrix.py:1550-1677) on one cluster of kHelmCTAs
+// CTAs that keeps the whole (N x n1) problem in distributed shared memory:
+// CTA c owns the Fourier columns [c KC, (c+1) KC) for the x-direction work
+// (products against the x operators, the per-mode solves) and the x rows
+// [c JR, (c+1) JR) for the y transforms; the stages exchange their slices
+// through DSMEM reads between cluster barriers, instead of about ten
+// launches through global memory.
+// ---------------------------------------------------------------------------
+constexpr int kHelmMaxDiag = 256;
+constexpr int kHelmCTAs = 8;
+constexpr int kHelmThreads = 256;
+constexpr int kHelmChunk = 8;  // solve columns whose factor entries are loaded together
+struct Helm2DArgs {
+  const double* BC;  // orthogonal backward, N x N (row j: T_n(x_j))
+  const double* SD;  // Dirichlet scalar products, nb x N
+  const double* BD;  // Dirichlet backward, N x nb
+  const c64* tw;     // n1-point twiddles
+  FFTPlan plan;
+  const double *L, *U;  // (n1, nL, nb), (n1, nU, nb)
+  int nL, nU, umain;
+  int loff[kHelmMaxDiag], uoff[kHelmMaxDiag];
+  int N, nb, M, KC, JR, QS;
+  double scale;  // Fourier scalar-product weight / fourier_mass / n1
+  const c64* f;
+  c64* u;
+};
+
+__global__ void __cluster_dims__(kHelmCTAs, 1, 1) __launch_bounds__(kHelmThreads, 1)
+    helmholtz2d_kernel(const __grid_constant__ Helm2DArgs h) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int N = h.N, M = h.M, nb = h.nb, KC = h.KC, JR = h.JR, QS = h.QS;
+  const int k0 = rank * KC, kn = min(KC, M - k0);  // owned Fourier columns
+  const int j0 = rank * JR, jn = min(JR, N - j0);  // owned x rows
+  c64* A = reinterpret_cast<c64*>(smem_raw);  // [n][kk]: f slice, then gathered columns
+  c64* B = A + (size_t)N * KC;                // [j][kk]: x-backward slices
+  c64* Q = B + (size_t)N * KC;                // [r][kk] (row stride QS): scalar products -> solutions
+  c64* F0 = Q + (size_t)N * h.QS;             // [k][jj]: y-transform lines
+  c64* F1 = F0 + (size_t)M * JR;
+  double* SdT = reinterpret_cast<double*>(F1 + (size_t)M * JR);  // [j][r]
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i = tid; i < N * KC; i += nt) {
+    const int kk = i % KC, n = i / KC;
+    A[i] = (kk < kn) ? h.f[(size_t)n * M + k0 + kk] : cmk(0.0, 0.0);
+  }
+  for (int i = tid; i < nb * N; i += nt) {
+    const int j = i % N, r = i / N;
+    SdT[j * nb + r] = h.SD[i];
+  }
+  __syncthreads();
+  // x backward (orthogonal) of the owned columns: B[j][kk] = sum_n BC[j][n] f[n][kk]
+  for (int i = tid; i < N * KC; i += nt) {
+    const int kk = i % KC, j = i / KC;
+    const double* a = h.BC + (size_t)j * N;
+    c64 s = cmk(0.0, 0.0);
+    for (int n = 0; n < N; ++n) s = s + __ldg(a + n) * A[n * KC + kk];
+    B[i] = s;
+  }
+  cluster.sync();
+  // y: gather the owned rows across all columns, inverse (unnormalised) then
+  // forward transform
+  for (int i = tid; i < M * JR; i += nt) {
+    const int jj = i % JR, k = i / JR;
+    c64 v = cmk(0.0, 0.0);
+    if (jj < jn) {
+      const c64* src = cluster.map_shared_rank(B, (unsigned)(k / KC));
+      v = src[(j0 + jj) * KC + k % KC];
+    }
+    F0[i] = v;
+  }
+  __syncthreads();
+  c64* P = fft_columns<double>(F0, F1, h.plan, JR, JR, h.tw, +1);
+  P = fft_columns<double>(P, (P == F0) ? F1 : F0, h.plan, JR, JR, h.tw, -1);
+  cluster.sync();
+  // gather the owned columns across all rows (P sits at the same offset in
+  // every CTA), then the Dirichlet scalar products Q[r][kk]
+  for (int i = tid; i < N * KC; i += nt) {
+    const int kk = i % KC, j = i / KC;
+    c64 v = cmk(0.0, 0.0);
+    if (kk < kn) {
+      const c64* src = cluster.map_shared_rank(P, (unsigned)(j / JR));
+      v = src[(k0 + kk) * JR + j % JR];
+    }
+    A[i] = v;
+  }
+  __syncthreads();
+  for (int i = tid; i < nb * KC; i += nt) {
+    const int r = i % nb, kk = i / nb;
+    c64 s = cmk(0.0, 0.0);
+    for (int j = 0; j < N; ++j) s = s + SdT[j * nb + r] * A[j * KC + kk];
+    Q[r * QS + kk] = h.scale * s;
+  }
+  __syncthreads();
+  // per-wavenumber solves, a warp per owned mode, column-oriented
+  // substitution: once x_c is final each lane applies its diagonals' entries
+  // of column c to their rows (distinct rows per diagonal); the entries of
+  // diagonals lane and lane + 32 are loaded one column ahead
+  {
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    for (int kk = warp; kk < kn; kk += nwarps) {
+      const int k = k0 + kk;
+      const double* Lk = h.L + (size_t)k * h.nL * nb;
+      const double* Uk = h.U + (size_t)k * h.nU * nb;
+      c64* x = Q + kk;  // element c at x[c * QS]
+      c64* O = A + kk;  // solution, element c at O[c * KC] (A is free after the scalar products)
+      auto lld = [&](int d, int c) {
+        return (d < h.nL && c < nb) ? __ldg(Lk + (size_t)d * nb + c) : 0.0;
+      };
+      auto uld = [&](int d, int c) {
+        return (d < h.nU && c >= 0) ? __ldg(Uk + (size_t)d * nb + c) : 0.0;
+      };
+      // row shifts of this lane's diagonals (lane, lane + 32), held in
+      // registers: s > 0 below / above the diagonal, 0 when the lane has none
+      const int ls0 = lane < h.nL ? -h.loff[lane] : 0;
+      const int ls1 = lane + 32 < h.nL ? -h.loff[lane + 32] : 0;
+      const int us0 = lane < h.nU ? h.uoff[lane] : 0;
+      const int us1 = lane + 32 < h.nU ? h.uoff[lane + 32] : 0;
+      // factor entries of diagonals lane and lane + 32, kHelmChunk columns at
+      // a time, loaded one chunk ahead (the chunk's work covers the latency)
+      double a0[kHelmChunk], a1[kHelmChunk], b0[kHelmChunk], b1[kHelmChunk];
+#pragma unroll
+      for (int q = 0; q < kHelmChunk; ++q) {
+        a0[q] = lld(lane, q);
+        a1[q] = lld(lane + 32, q);
+      }
+      for (int c0 = 0; c0 < nb; c0 += kHelmChunk) {  // unit lower: L[c - s][c] at Lk[d][c], s < 0
+#pragma unroll
+        for (int q = 0; q < kHelmChunk; ++q) {
+          b0[q] = lld(lane, c0 + kHelmChunk + q);
+          b1[q] = lld(lane + 32, c0 + kHelmChunk + q);
+        }
+#pragma unroll
+        for (int q = 0; q < kHelmChunk; ++q) {
+          const int c = c0 + q;
+          if (c >= nb) break;
+          const c64 y = x[c * QS];
+          if (ls0 > 0 && c + ls0 < nb) x[(c + ls0) * QS] = x[(c + ls0) * QS] - a0[q] * y;
+          if (ls1 > 0 && c + ls1 < nb) x[(c + ls1) * QS] = x[(c + ls1) * QS] - a1[q] * y;
+          for (int d = lane + 64; d < h.nL; d += 32) {
+            const int r = c - h.loff[d];
+            if (r < nb) x[r * QS] = x[r * QS] - __ldg(Lk + (size_t)d * nb + c) * y;
+          }
+          __syncwarp();
+        }
+#pragma unroll
+        for (int q = 0; q < kHelmChunk; ++q) {
+          a0[q] = b0[q];
+          a1[q] = b1[q];
+        }
+      }
+      // reciprocal main-diagonal entries of the current / next chunk (formed
+      // off the dependent chain)
+      double g0[kHelmChunk], g1[kHelmChunk];
+#pragma unroll
+      for (int q = 0; q < kHelmChunk; ++q) {
+        a0[q] = uld(lane, nb - 1 - q);
+        a1[q] = uld(lane + 32, nb - 1 - q);
+        g0[q] = 1.0 / uld(h.umain, nb - 1 - q);
+      }
+      for (int t0 = 0; t0 < nb; t0 += kHelmChunk) {  // upper: U[c - s][c] at Uk[d][c], s > 0
+#pragma unroll
+        for (int q = 0; q < kHelmChunk; ++q) {
+          const int c = nb - 1 - (t0 + kHelmChunk + q);
+          b0[q] = uld(lane, c);
+          b1[q] = uld(lane + 32, c);
+          g1[q] = (c >= 0) ? 1.0 / uld(h.umain, c) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < kHelmChunk; ++q) {
+          const int c = nb - 1 - (t0 + q);
+          if (c < 0) break;
+          const c64 v = x[c * QS];
+          const c64 xc = cmk(v.re * g0[q], v.im * g0[q]);
+          if (lane == 0) O[c * KC] = xc;  // the solution goes to O: x[c] is not written
+          if (us0 > 0 && c - us0 >= 0) x[(c - us0) * QS] = x[(c - us0) * QS] - a0[q] * xc;
+          if (us1 > 0 && c - us1 >= 0) x[(c - us1) * QS] = x[(c - us1) * QS] - a1[q] * xc;
+          for (int d = lane + 64; d < h.nU; d += 32) {
+            const int sft = h.uoff[d], r = c - sft;
+            if (sft > 0 && r >= 0) x[r * QS] = x[r * QS] - __ldg(Uk + (size_t)d * nb + c) * xc;
+          }
+          __syncwarp();
+        }
+#pragma unroll
+        for (int q = 0; q < kHelmChunk; ++q) {
+          a0[q] = b0[q];
+          a1[q] = b1[q];
+          g0[q] = g1[q];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // x backward (Dirichlet) of the owned solutions (in A) into B (its earlier
+  // contents were read by the other CTAs before the last cluster barrier)
+  for (int i = tid; i < N * KC; i += nt) {
+    const int kk = i % KC, j = i / KC;
+    const double* a = h.BD + (size_t)j * nb;
+    c64 s = cmk(0.0, 0.0);
+    for (int r = 0; r < nb; ++r) s = s + __ldg(a + r) * A[r * KC + kk];
+    B[i] = s;
+  }
+  cluster.sync();
+  // y: gather the owned rows, inverse transform, store u[j][l]
+  for (int i = tid; i < M * JR; i += nt) {
+    const int jj = i % JR, k = i / JR;
+    c64 v = cmk(0.0, 0.0);
+    if (jj < jn) {
+      const c64* src = cluster.map_shared_rank(B, (unsigned)(k / KC));
+      v = src[(j0 + jj) * KC + k % KC];
+    }
+    F0[i] = v;
+  }
+  __syncthreads();
+  const c64* R = fft_columns<double>(F0, F1, h.plan, JR, JR, h.tw, +1);
+  for (int i = tid; i < jn * M; i += nt) {
+    const int l = i % M, jj = i / M;
+    h.u[(size_t)(j0 + jj) * M + l] = R[l * JR + jj];
+  }
+  cluster.sync();  // no CTA leaves while another still reads its slices
+}
+
 }  // namespace jfb
 
 struct jfb_tps {
@@ -301,5 +527,83 @@ extern "C" int jfb_tps_get_sizes(const jfb_tps* t, int32_t* out4) {
   out4[1] = t->N;
   out4[2] = t->m1;
   out4[3] = t->m2;
+  return JFB_OK;
+}
+
+extern "C" int jfb_helmholtz2d_solve(const jfb_tps* tc, const jfb_tps* td, const double* L,
+                                     const int64_t* L_offsets, int64_t n_L, const double* U,
+                                     const int64_t* U_offsets, int64_t n_U, double fourier_mass,
+                                     const void* f_hat, void* u, void* stream) {
+  JFB_REQUIRE(tc && td && U && U_offsets && f_hat && u, "null pointer");
+  JFB_REQUIRE(n_L == 0 || (L && L_offsets), "null L factor");
+  JFB_REQUIRE(tc->cfg.ndim == 2 && td->cfg.ndim == 2, "2-D spaces only");
+  JFB_REQUIRE(tc->cfg.basis == JFB_BASIS_ORTHOGONAL && td->cfg.basis == JFB_BASIS_DIRICHLET,
+              "tc must be orthogonal, td Dirichlet");
+  JFB_REQUIRE(tc->N == td->N && tc->n1 == td->n1 && tc->nb == tc->N, "tc, td sizes differ");
+  JFB_REQUIRE(fourier_mass != 0.0, "fourier_mass must be nonzero");
+  JFB_REQUIRE(n_L >= 0 && n_L <= kHelmMaxDiag && n_U >= 1 && n_U <= kHelmMaxDiag,
+              "too many diagonals");
+  const int N = td->N, nb = td->nb, M = td->n1;
+  const int KC = (M + kHelmCTAs - 1) / kHelmCTAs, JR = (N + kHelmCTAs - 1) / kHelmCTAs;
+  // solve vectors: row stride QS = 1 mod 4 complex values, so that the rows
+  // one column step updates (even offsets apart) spread over the banks
+  const int QS = KC + ((5 - KC % 4) % 4);
+  const size_t smem = ((size_t)2 * N * KC + (size_t)N * QS + (size_t)2 * M * JR) * sizeof(c64) +
+                      (size_t)nb * N * sizeof(double);
+  int dev = 0, optin = 0;
+  JFB_CHECK_CUDA(cudaGetDevice(&dev));
+  JFB_CHECK_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (smem > (size_t)optin) {
+    set_error("problem too large for the one-cluster Helmholtz solve");
+    return JFB_ERR_ARG;
+  }
+  Helm2DArgs h;
+  std::memset(&h, 0, sizeof(h));
+  h.nL = (int)n_L;
+  h.nU = (int)n_U;
+  h.umain = -1;
+  for (int d = 0; d < h.nL; ++d) {
+    h.loff[d] = (int)L_offsets[d];
+    JFB_REQUIRE(h.loff[d] < 0, "L offsets must be < 0");
+  }
+  for (int d = 0; d < h.nU; ++d) {
+    h.uoff[d] = (int)U_offsets[d];
+    JFB_REQUIRE(h.uoff[d] >= 0, "U offsets must be >= 0");
+    if (h.uoff[d] == 0) h.umain = d;
+  }
+  JFB_REQUIRE(h.umain >= 0, "U offsets must contain the main diagonal");
+  // the column updates of one step write one row per diagonal
+  for (int a = 0; a < h.nU; ++a)
+    for (int b = a + 1; b < h.nU; ++b) JFB_REQUIRE(h.uoff[a] != h.uoff[b], "repeated U offset");
+  for (int a = 0; a < h.nL; ++a)
+    for (int b = a + 1; b < h.nL; ++b) JFB_REQUIRE(h.loff[a] != h.loff[b], "repeated L offset");
+  h.BC = tc->B;
+  h.SD = td->Sq;
+  h.BD = td->B;
+  h.tw = td->tw1n;
+  h.plan = td->f1n;
+  h.L = L;
+  h.U = U;
+  h.N = N;
+  h.nb = nb;
+  h.M = M;
+  h.KC = KC;
+  h.JR = JR;
+  h.QS = QS;
+  // Fourier scalar-product weight 2 pi / df (Fourier.py:152-167), the
+  // caller's division by the Fourier mass, the 1/n1 of the forward transform
+  const double Ly = td->cfg.l[0];
+  const double df = std::fabs(Ly - 2.0 * M_PI) < 1e-12 ? 1.0 : 2.0 * M_PI / Ly;
+  h.scale = (2.0 * M_PI / df) / fourier_mass / M;
+  h.f = (const c64*)f_hat;
+  h.u = (c64*)u;
+  static bool attr = false;
+  if (!attr) {
+    JFB_CHECK_CUDA(cudaFuncSetAttribute((const void*)helmholtz2d_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    attr = true;
+  }
+  helmholtz2d_kernel<<<kHelmCTAs, kHelmThreads, smem, (cudaStream_t)stream>>>(h);
+  JFB_CHECK_LAUNCH();
   return JFB_OK;
 }

@@ -148,6 +148,19 @@ class Helmholtz2D:
         self.solver = tpmats_wavenumber_factor(A)
         # the Fourier mass 2 pi / df = L of the scalar product is not in A
         self._fourier_mass = domain[1][1] - domain[1][0]
+        # one-launch path (jfb_helmholtz2d_solve) while the problem fits the
+        # shared memory of one CTA cluster; the separate launches otherwise
+        L, U = self.solver.runtime_args()
+        self._L, self._U = L.contiguous(), U.contiguous()
+        self._offs = (_lib.int64_array(self.solver.L_offsets),
+                      _lib.int64_array(self.solver.U_offsets))
+        props = torch.cuda.get_device_properties(self.device)
+        optin = getattr(props, "shared_memory_per_block_optin", 0)
+        n, m, nb = self.TD.N[0], self.TD.N[1], self.TD.num_dofs[0]
+        kc, jr = -(-m // 8), -(-n // 8)  # columns / rows per CTA of the 8-CTA cluster
+        qs = kc + (5 - kc % 4) % 4  # padded row of the solve vectors
+        need = 16 * (2 * n * kc + n * qs + 2 * m * jr) + 8 * n * nb
+        self.fused = need <= optin
 
     def solve_coefficients(self, f_phys: torch.Tensor) -> torch.Tensor:
         """Dirichlet x Fourier coefficients of u from samples of f."""
@@ -156,7 +169,25 @@ class Helmholtz2D:
 
     def __call__(self, f_hat: torch.Tensor) -> torch.Tensor:
         """f given by orthogonal Chebyshev x Fourier coefficients: backward,
-        scalar products, per-mode solves, backward; returns u on the mesh."""
+        scalar products, per-mode solves, backward; returns u on the mesh.
+        One launch (the whole problem in the shared memory of one 8-CTA
+        cluster) when it fits, else the separate transforms and the
+        wavenumber solve."""
+        if not self.fused:
+            return self.separate(f_hat)
+        f = self.TC._check(f_hat, self.TC.num_dofs)
+        u = torch.empty(self.TD.N, dtype=torch.complex128, device=self.device)
+        lo, uo = self._offs
+        _lib.call("jfb_helmholtz2d_solve", self.TC._h, self.TD._h,
+                  self._L.data_ptr() if self._L.numel() else None, lo,
+                  len(self.solver.L_offsets), self._U.data_ptr(), uo,
+                  len(self.solver.U_offsets), self._fourier_mass, f.data_ptr(), u.data_ptr(),
+                  _stream(self.device))
+        return u
+
+    def separate(self, f_hat: torch.Tensor) -> torch.Tensor:
+        """The same solve as separate launches: TC.backward, scalar products,
+        jfb_wavenumber_solve, TD.backward."""
         f_phys = self.TC.backward(f_hat)
         return self.TD.backward(self.solve_coefficients(f_phys))
 

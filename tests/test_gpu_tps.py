@@ -93,3 +93,26 @@ def test_helmholtz2d_graph_replay_matches_eager(cuda):
     g.replay()
     torch.cuda.synchronize()
     assert torch.equal(u_out, h(f2))
+
+
+@pytest.mark.parametrize("N", [(64, 64), (33, 48), (80, 32), (96, 96)])
+def test_helmholtz2d_one_launch_matches_separate_launches(cuda, N):
+    """jfb_helmholtz2d_solve (the whole pipeline in one CTA cluster) against the
+    separate transforms and wavenumber solve, and against the oracle's
+    per-mode dense solves."""
+    h = Helmholtz2D(N, device=cuda)
+    assert h.fused
+    f_hat = ok.helmholtz2d_forcing(N, seed=5)
+    f = torch.from_numpy(f_hat).to(cuda)
+    one, sep = h(f), h.separate(f)
+    assert rel(one, sep.cpu().numpy()) < 1e-12
+    if N == (64, 64):
+        _, u_ref = ok.helmholtz2d_solve(f_hat)
+        assert rel(one, u_ref) < 1e-12
+
+
+def test_helmholtz2d_too_large_for_one_cluster_uses_separate_launches(cuda):
+    h = Helmholtz2D((144, 144), device=cuda)
+    assert not h.fused
+    f = torch.from_numpy(ok.helmholtz2d_forcing((144, 144), seed=6)).to(cuda)
+    assert rel(h(f), h.separate(f).cpu().numpy()) == 0.0
