@@ -632,6 +632,15 @@ def main(argv=None):
         e1.record(stream)
         torch.cuda.synchronize(dev)
         us = e0.elapsed_time(e1) * 1000.0 / K
+        for _ in range(5):
+            h.separate(f_hat)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(K):
+            h.separate(f_hat)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        us_sep = e0.elapsed_time(e1) * 1000.0 / K
         graph, f_in, _ = h.graphed(f_hat)
         for _ in range(3):
             graph.replay()
@@ -645,7 +654,10 @@ def main(argv=None):
         out = {
             "workload": "-lap u + u = f, 64 Chebyshev-Dirichlet x 64 Fourier, seeded forcing",
             "us_per_solve": us,
+            "path": ("one launch (jfb_helmholtz2d_solve: 8-CTA cluster, problem in distributed "
+                     "shared memory)" if h.fused else "separate launches"),
             "us_per_solve_graph_replay": us_graph,
+            "us_per_solve_separate_launches": us_sep,
             "solves": K,
             "manufactured_rel_l2": err,
             "u_max": float(u.abs().max()),
