@@ -334,11 +334,14 @@ int jfb_tps_galerkin(const jfb_tps* tps, int order, double* out);
  * shared memory (per CTA 16 (2 N c + N q + 2 n1 ceil(N/8)) + 8 N (N - 2)
  * bytes, c = ceil(n1/8), q = c rounded up to 1 mod 4): JFB_ERR_ARG when that
  * exceeds a CTA's shared memory (use the separate transforms and
- * jfb_wavenumber_solve then). */
+ * jfb_wavenumber_solve then).  U_inv (optional, N - 2 <= 128): the inverse of
+ * each mode's U, (n1, N - 2, N - 2) with entry (r, c) at c (N - 2) + r; with
+ * it and L offsets among {-2, -4} the solve is two short recurrences and a
+ * product (no dependent column chain); NULL: column-oriented substitution. */
 int jfb_helmholtz2d_solve(const jfb_tps* tc, const jfb_tps* td, const double* L,
                           const int64_t* L_offsets, int64_t n_L, const double* U,
-                          const int64_t* U_offsets, int64_t n_U, double fourier_mass,
-                          const void* f_hat, void* u, void* stream);
+                          const int64_t* U_offsets, int64_t n_U, const double* U_inv,
+                          double fourier_mass, const void* f_hat, void* u, void* stream);
 
 /* ---- ensembles ------------------------------------------------------------ */
 

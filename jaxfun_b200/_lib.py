@@ -167,8 +167,8 @@ SIGNATURES = {
     "jfb_tps_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]),
     "jfb_tps_galerkin": (c_int, [c_void_p, c_int, POINTER(c_double)]),
     "jfb_helmholtz2d_solve": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
-                                       c_void_p, c_void_p, c_int64, c_double, c_void_p,
-                                       c_void_p, c_void_p]),
+                                       c_void_p, c_void_p, c_int64, c_void_p, c_double,
+                                       c_void_p, c_void_p, c_void_p]),
     "jfb_ensemble_create": (c_int, [POINTER(c_void_p), c_int32, POINTER(c_void_p)]),
     "jfb_ensemble_advance": (c_int, [c_void_p, c_int64, c_void_p]),
     "jfb_ensemble_destroy": (c_int, [c_void_p]),

@@ -107,7 +107,9 @@ struct Helm2DArgs {
   const c64* tw;     // n1-point twiddles
   FFTPlan plan;
   const double *L, *U;  // (n1, nL, nb), (n1, nU, nb)
+  const double* Uinv;   // optional (n1, nb, nb): U^-1 per mode, entry (r, c) at c nb + r
   int nL, nU, umain;
+  int l2, l4;  // indices of the L offsets -2 / -4 (-1: absent) when those are all of L
   int loff[kHelmMaxDiag], uoff[kHelmMaxDiag];
   int N, nb, M, KC, JR, QS;
   double scale;  // Fourier scalar-product weight / fourier_mass / n1
@@ -187,7 +189,57 @@ __global__ void __cluster_dims__(kHelmCTAs, 1, 1) __launch_bounds__(kHelmThreads
   // substitution: once x_c is final each lane applies its diagonals' entries
   // of column c to their rows (distinct rows per diagonal); the entries of
   // diagonals lane and lane + 32 are loaded one column ahead
-  {
+  if (h.Uinv && h.l2 + h.l4 > -2) {
+    // fast form: L with offsets -2 / -4 only is two independent recurrences
+    // (one per parity class, lanes 0 and 1, in registers); then x = U^-1 y
+    // as a product with the mode's explicit inverse (lanes = rows)
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    for (int kk = warp; kk < kn; kk += nwarps) {
+      const int k = k0 + kk;
+      const double* Lk = h.L + (size_t)k * h.nL * nb;
+      c64* x = Q + kk;  // element c at x[c * QS]
+      if (lane < 2) {
+        // the right-hand side and the multipliers of the next row are loaded
+        // before the current row's update (off the dependent chain)
+        auto l2v = [&](int r) { return (h.l2 >= 0 && r >= 2 && r < nb) ? __ldg(Lk + (size_t)h.l2 * nb + r - 2) : 0.0; };
+        auto l4v = [&](int r) { return (h.l4 >= 0 && r >= 4 && r < nb) ? __ldg(Lk + (size_t)h.l4 * nb + r - 4) : 0.0; };
+        c64 ym2 = cmk(0.0, 0.0), ym4 = cmk(0.0, 0.0);  // y_{r-2}, y_{r-4}
+        c64 vn = (lane < nb) ? x[lane * QS] : cmk(0.0, 0.0);
+        double an = l2v(lane), bn = l4v(lane);
+        for (int r = lane; r < nb; r += 2) {
+          const c64 v0 = vn;
+          const double a2 = an, a4 = bn;
+          if (r + 2 < nb) {
+            vn = x[(r + 2) * QS];
+            an = l2v(r + 2);
+            bn = l4v(r + 2);
+          }
+          const c64 v = v0 - a2 * ym2 - a4 * ym4;
+          x[r * QS] = v;
+          ym4 = ym2;
+          ym2 = v;
+        }
+      }
+      __syncwarp();
+      const double* Ui = h.Uinv + (size_t)k * nb * nb;
+      c64 acc0 = cmk(0.0, 0.0), acc1 = cmk(0.0, 0.0);  // rows lane, lane + 32, ...
+      c64 acc2 = cmk(0.0, 0.0), acc3 = cmk(0.0, 0.0);
+#pragma unroll 8
+      for (int c = 0; c < nb; ++c) {
+        const c64 y = x[c * QS];
+        const double* col = Ui + (size_t)c * nb;
+        if (lane <= c) acc0 = acc0 + __ldg(col + lane) * y;
+        if (lane + 32 <= c) acc1 = acc1 + __ldg(col + lane + 32) * y;
+        if (lane + 64 <= c) acc2 = acc2 + __ldg(col + lane + 64) * y;
+        if (lane + 96 <= c) acc3 = acc3 + __ldg(col + lane + 96) * y;
+      }
+      c64* O = A + kk;
+      if (lane < nb) O[lane * KC] = acc0;
+      if (lane + 32 < nb) O[(lane + 32) * KC] = acc1;
+      if (lane + 64 < nb) O[(lane + 64) * KC] = acc2;
+      if (lane + 96 < nb) O[(lane + 96) * KC] = acc3;
+    }
+  } else {
     const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
     for (int kk = warp; kk < kn; kk += nwarps) {
       const int k = k0 + kk;
@@ -532,8 +584,9 @@ extern "C" int jfb_tps_get_sizes(const jfb_tps* t, int32_t* out4) {
 
 extern "C" int jfb_helmholtz2d_solve(const jfb_tps* tc, const jfb_tps* td, const double* L,
                                      const int64_t* L_offsets, int64_t n_L, const double* U,
-                                     const int64_t* U_offsets, int64_t n_U, double fourier_mass,
-                                     const void* f_hat, void* u, void* stream) {
+                                     const int64_t* U_offsets, int64_t n_U, const double* U_inv,
+                                     double fourier_mass, const void* f_hat, void* u,
+                                     void* stream) {
   JFB_REQUIRE(tc && td && U && U_offsets && f_hat && u, "null pointer");
   JFB_REQUIRE(n_L == 0 || (L && L_offsets), "null L factor");
   JFB_REQUIRE(tc->cfg.ndim == 2 && td->cfg.ndim == 2, "2-D spaces only");
@@ -572,6 +625,16 @@ extern "C" int jfb_helmholtz2d_solve(const jfb_tps* tc, const jfb_tps* td, const
     if (h.uoff[d] == 0) h.umain = d;
   }
   JFB_REQUIRE(h.umain >= 0, "U offsets must contain the main diagonal");
+  JFB_REQUIRE(!U_inv || td->nb <= 128, "U_inv form: at most 128 unknowns per mode");
+  h.Uinv = U_inv;
+  h.l2 = h.l4 = -1;
+  bool two_four = true;
+  for (int d = 0; d < h.nL; ++d) {
+    if (h.loff[d] == -2) h.l2 = d;
+    else if (h.loff[d] == -4) h.l4 = d;
+    else two_four = false;
+  }
+  if (!two_four) h.l2 = h.l4 = -1;  // the general column-oriented form
   // the column updates of one step write one row per diagonal
   for (int a = 0; a < h.nU; ++a)
     for (int b = a + 1; b < h.nU; ++b) JFB_REQUIRE(h.uoff[a] != h.uoff[b], "repeated U offset");

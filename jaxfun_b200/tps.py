@@ -161,6 +161,21 @@ class Helmholtz2D:
         qs = kc + (5 - kc % 4) % 4  # padded row of the solve vectors
         need = 16 * (2 * n * kc + n * qs + 2 * m * jr) + 8 * n * nb
         self.fused = need <= optin
+        # explicit inverse of each mode's U (entry (r, c) at c nb + r): the
+        # back substitution of the one-launch solve becomes a product
+        self._Uinv = None
+        if self.fused and nb <= 128:
+            offs = torch.tensor(self.solver.U_offsets, device=self.device)
+            Ud = self._U  # (modes, n_diag, nb): U[i, i + s] at [d, i + s]
+            dense = torch.zeros((Ud.shape[0], nb, nb), dtype=torch.float64, device=self.device)
+            cols = torch.arange(nb, device=self.device)
+            for d in range(Ud.shape[1]):
+                s_ = int(offs[d])
+                c = cols[s_:]
+                dense[:, c - s_, c] = Ud[:, d, s_:]
+            eye = torch.eye(nb, dtype=torch.float64, device=self.device).expand_as(dense)
+            inv = torch.linalg.solve_triangular(dense, eye, upper=True)
+            self._Uinv = inv.transpose(1, 2).contiguous()
 
     def solve_coefficients(self, f_phys: torch.Tensor) -> torch.Tensor:
         """Dirichlet x Fourier coefficients of u from samples of f."""
@@ -181,8 +196,9 @@ class Helmholtz2D:
         _lib.call("jfb_helmholtz2d_solve", self.TC._h, self.TD._h,
                   self._L.data_ptr() if self._L.numel() else None, lo,
                   len(self.solver.L_offsets), self._U.data_ptr(), uo,
-                  len(self.solver.U_offsets), self._fourier_mass, f.data_ptr(), u.data_ptr(),
-                  _stream(self.device))
+                  len(self.solver.U_offsets),
+                  self._Uinv.data_ptr() if self._Uinv is not None else None,
+                  self._fourier_mass, f.data_ptr(), u.data_ptr(), _stream(self.device))
         return u
 
     def separate(self, f_hat: torch.Tensor) -> torch.Tensor:

@@ -101,11 +101,14 @@ def test_helmholtz2d_one_launch_matches_separate_launches(cuda, N):
     separate transforms and wavenumber solve, and against the oracle's
     per-mode dense solves."""
     h = Helmholtz2D(N, device=cuda)
-    assert h.fused
+    assert h.fused and h._Uinv is not None
     f_hat = ok.helmholtz2d_forcing(N, seed=5)
     f = torch.from_numpy(f_hat).to(cuda)
     one, sep = h(f), h.separate(f)
     assert rel(one, sep.cpu().numpy()) < 1e-12
+    # the general form of the in-cluster solve (column-oriented substitution)
+    h._Uinv = None
+    assert rel(h(f), sep.cpu().numpy()) < 1e-12
     if N == (64, 64):
         _, u_ref = ok.helmholtz2d_solve(f_hat)
         assert rel(one, u_ref) < 1e-12
