@@ -2003,11 +2003,17 @@ static int adj_mass(jfb_kmm_plan* pl, const AState& mu, double cm, double gl, co
 static int adj_solve(jfb_kmm_plan* pl, const FactorSet& fs, const AState& src, const AState& dst,
                      cudaStream_t s) {
   const Dims& d = pl->d;
-  const int blocks = ceil_div(d.P, 128);
-  band_solve_t_kernel<<<blocks, 128, 0, s>>>(d, fs.band[0], fs.bp[0], fs.bq[0], d.nB, 0, src.u, dst.u);
-  band_solve_t_kernel<<<blocks, 128, 0, s>>>(d, fs.band[1], fs.bp[1], fs.bq[1], d.nD, 0, src.g, dst.g);
-  band_solve_t_kernel<<<1, 32, 0, s>>>(d, fs.band[2], fs.bp[2], fs.bq[2], d.nD, 1, src.v, dst.v);
-  band_solve_t_kernel<<<1, 32, 0, s>>>(d, fs.band[2], fs.bp[2], fs.bq[2], d.nD, 1, src.w, dst.w);
+  // a warp per pencil (kBandWarps pencils per block), the vector in shared memory
+  const int blocks = ceil_div(d.P, kBandWarps);
+  const size_t smB = (size_t)kBandWarps * d.nB * sizeof(c64), smD = (size_t)kBandWarps * d.nD * sizeof(c64);
+  band_solve_t_warp_kernel<<<blocks, 32 * kBandWarps, smB, s>>>(d, fs.band[0], fs.bp[0], fs.bq[0],
+                                                                d.nB, 0, src.u, dst.u);
+  band_solve_t_warp_kernel<<<blocks, 32 * kBandWarps, smD, s>>>(d, fs.band[1], fs.bp[1], fs.bq[1],
+                                                                d.nD, 0, src.g, dst.g);
+  band_solve_t_warp_kernel<<<1, 32 * kBandWarps, smD, s>>>(d, fs.band[2], fs.bp[2], fs.bq[2], d.nD,
+                                                           1, src.v, dst.v);
+  band_solve_t_warp_kernel<<<1, 32 * kBandWarps, smD, s>>>(d, fs.band[2], fs.bp[2], fs.bq[2], d.nD,
+                                                           1, src.w, dst.w);
   JFB_CHECK_LAUNCH();
   return JFB_OK;
 }

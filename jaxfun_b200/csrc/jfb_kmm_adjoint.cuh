@@ -17,7 +17,9 @@
 //   pencil_terms_kernel  dst[:, p] (+)= sum_t c_t(ky, kz) Op_t src_t[:, p],
 //                        Op_t a real x-matrix, its transpose or the identity
 //   band_solve_t_kernel  A^T x = b per wavenumber from the no-pivot LU band of
-//                        A (the factors of the forward solves, kept)
+//                        A (the factors of the forward solves, kept); the
+//                        production path is band_solve_t_warp_kernel (a warp
+//                        per pencil)
 //   z_adjoint_kernel     transposed rotational product: with w the adjoint of
 //                        n = -(u_t x omega_t), adj u = w x omega_t and
 //                        adj omega = u_t x w
@@ -129,6 +131,97 @@ __global__ void __launch_bounds__(128) band_solve_t_kernel(Dims d, const double*
     for (int k = i + 1; k <= k1; ++k) s = s - at(i - k, i) * out[(size_t)k * P + pen];
     out[(size_t)i * P + pen] = s;
   }
+}
+
+// The same solve with a warp per pencil: the vector in shared memory,
+// column-oriented substitution (once an unknown is final, lane j applies the
+// j-th band entry of its column / row to the unknown j places away; distinct
+// targets per lane), the band entries of kBandChunk steps loaded one chunk
+// ahead.  U^T y = b: y_k = b_k / U[k][k], then b_{k+j} -= U[k][k+j] y_k
+// (j = 1..q); L^T x = y from the bottom: x_{k-j} -= L[k][k-j] x_k (j = 1..p).
+constexpr int kBandChunk = 8;
+constexpr int kBandWarps = 4;  // pencils per block
+__global__ void __launch_bounds__(32 * kBandWarps) band_solve_t_warp_kernel(
+    Dims d, const double* __restrict__ band, int p, int q, int n, int mean_only,
+    const c64* __restrict__ rhs, c64* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int pen = blockIdx.x * kBandWarps + wib;
+  if (pen >= (mean_only ? 1 : d.P)) return;  // whole warps
+  c64* x = reinterpret_cast<c64*>(smem_raw) + (size_t)wib * n;
+  const size_t P = (size_t)d.P;
+  const int row = pen / d.Kz, kz = pen % d.Kz;
+  if (row == d.Ny / 2) {
+    for (int i = lane; i < n; i += 32) out[(size_t)i * P + pen] = cmk(0.0, 0.0);
+    return;
+  }
+  const int kyi = (row < d.Ny / 2) ? row : d.Ny - row;
+  const size_t mode = mean_only ? 0 : (size_t)kyi * d.Kz + kz;
+  const double* B = band + mode * (size_t)(p + q + 1) * n;
+  auto at = [&](int off, int col) { return __ldg(B + (size_t)(p + off) * n + col); };
+  for (int i = lane; i < n; i += 32) x[i] = rhs[(size_t)i * P + pen];
+  __syncwarp();
+  // U^T y = b.  Lane owns band offsets j0 = lane + 1 and j1 = lane + 33.
+  const int j0 = lane + 1, j1 = lane + 33;
+  double u0[kBandChunk], u1[kBandChunk], rd[kBandChunk];
+  double v0[kBandChunk], v1[kBandChunk], sd[kBandChunk];
+  auto uload = [&](int k, double& a, double& b, double& r) {
+    a = (k < n && j0 <= q && k + j0 < n) ? at(j0, k + j0) : 0.0;
+    b = (k < n && j1 <= q && k + j1 < n) ? at(j1, k + j1) : 0.0;
+    r = (k < n) ? 1.0 / at(0, k) : 0.0;
+  };
+#pragma unroll
+  for (int t = 0; t < kBandChunk; ++t) uload(t, u0[t], u1[t], rd[t]);
+  for (int k0 = 0; k0 < n; k0 += kBandChunk) {
+#pragma unroll
+    for (int t = 0; t < kBandChunk; ++t) uload(k0 + kBandChunk + t, v0[t], v1[t], sd[t]);
+#pragma unroll
+    for (int t = 0; t < kBandChunk; ++t) {
+      const int k = k0 + t;
+      if (k >= n) break;
+      const c64 b = x[k];
+      __syncwarp();
+      const c64 y = rd[t] * b;
+      if (lane == 0) x[k] = y;
+      if (j0 <= q && k + j0 < n) x[k + j0] = x[k + j0] - u0[t] * y;
+      if (j1 <= q && k + j1 < n) x[k + j1] = x[k + j1] - u1[t] * y;
+      for (int j = lane + 65; j <= q && k + j < n; j += 32) x[k + j] = x[k + j] - at(j, k + j) * y;
+      __syncwarp();
+    }
+#pragma unroll
+    for (int t = 0; t < kBandChunk; ++t) {
+      u0[t] = v0[t];
+      u1[t] = v1[t];
+      rd[t] = sd[t];
+    }
+  }
+  // L^T x = y, k from n - 1 down
+  auto lload = [&](int k, double& a, double& b) {
+    a = (k >= 0 && j0 <= p && k - j0 >= 0) ? at(-j0, k - j0) : 0.0;
+    b = (k >= 0 && j1 <= p && k - j1 >= 0) ? at(-j1, k - j1) : 0.0;
+  };
+#pragma unroll
+  for (int t = 0; t < kBandChunk; ++t) lload(n - 1 - t, u0[t], u1[t]);
+  for (int k0 = n - 1; k0 >= 0; k0 -= kBandChunk) {
+#pragma unroll
+    for (int t = 0; t < kBandChunk; ++t) lload(k0 - kBandChunk - t, v0[t], v1[t]);
+#pragma unroll
+    for (int t = 0; t < kBandChunk; ++t) {
+      const int k = k0 - t;
+      if (k < 0) break;
+      const c64 xk = x[k];
+      if (j0 <= p && k - j0 >= 0) x[k - j0] = x[k - j0] - u0[t] * xk;
+      if (j1 <= p && k - j1 >= 0) x[k - j1] = x[k - j1] - u1[t] * xk;
+      for (int j = lane + 65; j <= p && k - j >= 0; j += 32) x[k - j] = x[k - j] - at(-j, k - j) * xk;
+      __syncwarp();
+    }
+#pragma unroll
+    for (int t = 0; t < kBandChunk; ++t) {
+      u0[t] = v0[t];
+      u1[t] = v1[t];
+    }
+  }
+  for (int i = lane; i < n; i += 32) out[(size_t)i * P + pen] = x[i];
 }
 
 // Transposed z stage, per group of kZRows (x, y) rows: the forward u, omega
