@@ -1887,7 +1887,7 @@ static void term(PTermList& L, const c64* src, const double* mat, int src_rows, 
 
 static int run(jfb_kmm_plan* pl, const PTermList& L, cudaStream_t s) {
   JFB_REQUIRE(L.n <= kMaxTerms, "term list too long");
-  dim3 g(ceil_div(pl->d.P, 32), ceil_div(L.dst_rows, 8));
+  dim3 g(ceil_div(pl->d.P, 32), ceil_div(L.dst_rows, 8 * kTermRows));
   pencil_terms_kernel<<<g, 256, 0, s>>>(pl->d, L);
   JFB_CHECK_LAUNCH();
   return JFB_OK;

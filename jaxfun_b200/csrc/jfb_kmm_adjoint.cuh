@@ -53,14 +53,20 @@ struct PTermList {
   PTerm t[kMaxTerms];
 };
 
-// block: 32 pencils x 8 rows; grid (ceil(P / 32), ceil(dst_rows / 8))
+// block: 32 pencils (lanes) x 8 warps, each thread kTermRows consecutive
+// destination rows of one pencil (every source value it loads serves all of
+// them); grid (ceil(P / 32), ceil(dst_rows / (8 kTermRows)))
+constexpr int kTermRows = 8;
 __global__ void __launch_bounds__(256) pencil_terms_kernel(Dims d, PTermList L) {
   const int p = blockIdx.x * 32 + (threadIdx.x & 31);
-  const int r = blockIdx.y * 8 + (threadIdx.x >> 5);
-  if (p >= d.P || r >= L.dst_rows) return;
+  const int r0 = (blockIdx.y * 8 + (threadIdx.x >> 5)) * kTermRows;
+  if (p >= d.P || r0 >= L.dst_rows) return;
   const size_t P = (size_t)d.P;
+  const int nr = min(kTermRows, L.dst_rows - r0);
   const int row = p / d.Kz, kzi = p % d.Kz;
-  c64 acc = cmk(0.0, 0.0);
+  c64 acc[kTermRows];
+#pragma unroll
+  for (int q = 0; q < kTermRows; ++q) acc[q] = cmk(0.0, 0.0);
   if (row != d.Ny / 2) {  // the y Nyquist row stays zero
     const double ky = ((row < d.Ny / 2) ? row : row - d.Ny) * d.dfy;
     const double kz = kzi * d.dfz;
@@ -78,23 +84,43 @@ __global__ void __launch_bounds__(256) pencil_terms_kernel(Dims d, PTermList L) 
       } else {
         for (int e = 0; e < T.c; ++e) s *= k2;
       }
-      c64 v = cmk(0.0, 0.0);
+      c64 v[kTermRows];
+#pragma unroll
+      for (int q = 0; q < kTermRows; ++q) v[q] = cmk(0.0, 0.0);
       if (!T.mat) {
-        v = T.src[(size_t)r * P + p];
+#pragma unroll
+        for (int q = 0; q < kTermRows; ++q)
+          if (q < nr) v[q] = T.src[(size_t)(r0 + q) * P + p];
       } else if (T.trans) {
-        for (int k = 0; k < T.src_rows; ++k)
-          v = v + __ldg(T.mat + (size_t)k * L.dst_rows + r) * T.src[(size_t)k * P + p];
+        for (int k = 0; k < T.src_rows; ++k) {
+          const c64 x = T.src[(size_t)k * P + p];
+          const double* m = T.mat + (size_t)k * L.dst_rows + r0;
+#pragma unroll
+          for (int q = 0; q < kTermRows; ++q)
+            if (q < nr) v[q] = v[q] + __ldg(m + q) * x;
+        }
       } else {
-        for (int k = 0; k < T.src_rows; ++k)
-          v = v + __ldg(T.mat + (size_t)r * T.src_rows + k) * T.src[(size_t)k * P + p];
+        for (int k = 0; k < T.src_rows; ++k) {
+          const c64 x = T.src[(size_t)k * P + p];
+#pragma unroll
+          for (int q = 0; q < kTermRows; ++q)
+            if (q < nr) v[q] = v[q] + __ldg(T.mat + (size_t)(r0 + q) * T.src_rows + k) * x;
+        }
       }
-      if (T.realpart) v.im = 0.0;
       const c64 cf = cmk(T.cre * s, T.cim * s);
-      acc = acc + cf * v;
+#pragma unroll
+      for (int q = 0; q < kTermRows; ++q) {
+        if (T.realpart) v[q].im = 0.0;
+        acc[q] = acc[q] + cf * v[q];
+      }
     }
   }
-  c64* out = L.dst + (size_t)r * P + p;
-  *out = L.accumulate ? *out + acc : acc;
+#pragma unroll
+  for (int q = 0; q < kTermRows; ++q) {
+    if (q >= nr) break;
+    c64* out = L.dst + (size_t)(r0 + q) * P + p;
+    *out = L.accumulate ? *out + acc[q] : acc[q];
+  }
 }
 
 // A^T x = b for every pencil of the half spectrum, A the system of the
