@@ -119,3 +119,23 @@ def test_helmholtz2d_too_large_for_one_cluster_uses_separate_launches(cuda):
     assert not h.fused
     f = torch.from_numpy(ok.helmholtz2d_forcing((144, 144), seed=6)).to(cuda)
     assert rel(h(f), h.separate(f).cpu().numpy()) == 0.0
+
+
+def test_helmholtz2d_solve_rejects_mismatched_spaces(cuda):
+    """The one-launch entry point checks its spaces and factors like the
+    reference's solver construction (errors, no launch)."""
+    from jaxfun_b200 import _lib
+
+    h = Helmholtz2D((32, 16), device=cuda)
+    f = torch.zeros((32, 16), dtype=torch.complex128, device=cuda)
+    u = torch.empty((32, 16), dtype=torch.complex128, device=cuda)
+    lo, uo = h._offs
+    args = lambda tc, td: (tc._h, td._h, h._L.data_ptr(), lo, len(h.solver.L_offsets),  # noqa: E731
+                           h._U.data_ptr(), uo, len(h.solver.U_offsets), None,
+                           h._fourier_mass, f.data_ptr(), u.data_ptr(), None)
+    with pytest.raises(_lib.JFBError) as e:  # Dirichlet space in the orthogonal slot
+        _lib.call("jfb_helmholtz2d_solve", *args(h.TD, h.TD))
+    assert e.value.status == _lib.JFB_ERR_ARG
+    other = Helmholtz2D((33, 16), device=cuda)
+    with pytest.raises(_lib.JFBError):  # sizes differ
+        _lib.call("jfb_helmholtz2d_solve", *args(h.TC, other.TD))
