@@ -1010,9 +1010,9 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   if (pl->mhd) {
     // the coupled step transforms twelve fields with the shared-memory kernels
     pl->plane = false;
-    pl->smem_mhd = mhd_smem_bytes(d.nD);
+    pl->smem_mhd = mhd_smem_bytes(d.nD, d.Nx);
     pl->smem_zm = (size_t)2 * d.Mz * kZRows * 6 * sizeof(c64);
-    if (pl->smem_mhd > 227 * 1024 || pl->smem_zm > 227 * 1024) {
+    if (pl->smem_mhd > 227 * 1024 || pl->smem_zm > 227 * 1024 || (d.nD + 1) / 2 > kMaxM) {
       set_error("grid too large for the MHD shared-memory tiling");
       return fail(JFB_ERR_ARG);
     }

@@ -31,6 +31,7 @@
 // index, a column of B2 or C1 the opposite one.
 #pragma once
 
+#include "jfb_kmm_gemm.cuh"
 #include "jfb_kmm_kernels.cuh"
 
 namespace jfb {
@@ -71,9 +72,10 @@ struct MhdArgs {
 constexpr int kMhdThreads = 512;
 constexpr int kMhdW = 16;  // pencils per CTA
 
-inline size_t mhd_smem_bytes(int nD) {
-  // right-hand sides and solutions, 3 components x nD rows x 16 pencils
-  return (size_t)2 * 3 * nD * kMhdW * sizeof(c64);
+inline size_t mhd_smem_bytes(int nD, int N) {
+  // right-hand sides and solutions (3 components x nD rows x 16 pencils),
+  // then the tile's x samples (3 components x N rows x 16 pencils)
+  return ((size_t)2 * 3 * nD + (size_t)3 * N) * kMhdW * sizeof(c64);
 }
 
 __global__ void __launch_bounds__(kMhdThreads, 1) mhd_a_kernel(Dims d, DevOps o, MhdOps M,
@@ -89,6 +91,7 @@ __global__ void __launch_bounds__(kMhdThreads, 1) mhd_a_kernel(Dims d, DevOps o,
   const size_t P = (size_t)d.P;
   c64* RHS = reinterpret_cast<c64*>(smem_raw);  // [3][nD][kMhdW], split parity order
   c64* SOL = RHS + (size_t)3 * nD * kMhdW;       // [3][nD][kMhdW], split parity order
+  c64* HS = SOL + (size_t)3 * nD * kMhdW;        // [3][N][kMhdW]: the tile's x samples
   // split parity order: even rows first, then odd rows
   auto srow = [&](int i) { return (i & 1) ? M.nDe + (i >> 1) : (i >> 1); };
 
@@ -111,6 +114,14 @@ __global__ void __launch_bounds__(kMhdThreads, 1) mhd_a_kernel(Dims d, DevOps o,
   __syncthreads();
 
   if (a.mode != kMhdFields) {
+    // the tile's x samples, read once into shared memory (every row i of the
+    // scalar products uses all of them)
+    for (int e = tid; e < 3 * N * kMhdW; e += kMhdThreads) {
+      const int w = e % kMhdW, cj = e / kMhdW;  // cj = c N + j
+      const int p = s_p[w];
+      HS[e] = (p >= 0) ? a.HXA[(size_t)cj * P + p] : cmk(0.0, 0.0);
+    }
+    __syncthreads();
     // 1. scalar products S_D Q v of the three x profiles (mirror sums), and
     //    for a step the right-hand sides; one thread per (comp, row, pencil)
     const bool step = a.mode == kMhdStep;
@@ -119,16 +130,16 @@ __global__ void __launch_bounds__(kMhdThreads, 1) mhd_a_kernel(Dims d, DevOps o,
       const int p = s_p[w];
       c64 rhs = cmk(0.0, 0.0);
       if (p >= 0) {
-        const c64* h = a.HXA + (size_t)c * N * P + p;
+        const c64* h = HS + (size_t)c * N * kMhdW + w;  // row j at h[j kMhdW]
         const double* r3 = M.R3 + (size_t)i * N;
         const double sg = (i & 1) ? -1.0 : 1.0;
         c64 s0 = cmk(0.0, 0.0), s1 = s0;
         for (int j = 0; j < Jl; ++j) {
-          const c64 x = h[(size_t)j * P] + sg * h[(size_t)(N - 1 - j) * P];
+          const c64 x = h[j * kMhdW] + sg * h[(N - 1 - j) * kMhdW];
           if (j & 1) s1 = s1 + __ldg(r3 + j) * x;
           else s0 = s0 + __ldg(r3 + j) * x;
         }
-        if ((N & 1) && !(i & 1)) s0 = s0 + __ldg(r3 + Jl) * h[(size_t)Jl * P];
+        if ((N & 1) && !(i & 1)) s0 = s0 + __ldg(r3 + Jl) * h[Jl * kMhdW];
         if (!step) {
           rhs = s0 + s1;
         } else {
@@ -176,16 +187,7 @@ __global__ void __launch_bounds__(kMhdThreads, 1) mhd_a_kernel(Dims d, DevOps o,
           const double* rec = a.sa + (size_t)s_mode[w] * a.sa_rec;
           const int m = par ? nD / 2 : (nD + 1) / 2;
           c64* y = RHS + ((size_t)c * nD + (par ? M.nDe : 0)) * kMhdW + w;
-          c64 y1 = cmk(0.0, 0.0), y2 = y1;
-          for (int r = 0; r < m; ++r) {
-            const int i = 2 * r + par;
-            c64 v = y[r * kMhdW];
-            v = v - __ldg(rec + 2 * i) * y1;
-            v = v - __ldg(rec + 2 * i + 1) * y2;
-            y[r * kMhdW] = v;
-            y2 = y1;
-            y1 = v;
-          }
+          forward_elim(rec, par, m, y, kMhdW);  // multipliers loaded ahead of their rows
         }
       }
       __syncthreads();
