@@ -568,29 +568,34 @@ template <> struct Tx<float> {
 };
 template <typename T> static cpx<T>* buf(void* p) { return reinterpret_cast<cpx<T>*>(p); }
 
+// nb / nf: fields transformed backward / forward (6 / 3 for the flow step,
+// 12 / 6 for the coupled MHD step)
 template <int P, typename T>
-static void launch_y_warp(jfb_kmm_plan* pl, cudaStream_t s, bool backward) {
+static void launch_y_warp(jfb_kmm_plan* pl, cudaStream_t s, bool backward, int nb = 6,
+                          int nf = 3) {
   const Dims d = tdims<T>(pl);
   const size_t sm = backward ? pl->smem_yw_b : pl->smem_yw_f;
   const size_t smT = sm / sizeof(c64) * sizeof(cpx<T>);
+  const int chunks = ceil_div(d.Kz, pl->KCw);
   if (backward) {
-    dim3 g(d.Nx, 6, d.Kz / pl->KCw);
+    dim3 g(d.Nx, nb, chunks);
     y_backward_warp_kernel<P, T><<<g, 256, smT, s>>>(d, pl->KCw, Tx<T>::twy(pl), buf<T>(pl->X),
                                                        buf<T>(pl->Y));
   } else {
-    dim3 g(d.Nx, 3, d.Kz / pl->KCw);
+    dim3 g(d.Nx, nf, chunks);
     y_forward_warp_kernel<P, T><<<g, 256, smT, s>>>(d, pl->KCw, Tx<T>::twy(pl), buf<T>(pl->HZ),
                                                       buf<T>(pl->HX), pl->ops.xphys);
   }
 }
 
 template <typename T>
-static void launch_y_warp_any(jfb_kmm_plan* pl, cudaStream_t s, bool backward) {
+static void launch_y_warp_any(jfb_kmm_plan* pl, cudaStream_t s, bool backward, int nb = 6,
+                              int nf = 3) {
   switch (pl->py) {
-    case 2: launch_y_warp<2, T>(pl, s, backward); break;
-    case 3: launch_y_warp<3, T>(pl, s, backward); break;
-    case 4: launch_y_warp<4, T>(pl, s, backward); break;
-    default: launch_y_warp<6, T>(pl, s, backward); break;
+    case 2: launch_y_warp<2, T>(pl, s, backward, nb, nf); break;
+    case 3: launch_y_warp<3, T>(pl, s, backward, nb, nf); break;
+    case 4: launch_y_warp<4, T>(pl, s, backward, nb, nf); break;
+    default: launch_y_warp<6, T>(pl, s, backward, nb, nf); break;
   }
 }
 
@@ -682,8 +687,12 @@ static int launch_transforms_t(jfb_kmm_plan* pl, cudaStream_t s) {
 // stage with the Lorentz force and the EMF, six fields (n, emf) forward in y.
 static int launch_transforms_mhd(jfb_kmm_plan* pl, cudaStream_t s) {
   const Dims& d = pl->d;
-  dim3 gy(d.Nx, 12, d.Kz / pl->KC);
-  y_backward_kernel<double><<<gy, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->X, pl->Y);
+  if (pl->py) {  // warp-shuffle transforms along y (My = 32 P)
+    launch_y_warp_any<double>(pl, s, true, 12, 6);
+  } else {
+    dim3 gy(d.Nx, 12, d.Kz / pl->KC);
+    y_backward_kernel<double><<<gy, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->X, pl->Y);
+  }
   JFB_CHECK_LAUNCH();
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[2], s));
   const int zb = ceil_div((int64_t)d.Nx * d.My, kZRows);
@@ -691,9 +700,13 @@ static int launch_transforms_mhd(jfb_kmm_plan* pl, cudaStream_t s) {
                                                   pl->HZ);
   JFB_CHECK_LAUNCH();
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[3], s));
-  dim3 gf(d.Nx, 6, d.Kz / pl->KC);
-  y_forward_kernel<double><<<gf, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->HZ, pl->HX,
-                                                       pl->ops.xphys);
+  if (pl->py) {
+    launch_y_warp_any<double>(pl, s, false, 12, 6);
+  } else {
+    dim3 gf(d.Nx, 6, d.Kz / pl->KC);
+    y_forward_kernel<double><<<gf, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->HZ,
+                                                         pl->HX, pl->ops.xphys);
+  }
   JFB_CHECK_LAUNCH();
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[4], s));
   return JFB_OK;
@@ -993,8 +1006,8 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   pl->py = warp_radix(d.My);
   pl->pz = (pl->qk <= 2) ? warp_radix(d.Mz) : 0;
   pl->pnz = (pl->qk <= 2) ? warp_radix(d.Nz) : 0;
-  pl->KCw = 16;
-  while (d.Kz % pl->KCw) pl->KCw /= 2;
+  // kz columns per warp-FFT y block (a warp each; the last chunk may be partial)
+  pl->KCw = std::min(8, d.Kz);
   pl->smem_yw_b = (size_t)(d.Ny + d.My) * (pl->KCw + 1) * sizeof(c64);
   pl->smem_yw_f = pl->smem_yw_b;
   // fused plane transforms: warp-FFT lengths 64 or 96 on both periodic axes,

@@ -27,9 +27,10 @@ __global__ void __launch_bounds__(256) y_backward_warp_kernel(Dims d, int KC,
   const int j = blockIdx.x, f = blockIdx.y, kc0 = blockIdx.z * KC;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const cpx<T>* src = X + ((size_t)f * d.Nx + j) * d.P + kc0;
+  const int kcn = min(KC, d.Kz - kc0);  // columns of this chunk (the last may be partial)
   for (int idx = threadIdx.x; idx < d.Ny * KC; idx += blockDim.x) {
     const int c = idx % KC, r = idx / KC;
-    in[r * ld + c] = src[(size_t)r * d.Kz + c];
+    in[r * ld + c] = (c < kcn) ? src[(size_t)r * d.Kz + c] : cmk(T(0), T(0));
   }
   WarpTw<P, T> w;
   load_warp_tw<P, T>(w, tw, lane);
@@ -54,7 +55,7 @@ __global__ void __launch_bounds__(256) y_backward_warp_kernel(Dims d, int KC,
   cpx<T>* dst = Y + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
   for (int idx = threadIdx.x; idx < d.My * KC; idx += blockDim.x) {
     const int c = idx % KC, r = idx / KC;
-    dst[(size_t)r * d.Kz + c] = out[r * ld + c];
+    if (c < kcn) dst[(size_t)r * d.Kz + c] = out[r * ld + c];
   }
 }
 
@@ -75,9 +76,10 @@ __global__ void __launch_bounds__(256) y_forward_warp_kernel(Dims d, int KC,
   const int j = blockIdx.x, f = blockIdx.y, kc0 = blockIdx.z * KC;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const cpx<T>* src = HZ + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
+  const int kcn = min(KC, d.Kz - kc0);  // columns of this chunk (the last may be partial)
   for (int idx = threadIdx.x; idx < d.My * KC; idx += blockDim.x) {
     const int c = idx % KC, r = idx / KC;
-    in[r * ld + c] = src[(size_t)r * d.Kz + c];
+    in[r * ld + c] = (c < kcn) ? src[(size_t)r * d.Kz + c] : cmk(T(0), T(0));
   }
   WarpTw<P, T> w;
   load_warp_tw<P, T>(w, tw, lane);
@@ -107,7 +109,7 @@ __global__ void __launch_bounds__(256) y_forward_warp_kernel(Dims d, int KC,
   cpx<T>* dst = HX + ((size_t)f * d.Nx + j) * d.P + kc0;
   for (int idx = threadIdx.x; idx < d.Ny * KC; idx += blockDim.x) {
     const int c = idx % KC, r = idx / KC;
-    dst[(size_t)r * d.Kz + c] = out[r * ld + c];
+    if (c < kcn) dst[(size_t)r * d.Kz + c] = out[r * ld + c];
   }
 }
 
