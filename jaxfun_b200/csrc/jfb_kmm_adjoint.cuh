@@ -272,8 +272,9 @@ __global__ void __launch_bounds__(256) z_adjoint_kernel(DevOps o, Dims d, FFTPla
   auto field = [&](int f) -> const c64* {  // 0..5 forward u, omega; 6..8 adjoint w; 9 none
     return (f < 6) ? Y + (size_t)f * plane : (f < 9) ? Wa + (size_t)(f - 6) * plane : nullptr;
   };
+  // k fastest: a warp reads consecutive spectral values of one row and field
   for (int idx = threadIdx.x; idx < d.Mz * NC; idx += blockDim.x) {
-    const int c = idx % NC, k = idx / NC;
+    const int k = idx % d.Mz, c = idx / d.Mz;
     const int rl = c / NP, pr = c % NP;
     const int row = row0 + rl;
     c64 z = cmk(0.0, 0.0);

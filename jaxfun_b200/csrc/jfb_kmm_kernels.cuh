@@ -1110,8 +1110,9 @@ __global__ void __launch_bounds__(256) z_cross_kernel(DevOps o, Dims d, FFTPlan 
   const int nrows = d.Nx * d.My;
   const size_t plane = (size_t)d.Nx * d.My * d.Kz;
   // build the Hermitian-extended packed spectra Z = A_f + i A_{f+1}
+  // k fastest: a warp reads consecutive spectral values of one row and field
   for (int idx = threadIdx.x; idx < d.Mz * NC; idx += blockDim.x) {
-    const int c = idx % NC, k = idx / NC;
+    const int k = idx % d.Mz, c = idx / d.Mz;
     const int rl = c / 3, pr = c % 3;
     const int row = row0 + rl;
     cpx<T> z = cmk(T(0), T(0));

@@ -325,8 +325,9 @@ __global__ void __launch_bounds__(256) z_cross_mhd_kernel(DevOps o, Dims d, MhdP
   const int row0 = blockIdx.x * kZRows;  // row = j * My + y
   const int nrows = d.Nx * d.My;
   const size_t plane = (size_t)d.Nx * d.My * d.Kz;
+  // k fastest: a warp reads consecutive spectral values of one row and field
   for (int idx = threadIdx.x; idx < d.Mz * NC; idx += blockDim.x) {
-    const int c = idx % NC, k = idx / NC;
+    const int k = idx % d.Mz, c = idx / d.Mz;
     const int rl = c / 6, pr = c % 6;
     const int row = row0 + rl;
     c64 z = cmk(0.0, 0.0);
