@@ -1006,8 +1006,8 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   pl->py = warp_radix(d.My);
   pl->pz = (pl->qk <= 2) ? warp_radix(d.Mz) : 0;
   pl->pnz = (pl->qk <= 2) ? warp_radix(d.Nz) : 0;
-  // kz columns per warp-FFT y block (a warp each; the last chunk may be partial)
-  pl->KCw = std::min(8, d.Kz);
+  // kz columns per warp-FFT y block (two per warp; the last chunk may be partial)
+  pl->KCw = std::min(16, d.Kz);
   pl->smem_yw_b = (size_t)(d.Ny + d.My) * (pl->KCw + 1) * sizeof(c64);
   pl->smem_yw_f = pl->smem_yw_b;
   // fused plane transforms: warp-FFT lengths 64 or 96 on both periodic axes,
