@@ -218,6 +218,42 @@ def cpu_oracle_rate(fields, grid, seconds, threads):
     return n / dt, n
 
 
+def _single_threaded_worker():
+    """Pool initializer: one BLAS / FFT thread per worker process (set before
+    the worker imports numpy)."""
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[k] = "1"
+
+
+def _helmholtz_cpu_worker(seconds):
+    """Oracle 2-D Helmholtz solves of the seeded 64 x 64 forcing for about
+    `seconds` in one process: (solves, elapsed seconds)."""
+    from jaxfun_b200.workloads import helmholtz2d_forcing
+    from oracle import kmm as ok
+
+    fh = helmholtz2d_forcing((64, 64), seed=1)
+    ok.helmholtz2d_solve(fh)  # warm
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        ok.helmholtz2d_solve(fh)
+        n += 1
+    return n, time.perf_counter() - t0
+
+
+def helmholtz_cpu_rate(threads, seconds=2.0):
+    """Throughput of the oracle's 2-D Helmholtz solve on all host cores: one
+    spawned process per core, each solving the same seeded problem for about
+    `seconds`; returns (microseconds per solve at that throughput, solves)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    with ProcessPoolExecutor(max_workers=threads, mp_context=mp.get_context("spawn"),
+                             initializer=_single_threaded_worker) as pool:
+        res = list(pool.map(_helmholtz_cpu_worker, [seconds] * threads))
+    rate = sum(n / t for n, t in res)
+    return 1e6 / rate, sum(n for n, _ in res)
+
+
 def max_over_ranks(value: float, device) -> float:
     """Max of a per-rank scalar over the process group (identity if none)."""
     import torch
@@ -587,6 +623,14 @@ def main(argv=None):
         ms_step = e0.elapsed_time(e1) / K
         launches = sum(m.info().launches_per_step for m in members)
         diags = [m.diagnostics(m._fetch_mhd(2.0)) for m in members[:3]]
+        # stage model of one MHD member step (FP64): (91 E_s + 36 E_m) x 16 B
+        step_bytes = 0
+        for m in members:
+            nx, ny, nz = m.N
+            H = nz // 2 + 1
+            step_bytes += (91 * nx * ny * H + 36 * nx * m.info().my * H) * 16
+        peak, peak_kind = measured_peak()
+        achieved = step_bytes / (ms_step * 1e-3) / 1e9
         return {
             "workload": f"{len(members)} MHD members, N cycling {sizes} x {grid[1]} x {grid[2]}, "
                         "Re = Rm = 1000, B0 = 0.1 e_z, u and b perturbation energies 1e-4",
@@ -597,6 +641,9 @@ def main(argv=None):
             "steps": K,
             "gpu_launches_per_step": launches,
             "launch": "one CUDA graph per ensemble step, one stream per member",
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
+                         "algorithmic_bytes_per_ensemble_step": step_bytes},
             "l2": "not flushed: the ensemble's state exceeds L2",
             "device_bytes": sum(m.info().device_bytes for m in members),
             "sample_diagnostics": [{k: d[k] for k in ("Epert", "Emag", "divB_L2")} for d in diags],
@@ -671,16 +718,12 @@ def main(argv=None):
             "u_max": float(u.abs().max()),
         }
         if not args.no_cpu_baseline:
-            from oracle import kmm as ok
-
-            fh = helmholtz2d_forcing(N, seed=1)
-            t0 = time.perf_counter()
-            n = 0
-            while time.perf_counter() - t0 < 2.0:
-                ok.helmholtz2d_solve(fh)
-                n += 1
-            out["cpu_baseline"] = {"us_per_solve": (time.perf_counter() - t0) * 1e6 / n,
-                                   "kind": "port", "cores": 1, "sample": f"{n} oracle solves"}
+            threads = host_threads()
+            us_cpu, n = helmholtz_cpu_rate(threads)
+            out["cpu_baseline"] = {
+                "us_per_solve": us_cpu, "kind": "port", "cores": threads,
+                "sample": f"{n} oracle solves, one single-threaded process per core for 2 s "
+                          "(throughput over all host cores)"}
         return out
 
     def sizes_block():
@@ -782,6 +825,7 @@ def main(argv=None):
         line["mixed_vs_fp64_rel_l2"] = err
     if adj is not None:
         line["adjoint"] = adj
+        line["adjoint_fd_max_rel_err"] = adj["fd_check"]["max_rel_err"]
     if ensb is not None:
         line["mhd_ensemble"] = ensb
     if helm is not None:

@@ -27,6 +27,7 @@ extern "C" {
 #define JFB_ERR_SINGULAR 3   /* zero or non-finite pivot (diamatrix.py:461)  */
 #define JFB_ERR_NONFINITE 4  /* non-finite value detected in the state       */
 #define JFB_ERR_STATE 5      /* call sequence error (e.g. no state set)      */
+#define JFB_ERR_DEVICE 6     /* a bounded device-side wait gave up           */
 
 /* ---- library ------------------------------------------------------------ */
 int jfb_version(void);
@@ -57,17 +58,20 @@ int jfb_banded_lu_factor(double* band, int64_t n_batch, int64_t p, int64_t q,
                          int64_t n, void* stream);
 
 /* Allocation-free variant of jfb_banded_lu_factor (no counterpart in the
- * reference).  For callers that cannot allocate device memory: code running
- * during CUDA stream capture, inside an XLA custom call or under another
- * framework's memory pool.  It factors the same batch in place with the same
+ * reference).  For callers that cannot allocate device memory: an XLA custom
+ * call or another framework's operator whose device memory belongs to that
+ * framework's allocator, or a process whose caching pool already holds all
+ * of the GPU's memory.  It factors the same batch in place with the same
  * arithmetic but keeps the per-matrix pivot status in a fixed device array of
  * the library (256 KiB per GPU, held until exit), so it calls no allocator.
  * n_batch must not exceed JFB_NOALLOC_LU_MAX_BATCH (else JFB_ERR_ARG).  On a
  * zero or non-finite pivot it returns JFB_ERR_SINGULAR and, if
  * first_singular is non-NULL, the lowest singular matrix index there (-1 when
- * none).  Synchronises `stream`.  The first call on a device looks up the
- * array's device address, so make it before any stream capture.  All calls
- * share the array: calls that overlap on the GPU (different streams or
+ * none).  Synchronises `stream` (it reads that index back to the host).  The
+ * first call on a device looks up the array's device address and keeps it
+ * for the life of the process, so make that call before any stream capture,
+ * and do not keep using the library on a device after cudaDeviceReset.  All
+ * calls share the array: calls that overlap on the GPU (different streams or
  * threads) race. */
 #define JFB_NOALLOC_LU_MAX_BATCH 65536
 int jfb_banded_lu_factor_noalloc(double* band, int64_t n_batch, int64_t p, int64_t q,
@@ -180,6 +184,18 @@ int jfb_kmm_state_from_physical(jfb_kmm_plan* plan, const double* u0,
  * fixed-order reduction. */
 int jfb_kmm_diagnostics(jfb_kmm_plan* plan, double* out, void* stream);
 
+/* The non-finite-state guard of the production runner
+ * (production/oracles.py:3257-3261, `_tree_all_finite(candidate_state)` ->
+ * FloatingPointError("nonfinite solver state ...")).  The step kernels set a
+ * bit of a device status word of the plan when a solved coefficient (u0, g,
+ * the mean flow, A) is NaN or infinite, the diagnostics when one of their
+ * values is, and the tensor-core pencil stage when its bounded wait for a
+ * bulk copy gave up.  This call synchronises `stream`, returns the word in
+ * *flags (may be NULL), clears it, and returns JFB_ERR_NONFINITE if a
+ * non-finite value was seen, JFB_ERR_DEVICE if a wait timed out, else
+ * JFB_OK.  Cheap enough to call after every advance. */
+int jfb_kmm_check(jfb_kmm_plan* plan, int32_t* flags, void* stream);
+
 /* Measurement entry point (no reference counterpart; the reference's
  * production/benchmark.py:282-354 times blocks of KMM.solve with host
  * clocks): advances `steps` steady steps with the same kernels as
@@ -283,15 +299,19 @@ int jfb_mhd_diagnostics(jfb_kmm_plan* plan, double* out, void* stream);
 
 /* ---- tensor-product spaces ------------------------------------------------ */
 
-#define JFB_BASIS_ORTHOGONAL 0  /* Chebyshev T_k                              */
-#define JFB_BASIS_DIRICHLET 1   /* T_k - T_{k+2} (Composite, u(+-1) = 0)      */
+#define JFB_BASIS_ORTHOGONAL 0  /* T_k / P_k of the family                   */
+#define JFB_BASIS_DIRICHLET 1   /* P_k - P_{k+2} (Composite, u(+-1) = 0)      */
 #define JFB_BASIS_BIHARMONIC 2  /* u(+-1) = u'(+-1) = 0 (Composite)           */
+#define JFB_FAMILY_LEGENDRE 1   /* family of a tensor-product space x axis    */
 
-/* TensorProduct(Chebyshev-family x axis, Fourier[, Fourier])
- * (src/jaxfun/galerkin/tensorproductspace.py:104-293): n[0] Gauss-Chebyshev
- * points on [x_lo, x_hi], n[1] (and n[2]) Fourier modes on periods l[0]
- * (l[1]), padding factors pad[] for the padded backward / forward
- * (get_dealiased: max(N, int(pad N)) points). */
+/* TensorProduct(orthogonal-family x axis, Fourier[, Fourier])
+ * (src/jaxfun/galerkin/tensorproductspace.py:104-293): n[0] Gauss points of
+ * the family (Gauss-Chebyshev, Chebyshev.py:159-180, or Gauss-Legendre,
+ * Legendre.py:136-147) on [x_lo, x_hi], n[1] (and n[2]) Fourier modes on
+ * periods l[0] (l[1]), padding factors pad[] for the padded backward /
+ * forward (get_dealiased: max(N, int(pad N)) points).  The wall-normal
+ * transforms are dense Vandermonde contractions (orthogonal.py:121-145,
+ * 240-331) with the Shen stencil folded in. */
 typedef struct jfb_tps_config {
   int32_t ndim;   /* 2: (x, y), 3: (x, y, z) */
   int32_t basis;  /* JFB_BASIS_*             */
@@ -299,6 +319,7 @@ typedef struct jfb_tps_config {
   double x_lo, x_hi;
   double l[2];
   double pad[2];
+  int32_t family; /* JFB_FAMILY_CHEBYSHEV or JFB_FAMILY_LEGENDRE */
 } jfb_tps_config;
 
 typedef struct jfb_tps jfb_tps;
@@ -322,6 +343,38 @@ int jfb_tps_forward(jfb_tps* tps, const void* phys, void* coeffs, int padded, in
 /* Galerkin x-matrix (phi_i, phi_j^(order))_w, order 0 or 2, dense row-major
  * nb x nb on the host (the 1-D mass / stiffness of inner.py, domain-scaled). */
 int jfb_tps_galerkin(const jfb_tps* tps, int order, double* out);
+
+/* TensorProductSpace.backward_primitive(c, k) (tensorproductspace.py:553-594):
+ * the mixed derivative d^k0/dx^k0 d^k1/dy^k1 [d^k2/dz^k2] of the field on the
+ * (padded) mesh; coeffs (nb, n1[, n2]) -> phys as jfb_tps_backward.  Along x
+ * the derivative is taken on the orthogonal coefficients (chebder / legder,
+ * domain-scaled); along Fourier axes (i m df)^k with the Nyquist mode zeroed
+ * for odd k (Fourier.py:210-223).  k: ndim non-negative orders. */
+int jfb_tps_backward_primitive(jfb_tps* tps, const void* coeffs, void* phys, const int32_t* k,
+                               int padded, void* stream);
+
+/* TensorProductSpace.to_orthogonal (tensorproductspace.py:596-616):
+ * coeffs (nb, n1[, n2]) -> orthogonal coefficients (N, n1[, n2]) (c @ S). */
+int jfb_tps_to_orthogonal(jfb_tps* tps, const void* coeffs, void* orth, void* stream);
+
+/* TensorProductSpace.differentiate_orthogonal_coeffs(c, k)
+ * (tensorproductspace.py:638-682): orthogonal coefficients (N, n1[, n2]) ->
+ * the coefficients of the k-th mixed derivative, same shape. */
+int jfb_tps_differentiate_orthogonal(jfb_tps* tps, const void* orth, void* out, const int32_t* k,
+                                     void* stream);
+
+/* TensorProductSpace.project_from_orthogonal (tensorproductspace.py:706-728;
+ * composite.py:292-298 per axis): Galerkin projection of orthogonal
+ * coefficients (N, n1[, n2]) into this space (nb, n1[, n2]): mass-weight,
+ * stencil, mass solve; Fourier axes are identities. */
+int jfb_tps_project_from_orthogonal(jfb_tps* tps, const void* orth, void* coeffs, void* stream);
+
+/* TensorProductSpace.scalar_product_from_orthogonal (tensorproductspace.py:
+ * 730-754; composite.py:300-305): scalar products of the field given by
+ * orthogonal coefficients (N, n1[, n2]) -> (nb, n1[, n2]); Fourier axes
+ * multiply by their mass 2 pi / df. */
+int jfb_tps_scalar_product_from_orthogonal(jfb_tps* tps, const void* orth, void* out,
+                                           void* stream);
 
 /* The 2-D Helmholtz solve -lap u + alpha u = f of la/solvers.py:22-61 as one
  * launch: orthogonal-Chebyshev x Fourier coefficients f_hat (N, n1) ->

@@ -12,7 +12,9 @@ import os
 from ctypes import POINTER, c_double, c_int, c_int32, c_int64, c_void_p
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libjfb200.so")
+# JFB200_LIB may name another in-tree build of the same library (the
+# phase-stamp build, libjfb200_stamps.so, for profiling).
+LIB_PATH = os.environ.get("JFB200_LIB") or os.path.join(_HERE, "libjfb200.so")
 
 JFB_OK = 0
 JFB_ERR_ARG = 1
@@ -20,6 +22,7 @@ JFB_ERR_CUDA = 2
 JFB_ERR_SINGULAR = 3
 JFB_ERR_NONFINITE = 4
 JFB_ERR_STATE = 5
+JFB_ERR_DEVICE = 6
 
 JFB_FAMILY_CHEBYSHEV = 0
 JFB_PRECISION_FP64 = 0
@@ -28,6 +31,7 @@ JFB_NONLINEAR_ROTATIONAL = 0
 JFB_BASIS_ORTHOGONAL = 0
 JFB_BASIS_DIRICHLET = 1
 JFB_BASIS_BIHARMONIC = 2
+JFB_FAMILY_LEGENDRE = 1
 
 
 class KMMConfig(ctypes.Structure):
@@ -102,6 +106,7 @@ class TPSConfig(ctypes.Structure):
         ("x_hi", c_double),
         ("l", c_double * 2),
         ("pad", c_double * 2),
+        ("family", c_int32),
     ]
 
 
@@ -147,6 +152,7 @@ SIGNATURES = {
         c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
     ),
     "jfb_kmm_diagnostics": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "jfb_kmm_check": (c_int, [c_void_p, POINTER(c_int32), c_void_p]),
     "jfb_kmm_timed_steps": (
         c_int,
         [c_void_p, c_int64, c_void_p, c_int64, POINTER(c_double), POINTER(c_double), c_void_p],
@@ -166,6 +172,17 @@ SIGNATURES = {
     "jfb_tps_backward": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "jfb_tps_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]),
     "jfb_tps_galerkin": (c_int, [c_void_p, c_int, POINTER(c_double)]),
+    "jfb_tps_backward_primitive": (
+        c_int, [c_void_p, c_void_p, c_void_p, POINTER(c_int32), c_int, c_void_p]
+    ),
+    "jfb_tps_to_orthogonal": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "jfb_tps_differentiate_orthogonal": (
+        c_int, [c_void_p, c_void_p, c_void_p, POINTER(c_int32), c_void_p]
+    ),
+    "jfb_tps_project_from_orthogonal": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "jfb_tps_scalar_product_from_orthogonal": (
+        c_int, [c_void_p, c_void_p, c_void_p, c_void_p]
+    ),
     "jfb_helmholtz2d_solve": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
                                        c_void_p, c_void_p, c_int64, c_void_p, c_double,
                                        c_void_p, c_void_p, c_void_p]),
@@ -213,10 +230,19 @@ class JFBError(RuntimeError):
         self.status = status
 
 
+class NonFiniteStateError(JFBError, FloatingPointError):
+    """JFB_ERR_NONFINITE: the state holds NaN or infinite values.  A
+    ``FloatingPointError``, as the reference's runner raises for a non-finite
+    solver state (production/oracles.py:3257-3261)."""
+
+
 def check(status: int) -> None:
     if status != JFB_OK:
         msg = load().jfb_last_error()
-        raise JFBError(status, msg.decode() if msg else "")
+        text = msg.decode() if msg else ""
+        if status == JFB_ERR_NONFINITE:
+            raise NonFiniteStateError(status, text)
+        raise JFBError(status, text)
 
 
 def call(name: str, *args) -> None:

@@ -28,24 +28,35 @@ def nvcc() -> str:
     return path
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile the CUDA sources into ``libjfb200.so`` if any source is newer."""
+STAMPS_OUT = os.path.join(HERE, "libjfb200_stamps.so")
+
+
+def build(force: bool = False, verbose: bool = False, stamps: bool = False) -> str:
+    """Compile the CUDA sources into ``libjfb200.so`` if any source is newer.
+
+    ``stamps=True`` builds ``libjfb200_stamps.so`` instead: the same library
+    with -DJFB_PHASE_STAMPS, whose step kernels record global-timer stamps
+    at their phase boundaries (``jfb_debug_read_stamps``; load it with
+    JFB200_LIB pointing at it).  For profiling only."""
+    out = STAMPS_OUT if stamps else OUT
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [
         os.path.join(CSRC, f)
         for f in os.listdir(CSRC)
         if f.endswith((".cuh", ".h"))
     ] + [os.path.join(HERE, "..", "include", "jfb200.h")]
-    if not force and os.path.exists(OUT):
-        out_mtime = os.path.getmtime(OUT)
+    if not force and os.path.exists(out):
+        out_mtime = os.path.getmtime(out)
         if all(os.path.getmtime(d) <= out_mtime for d in deps):
-            return OUT
-    cmd = [nvcc(), *FLAGS, "-o", OUT, *srcs]
+            return out
+    cmd = [nvcc(), *FLAGS, *(["-DJFB_PHASE_STAMPS"] if stamps else []), "-o", out, *srcs]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
-    return OUT
+    return out
 
 
 if __name__ == "__main__":
-    build(force=True, verbose=True)
+    import sys
+
+    build(force=True, verbose=True, stamps="--stamps" in sys.argv)

@@ -86,4 +86,43 @@ using c32 = cpx<float>;
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
+// Programmatic dependent launch: let the next kernel on the stream begin its
+// prologue (pdl_trigger), and wait until the previous kernel's results are
+// complete and visible (pdl_wait; returns at once for a plain launch).
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Phase stamps (off by default; built into libjfb200_stamps.so by
+// jaxfun_b200.build with stamps=True): thread 0 of every CTA writes the
+// global timer at the phase boundaries of the step kernels into
+// g_jfb_stamps[kernel][cta][phase]; jfb_debug_read_stamps copies them out.
+constexpr int kStampCTAs = 1024, kStampPhases = 16;
+#ifdef JFB_PHASE_STAMPS
+static __device__ unsigned long long g_jfb_stamps[4 * kStampCTAs * kStampPhases];
+#define JFB_STAMP(kernel, phase)                                                        \
+  do {                                                                                  \
+    if (threadIdx.x == 0 && blockIdx.x < kStampCTAs) {                                  \
+      unsigned long long t_;                                                            \
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_));                           \
+      g_jfb_stamps[((size_t)(kernel) * kStampCTAs + blockIdx.x) * kStampPhases + (phase)] = t_; \
+    }                                                                                   \
+  } while (0)
+#else
+#define JFB_STAMP(kernel, phase) \
+  do {                           \
+  } while (0)
+#endif
+
+// Bits of a plan's device status word (read and cleared by jfb_kmm_check).
+constexpr int kStatusWaitTimeout = 1;  // a bounded device-side wait gave up
+constexpr int kStatusNonFinite = 2;    // a solved coefficient was NaN or infinite
+
+__device__ __forceinline__ bool finite_c(c64 v) { return isfinite(v.re) && isfinite(v.im); }
+// Records a non-finite value seen by this thread (one atomic, only when set).
+__device__ __forceinline__ void flag_nonfinite(int* status, bool bad) {
+  if (bad && status) atomicOr(status, kStatusNonFinite);
+}
+
 }  // namespace jfb

@@ -8,7 +8,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "jfb_common.cuh"
@@ -18,6 +20,17 @@
 #include "jfb_kmm_gemm.cuh"
 #include "jfb_kmm_mhd.cuh"
 #include "jfb_kmm_adjoint.cuh"
+
+#ifdef JFB_PHASE_STAMPS
+// Copies the phase stamps (kernel 0: pencil_gemm_kernel, 1: plane_cross_kernel;
+// [kernel][cta][phase] global-timer nanoseconds) to host memory.
+extern "C" int jfb_debug_read_stamps(unsigned long long* host, int64_t count) {
+  JFB_REQUIRE(host && count > 0 && count <= 4 * jfb::kStampCTAs * jfb::kStampPhases,
+              "bad stamp buffer");
+  JFB_CHECK_CUDA(cudaMemcpyFromSymbol(host, jfb::g_jfb_stamps, (size_t)count * sizeof(*host)));
+  return JFB_OK;
+}
+#endif
 
 namespace jfb {
 
@@ -215,6 +228,7 @@ struct jfb_kmm_plan {
   size_t smem_pencil = 0, smem_y = 0, smem_z = 0;
   std::vector<void*> allocs;
   int64_t device_bytes = 0;
+  int* status = nullptr;  // device status word (kStatus* bits), read by jfb_kmm_check
   jfb::FactorSet steady, startup[3];
   jfb::c64 *U0[3], *G[3], *NU[3], *NG[3], *VW[3], *NVW[3];
   jfb::c64 *NUst, *NGst, *NVWst;
@@ -240,6 +254,7 @@ struct jfb_kmm_plan {
   cudaStream_t cap = nullptr;  // private stream used only to capture the graphs
   cudaEvent_t* timing_events = nullptr;  // set by jfb_kmm_timed_steps
   bool gemm = false;       // tensor-core pencil stage (pencil_gemm_kernel)
+  bool pdl = true;         // programmatic dependent launch of the step kernels
   bool plane = false;      // fused periodic-axis transforms (plane_cross_kernel)
   size_t smem_plane = 0;
   jfb::GemmOps gops;
@@ -277,6 +292,27 @@ static cudaError_t allow_smem(const void* fn) {
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              optin - (int)fa.sharedSizeBytes);
   return e;
+}
+
+// Launch with programmatic dependent launch (PDL) when `pdl`: the kernel may
+// start while its predecessor on the stream finishes; it runs its read-only
+// prologue, then waits in griddepcontrol.wait for the predecessor's results
+// (kernels launched this way call pdl_wait() before their first global read
+// of a produced array and their first global write).
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_ex(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block,
+                             size_t smem, cudaStream_t s, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl ? attr : nullptr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 static int dalloc(jfb_kmm_plan* pl, void** ptr, size_t bytes) {
@@ -476,8 +512,10 @@ static StageArgs blank_args() {
   return a;
 }
 
-static int launch_pencil(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s) {
+static int launch_pencil(jfb_kmm_plan* pl, const StageArgs& a0, cudaStream_t s) {
   const int blocks = pl->d.Ny * pl->d.nKb;
+  StageArgs a = a0;
+  a.status = pl->status;
   if (pl->d.nD <= 64)
     pencil_stage_kernel<1><<<blocks, kNW * 32, pl->smem_pencil, s>>>(pl->ops, pl->d, a);
   else
@@ -535,8 +573,8 @@ static int launch_implicit(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s)
   g.x32 = pl->mixed ? 1 : 0;
   g.Xlin = pl->mixed ? reinterpret_cast<const c32*>(pl->X) : nullptr;
   const int blocks = (pl->d.Ny / 2) * ceil_div(pl->d.Kz, 8);
-  pencil_gemm_kernel<<<blocks, kGThreads, pl->smem_gemm, s>>>(pl->d, pl->ops, pl->gops, g);
-  JFB_CHECK_LAUNCH();
+  JFB_CHECK_CUDA(launch_ex(pl->pdl, pencil_gemm_kernel, dim3(blocks), dim3(kGThreads),
+                           pl->smem_gemm, s, pl->d, pl->ops, pl->gops, g));
   return JFB_OK;
 }
 
@@ -625,10 +663,11 @@ static void launch_zfwd_warp(jfb_kmm_plan* pl, const double* u0, const double* u
 }
 
 template <int PY, int PZ, typename T>
-static void launch_plane(jfb_kmm_plan* pl, cudaStream_t s) {
-  plane_cross_kernel<PY, PZ, 1, T><<<2 * pl->d.Nx, kPlaneThreads,
-                                     plane_smem_bytes(pl->d.My, pl->d.Kz, sizeof(cpx<T>)), s>>>(
-      pl->ops, tdims<T>(pl), Tx<T>::twy(pl), Tx<T>::twz(pl), buf<T>(pl->X), buf<T>(pl->HX));
+static cudaError_t launch_plane(jfb_kmm_plan* pl, cudaStream_t s) {
+  return launch_ex(pl->pdl, plane_cross_kernel<PY, PZ, 1, T>, dim3(2 * pl->d.Nx),
+                   dim3(kPlaneThreads), plane_smem_bytes(pl->d.My, pl->d.Kz, sizeof(cpx<T>)),
+                   s, pl->ops, tdims<T>(pl), Tx<T>::twy(pl), Tx<T>::twz(pl),
+                   (const cpx<T>*)buf<T>(pl->X), buf<T>(pl->HX));
 }
 
 // y_backward -> z_cross -> y_forward: HX <- H(state whose x-physical fields are in X)
@@ -637,11 +676,10 @@ static int launch_transforms_t(jfb_kmm_plan* pl, cudaStream_t s) {
   const Dims d = tdims<T>(pl);
   if (pl->plane) {
     const int key = pl->py * 10 + pl->pz;
-    if (key == 22) launch_plane<2, 2, T>(pl, s);
-    else if (key == 23) launch_plane<2, 3, T>(pl, s);
-    else if (key == 32) launch_plane<3, 2, T>(pl, s);
-    else launch_plane<3, 3, T>(pl, s);
-    JFB_CHECK_LAUNCH();
+    if (key == 22) JFB_CHECK_CUDA((launch_plane<2, 2, T>(pl, s)));
+    else if (key == 23) JFB_CHECK_CUDA((launch_plane<2, 3, T>(pl, s)));
+    else if (key == 32) JFB_CHECK_CUDA((launch_plane<3, 2, T>(pl, s)));
+    else JFB_CHECK_CUDA((launch_plane<3, 3, T>(pl, s)));
     if (pl->timing_events)
       for (int k = 2; k <= 4; ++k) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[k], s));
     return JFB_OK;
@@ -723,8 +761,10 @@ static MhdArgs blank_mhd() {
   return a;
 }
 
-static int launch_mhd(jfb_kmm_plan* pl, const MhdArgs& a, cudaStream_t s) {
+static int launch_mhd(jfb_kmm_plan* pl, const MhdArgs& a0, cudaStream_t s) {
   const int blocks = (pl->d.Ny / 2) * ceil_div(pl->d.Kz, 8);
+  MhdArgs a = a0;
+  a.status = pl->status;
   mhd_a_kernel<<<blocks, kMhdThreads, pl->smem_mhd, s>>>(pl->d, pl->ops, pl->mops, a);
   JFB_CHECK_LAUNCH();
   return JFB_OK;
@@ -994,6 +1034,11 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
     set_error("padding must not truncate");
     return fail(JFB_ERR_ARG);
   }
+  if ((st = dalloc(pl, (void**)&pl->status, sizeof(int)))) return fail(st);
+  {
+    const char* env = std::getenv("JFB200_PDL");
+    pl->pdl = !(env && std::string(env) == "0");
+  }
   // kz column chunk of the y transforms: two My x KC complex buffers <= 100 KB
   pl->KC = d.Kz;
   while ((size_t)2 * d.My * pl->KC * sizeof(c64) > 100 * 1024 && pl->KC % 2 == 0) pl->KC /= 2;
@@ -1202,19 +1247,18 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
       for (int r = 0; r < kReplicas; ++r)
         std::copy(gh.frag.begin(), gh.frag.end(), rep.begin() + (size_t)r * gh.frag.size());
       double *fr, *r3, *x2, *md;
-      int *kr, *stw;
+      int* kr;
       if ((st = upload(pl, &fr, rep))) return fail(st);
       if ((st = upload(pl, &kr, gh.krange))) return fail(st);
       if ((st = upload(pl, &r3, gh.R3))) return fail(st);
       if ((st = upload(pl, &x2, gh.X2D))) return fail(st);
       if ((st = upload(pl, &md, gh.mid))) return fail(st);
-      if ((st = dalloc(pl, (void**)&stw, sizeof(int)))) return fail(st);
       G.frag = fr;
       G.krange = kr;
       G.R3 = r3;
       G.X2D = x2;
       G.mid = md;
-      G.status = stw;
+      G.status = pl->status;
       G.mid_stride = gh.mid_stride;
       G.nfrag = (int)gh.frag.size();
       G.nrep = kReplicas;
@@ -1597,8 +1641,27 @@ extern "C" int jfb_kmm_diagnostics(jfb_kmm_plan* pl, double* out, void* stream) 
   JFB_CHECK_LAUNCH();
   diag_finish_kernel<<<1, 32, 0, s>>>(d, pl->diag_partial, pl->diag_blocks, pl->diag_mean,
                                       pl->cfg.ly, pl->cfg.lz, pl->cfg.x_lo, pl->cfg.x_hi,
-                                      out);
+                                      out, pl->status);
   JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_check(jfb_kmm_plan* pl, int32_t* flags, void* stream) {
+  JFB_REQUIRE(pl, "null pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  int word = 0;
+  JFB_CHECK_CUDA(cudaMemcpyAsync(&word, pl->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  JFB_CHECK_CUDA(cudaStreamSynchronize(s));
+  JFB_CHECK_CUDA(cudaMemsetAsync(pl->status, 0, sizeof(int), s));
+  if (flags) *flags = word;
+  if (word & kStatusNonFinite) {
+    set_error("nonfinite solver state: a solved coefficient or diagnostic was NaN or infinite");
+    return JFB_ERR_NONFINITE;
+  }
+  if (word & kStatusWaitTimeout) {
+    set_error("a bounded device-side wait timed out; the step's results are invalid");
+    return JFB_ERR_DEVICE;
+  }
   return JFB_OK;
 }
 
@@ -1782,7 +1845,7 @@ extern "C" int jfb_mhd_diagnostics(jfb_kmm_plan* pl, double* out, void* stream) 
                                                        pl->mdiag_partial);
   JFB_CHECK_LAUNCH();
   mhd_diag_finish_kernel<<<1, 32, 0, s>>>(pl->mdiag_partial, pl->diag_blocks, pl->cfg.ly,
-                                          pl->cfg.lz, out + 8);
+                                          pl->cfg.lz, out + 8, pl->status);
   JFB_CHECK_LAUNCH();
   return JFB_OK;
 }

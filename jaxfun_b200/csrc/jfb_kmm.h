@@ -77,6 +77,33 @@ struct TpsX {
 };
 void build_tps_x_operators(const HostOperators& op, int basis, TpsX& t);
 
+// 1-D data of the wall-normal basis of a standalone tensor-product space,
+// in long double, row-major: V[j][n] = P_n(X_j) on the family's Gauss nodes,
+// Q[n][j] = P_n(X_j) w_j / df (scalar products), ns[n] = (P_n, P_n) / df,
+// D[i][j] the coefficients of d/dX (P_j)' = sum_i D[i][j] P_i, and the Shen
+// stencil S (nb x N; the identity for the orthogonal basis).
+// family: 0 Chebyshev (Chebyshev.py), 1 Legendre (Legendre.py);
+// basis: 0 orthogonal, 1 Dirichlet, 2 biharmonic (composite.py:797-864).
+struct XBasis {
+  int family = 0, basis = 0, N = 0, nb = 0;
+  double dfx = 1.0;
+  std::vector<long double> X, V, Q, ns, D, S;
+};
+void build_x_basis(int family, int basis, int N, double x_lo, double x_hi, XBasis& xb);
+
+// Separable x-axis maps of a standalone space (row-major double matrices).
+enum XMap {
+  kXBackward = 0,      // V D^k S^T df^k            (N x nb)  backward_primitive
+  kXToOrth = 1,        // S^T                       (N x nb)  to_orthogonal
+  kXDiffOrth = 2,      // D^k df^k                  (N x N)   differentiate_orthogonal_coeffs
+  kXProjectOrth = 3,   // M^-1 S diag(ns)           (nb x N)  project_from_orthogonal
+  kXSpFromOrth = 4,    // S diag(ns)                (nb x N)  scalar_product_from_orthogonal
+  kXForward = 5,       // M^-1 S Q                  (nb x N)  forward (L2 projection)
+  kXScalarProd = 6,    // S Q                       (nb x N)  scalar_product
+  kXGalerkin = 7,      // S diag(ns) D^k S^T df^k   (nb x nb) (phi_i, phi_j^(k))_w
+};
+std::vector<double> x_map_matrix(const XBasis& xb, int map, int k, int* rows, int* cols);
+
 Stencil make_stencil(int N, bool biharmonic);
 // Builds GemmHost from the 1-D operators; returns false (with a message) if a
 // parity property the split relies on does not hold.

@@ -157,15 +157,15 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 // Wait for phase `parity` of `bar` for at most ~2^27 cycles (tens of ms).
-// On time-out the status word gets `code`, the wait is repeated once with
-// the same limit (the copy in flight targets this CTA's shared memory), and
-// false is returned.
+// On time-out the status word gets the bit `code`, the wait is repeated once
+// with the same limit (the copy in flight targets this CTA's shared memory),
+// and false is returned.
 __device__ __noinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* status, int code) {
   for (int round = 0; round < 2; ++round) {
     const long long t0 = clock64();
     while (clock64() - t0 < (1ll << 27))
       if (mbar_try(bar, parity)) return round == 0;
-    if (round == 0 && status) atomicExch(status, code);
+    if (round == 0 && status) atomicOr(status, code);
   }
   return false;
 }
@@ -341,6 +341,7 @@ __device__ void mean_flow(const Dims& d, const DevOps& o, const GemmOps& G,
     const c64 xv = x0 + x1;
     vwx[i] = xv;
     a.vw_out[i] = xv;
+    flag_nonfinite(G.status, !finite_c(xv));
   }
 }
 
@@ -362,6 +363,8 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
   c64* rowc = reinterpret_cast<c64*>(sm);  // row r, pencil w: rowc[r * LC + w]
   const int LC = kGLd / 2;
   const double sl = a.slin;
+  JFB_STAMP(0, 0);
+  pdl_trigger();
 
   if (tid < kGW) {
     const int side = tid >> 3, kz = kz0 + (tid & 7);
@@ -398,6 +401,10 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     if (sl != 0.0) prefetch_l2(G.X2D, (size_t)d.nD * d.nD * sizeof(double));
   }
   __syncthreads();
+  // everything above reads only constant operators and factor records; the
+  // arrays below are produced (HX) or still read (X) by the previous kernel
+  pdl_wait();
+  JFB_STAMP(0, 1);
 
   // ------------------------------------------------------------------ A --
   // 16-byte asynchronous copies of this tile's values straight into the
@@ -470,6 +477,7 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     cp_async_wait_all();
   }
   __syncthreads();
+  JFB_STAMP(0, 2);
 
   // in-place transform: mirror sums / differences, (i ky, i kz, k^2) weights
   double* mean = sm + G.oMean;  // mean-flow scratch
@@ -578,6 +586,7 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
       for (int e = tid; e < pads[q][1] * kGLd; e += kGThreads) sm[pads[q][0] * kGLd + e] = 0.0;
   }
   __syncthreads();
+  JFB_STAMP(0, 3);
 
   // ------------------------------------------------------------------ B --
   {
@@ -644,6 +653,7 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     }
   }
   __syncthreads();
+  JFB_STAMP(0, 4);
 
   // ------------------------------------------------------------------ C --
   // stage the velocity operators (tail of the operator copy) into dead rows
@@ -680,6 +690,7 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
       for (int e = t2; e < pads[q][1] * kGLd; e += n2) sm[pads[q][0] * kGLd + e] = 0.0;
   }
   __syncthreads();
+  JFB_STAMP(0, 5);
   // C2: x = U^-1 y for both pencils of a wavenumber; one warp per (pair,
   // system, parity), lane = row
   for (int task = warp; task < 4 * (kGW / 2); task += kGWarps) {
@@ -711,14 +722,25 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     }
   }
   __syncthreads();
+  JFB_STAMP(0, 6);
   // C3: solved coefficients to global memory (coalesced along pencils)
-  for (int idx = tid; idx < d.nD * kGW; idx += kGThreads) {
-    const int i = idx / kGW, w = idx % kGW;
-    const int p = s_p[w];
-    if (p < 0) continue;
-    const int par = i & 1, m = i >> 1;
-    if (i < d.nB) a.u0_out[(size_t)i * P + p] = rowc[((par ? G.oUO : G.oUE) + m) * LC + w];
-    a.g_out[(size_t)i * P + p] = rowc[((par ? G.oGO : G.oGE) + m) * LC + w];
+  {
+    bool bad = false;
+    for (int idx = tid; idx < d.nD * kGW; idx += kGThreads) {
+      const int i = idx / kGW, w = idx % kGW;
+      const int p = s_p[w];
+      if (p < 0) continue;
+      const int par = i & 1, m = i >> 1;
+      if (i < d.nB) {
+        const c64 v = rowc[((par ? G.oUO : G.oUE) + m) * LC + w];
+        bad |= !finite_c(v);
+        a.u0_out[(size_t)i * P + p] = v;
+      }
+      const c64 v = rowc[((par ? G.oGO : G.oGE) + m) * LC + w];
+      bad |= !finite_c(v);
+      a.g_out[(size_t)i * P + p] = v;
+    }
+    flag_nonfinite(G.status, bad);
   }
   if (mean_cta) {
     // the mean flow (v + i w) replaces g in the velocity operand of pencil 0
@@ -726,11 +748,14 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     for (int i = tid; i < d.nD; i += kGThreads)
       rowc[(((i & 1) ? G.oGO : G.oGE) + (i >> 1)) * LC + 0] = m_x[i];
   }
-  mbar_wait_bounded(&s_bar, 0, G.status, 2);
-  __syncthreads();
+  const bool staged = mbar_wait_bounded(&s_bar, 0, G.status, kStatusWaitTimeout);
+  // a timed-out copy leaves the velocity operators incomplete: skip D (the
+  // status word makes the host call fail)
+  const bool skip_d = __syncthreads_or(!staged);
+  JFB_STAMP(0, 7);
 
   // ------------------------------------------------------------------ D --
-  {
+  if (!skip_d) {
     const int MTv = G.sub[gA0Ee].mt;
     const double* vs = sm + (size_t)G.oVel * kGLd - G.sub[gA0Ee].off + lane;
     for (int task = warp; task < 4 * MTv; task += kGWarps) {
@@ -799,7 +824,8 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
       }
     }
   }
-  if (Jh > Jl) {
+  JFB_STAMP(0, 8);
+  if (Jh > Jl && !skip_d) {
     // middle Gauss node (odd N): symmetric halves only, one dot product per
     // (operator, pencil, re/im) thread
     double* md = sm + G.oMid;
@@ -826,6 +852,7 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
       }
     }
   }
+  JFB_STAMP(0, 9);
 }
 
 }  // namespace jfb

@@ -84,6 +84,7 @@ struct StageArgs {
   c64 *u1_out, *u2_out;        // kFromPhys: tangential velocity (nD x P)
   int x32;  // HX (read, step modes) and X (written by the x-backward) hold complex64
   const c32* Xlin;  // mixed form: u, omega of HX's state; FP64 base-flow terms added here
+  int* status;      // plan status word: kStatusNonFinite when a solved value is not finite
 };
 
 __host__ __device__ inline int packed_rec_size(int n) {
@@ -986,8 +987,16 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
         for (int i = lane; i < d.nD; i += 32) a.vw_out[i] = sVW[i];
         __syncwarp();
       }
-      for (int i = lane; i < d.nB; i += 32) a.u0_out[(size_t)i * P + p] = A3[i];
-      for (int i = lane; i < d.nD; i += 32) a.g_out[(size_t)i * P + p] = A4[i];
+      bool bad = false;
+      for (int i = lane; i < d.nB; i += 32) {
+        bad |= !finite_c(A3[i]);
+        a.u0_out[(size_t)i * P + p] = A3[i];
+      }
+      for (int i = lane; i < d.nD; i += 32) {
+        bad |= !finite_c(A4[i]);
+        a.g_out[(size_t)i * P + p] = A4[i];
+      }
+      flag_nonfinite(a.status, bad);
 
       reconstruct_warp(o, d, A3, A4, sVW, mean_pencil, kyp, kzp, A0, A1, A2, A5, lane);
     }
@@ -1393,7 +1402,8 @@ __global__ void __launch_bounds__(256) diag_kernel(DevOps o, Dims d, const c64* 
 // out = (Epert, Etot, divL2, u_top, u_bot, wall_shear_top, wall_shear_bot, mean_shear)
 __global__ void diag_finish_kernel(Dims d, const double* __restrict__ partial, int nblocks,
                                    const double* __restrict__ meanterms, double ly, double lz,
-                                   double x_lo, double x_hi, double* __restrict__ out) {
+                                   double x_lo, double x_hi, double* __restrict__ out,
+                                   int* status) {
   const double lx = x_hi - x_lo;
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double eu = 0.0, ed = 0.0, base = 0.0;
@@ -1411,6 +1421,9 @@ __global__ void diag_finish_kernel(Dims d, const double* __restrict__ partial, i
   out[5] = meanterms[2] + d.uwall;
   out[6] = meanterms[3] + d.uwall;
   out[7] = (area * meanterms[4] + d.uwall * lx * area) / (lx * area);
+  bool bad = false;
+  for (int k = 0; k < 8; ++k) bad |= !isfinite(out[k]);
+  flag_nonfinite(status, bad);
 }
 
 }  // namespace jfb

@@ -67,6 +67,7 @@ struct MhdArgs {
   int sa_rec;
   c64* A_out;
   c64* XB;  // b, j at the x nodes: 6 x [Nx][P] (null: not wanted)
+  int* status;  // plan status word (kStatusNonFinite)
 };
 
 constexpr int kMhdThreads = 512;
@@ -238,11 +239,16 @@ __global__ void __launch_bounds__(kMhdThreads, 1) mhd_a_kernel(Dims d, DevOps o,
       }
     }
     __syncthreads();
+    bool bad = false;
     for (int e = tid; e < 3 * nD * kMhdW; e += kMhdThreads) {
       const int w = e % kMhdW, i = (e / kMhdW) % nD, c = e / (kMhdW * nD);
-      if (s_p[w] >= 0)
-        a.A_out[((size_t)c * nD + i) * P + s_p[w]] = SOL[((size_t)c * nD + srow(i)) * kMhdW + w];
+      if (s_p[w] >= 0) {
+        const c64 v = SOL[((size_t)c * nD + srow(i)) * kMhdW + w];
+        bad |= !finite_c(v);
+        a.A_out[((size_t)c * nD + i) * P + s_p[w]] = v;
+      }
     }
+    flag_nonfinite(a.status, bad);
   } else {
     for (int e = tid; e < 3 * nD * kMhdW; e += kMhdThreads) {
       const int w = e % kMhdW, i = (e / kMhdW) % nD, c = e / (kMhdW * nD);
@@ -467,7 +473,8 @@ __global__ void __launch_bounds__(256) mhd_diag_kernel(DevOps o, Dims d, MhdOps 
 
 // out[0] = divB_L2, out[1] = Emag (fixed-order reduction)
 __global__ void mhd_diag_finish_kernel(const double* __restrict__ partial, int nblocks,
-                                       double ly, double lz, double* __restrict__ out) {
+                                       double ly, double lz, double* __restrict__ out,
+                                       int* status) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double eb = 0.0, ed = 0.0;
   for (int b = 0; b < nblocks; ++b) {
@@ -476,6 +483,7 @@ __global__ void mhd_diag_finish_kernel(const double* __restrict__ partial, int n
   }
   out[0] = sqrt(ly * lz * ed);
   out[1] = ly * lz * eb;
+  flag_nonfinite(status, !isfinite(out[0]) || !isfinite(out[1]));
 }
 
 }  // namespace jfb

@@ -524,6 +524,147 @@ bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& er
 }
 
 
+// ---------------------------------------------------------------------------
+// Standalone wall-normal bases (Chebyshev and Legendre) and their separable
+// maps, for the tensor-product space entry points.
+// ---------------------------------------------------------------------------
+
+// Gauss-Legendre nodes (ascending) and weights in long double: Newton on P_N
+// from the Chebyshev-like first guess, w = 2 / ((1 - x^2) P_N'(x)^2)
+// (the nodes numpy's leggauss returns, Legendre.py:136-147).
+static void gauss_legendre(int N, std::vector<LD>& x, std::vector<LD>& w) {
+  x.assign(N, 0.0L);
+  w.assign(N, 0.0L);
+  const LD pi = 3.141592653589793238462643383279502884L;
+  for (int i = 0; i < N; ++i) {
+    LD z = std::cos(pi * ((LD)i + 0.75L) / ((LD)N + 0.5L));
+    LD dp = 1.0L;
+    for (int it = 0; it < 100; ++it) {
+      LD p0 = 1.0L, p1 = z;
+      for (int n = 2; n <= N; ++n) {
+        const LD p2 = ((2 * n - 1) * z * p1 - (n - 1) * p0) / n;
+        p0 = p1;
+        p1 = p2;
+      }
+      const LD pN = (N == 1) ? z : p1, pNm1 = (N == 1) ? 1.0L : p0;
+      dp = N * (z * pN - pNm1) / (z * z - 1.0L);
+      const LD dz = pN / dp;
+      z -= dz;
+      if (std::fabs((double)dz) < 1e-19) break;
+    }
+    // recompute the derivative at the converged node for the weight
+    LD p0 = 1.0L, p1 = z;
+    for (int n = 2; n <= N; ++n) {
+      const LD p2 = ((2 * n - 1) * z * p1 - (n - 1) * p0) / n;
+      p0 = p1;
+      p1 = p2;
+    }
+    dp = N * (z * p1 - p0) / (z * z - 1.0L);
+    x[N - 1 - i] = z;  // the guesses run from +1 down to -1
+    w[N - 1 - i] = 2.0L / ((1.0L - z * z) * dp * dp);
+  }
+}
+
+void build_x_basis(int family, int basis, int N, double x_lo, double x_hi, XBasis& xb) {
+  xb.family = family;
+  xb.basis = basis;
+  xb.N = N;
+  xb.nb = basis == 0 ? N : basis == 1 ? N - 2 : N - 4;
+  const double Lx = x_hi - x_lo;
+  xb.dfx = std::fabs(Lx - 2.0) < 1e-12 ? 1.0 : 2.0 / Lx;
+  const LD df = xb.dfx, pi = 3.141592653589793238462643383279502884L;
+  std::vector<LD> w(N);
+  xb.X.assign(N, 0.0L);
+  if (family == 0) {
+    for (int j = 0; j < N; ++j) {
+      xb.X[j] = std::cos(pi + (2.0L * j + 1.0L) * pi / (2.0L * N));
+      w[j] = pi / N;
+    }
+  } else {
+    gauss_legendre(N, xb.X, w);
+  }
+  xb.V.assign((size_t)N * N, 0.0L);
+  for (int j = 0; j < N; ++j) {
+    const LD x = xb.X[j];
+    LD p0 = 1.0L, p1 = x;
+    xb.V[(size_t)j * N] = 1.0L;
+    if (N > 1) xb.V[(size_t)j * N + 1] = x;
+    for (int n = 2; n < N; ++n) {
+      const LD p2 = family == 0 ? 2.0L * x * p1 - p0 : ((2 * n - 1) * x * p1 - (n - 1) * p0) / n;
+      xb.V[(size_t)j * N + n] = p2;
+      p0 = p1;
+      p1 = p2;
+    }
+  }
+  xb.Q.assign((size_t)N * N, 0.0L);
+  for (int n = 0; n < N; ++n)
+    for (int j = 0; j < N; ++j) xb.Q[(size_t)n * N + j] = xb.V[(size_t)j * N + n] * w[j] / df;
+  xb.ns.assign(N, 0.0L);
+  for (int n = 0; n < N; ++n)
+    xb.ns[n] = (family == 0 ? (n == 0 ? pi : pi / 2.0L) : 2.0L / (2.0L * n + 1.0L)) / df;
+  // d/dX on coefficients: Chebyshev (T_j)' = sum_{i<j, j-i odd} (2/c_i) j T_i
+  // (Chebyshev.py:319-353); Legendre (P_j)' = sum_{i<j, j-i odd} (2i+1) P_i
+  // (Legendre.py:195-227)
+  xb.D.assign((size_t)N * N, 0.0L);
+  for (int i = 0; i < N; ++i)
+    for (int j = i + 1; j < N; j += 2)
+      xb.D[(size_t)i * N + j] = family == 0 ? (i == 0 ? (LD)j : 2.0L * j) : 2.0L * i + 1.0L;
+  xb.S.assign((size_t)xb.nb * N, 0.0L);
+  for (int i = 0; i < xb.nb; ++i) {
+    const LD n = i;
+    xb.S[(size_t)i * N + i] = 1.0L;
+    if (basis == 1) {
+      xb.S[(size_t)i * N + i + 2] = -1.0L;
+    } else if (basis == 2) {
+      if (family == 0) {
+        xb.S[(size_t)i * N + i + 2] = 2.0L * (-n - 2.0L) / (n + 3.0L);
+        xb.S[(size_t)i * N + i + 4] = (n + 1.0L) / (n + 3.0L);
+      } else {
+        xb.S[(size_t)i * N + i + 2] = 2.0L * (-2.0L * n - 5.0L) / (2.0L * n + 7.0L);
+        xb.S[(size_t)i * N + i + 4] = (2.0L * n + 3.0L) / (2.0L * n + 7.0L);
+      }
+    }
+  }
+}
+
+std::vector<double> x_map_matrix(const XBasis& xb, int map, int k, int* rows, int* cols) {
+  const int N = xb.N, nb = xb.nb;
+  LMat V(N, N), Q(N, N), D(N, N), S(nb, N), W(N, N), Dk(N, N);
+  V.v = xb.V;
+  Q.v = xb.Q;
+  D.v = xb.D;
+  S.v = xb.S;
+  for (int n = 0; n < N; ++n) {
+    W(n, n) = xb.ns[n];
+    Dk(n, n) = 1.0L;
+  }
+  LD scale = 1.0L;
+  for (int t = 0; t < k; ++t) {
+    Dk = mul(D, Dk);
+    scale *= (LD)xb.dfx;
+  }
+  const LMat St = transpose(S);
+  auto mass_inv = [&]() { return inverse(mul(mul(S, W), St)); };
+  LMat R(1, 1);
+  switch (map) {
+    case kXBackward: R = mul(mul(V, Dk), St); break;
+    case kXToOrth: R = St; break;
+    case kXDiffOrth: R = Dk; break;
+    case kXProjectOrth: R = mul(mass_inv(), mul(S, W)); break;
+    case kXSpFromOrth: R = mul(S, W); break;
+    case kXForward: R = mul(mass_inv(), mul(S, Q)); break;
+    case kXScalarProd: R = mul(S, Q); break;
+    default: R = mul(mul(mul(S, W), Dk), St); break;  // kXGalerkin
+  }
+  if (map == kXBackward || map == kXDiffOrth || map == kXGalerkin)
+    for (LD& v : R.v) v *= scale;
+  *rows = R.r;
+  *cols = R.c;
+  std::vector<double> o(R.v.size());
+  for (size_t i = 0; i < o.size(); ++i) o[i] = (double)R.v[i];
+  return o;
+}
+
 void build_tps_x_operators(const HostOperators& op, int basis, TpsX& t) {
   const int N = op.N;
   const int nb = basis == 0 ? N : basis == 1 ? N - 2 : N - 4;

@@ -344,6 +344,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
   const size_t P = (size_t)d.P;
   const int half = d.Ny / 2;
   const int br = bitrev5(lane);
+  JFB_STAMP(1, 0);
+  pdl_trigger();
+  pdl_wait();  // X is written by the previous kernel, HX still read by it
+  JFB_STAMP(1, 1);
 
   // 1. inverse y transforms of this CTA's columns (complex64: staged row
   //    by row, coalesced along kz, into Ys in padded order, then one column
@@ -366,6 +370,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
       }
     }
     __syncthreads();
+    JFB_STAMP(1, 2);
     WarpTw<PY, T> w;
     load_warp_tw<PY, T>(w, twy, lane);
     for (int t = warp; t < 6 * KH; t += NW) {
@@ -380,6 +385,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
       for (int k1 = 0; k1 < PY; ++k1) col[(size_t)(k1 + PY * br) * LDZ] = v[k1];
     }
   } else {
+    JFB_STAMP(1, 2);
     WarpTw<PY, T> w;
     load_warp_tw<PY, T>(w, twy, lane);
     for (int t = warp; t < 6 * KH; t += NW) {
@@ -400,6 +406,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
     }
   }
   cluster.sync();
+  JFB_STAMP(1, 3);
 
   // 2. z stage on this CTA's rows, two rows per warp
   {
@@ -466,6 +473,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
     }
   }
   cluster.sync();
+  JFB_STAMP(1, 4);
 
   // 3. forward y transforms of this CTA's columns (complex64: into Ys,
   //    free once the peer has passed the barrier above, then row-wise
@@ -490,6 +498,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
       for (int k1 = 0; k1 < PY; ++k1) col[(size_t)(32 * k1 + lane) * LDZ] = scale * v[k1];
     }
     __syncthreads();
+    JFB_STAMP(1, 5);
     for (int e = threadIdx.x; e < 3 * d.Ny * KH; e += kPlaneThreads) {
       const int cl = e % KH, rf = e / KH, r = rf % d.Ny, f = rf / d.Ny;
       const int kz = rank * KH + cl;
@@ -530,8 +539,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
         else if (k == MY - half) dst[(size_t)half * Kz] = cmk(T(0), T(0));  // Nyquist
       }
     }
+    JFB_STAMP(1, 5);
   }
+  JFB_STAMP(1, 6);
   cluster.sync();
+  JFB_STAMP(1, 7);
 }
 
 }  // namespace jfb

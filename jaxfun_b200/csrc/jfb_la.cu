@@ -413,15 +413,16 @@ extern "C" int jfb_wavenumber_solve(const double* L, const int64_t* L_offsets, i
 // ===========================================================================
 // Allocation-free variant of the batched banded LU.
 //
-// Some callers cannot call cudaMalloc at all: code that runs while a stream
-// is being captured into a CUDA graph, kernels launched from a host callback,
-// or hosts whose device memory is fully owned by another framework's pool
-// (an XLA custom call, for example).  jfb_banded_lu_factor above allocates its
-// pivot-status word with cudaMallocAsync; this entry point keeps the pivot
-// status of every matrix in a fixed file-scope device array instead, so it
-// allocates nothing.  The array holds JFB_NOALLOC_LU_MAX_BATCH per-matrix
-// flags plus one slot for the index of the first singular matrix; every GPU
-// that loads the library holds it (256 KiB) until the process exits.
+// Some callers cannot call cudaMalloc at all: an XLA custom call or another
+// framework's operator, whose device memory belongs to that framework's
+// allocator, or a process whose caching pool already holds all of the GPU's
+// memory.  jfb_banded_lu_factor above allocates its pivot-status word with
+// cudaMallocAsync; this entry point keeps the pivot status of every matrix in
+// a fixed file-scope device array instead, so it allocates nothing.  The
+// array holds JFB_NOALLOC_LU_MAX_BATCH per-matrix flags plus one slot for the
+// index of the first singular matrix; every GPU that loads the library holds
+// it (256 KiB) until the process exits.  The call reads that index back to
+// the host, so it synchronises its stream.
 // ===========================================================================
 
 static __device__ __align__(256) int g_noalloc_lu_status[JFB_NOALLOC_LU_MAX_BATCH + 1];
@@ -472,7 +473,8 @@ __global__ void noalloc_lu_first_kernel(int* status, int64_t n_batch) {
 
 // Device address of the status array, looked up once per device with that
 // device current (the host-side symbol is only a stand-in, not a device
-// address, so it must never be passed to a kernel).
+// address, so it must never be passed to a kernel).  The address is kept for
+// the life of the process: it is not valid after cudaDeviceReset.
 static int noalloc_status_address(int** out) {
   static std::mutex mu;
   static int* addr[128] = {nullptr};

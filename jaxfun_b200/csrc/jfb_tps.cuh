@@ -35,6 +35,48 @@ __global__ void __launch_bounds__(256) x_apply_kernel(const double* __restrict__
   out[(size_t)i * M + m] = s0 + s1;
 }
 
+// Per-mode Fourier weight of the separable maps: scale * prod over the
+// periodic axes of (i m df)^k, m the FFT-ordered wavenumber, with the Nyquist
+// mode zeroed for odd k (Fourier.py:210-223).
+struct FourierWeight {
+  int n1, n2, k1, k2;
+  double df1, df2, scale;
+};
+
+__device__ __forceinline__ c64 ipow_times(c64 w, int idx, int n, int k, double df) {
+  if (k == 0) return w;
+  if ((k & 1) && 2 * idx == n) return cmk(0.0, 0.0);
+  const int m = (idx < (n + 1) / 2) ? idx : idx - n;
+  double a = 1.0;
+  for (int t = 0; t < k; ++t) a *= (double)m * df;
+  w = a * w;
+  for (int t = 0; t < (k & 3); ++t) w = mul_i(w);  // i^k
+  return w;
+}
+
+// out[i][m] = w(m) sum_k A[i][k] in[k][m]: an x-axis matrix with per-mode
+// Fourier weights (m = i1 n2 + i2 over the periodic axes).
+__global__ void __launch_bounds__(256) x_apply_w_kernel(const double* __restrict__ A, int rows,
+                                                        int cols, const c64* __restrict__ in,
+                                                        c64* __restrict__ out, FourierWeight fw) {
+  const int64_t M = (int64_t)fw.n1 * fw.n2;
+  const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (m >= M || i >= rows) return;
+  const double* a = A + (size_t)i * cols;
+  c64 s0 = cmk(0.0, 0.0), s1 = s0;
+  int k = 0;
+  for (; k + 1 < cols; k += 2) {
+    s0 = s0 + __ldg(a + k) * in[(size_t)k * M + m];
+    s1 = s1 + __ldg(a + k + 1) * in[(size_t)(k + 1) * M + m];
+  }
+  if (k < cols) s0 = s0 + __ldg(a + k) * in[(size_t)k * M + m];
+  c64 w = cmk(fw.scale, 0.0);
+  w = ipow_times(w, (int)(m / fw.n2), fw.n1, fw.k1, fw.df1);
+  w = ipow_times(w, (int)(m % fw.n2), fw.n2, fw.k2, fw.df2);
+  out[(size_t)i * M + m] = w * (s0 + s1);
+}
+
 // Complex FFT along contiguous lines: `lines` rows of length nin -> nout.
 // Inverse (sign +1, transform length nout): pad nin -> nout in the middle,
 // unnormalised.  Forward (sign -1, transform length nin): scaled 1/nin,
@@ -367,6 +409,8 @@ __global__ void __cluster_dims__(kHelmCTAs, 1, 1) __launch_bounds__(kHelmThreads
 
 struct jfb_tps {
   jfb_tps_config cfg;
+  jfb::XBasis xb;  // 1-D wall-normal basis data (long double)
+  std::map<int64_t, std::pair<double*, std::pair<int, int>>> xmaps;  // (map, k) -> device matrix
   int nb = 0, N = 0;
   int n1 = 1, n2 = 1, m1 = 1, m2 = 1;  // Fourier modes and padded counts
   double *B = nullptr, *F = nullptr, *Sq = nullptr;
@@ -379,6 +423,7 @@ struct jfb_tps {
 
 extern "C" int jfb_tps_destroy(jfb_tps* t) {
   if (!t) return JFB_OK;
+  for (auto& kv : t->xmaps) cudaFree(kv.second.first);
   for (void* p : t->allocs) cudaFree(p);
   delete t;
   return JFB_OK;
@@ -389,6 +434,8 @@ extern "C" int jfb_tps_create(const jfb_tps_config* cfg, jfb_tps** out) {
   *out = nullptr;
   JFB_REQUIRE(cfg->ndim == 2 || cfg->ndim == 3, "ndim must be 2 or 3");
   JFB_REQUIRE(cfg->basis >= 0 && cfg->basis <= 2, "unknown basis");
+  JFB_REQUIRE(cfg->family == JFB_FAMILY_CHEBYSHEV || cfg->family == JFB_FAMILY_LEGENDRE,
+              "family must be JFB_FAMILY_CHEBYSHEV or JFB_FAMILY_LEGENDRE");
   JFB_REQUIRE(cfg->n[0] >= 8 && cfg->n[0] <= 513, "n[0] out of range [8, 513]");
   for (int a = 1; a < cfg->ndim; ++a)
     JFB_REQUIRE(cfg->n[a] >= 2 && cfg->n[a] % 2 == 0, "Fourier sizes must be even");
@@ -407,10 +454,24 @@ extern "C" int jfb_tps_create(const jfb_tps_config* cfg, jfb_tps** out) {
   kc.x_lo = cfg->x_lo;
   kc.x_hi = cfg->x_hi;
   kc.ly = kc.lz = 2.0 * M_PI;
-  HostOperators op;
-  build_host_operators(kc, op);
+  build_x_basis(cfg->family, cfg->basis, cfg->n[0], cfg->x_lo, cfg->x_hi, t->xb);
   TpsX x;
-  build_tps_x_operators(op, cfg->basis, x);
+  if (cfg->family == JFB_FAMILY_CHEBYSHEV) {
+    HostOperators op;
+    build_host_operators(kc, op);
+    build_tps_x_operators(op, cfg->basis, x);
+  } else {
+    // Legendre: backward V S^T, forward M^-1 S Q, scalar product S Q and the
+    // Galerkin matrices, all from the Gauss-Legendre Vandermonde matrix
+    int r, c;
+    x.N = t->xb.N;
+    x.nb = t->xb.nb;
+    x.B = x_map_matrix(t->xb, kXBackward, 0, &r, &c);
+    x.F = x_map_matrix(t->xb, kXForward, 0, &r, &c);
+    x.Sq = x_map_matrix(t->xb, kXScalarProd, 0, &r, &c);
+    x.G0 = x_map_matrix(t->xb, kXGalerkin, 0, &r, &c);
+    x.G2 = x_map_matrix(t->xb, kXGalerkin, 2, &r, &c);
+  }
   t->N = x.N;
   t->nb = x.nb;
   t->G0 = x.G0;
@@ -466,6 +527,62 @@ extern "C" int jfb_tps_create(const jfb_tps_config* cfg, jfb_tps** out) {
 }
 
 namespace jfb {
+
+// Device copy of one separable x-axis map (built and uploaded on first use).
+static int tps_xmap(jfb_tps* t, int map, int k, const double** A, int* rows, int* cols) {
+  const int64_t key = (int64_t)map * 64 + k;
+  auto it = t->xmaps.find(key);
+  if (it == t->xmaps.end()) {
+    int r = 0, c = 0;
+    const std::vector<double> h = x_map_matrix(t->xb, map, k, &r, &c);
+    double* d = nullptr;
+    JFB_CHECK_CUDA(cudaMalloc((void**)&d, h.size() * sizeof(double)));
+    cudaError_t e = cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cudaFree(d);
+      JFB_CHECK_CUDA(e);
+    }
+    it = t->xmaps.emplace(key, std::make_pair(d, std::make_pair(r, c))).first;
+  }
+  *A = it->second.first;
+  *rows = it->second.second.first;
+  *cols = it->second.second.second;
+  return JFB_OK;
+}
+
+static double fourier_df(const jfb_tps* t, int a) {
+  const double L = t->cfg.l[a];
+  return std::fabs(L - 2.0 * M_PI) < 1e-12 ? 1.0 : 2.0 * M_PI / L;
+}
+
+// out = w * (map_k along x) in, w the Fourier weights of orders k1, k2.
+static int tps_xw(jfb_tps* t, int map, int kx, int k1, int k2, double scale, const c64* in,
+                  c64* out, cudaStream_t s) {
+  const double* A;
+  int rows, cols;
+  int st = tps_xmap(t, map, kx, &A, &rows, &cols);
+  if (st) return st;
+  FourierWeight fw;
+  fw.n1 = t->n1;
+  fw.n2 = t->n2;
+  fw.k1 = k1;
+  fw.k2 = t->cfg.ndim == 3 ? k2 : 0;
+  fw.df1 = fourier_df(t, 0);
+  fw.df2 = t->cfg.ndim == 3 ? fourier_df(t, 1) : 1.0;
+  fw.scale = scale;
+  const int64_t M = (int64_t)t->n1 * t->n2;
+  dim3 g((unsigned)((M + 255) / 256), rows);
+  x_apply_w_kernel<<<g, 256, 0, s>>>(A, rows, cols, in, out, fw);
+  JFB_CHECK_LAUNCH();
+  return JFB_OK;
+}
+
+static int check_orders(const jfb_tps* t, const int32_t* k) {
+  JFB_REQUIRE(k, "null derivative orders");
+  for (int a = 0; a < t->cfg.ndim; ++a)
+    JFB_REQUIRE(k[a] >= 0 && k[a] < 32, "derivative orders must be in [0, 32)");
+  return JFB_OK;
+}
 
 static int tps_x(const double* A, int rows, int cols, const c64* in, c64* out, int64_t M,
                  cudaStream_t s) {
@@ -565,6 +682,51 @@ extern "C" int jfb_tps_forward(jfb_tps* t, const void* phys, void* coeffs, int p
   return JFB_OK;
 }
 
+extern "C" int jfb_tps_backward_primitive(jfb_tps* t, const void* coeffs, void* phys,
+                                          const int32_t* k, int padded, void* stream) {
+  JFB_REQUIRE(t && coeffs && phys, "null pointer");
+  int st = check_orders(t, k);
+  if (st) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const bool pad = padded != 0;
+  const int m1 = pad ? t->m1 : t->n1;
+  const int k2 = t->cfg.ndim == 3 ? k[2] : 0;
+  if ((st = tps_xw(t, kXBackward, k[0], k[1], k2, 1.0, (const c64*)coeffs, t->w0, s))) return st;
+  if (t->cfg.ndim == 2) return tps_y(t, +1, t->N, 1, t->w0, (c64*)phys, pad, s);
+  if ((st = tps_y(t, +1, t->N, t->n2, t->w0, t->w1, pad, s))) return st;
+  return tps_z(t, +1, (int64_t)t->N * m1, t->w1, (c64*)phys, pad, s);
+}
+
+extern "C" int jfb_tps_to_orthogonal(jfb_tps* t, const void* coeffs, void* orth, void* stream) {
+  JFB_REQUIRE(t && coeffs && orth, "null pointer");
+  return tps_xw(t, kXToOrth, 0, 0, 0, 1.0, (const c64*)coeffs, (c64*)orth,
+                (cudaStream_t)stream);
+}
+
+extern "C" int jfb_tps_differentiate_orthogonal(jfb_tps* t, const void* orth, void* out,
+                                                const int32_t* k, void* stream) {
+  JFB_REQUIRE(t && orth && out, "null pointer");
+  int st = check_orders(t, k);
+  if (st) return st;
+  return tps_xw(t, kXDiffOrth, k[0], k[1], t->cfg.ndim == 3 ? k[2] : 0, 1.0, (const c64*)orth,
+                (c64*)out, (cudaStream_t)stream);
+}
+
+extern "C" int jfb_tps_project_from_orthogonal(jfb_tps* t, const void* orth, void* coeffs,
+                                               void* stream) {
+  JFB_REQUIRE(t && orth && coeffs, "null pointer");
+  return tps_xw(t, kXProjectOrth, 0, 0, 0, 1.0, (const c64*)orth, (c64*)coeffs,
+                (cudaStream_t)stream);
+}
+
+extern "C" int jfb_tps_scalar_product_from_orthogonal(jfb_tps* t, const void* orth, void* out,
+                                                      void* stream) {
+  JFB_REQUIRE(t && orth && out, "null pointer");
+  double w = 1.0;  // Fourier mass 2 pi / df per periodic axis
+  for (int a = 0; a + 1 < t->cfg.ndim; ++a) w *= 2.0 * M_PI / fourier_df(t, a);
+  return tps_xw(t, kXSpFromOrth, 0, 0, 0, w, (const c64*)orth, (c64*)out, (cudaStream_t)stream);
+}
+
 extern "C" int jfb_tps_galerkin(const jfb_tps* t, int order, double* out) {
   JFB_REQUIRE(t && out, "null pointer");
   JFB_REQUIRE(order == 0 || order == 2, "order must be 0 or 2");
@@ -593,6 +755,7 @@ extern "C" int jfb_helmholtz2d_solve(const jfb_tps* tc, const jfb_tps* td, const
   JFB_REQUIRE(tc->cfg.basis == JFB_BASIS_ORTHOGONAL && td->cfg.basis == JFB_BASIS_DIRICHLET,
               "tc must be orthogonal, td Dirichlet");
   JFB_REQUIRE(tc->N == td->N && tc->n1 == td->n1 && tc->nb == tc->N, "tc, td sizes differ");
+  JFB_REQUIRE(tc->cfg.family == td->cfg.family, "tc, td families differ");
   JFB_REQUIRE(fourier_mass != 0.0, "fourier_mass must be nonzero");
   JFB_REQUIRE(n_L >= 0 && n_L <= kHelmMaxDiag && n_U >= 1 && n_U <= kHelmMaxDiag,
               "too many diagonals");

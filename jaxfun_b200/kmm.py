@@ -248,12 +248,23 @@ class KMM:
         return self.solve(state, 1)
 
     def solve(self, state: KMMState, steps: int) -> KMMState:
-        """Advance ``steps`` steps (channelflow_kmm.py:1231-1247)."""
+        """Advance ``steps`` steps (channelflow_kmm.py:1231-1247).
+
+        Raises ``FloatingPointError`` (``_lib.NonFiniteStateError``) when a
+        solved coefficient became NaN or infinite, as the reference's runner
+        does for a non-finite state (production/oracles.py:3257-3261)."""
         steps = int(steps)
         self._load(state)
         hist = float(self._current.history_steps)
         _lib.call("jfb_kmm_advance", self._plan, steps, self._stream())
-        return self._fetch(min(2.0, hist + steps))
+        out = self._fetch(min(2.0, hist + steps))
+        self.check()
+        return out
+
+    def check(self) -> None:
+        """Read and clear the plan's device status word (synchronises the
+        stream); raise if a step saw a non-finite value or a timed-out wait."""
+        _lib.call("jfb_kmm_check", self._plan, None, self._stream())
 
     def advance_resident(self, steps: int) -> None:
         """Advance the device-resident state without materialising it."""

@@ -190,7 +190,9 @@ class PlaneCouetteMHD(PlaneCouetteFluctuation):
         self._load(state)
         hist = float(self._current.flow.history_steps)
         _lib.call("jfb_kmm_advance", self._plan, steps, self._stream())
-        return self._fetch_mhd(min(2.0, hist + steps))
+        out = self._fetch_mhd(min(2.0, hist + steps))
+        self.check()
+        return out
 
     def step(self, state: MHDState, dt=None, factor_args=None) -> MHDState:
         return self.solve(state, 1)
@@ -347,6 +349,8 @@ class Ensemble:
         for m, h in zip(self.members, hist, strict=True):
             h = min(2.0, h + int(steps))
             out.append(m._fetch_mhd(h) if isinstance(m, PlaneCouetteMHD) else m._fetch(h))
+        for m in self.members:
+            m.check()
         return out
 
 

@@ -25,7 +25,11 @@ LEAVES = ("u", "g")
 
 @dataclass(frozen=True)
 class MinimalSeedIteration:
-    """One accepted or terminal step from the fixed-energy ascent loop."""
+    """Record of one outer iteration of ``minimal_seed_ascent``.
+
+    ``gain`` and ``energy`` belong to the iterate the gradient was taken at;
+    ``step_size`` is the trial step that was taken (0.0 when none was), and
+    ``accepted`` says whether the iterate moved."""
 
     iteration: int
     gain: float
@@ -158,53 +162,102 @@ def gain_and_projected_gradient(solver: KMM, state: KMMState, steps: int, *,
     return gain, project_to_energy_tangent(solver, state, grad)
 
 
+def _check_ascent_options(steps, iterations, step_size, backtracking, min_step_size):
+    """Argument validation of ``minimal_seed_ascent``; returns the integer
+    horizon and iteration count."""
+    steps, iterations = int(steps), int(iterations)
+    problems = []
+    if steps < 0:
+        problems.append(f"the horizon (steps={steps}) cannot be negative")
+    if iterations < 0:
+        problems.append(f"the iteration count ({iterations}) cannot be negative")
+    for name, value in (("step_size", step_size), ("min_step_size", min_step_size)):
+        if not (math.isfinite(float(value)) and float(value) > 0.0):
+            problems.append(f"{name} has to be a finite number > 0 (got {value!r})")
+    if not (0.0 < float(backtracking) < 1.0):
+        problems.append(f"backtracking has to lie strictly inside (0, 1) (got {backtracking!r})")
+    if problems:
+        raise ValueError("minimal_seed_ascent: " + "; ".join(problems))
+    return steps, iterations
+
+
+class _TrialSteps:
+    """Geometric sequence of trial step lengths ``first, first*r, ...`` down
+    to (and including) the last one that is still >= ``floor``."""
+
+    def __init__(self, first: float, ratio: float, floor: float):
+        self.first, self.ratio, self.floor = float(first), float(ratio), float(floor)
+
+    def __iter__(self):
+        t = self.first
+        while t >= self.floor:
+            yield t
+            t *= self.ratio
+
+
+class _FixedEnergyLineSearch:
+    """Backtracking search along a unit ascent direction on the sphere of
+    fixed initial energy: every trial point is renormalised to the target
+    energy and scored by its gain E(T)/E(0), evaluated by the forward step on
+    the GPU; the first trial whose gain is finite and not below the current
+    gain wins (the acceptance rule of pcf_minimal_seed_jax.py:207-223)."""
+
+    def __init__(self, solver: KMM, steps: int, target_energy: float):
+        self.solver, self.steps, self.target = solver, steps, float(target_energy)
+
+    def point(self, origin: KMMState, direction: KMMState, length: float) -> KMMState:
+        return normalize_to_energy(self.solver, tree_add_scaled(origin, direction, length),
+                                   self.target)
+
+    def run(self, origin: KMMState, direction: KMMState, gain_now: float, trials):
+        for length in trials:
+            cand = self.point(origin, direction, length)
+            g = perturbation_gain(self.solver, cand, self.steps)
+            if math.isfinite(g) and g >= gain_now:
+                return length, cand
+        return None, origin
+
+
 def minimal_seed_ascent(solver: KMM, state: KMMState, *, target_energy: float, steps: int,
                         iterations: int = 10, step_size: float = 1.0, backtracking: float = 0.5,
                         min_step_size: float = 1.0e-8, tolerance: float = 1.0e-10,
                         checkpoint: int = 20):
-    """Projected-gradient fixed-energy ascent (pcf_minimal_seed_jax.py:153-238)."""
-    steps, iterations = int(steps), int(iterations)
-    if steps < 0:
-        raise ValueError("steps must be non-negative")
-    if iterations < 0:
-        raise ValueError("iterations must be non-negative")
-    if step_size <= 0.0 or not math.isfinite(float(step_size)):
-        raise ValueError("step_size must be positive and finite")
-    if not (0.0 < backtracking < 1.0):
-        raise ValueError("backtracking must be between 0 and 1")
-    if min_step_size <= 0.0 or not math.isfinite(float(min_step_size)):
-        raise ValueError("min_step_size must be positive and finite")
-    current = normalize_to_energy(solver, state, target_energy)
-    history = []
-    base_step = float(step_size)
-    for iteration in range(iterations):
-        gain, projected = gain_and_projected_gradient(solver, current, steps,
-                                                      checkpoint=checkpoint)
-        grad_norm = tree_l2_norm(projected)
-        energy = solver.perturbation_energy(current)
-        if not (math.isfinite(gain) and math.isfinite(grad_norm)):
-            raise FloatingPointError("minimal-seed ascent produced nonfinite gain/gradient")
-        if grad_norm <= tolerance:
-            history.append(MinimalSeedIteration(iteration, gain, 0.0, grad_norm, energy, False))
+    """Projected-gradient ascent of the gain at fixed initial energy
+    (pcf_minimal_seed_jax.py:153-238).
+
+    Each iteration takes the gain and its energy-projected gradient from the
+    hand-written adjoint (``gain_and_projected_gradient``), stops when the
+    gradient norm is at most ``tolerance``, and otherwise runs a backtracking
+    line search along the normalised gradient that starts from the last
+    accepted step length (``step_size`` at first), shrinks it by
+    ``backtracking`` and gives up below ``min_step_size``; the loop ends at
+    the first iteration whose search fails.  Returns the final iterate and
+    one ``MinimalSeedIteration`` per iteration run."""
+    steps, iterations = _check_ascent_options(steps, iterations, step_size, backtracking,
+                                              min_step_size)
+    search = _FixedEnergyLineSearch(solver, steps, target_energy)
+    x = normalize_to_energy(solver, state, target_energy)
+    length = float(step_size)
+    records = []
+    for it in range(iterations):
+        gain, pgrad = gain_and_projected_gradient(solver, x, steps, checkpoint=checkpoint)
+        gnorm = tree_l2_norm(pgrad)
+        energy = solver.perturbation_energy(x)
+        if not math.isfinite(gain) or not math.isfinite(gnorm):
+            raise FloatingPointError(
+                f"minimal_seed_ascent: iteration {it} gave gain={gain!r}, "
+                f"projected-gradient norm={gnorm!r}")
+        if gnorm <= tolerance:  # stationary on the energy sphere
+            records.append(MinimalSeedIteration(it, gain, 0.0, gnorm, energy, False))
             break
-        direction = tree_scale(projected, 1.0 / grad_norm)
-        trial = base_step
-        accepted = False
-        nxt = current
-        while trial >= min_step_size:
-            candidate = normalize_to_energy(
-                solver, tree_add_scaled(current, direction, trial), target_energy)
-            cgain = perturbation_gain(solver, candidate, steps)
-            if math.isfinite(cgain) and cgain >= gain:
-                nxt, accepted = candidate, True
-                break
-            trial *= backtracking
-        history.append(MinimalSeedIteration(iteration, gain, trial if accepted else 0.0,
-                                            grad_norm, energy, accepted))
-        if not accepted:
+        taken, x_next = search.run(x, tree_scale(pgrad, 1.0 / gnorm), gain,
+                                   _TrialSteps(length, backtracking, min_step_size))
+        records.append(MinimalSeedIteration(it, gain, taken or 0.0, gnorm, energy,
+                                            taken is not None))
+        if taken is None:
             break
-        current, base_step = nxt, trial
-    return current, tuple(history)
+        x, length = x_next, taken
+    return x, tuple(records)
 
 
 class GainFunction(torch.autograd.Function):

@@ -33,12 +33,15 @@ def _stream(dev) -> ctypes.c_void_p:
 class TensorProductSpace:
     """``TensorProduct(x_space, Fourier[, Fourier])``.
 
-    basis: "C" (orthogonal Chebyshev), "D" (Dirichlet), "B" (biharmonic);
+    basis: "C" (the orthogonal basis of the family), "D" (Dirichlet),
+    "B" (biharmonic); family: "C" (Chebyshev) or "L" (Legendre: Gauss-Legendre
+    nodes, Vandermonde contractions, orthogonal.py:121-145, 240-331);
     N = (x points, Fourier modes...); domain = ((x_lo, x_hi), (y0, y1)[, (z0, z1)]);
     padding_factor as in ``get_dealiased`` (the x entry is ignored).
     """
 
-    def __init__(self, basis: str, N, domain, padding_factor=None, device="cuda"):
+    def __init__(self, basis: str, N, domain, padding_factor=None, device="cuda",
+                 family: str = "C"):
         self.N = tuple(int(n) for n in N)
         self.ndim = len(self.N)
         if self.ndim not in (2, 3):
@@ -46,6 +49,10 @@ class TensorProductSpace:
         if basis not in _BASES:
             raise ValueError("basis must be 'C', 'D' or 'B'")
         self.basis = basis
+        fam = str(family).upper()[:1]
+        if fam not in ("C", "L"):
+            raise ValueError("family must be 'C' (Chebyshev) or 'L' (Legendre)")
+        self.family = fam
         self.domain = tuple(tuple(float(v) for v in d) for d in domain)
         pad = tuple(padding_factor) if padding_factor is not None else (1.0,) * self.ndim
         self.device = torch.device(device)
@@ -54,6 +61,7 @@ class TensorProductSpace:
         cfg = _lib.TPSConfig()
         cfg.ndim = self.ndim
         cfg.basis = _BASES[basis]
+        cfg.family = _lib.JFB_FAMILY_LEGENDRE if fam == "L" else _lib.JFB_FAMILY_CHEBYSHEV
         for a in range(3):
             cfg.n[a] = self.N[a] if a < self.ndim else 1
         cfg.x_lo, cfg.x_hi = self.domain[0]
@@ -106,6 +114,58 @@ class TensorProductSpace:
 
     def scalar_product(self, u: torch.Tensor, padded: bool = False) -> torch.Tensor:
         return self._fwd(u, padded, 1)
+
+    def _orders(self, k) -> ctypes.Array:
+        k = tuple(int(v) for v in k)
+        if len(k) != self.ndim:
+            raise ValueError(f"expected {self.ndim} derivative orders, received {len(k)}")
+        if any(v < 0 for v in k):
+            raise ValueError("derivative orders must be non-negative")
+        return (ctypes.c_int32 * 3)(*(k + (0,) * (3 - len(k))))
+
+    @property
+    def orthogonal_shape(self):
+        return (self.N[0],) + self.N[1:]
+
+    def backward_primitive(self, c: torch.Tensor, k, padded: bool = False) -> torch.Tensor:
+        """Mixed derivative of the field on the (padded) mesh
+        (tensorproductspace.py:553-594)."""
+        kk = self._orders(k)
+        c = self._check(c, self.num_dofs)
+        shape = self.padded_counts if padded else self.counts
+        out = torch.empty(shape, dtype=torch.complex128, device=self.device)
+        _lib.call("jfb_tps_backward_primitive", self._h, c.data_ptr(), out.data_ptr(), kk,
+                  int(padded), _stream(self.device))
+        return out
+
+    def _coeff_map(self, name, c, shape_in, shape_out, *extra) -> torch.Tensor:
+        c = self._check(c, shape_in)
+        out = torch.empty(shape_out, dtype=torch.complex128, device=self.device)
+        _lib.call(name, self._h, c.data_ptr(), out.data_ptr(), *extra, _stream(self.device))
+        return out
+
+    def to_orthogonal(self, c: torch.Tensor) -> torch.Tensor:
+        """``c @ S`` along x (tensorproductspace.py:596-616)."""
+        return self._coeff_map("jfb_tps_to_orthogonal", c, self.num_dofs, self.orthogonal_shape)
+
+    def differentiate_orthogonal_coeffs(self, c: torch.Tensor, k) -> torch.Tensor:
+        """tensorproductspace.py:638-682."""
+        return self._coeff_map("jfb_tps_differentiate_orthogonal", c, self.orthogonal_shape,
+                               self.orthogonal_shape, self._orders(k))
+
+    def derivative_orthogonal_coeffs(self, c: torch.Tensor, k) -> torch.Tensor:
+        """tensorproductspace.py:618-636."""
+        return self.differentiate_orthogonal_coeffs(self.to_orthogonal(c), k)
+
+    def project_from_orthogonal(self, c: torch.Tensor) -> torch.Tensor:
+        """tensorproductspace.py:706-728."""
+        return self._coeff_map("jfb_tps_project_from_orthogonal", c, self.orthogonal_shape,
+                               self.num_dofs)
+
+    def scalar_product_from_orthogonal(self, c: torch.Tensor) -> torch.Tensor:
+        """tensorproductspace.py:730-754."""
+        return self._coeff_map("jfb_tps_scalar_product_from_orthogonal", c,
+                               self.orthogonal_shape, self.num_dofs)
 
     def galerkin(self, order: int) -> np.ndarray:
         """Dense (phi_i, phi_j^(order))_w along x (host array)."""

@@ -27,6 +27,6 @@ int main(void) {
   F(jfb_mhd_params, eta); F(jfb_mhd_params, omega); F(jfb_mhd_params, b0);
   printf("jfb_tps_config %zu\n", sizeof(jfb_tps_config));
   F(jfb_tps_config, ndim); F(jfb_tps_config, n); F(jfb_tps_config, x_lo);
-  F(jfb_tps_config, l); F(jfb_tps_config, pad);
+  F(jfb_tps_config, l); F(jfb_tps_config, pad); F(jfb_tps_config, family);
   return 0;
 }

@@ -21,8 +21,8 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-def oracle_space(basis, N):
-    orth = ok.make_orthogonal("C", N[0], DOM3[0])
+def oracle_space(basis, N, family="C"):
+    orth = ok.make_orthogonal(family, N[0], DOM3[0])
     x = orth if basis == "C" else ok.Composite1D(orth, "dirichlet" if basis == "D" else "biharmonic")
     return ok.TensorSpace(x, ok.Fourier1D(N[1], DOM3[1]), ok.Fourier1D(N[2], DOM3[2]))
 
@@ -139,3 +139,59 @@ def test_helmholtz2d_solve_rejects_mismatched_spaces(cuda):
     other = Helmholtz2D((33, 16), device=cuda)
     with pytest.raises(_lib.JFBError):  # sizes differ
         _lib.call("jfb_helmholtz2d_solve", *args(h.TC, other.TD))
+
+
+@pytest.mark.parametrize("basis", ["C", "D", "B"])
+@pytest.mark.parametrize("N", [(17, 16, 12), (33, 32, 32)])
+def test_legendre_transforms_match_oracle(cuda, basis, N):
+    """The Legendre family: Gauss-Legendre nodes and the dense Vandermonde
+    contractions V @ c and (u w) @ V (orthogonal.py:121-145, 240-331)."""
+    T = TensorProductSpace(basis, N, DOM3, padding_factor=(1.0, 1.5, 1.5), device=cuda,
+                           family="L")
+    O = oracle_space(basis, N, "L")
+    rng = np.random.default_rng(7)
+    c = rng.standard_normal(T.num_dofs) + 1j * rng.standard_normal(T.num_dofs)
+    ct = torch.from_numpy(c).to(cuda)
+    for padded in (False, True):
+        counts = O.quad_counts((1.0, 1.5, 1.5)) if padded else O.quad_counts()
+        assert rel(T.backward(ct, padded=padded), O.backward(c, counts)) < 1e-13, padded
+    u = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    ut = torch.from_numpy(u).to(cuda)
+    assert rel(T.forward(ut), O.forward(u)) < 1e-13
+    assert rel(T.scalar_product(ut), O.scalar_product(u)) < 1e-13
+    # forward inverts backward on the space
+    assert rel(T.forward(T.backward(ct)), c) < 1e-12
+    if basis != "C":
+        G0 = O.x.galerkin_matrix(0)
+        assert np.abs(T.galerkin(0) - G0).max() <= 1e-13 * np.abs(G0).max()
+
+
+@pytest.mark.parametrize("family", ["C", "L"])
+@pytest.mark.parametrize("basis", ["C", "D", "B"])
+def test_coefficient_space_maps_match_oracle(cuda, family, basis):
+    """backward_primitive, to_orthogonal, differentiate_orthogonal_coeffs,
+    project_from_orthogonal and scalar_product_from_orthogonal
+    (tensorproductspace.py:553-754) against the oracle."""
+    N = (25, 16, 12)
+    T = TensorProductSpace(basis, N, DOM3, padding_factor=(1.0, 1.5, 1.5), device=cuda,
+                           family=family)
+    O = oracle_space(basis, N, family)
+    rng = np.random.default_rng(11)
+    c = rng.standard_normal(T.num_dofs) + 1j * rng.standard_normal(T.num_dofs)
+    ct = torch.from_numpy(c).to(cuda)
+    a = rng.standard_normal((N[0],) + N[1:]) + 1j * rng.standard_normal((N[0],) + N[1:])
+    at = torch.from_numpy(a).to(cuda)
+    for k in ((0, 0, 0), (1, 0, 0), (2, 1, 0), (0, 1, 2), (1, 3, 1)):
+        for padded in (False, True):
+            counts = O.quad_counts((1.0, 1.5, 1.5)) if padded else O.quad_counts()
+            got = T.backward_primitive(ct, k, padded=padded)
+            assert rel(got, O.backward_primitive(c, k, counts)) < 1e-12, (k, padded)
+        assert rel(T.differentiate_orthogonal_coeffs(at, k),
+                   O.differentiate_orthogonal_coeffs(a, k)) < 1e-12, k
+        assert rel(T.derivative_orthogonal_coeffs(ct, k),
+                   O.differentiate_orthogonal_coeffs(O.to_orthogonal(c), k)) < 1e-12, k
+    assert rel(T.to_orthogonal(ct), O.to_orthogonal(c)) < 1e-14
+    assert rel(T.project_from_orthogonal(at), O.project_from_orthogonal(a)) < 1e-13
+    assert rel(T.scalar_product_from_orthogonal(at), O.scalar_product_from_orthogonal(a)) < 1e-13
+    # project_from_orthogonal(to_orthogonal(c)) == c on the space
+    assert rel(T.project_from_orthogonal(T.to_orthogonal(ct)), c) < 1e-13

@@ -65,3 +65,41 @@ def test_measured_peak_has_a_source():
     peak, kind = bench.measured_peak()
     assert peak > 1000 and kind in ("measured", "fallback")
     assert math.isfinite(peak)
+
+
+def test_torch_library_ops_are_registered_with_fake_kernels():
+    """The jaxfun_b200::* operators exist and their fake (meta) kernels give
+    the output shapes without a GPU."""
+    import torch
+    from torch._subclasses.fake_tensor import FakeTensorMode
+
+    from jaxfun_b200 import torch_ops  # noqa: F401
+
+    ops = torch.ops.jaxfun_b200
+    for name in ("dia_matvec", "wavenumber_solve", "tps_backward", "tps_forward", "kmm_gain"):
+        assert hasattr(ops, name), name
+    with FakeTensorMode():
+        data = torch.empty((3, 9), dtype=torch.float64)
+        x = torch.empty((4, 9, 2), dtype=torch.complex128)
+        y = ops.dia_matvec(data, [-1, 0, 2], 11, 9, x, 1, False)
+        assert tuple(y.shape) == (4, 11, 2) and y.dtype == torch.complex128
+        z = ops.dia_matvec(data, [-1, 0, 2], 11, 9, torch.empty((11, 3)), 0, True)
+        assert tuple(z.shape) == (9, 3)
+        r = ops.wavenumber_solve(torch.empty((5, 1, 7)), [-2], torch.empty((5, 2, 7)), [0, 2],
+                                 torch.empty((5, 7), dtype=torch.complex128))
+        assert tuple(r.shape) == (5, 7)
+
+
+def test_minimal_seed_ascent_rejects_bad_options():
+    import pytest as _pytest
+
+    from jaxfun_b200 import minimal_seed as ms
+
+    for kw in (dict(steps=-1), dict(iterations=-2), dict(step_size=0.0),
+               dict(min_step_size=float("inf")), dict(backtracking=1.0)):
+        args = dict(steps=3, iterations=1, step_size=1.0, backtracking=0.5, min_step_size=1e-8)
+        args.update(kw)
+        with _pytest.raises(ValueError, match="minimal_seed_ascent"):
+            ms._check_ascent_options(**args)
+    assert ms._check_ascent_options(4, 2, 0.5, 0.5, 1e-8) == (4, 2)
+    assert list(ms._TrialSteps(1.0, 0.5, 0.2)) == [1.0, 0.5, 0.25]

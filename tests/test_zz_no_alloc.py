@@ -1,11 +1,12 @@
 """The allocation-free banded LU entry point (jfb_banded_lu_factor_noalloc).
 
-Callers that cannot allocate device memory -- code running while a stream is
-captured into a CUDA graph, an XLA custom call, a host whose device memory is
-owned by another framework's pool -- use this variant, which keeps its
-per-matrix pivot status in a fixed device array of the library instead of
-allocating it.  Its factors must be those of jfb_banded_lu_factor, call after
-call (the shared status array is cleared by every call).
+Callers that cannot allocate device memory -- an XLA custom call or another
+framework's operator whose device memory belongs to that framework's
+allocator, a process whose caching pool already holds all of the GPU's memory
+-- use this variant, which keeps its per-matrix pivot status in a fixed device
+array of the library instead of allocating it.  Its factors must be those of
+jfb_banded_lu_factor, call after call (the shared status array is cleared by
+every call).
 """
 
 import ctypes
