@@ -71,6 +71,8 @@ def parse_args(argv=None):
                    help="skip the 2-D Helmholtz block")
     p.add_argument("--no-sizes", action="store_true",
                    help="skip the 97^3 / 129^3 mixed-vs-FP64 block")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="time the default kernel variant instead of the autotuner's choice")
     return p.parse_args(argv)
 
 
@@ -365,6 +367,9 @@ def main(argv=None):
         e0 = solver.diagnostics(solver.state_from_physical(fields0))["Epert"]
         fields = scale_to_energy(fields0, e0, ENERGY)
         state = solver.state_from_physical(fields)
+        # kernel variant: the autotuner's choice for this grid and form
+        # (CUDA-event timing of graph-replayed steps, untimed here)
+        tuned = solver.autotune(state, steps=20, cache=False) if not args.no_autotune else None
         # warm-up: startup + W steady steps (graph replay), device resident
         state = solver.solve(state, 2 + max(3, args.warmup))
         torch.cuda.synchronize(dev)
@@ -401,6 +406,7 @@ def main(argv=None):
                   kms, ctypes.byref(sms), ctypes.c_void_p(stream.cuda_stream))
         torch.cuda.synchronize(dev)
         solver._current = None
+        info = solver.info()  # launches per step of the selected variant
         if info.launches_per_step == 2:  # pencil stage + fused plane transforms
             names = ("pencil_stage", "plane_transforms")
         else:
@@ -496,7 +502,8 @@ def main(argv=None):
                 "path": f"solve(state, {BLOCK}) per block with pinned-host state in/out and "
                         "diagnostics read back",
             },
-            "gpu_launches": info.launches_per_step * args.steps,
+            "gpu_launches": solver.info().launches_per_step * args.steps,
+            "autotune": tuned,
             "clocks": clocks,
             "final_diagnostics": final_diag,
             "device_bytes": info.device_bytes,
@@ -744,6 +751,7 @@ def main(argv=None):
                     e0 = sv.diagnostics(sv.state_from_physical(f0))["Epert"]
                     fields_n = scale_to_energy(f0, e0, ENERGY)
                 st = sv.state_from_physical(fields_n)
+                tuned = sv.autotune(st, steps=10, cache=False) if not args.no_autotune else None
                 st = sv.solve(st, 5)
                 torch.cuda.synchronize(dev)
                 K = 20
@@ -764,7 +772,7 @@ def main(argv=None):
                 names = (("pencil_stage", "plane_transforms") if lps == 2 else
                          ("pencil_stage", "y_backward", "z_cross", "y_forward"))
                 rec[prec] = {"ms_per_step": ms, "steps_per_s": 1000.0 / ms,
-                             "launches_per_step": lps,
+                             "launches_per_step": lps, "autotune": tuned,
                              "kernel_us": {k: kms[i] * 1000.0 / K for i, k in enumerate(names)}}
                 states[prec] = (sv, sv.state_from_physical(fields_n))
             (g64, a), (g32, b) = states["fp64"], states["mixed"]
@@ -820,7 +828,8 @@ def main(argv=None):
         r = results[p]
         r.pop("fields")
         line[p] = {k: r[k] for k in ("value", "ms_per_step", "roofline", "step_roofline",
-                                     "kernel_ms", "graph_l2_resident", "e2e", "gpu_launches")}
+                                     "kernel_ms", "graph_l2_resident", "e2e", "gpu_launches",
+                                     "autotune")}
     if err is not None:
         line["mixed_vs_fp64_rel_l2"] = err
     if adj is not None:

@@ -234,6 +234,40 @@ int jfb_kmm_gain_gradient(jfb_kmm_plan* plan, const jfb_kmm_state* init, int64_t
 int jfb_kmm_energy_gradient(jfb_kmm_plan* plan, const jfb_kmm_state* state,
                             const jfb_kmm_state* grad, void* stream);
 
+/* ---- kernel variants and the autotuner --------------------------------- */
+
+/* Kernel choices of a flow plan (no counterpart in the reference, whose XLA
+ * compiler picks its own kernels): pencil 1 = the FP64 tensor-core pencil
+ * stage (folded operators, needs nx <= 65), 0 = one warp per pencil;
+ * transforms 1 = the fused plane transforms (one launch per step, padded
+ * sizes 64 or 96), 0 = three launches; tc_velocity 1 = the mixed form's
+ * velocity products on tcgen05 (split BF16, FP32 accumulation); pdl 1 =
+ * programmatic dependent launch between the step kernels; replicas = copies
+ * of the folded operators the CTAs spread their L2 reads over (1-16). */
+typedef struct jfb_kmm_variant {
+  int32_t pencil;
+  int32_t transforms;
+  int32_t tc_velocity;
+  int32_t pdl;
+  int32_t replicas;
+} jfb_kmm_variant;
+
+/* The plan's current variant (cur) and, field by field, the largest value
+ * it accepts (avail); either may be NULL. */
+int jfb_kmm_get_variant(const jfb_kmm_plan* plan, jfb_kmm_variant* cur, jfb_kmm_variant* avail);
+/* Selects a variant (JFB_ERR_ARG if the plan cannot run it); drops the
+ * captured step graphs. */
+int jfb_kmm_set_variant(jfb_kmm_plan* plan, const jfb_kmm_variant* v);
+/* Times every variant the plan accepts (replicas 4, 8, 16) on copies of the
+ * loaded state: `steps` CUDA-graph steps each after five warm-up steps,
+ * CUDA events on `stream`; selects the fastest, returns it in *best and its
+ * time per step in *best_ms, and leaves the loaded state unchanged.  Only
+ * choices with the same arithmetic are compared: tc_velocity (a different
+ * accumulation precision) keeps its current value.  Allocates a temporary
+ * copy of the state; flow plans only. */
+int jfb_kmm_autotune(jfb_kmm_plan* plan, int64_t steps, jfb_kmm_variant* best, double* best_ms,
+                     void* stream);
+
 /* ---- plane-Couette MHD (vector potential, conducting walls) ------------- */
 
 /* Device pointers to an MHDState (examples/pcf_mhd_jax.py:34-66): the flow

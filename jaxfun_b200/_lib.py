@@ -110,6 +110,21 @@ class TPSConfig(ctypes.Structure):
     ]
 
 
+class KMMVariant(ctypes.Structure):
+    """``jfb_kmm_variant``: kernel choices of a flow plan."""
+
+    _fields_ = [
+        ("pencil", c_int32),
+        ("transforms", c_int32),
+        ("tc_velocity", c_int32),
+        ("pdl", c_int32),
+        ("replicas", c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
 class KMMInfo(ctypes.Structure):
     _fields_ = [
         ("n_pencils", c_int64),
@@ -153,6 +168,11 @@ SIGNATURES = {
     ),
     "jfb_kmm_diagnostics": (c_int, [c_void_p, c_void_p, c_void_p]),
     "jfb_kmm_check": (c_int, [c_void_p, POINTER(c_int32), c_void_p]),
+    "jfb_kmm_get_variant": (c_int, [c_void_p, POINTER(KMMVariant), POINTER(KMMVariant)]),
+    "jfb_kmm_set_variant": (c_int, [c_void_p, POINTER(KMMVariant)]),
+    "jfb_kmm_autotune": (
+        c_int, [c_void_p, c_int64, POINTER(KMMVariant), POINTER(c_double), c_void_p]
+    ),
     "jfb_kmm_timed_steps": (
         c_int,
         [c_void_p, c_int64, c_void_p, c_int64, POINTER(c_double), POINTER(c_double), c_void_p],

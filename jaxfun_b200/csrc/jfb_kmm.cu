@@ -254,7 +254,8 @@ struct jfb_kmm_plan {
   cudaStream_t cap = nullptr;  // private stream used only to capture the graphs
   cudaEvent_t* timing_events = nullptr;  // set by jfb_kmm_timed_steps
   bool gemm = false;       // tensor-core pencil stage (pencil_gemm_kernel)
-  bool pdl = true;         // programmatic dependent launch of the step kernels
+  bool gemm_ok = false, plane_ok = false, tc_ok = false;  // variants this plan can run
+  bool pdl = false;        // programmatic dependent launch of the step kernels
   bool plane = false;      // fused periodic-axis transforms (plane_cross_kernel)
   size_t smem_plane = 0;
   jfb::GemmOps gops;
@@ -1036,8 +1037,11 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   }
   if ((st = dalloc(pl, (void**)&pl->status, sizeof(int)))) return fail(st);
   {
+    // programmatic dependent launch of the step kernels: off unless
+    // JFB200_PDL=1 (measured slower here: the plane kernel's early CTAs and
+    // its clusters' placement stretch the transforms)
     const char* env = std::getenv("JFB200_PDL");
-    pl->pdl = !(env && std::string(env) == "0");
+    pl->pdl = env && std::string(env) == "1";
   }
   // kz column chunk of the y transforms: two My x KC complex buffers <= 100 KB
   pl->KC = d.Kz;
@@ -1060,7 +1064,8 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   pl->mixed = cfg->precision == JFB_PRECISION_MIXED;
   pl->smem_plane = plane_smem_bytes(d.My, d.Kz, pl->mixed ? sizeof(c32) : sizeof(c64));
   pl->plane = (pl->py == 2 || pl->py == 3) && (pl->pz == 2 || pl->pz == 3) && d.Kz % 2 == 0 &&
-              d.Kz <= 32 && pl->smem_plane <= 227 * 1024;
+              d.Kz <= 32 && pl->smem_plane <= 227 * 1024 && !pl->mhd;
+  pl->plane_ok = pl->plane;
   {
     const char* ev = std::getenv("JFB200_TRANSFORMS");
     if (ev && std::string(ev) == "split") pl->plane = false;
@@ -1220,7 +1225,7 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
     const size_t smem = ((size_t)G.oMid + 5 * 2 * kGW) * sizeof(double);
     const char* env = std::getenv("JFB200_PENCIL");
     const bool want = !(env && std::string(env) == "warp");
-    pl->gemm = want && smem <= 227 * 1024 && (d.nD + 1) / 2 <= kMaxM && Jl <= kMaxM;
+    pl->gemm = smem <= 227 * 1024 && (d.nD + 1) / 2 <= kMaxM && Jl <= kMaxM;
     GemmHost gh;
     if (pl->gemm) {
       std::string err;
@@ -1238,6 +1243,7 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
         }
       pl->gemm = fits;  // otherwise the warp-per-pencil kernel handles this size
     }
+    pl->gemm_ok = pl->gemm;
     if (pl->gemm) {
       // kReplicas copies of the operators: CTA b reads copy b % kReplicas, so
       // the CTAs that all read every operator line do not queue on the same
@@ -1275,7 +1281,71 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
       G.kt_mg_lin[1] = ceil_div(nDo, 4);
       pl->smem_gemm = smem;
       JFB_CHECK_CUDA(allow_smem((const void*)pencil_gemm_kernel));
+      // mixed form, JFB200_TC=1: the velocity products on the tcgen05
+      // tensor cores (split-BF16 operands, FP32 accumulation) when the
+      // halves fit the 32-row quarters / 32-deep K blocks and the images fit
+      // dead rows.  Off by default: measured slower than the FP64 DMMA
+      // products here, and the FP32 accumulation raises the mixed form's
+      // distance to FP64 about 30-fold (the base-flow terms are formed from
+      // these velocities).
+      const char* tce = std::getenv("JFB200_TC");
+      const size_t oTA = (size_t)G.oVel * kGLd * sizeof(double);
+      const size_t oTB = (size_t)G.oRU * kGLd * sizeof(double);
+      const bool tc_fit = Jl <= 32 && nBe <= 32 && nBo <= 32 && nDe <= 32 && nDo <= 32 &&
+                          oTA + kTcImgA <= oTB &&
+                          oTB + kTcImgB <= (size_t)G.rows * kGLd * sizeof(double) &&
+                          (size_t)10 * 32 * kTcStagePitch * sizeof(float) <= (size_t)kTcImgA;
+      if (pl->mixed && tc_fit) {
+        std::vector<unsigned char> img(kTcImgA, 0);
+        auto bf16_bits = [](float f) -> uint16_t {  // round to nearest even
+          uint32_t u;
+          std::memcpy(&u, &f, 4);
+          u += 0x7FFFu + ((u >> 16) & 1u);
+          return (uint16_t)(u >> 16);
+        };
+        auto bf16_val = [](uint16_t h) -> double {
+          const uint32_t u = (uint32_t)h << 16;
+          float f;
+          std::memcpy(&f, &u, 4);
+          return (double)f;
+        };
+        const int Nn = d.Nx;
+        // (group, quarter) -> (matrix N x n, coefficient parity, K offset in the group)
+        struct Q {
+          const std::vector<double>* M;
+          int ncol, par, koff;
+        };
+        const Q qs[3][4] = {
+            {{&gh.A0, d.nB, 0, 0}, {&gh.P2, d.nB, 0, 0}, {&gh.P1, d.nB, 0, 0}, {nullptr, 0, 0, 0}},
+            {{&gh.P1, d.nB, 1, 0}, {&gh.A0, d.nB, 1, 0}, {&gh.P2, d.nB, 1, 0}, {nullptr, 0, 0, 0}},
+            {{&gh.B1, d.nD, 0, 0}, {&gh.B2, d.nD, 0, 0}, {&gh.B2, d.nD, 1, 32}, {&gh.B1, d.nD, 1, 32}}};
+        for (int g = 0; g < 3; ++g)
+          for (int q = 0; q < 4; ++q) {
+            const Q& e = qs[g][q];
+            if (!e.M) continue;
+            const int nh = e.par ? e.ncol / 2 : (e.ncol + 1) / 2;
+            for (int r = 0; r < Jl; ++r)
+              for (int k = 0; k < nh; ++k) {
+                double v = (*e.M)[(size_t)r * e.ncol + 2 * k + e.par];
+                for (int sp = 0; sp < 3; ++sp) {
+                  const uint16_t h = bf16_bits((float)v);
+                  v -= bf16_val(h);
+                  const size_t o = (size_t)tc_a_off(g, sp) + tc_offset(32 * q + r, e.koff + k, tc_k(g));
+                  std::memcpy(&img[o], &h, 2);
+                }
+              }
+          }
+        (void)Nn;
+        unsigned char* dimg;
+        if ((st = upload(pl, &dimg, img))) return fail(st);
+        G.tc = (tce && std::string(tce) == "1") ? 1 : 0;
+        G.vimg = dimg;
+        G.oTA = (int)oTA;
+        G.oTB = (int)oTB;
+        pl->tc_ok = true;
+      }
     }
+    pl->gemm = pl->gemm_ok && want;
   }
 
   if (pl->mhd) {
@@ -2492,6 +2562,160 @@ extern "C" int jfb_kmm_energy_gradient(jfb_kmm_plan* pl, const jfb_kmm_state* st
 // step on its own stream (fork / join inside the capture), so members of
 // uneven wall-normal size run concurrently.
 // ---------------------------------------------------------------------------
+
+// ---------------------------------------------------------------------------
+// Kernel variants and their autotuner
+// ---------------------------------------------------------------------------
+
+extern "C" int jfb_kmm_get_variant(const jfb_kmm_plan* pl, jfb_kmm_variant* cur,
+                                   jfb_kmm_variant* avail) {
+  JFB_REQUIRE(pl, "null pointer");
+  if (cur) {
+    cur->pencil = pl->gemm ? 1 : 0;
+    cur->transforms = pl->plane ? 1 : 0;
+    cur->tc_velocity = pl->gops.tc;
+    cur->pdl = pl->pdl ? 1 : 0;
+    cur->replicas = pl->gemm_ok ? pl->gops.nrep : 0;
+  }
+  if (avail) {  // the largest value each field accepts
+    avail->pencil = pl->gemm_ok ? 1 : 0;
+    avail->transforms = pl->plane_ok ? 1 : 0;
+    avail->tc_velocity = pl->tc_ok ? 1 : 0;
+    avail->pdl = pl->mhd ? 0 : 1;
+    avail->replicas = pl->gemm_ok ? 16 : 0;
+  }
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_set_variant(jfb_kmm_plan* pl, const jfb_kmm_variant* v) {
+  JFB_REQUIRE(pl && v, "null pointer");
+  JFB_REQUIRE(v->pencil == 0 || (v->pencil == 1 && pl->gemm_ok), "pencil variant unavailable");
+  JFB_REQUIRE(v->transforms == 0 || (v->transforms == 1 && pl->plane_ok),
+              "fused plane transforms unavailable for this grid");
+  JFB_REQUIRE(v->tc_velocity == 0 || (v->tc_velocity == 1 && pl->tc_ok && v->pencil == 1),
+              "tensor-core velocity products need the mixed form and the tensor-core pencil stage");
+  JFB_REQUIRE(v->pdl == 0 || (v->pdl == 1 && !pl->mhd), "bad pdl flag");
+  JFB_REQUIRE(!pl->gemm_ok || (v->replicas >= 1 && v->replicas <= 16),
+              "replicas must be in [1, 16]");
+  destroy_graphs(pl);  // the captured steps hold the previous variant
+  pl->gemm = v->pencil == 1;
+  pl->plane = v->transforms == 1;
+  pl->gops.tc = v->tc_velocity;
+  pl->pdl = v->pdl == 1;
+  if (pl->gemm_ok) pl->gops.nrep = v->replicas;
+  return JFB_OK;
+}
+
+extern "C" int jfb_kmm_autotune(jfb_kmm_plan* pl, int64_t steps, jfb_kmm_variant* best,
+                                double* best_ms, void* stream) {
+  JFB_REQUIRE(pl && best && best_ms, "null pointer");
+  JFB_REQUIRE(steps >= 1 && steps <= 10000, "steps must be in [1, 10000]");
+  JFB_REQUIRE(!pl->mhd, "the autotuner covers flow plans");
+  if (!pl->have_state) {
+    set_error("no state loaded");
+    return JFB_ERR_STATE;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  // keep the loaded state: every trial starts from a copy of it
+  const size_t ne = checkpoint_elems(pl);
+  c64 *save = nullptr, *x_save = nullptr;
+  // X: six x-physical fields, complex64 (half the c64 count) in the mixed form
+  const size_t nx = ((size_t)6 * pl->d.Nx * pl->d.P + (pl->mixed ? 1 : 0)) / (pl->mixed ? 2 : 1);
+  JFB_CHECK_CUDA(cudaMalloc((void**)&save, ne * sizeof(c64)));
+  cudaError_t ce = cudaMalloc((void**)&x_save, (nx + 2 * (size_t)pl->d.nD * pl->d.P) * sizeof(c64));
+  if (ce != cudaSuccess) {
+    cudaFree(save);
+    JFB_CHECK_CUDA(ce);
+  }
+  const int64_t n0 = pl->n;
+  const int hist0 = pl->hist;
+  const bool haveH0 = pl->have_H, expl0 = pl->explicit_u12;
+  jfb_kmm_variant start;
+  jfb_kmm_get_variant(pl, &start, nullptr);
+  auto restore = [&]() -> int {
+    int st = checkpoint_io(pl, save, false, s);
+    if (st) return st;
+    JFB_CHECK_CUDA(cudaMemcpyAsync(pl->X, x_save, nx * sizeof(c64), cudaMemcpyDeviceToDevice, s));
+    JFB_CHECK_CUDA(cudaMemcpyAsync(pl->U1S, x_save + nx, (size_t)pl->d.nD * pl->d.P * sizeof(c64),
+                                   cudaMemcpyDeviceToDevice, s));
+    JFB_CHECK_CUDA(cudaMemcpyAsync(pl->U2S, x_save + nx + (size_t)pl->d.nD * pl->d.P,
+                                   (size_t)pl->d.nD * pl->d.P * sizeof(c64),
+                                   cudaMemcpyDeviceToDevice, s));
+    pl->n = n0;
+    pl->hist = hist0;
+    pl->have_H = haveH0;
+    pl->explicit_u12 = expl0;
+    return JFB_OK;
+  };
+  int st = checkpoint_io(pl, save, true, s);
+  if (!st) {
+    cudaError_t e = cudaMemcpyAsync(x_save, pl->X, nx * sizeof(c64), cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(x_save + nx, pl->U1S, (size_t)pl->d.nD * pl->d.P * sizeof(c64),
+                          cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(x_save + nx + (size_t)pl->d.nD * pl->d.P, pl->U2S,
+                          (size_t)pl->d.nD * pl->d.P * sizeof(c64), cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) {
+      set_error(std::string("autotune save: ") + cudaGetErrorString(e));
+      st = JFB_ERR_CUDA;
+    }
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (!st && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) {
+    set_error("autotune: cudaEventCreate failed");
+    st = JFB_ERR_CUDA;
+  }
+  double bms = 1e300;
+  jfb_kmm_variant bv = start;
+  jfb_kmm_variant avail;
+  jfb_kmm_get_variant(pl, nullptr, &avail);
+  const int reps[3] = {4, 8, 16};
+  for (int pc = avail.pencil; pc >= 0 && !st; --pc)
+    for (int tr = avail.transforms; tr >= 0 && !st; --tr)
+      for (int tc = (pc ? start.tc_velocity : 0); tc >= (pc ? start.tc_velocity : 0) && !st; --tc)
+        for (int pdl = 0; pdl <= avail.pdl && !st; ++pdl)
+          for (int ri = 0; ri < (pc ? 3 : 1) && !st; ++ri) {
+            jfb_kmm_variant v;
+            v.pencil = pc;
+            v.transforms = tr;
+            v.tc_velocity = tc;
+            v.pdl = pdl;
+            v.replicas = pl->gemm_ok ? (pc ? reps[ri] : start.replicas) : 0;
+            if ((st = jfb_kmm_set_variant(pl, &v))) break;
+            if ((st = restore())) break;
+            if ((st = jfb_kmm_advance(pl, 5, stream))) break;  // startup, capture, warm-up
+            if (cudaEventRecord(e0, s) != cudaSuccess) st = JFB_ERR_CUDA;
+            if (!st) st = jfb_kmm_advance(pl, steps, stream);
+            if (!st && cudaEventRecord(e1, s) != cudaSuccess) st = JFB_ERR_CUDA;
+            float ms = 0.0f;
+            if (!st && (cudaEventSynchronize(e1) != cudaSuccess ||
+                        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+              st = JFB_ERR_CUDA;
+            if (st) {
+              if (st == JFB_ERR_CUDA) set_error("autotune: timing failed");
+              break;
+            }
+            const double per = (double)ms / (double)steps;
+            if (per < bms) {
+              bms = per;
+              bv = v;
+            }
+          }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (!st) st = jfb_kmm_set_variant(pl, &bv);
+  else jfb_kmm_set_variant(pl, &start);
+  const int rs = restore();
+  cudaStreamSynchronize(s);
+  cudaFree(save);
+  cudaFree(x_save);
+  if (st) return st;
+  if (rs) return rs;
+  *best = bv;
+  *best_ms = bms;
+  return JFB_OK;
+}
 
 struct jfb_ensemble {
   std::vector<jfb_kmm_plan*> m;

@@ -57,6 +57,8 @@ struct GemmHost {
   // of TD projections of its derivatives: B1 = V S_D^T, B2 = V D S_D^T,
   // C1 = V S_D^T M_D^-1 S_D W D S_D^T, C2 = V S_D^T M_D^-1 S_D W D^2 S_D^T
   std::vector<double> B1, B2, C1, C2;
+  // P1 = B1 F, P2 = B2 F (N x nB, row-major): velocity from u0 (phase D)
+  std::vector<double> P1, P2;
   // Adjoint of the step: A0 = V S_B^T (N x nB), F = M_D^-1 S_D W D S_B^T
   // (nD x nB, the TD projection of d/dx of a TB field), the nonlinear-row
   // operators R0 = S_B W Pi, R1 = S_B W D Pi (nB x N), R2 = S_D W Pi (nD x N)

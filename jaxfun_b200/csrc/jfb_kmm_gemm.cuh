@@ -29,6 +29,7 @@
 
 #include "jfb_kmm.h"
 #include "jfb_kmm_kernels.cuh"
+#include "jfb_tc.cuh"
 
 namespace jfb {
 
@@ -58,7 +59,37 @@ struct GemmOps {
   int nfrag;    // doubles in one copy of frag; the velocity sub-matrices are its tail
   int nrep;     // copies of frag (CTA b reads copy b % nrep)
   int mid_stride;
+  // Tensor-core velocity products (mixed form): split-BF16 operator image in
+  // the tcgen05 operand layout (kTcImgA bytes), copied into dead shared
+  // memory at byte offset oTA; the split state operand goes to byte oTB.
+  int tc;
+  const unsigned char* vimg;
+  int oTA, oTB;
 };
+
+// Tensor-core velocity stage: three product groups of M = 128 rows (four
+// 32-row quarters, one velocity / vorticity half-product each) x N = 32
+// columns (16 pencils x re/im), K = 32, 32, 64 coefficient rows:
+//   group 0 (B = u0 even): A0Ee, P2Ee, P1Oe, -
+//   group 1 (B = u0 odd):  P1Eo, A0Oo, P2Oo, -
+//   group 2 (B = [g even; g odd]): B1Ee | 0, B2Oe | 0, 0 | B2Eo, 0 | B1Oo
+// Every operand is split into three BF16 parts (hi, mid, lo) and the six
+// products of combined order <= 2 are accumulated in FP32 in TMEM.
+__host__ __device__ constexpr int tc_k(int g) { return g == 2 ? 64 : 32; }
+constexpr int kTcImgA = 3 * 128 * (32 + 32 + 64) * 2;  // 98304 bytes
+constexpr int kTcImgB = 3 * 32 * (32 + 32 + 64) * 2;   // 24576 bytes
+__host__ __device__ inline int tc_a_off(int g, int s) {
+  return 3 * 128 * 2 * (g == 0 ? 0 : g == 1 ? 32 : 64) + s * 128 * 2 * (g == 2 ? 64 : 32);
+}
+__host__ __device__ inline int tc_b_off(int g, int s) {
+  return 3 * 32 * 2 * (g == 0 ? 0 : g == 1 ? 32 : 64) + s * 32 * 2 * (g == 2 ? 64 : 32);
+}
+// acc slot (velocity_fields argument order, see phase D) of group g, quarter q
+__host__ __device__ inline int tc_slot(int g, int q) {
+  const int t[3][4] = {{0, 2, 6, -1}, {1, 5, 7, -1}, {3, 9, 4, 8}};
+  return t[g][q];
+}
+constexpr int kTcStagePitch = 33;  // floats per staged row (conflict-free)
 
 // Largest k-tile ranges of the pipelined products (checked on the host).
 constexpr int kKtN = 20;   // Nu / Ng products
@@ -345,12 +376,42 @@ __device__ void mean_flow(const Dims& d, const DevOps& o, const GemmOps& G,
   }
 }
 
+// One value of the middle-node products (odd N): operator op = e / 32 of
+// (A0, P2 | u0 even; P1 | u0 odd; B1 | g even; B2 | g odd), column e % 32.
+__device__ __forceinline__ double mid_dot(const GemmOps& G, const double* sm, int e) {
+  const int col = e % (2 * kGW), op = e / (2 * kGW);
+  const int oB = (op <= 1) ? G.oUE : (op == 2) ? G.oUO : (op == 3) ? G.oGE : G.oGO;
+  const int K = (op <= 1) ? G.nBe : (op == 2) ? G.nBo : (op == 3) ? G.nDe : G.nDo;
+  const double* row = G.mid + op * G.mid_stride;
+  double s = 0.0;
+  for (int k = 0; k < K; ++k) s += __ldg(row + k) * sm[(size_t)(oB + k) * kGLd + col];
+  return s;
+}
+
+// u, omega at the middle node of pencil w from the products md[].
+__device__ __forceinline__ void mid_store(const Dims& d, const GemmStageArgs& a, const double* md,
+                                          const int* s_p, const double* s_ky, const double* s_kz,
+                                          int w, int N, int Jl, size_t P) {
+  if (s_p[w] < 0) return;
+  auto val = [&](int op) { return cmk(md[op * 2 * kGW + 2 * w], md[op * 2 * kGW + 2 * w + 1]); };
+  c64 f[6];
+  velocity_fields(s_ky[w], s_kz[w], val(0), val(2), val(1), val(3), val(4), f);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const size_t e = (size_t)q * N * P + (size_t)Jl * P + s_p[w];
+    if (a.x32) reinterpret_cast<c32*>(a.X)[e] = cmk((float)f[q].re, (float)f[q].im);
+    else a.X[e] = f[q];
+  }
+}
+
 __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOps o, GemmOps G,
                                                                    GemmStageArgs a) {
   extern __shared__ __align__(128) double sm[];
   __shared__ int s_p[kGW], s_mode[kGW];
   __shared__ double s_ky[kGW], s_kz[kGW];
   __shared__ __align__(8) uint64_t s_bar;
+  __shared__ __align__(8) uint64_t s_bar_mma;
+  __shared__ uint32_t s_tmem;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t4 = lane & 3;
   const int nKc = (d.Kz + 7) / 8;
@@ -383,6 +444,7 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     s_kz[tid] = kzp;
   } else if (tid == 32) {
     mbar_init(&s_bar, 1);
+    mbar_init(&s_bar_mma, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   } else if (tid == 64) {
     // factor records of this tile's wavenumbers (consecutive modes) into L2
@@ -400,7 +462,14 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     prefetch_l2(a.s00inv, (size_t)d.nD * d.nD * sizeof(double));
     if (sl != 0.0) prefetch_l2(G.X2D, (size_t)d.nD * d.nD * sizeof(double));
   }
+  if (G.tc && warp == 3) {  // 128 TMEM columns: the three 32-column accumulators
+    __syncwarp();
+    tc_alloc(&s_tmem, 128);
+  }
+  tc_fence_before();
   __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = G.tc ? s_tmem : 0u;
   // everything above reads only constant operators and factor records; the
   // arrays below are produced (HX) or still read (X) by the previous kernel
   pdl_wait();
@@ -659,10 +728,15 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
   // stage the velocity operators (tail of the operator copy) into dead rows
   if (tid == 0) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    const int voff = G.sub[gA0Ee].off;
-    const uint32_t bytes = (uint32_t)(G.nfrag - voff) * sizeof(double);
-    mbar_arrive_expect(&s_bar, bytes);
-    bulk_g2s(sm + (size_t)G.oVel * kGLd, frag + voff, bytes, &s_bar);
+    if (G.tc) {  // split-BF16 velocity operators in the tcgen05 operand layout
+      mbar_arrive_expect(&s_bar, (uint32_t)kTcImgA);
+      bulk_g2s(reinterpret_cast<unsigned char*>(sm) + G.oTA, G.vimg, (uint32_t)kTcImgA, &s_bar);
+    } else {
+      const int voff = G.sub[gA0Ee].off;
+      const uint32_t bytes = (uint32_t)(G.nfrag - voff) * sizeof(double);
+      mbar_arrive_expect(&s_bar, bytes);
+      bulk_g2s(sm + (size_t)G.oVel * kGLd, frag + voff, bytes, &s_bar);
+    }
   }
   // C1: forward elimination, one thread per (pencil, system, parity), in place;
   // warps 2..7 of the mean CTA solve the mean-flow system meanwhile
@@ -755,7 +829,102 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
   JFB_STAMP(0, 7);
 
   // ------------------------------------------------------------------ D --
-  if (!skip_d) {
+  if (!skip_d && G.tc) {
+    unsigned char* smb = reinterpret_cast<unsigned char*>(sm);
+    // state operand: FP64 coefficient rows -> three BF16 parts, K-major
+    // (row n = pencil column: 2 w + re/im, k = coefficient row of the half)
+    for (int e = tid; e < 32 * 128; e += kGThreads) {
+      const int n = e & 31, kk = e >> 5;  // kk over the groups' K: 0-31, 32-63, 64-127
+      const int g = kk < 32 ? 0 : kk < 64 ? 1 : 2;
+      const int k = kk - (g == 0 ? 0 : g == 1 ? 32 : 64);
+      int row = -1;
+      if (g == 0) row = k < G.nBe ? G.oUE + k : -1;
+      else if (g == 1) row = k < G.nBo ? G.oUO + k : -1;
+      else if (k < 32) row = k < G.nDe ? G.oGE + k : -1;
+      else row = (k - 32) < G.nDo ? G.oGO + (k - 32) : -1;
+      const double v = row >= 0 ? sm[(size_t)row * kGLd + n] : 0.0;
+      __nv_bfloat16 b[3];
+      bf16_split3(v, b);
+      const uint32_t o = tc_offset(n, k, tc_k(g));
+#pragma unroll
+      for (int sp = 0; sp < 3; ++sp)
+        *reinterpret_cast<__nv_bfloat16*>(smb + G.oTB + tc_b_off(g, sp) + o) = b[sp];
+    }
+    fence_async_smem();
+    __syncthreads();
+    JFB_STAMP(0, 10);
+    if (tid == 0) {
+      tc_fence_after();
+      // descriptors: a base per operand and group, then constant offsets
+      // (start addresses in 16-byte units in the low bits)
+      const uint32_t a0 = smem_u32(smb + G.oTA), b0 = smem_u32(smb + G.oTB);
+      const uint32_t idesc = tc_idesc_bf16(128, 32);
+#pragma unroll
+      for (int g = 0; g < 3; ++g) {
+        const int K = g == 2 ? 64 : 32;
+        const uint64_t ad0 = tc_smem_desc(a0 + tc_a_off(g, 0), (uint32_t)(K / 8) * 128);
+        const uint64_t bd0 = tc_smem_desc(b0 + tc_b_off(g, 0), (uint32_t)(K / 8) * 128);
+        const uint32_t sa = (uint32_t)(128 * K * 2) >> 4, sb = (uint32_t)(32 * K * 2) >> 4;
+#pragma unroll
+        for (int t = 0; t < K / 16; ++t)
+#pragma unroll
+          for (int q = 0; q < 6; ++q) {
+            const uint32_t pa = (q == 2 || q == 4) ? 1 : (q == 5) ? 2 : 0;
+            const uint32_t pb = (q == 1 || q == 4) ? 1 : (q == 3) ? 2 : 0;
+            const uint32_t kt = (uint32_t)(t * 2 * kTcLBO) >> 4;
+            tc_mma_bf16(tmem + 32 * g, ad0 + pa * sa + kt, bd0 + pb * sb + kt, idesc,
+                        t > 0 || q > 0);
+          }
+      }
+      tc_commit(&s_bar_mma);
+    }
+    JFB_STAMP(0, 11);
+    // middle Gauss node (odd N) on the last four warps while the MMAs run:
+    // one FP64 dot product per (operator, pencil, re/im)
+    if (Jh > Jl && warp >= kGWarps - 4) {
+      for (int e = tid - (kGThreads - 128); e < 5 * 2 * kGW; e += 128)
+        sm[G.oMid + e] = mid_dot(G, sm, e);
+    }
+    const bool done = mbar_wait_bounded(&s_bar_mma, 0, G.status, kStatusWaitTimeout);
+    tc_fence_after();
+    const bool skip_epi = __syncthreads_or(!done);
+    JFB_STAMP(0, 12);
+    float* st = reinterpret_cast<float*>(smb + G.oTA);  // [10][32][kTcStagePitch]
+    if (!skip_epi) {
+      const int g = warp >> 2, q = warp & 3;
+      if (g < 3 && tc_slot(g, q) >= 0) {
+        float v[32];
+        tc_ld32(tmem + ((uint32_t)(32 * q) << 16) + 32 * g, v);
+        float* row = st + ((size_t)tc_slot(g, q) * 32 + lane) * kTcStagePitch;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) row[c] = v[c];
+      }
+    }
+    __syncthreads();
+    JFB_STAMP(0, 13);
+    if (!skip_epi) {
+      const int j = tid >> 4, w = tid & 15;
+      const int p = s_p[w];
+      if (j < Jl && p >= 0) {
+        auto val = [&](int slot) {
+          const float* r = st + ((size_t)slot * 32 + j) * kTcStagePitch + 2 * w;
+          return cmk((double)r[0], (double)r[1]);
+        };
+        c64 fe[6], fo[6];
+        velocity_fields(s_ky[w], s_kz[w], val(0), val(1), val(2), val(3), val(4), fe);
+        velocity_fields(s_ky[w], s_kz[w], val(5), val(6), val(7), val(8), val(9), fo);
+        const int jm = N - 1 - j;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          const c64 vp = fe[q] + fo[q], vm = fe[q] - fo[q];
+          c32* X = reinterpret_cast<c32*>(a.X) + (size_t)q * N * P + p;
+          X[(size_t)j * P] = cmk((float)vp.re, (float)vp.im);
+          X[(size_t)jm * P] = cmk((float)vm.re, (float)vm.im);
+        }
+      }
+      if (Jh > Jl && tid < kGW) mid_store(d, a, sm + G.oMid, s_p, s_ky, s_kz, tid, N, Jl, P);
+    }
+  } else if (!skip_d) {
     const int MTv = G.sub[gA0Ee].mt;
     const double* vs = sm + (size_t)G.oVel * kGLd - G.sub[gA0Ee].off + lane;
     for (int task = warp; task < 4 * MTv; task += kGWarps) {
@@ -825,31 +994,19 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     }
   }
   JFB_STAMP(0, 8);
-  if (Jh > Jl && !skip_d) {
+  if (Jh > Jl && !skip_d && !G.tc) {
     // middle Gauss node (odd N): symmetric halves only, one dot product per
     // (operator, pencil, re/im) thread
-    double* md = sm + G.oMid;
-    if (tid < 5 * 2 * kGW) {
-      const int col = tid % (2 * kGW), op = tid / (2 * kGW);
-      const int oB = (op <= 1) ? G.oUE : (op == 2) ? G.oUO : (op == 3) ? G.oGE : G.oGO;
-      const int K = (op <= 1) ? G.nBe : (op == 2) ? G.nBo : (op == 3) ? G.nDe : G.nDo;
-      const double* row = G.mid + op * G.mid_stride;
-      double s = 0.0;
-      for (int k = 0; k < K; ++k) s += __ldg(row + k) * sm[(size_t)(oB + k) * kGLd + col];
-      md[tid] = s;
-    }
+    if (tid < 5 * 2 * kGW) sm[G.oMid + tid] = mid_dot(G, sm, tid);
     __syncthreads();
-    if (tid < kGW && s_p[tid] >= 0) {
-      const int w = tid;
-      auto val = [&](int op) { return cmk(md[op * 2 * kGW + 2 * w], md[op * 2 * kGW + 2 * w + 1]); };
-      c64 f[6];
-      velocity_fields(s_ky[w], s_kz[w], val(0), val(2), val(1), val(3), val(4), f);
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        const size_t e = (size_t)q * N * P + (size_t)Jl * P + s_p[w];
-        if (a.x32) reinterpret_cast<c32*>(a.X)[e] = cmk((float)f[q].re, (float)f[q].im);
-        else a.X[e] = f[q];
-      }
+    if (tid < kGW) mid_store(d, a, sm + G.oMid, s_p, s_ky, s_kz, tid, N, Jl, P);
+  }
+  if (G.tc) {  // free the TMEM columns (every tcgen05 load has completed)
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 3) {
+      tc_fence_after();
+      tc_dealloc(tmem, 128);
     }
   }
   JFB_STAMP(0, 9);

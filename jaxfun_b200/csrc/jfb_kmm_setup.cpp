@@ -504,6 +504,8 @@ bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& er
     };
     gh.B1 = dense(B1);
     gh.B2 = dense(B2);
+    gh.P1 = dense(P1);
+    gh.P2 = dense(P2);
     gh.C1 = dense(C1);
     gh.C2 = dense(C2);
     gh.A0 = dense(A0);

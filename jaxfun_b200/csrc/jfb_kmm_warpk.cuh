@@ -354,19 +354,32 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
   //    per warp in place; FP64: gathered per column straight from X)
   if constexpr (sizeof(T) == 4) {
     // half-warp per row (KH <= 16 columns), no per-element index division
+    // (all loads of a thread are issued before its stores: Ny <= MY <= 96
+    // gives at most three rows per half-warp and field)
     const int hw = threadIdx.x >> 4, cl = threadIdx.x & 15;
+    constexpr int RS = kPlaneThreads / 16, RMAX = (MY + RS - 1) / RS;
     if (cl < KH) {
-#pragma unroll 1
+      cpx<T> v[6][RMAX];
+#pragma unroll
       for (int f = 0; f < 6; ++f) {
         const cpx<T>* src = X + ((size_t)f * d.Nx + j) * P + rank * KH + cl;
-        cpx<T>* dst = Ys + (size_t)f * MY * LDZ + cl;
-        for (int r = hw; r < d.Ny; r += kPlaneThreads / 16) {
-          if (r == half) continue;  // Nyquist row: zero, below
-          const int k = (r < half) ? r : r - d.Ny + MY;  // padded row
-          dst[(size_t)k * LDZ] = src[(size_t)r * Kz];
+#pragma unroll
+        for (int i = 0; i < RMAX; ++i) {
+          const int r = hw + RS * i;
+          v[f][i] = (r < d.Ny && r != half) ? src[(size_t)r * Kz] : cmk(T(0), T(0));
         }
-        for (int k = half + hw; k <= MY - half; k += kPlaneThreads / 16)
-          dst[(size_t)k * LDZ] = cmk(T(0), T(0));
+      }
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        cpx<T>* dst = Ys + (size_t)f * MY * LDZ + cl;
+#pragma unroll
+        for (int i = 0; i < RMAX; ++i) {
+          const int r = hw + RS * i;  // the Nyquist row r == half stays zero
+          if (r < d.Ny) dst[(size_t)((r < half) ? r : r - d.Ny + MY) * LDZ] = v[f][i];
+        }
+        // padding rows half .. MY - half - 1 (row MY - half is the Nyquist
+        // row's slot, zeroed above)
+        for (int k = half + hw; k < MY - half; k += RS) dst[(size_t)k * LDZ] = cmk(T(0), T(0));
       }
     }
     __syncthreads();

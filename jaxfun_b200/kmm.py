@@ -266,6 +266,54 @@ class KMM:
         stream); raise if a step saw a non-finite value or a timed-out wait."""
         _lib.call("jfb_kmm_check", self._plan, None, self._stream())
 
+    # -- kernel variants -------------------------------------------------------
+    def variant(self) -> dict:
+        """The plan's kernel choices (``jfb_kmm_variant``) and the largest
+        value each accepts."""
+        cur, avail = _lib.KMMVariant(), _lib.KMMVariant()
+        _lib.call("jfb_kmm_get_variant", self._plan, ctypes.byref(cur), ctypes.byref(avail))
+        return {"current": cur.as_dict(), "available": avail.as_dict()}
+
+    def set_variant(self, **fields) -> None:
+        """Select kernel choices by field name (see ``jfb_kmm_variant``)."""
+        v = _lib.KMMVariant(**self.variant()["current"])
+        for k, val in fields.items():
+            if not hasattr(v, k):
+                raise ValueError(f"unknown variant field {k!r}")
+            setattr(v, k, int(val))
+        _lib.call("jfb_kmm_set_variant", self._plan, ctypes.byref(v))
+
+    def autotune(self, state: KMMState | None = None, steps: int = 20,
+                 cache: bool = True) -> dict:
+        """Time every kernel variant this plan accepts on copies of ``state``
+        (default: the loaded state), select the fastest and return
+        ``{"variant": ..., "ms_per_step": ...}``.  With ``cache`` the choice
+        is remembered per (device, grid, precision) in the file named by
+        JFB200_AUTOTUNE_CACHE (default ~/.cache/jaxfun_b200/autotune.json)
+        and reused without timing."""
+        from . import autotune as at
+
+        key = at.cache_key(self)
+        if cache:
+            hit = at.lookup(key)
+            if hit is not None:
+                try:
+                    self.set_variant(**hit["variant"])
+                    return dict(hit, cached=True)
+                except _lib.JFBError:
+                    pass
+        if state is not None:
+            self._load(state)
+        if self._current is None:
+            raise ValueError("autotune needs a state: pass one or load one first")
+        best, ms = _lib.KMMVariant(), ctypes.c_double()
+        _lib.call("jfb_kmm_autotune", self._plan, int(steps), ctypes.byref(best),
+                  ctypes.byref(ms), self._stream())
+        out = {"variant": best.as_dict(), "ms_per_step": ms.value, "cached": False}
+        if cache:
+            at.store(key, out)
+        return out
+
     def advance_resident(self, steps: int) -> None:
         """Advance the device-resident state without materialising it."""
         _lib.call("jfb_kmm_advance", self._plan, int(steps), self._stream())

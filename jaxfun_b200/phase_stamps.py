@@ -80,9 +80,21 @@ def main(argv=None) -> int:
         tot = statistics.median(statistics.median((c[-1] - c[0]) / 1e3 for c in r)
                                 for r in runs[k] if r)
         span = (max(c[-1] for c in last) - t0) / 1e3
-        out["pencil_gemm" if k == 0 else "plane_cross"] = {
-            "ctas": len(last), "phases_median_cta": per, "cta_total_median": tot,
-            "first_start_to_last_end": span}
+        rec = {"ctas": len(last), "phases_median_cta": per, "cta_total_median": tot,
+               "first_start_to_last_end": span}
+        if k == 0:  # tensor-core velocity stage (JFB200_TC=1): stamps 10-13 inside D
+            sub = []
+            for c in range(n_cta):
+                st = [buf[c * n_ph + i] for i in (7, 10, 11, 12, 13, 8)]
+                if all(st) and all(st[i + 1] >= st[i] for i in range(5)):
+                    sub.append(st)
+            if sub:
+                names = ("D: state split", "D: MMA issue", "D: MMA wait", "D: TMEM load",
+                         "D: epilogue")
+                rec["tc_subphases_median_cta"] = {
+                    n: statistics.median((c[i + 1] - c[i]) / 1e3 for c in sub)
+                    for i, n in enumerate(names)}
+        out["pencil_gemm" if k == 0 else "plane_cross"] = rec
     print(json.dumps(out))
     return 0
 

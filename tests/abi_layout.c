@@ -28,5 +28,7 @@ int main(void) {
   printf("jfb_tps_config %zu\n", sizeof(jfb_tps_config));
   F(jfb_tps_config, ndim); F(jfb_tps_config, n); F(jfb_tps_config, x_lo);
   F(jfb_tps_config, l); F(jfb_tps_config, pad); F(jfb_tps_config, family);
+  printf("jfb_kmm_variant %zu\n", sizeof(jfb_kmm_variant));
+  F(jfb_kmm_variant, pencil); F(jfb_kmm_variant, tc_velocity); F(jfb_kmm_variant, replicas);
   return 0;
 }

@@ -66,7 +66,8 @@ def c_layout(tmp_path_factory):
                                         ("jfb_kmm_info", _lib.KMMInfo),
                                         ("jfb_mhd_state", _lib.MHDStateC),
                                         ("jfb_mhd_params", _lib.MHDParams),
-                                        ("jfb_tps_config", _lib.TPSConfig)])
+                                        ("jfb_tps_config", _lib.TPSConfig),
+                                        ("jfb_kmm_variant", _lib.KMMVariant)])
 def test_struct_layouts_match_c(c_layout, cname, cls):
     assert int(c_layout[cname]) == ctypes.sizeof(cls)
     for key, off in c_layout.items():

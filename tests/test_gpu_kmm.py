@@ -257,3 +257,43 @@ def test_wide_wall_normal_grids_match_oracle(cuda, N, precision):
     tol = 1e-12 if precision == "fp64" else 1e-6
     for a, b in zip((*gs.u, gs.g), (*st.u, st.g), strict=True):
         assert rel(a, b) < tol
+
+
+@pytest.mark.parametrize("N", [(65, 64, 64), (33, 32, 32)])
+def test_tensor_core_velocity_products_track_dmma(cuda, N, monkeypatch):
+    """Mixed form with JFB200_TC=1: the velocity / vorticity products of the
+    pencil stage on the tcgen05 tensor cores (three-way split-BF16 operands,
+    FP32 accumulation in TMEM) against the default FP64 DMMA products.  Both
+    round the fields to complex64; the FP32 accumulation leaves the state
+    after 12 steps within 5e-8 (measured 1.6e-8 at 65x64x64)."""
+    kw = dict(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02, precision="mixed",
+              device=cuda)
+    g2 = PlaneCouetteFluctuation(**kw)
+    monkeypatch.setenv("JFB200_TC", "1")
+    g1 = PlaneCouetteFluctuation(**kw)
+    s0 = g1.initial_state()
+    a, b = g1.solve(s0, 12), g2.solve(s0, 12)
+    for x, y in zip((*a.u, a.g), (*b.u, b.g), strict=True):
+        assert rel(x, y.cpu().numpy()) < 5e-8
+
+
+def test_autotune_selects_a_variant_and_keeps_the_state(cuda, tmp_path, monkeypatch):
+    """jfb_kmm_autotune times the plan's kernel variants on copies of the
+    loaded state: the state is unchanged afterwards, the chosen variant is
+    active and accepted by the plan, and a second call reads the cache."""
+    monkeypatch.setenv("JFB200_AUTOTUNE_CACHE", str(tmp_path / "autotune.json"))
+    kw = dict(N=(33, 32, 32), Re=1000.0, dt=0.01, perturbation_amplitude=0.02, device=cuda)
+    ref_solver = PlaneCouetteFluctuation(**kw)
+    s0 = ref_solver.initial_state()
+    ref = ref_solver.solve(s0, 6)
+    g = PlaneCouetteFluctuation(**kw)
+    res = g.autotune(s0, steps=5)
+    assert res["ms_per_step"] > 0 and not res["cached"]
+    assert g.variant()["current"] == res["variant"]
+    out = g.solve(s0, 6)  # every variant of the FP64 form agrees to round-off
+    for x, y in zip((*out.u, out.g), (*ref.u, ref.g), strict=True):
+        assert rel(x, y.cpu().numpy()) < 1e-12
+    again = g.autotune(s0, steps=5)
+    assert again["cached"] and again["variant"] == res["variant"]
+    with pytest.raises(Exception):
+        g.set_variant(replicas=99)
