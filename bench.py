@@ -598,7 +598,7 @@ def main(argv=None):
         wall-normal sizes cycling 33, 49, 65 x 64 x 64 Fourier modes, Re = Rm
         = 1000, imposed field B0 = 0.1 e_z, base flow U_b = x, seeded
         divergence-free perturbations of u and b (energies 1e-4 each), FP64;
-        one CUDA graph per ensemble step with every member on its own stream."""
+        one CUDA graph per ensemble step."""
         from jaxfun_b200.mhd import Ensemble, MHDState, PlaneCouetteMRIShearpy
 
         sizes = (33, 49, 65)
@@ -628,8 +628,32 @@ def main(argv=None):
         e1.record(stream)
         torch.cuda.synchronize(dev)
         ms_step = e0.elapsed_time(e1) / K
-        launches = sum(m.info().launches_per_step for m in members)
+        launches = ens.launches_per_step
         diags = [m.diagnostics(m._fetch_mhd(2.0)) for m in members[:3]]
+
+        def other_form(mode):
+            """The same members with JFB200_ENSEMBLE=mode: ms per ensemble step."""
+            os.environ["JFB200_ENSEMBLE"] = mode
+            try:
+                ens_o = Ensemble(members)
+            finally:
+                del os.environ["JFB200_ENSEMBLE"]
+            ens_o.load(states)
+            ens_o.advance_resident(2 + max(3, args.warmup))
+            torch.cuda.synchronize(dev)
+            e0.record(stream)
+            ens_o.advance_resident(K)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            return {"ms_per_ensemble_step": e0.elapsed_time(e1) / K,
+                    "gpu_launches_per_step": ens_o.launches_per_step}
+
+        # the other forms: every member on its own stream (the form of plans
+        # that cannot batch) and all members in one group
+        others = {}
+        if ens.batched:
+            others = {"one_stream_per_member": other_form("streams"),
+                      "one_group": other_form("batched")}
         # stage model of one MHD member step (FP64): (91 E_s + 36 E_m) x 16 B
         step_bytes = 0
         for m in members:
@@ -647,7 +671,11 @@ def main(argv=None):
             "member_steps_per_s": len(members) * 1000.0 / ms_step,
             "steps": K,
             "gpu_launches_per_step": launches,
-            "launch": "one CUDA graph per ensemble step, one stream per member",
+            "other_forms": others,
+            "launch": ("one CUDA graph per ensemble step: five launches per wall-normal size, "
+                       "one per stage over that size's members' tiles, the sizes on parallel "
+                       "branches" if ens.batched else
+                       "one CUDA graph per ensemble step, one stream per member"),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
                          "algorithmic_bytes_per_ensemble_step": step_bytes},

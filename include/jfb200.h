@@ -97,12 +97,19 @@ int jfb_wavenumber_solve(const double* L, const int64_t* L_offsets, int64_t n_L,
 #define JFB_PRECISION_FP64 0
 #define JFB_PRECISION_MIXED 1
 #define JFB_NONLINEAR_ROTATIONAL 0
+/* time integrators of KMM.step (channelflow_kmm.py:937-1192): SBDF3 with an
+ * IMEXRK3 startup (sbdf3.py:15-62), the three-stage IMEXRK3 every step
+ * (imex_rk.py:96-125, channelflow_kmm.py:872-935), the two-stage ARS
+ * IMEXRK222 (imex_rk.py:175-198, integrators/coupled.py:13-44) */
+#define JFB_INTEGRATOR_SBDF3 0
+#define JFB_INTEGRATOR_IMEXRK3 1
+#define JFB_INTEGRATOR_IMEXRK222 2
 
 /* Constructor arguments of KMM / PlaneCouetteFluctuationJax
  * (examples/channelflow_kmm.py:107-230, examples/pcf_fluctuations_jax.py:35-75)
- * restricted to the hot path: Chebyshev family, x unpadded, SBDF3 with an
- * IMEXRK3 startup, rotational nonlinear form.  u_wall = 0 gives the plain
- * KMM channel (no base flow). */
+ * restricted to the hot path: Chebyshev family, x unpadded, rotational
+ * nonlinear form, the time integrators above (MHD plans and the adjoint:
+ * SBDF3).  u_wall = 0 gives the plain KMM channel (no base flow). */
 typedef struct jfb_kmm_config {
   int32_t nx, ny, nz;     /* N = (wall-normal orthogonal size, Fourier y, z) */
   int32_t family;         /* JFB_FAMILY_CHEBYSHEV                           */
@@ -114,6 +121,7 @@ typedef struct jfb_kmm_config {
   double u_wall;          /* base flow U_b(x) = u_wall * x                  */
   int32_t precision;      /* JFB_PRECISION_FP64 or JFB_PRECISION_MIXED      */
   int32_t nonlinear_form; /* JFB_NONLINEAR_ROTATIONAL                       */
+  int32_t time_integrator; /* JFB_INTEGRATOR_* (0: SBDF3)                   */
 } jfb_kmm_config;
 
 /* Device pointers to a KMMState in the reference layout
@@ -433,15 +441,23 @@ int jfb_helmholtz2d_solve(const jfb_tps* tc, const jfb_tps* td, const double* L,
 /* ---- ensembles ------------------------------------------------------------ */
 
 /* Independent members (flow or MHD plans, any sizes; no reference counterpart:
- * the reference runs members one solver at a time) advanced together.  Each
- * steady step is one CUDA graph holding every member's step on its own
- * stream, so members of uneven wall-normal size run concurrently.  Members
- * keep their own states (jfb_kmm_set_state / jfb_mhd_set_state, get_state);
- * all must share the step phase and history count when advanced.  Destroy
- * the ensemble before its members. */
+ * the reference runs members one solver at a time, pcf_mhd_mri_shearpy_jax.py
+ * / pcf_mhd_jax.py:563-715 per member) advanced together, one CUDA graph per
+ * steady step.  When every member is an MHD plan on the tensor-core pencil
+ * stage with warp-FFT y transforms of one length (up to 64 members of any
+ * wall-normal size), the step is FIVE launches, one per stage over all
+ * members' tiles (a work list; JFB200_ENSEMBLE=streams disables it);
+ * otherwise every member's step runs on its own stream.  Both forms give
+ * bitwise the results of the members' own plans.  Members keep their own
+ * states (jfb_kmm_set_state / jfb_mhd_set_state, get_state); all must share
+ * the step phase and history count when advanced.  Destroy the ensemble
+ * before its members. */
 typedef struct jfb_ensemble jfb_ensemble;
 int jfb_ensemble_create(jfb_kmm_plan* const* plans, int32_t n, jfb_ensemble** ensemble);
 int jfb_ensemble_advance(jfb_ensemble* ensemble, int64_t steps, void* stream);
+/* *batched = 1 for the five-launch form; *launches_per_step = kernels per
+ * steady step of the whole ensemble (either may be NULL). */
+int jfb_ensemble_info(const jfb_ensemble* ensemble, int32_t* batched, int64_t* launches_per_step);
 int jfb_ensemble_destroy(jfb_ensemble* ensemble);
 
 #ifdef __cplusplus

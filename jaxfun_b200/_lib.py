@@ -28,6 +28,9 @@ JFB_FAMILY_CHEBYSHEV = 0
 JFB_PRECISION_FP64 = 0
 JFB_PRECISION_MIXED = 1
 JFB_NONLINEAR_ROTATIONAL = 0
+JFB_INTEGRATOR_SBDF3 = 0
+JFB_INTEGRATOR_IMEXRK3 = 1
+JFB_INTEGRATOR_IMEXRK222 = 2
 JFB_BASIS_ORTHOGONAL = 0
 JFB_BASIS_DIRICHLET = 1
 JFB_BASIS_BIHARMONIC = 2
@@ -53,6 +56,7 @@ class KMMConfig(ctypes.Structure):
         ("u_wall", c_double),
         ("precision", c_int32),
         ("nonlinear_form", c_int32),
+        ("time_integrator", c_int32),
     ]
 
 
@@ -208,6 +212,7 @@ SIGNATURES = {
                                        c_void_p, c_void_p, c_void_p]),
     "jfb_ensemble_create": (c_int, [POINTER(c_void_p), c_int32, POINTER(c_void_p)]),
     "jfb_ensemble_advance": (c_int, [c_void_p, c_int64, c_void_p]),
+    "jfb_ensemble_info": (c_int, [c_void_p, POINTER(c_int32), POINTER(c_int64)]),
     "jfb_ensemble_destroy": (c_int, [c_void_p]),
     "jfb_mhd_set_state": (c_int, [c_void_p, POINTER(MHDStateC), c_void_p]),
     "jfb_mhd_get_state": (c_int, [c_void_p, POINTER(MHDStateC), c_void_p]),

@@ -20,6 +20,7 @@
 #include "jfb_kmm_gemm.cuh"
 #include "jfb_kmm_mhd.cuh"
 #include "jfb_kmm_adjoint.cuh"
+#include "jfb_kmm_ens.cuh"
 
 #ifdef JFB_PHASE_STAMPS
 // Copies the phase stamps (kernel 0: pencil_gemm_kernel, 1: plane_cross_kernel;
@@ -38,6 +39,10 @@ namespace jfb {
 static const double kRK3A[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
 static const double kRK3B[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
 static const double kSBDF3Implicit = 6.0 / 11.0;  // integrators/sbdf3.py:11-12
+// ARS IMEXRK222 (imex_rk.py:175-198): implicit diagonal g, explicit weights
+// b10 = g, (b20, b21) = (d, 1 - d), explicit linear weight a21 = 1 - g
+static const double kG222 = (2.0 - 1.4142135623730950488) / 2.0;
+static const double kD222 = 1.0 - 1.0 / (2.0 * kG222);
 
 // ---------------------------------------------------------------------------
 // set-up kernels
@@ -230,6 +235,7 @@ struct jfb_kmm_plan {
   int64_t device_bytes = 0;
   int* status = nullptr;  // device status word (kStatus* bits), read by jfb_kmm_check
   jfb::FactorSet steady, startup[3];
+  jfb::FactorSet rk222;  // IMEXRK222 plans: the factors of gamma = g dt
   jfb::c64 *U0[3], *G[3], *NU[3], *NG[3], *VW[3], *NVW[3];
   jfb::c64 *NUst, *NGst, *NVWst;
   jfb::c64 *U1S, *U2S;
@@ -525,15 +531,8 @@ static int launch_pencil(jfb_kmm_plan* pl, const StageArgs& a0, cudaStream_t s) 
   return JFB_OK;
 }
 
-// One implicit stage (mode kImplicit): the tensor-core pencil stage when the
-// plan has it, else the warp-per-pencil kernel.
-static int launch_implicit(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s) {
-  if (!pl->gemm) {
-    StageArgs b = a;
-    b.x32 = pl->mixed ? 1 : 0;
-    b.Xlin = pl->mixed ? reinterpret_cast<const c32*>(pl->X) : nullptr;
-    return launch_pencil(pl, b, s);
-  }
+// The tensor-core pencil stage's arguments of one implicit stage.
+static GemmStageArgs gemm_args(const jfb_kmm_plan* pl, const StageArgs& a) {
   GemmStageArgs g;
   g.HX = a.HX;
   g.c0 = a.c0;
@@ -573,6 +572,19 @@ static int launch_implicit(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s)
   g.X = a.X;
   g.x32 = pl->mixed ? 1 : 0;
   g.Xlin = pl->mixed ? reinterpret_cast<const c32*>(pl->X) : nullptr;
+  return g;
+}
+
+// One implicit stage (mode kImplicit): the tensor-core pencil stage when the
+// plan has it, else the warp-per-pencil kernel.
+static int launch_implicit(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s) {
+  if (!pl->gemm) {
+    StageArgs b = a;
+    b.x32 = pl->mixed ? 1 : 0;
+    b.Xlin = pl->mixed ? reinterpret_cast<const c32*>(pl->X) : nullptr;
+    return launch_pencil(pl, b, s);
+  }
+  const GemmStageArgs g = gemm_args(pl, a);
   const int blocks = (pl->d.Ny / 2) * ceil_div(pl->d.Kz, 8);
   JFB_CHECK_CUDA(launch_ex(pl->pdl, pencil_gemm_kernel, dim3(blocks), dim3(kGThreads),
                            pl->smem_gemm, s, pl->d, pl->ops, pl->gops, g));
@@ -820,9 +832,10 @@ static int ensure_H(jfb_kmm_plan* pl, cudaStream_t s) {
   return JFB_OK;
 }
 
-// One steady SBDF3 step from ring position m (u^m in slot m % 3).
-static int steady_step(jfb_kmm_plan* pl, int64_t m, cudaStream_t s) {
-  StageArgs a = blank_args();
+// Arguments of the pencil stage (a) and, for an MHD plan, of the A stage
+// (mm) of one steady SBDF3 step from ring position m (u^m in slot m % 3).
+static void steady_args(jfb_kmm_plan* pl, int64_t m, StageArgs& a, MhdArgs& mm) {
+  a = blank_args();
   a.mode = kImplicit;
   a.HX = pl->HX;
   const int c = slot(m), o1 = slot(m - 1), o2 = slot(m - 2), nw = slot(m + 1);
@@ -856,30 +869,38 @@ static int steady_step(jfb_kmm_plan* pl, int64_t m, cudaStream_t s) {
   a.g_out = pl->G[nw];
   a.vw_out = pl->VW[nw];
   a.X = pl->X;
+  mm = blank_mhd();
+  if (pl->mhd) {
+    mm.mode = kMhdStep;
+    mm.HXA = pl->HX + (size_t)3 * pl->d.Nx * pl->d.P;
+    mm.c0 = a.c0;
+    mm.c1 = a.c1;
+    mm.c2 = a.c2;
+    mm.d0 = a.d0;
+    mm.d1 = a.d1;
+    mm.d2 = a.d2;
+    mm.Aa = pl->AR[c];
+    mm.Ab = pl->AR[o1];
+    mm.Ac = pl->AR[o2];
+    mm.NAp = pl->NA[o1];
+    mm.NAq = pl->NA[o2];
+    mm.NA_out = pl->NA[c];
+    mm.sa = pl->sa_steady;
+    mm.sa_rec = pl->sg_rec;
+    mm.A_out = pl->AR[nw];
+    mm.XB = pl->X + (size_t)6 * pl->d.Nx * pl->d.P;
+    mm.status = pl->status;
+  }
+}
+
+// One steady SBDF3 step from ring position m (u^m in slot m % 3).
+static int steady_step(jfb_kmm_plan* pl, int64_t m, cudaStream_t s) {
+  StageArgs a;
+  MhdArgs mm;
+  steady_args(pl, m, a, mm);
   int st = launch_implicit(pl, a, s);
   if (st) return st;
-  if (pl->mhd) {
-    MhdArgs m = blank_mhd();
-    m.mode = kMhdStep;
-    m.HXA = pl->HX + (size_t)3 * pl->d.Nx * pl->d.P;
-    m.c0 = a.c0;
-    m.c1 = a.c1;
-    m.c2 = a.c2;
-    m.d0 = a.d0;
-    m.d1 = a.d1;
-    m.d2 = a.d2;
-    m.Aa = pl->AR[c];
-    m.Ab = pl->AR[o1];
-    m.Ac = pl->AR[o2];
-    m.NAp = pl->NA[o1];
-    m.NAq = pl->NA[o2];
-    m.NA_out = pl->NA[c];
-    m.sa = pl->sa_steady;
-    m.sa_rec = pl->sg_rec;
-    m.A_out = pl->AR[nw];
-    m.XB = pl->X + (size_t)6 * pl->d.Nx * pl->d.P;
-    if ((st = launch_mhd(pl, m, s))) return st;
-  }
+  if (pl->mhd && (st = launch_mhd(pl, mm, s))) return st;
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[1], s));
   return launch_transforms(pl, s);
 }
@@ -970,6 +991,68 @@ static int startup_step(jfb_kmm_plan* pl, cudaStream_t s, c64* const* rec = null
   return JFB_OK;
 }
 
+// One IMEXRK222 step from ring position m (channelflow_kmm.py:1137-1192,
+// integrators/coupled.py:13-44): stage 1 solves
+//   M u1 - g dt L u1 = M u^n + dt g N(u^n)
+// into the ring slot m - 1 (no history is kept by this integrator), stage 2
+//   M u' - g dt L u' = M u^n + dt (d N(u^n) + (1 - d) N(u1)) + dt (1 - g) L u1
+// into slot m + 1; each stage is followed by the transforms of its result.
+static int imexrk222_step(jfb_kmm_plan* pl, int64_t m, cudaStream_t s) {
+  const int c = slot(m), t1 = slot(m - 1), nw = slot(m + 1);
+  StageArgs a = blank_args();
+  a.mode = kImplicit;
+  a.HX = pl->HX;
+  a.c0 = 1.0;
+  a.d0 = kG222;
+  a.u0a = pl->U0[c];
+  a.ga = pl->G[c];
+  a.vwa = pl->VW[c];
+  a.Nu_out = pl->NU[c];
+  a.Ng_out = pl->NG[c];
+  a.NVW_out = pl->NVW[c];
+  a.fac = packed(pl, pl->rk222);
+  a.u0_out = pl->U0[t1];
+  a.g_out = pl->G[t1];
+  a.vw_out = pl->VW[t1];
+  a.X = pl->X;
+  int st = launch_implicit(pl, a, s);
+  if (st || (st = launch_transforms(pl, s))) return st;
+  StageArgs b = blank_args();
+  b.mode = kImplicit;
+  b.HX = pl->HX;
+  b.c0 = 0.0;  // the linear term acts on u1 (level a), the mass on u^n (level b)
+  b.c1 = 1.0;
+  b.cL = (1.0 - kG222) * pl->cfg.dt;
+  b.d0 = 1.0 - kD222;
+  b.d1 = kD222;
+  b.u0a = pl->U0[t1];
+  b.ga = pl->G[t1];
+  b.vwa = pl->VW[t1];
+  b.u0b = pl->U0[c];
+  b.gb = pl->G[c];
+  b.vwb = pl->VW[c];
+  b.Nup = pl->NU[c];
+  b.Ngp = pl->NG[c];
+  b.NVWp = pl->NVW[c];
+  b.fac = packed(pl, pl->rk222);
+  b.u0_out = pl->U0[nw];
+  b.g_out = pl->G[nw];
+  b.vw_out = pl->VW[nw];
+  b.X = pl->X;
+  if ((st = launch_implicit(pl, b, s))) return st;
+  return launch_transforms(pl, s);
+}
+
+// One step of the plan's integrator once past the SBDF3 startup (the body
+// of the captured step graphs).
+static int graph_step(jfb_kmm_plan* pl, int64_t m, cudaStream_t s) {
+  switch (pl->cfg.time_integrator) {
+    case JFB_INTEGRATOR_IMEXRK3: return startup_step(pl, s);
+    case JFB_INTEGRATOR_IMEXRK222: return imexrk222_step(pl, m, s);
+    default: return steady_step(pl, m, s);
+  }
+}
+
 static void destroy_graphs(jfb_kmm_plan* pl) {
   for (int k = 0; k < 3; ++k)
     if (pl->graph[k]) {
@@ -991,6 +1074,11 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
               "only the rotational nonlinear form is supported");
   JFB_REQUIRE(cfg->precision == JFB_PRECISION_FP64 || cfg->precision == JFB_PRECISION_MIXED,
               "precision must be JFB_PRECISION_FP64 or JFB_PRECISION_MIXED");
+  JFB_REQUIRE(cfg->time_integrator >= JFB_INTEGRATOR_SBDF3 &&
+                  cfg->time_integrator <= JFB_INTEGRATOR_IMEXRK222,
+              "time_integrator must be SBDF3, IMEXRK3 or IMEXRK222");
+  JFB_REQUIRE(!mhd || cfg->time_integrator == JFB_INTEGRATOR_SBDF3,
+              "the MHD step is SBDF3 (with its IMEXRK3 startup) only");
   JFB_REQUIRE(cfg->nx >= 9 && cfg->nx <= 64 * kMaxNR + 1, "nx out of range [9, 129]");
   JFB_REQUIRE(cfg->ny >= 4 && cfg->ny % 2 == 0 && cfg->nz >= 4 && cfg->nz % 2 == 0,
               "ny, nz must be even");
@@ -1344,6 +1432,19 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
         G.oTB = (int)oTB;
         pl->tc_ok = true;
       }
+      // forward-elimination multipliers of the tile's modes, staged at the
+      // start of phase C below the right-hand-side rows and above whatever
+      // the velocity-operator copy of either variant writes
+      {
+        const size_t vel_end = std::max(
+            oTA + (gh.frag.size() - (size_t)gh.off[gA0Ee]) * sizeof(double),
+            pl->tc_ok ? oTA + (size_t)kTcImgA : (size_t)0);
+        const size_t lbytes = (size_t)8 * 2 * (d.nB + d.nD) * sizeof(double);
+        const size_t top = (size_t)G.oRU * kGLd * sizeof(double);
+        G.oL = -1;
+        if (top >= lbytes && (top - lbytes) / 16 * 16 >= vel_end)
+          G.oL = (int)((top - lbytes) / 16 * 16 / sizeof(double));
+      }
     }
     pl->gemm = pl->gemm_ok && want;
   }
@@ -1383,6 +1484,10 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   for (int rk = 0; rk < 3; ++rk) {
     st = build_factor_set(pl, (kRK3A[rk] + kRK3B[rk]) * cfg->dt / 2.0, pl->startup[rk],
                           cfg->nu, 0, 2, true);
+    if (st) return fail(st);
+  }
+  if (cfg->time_integrator == JFB_INTEGRATOR_IMEXRK222) {
+    st = build_factor_set(pl, kG222 * cfg->dt, pl->rk222, cfg->nu, 0, 2, true);
     if (st) return fail(st);
   }
   if (pl->mhd) {
@@ -1573,7 +1678,9 @@ extern "C" int jfb_kmm_advance(jfb_kmm_plan* pl, int64_t steps, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   int st = ensure_H(pl, s);
   if (st) return st;
-  while (steps > 0 && pl->hist < 2) {
+  // SBDF3: IMEXRK3 startup steps until two history levels exist; the
+  // one-step integrators keep no history
+  while (steps > 0 && pl->hist < 2 && pl->cfg.time_integrator == JFB_INTEGRATOR_SBDF3) {
     st = startup_step(pl, s);
     if (st) return st;
     pl->n += 1;
@@ -1584,13 +1691,13 @@ extern "C" int jfb_kmm_advance(jfb_kmm_plan* pl, int64_t steps, void* stream) {
   while (steps > 0) {
     const int k = slot(pl->n);
     if (!pl->graph[k]) {
-      // Capture one steady step for ring phase k on the private stream; the
+      // Capture one step for ring phase k on the private stream; the
       // instantiated graph is then launched on the caller's stream (which
       // may be the legacy default stream, where capture is not allowed).
       if (!pl->cap) JFB_CHECK_CUDA(cudaStreamCreateWithFlags(&pl->cap, cudaStreamNonBlocking));
       cudaGraph_t g;
       JFB_CHECK_CUDA(cudaStreamBeginCapture(pl->cap, cudaStreamCaptureModeThreadLocal));
-      st = steady_step(pl, pl->n, pl->cap);
+      st = graph_step(pl, pl->n, pl->cap);
       cudaError_t ec = cudaStreamEndCapture(pl->cap, &g);
       if (st) return st;
       JFB_CHECK_CUDA(ec);
@@ -1739,6 +1846,7 @@ extern "C" int jfb_kmm_timed_steps(jfb_kmm_plan* pl, int64_t steps, void* flush_
                                    int64_t flush_bytes, double* kernel_ms, double* step_ms,
                                    void* stream) {
   JFB_REQUIRE(pl && kernel_ms && step_ms, "null pointer");
+  JFB_REQUIRE(pl->cfg.time_integrator == JFB_INTEGRATOR_SBDF3, "timed steps: SBDF3 plans");
   JFB_REQUIRE(steps >= 0, "steps must be >= 0");
   if (!pl->have_state) {
     set_error("no state loaded");
@@ -2311,6 +2419,8 @@ static int record_state(jfb_kmm_plan* pl, AdjRun& R, int slot_idx, cudaStream_t 
 extern "C" int jfb_kmm_gain_gradient(jfb_kmm_plan* pl, const jfb_kmm_state* init, int64_t steps,
                                      int64_t checkpoint, double* gain_out,
                                      const jfb_kmm_state* grad, void* stream) {
+  JFB_REQUIRE(pl && pl->cfg.time_integrator == JFB_INTEGRATOR_SBDF3,
+              "the adjoint differentiates the SBDF3 step");
   JFB_REQUIRE(pl && init && gain_out, "null pointer");
   JFB_REQUIRE(!pl->mhd && !pl->mixed, "the adjoint runs on FP64 flow plans");
   JFB_REQUIRE(steps >= 1, "steps must be >= 1");
@@ -2717,6 +2827,15 @@ extern "C" int jfb_kmm_autotune(jfb_kmm_plan* pl, int64_t steps, jfb_kmm_variant
   return JFB_OK;
 }
 
+// A set of ensemble members whose five stages run as one launch each.
+struct EnsGroup {
+  std::vector<int> order;  // member indices, in work-list order
+  jfb::EnsTiles htiles;
+  jfb::EnsTiles* tiles = nullptr;                         // device copy of htiles
+  jfb::EnsMember* tab[3] = {nullptr, nullptr, nullptr};  // per ring phase
+  size_t smem[5] = {0, 0, 0, 0, 0};
+};
+
 struct jfb_ensemble {
   std::vector<jfb_kmm_plan*> m;
   std::vector<cudaStream_t> streams;
@@ -2724,12 +2843,128 @@ struct jfb_ensemble {
   cudaStream_t cap = nullptr;
   cudaEvent_t fork = nullptr;
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  // batched form: five launches per steady step for each group of members
+  // (one group per wall-normal size, or one for all), the groups on
+  // parallel branches of the step graph
+  bool batched = false;
+  int py = 0;
+  std::vector<EnsGroup> groups;
 };
+
+namespace jfb {
+
+// Every member an MHD plan on the tensor-core pencil stage with warp-FFT y
+// transforms of one length: then the five stages batch across members.
+static bool ensemble_batchable(const jfb_ensemble* e) {
+  const char* env = std::getenv("JFB200_ENSEMBLE");
+  if (env && std::string(env) == "streams") return false;
+  if (e->m.size() > (size_t)kEnsMax) return false;
+  for (const jfb_kmm_plan* pl : e->m)
+    if (!pl->mhd || !pl->gemm || pl->py == 0 || pl->py != e->m[0]->py || pl->mixed) return false;
+  return true;
+}
+
+template <int P>
+static cudaError_t ens_y_launch(const EnsGroup& G, const EnsMember* tab, bool backward,
+                                cudaStream_t s) {
+  const int stage = backward ? 2 : 4;
+  const int blocks = G.htiles.first[stage][G.htiles.nm];
+  if (backward)
+    ens_y_backward_kernel<P><<<blocks, 256, G.smem[2], s>>>(tab, G.tiles);
+  else
+    ens_y_forward_kernel<P><<<blocks, 256, G.smem[4], s>>>(tab, G.tiles);
+  return cudaGetLastError();
+}
+
+// The five launches of one group's steady step with ring-phase table `tab`.
+static int ensemble_group_step(const jfb_ensemble* e, const EnsGroup& G, const EnsMember* tab,
+                               cudaStream_t s) {
+  const EnsTiles& T = G.htiles;
+  ens_pencil_kernel<<<T.first[0][T.nm], kGThreads, G.smem[0], s>>>(tab, G.tiles);
+  JFB_CHECK_LAUNCH();
+  ens_mhd_a_kernel<<<T.first[1][T.nm], kMhdThreads, G.smem[1], s>>>(tab, G.tiles);
+  JFB_CHECK_LAUNCH();
+  cudaError_t ce;
+  switch (e->py) {
+    case 2: ce = ens_y_launch<2>(G, tab, true, s); break;
+    case 3: ce = ens_y_launch<3>(G, tab, true, s); break;
+    case 4: ce = ens_y_launch<4>(G, tab, true, s); break;
+    default: ce = ens_y_launch<6>(G, tab, true, s); break;
+  }
+  JFB_CHECK_CUDA(ce);
+  ens_z_cross_kernel<<<T.first[3][T.nm], 256, G.smem[3], s>>>(tab, G.tiles);
+  JFB_CHECK_LAUNCH();
+  switch (e->py) {
+    case 2: ce = ens_y_launch<2>(G, tab, false, s); break;
+    case 3: ce = ens_y_launch<3>(G, tab, false, s); break;
+    case 4: ce = ens_y_launch<4>(G, tab, false, s); break;
+    default: ce = ens_y_launch<6>(G, tab, false, s); break;
+  }
+  JFB_CHECK_CUDA(ce);
+  return JFB_OK;
+}
+
+// Device table of a group's members' steady-step arguments for ring phase k.
+static int ensemble_table(jfb_ensemble* e, EnsGroup& G, int k) {
+  if (G.tab[k]) return JFB_OK;
+  std::vector<EnsMember> h(G.order.size());
+  for (size_t i = 0; i < G.order.size(); ++i) {
+    jfb_kmm_plan* pl = e->m[G.order[i]];
+    StageArgs a;
+    MhdArgs mm;
+    steady_args(pl, pl->n, a, mm);
+    EnsMember& x = h[i];
+    std::memset(&x, 0, sizeof(x));
+    x.d = pl->d;
+    x.o = pl->ops;
+    x.G = pl->gops;
+    x.ga = gemm_args(pl, a);
+    x.M = pl->mops;
+    x.ma = mm;
+    x.ph = pl->mphys;
+    x.fz = pl->fz;
+    x.twy = pl->twy;
+    x.twz = pl->twz;
+    x.X = pl->X;
+    x.Y = pl->Y;
+    x.HZ = pl->HZ;
+    x.HX = pl->HX;
+    x.xb = pl->ops.xphys;
+    x.KCw = pl->KCw;
+    x.chunks = ceil_div(pl->d.Kz, pl->KCw);
+  }
+  JFB_CHECK_CUDA(cudaMalloc((void**)&G.tab[k], h.size() * sizeof(EnsMember)));
+  JFB_CHECK_CUDA(cudaMemcpy(G.tab[k], h.data(), h.size() * sizeof(EnsMember),
+                            cudaMemcpyHostToDevice));
+  return JFB_OK;
+}
+
+// One steady step of a batched ensemble: the groups fork from the capture
+// stream onto their own streams and join back.
+static int ensemble_batched_step(jfb_ensemble* e, int k, cudaStream_t cap) {
+  JFB_CHECK_CUDA(cudaEventRecord(e->fork, cap));
+  for (size_t gi = 0; gi < e->groups.size(); ++gi) {
+    cudaStream_t s = e->streams[gi];
+    JFB_CHECK_CUDA(cudaStreamWaitEvent(s, e->fork, 0));
+    int st = ensemble_group_step(e, e->groups[gi], e->groups[gi].tab[k], s);
+    if (st) return st;
+    JFB_CHECK_CUDA(cudaEventRecord(e->join[gi], s));
+    JFB_CHECK_CUDA(cudaStreamWaitEvent(cap, e->join[gi], 0));
+  }
+  return JFB_OK;
+}
+
+}  // namespace jfb
 
 extern "C" int jfb_ensemble_destroy(jfb_ensemble* e) {
   if (!e) return JFB_OK;
   for (auto& g : e->graph)
     if (g) cudaGraphExecDestroy(g);
+  for (EnsGroup& G : e->groups) {
+    for (auto* t : G.tab)
+      if (t) cudaFree(t);
+    if (G.tiles) cudaFree(G.tiles);
+  }
   for (cudaStream_t s : e->streams) cudaStreamDestroy(s);
   for (cudaEvent_t ev : e->join) cudaEventDestroy(ev);
   if (e->fork) cudaEventDestroy(e->fork);
@@ -2742,6 +2977,9 @@ extern "C" int jfb_ensemble_create(jfb_kmm_plan* const* plans, int32_t n, jfb_en
   JFB_REQUIRE(plans && out && n >= 1, "null pointer or empty ensemble");
   *out = nullptr;
   for (int i = 0; i < n; ++i) JFB_REQUIRE(plans[i], "null member plan");
+  for (int i = 0; i < n; ++i)
+    JFB_REQUIRE(plans[i]->cfg.time_integrator == JFB_INTEGRATOR_SBDF3,
+                "ensemble members step with SBDF3");
   jfb_ensemble* e = new jfb_ensemble();
   e->m.assign(plans, plans + n);
   auto fail = [&](cudaError_t err) {
@@ -2760,7 +2998,68 @@ extern "C" int jfb_ensemble_create(jfb_kmm_plan* const* plans, int32_t n, jfb_en
     if ((err = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming)) != cudaSuccess)
       return fail(err);
   }
+  e->batched = ensemble_batchable(e);
+  if (e->batched) {
+    e->py = e->m[0]->py;
+    // one group per wall-normal size (its launches use that size's shared
+    // memory and run beside the other sizes'), or JFB200_ENSEMBLE=batched:
+    // a single group, largest members first
+    const char* env = std::getenv("JFB200_ENSEMBLE");
+    const bool single = env && std::string(env) == "batched";
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(),
+                     [&](int a, int b) { return e->m[a]->d.Nx > e->m[b]->d.Nx; });
+    for (int i : idx) {
+      if (e->groups.empty() ||
+          (!single && e->m[e->groups.back().order.back()]->d.Nx != e->m[i]->d.Nx))
+        e->groups.emplace_back();
+      e->groups.back().order.push_back(i);
+    }
+    for (EnsGroup& G : e->groups) {
+      EnsTiles& T = G.htiles;
+      std::memset(&T, 0, sizeof(T));
+      T.nm = (int)G.order.size();
+      for (int q = 0; q < T.nm; ++q) {
+        const jfb_kmm_plan* pl = e->m[G.order[q]];
+        const Dims& d = pl->d;
+        const int chunks = ceil_div(d.Kz, pl->KCw);
+        const int t[5] = {(d.Ny / 2) * ceil_div(d.Kz, 8), (d.Ny / 2) * ceil_div(d.Kz, 8),
+                          d.Nx * 12 * chunks, ceil_div((int64_t)d.Nx * d.My, kZRows),
+                          d.Nx * 6 * chunks};
+        const size_t sm[5] = {pl->smem_gemm, pl->smem_mhd, pl->smem_yw_b, pl->smem_zm,
+                              pl->smem_yw_f};
+        for (int st = 0; st < 5; ++st) {
+          T.first[st][q + 1] = T.first[st][q] + t[st];
+          G.smem[st] = std::max(G.smem[st], sm[st]);
+        }
+      }
+      if ((err = cudaMalloc((void**)&G.tiles, sizeof(EnsTiles))) != cudaSuccess) return fail(err);
+      if ((err = cudaMemcpy(G.tiles, &T, sizeof(EnsTiles), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(err);
+    }
+    const void* fns[] = {(const void*)ens_pencil_kernel, (const void*)ens_mhd_a_kernel,
+                         (const void*)ens_z_cross_kernel,
+                         (const void*)ens_y_backward_kernel<2>, (const void*)ens_y_forward_kernel<2>,
+                         (const void*)ens_y_backward_kernel<3>, (const void*)ens_y_forward_kernel<3>,
+                         (const void*)ens_y_backward_kernel<4>, (const void*)ens_y_forward_kernel<4>,
+                         (const void*)ens_y_backward_kernel<6>, (const void*)ens_y_forward_kernel<6>};
+    for (const void* f : fns)
+      if ((err = allow_smem(f)) != cudaSuccess) return fail(err);
+  }
   *out = e;
+  return JFB_OK;
+}
+
+extern "C" int jfb_ensemble_info(const jfb_ensemble* e, int32_t* batched,
+                                 int64_t* launches_per_step) {
+  JFB_REQUIRE(e, "null pointer");
+  if (batched) *batched = e->batched ? 1 : 0;
+  if (launches_per_step) {
+    int64_t n = 0;
+    for (const jfb_kmm_plan* pl : e->m) n += pl->mhd ? 5 : pl->plane ? 2 : 4;
+    *launches_per_step = e->batched ? 5 * (int64_t)e->groups.size() : n;
+  }
   return JFB_OK;
 }
 
@@ -2793,6 +3092,20 @@ extern "C" int jfb_ensemble_advance(jfb_ensemble* e, int64_t steps, void* stream
   }
   while (steps > 0) {
     const int k = slot(e->m[0]->n);
+    if (!e->graph[k] && e->batched) {
+      // five launches per group; the member tables of this ring phase are
+      // built (with blocking copies) before the capture
+      for (EnsGroup& G : e->groups)
+        if ((st = ensemble_table(e, G, k))) return st;
+      cudaGraph_t g;
+      JFB_CHECK_CUDA(cudaStreamBeginCapture(e->cap, cudaStreamCaptureModeThreadLocal));
+      st = ensemble_batched_step(e, k, e->cap);
+      cudaError_t ec = cudaStreamEndCapture(e->cap, &g);
+      if (st) return st;
+      JFB_CHECK_CUDA(ec);
+      JFB_CHECK_CUDA(cudaGraphInstantiate(&e->graph[k], g, 0));
+      cudaGraphDestroy(g);
+    }
     if (!e->graph[k]) {
       cudaGraph_t g;
       JFB_CHECK_CUDA(cudaStreamBeginCapture(e->cap, cudaStreamCaptureModeThreadLocal));

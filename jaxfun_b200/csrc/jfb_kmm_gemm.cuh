@@ -65,6 +65,10 @@ struct GemmOps {
   int tc;
   const unsigned char* vimg;
   int oTA, oTB;
+  // forward-elimination multipliers of the tile's wavenumbers, staged into
+  // dead shared memory at the start of phase C (first double; -1: read from
+  // L2 instead)
+  int oL;
 };
 
 // Tensor-core velocity stage: three product groups of M = 128 rows (four
@@ -303,6 +307,22 @@ __device__ __forceinline__ void forward_elim(const double* __restrict__ rec, int
   }
 }
 
+// forward_elim with the multipliers staged in shared memory (ls = the first
+// 2 n doubles of the record: L[i, i-2], L[i, i-4] for i = 0..n-1).
+__device__ __forceinline__ void forward_elim_smem(const double* ls, int par, int m, c64* y,
+                                                  int stride) {
+  c64 y1 = cmk(0.0, 0.0), y2 = y1;
+  for (int r = 0; r < m; ++r) {
+    const int i = 2 * r + par;
+    c64 v = y[r * stride];
+    v = v - ls[2 * i] * y1;
+    v = v - ls[2 * i + 1] * y2;
+    y[r * stride] = v;
+    y2 = y1;
+    y1 = v;
+  }
+}
+
 // Named barrier over `count` threads.
 __device__ __forceinline__ void bar_sync(int id, int count) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
@@ -404,8 +424,11 @@ __device__ __forceinline__ void mid_store(const Dims& d, const GemmStageArgs& a,
   }
 }
 
-__global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOps o, GemmOps G,
-                                                                   GemmStageArgs a) {
+// The pencil stage of one tile `bid` of `nbid` (the kernel below, or one
+// member's tile of the ensemble kernel in jfb_kmm_ens.cuh).
+__device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o, const GemmOps& G,
+                                                 const GemmStageArgs& a, const int bid,
+                                                 const int nbid) {
   extern __shared__ __align__(128) double sm[];
   __shared__ int s_p[kGW], s_mode[kGW];
   __shared__ double s_ky[kGW], s_kz[kGW];
@@ -415,12 +438,12 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t4 = lane & 3;
   const int nKc = (d.Kz + 7) / 8;
-  const int kyi = blockIdx.x / nKc, kz0 = (blockIdx.x % nKc) * 8;
+  const int kyi = bid / nKc, kz0 = (bid % nKc) * 8;
   const int nkz = min(8, d.Kz - kz0);  // valid kz columns per side
   const bool mean_cta = (kyi == 0 && kz0 == 0);
   const int N = d.Nx, Jh = G.Jh, Jl = G.Jl;
   const size_t P = (size_t)d.P;
-  const double* __restrict__ frag = G.frag + (size_t)(blockIdx.x % G.nrep) * G.nfrag;
+  const double* __restrict__ frag = G.frag + (size_t)(bid % G.nrep) * G.nfrag;
   c64* rowc = reinterpret_cast<c64*>(sm);  // row r, pencil w: rowc[r * LC + w]
   const int LC = kGLd / 2;
   const double sl = a.slin;
@@ -453,7 +476,7 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     prefetch_l2(a.sg + m0 * a.sg_rec, (size_t)nkz * a.sg_rec * sizeof(double));
   } else if (tid == 96) {
     // this CTA's share of its operator copy
-    const int users = (gridDim.x + G.nrep - 1) / G.nrep, slot = blockIdx.x / G.nrep;
+    const int users = (nbid + G.nrep - 1) / G.nrep, slot = bid / G.nrep;
     const int chunk = (G.nfrag + users - 1) / users;
     const int b0 = min(G.nfrag, slot * chunk), b1 = min(G.nfrag, b0 + chunk);
     if (b1 > b0) prefetch_l2(frag + b0, (size_t)(b1 - b0) * sizeof(double));
@@ -738,6 +761,23 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
       bulk_g2s(sm + (size_t)G.oVel * kGLd, frag + voff, bytes, &s_bar);
     }
   }
+  // the multipliers of the tile's (up to 8) wavenumbers: 8-byte copies by
+  // all threads, one latency instead of a chain of dependent chunk loads
+  double* Ls = sm + (G.oL >= 0 ? G.oL : 0);
+  if (G.oL >= 0) {
+    const int per = 2 * (d.nB + d.nD);  // doubles per mode: Su then Sg multipliers
+    for (int e = tid; e < 8 * per; e += kGThreads) {
+      const int md = e / per, k = e % per;
+      if (md >= nkz) continue;
+      const size_t mode = (size_t)kyi * d.Kz + kz0 + md;
+      const double* src = (k < 2 * d.nB) ? a.su + mode * a.su_rec + k
+                                         : a.sg + mode * a.sg_rec + (k - 2 * d.nB);
+      cp_async8(Ls + e, src);
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+  }
   // C1: forward elimination, one thread per (pencil, system, parity), in place;
   // warps 2..7 of the mean CTA solve the mean-flow system meanwhile
   if (tid < 4 * kGW) {
@@ -746,10 +786,15 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     if (p >= 0) {
       const int n = sys ? d.nD : d.nB;
       const int m = par ? n / 2 : (n + 1) / 2;
-      const double* __restrict__ rec =
-          sys ? a.sg + (size_t)s_mode[w] * a.sg_rec : a.su + (size_t)s_mode[w] * a.su_rec;
-      forward_elim(rec, par, m,
-                   rowc + (size_t)(sys ? G.oRG + par * G.nDe : G.oRU + par * G.nBe) * LC + w, LC);
+      c64* y = rowc + (size_t)(sys ? G.oRG + par * G.nDe : G.oRU + par * G.nBe) * LC + w;
+      if (G.oL >= 0) {
+        const int per = 2 * (d.nB + d.nD);
+        forward_elim_smem(Ls + (w & 7) * per + (sys ? 2 * d.nB : 0), par, m, y, LC);
+      } else {
+        const double* __restrict__ rec =
+            sys ? a.sg + (size_t)s_mode[w] * a.sg_rec : a.su + (size_t)s_mode[w] * a.su_rec;
+        forward_elim(rec, par, m, y, LC);
+      }
     }
   } else if (tid < 4 * kGW + kMeanThreads) {
     if (mean_cta) mean_flow(d, o, G, a, mean, m_nvw, m_vw, m_x, tid - 4 * kGW);
@@ -821,6 +866,12 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     __syncthreads();
     for (int i = tid; i < d.nD; i += kGThreads)
       rowc[(((i & 1) ? G.oGO : G.oGE) + (i >> 1)) * LC + 0] = m_x[i];
+  }
+  if (Jh > Jl && !G.tc) {
+    // middle Gauss node (odd N) while the velocity operators arrive: one FP64
+    // dot product per (operator, pencil, re/im)
+    __syncthreads();
+    if (tid < 5 * 2 * kGW) sm[G.oMid + tid] = mid_dot(G, sm, tid);
   }
   const bool staged = mbar_wait_bounded(&s_bar, 0, G.status, kStatusWaitTimeout);
   // a timed-out copy leaves the velocity operators incomplete: skip D (the
@@ -994,13 +1045,8 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     }
   }
   JFB_STAMP(0, 8);
-  if (Jh > Jl && !skip_d && !G.tc) {
-    // middle Gauss node (odd N): symmetric halves only, one dot product per
-    // (operator, pencil, re/im) thread
-    if (tid < 5 * 2 * kGW) sm[G.oMid + tid] = mid_dot(G, sm, tid);
-    __syncthreads();
-    if (tid < kGW) mid_store(d, a, sm + G.oMid, s_p, s_ky, s_kz, tid, N, Jl, P);
-  }
+  if (Jh > Jl && !skip_d && !G.tc && tid < kGW)  // products formed in C3
+    mid_store(d, a, sm + G.oMid, s_p, s_ky, s_kz, tid, N, Jl, P);
   if (G.tc) {  // free the TMEM columns (every tcgen05 load has completed)
     tc_fence_before();
     __syncthreads();
@@ -1010,6 +1056,12 @@ __global__ void __launch_bounds__(kGThreads, 1) pencil_gemm_kernel(Dims d, DevOp
     }
   }
   JFB_STAMP(0, 9);
+}
+
+__global__ void __launch_bounds__(kGThreads, 1)
+    pencil_gemm_kernel(const __grid_constant__ Dims d, const __grid_constant__ DevOps o,
+                       const __grid_constant__ GemmOps G, const __grid_constant__ GemmStageArgs a) {
+  pencil_gemm_body(d, o, G, a, blockIdx.x, gridDim.x);
 }
 
 }  // namespace jfb

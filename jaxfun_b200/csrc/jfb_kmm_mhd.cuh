@@ -79,15 +79,17 @@ inline size_t mhd_smem_bytes(int nD, int N) {
   return ((size_t)2 * 3 * nD + (size_t)3 * N) * kMhdW * sizeof(c64);
 }
 
-__global__ void __launch_bounds__(kMhdThreads, 1) mhd_a_kernel(Dims d, DevOps o, MhdOps M,
-                                                               MhdArgs a) {
+// The A stage of tile `bid` (the kernel below, or one member's tile of the
+// ensemble kernel).
+__device__ __forceinline__ void mhd_a_body(const Dims& d, const DevOps& o, const MhdOps& M,
+                                           const MhdArgs& a, const int bid) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_p[kMhdW], s_mode[kMhdW];
   __shared__ double s_ky[kMhdW], s_kz[kMhdW];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   constexpr int NWp = kMhdThreads / 32;
   const int nKc = (d.Kz + 7) / 8;
-  const int kyi = blockIdx.x / nKc, kz0 = (blockIdx.x % nKc) * 8;
+  const int kyi = bid / nKc, kz0 = (bid % nKc) * 8;
   const int N = d.Nx, nD = d.nD, Jh = M.Jh, Jl = M.Jl;
   const size_t P = (size_t)d.P;
   c64* RHS = reinterpret_cast<c64*>(smem_raw);  // [3][nD][kMhdW], split parity order
@@ -309,6 +311,12 @@ __global__ void __launch_bounds__(kMhdThreads, 1) mhd_a_kernel(Dims d, DevOps o,
   }
 }
 
+__global__ void __launch_bounds__(kMhdThreads, 1)
+    mhd_a_kernel(const __grid_constant__ Dims d, const __grid_constant__ DevOps o,
+                 const __grid_constant__ MhdOps M, const __grid_constant__ MhdArgs a) {
+  mhd_a_body(d, o, M, a, blockIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 // z stage of the coupled step, per group of kZRows (x, y) rows: twelve half
 // spectra (u, omega, b, j) -> six packed complex inverse FFTs, the products
@@ -318,17 +326,19 @@ __global__ void __launch_bounds__(kMhdThreads, 1) mhd_a_kernel(Dims d, DevOps o,
 // includes the imposed field and n the Coriolis term of MhdPhys), then three
 // packed forward transforms: HZ fields (n_x, n_y, n_z, e_x, e_y, e_z).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) z_cross_mhd_kernel(DevOps o, Dims d, MhdPhys ph,
-                                                          FFTPlan plan,
-                                                          const c64* __restrict__ tw,
-                                                          const c64* __restrict__ Y,
-                                                          c64* __restrict__ HZ) {
+// The z stage of rows [bid kZRows, (bid + 1) kZRows) (the kernel below, or
+// one member's rows of the ensemble kernel).
+__device__ __forceinline__ void z_cross_mhd_body(const DevOps& o, const Dims& d,
+                                                 const MhdPhys& ph, const FFTPlan& plan,
+                                                 const c64* __restrict__ tw,
+                                                 const c64* __restrict__ Y,
+                                                 c64* __restrict__ HZ, const int bid) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int NC = kZRows * 6;   // packed input columns
   constexpr int NCf = kZRows * 3;  // packed output columns
   c64* A = reinterpret_cast<c64*>(smem_raw);
   c64* B = A + d.Mz * NC;
-  const int row0 = blockIdx.x * kZRows;  // row = j * My + y
+  const int row0 = bid * kZRows;  // row = j * My + y
   const int nrows = d.Nx * d.My;
   const size_t plane = (size_t)d.Nx * d.My * d.Kz;
   // k fastest: a warp reads consecutive spectral values of one row and field
@@ -400,6 +410,13 @@ __global__ void __launch_bounds__(256) z_cross_mhd_kernel(DevOps o, Dims d, MhdP
     else v = cmk(0.5 * (Zk.im + Zm.im), -0.5 * (Zk.re - Zm.re));
     HZ[(size_t)f * plane + (size_t)row * d.Kz + k] = scale * v;
   }
+}
+
+__global__ void __launch_bounds__(256)
+    z_cross_mhd_kernel(const __grid_constant__ DevOps o, const __grid_constant__ Dims d,
+                       const __grid_constant__ MhdPhys ph, const __grid_constant__ FFTPlan plan,
+                       const c64* __restrict__ tw, const c64* __restrict__ Y, c64* __restrict__ HZ) {
+  z_cross_mhd_body(o, d, ph, plan, tw, Y, HZ, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------

@@ -16,15 +16,16 @@ namespace jfb {
 // plane is written back with coalesced rows.
 // ---------------------------------------------------------------------------
 template <int P, typename T>
-__global__ void __launch_bounds__(256) y_backward_warp_kernel(Dims d, int KC,
-                                                              const cpx<T>* __restrict__ tw,
-                                                              const cpx<T>* __restrict__ X,
-                                                              cpx<T>* __restrict__ Y) {
+__device__ __forceinline__ void y_backward_warp_body(const Dims& d, const int KC,
+                                                     const cpx<T>* __restrict__ tw,
+                                                     const cpx<T>* __restrict__ X,
+                                                     cpx<T>* __restrict__ Y, const int j,
+                                                     const int f, const int zc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ld = KC + 1;
   cpx<T>* in = reinterpret_cast<cpx<T>*>(smem_raw);  // Ny x ld
   cpx<T>* out = in + d.Ny * ld;                   // My x ld
-  const int j = blockIdx.x, f = blockIdx.y, kc0 = blockIdx.z * KC;
+  const int kc0 = zc * KC;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const cpx<T>* src = X + ((size_t)f * d.Nx + j) * d.P + kc0;
   const int kcn = min(KC, d.Kz - kc0);  // columns of this chunk (the last may be partial)
@@ -59,21 +60,30 @@ __global__ void __launch_bounds__(256) y_backward_warp_kernel(Dims d, int KC,
   }
 }
 
+template <int P, typename T>
+__global__ void __launch_bounds__(256) y_backward_warp_kernel(const __grid_constant__ Dims d, int KC,
+                                                              const cpx<T>* __restrict__ tw,
+                                                              const cpx<T>* __restrict__ X,
+                                                              cpx<T>* __restrict__ Y) {
+  y_backward_warp_body<P, T>(d, KC, tw, X, Y, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 // ---------------------------------------------------------------------------
 // y_forward: per (x-plane, field, kz chunk): forward FFT My along y, keep the
 // Ny retained modes (Nyquist zeroed), scale 1/My.
 // ---------------------------------------------------------------------------
 template <int P, typename T>
-__global__ void __launch_bounds__(256) y_forward_warp_kernel(Dims d, int KC,
-                                                             const cpx<T>* __restrict__ tw,
-                                                             const cpx<T>* __restrict__ HZ,
-                                                             cpx<T>* __restrict__ HX,
-                                                             const double* __restrict__ xb) {
+__device__ __forceinline__ void y_forward_warp_body(const Dims& d, const int KC,
+                                                    const cpx<T>* __restrict__ tw,
+                                                    const cpx<T>* __restrict__ HZ,
+                                                    cpx<T>* __restrict__ HX,
+                                                    const double* __restrict__ xb, const int j,
+                                                    const int f, const int zc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ld = KC + 1;
   cpx<T>* in = reinterpret_cast<cpx<T>*>(smem_raw);  // My x ld
   cpx<T>* out = in + d.My * ld;                   // Ny x ld
-  const int j = blockIdx.x, f = blockIdx.y, kc0 = blockIdx.z * KC;
+  const int kc0 = zc * KC;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const cpx<T>* src = HZ + ((size_t)f * d.Nx + j) * (size_t)d.My * d.Kz + kc0;
   const int kcn = min(KC, d.Kz - kc0);  // columns of this chunk (the last may be partial)
@@ -111,6 +121,15 @@ __global__ void __launch_bounds__(256) y_forward_warp_kernel(Dims d, int KC,
     const int c = idx % KC, r = idx / KC;
     if (c < kcn) dst[(size_t)r * d.Kz + c] = out[r * ld + c];
   }
+}
+
+template <int P, typename T>
+__global__ void __launch_bounds__(256) y_forward_warp_kernel(const __grid_constant__ Dims d, int KC,
+                                                             const cpx<T>* __restrict__ tw,
+                                                             const cpx<T>* __restrict__ HZ,
+                                                             cpx<T>* __restrict__ HX,
+                                                             const double* __restrict__ xb) {
+  y_forward_warp_body<P, T>(d, KC, tw, HZ, HX, xb, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Hermitian-extended packed spectrum Z = A + i B of two real fields whose
@@ -349,37 +368,41 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
   pdl_wait();  // X is written by the previous kernel, HX still read by it
   JFB_STAMP(1, 1);
 
-  // 1. inverse y transforms of this CTA's columns (complex64: staged row
-  //    by row, coalesced along kz, into Ys in padded order, then one column
-  //    per warp in place; FP64: gathered per column straight from X)
-  if constexpr (sizeof(T) == 4) {
-    // half-warp per row (KH <= 16 columns), no per-element index division
-    // (all loads of a thread are issued before its stores: Ny <= MY <= 96
-    // gives at most three rows per half-warp and field)
+  // 1. inverse y transforms of this CTA's columns: the six fields staged row
+  //    by row (coalesced along kz) into Ys in padded order, then one column
+  //    per warp in place
+  {
+    // half-warp per row (KH <= 16 columns), no per-element index division;
+    // FB fields at a time, all loads of a thread before its stores (Ny <=
+    // MY <= 96 gives at most three rows per half-warp and field)
     const int hw = threadIdx.x >> 4, cl = threadIdx.x & 15;
     constexpr int RS = kPlaneThreads / 16, RMAX = (MY + RS - 1) / RS;
+    constexpr int FB = sizeof(T) == 4 ? 6 : 2;  // register budget of the FP64 form
     if (cl < KH) {
-      cpx<T> v[6][RMAX];
 #pragma unroll
-      for (int f = 0; f < 6; ++f) {
-        const cpx<T>* src = X + ((size_t)f * d.Nx + j) * P + rank * KH + cl;
+      for (int f0 = 0; f0 < 6; f0 += FB) {
+        cpx<T> v[FB][RMAX];
 #pragma unroll
-        for (int i = 0; i < RMAX; ++i) {
-          const int r = hw + RS * i;
-          v[f][i] = (r < d.Ny && r != half) ? src[(size_t)r * Kz] : cmk(T(0), T(0));
+        for (int f = 0; f < FB; ++f) {
+          const cpx<T>* src = X + ((size_t)(f0 + f) * d.Nx + j) * P + rank * KH + cl;
+#pragma unroll
+          for (int i = 0; i < RMAX; ++i) {
+            const int r = hw + RS * i;
+            v[f][i] = (r < d.Ny && r != half) ? src[(size_t)r * Kz] : cmk(T(0), T(0));
+          }
         }
-      }
 #pragma unroll
-      for (int f = 0; f < 6; ++f) {
-        cpx<T>* dst = Ys + (size_t)f * MY * LDZ + cl;
+        for (int f = 0; f < FB; ++f) {
+          cpx<T>* dst = Ys + (size_t)(f0 + f) * MY * LDZ + cl;
 #pragma unroll
-        for (int i = 0; i < RMAX; ++i) {
-          const int r = hw + RS * i;  // the Nyquist row r == half stays zero
-          if (r < d.Ny) dst[(size_t)((r < half) ? r : r - d.Ny + MY) * LDZ] = v[f][i];
+          for (int i = 0; i < RMAX; ++i) {
+            const int r = hw + RS * i;  // the Nyquist row r == half stays zero
+            if (r < d.Ny) dst[(size_t)((r < half) ? r : r - d.Ny + MY) * LDZ] = v[f][i];
+          }
+          // padding rows half .. MY - half - 1 (row MY - half is the Nyquist
+          // row's slot, zeroed above)
+          for (int k = half + hw; k < MY - half; k += RS) dst[(size_t)k * LDZ] = cmk(T(0), T(0));
         }
-        // padding rows half .. MY - half - 1 (row MY - half is the Nyquist
-        // row's slot, zeroed above)
-        for (int k = half + hw; k < MY - half; k += RS) dst[(size_t)k * LDZ] = cmk(T(0), T(0));
       }
     }
     __syncthreads();
@@ -397,41 +420,30 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
 #pragma unroll
       for (int k1 = 0; k1 < PY; ++k1) col[(size_t)(k1 + PY * br) * LDZ] = v[k1];
     }
-  } else {
-    JFB_STAMP(1, 2);
-    WarpTw<PY, T> w;
-    load_warp_tw<PY, T>(w, twy, lane);
-    for (int t = warp; t < 6 * KH; t += NW) {
-      const int f = t / KH, cl = t % KH, kz = rank * KH + cl;
-      const cpx<T>* src = X + ((size_t)f * d.Nx + j) * P + kz;
-      cpx<T> v[PY];
-#pragma unroll
-      for (int r = 0; r < PY; ++r) {
-        const int k = 32 * r + lane;
-        cpx<T> z = cmk(T(0), T(0));
-        if (k < half) z = src[(size_t)k * Kz];
-        else if (k >= MY - half) z = src[(size_t)(k - MY + d.Ny) * Kz];
-        v[r] = z;
-      }
-      warp_fft_inverse<PY, T>(v, w, lane);
-#pragma unroll
-      for (int k1 = 0; k1 < PY; ++k1) Ys[((size_t)f * MY + k1 + PY * br) * LDZ + cl] = v[k1];
-    }
   }
   cluster.sync();
   JFB_STAMP(1, 3);
 
-  // 2. z stage on this CTA's rows, two rows per warp
+  // 2. z stage on this CTA's rows (two, or at 96 points three, per warp)
   {
     WarpTw<PZ, T> w;
     load_warp_tw<PZ, T>(w, twz, lane);
     const T ub = T(d.uwall * o.xphys[j]), uw = T(d.uwall);
     const T scale = T(1.0 / MZ);
-    for (int pair = warp; pair < MH / 2; pair += NW) {
+    // rows ya and (if hasb) ya + 1 of this CTA: inverse real z FFTs of the
+    // six fields (two per complex FFT), -(u x omega), forward real z FFTs
+    // of the three products (two rows per complex FFT; a lone row pairs its
+    // third product with zero)
+    auto z_rows = [&](int ya, bool hasb) {
       T nrm[2][3][PZ];
 #pragma unroll
       for (int rb = 0; rb < 2; ++rb) {
-        const int y = rank * MH + 2 * pair + rb;
+        if (rb == 1 && !hasb) {
+#pragma unroll
+          for (int r = 0; r < PZ; ++r) nrm[1][0][r] = nrm[1][1][r] = nrm[1][2][r] = T(0);
+          break;
+        }
+        const int y = rank * MH + ya + rb;
         cpx<T> ph[3][PZ];
 #pragma unroll
         for (int pr = 0; pr < 3; ++pr) {
@@ -464,13 +476,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
         F2[r] = cmk(nrm[0][2][r], nrm[1][2][r]);
       }
       warp_fft_forward<PZ, T>(F0, w, lane);
-      warp_fft_forward<PZ, T>(F1, w, lane);
+      if (hasb) warp_fft_forward<PZ, T>(F1, w, lane);
       warp_fft_forward<PZ, T>(F2, w, lane);
       cpx<T> xa0[QK], xa1[QK], xb0[QK], xb1[QK], x2a[QK], x2b[QK];
       unpack_pair<PZ, QK, T>(F0, lane, xa0, xa1);
-      unpack_pair<PZ, QK, T>(F1, lane, xb0, xb1);
+      if (hasb) unpack_pair<PZ, QK, T>(F1, lane, xb0, xb1);
       unpack_pair<PZ, QK, T>(F2, lane, x2a, x2b);
-      const int ya = 2 * pair, yb = ya + 1;  // local rows
+      const int yb = ya + 1;  // local rows
 #pragma unroll
       for (int q = 0; q < QK; ++q) {
         const int kz = 32 * q + lane;
@@ -479,19 +491,26 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
         Hs[((size_t)0 * MH + ya) * Kz + ca] = scale * xa0[q];
         Hs[((size_t)1 * MH + ya) * Kz + ca] = scale * xa1[q];
         Hs[((size_t)2 * MH + ya) * Kz + ca] = scale * x2a[q];
-        Hs[((size_t)0 * MH + yb) * Kz + cb] = scale * xb0[q];
-        Hs[((size_t)1 * MH + yb) * Kz + cb] = scale * xb1[q];
-        Hs[((size_t)2 * MH + yb) * Kz + cb] = scale * x2b[q];
+        if (hasb) {
+          Hs[((size_t)0 * MH + yb) * Kz + cb] = scale * xb0[q];
+          Hs[((size_t)1 * MH + yb) * Kz + cb] = scale * xb1[q];
+          Hs[((size_t)2 * MH + yb) * Kz + cb] = scale * x2b[q];
+        }
       }
+    };
+    if (MH == 3 * NW) {  // three rows per warp: a pair and a lone row
+      z_rows(3 * warp, true);
+      z_rows(3 * warp + 2, false);
+    } else {
+      for (int pair = warp; pair < MH / 2; pair += NW) z_rows(2 * pair, true);
     }
   }
   cluster.sync();
   JFB_STAMP(1, 4);
 
-  // 3. forward y transforms of this CTA's columns (complex64: into Ys,
-  //    free once the peer has passed the barrier above, then row-wise
-  //    coalesced stores; FP64: stored per column)
-  if constexpr (sizeof(T) == 4) {
+  // 3. forward y transforms of this CTA's columns into Ys (free once the
+  //    peer has passed the barrier above), then row-wise coalesced stores
+  {
     WarpTw<PY, T> w;
     load_warp_tw<PY, T>(w, twy, lane);
     const T scale = T(1.0 / MY);
@@ -523,36 +542,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
       }
       HX[((size_t)f * d.Nx + j) * P + (size_t)r * Kz + kz] = val;
     }
-  } else {
-    WarpTw<PY, T> w;
-    load_warp_tw<PY, T>(w, twy, lane);
-    const T scale = T(1.0 / MY);
-    for (int t = warp; t < 3 * KH; t += NW) {
-      const int f = t / KH, cl = t % KH, kz = rank * KH + cl;
-      cpx<T> v[PY];
-#pragma unroll
-      for (int n1 = 0; n1 < PY; ++n1) {
-        const int y = n1 + PY * br;
-        const int own = y / MH, yl = y - own * MH;
-        const cpx<T>* base = (own == rank) ? Hs : Hpeer;
-        v[n1] = base[((size_t)f * MH + yl) * Kz + (swz ? (kz ^ (yl & 7)) : kz)];
-      }
-      warp_fft_forward<PY, T>(v, w, lane);
-      cpx<T>* dst = HX + ((size_t)f * d.Nx + j) * P + kz;
-#pragma unroll
-      for (int k1 = 0; k1 < PY; ++k1) {
-        const int k = 32 * k1 + lane;
-        if (k < half) {
-          cpx<T> val = scale * v[k1];
-          if (f == 0 && kz == 0 && k == 0) val.re += T(-d.uwall * o.xphys[j] * d.uwall);
-          dst[(size_t)k * Kz] = val;
-        } else if (k > MY - half) {
-          dst[(size_t)(k - MY + d.Ny) * Kz] = scale * v[k1];
-        }
-        else if (k == MY - half) dst[(size_t)half * Kz] = cmk(T(0), T(0));  // Nyquist
-      }
-    }
-    JFB_STAMP(1, 5);
   }
   JFB_STAMP(1, 6);
   cluster.sync();

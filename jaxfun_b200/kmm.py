@@ -19,6 +19,8 @@ import torch
 from . import _lib
 
 _STEPPERS = {"IMEXRK222", "IMEXRK3", "CNAB2", "SBDF3"}
+_GPU_STEPPERS = {"SBDF3": _lib.JFB_INTEGRATOR_SBDF3, "IMEXRK3": _lib.JFB_INTEGRATOR_IMEXRK3,
+                 "IMEXRK222": _lib.JFB_INTEGRATOR_IMEXRK222}
 
 
 @dataclass(frozen=True)
@@ -48,8 +50,11 @@ class KMM:
     """Velocity-vorticity KMM channel solver (channelflow_kmm.py:104-230).
 
     Supported on the GPU path: Chebyshev family, wall-normal axis unpadded,
-    SBDF3 with IMEXRK3 startup, rotational nonlinear form.  The coefficient
-    path ("optimized" or "transform") only changes round-off in the reference
+    rotational nonlinear form; time integrators SBDF3 (IMEXRK3 startup),
+    IMEXRK3 and IMEXRK222 (the one-step integrators keep no history: the
+    state's history fields pass through unchanged, as in the reference's
+    ``KMM.step``).  The coefficient path ("optimized" or "transform") only
+    changes round-off in the reference
     (tests/couette/test_pcf_fluctuations_jax.py:16-52), so both names select
     the same coefficient-space kernels.
     """
@@ -90,7 +95,7 @@ class KMM:
                 "{'IMEXRK222', 'IMEXRK3', 'CNAB2', 'SBDF3'}"
             )
         unsupported = []
-        if time_integrator != "SBDF3":
+        if time_integrator not in _GPU_STEPPERS:
             unsupported.append(f"time_integrator={time_integrator!r}")
         if self.nonlinear_form != "rotational":
             unsupported.append(f"nonlinear_form={self.nonlinear_form!r}")
@@ -102,10 +107,10 @@ class KMM:
             unsupported.append("dpdy != 0")
         if unsupported:
             raise NotImplementedError(
-                "the B200 step supports SBDF3 / rotational / Chebyshev / unpadded x "
-                "only; requested " + ", ".join(unsupported)
+                "the B200 step supports SBDF3, IMEXRK3 or IMEXRK222 / rotational / "
+                "Chebyshev / unpadded x only; requested " + ", ".join(unsupported)
             )
-        self.time_integrator = "SBDF3"
+        self.time_integrator = time_integrator
         self.family = "C"
         self.precision = precision
         self.device = torch.device(device)
@@ -130,6 +135,7 @@ class KMM:
             "mixed": _lib.JFB_PRECISION_MIXED,
         }[precision]
         cfg.nonlinear_form = _lib.JFB_NONLINEAR_ROTATIONAL
+        cfg.time_integrator = _GPU_STEPPERS[self.time_integrator]
         self._cfg = cfg
         handle = ctypes.c_void_p()
         with torch.cuda.device(self.device):
@@ -255,9 +261,17 @@ class KMM:
         does for a non-finite state (production/oracles.py:3257-3261)."""
         steps = int(steps)
         self._load(state)
-        hist = float(self._current.history_steps)
+        loaded = self._current
+        hist = float(loaded.history_steps)
         _lib.call("jfb_kmm_advance", self._plan, steps, self._stream())
-        out = self._fetch(min(2.0, hist + steps))
+        if self.time_integrator == "SBDF3":
+            out = self._fetch(min(2.0, hist + steps))
+        else:  # one-step integrators: the history fields pass through
+            out = replace(self._fetch(hist), nonlinear_old=loaded.nonlinear_old,
+                          nonlinear_older=loaded.nonlinear_older,
+                          solution_old=loaded.solution_old,
+                          solution_older=loaded.solution_older)
+            self._current = out
         self.check()
         return out
 

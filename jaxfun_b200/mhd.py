@@ -309,10 +309,11 @@ class PlaneCouetteMRIShearpy(PlaneCouetteMHD):
 
 
 class Ensemble:
-    """Independent solvers (flow or MHD, any sizes) advanced together: one
-    CUDA graph per step with every member on its own stream
-    (``jfb_ensemble_*``).  ``solve(states, steps)`` takes and returns one state
-    per member."""
+    """Independent solvers (flow or MHD, any sizes) advanced together, one
+    CUDA graph per step (``jfb_ensemble_*``): five launches per step over
+    all members when every member is an MHD plan (``batched``), else every
+    member on its own stream.  ``solve(states, steps)`` takes and returns
+    one state per member."""
 
     def __init__(self, members) -> None:
         self.members = list(members)
@@ -320,6 +321,10 @@ class Ensemble:
         handle = ctypes.c_void_p()
         _lib.call("jfb_ensemble_create", arr, len(self.members), ctypes.byref(handle))
         self._handle = handle
+        b, n = ctypes.c_int32(), ctypes.c_int64()
+        _lib.call("jfb_ensemble_info", handle, ctypes.byref(b), ctypes.byref(n))
+        self.batched = bool(b.value)
+        self.launches_per_step = int(n.value)
 
     def __del__(self):
         h = getattr(self, "_handle", None)

@@ -12,7 +12,7 @@ int main(void) {
   F(jfb_kmm_config, nx); F(jfb_kmm_config, family); F(jfb_kmm_config, x_lo);
   F(jfb_kmm_config, ly); F(jfb_kmm_config, pad_y); F(jfb_kmm_config, nu);
   F(jfb_kmm_config, dt); F(jfb_kmm_config, u_wall); F(jfb_kmm_config, precision);
-  F(jfb_kmm_config, nonlinear_form);
+  F(jfb_kmm_config, nonlinear_form); F(jfb_kmm_config, time_integrator);
   printf("jfb_kmm_state %zu\n", sizeof(jfb_kmm_state));
   F(jfb_kmm_state, u0); F(jfb_kmm_state, g); F(jfb_kmm_state, nonlinear_old);
   F(jfb_kmm_state, nonlinear_older); F(jfb_kmm_state, solution_old);

@@ -297,3 +297,25 @@ def test_autotune_selects_a_variant_and_keeps_the_state(cuda, tmp_path, monkeypa
     assert again["cached"] and again["variant"] == res["variant"]
     with pytest.raises(Exception):
         g.set_variant(replicas=99)
+
+
+@pytest.mark.parametrize("integrator", ["IMEXRK3", "IMEXRK222"])
+@pytest.mark.parametrize("N, precision", [((17, 16, 16), "fp64"), ((33, 32, 32), "fp64"),
+                                          ((97, 16, 16), "fp64"), ((33, 32, 32), "mixed")])
+def test_one_step_integrators_match_oracle(cuda, integrator, N, precision):
+    """KMM with time_integrator IMEXRK3 (every step three Spalart stages,
+    channelflow_kmm.py:872-935) or IMEXRK222 (two ARS stages,
+    channelflow_kmm.py:1137-1192) against the oracle after five steps: FP64
+    at 1e-12 on the tensor-core pencil stage (17, 33) and the warp-per-pencil
+    stage (97), the mixed form at 1e-7.  The history fields pass through."""
+    kw = dict(N=N, Re=400.0, dt=1e-3, perturbation_amplitude=0.05, time_integrator=integrator)
+    o = PlaneCouetteOracle(**kw)
+    g = PlaneCouetteFluctuation(precision=precision, device=cuda, **kw)
+    st = o.initial_state()
+    gs = g._ensure_history(to_dev(st, cuda))
+    st, gs = o.solve(st, 5), g.solve(gs, 5)
+    tol = 1e-12 if precision == "fp64" else 1e-7
+    for a, b in zip((*gs.u, gs.g), (*st.u, st.g), strict=True):
+        assert rel(a, b) < tol
+    assert gs.history_steps == 0.0
+    assert all(float(t.abs().max()) == 0.0 for t in gs.nonlinear_old)

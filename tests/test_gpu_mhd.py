@@ -225,3 +225,37 @@ def test_ensemble_of_uneven_members_equals_separate_runs(cuda):
             la, lb = (*a.u, a.g), (*b.u, b.g)
         for x, y in zip(la, lb, strict=True):
             assert torch.equal(x, y)
+
+
+def test_batched_ensemble_of_uneven_mhd_members_equals_separate_runs(cuda, monkeypatch):
+    """All-MHD ensembles of uneven wall-normal size advance as five launches
+    per steady step for each wall-normal size (one per stage, a work list
+    over that size's members' tiles, the sizes on parallel graph branches),
+    or as five launches over all members (JFB200_ENSEMBLE=batched); either
+    result is bitwise that of separate runs, and that of the
+    one-stream-per-member graph."""
+    from jaxfun_b200.mhd import Ensemble
+
+    def members():
+        # 64 Fourier modes: padded length 96 = 32 x 3, the warp-FFT y transforms
+        return [PlaneCouetteMHD(N=(n, 64, 64), dt=1e-3, magnetic_amplitude=0.1, device=cuda)
+                for n in (33, 17, 25, 33)]
+
+    sep = members()
+    ref = [m.solve(m.initial_state(), 7) for m in sep]
+    outs = []
+    for mode, batched, launches in ((None, True, 15), ("batched", True, 5),
+                                    ("streams", False, 4)):
+        if mode is None:
+            monkeypatch.delenv("JFB200_ENSEMBLE", raising=False)
+        else:
+            monkeypatch.setenv("JFB200_ENSEMBLE", mode)
+        ms = members()
+        ens = Ensemble(ms)
+        assert ens.batched == batched, mode
+        assert ens.launches_per_step == launches, mode
+        outs.append(ens.solve([m.initial_state() for m in ms], 7))
+    for a, b, c, d in zip(*outs, ref, strict=True):
+        la, lb, lc, ld = ((*x.flow.u, x.flow.g, *x.A) for x in (a, b, c, d))
+        for x, y, z, w in zip(la, lb, lc, ld, strict=True):
+            assert torch.equal(x, w) and torch.equal(y, w) and torch.equal(z, w)

@@ -12,7 +12,7 @@ from jaxfun_b200.kmm import KMM, PlaneCouetteFluctuation
 
 
 @pytest.mark.parametrize("kw", [
-    {"time_integrator": "IMEXRK222"},
+    {"time_integrator": "CNAB2"},
     {"nonlinear_form": "gradient"},
     {"family": "L"},
     {"padding_factor": (1.5, 1.5, 1.5)},
