@@ -362,7 +362,8 @@ def main(argv=None):
         """Timed steady steps, per-kernel breakdown, graph replay and the
         end-to-end figure of one form on the seeded workload."""
         solver = PlaneCouetteFluctuation(N=grid, domain=domain(), Re=RE, dt=DT,
-                                         precision=precision, device=dev)
+                                         precision=precision, device=dev,
+                                         time_integrator="SBDF3", nonlinear_form="rotational")
         info = solver.info()
         e0 = solver.diagnostics(solver.state_from_physical(fields0))["Epert"]
         fields = scale_to_energy(fields0, e0, ENERGY)
@@ -513,9 +514,11 @@ def main(argv=None):
     def mixed_error():
         """Per-field relative L2 of the mixed form against the FP64 form after
         100 and 1000 steps from the same FP64-projected initial state."""
-        g64 = PlaneCouetteFluctuation(N=grid, domain=domain(), Re=RE, dt=DT, device=dev)
+        g64 = PlaneCouetteFluctuation(N=grid, domain=domain(), Re=RE, dt=DT, device=dev,
+                                      time_integrator="SBDF3", nonlinear_form="rotational")
         g32 = PlaneCouetteFluctuation(N=grid, domain=domain(), Re=RE, dt=DT,
-                                      precision="mixed", device=dev)
+                                      precision="mixed", device=dev,
+                                      time_integrator="SBDF3", nonlinear_form="rotational")
         e0 = g64.diagnostics(g64.state_from_physical(fields0))["Epert"]
         f = scale_to_energy(fields0, e0, ENERGY)
         a, b = g64.state_from_physical(f), g32.state_from_physical(f)
@@ -542,7 +545,8 @@ def main(argv=None):
         from jaxfun_b200 import minimal_seed as ms
 
         T, ck = args.adjoint_steps, 20
-        g64 = PlaneCouetteFluctuation(N=grid, domain=domain(), Re=RE, dt=DT, device=dev)
+        g64 = PlaneCouetteFluctuation(N=grid, domain=domain(), Re=RE, dt=DT, device=dev,
+                                      time_integrator="SBDF3", nonlinear_form="rotational")
         e0 = g64.diagnostics(g64.state_from_physical(fields0))["Epert"]
         x0 = ms._primary(g64.state_from_physical(scale_to_energy(fields0, e0, ENERGY)))
         ms.gain_and_gradient(g64, x0, 4, checkpoint=2)  # operators and bands, untimed
@@ -774,7 +778,8 @@ def main(argv=None):
             states = {}
             for prec in ("fp64", "mixed"):
                 sv = PlaneCouetteFluctuation(N=grid_n, domain=domain(), Re=RE, dt=DT,
-                                             precision=prec, device=dev)
+                                             precision=prec, device=dev,
+                                             time_integrator="SBDF3", nonlinear_form="rotational")
                 if prec == "fp64":
                     e0 = sv.diagnostics(sv.state_from_physical(f0))["Epert"]
                     fields_n = scale_to_energy(f0, e0, ENERGY)

@@ -96,23 +96,30 @@ int jfb_wavenumber_solve(const double* L, const int64_t* L_offsets, int64_t n_L,
 #define JFB_FAMILY_CHEBYSHEV 0
 #define JFB_PRECISION_FP64 0
 #define JFB_PRECISION_MIXED 1
+/* nonlinear term (channelflow_kmm.py:754-770): rotational -(u x omega) or the
+ * gradient form u . grad u (the reference's default) */
 #define JFB_NONLINEAR_ROTATIONAL 0
+#define JFB_NONLINEAR_GRADIENT 1
 /* time integrators of KMM.step (channelflow_kmm.py:937-1192): SBDF3 with an
  * IMEXRK3 startup (sbdf3.py:15-62), the three-stage IMEXRK3 every step
  * (imex_rk.py:96-125, channelflow_kmm.py:872-935), the two-stage ARS
- * IMEXRK222 (imex_rk.py:175-198, integrators/coupled.py:13-44) */
+ * IMEXRK222 (imex_rk.py:175-198, integrators/coupled.py:13-44), CNAB2 with a
+ * fixed step (channelflow_kmm.py:1071-1121, cnab2.py:185-240; a state's
+ * history_steps holds the reference's have_old, 0 or 1) */
 #define JFB_INTEGRATOR_SBDF3 0
 #define JFB_INTEGRATOR_IMEXRK3 1
 #define JFB_INTEGRATOR_IMEXRK222 2
+#define JFB_INTEGRATOR_CNAB2 3
 
 /* Constructor arguments of KMM / PlaneCouetteFluctuationJax
  * (examples/channelflow_kmm.py:107-230, examples/pcf_fluctuations_jax.py:35-75)
- * restricted to the hot path: Chebyshev family, x unpadded, rotational
- * nonlinear form, the time integrators above (MHD plans and the adjoint:
- * SBDF3).  u_wall = 0 gives the plain KMM channel (no base flow). */
+ * restricted to the hot path: Chebyshev or Legendre family, x unpadded, the
+ * rotational or gradient nonlinear form (gradient: FP64 precision), the time
+ * integrators above (MHD plans and the adjoint: SBDF3, Chebyshev, rotational).
+ * u_wall = 0 gives the plain KMM channel (no base flow). */
 typedef struct jfb_kmm_config {
   int32_t nx, ny, nz;     /* N = (wall-normal orthogonal size, Fourier y, z) */
-  int32_t family;         /* JFB_FAMILY_CHEBYSHEV                           */
+  int32_t family;         /* JFB_FAMILY_CHEBYSHEV or JFB_FAMILY_LEGENDRE    */
   double x_lo, x_hi;      /* wall-normal domain                             */
   double ly, lz;          /* periodic lengths of the y and z axes           */
   double pad_y, pad_z;    /* dealiasing padding factors (1.5 = 3/2 rule)    */
@@ -120,7 +127,7 @@ typedef struct jfb_kmm_config {
   double dt;              /* fixed time step                                */
   double u_wall;          /* base flow U_b(x) = u_wall * x                  */
   int32_t precision;      /* JFB_PRECISION_FP64 or JFB_PRECISION_MIXED      */
-  int32_t nonlinear_form; /* JFB_NONLINEAR_ROTATIONAL                       */
+  int32_t nonlinear_form; /* JFB_NONLINEAR_ROTATIONAL or _GRADIENT          */
   int32_t time_integrator; /* JFB_INTEGRATOR_* (0: SBDF3)                   */
 } jfb_kmm_config;
 

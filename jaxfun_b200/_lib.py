@@ -28,9 +28,11 @@ JFB_FAMILY_CHEBYSHEV = 0
 JFB_PRECISION_FP64 = 0
 JFB_PRECISION_MIXED = 1
 JFB_NONLINEAR_ROTATIONAL = 0
+JFB_NONLINEAR_GRADIENT = 1
 JFB_INTEGRATOR_SBDF3 = 0
 JFB_INTEGRATOR_IMEXRK3 = 1
 JFB_INTEGRATOR_IMEXRK222 = 2
+JFB_INTEGRATOR_CNAB2 = 3
 JFB_BASIS_ORTHOGONAL = 0
 JFB_BASIS_DIRICHLET = 1
 JFB_BASIS_BIHARMONIC = 2

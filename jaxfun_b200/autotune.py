@@ -2,7 +2,8 @@
 
 The choice (``jfb_kmm_autotune``: the fastest of the plan's kernel variants
 by CUDA-event timing of graph-replayed steps) depends on the GPU model, the
-grid and the precision form; it is stored as JSON keyed by those, in the
+grid, the wall-normal family, the nonlinear form and the precision form; it
+is stored as JSON keyed by those, in the
 file named by JFB200_AUTOTUNE_CACHE (default
 ``~/.cache/jaxfun_b200/autotune.json``).
 """
@@ -24,7 +25,9 @@ def cache_key(solver) -> str:
     name = torch.cuda.get_device_name(solver.device).replace(" ", "_")
     nx, ny, nz = solver.N
     pad = "x".join(f"{p:g}" for p in solver.padding_factor[1:])
-    return f"{name}/{nx}x{ny}x{nz}/pad{pad}/{solver.precision}"
+    form = getattr(solver, "nonlinear_form", "rotational")
+    fam = getattr(solver, "family", "C")
+    return f"{name}/{nx}x{ny}x{nz}/pad{pad}/{fam}/{form}/{solver.precision}"
 
 
 def _read() -> dict:

@@ -236,6 +236,7 @@ struct jfb_kmm_plan {
   int* status = nullptr;  // device status word (kStatus* bits), read by jfb_kmm_check
   jfb::FactorSet steady, startup[3];
   jfb::FactorSet rk222;  // IMEXRK222 plans: the factors of gamma = g dt
+  jfb::FactorSet cnab2;  // CNAB2 plans: the factors of gamma = dt / 2
   jfb::c64 *U0[3], *G[3], *NU[3], *NG[3], *VW[3], *NVW[3];
   jfb::c64 *NUst, *NGst, *NVWst;
   jfb::c64 *U1S, *U2S;
@@ -264,6 +265,7 @@ struct jfb_kmm_plan {
   bool pdl = false;        // programmatic dependent launch of the step kernels
   bool plane = false;      // fused periodic-axis transforms (plane_cross_kernel)
   size_t smem_plane = 0;
+  size_t smem_zg = 0;      // gradient-form z stage (z_grad_kernel)
   jfb::GemmOps gops;
   size_t smem_gemm = 0;
   // MHD (vector potential A, three Dirichlet components per level)
@@ -623,7 +625,7 @@ template <typename T> static cpx<T>* buf(void* p) { return reinterpret_cast<cpx<
 // 12 / 6 for the coupled MHD step)
 template <int P, typename T>
 static void launch_y_warp(jfb_kmm_plan* pl, cudaStream_t s, bool backward, int nb = 6,
-                          int nf = 3) {
+                          int nf = 3, bool self_term = true) {
   const Dims d = tdims<T>(pl);
   const size_t sm = backward ? pl->smem_yw_b : pl->smem_yw_f;
   const size_t smT = sm / sizeof(c64) * sizeof(cpx<T>);
@@ -635,18 +637,19 @@ static void launch_y_warp(jfb_kmm_plan* pl, cudaStream_t s, bool backward, int n
   } else {
     dim3 g(d.Nx, nf, chunks);
     y_forward_warp_kernel<P, T><<<g, 256, smT, s>>>(d, pl->KCw, Tx<T>::twy(pl), buf<T>(pl->HZ),
-                                                      buf<T>(pl->HX), pl->ops.xphys);
+                                                      buf<T>(pl->HX),
+                                                      self_term ? pl->ops.xphys : nullptr);
   }
 }
 
 template <typename T>
 static void launch_y_warp_any(jfb_kmm_plan* pl, cudaStream_t s, bool backward, int nb = 6,
-                              int nf = 3) {
+                              int nf = 3, bool self_term = true) {
   switch (pl->py) {
-    case 2: launch_y_warp<2, T>(pl, s, backward, nb, nf); break;
-    case 3: launch_y_warp<3, T>(pl, s, backward, nb, nf); break;
-    case 4: launch_y_warp<4, T>(pl, s, backward, nb, nf); break;
-    default: launch_y_warp<6, T>(pl, s, backward, nb, nf); break;
+    case 2: launch_y_warp<2, T>(pl, s, backward, nb, nf, self_term); break;
+    case 3: launch_y_warp<3, T>(pl, s, backward, nb, nf, self_term); break;
+    case 4: launch_y_warp<4, T>(pl, s, backward, nb, nf, self_term); break;
+    default: launch_y_warp<6, T>(pl, s, backward, nb, nf, self_term); break;
   }
 }
 
@@ -695,6 +698,33 @@ static int launch_transforms_t(jfb_kmm_plan* pl, cudaStream_t s) {
     else JFB_CHECK_CUDA((launch_plane<3, 3, T>(pl, s)));
     if (pl->timing_events)
       for (int k = 2; k <= 4; ++k) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[k], s));
+    return JFB_OK;
+  }
+  if (d.grad) {
+    // gradient form (FP64): u_i, d/dx u_i, d/dy u_i backward in y, the
+    // twelve-field z stage, n_i forward in y (no constant base-flow term)
+    if (pl->py) {
+      launch_y_warp_any<T>(pl, s, true, 9);
+    } else {
+      dim3 gy(d.Nx, 9, d.Kz / pl->KC);
+      y_backward_kernel<T><<<gy, 256, pl->smem_y / sizeof(c64) * sizeof(cpx<T>), s>>>(
+          d, pl->fy, pl->KC, Tx<T>::twy(pl), buf<T>(pl->X), buf<T>(pl->Y));
+    }
+    JFB_CHECK_LAUNCH();
+    if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[2], s));
+    const int zb = ceil_div((int64_t)d.Nx * d.My, kZRows);
+    z_grad_kernel<<<zb, 256, pl->smem_zg, s>>>(pl->ops, pl->d, pl->fz, pl->twz, pl->Y, pl->HZ);
+    JFB_CHECK_LAUNCH();
+    if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[3], s));
+    if (pl->py) {
+      launch_y_warp_any<T>(pl, s, false, 9, 3, false);
+    } else {
+      dim3 gf(d.Nx, 3, d.Kz / pl->KC);
+      y_forward_kernel<T><<<gf, 256, pl->smem_y / sizeof(c64) * sizeof(cpx<T>), s>>>(
+          d, pl->fy, pl->KC, Tx<T>::twy(pl), buf<T>(pl->HZ), buf<T>(pl->HX), nullptr);
+    }
+    JFB_CHECK_LAUNCH();
+    if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[4], s));
     return JFB_OK;
   }
   if (pl->py && pl->pz) {
@@ -1043,12 +1073,49 @@ static int imexrk222_step(jfb_kmm_plan* pl, int64_t m, cudaStream_t s) {
   return launch_transforms(pl, s);
 }
 
-// One step of the plan's integrator once past the SBDF3 startup (the body
-// of the captured step graphs).
+// One CNAB2 step from ring position m (channelflow_kmm.py:1071-1121,
+// integrators/cnab2.py:211-240 with a fixed step, r = dt / previous_dt = 1):
+//   (M - dt/2 L) u' = M u^n + dt/2 L u^n + dt N_ab,
+//   N_ab = 3/2 N(u^n) - 1/2 N(u^(n-1)), or N(u^n) on the first step.
+// N(u^n) goes into the ring slot of u^n, where the next step finds it as
+// its previous nonlinear term.
+static int cnab2_step(jfb_kmm_plan* pl, int64_t m, cudaStream_t s, bool have_old) {
+  const int c = slot(m), o1 = slot(m - 1), nw = slot(m + 1);
+  StageArgs a = blank_args();
+  a.mode = kImplicit;
+  a.HX = pl->HX;
+  a.c0 = 1.0;
+  a.cL = 0.5 * pl->cfg.dt;
+  a.d0 = have_old ? 1.5 : 1.0;
+  a.d1 = have_old ? -0.5 : 0.0;
+  a.u0a = pl->U0[c];
+  a.ga = pl->G[c];
+  a.vwa = pl->VW[c];
+  if (have_old) {
+    a.Nup = pl->NU[o1];
+    a.Ngp = pl->NG[o1];
+    a.NVWp = pl->NVW[o1];
+  }
+  a.Nu_out = pl->NU[c];
+  a.Ng_out = pl->NG[c];
+  a.NVW_out = pl->NVW[c];
+  a.fac = packed(pl, pl->cnab2);
+  a.u0_out = pl->U0[nw];
+  a.g_out = pl->G[nw];
+  a.vw_out = pl->VW[nw];
+  a.X = pl->X;
+  const int st = launch_implicit(pl, a, s);
+  if (st) return st;
+  return launch_transforms(pl, s);
+}
+
+// One step of the plan's integrator once past the SBDF3 / CNAB2 startup (the
+// body of the captured step graphs).
 static int graph_step(jfb_kmm_plan* pl, int64_t m, cudaStream_t s) {
   switch (pl->cfg.time_integrator) {
     case JFB_INTEGRATOR_IMEXRK3: return startup_step(pl, s);
     case JFB_INTEGRATOR_IMEXRK222: return imexrk222_step(pl, m, s);
+    case JFB_INTEGRATOR_CNAB2: return cnab2_step(pl, m, s, true);
     default: return steady_step(pl, m, s);
   }
 }
@@ -1069,14 +1136,22 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
                        jfb_kmm_plan** out) {
   JFB_REQUIRE(cfg && out, "null pointer");
   *out = nullptr;
-  JFB_REQUIRE(cfg->family == JFB_FAMILY_CHEBYSHEV, "only the Chebyshev family is supported");
-  JFB_REQUIRE(cfg->nonlinear_form == JFB_NONLINEAR_ROTATIONAL,
-              "only the rotational nonlinear form is supported");
+  JFB_REQUIRE(cfg->family == JFB_FAMILY_CHEBYSHEV || cfg->family == JFB_FAMILY_LEGENDRE,
+              "family must be JFB_FAMILY_CHEBYSHEV or JFB_FAMILY_LEGENDRE");
+  JFB_REQUIRE(cfg->nonlinear_form == JFB_NONLINEAR_ROTATIONAL ||
+                  cfg->nonlinear_form == JFB_NONLINEAR_GRADIENT,
+              "nonlinear_form must be JFB_NONLINEAR_ROTATIONAL or JFB_NONLINEAR_GRADIENT");
+  JFB_REQUIRE(cfg->nonlinear_form == JFB_NONLINEAR_ROTATIONAL ||
+                  cfg->precision == JFB_PRECISION_FP64,
+              "the gradient nonlinear form runs in FP64 precision");
+  JFB_REQUIRE(!mhd || (cfg->family == JFB_FAMILY_CHEBYSHEV &&
+                       cfg->nonlinear_form == JFB_NONLINEAR_ROTATIONAL),
+              "the MHD step is Chebyshev / rotational only");
   JFB_REQUIRE(cfg->precision == JFB_PRECISION_FP64 || cfg->precision == JFB_PRECISION_MIXED,
               "precision must be JFB_PRECISION_FP64 or JFB_PRECISION_MIXED");
   JFB_REQUIRE(cfg->time_integrator >= JFB_INTEGRATOR_SBDF3 &&
-                  cfg->time_integrator <= JFB_INTEGRATOR_IMEXRK222,
-              "time_integrator must be SBDF3, IMEXRK3 or IMEXRK222");
+                  cfg->time_integrator <= JFB_INTEGRATOR_CNAB2,
+              "time_integrator must be SBDF3, IMEXRK3, IMEXRK222 or CNAB2");
   JFB_REQUIRE(!mhd || cfg->time_integrator == JFB_INTEGRATOR_SBDF3,
               "the MHD step is SBDF3 (with its IMEXRK3 startup) only");
   JFB_REQUIRE(cfg->nx >= 9 && cfg->nx <= 64 * kMaxNR + 1, "nx out of range [9, 129]");
@@ -1115,6 +1190,8 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   d.nu = cfg->nu;
   d.dt = cfg->dt;
   d.uwall = cfg->u_wall;
+  d.family = cfg->family == JFB_FAMILY_LEGENDRE ? 1 : 0;
+  d.grad = cfg->nonlinear_form == JFB_NONLINEAR_GRADIENT ? 1 : 0;
   if (!make_fft_plan(d.My, pl->fy) || !make_fft_plan(d.Mz, pl->fz)) {
     set_error("padded sizes must be of the form 2^a 3^b");
     return fail(JFB_ERR_ARG);
@@ -1152,7 +1229,14 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   pl->mixed = cfg->precision == JFB_PRECISION_MIXED;
   pl->smem_plane = plane_smem_bytes(d.My, d.Kz, pl->mixed ? sizeof(c32) : sizeof(c64));
   pl->plane = (pl->py == 2 || pl->py == 3) && (pl->pz == 2 || pl->pz == 3) && d.Kz % 2 == 0 &&
-              d.Kz <= 32 && pl->smem_plane <= 227 * 1024 && !pl->mhd;
+              d.Kz <= 32 && pl->smem_plane <= 227 * 1024 && !pl->mhd && !d.grad;
+  // gradient form: nine fields backward in y (u_i, d/dx u_i, d/dy u_i), the
+  // twelve-field z stage z_grad_kernel (shared-memory transforms)
+  pl->smem_zg = (size_t)2 * d.Mz * kZRows * 6 * sizeof(c64);
+  if (d.grad && (pl->smem_zg > 227 * 1024 || allow_smem((const void*)z_grad_kernel) != cudaSuccess)) {
+    set_error("grid too large for the gradient-form z stage");
+    return fail(JFB_ERR_ARG);
+  }
   pl->plane_ok = pl->plane;
   {
     const char* ev = std::getenv("JFB200_TRANSFORMS");
@@ -1313,7 +1397,8 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
     const size_t smem = ((size_t)G.oMid + 5 * 2 * kGW) * sizeof(double);
     const char* env = std::getenv("JFB200_PENCIL");
     const bool want = !(env && std::string(env) == "warp");
-    pl->gemm = smem <= 227 * 1024 && (d.nD + 1) / 2 <= kMaxM && Jl <= kMaxM;
+    // the tensor-core stage writes the rotational form's fields (u, omega)
+    pl->gemm = smem <= 227 * 1024 && (d.nD + 1) / 2 <= kMaxM && Jl <= kMaxM && !d.grad;
     GemmHost gh;
     if (pl->gemm) {
       std::string err;
@@ -1486,6 +1571,11 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
                           cfg->nu, 0, 2, true);
     if (st) return fail(st);
   }
+  if (cfg->time_integrator == JFB_INTEGRATOR_CNAB2) {
+    // Crank-Nicolson implicit half: gamma = dt / 2 (channelflow_kmm.py:267-274)
+    st = build_factor_set(pl, 0.5 * cfg->dt, pl->cnab2, cfg->nu, 0, 2, true);
+    if (st) return fail(st);
+  }
   if (cfg->time_integrator == JFB_INTEGRATOR_IMEXRK222) {
     st = build_factor_set(pl, kG222 * cfg->dt, pl->rk222, cfg->nu, 0, 2, true);
     if (st) return fail(st);
@@ -1527,7 +1617,7 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   // (the coupled MHD step: twelve x-physical fields u, omega, b, j and six
   // nonlinear fields n, emf)
   const size_t xs = pl->mixed ? 2 : 1;
-  const size_t nxf = pl->mhd ? 12 : 6, nhf = pl->mhd ? 6 : 3;
+  const size_t nxf = pl->mhd ? 12 : d.grad ? 9 : 6, nhf = pl->mhd ? 6 : 3;
   if ((st = cal(&pl->X, (nxf * d.Nx * P + xs - 1) / xs))) return fail(st);
   if ((st = cal(&pl->Y, (nxf * d.Nx * d.My * d.Kz + xs - 1) / xs))) return fail(st);
   if ((st = cal(&pl->HZ, nhf * d.Nx * d.My * d.Kz))) return fail(st);
@@ -1685,6 +1775,16 @@ extern "C" int jfb_kmm_advance(jfb_kmm_plan* pl, int64_t steps, void* stream) {
     if (st) return st;
     pl->n += 1;
     pl->hist += 1;
+    pl->explicit_u12 = false;
+    --steps;
+  }
+  // CNAB2: the first step without a previous nonlinear term (IMEX Euler on
+  // the nonlinear part, cnab2.py:185-208); history_steps holds have_old
+  while (steps > 0 && pl->hist < 1 && pl->cfg.time_integrator == JFB_INTEGRATOR_CNAB2) {
+    st = cnab2_step(pl, pl->n, s, false);
+    if (st) return st;
+    pl->n += 1;
+    pl->hist = 1;
     pl->explicit_u12 = false;
     --steps;
   }
@@ -2423,6 +2523,8 @@ extern "C" int jfb_kmm_gain_gradient(jfb_kmm_plan* pl, const jfb_kmm_state* init
               "the adjoint differentiates the SBDF3 step");
   JFB_REQUIRE(pl && init && gain_out, "null pointer");
   JFB_REQUIRE(!pl->mhd && !pl->mixed, "the adjoint runs on FP64 flow plans");
+  JFB_REQUIRE(pl->d.family == 0 && !pl->d.grad,
+              "the adjoint differentiates the Chebyshev rotational-form step");
   JFB_REQUIRE(steps >= 1, "steps must be >= 1");
   JFB_REQUIRE(init->history_steps == 0.0, "the initial state must have history_steps == 0");
   cudaStream_t s = (cudaStream_t)stream;
@@ -2730,7 +2832,8 @@ extern "C" int jfb_kmm_autotune(jfb_kmm_plan* pl, int64_t steps, jfb_kmm_variant
   const size_t ne = checkpoint_elems(pl);
   c64 *save = nullptr, *x_save = nullptr;
   // X: six x-physical fields, complex64 (half the c64 count) in the mixed form
-  const size_t nx = ((size_t)6 * pl->d.Nx * pl->d.P + (pl->mixed ? 1 : 0)) / (pl->mixed ? 2 : 1);
+  const size_t nx = ((size_t)(pl->d.grad ? 9 : 6) * pl->d.Nx * pl->d.P + (pl->mixed ? 1 : 0)) /
+                    (pl->mixed ? 2 : 1);
   JFB_CHECK_CUDA(cudaMalloc((void**)&save, ne * sizeof(c64)));
   cudaError_t ce = cudaMalloc((void**)&x_save, (nx + 2 * (size_t)pl->d.nD * pl->d.P) * sizeof(c64));
   if (ce != cudaSuccess) {

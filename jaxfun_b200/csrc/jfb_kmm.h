@@ -16,18 +16,22 @@ struct Stencil {
 
 struct HostOperators {
   int N = 0, nB = 0, nD = 0;
+  int family = 0;                     // 0 Chebyshev, 1 Legendre (JFB_FAMILY_*)
+  double x_lo = -1, x_hi = 1;
   double dfx = 1, dfy = 1, dfz = 1;
   std::vector<double> xnodes, xphys;  // reference / physical Gauss nodes
-  std::vector<double> V;              // V[j][n] = T_n(X_j)
-  std::vector<double> Q;              // Q[n][j] = T_n(X_j) pi / N / df
-  std::vector<double> ns;             // Chebyshev norms^2 / df
+  std::vector<double> V;              // V[j][n] = P_n(X_j) (T_n or L_n)
+  std::vector<double> Q;              // Q[n][j] = P_n(X_j) w_j / df
+  std::vector<double> ns;             // norms^2 (P_n, P_n) / df
   Stencil SB, SD;
   std::vector<double> XB0, XB2, XB4, XD0, XD2;  // dense Galerkin x-matrices
   std::vector<double> mlo, mdi, mhi;            // Dirichlet mass (= M00) tri-band
   std::vector<double> lu_l, lu_u;               // its no-pivot LU
   // biharmonic mass (offsets -4..4) no-pivot LU: L[i,i-2], L[i,i-4], U[i,i], U[i,i+2], U[i,i+4]
   std::vector<double> bl2, bl4, bu0, bu2, bu4;
-  std::vector<double> fejer;  // Fejer-I weights on the Gauss nodes / df
+  // physical-volume quadrature weights on the Gauss nodes / df: Fejer-I
+  // (Chebyshev.py:182-208) or the Gauss-Legendre weights (Legendre.py:136-147)
+  std::vector<double> fejer;
 };
 
 // Parity-split x-operators of the step in mma.sync m8n8k4 fragment order.
@@ -106,7 +110,7 @@ enum XMap {
 };
 std::vector<double> x_map_matrix(const XBasis& xb, int map, int k, int* rows, int* cols);
 
-Stencil make_stencil(int N, bool biharmonic);
+Stencil make_stencil(int N, bool biharmonic, int family = 0);
 // Builds GemmHost from the 1-D operators; returns false (with a message) if a
 // parity property the split relies on does not hold.
 bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& err);

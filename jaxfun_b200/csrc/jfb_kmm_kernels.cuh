@@ -55,6 +55,8 @@ struct DevOps {
 struct Dims {
   int Nx, nB, nD, Ny, Nz, Kz, P, My, Mz, nKb;
   double dfx, dfy, dfz, Myz, nu, dt, uwall;
+  int family;  // wall-normal family: 0 Chebyshev, 1 Legendre
+  int grad;    // nonlinear term in gradient form u . grad u (else rotational)
 };
 
 struct PackedFactors {
@@ -96,14 +98,16 @@ __host__ __device__ inline int packed_rec_size(int n) {
 // Warp-level helpers (all lanes of the warp call them; arrays in smem).
 // ---------------------------------------------------------------------------
 
-// d = scale * chebder(c) on a length-L coefficient vector; in place allowed.
-// d_n = sum_{m > n, m - n odd} 2 m c_m, d_0 halved (Chebyshev.py:319-353).
-__device__ void chebder_warp(const c64* c, c64* d, int L, double scale, int lane) {
+// d = scale * d/dX of a length-L coefficient vector; in place allowed.
+// Chebyshev (fam 0): d_n = sum_{m > n, m - n odd} 2 m c_m, d_0 halved
+// (Chebyshev.py:319-353); Legendre (fam 1): d_n = (2n + 1) sum_{m > n, m - n
+// odd} c_m (Legendre.py:195-227).
+__device__ void chebder_warp(const c64* c, c64* d, int L, double scale, int lane, int fam) {
   const int K = (L + 31) / 32;
   const int lo = lane * K, hi = min(L, lo + K);
   c64 se = cmk(0.0, 0.0), so = cmk(0.0, 0.0);
   for (int m = lo; m < hi; ++m) {
-    const c64 e = (2.0 * m) * c[m];
+    const c64 e = (fam ? 1.0 : 2.0 * m) * c[m];
     if (m & 1) so = so + e; else se = se + e;
   }
   // inclusive suffix sums over lanes >= lane
@@ -124,9 +128,10 @@ __device__ void chebder_warp(const c64* c, c64* d, int L, double scale, int lane
   for (int n = hi - 1; n >= lo; --n) {
     const c64 cn = c[n];
     c64 dn = (n & 1) ? run_e : run_o;
-    if (n == 0) dn = 0.5 * dn;
+    if (fam) dn = (2.0 * n + 1.0) * dn;
+    else if (n == 0) dn = 0.5 * dn;
     d[n] = scale * dn;
-    const c64 e = (2.0 * n) * cn;
+    const c64 e = (fam ? 1.0 : 2.0 * n) * cn;
     if (n & 1) run_o = run_o + e; else run_e = run_e + e;
   }
   __syncwarp();
@@ -362,7 +367,7 @@ __device__ void reconstruct_warp(const DevOps& o, const Dims& d, const c64* A3,
                                  double kyp, double kzp, c64* A0, c64* A1, c64* A2,
                                  c64* A5, int lane) {
   apply_SBT(o, d, A3, A5, lane);            // A5 = uo0 = S_B^T u0
-  chebder_warp(A5, A0, d.Nx, d.dfx, lane);   // A0 = d/dx uo0
+  chebder_warp(A5, A0, d.Nx, d.dfx, lane, d.family);   // A0 = d/dx uo0
   apply_SD_ns(o, d, A0, A2, 1.0, lane);      // A2 = S_D(ns du)
   if (lane < 2) mass_solve_lane(o, d, A2, lane);  // f = projection into TD
   __syncwarp();
@@ -891,7 +896,7 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
         A1[n] = mul_i(kzp * h1 - kyp * h2);
       }
       __syncwarp();
-      chebder_warp(A0, A2, d.Nx, d.dfx, lane);  // A2 = d/dx t
+      chebder_warp(A0, A2, d.Nx, d.dfx, lane, d.family);  // A2 = d/dx t
       for (int n = lane; n < d.Nx; n += 32) A2[n] = A2[n] + k2 * A3[n];  // Hu
       __syncwarp();
       // Nu = Myz S_B(ns Hu) -> A3 ; Ng = Myz S_D(ns Hg) -> A4
@@ -906,8 +911,8 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
       comb_rows(A0, a.u0a, a.u0b, a.u0c, a.c0, a.c1, a.c2, d.nB, P, p, lane);
       __syncwarp();
       apply_SBT(o, d, A0, A2, lane);            // A2 = S_B^T comb
-      chebder_warp(A2, A5, d.Nx, d.dfx, lane);   // A5 = D comb
-      chebder_warp(A5, A0, d.Nx, d.dfx, lane);   // A0 = D^2 comb
+      chebder_warp(A2, A5, d.Nx, d.dfx, lane, d.family);   // A5 = D comb
+      chebder_warp(A5, A0, d.Nx, d.dfx, lane, d.family);   // A0 = D^2 comb
       for (int n = lane; n < d.Nx; n += 32) A2[n] = A0[n] - k2 * A2[n];
       __syncwarp();
       if (a.cL != 0.0) {
@@ -915,14 +920,14 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
         for (int i = lane; i < d.nB; i += 32) A1[i] = a.u0a[(size_t)i * P + p];
         __syncwarp();
         apply_SBT(o, d, A1, A0, lane);           // A0 = w
-        chebder_warp(A0, A5, d.Nx, d.dfx, lane);
-        chebder_warp(A5, A1, d.Nx, d.dfx, lane);  // A1 = D^2 w
+        chebder_warp(A0, A5, d.Nx, d.dfx, lane, d.family);
+        chebder_warp(A5, A1, d.Nx, d.dfx, lane, d.family);  // A1 = D^2 w
         const double s = a.cL * d.nu;
         for (int n = lane; n < d.Nx; n += 32)
           A2[n] = A2[n] + s * (k2 * k2 * A0[n] - (2.0 * k2) * A1[n]);
         __syncwarp();
-        chebder_warp(A1, A5, d.Nx, d.dfx, lane);
-        chebder_warp(A5, A0, d.Nx, d.dfx, lane);  // A0 = D^4 w
+        chebder_warp(A1, A5, d.Nx, d.dfx, lane, d.family);
+        chebder_warp(A5, A0, d.Nx, d.dfx, lane, d.family);  // A0 = D^4 w
         for (int n = lane; n < d.Nx; n += 32) A2[n] = A2[n] + s * A0[n];
         __syncwarp();
       }
@@ -938,8 +943,8 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
         for (int i = lane; i < d.nD; i += 32) A1[i] = a.ga[(size_t)i * P + p];
         __syncwarp();
         apply_SDT(d, A1, A0, lane);  // A0 = w
-        chebder_warp(A0, A5, d.Nx, d.dfx, lane);
-        chebder_warp(A5, A1, d.Nx, d.dfx, lane);  // A1 = D^2 w
+        chebder_warp(A0, A5, d.Nx, d.dfx, lane, d.family);
+        chebder_warp(A5, A1, d.Nx, d.dfx, lane, d.family);  // A1 = D^2 w
         const double s = a.cL * d.nu;
         for (int n = lane; n < d.Nx; n += 32) A2[n] = A2[n] + s * (A1[n] - k2 * A0[n]);
         __syncwarp();
@@ -962,8 +967,8 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
           for (int i = lane; i < d.nD; i += 32) A1[i] = a.vwa[i];
           __syncwarp();
           apply_SDT(d, A1, A0, lane);
-          chebder_warp(A0, A5, d.Nx, d.dfx, lane);
-          chebder_warp(A5, A1, d.Nx, d.dfx, lane);
+          chebder_warp(A0, A5, d.Nx, d.dfx, lane, d.family);
+          chebder_warp(A5, A1, d.Nx, d.dfx, lane, d.family);
           for (int n = lane; n < d.Nx; n += 32) A2[n] = A2[n] + (a.cL * d.nu) * A1[n];
           __syncwarp();
         }
@@ -1016,13 +1021,20 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
     // A5 = uo0 (already); uo1 = S_D^T u1 -> A2, uo2 = S_D^T u2 -> A3
     apply_SDT(d, A0, A2, lane);
     apply_SDT(d, A1, A3, lane);
-    chebder_warp(A3, A4, d.Nx, d.dfx, lane);  // A4 = D uo2
-    chebder_warp(A2, A0, d.Nx, d.dfx, lane);  // A0 = D uo1
-    for (int n = lane; n < d.Nx; n += 32) {
-      const c64 u0 = A5[n], u1 = A2[n], u2 = A3[n];
-      A1[n] = mul_i(kyp * u2 - kzp * u1);        // omega_0
-      A4[n] = mul_i(kzp * u0) - A4[n];           // omega_1
-      A0[n] = A0[n] - mul_i(kyp * u0);           // omega_2
+    chebder_warp(A3, A4, d.Nx, d.dfx, lane, d.family);  // A4 = D uo2
+    chebder_warp(A2, A0, d.Nx, d.dfx, lane, d.family);  // A0 = D uo1
+    if (d.grad) {
+      // gradient form: the x-derivatives of the three components
+      // (channelflow_kmm.py:716-740); the y / z derivatives are wavenumber
+      // weights applied on the way to the periodic transforms
+      chebder_warp(A5, A1, d.Nx, d.dfx, lane, d.family);  // A1 = D uo0
+    } else {
+      for (int n = lane; n < d.Nx; n += 32) {
+        const c64 u0 = A5[n], u1 = A2[n], u2 = A3[n];
+        A1[n] = mul_i(kyp * u2 - kzp * u1);        // omega_0
+        A4[n] = mul_i(kzp * u0) - A4[n];           // omega_1
+        A0[n] = A0[n] - mul_i(kyp * u0);           // omega_2
+      }
     }
     __syncwarp();
   } else {
@@ -1031,13 +1043,16 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
   }
   __syncthreads();
   // x-backward of the six fields: field order (u0, u1, u2, w0, w1, w2) lives
-  // in arrays (A5, A2, A3, A1, A4, A0).  Their B-operand rows go into R1 (dead
-  // by now), the product into ARR (dead once the rows are built).
+  // in arrays (A5, A2, A3, A1, A4, A0); in the gradient form (u0, u1, u2,
+  // d/dx u0, d/dx u1, d/dx u2) in (A5, A2, A3, A1, A0, A4).  Their B-operand
+  // rows go into R1 (dead by now), the product into ARR (dead once the rows
+  // are built).
   double* Bs = reinterpret_cast<double*>(R1);
   for (int idx = threadIdx.x; idx < d.Nx * 6 * kNW; idx += blockDim.x) {
     const int n = idx % d.Nx, wf = idx / d.Nx;
     const int w = wf / 6, f = wf % 6;
-    const int arr = (f == 0) ? 5 : (f == 1) ? 2 : (f == 2) ? 3 : (f == 3) ? 1 : (f == 4) ? 4 : 0;
+    const int arr = (f == 0) ? 5 : (f == 1) ? 2 : (f == 2) ? 3 : (f == 3) ? 1
+                    : (f == 4) ? (d.grad ? 0 : 4) : (d.grad ? 4 : 0);
     const c64 v = ARR[(w * 6 + arr) * d.Nx + n];
     *reinterpret_cast<double2*>(Bs + (size_t)n * kLDB + 2 * wf) = make_double2(v.re, v.im);
   }
@@ -1051,6 +1066,13 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
       const c64 v = ARR[fi * kNW + w];
       if (a.x32) reinterpret_cast<c32*>(a.X)[e] = cmk((float)v.re, (float)v.im);
       else a.X[e] = v;
+      if (d.grad && fi < 3 * d.Nx) {
+        // fields 6..8: d/dy u_i = i ky u_i (the CTA's pencils share ky)
+        const c64 dy = mul_i(kyp * v);
+        const size_t ey = (size_t)(6 * d.Nx + fi) * P + p0 + w;
+        if (a.x32) reinterpret_cast<c32*>(a.X)[ey] = cmk((float)dy.re, (float)dy.im);
+        else a.X[ey] = dy;
+      }
     }
   }
 }
@@ -1180,6 +1202,92 @@ __global__ void __launch_bounds__(256) z_cross_kernel(DevOps o, Dims d, FFTPlan 
     const T h = T(0.5);
     if (take_real) v = cmk(h * (Zk.re + Zm.re), h * (Zk.im - Zm.im));
     else v = cmk(h * (Zk.im + Zm.im), -h * (Zk.re - Zm.re));
+    HZ[(size_t)f * plane + (size_t)row * d.Kz + k] = scale * v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z_grad: the z stage of the gradient form (channelflow_kmm.py:754-770 with
+// the base-flow terms of pcf_fluctuations_jax.py:99-106), per group of 4
+// (x, y) rows.  Y holds nine y-physical fields (u_i, d/dx u_i, d/dy u_i);
+// d/dz u_i = i kz u_i is formed here.  Twelve real fields, two per complex
+// inverse transform, give
+//   n_i = u_0 d/dx u_i + u_1 d/dy u_i + u_2 d/dz u_i + U_b d/dy u_i
+//         (+ u_0 dU_b/dx for i = 1),
+// forward transformed two per complex transform (n2 alone).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) z_grad_kernel(DevOps o, Dims d, FFTPlan plan,
+                                                     const c64* __restrict__ tw,
+                                                     const c64* __restrict__ Y,
+                                                     c64* __restrict__ HZ) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NC = kZRows * 6;   // packed input columns
+  constexpr int NCf = kZRows * 2;  // packed output columns: (n0 + i n1), (n2 + i 0)
+  c64* A = reinterpret_cast<c64*>(smem_raw);
+  c64* B = A + d.Mz * NC;
+  const int row0 = blockIdx.x * kZRows;  // row = j * My + y
+  const int nrows = d.Nx * d.My;
+  const size_t plane = (size_t)d.Nx * d.My * d.Kz;
+  // virtual real field v: v < 9 is Y field v, v >= 9 is i kz (Y field v - 9)
+  auto spec = [&](int v, int row, int k) -> c64 {
+    const c64 x = Y[(size_t)(v < 9 ? v : v - 9) * plane + (size_t)row * d.Kz + k];
+    return v < 9 ? x : mul_i((k * d.dfz) * x);
+  };
+  for (int idx = threadIdx.x; idx < d.Mz * NC; idx += blockDim.x) {
+    const int k = idx % d.Mz, c = idx / d.Mz;
+    const int rl = c / 6, pr = c % 6;
+    const int row = row0 + rl;
+    c64 z = cmk(0.0, 0.0);
+    if (row < nrows) {
+      if (k == 0) {
+        z = cmk(spec(2 * pr, row, 0).re, spec(2 * pr + 1, row, 0).re);
+      } else if (k < d.Kz) {
+        const c64 xa = spec(2 * pr, row, k), xb = spec(2 * pr + 1, row, k);
+        z = cmk(xa.re - xb.im, xa.im + xb.re);
+      } else if (k > d.Mz - d.Kz) {
+        const int kk = d.Mz - k;
+        const c64 xa = spec(2 * pr, row, kk), xb = spec(2 * pr + 1, row, kk);
+        z = cmk(xa.re + xb.im, -xa.im + xb.re);  // conj(xa) + i conj(xb)
+      }
+    }
+    A[k * NC + c] = z;
+  }
+  __syncthreads();
+  c64* phys = fft_columns<double>(A, B, plan, NC, NC, tw, +1);
+  c64* other = (phys == A) ? B : A;
+  for (int idx = threadIdx.x; idx < d.Mz * kZRows; idx += blockDim.x) {
+    const int rl = idx % kZRows, n = idx / kZRows;
+    const int row = row0 + rl;
+    const int j = (row < nrows) ? row / d.My : 0;
+    const c64* z = phys + n * NC + rl * 6;
+    const double u0 = z[0].re, u1 = z[0].im, u2 = z[1].re;
+    const double x0 = z[1].im, x1 = z[2].re, x2 = z[2].im;  // d/dx
+    const double y0 = z[3].re, y1 = z[3].im, y2 = z[4].re;  // d/dy
+    const double z0 = z[4].im, z1 = z[5].re, z2 = z[5].im;  // d/dz
+    const double ub = d.uwall * o.xphys[j];
+    const double n0 = (u0 * x0 + u1 * y0 + u2 * z0) + ub * y0;
+    const double n1 = ((u0 * x1 + u1 * y1 + u2 * z1) + ub * y1) + u0 * d.uwall;
+    const double n2 = (u0 * x2 + u1 * y2 + u2 * z2) + ub * y2;
+    c64* out = other + n * NCf + rl * 2;
+    out[0] = cmk(n0, n1);
+    out[1] = cmk(n2, 0.0);
+  }
+  __syncthreads();
+  c64* res = fft_columns<double>(other, phys, plan, NCf, NCf, tw, -1);
+  const double scale = 1.0 / d.Mz;
+  for (int idx = threadIdx.x; idx < d.Kz * kZRows * 3; idx += blockDim.x) {
+    const int k = idx % d.Kz;
+    const int rf = idx / d.Kz;
+    const int f = rf % 3, rl = rf / 3;
+    const int row = row0 + rl;
+    if (row >= nrows) continue;
+    const int col = rl * 2 + f / 2;
+    const c64 Zk = res[k * NCf + col];
+    const c64 Zm = res[((d.Mz - k) % d.Mz) * NCf + col];
+    // x + i y packed: X_k = (Z_k + conj Z_-k)/2, Y_k = (Z_k - conj Z_-k)/(2i)
+    c64 v;
+    if ((f & 1) == 0) v = cmk(0.5 * (Zk.re + Zm.re), 0.5 * (Zk.im - Zm.im));
+    else v = cmk(0.5 * (Zk.im + Zm.im), -0.5 * (Zk.re - Zm.re));
     HZ[(size_t)f * plane + (size_t)row * d.Kz + k] = scale * v;
   }
 }
@@ -1329,7 +1437,7 @@ __global__ void __launch_bounds__(256) diag_kernel(DevOps o, Dims d, const c64* 
       }
     }
     __syncwarp();
-    chebder_warp(B0, B3, d.Nx, d.dfx, lane);
+    chebder_warp(B0, B3, d.Nx, d.dfx, lane, d.family);
     for (int n = lane; n < d.Nx; n += 32) B3[n] = B3[n] + mul_i(kyp * B1[n] + kzp * B2[n]);
     __syncwarp();
     const double mult = (kz == 0) ? 1.0 : 2.0;
@@ -1354,14 +1462,15 @@ __global__ void __launch_bounds__(256) diag_kernel(DevOps o, Dims d, const c64* 
     }
     if (ky == 0 && kz == 0) {
       // wall values and wall derivatives of the mean streamwise velocity
-      chebder_warp(B1, B3, d.Nx, d.dfx, lane);
+      chebder_warp(B1, B3, d.Nx, d.dfx, lane, d.family);
       if (lane == 0) {
         double top = 0.0, bot = 0.0, stop = 0.0, sbot = 0.0, shear = 0.0;
         for (int n = 0; n < d.Nx; ++n) {
           const double sgn = (n & 1) ? -1.0 : 1.0;
           top += B1[n].re;
           bot += sgn * B1[n].re;
-          const double n2 = (double)n * n;
+          // d/dX P_n at X = 1: n^2 (Chebyshev), n (n + 1) / 2 (Legendre)
+          const double n2 = d.family ? 0.5 * n * (n + 1.0) : (double)n * n;
           stop += n2 * B1[n].re * d.dfx;
           sbot += -sgn * n2 * B1[n].re * d.dfx;
         }

@@ -59,6 +59,22 @@ static std::vector<double> chebyshev_galerkin(int N, int k) {
   return M;
 }
 
+// (L_i, d^k L_j / dX^k)_w of the Legendre polynomials as a dense N x N
+// matrix: (L_j)' = sum_{i<j, j-i odd} (2i+1) L_i (Legendre.py:195-227) and
+// (L_i, L_i) = 2 / (2i + 1) (Legendre.py:19-33, 229-268).
+static std::vector<double> legendre_galerkin(int N, int k) {
+  std::vector<int64_t> D((size_t)N * N, 0), D1((size_t)N * N, 0);
+  for (int i = 0; i < N; ++i) D[(size_t)i * N + i] = 1;
+  for (int i = 0; i < N; ++i)
+    for (int j = i + 1; j < N; j += 2) D1[(size_t)i * N + j] = 2 * i + 1;
+  for (int t = 0; t < k; ++t) D = int_matmul(D1, D, N);
+  std::vector<double> M((size_t)N * N);
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j)
+      M[(size_t)i * N + j] = 2.0 / (2.0 * i + 1.0) * (double)D[(size_t)i * N + j];
+  return M;
+}
+
 // S X S^T for a stencil with diagonals s0, s2, s4 (s4 may be empty).
 static std::vector<double> stencil_sandwich(const std::vector<double>& X, int N,
                                             const Stencil& S) {
@@ -82,7 +98,10 @@ static std::vector<double> stencil_sandwich(const std::vector<double>& X, int N,
   return R;
 }
 
-Stencil make_stencil(int N, bool biharmonic) {
+// Shen stencils (composite.py:797-864): Dirichlet P_i - P_{i+2} for both
+// families; biharmonic T_i - 2(i+2)/(i+3) T_{i+2} + (i+1)/(i+3) T_{i+4} or
+// L_i - 2(2i+5)/(2i+7) L_{i+2} + (2i+3)/(2i+7) L_{i+4}.
+Stencil make_stencil(int N, bool biharmonic, int family) {
   Stencil S;
   S.width = biharmonic ? 4 : 2;
   S.n = N - S.width;
@@ -92,8 +111,13 @@ Stencil make_stencil(int N, bool biharmonic) {
   if (biharmonic) {
     for (int i = 0; i < S.n; ++i) {
       const double n = i;
-      S.s2[i] = 2.0 * (-n - 2.0) / (n + 3.0);
-      S.s4[i] = (n + 1.0) / (n + 3.0);
+      if (family == 0) {
+        S.s2[i] = 2.0 * (-n - 2.0) / (n + 3.0);
+        S.s4[i] = (n + 1.0) / (n + 3.0);
+      } else {
+        S.s2[i] = 2.0 * (-2.0 * n - 5.0) / (2.0 * n + 7.0);
+        S.s4[i] = (2.0 * n + 3.0) / (2.0 * n + 7.0);
+      }
     }
   }
   return S;
@@ -104,47 +128,68 @@ void build_host_operators(const jfb_kmm_config& cfg, HostOperators& op) {
   op.N = N;
   op.nB = N - 4;
   op.nD = N - 2;
+  op.family = cfg.family == JFB_FAMILY_LEGENDRE ? 1 : 0;
+  op.x_lo = cfg.x_lo;
+  op.x_hi = cfg.x_hi;
   const double Lx = cfg.x_hi - cfg.x_lo;
   op.dfx = std::fabs(Lx - 2.0) < 1e-12 ? 1.0 : 2.0 / Lx;
   const double Ly = cfg.ly, Lz = cfg.lz;
   op.dfy = std::fabs(Ly - 2.0 * M_PI) < 1e-12 ? 1.0 : 2.0 * M_PI / Ly;
   op.dfz = std::fabs(Lz - 2.0 * M_PI) < 1e-12 ? 1.0 : 2.0 * M_PI / Lz;
 
-  // Gauss-Chebyshev nodes X_j = cos(pi + (2j+1) pi / (2N)) and T_n(X_j).
   op.xnodes.resize(N);
   op.xphys.resize(N);
-  for (int j = 0; j < N; ++j) {
-    op.xnodes[j] = std::cos(M_PI + (2.0 * j + 1.0) * M_PI / (2.0 * N));
-    op.xphys[j] = cfg.x_lo + (op.xnodes[j] + 1.0) / op.dfx;
-  }
-  op.V.assign((size_t)N * N, 0.0);  // V[j][n] = T_n(X_j)
-  for (int j = 0; j < N; ++j) {
-    double t0 = 1.0, t1 = op.xnodes[j];
-    op.V[(size_t)j * N + 0] = 1.0;
-    if (N > 1) op.V[(size_t)j * N + 1] = t1;
-    for (int n = 2; n < N; ++n) {
-      const double t2 = 2.0 * op.xnodes[j] * t1 - t0;
-      op.V[(size_t)j * N + n] = t2;
-      t0 = t1;
-      t1 = t2;
+  XBasis leg;  // Legendre: nodes, Vandermonde and quadrature in long double
+  if (op.family == 1) {
+    build_x_basis(1, 0, N, cfg.x_lo, cfg.x_hi, leg);
+    op.V.assign((size_t)N * N, 0.0);
+    op.Q.assign((size_t)N * N, 0.0);
+    op.ns.assign(N, 0.0);
+    for (int j = 0; j < N; ++j) {
+      op.xnodes[j] = (double)leg.X[j];
+      op.xphys[j] = cfg.x_lo + (op.xnodes[j] + 1.0) / op.dfx;
+      op.ns[j] = (double)leg.ns[j];
     }
+    for (size_t k = 0; k < op.V.size(); ++k) {
+      op.V[k] = (double)leg.V[k];
+      op.Q[k] = (double)leg.Q[k];
+    }
+  } else {
+    // Gauss-Chebyshev nodes X_j = cos(pi + (2j+1) pi / (2N)) and T_n(X_j).
+    for (int j = 0; j < N; ++j) {
+      op.xnodes[j] = std::cos(M_PI + (2.0 * j + 1.0) * M_PI / (2.0 * N));
+      op.xphys[j] = cfg.x_lo + (op.xnodes[j] + 1.0) / op.dfx;
+    }
+    op.V.assign((size_t)N * N, 0.0);  // V[j][n] = T_n(X_j)
+    for (int j = 0; j < N; ++j) {
+      double t0 = 1.0, t1 = op.xnodes[j];
+      op.V[(size_t)j * N + 0] = 1.0;
+      if (N > 1) op.V[(size_t)j * N + 1] = t1;
+      for (int n = 2; n < N; ++n) {
+        const double t2 = 2.0 * op.xnodes[j] * t1 - t0;
+        op.V[(size_t)j * N + n] = t2;
+        t0 = t1;
+        t1 = t2;
+      }
+    }
+    // Scalar products (T_n, u)_w by Gauss-Chebyshev quadrature: weight pi/N/df.
+    op.Q.assign((size_t)N * N, 0.0);
+    for (int n = 0; n < N; ++n)
+      for (int j = 0; j < N; ++j)
+        op.Q[(size_t)n * N + j] = op.V[(size_t)j * N + n] * (M_PI / N) / op.dfx;
+
+    op.ns = chebyshev_norm2(N);
+    for (double& v : op.ns) v /= op.dfx;
   }
-  // Scalar products (T_n, u)_w by Gauss-Chebyshev quadrature: weight pi/N/df.
-  op.Q.assign((size_t)N * N, 0.0);
-  for (int n = 0; n < N; ++n)
-    for (int j = 0; j < N; ++j)
-      op.Q[(size_t)n * N + j] = op.V[(size_t)j * N + n] * (M_PI / N) / op.dfx;
 
-  op.ns = chebyshev_norm2(N);
-  for (double& v : op.ns) v /= op.dfx;
-
-  op.SB = make_stencil(N, true);
-  op.SD = make_stencil(N, false);
+  op.SB = make_stencil(N, true, op.family);
+  op.SD = make_stencil(N, false, op.family);
 
   // Galerkin x-matrices (including the df^(k-1) domain scaling).
-  const std::vector<double> T0 = chebyshev_galerkin(N, 0);
-  const std::vector<double> T2 = chebyshev_galerkin(N, 2);
-  const std::vector<double> T4 = chebyshev_galerkin(N, 4);
+  auto galerkin = op.family == 1 ? legendre_galerkin : chebyshev_galerkin;
+  const std::vector<double> T0 = galerkin(N, 0);
+  const std::vector<double> T2 = galerkin(N, 2);
+  const std::vector<double> T4 = galerkin(N, 4);
   auto scaled = [&](std::vector<double> X, int k) {
     const double f = std::pow(op.dfx, k - 1);
     for (double& v : X) v *= f;
@@ -205,8 +250,13 @@ void build_host_operators(const jfb_kmm_config& cfg, HostOperators& op) {
     if (i + 4 < nB) op.bu4[i] = A[(size_t)i * nB + i + 4];
   }
 
-  // Fejer-I weights for physical-volume integrals (Chebyshev.py:182-208).
   op.fejer.assign(N, 0.0);
+  if (op.family == 1) {
+    // Gauss-Legendre weights / df: Q[0][j] = L_0(X_j) w_j / df
+    for (int j = 0; j < N; ++j) op.fejer[j] = (double)leg.Q[j];
+    return;
+  }
+  // Fejer-I weights for physical-volume integrals (Chebyshev.py:182-208).
   for (int j = 0; j < N; ++j) {
     const double theta = M_PI + (2.0 * j + 1.0) * M_PI / (2.0 * N);
     double corr = 0.0;
@@ -353,20 +403,31 @@ bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& er
   const LD pi = std::acos(-1.0L);
   const LD dfx = op.dfx;
   LMat V(N, N), Q(N, N), D(N, N), W(N, N), SB(nB, N), SD(nD, N);
-  for (int j = 0; j < N; ++j) {
-    const LD th = pi + (2.0L * j + 1.0L) * pi / (2.0L * N);
-    for (int n = 0; n < N; ++n) V(j, n) = std::cos((LD)n * th);
-  }
-  for (int n = 0; n < N; ++n)
-    for (int j = 0; j < N; ++j) Q(n, j) = V(j, n) * (pi / N) / dfx;
-  for (int i = 0; i < N; ++i)
-    for (int j = i + 1; j < N; j += 2) D(i, j) = dfx * (LD)((i == 0) ? j : 2 * j);
-  for (int n = 0; n < N; ++n) W(n, n) = ((n == 0) ? pi : pi / 2.0L) / dfx;
-  for (int i = 0; i < nB; ++i) {
-    const LD n = i;
-    SB(i, i) = 1.0L;
-    SB(i, i + 2) = 2.0L * (-n - 2.0L) / (n + 3.0L);
-    SB(i, i + 4) = (n + 1.0L) / (n + 3.0L);
+  if (op.family == 1) {
+    // Legendre: Gauss-Legendre nodes, L_n(X_j), legder, norms 2/(2n+1)/df
+    XBasis xb;
+    build_x_basis(1, 2, N, op.x_lo, op.x_hi, xb);
+    V.v = xb.V;
+    Q.v = xb.Q;
+    for (size_t k = 0; k < D.v.size(); ++k) D.v[k] = dfx * xb.D[k];
+    for (int n = 0; n < N; ++n) W(n, n) = xb.ns[n];
+    for (size_t k = 0; k < SB.v.size(); ++k) SB.v[k] = xb.S[k];
+  } else {
+    for (int j = 0; j < N; ++j) {
+      const LD th = pi + (2.0L * j + 1.0L) * pi / (2.0L * N);
+      for (int n = 0; n < N; ++n) V(j, n) = std::cos((LD)n * th);
+    }
+    for (int n = 0; n < N; ++n)
+      for (int j = 0; j < N; ++j) Q(n, j) = V(j, n) * (pi / N) / dfx;
+    for (int i = 0; i < N; ++i)
+      for (int j = i + 1; j < N; j += 2) D(i, j) = dfx * (LD)((i == 0) ? j : 2 * j);
+    for (int n = 0; n < N; ++n) W(n, n) = ((n == 0) ? pi : pi / 2.0L) / dfx;
+    for (int i = 0; i < nB; ++i) {
+      const LD n = i;
+      SB(i, i) = 1.0L;
+      SB(i, i + 2) = 2.0L * (-n - 2.0L) / (n + 3.0L);
+      SB(i, i + 4) = (n + 1.0L) / (n + 3.0L);
+    }
   }
   for (int i = 0; i < nD; ++i) {
     SD(i, i) = 1.0L;

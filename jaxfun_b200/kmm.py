@@ -14,13 +14,15 @@ import ctypes
 import math
 from dataclasses import dataclass, replace
 
+import numpy as np
 import torch
 
 from . import _lib
 
 _STEPPERS = {"IMEXRK222", "IMEXRK3", "CNAB2", "SBDF3"}
 _GPU_STEPPERS = {"SBDF3": _lib.JFB_INTEGRATOR_SBDF3, "IMEXRK3": _lib.JFB_INTEGRATOR_IMEXRK3,
-                 "IMEXRK222": _lib.JFB_INTEGRATOR_IMEXRK222}
+                 "IMEXRK222": _lib.JFB_INTEGRATOR_IMEXRK222,
+                 "CNAB2": _lib.JFB_INTEGRATOR_CNAB2}
 
 
 @dataclass(frozen=True)
@@ -34,6 +36,8 @@ class KMMState:
     solution_old: tuple | None = None
     solution_older: tuple | None = None
     history_steps: float = 0.0
+    have_old: float = 0.0  # CNAB2: nonlinear_old holds N(u^(n-1))
+    previous_dt: float = 0.0
 
 
 def _ptr(t: torch.Tensor | None) -> int | None:
@@ -49,12 +53,17 @@ def _ptr(t: torch.Tensor | None) -> int | None:
 class KMM:
     """Velocity-vorticity KMM channel solver (channelflow_kmm.py:104-230).
 
-    Supported on the GPU path: Chebyshev family, wall-normal axis unpadded,
-    rotational nonlinear form; time integrators SBDF3 (IMEXRK3 startup),
-    IMEXRK3 and IMEXRK222 (the one-step integrators keep no history: the
-    state's history fields pass through unchanged, as in the reference's
-    ``KMM.step``).  The coefficient path ("optimized" or "transform") only
-    changes round-off in the reference
+    Same constructor defaults as the reference: gradient nonlinear form,
+    ``time_integrator=None`` meaning IMEXRK222, the "transform" coefficient
+    path.  Supported on the GPU path: Chebyshev or Legendre family,
+    wall-normal axis unpadded, the gradient form ``u . grad u`` (FP64
+    precision) or the rotational form ``-(u x omega)`` (FP64 or mixed); time
+    integrators SBDF3 (IMEXRK3 startup), IMEXRK3, IMEXRK222 (the one-step
+    integrators keep no history: the state's history fields pass through
+    unchanged, as in the reference's ``KMM.step``) and CNAB2 with the
+    plan's fixed ``dt`` (``nonlinear_old``, ``have_old`` and ``previous_dt``
+    carry its history, as in the reference's ``_cnab2_flow_update``).  The coefficient path
+    ("optimized" or "transform") only changes round-off in the reference
     (tests/couette/test_pcf_fluctuations_jax.py:16-52), so both names select
     the same coefficient-space kernels.
     """
@@ -68,9 +77,9 @@ class KMM:
         family: str = "C",
         padding_factor=(1.0, 1.5, 1.5),
         dpdy: float = 0.0,
-        time_integrator: str | None = "SBDF3",
-        nonlinear_form: str = "rotational",
-        coefficient_path: str = "optimized",
+        time_integrator: str | None = None,
+        nonlinear_form: str = "gradient",
+        coefficient_path: str = "transform",
         solve_batching: str = "batched",
         precision: str = "fp64",
         device: str | torch.device = "cuda",
@@ -94,24 +103,28 @@ class KMM:
                 "time_integrator must be one of "
                 "{'IMEXRK222', 'IMEXRK3', 'CNAB2', 'SBDF3'}"
             )
+        # channelflow_kmm.py:149-193: no integrator named -> IMEXRK222
+        if time_integrator is None:
+            time_integrator = "IMEXRK222"
+        fam = str(family).upper()[:1]
+        if fam not in ("C", "L"):
+            raise ValueError("family must be 'C' (Chebyshev) or 'L' (Legendre)")
         unsupported = []
         if time_integrator not in _GPU_STEPPERS:
             unsupported.append(f"time_integrator={time_integrator!r}")
-        if self.nonlinear_form != "rotational":
-            unsupported.append(f"nonlinear_form={self.nonlinear_form!r}")
-        if not str(family).upper().startswith("C"):
-            unsupported.append(f"family={family!r}")
+        if self.nonlinear_form == "gradient" and precision != "fp64":
+            unsupported.append(f"nonlinear_form='gradient' with precision={precision!r}")
         if self.padding_factor[0] != 1.0:
             unsupported.append("wall-normal padding")
         if float(dpdy) != 0.0:
             unsupported.append("dpdy != 0")
         if unsupported:
             raise NotImplementedError(
-                "the B200 step supports SBDF3, IMEXRK3 or IMEXRK222 / rotational / "
-                "Chebyshev / unpadded x only; requested " + ", ".join(unsupported)
+                "the B200 step supports SBDF3, IMEXRK3 or IMEXRK222 / gradient (FP64) or "
+                "rotational / unpadded x only; requested " + ", ".join(unsupported)
             )
         self.time_integrator = time_integrator
-        self.family = "C"
+        self.family = fam
         self.precision = precision
         self.device = torch.device(device)
         if self.device.type != "cuda":
@@ -122,7 +135,7 @@ class KMM:
         self.shape_D = (Nx - 2, Ny, Nz)
         cfg = _lib.KMMConfig()
         cfg.nx, cfg.ny, cfg.nz = Nx, Ny, Nz
-        cfg.family = _lib.JFB_FAMILY_CHEBYSHEV
+        cfg.family = _lib.JFB_FAMILY_LEGENDRE if fam == "L" else _lib.JFB_FAMILY_CHEBYSHEV
         cfg.x_lo, cfg.x_hi = self.domain[0]
         cfg.ly = self.domain[1][1] - self.domain[1][0]
         cfg.lz = self.domain[2][1] - self.domain[2][0]
@@ -134,7 +147,8 @@ class KMM:
             "fp64": _lib.JFB_PRECISION_FP64,
             "mixed": _lib.JFB_PRECISION_MIXED,
         }[precision]
-        cfg.nonlinear_form = _lib.JFB_NONLINEAR_ROTATIONAL
+        cfg.nonlinear_form = (_lib.JFB_NONLINEAR_GRADIENT if self.nonlinear_form == "gradient"
+                              else _lib.JFB_NONLINEAR_ROTATIONAL)
         cfg.time_integrator = _GPU_STEPPERS[self.time_integrator]
         self._cfg = cfg
         handle = ctypes.c_void_p()
@@ -173,7 +187,8 @@ class KMM:
             arr = getattr(c, name)
             for k in range(4):
                 arr[k] = _ptr(lv[k]) if lv is not None else None
-        c.history_steps = float(st.history_steps)
+        c.history_steps = (float(bool(st.have_old)) if self.time_integrator == "CNAB2"
+                           else float(st.history_steps))
         return c
 
     def _empty_state(self) -> KMMState:
@@ -221,6 +236,15 @@ class KMM:
         """Zero history levels for a fresh state (channelflow_kmm.py:609-654)."""
         if state.solution_old is not None and state.nonlinear_old is not None:
             return state
+        if self.time_integrator == "CNAB2" and state.nonlinear_old is not None:
+            # CNAB2 keeps one nonlinear level; the plan's other levels are unused
+            z = (
+                torch.zeros_like(state.u[0]),
+                torch.zeros_like(state.g),
+                torch.zeros(self.shape_D[0], dtype=torch.float64, device=self.device),
+                torch.zeros(self.shape_D[0], dtype=torch.float64, device=self.device),
+            )
+            return replace(state, nonlinear_older=z, solution_old=z, solution_older=z)
         z = (
             torch.zeros_like(state.u[0]),
             torch.zeros_like(state.g),
@@ -234,6 +258,8 @@ class KMM:
             solution_old=z,
             solution_older=z,
             history_steps=0.0,
+            have_old=0.0,
+            previous_dt=0.0,
         )
 
     # -- reference API ----------------------------------------------------------
@@ -250,7 +276,11 @@ class KMM:
         return self._ensure_history(st)
 
     def step(self, state: KMMState, dt=None, factor_args=None) -> KMMState:
-        """One SBDF3 step (IMEXRK3 startup while history_steps < 2)."""
+        """One step of the plan's integrator (SBDF3: IMEXRK3 startup while
+        history_steps < 2).  The factors belong to the plan's fixed time
+        step, so ``dt`` must be None or equal to it."""
+        if dt is not None and float(dt) != self.dt:
+            raise NotImplementedError("the B200 step runs the plan's fixed dt")
         return self.solve(state, 1)
 
     def solve(self, state: KMMState, steps: int) -> KMMState:
@@ -260,12 +290,27 @@ class KMM:
         solved coefficient became NaN or infinite, as the reference's runner
         does for a non-finite state (production/oracles.py:3257-3261)."""
         steps = int(steps)
+        if (self.time_integrator == "CNAB2" and state.have_old
+                and float(state.previous_dt) not in (0.0, self.dt)):
+            raise NotImplementedError(
+                "CNAB2 history from a different step size (variable_ab2_extrapolate "
+                "ratio != 1); the B200 plan runs a fixed dt")
         self._load(state)
         loaded = self._current
         hist = float(loaded.history_steps)
         _lib.call("jfb_kmm_advance", self._plan, steps, self._stream())
         if self.time_integrator == "SBDF3":
             out = self._fetch(min(2.0, hist + steps))
+        elif self.time_integrator == "CNAB2":
+            was = float(bool(loaded.have_old))
+            out = self._fetch(0.0)
+            if steps > 0:
+                out = replace(out, have_old=1.0, previous_dt=self.dt,
+                              nonlinear_older=None, solution_old=None, solution_older=None)
+            else:
+                out = replace(out, have_old=was, previous_dt=loaded.previous_dt,
+                              nonlinear_older=None, solution_old=None, solution_older=None)
+            self._current = out
         else:  # one-step integrators: the history fields pass through
             out = replace(self._fetch(hist), nonlinear_old=loaded.nonlinear_old,
                           nonlinear_older=loaded.nonlinear_older,
@@ -335,13 +380,18 @@ class KMM:
 
     # -- meshes and physical-space entry points -------------------------------
     def mesh(self):
-        """Quadrature mesh (x on Gauss-Chebyshev nodes, y/z uniform), broadcast
-        like ``TensorProductSpace.mesh`` (tensorproductspace.py:207-232)."""
+        """Quadrature mesh (x on the Gauss-Chebyshev or Gauss-Legendre nodes,
+        y/z uniform), broadcast like ``TensorProductSpace.mesh``
+        (tensorproductspace.py:207-232; Legendre.py:136-147 takes numpy's
+        ``leggauss`` nodes)."""
         Nx, Ny, Nz = self.N
         (a, b), (y0, y1), (z0, z1) = self.domain
-        X = torch.cos(
-            math.pi + (2 * torch.arange(Nx, dtype=torch.float64) + 1) * math.pi / (2 * Nx)
-        )
+        if self.family == "L":
+            X = torch.from_numpy(np.polynomial.legendre.leggauss(Nx)[0])
+        else:
+            X = torch.cos(
+                math.pi + (2 * torch.arange(Nx, dtype=torch.float64) + 1) * math.pi / (2 * Nx)
+            )
         x = a + (X + 1.0) * (b - a) / 2.0
         y = y0 + torch.arange(Ny, dtype=torch.float64) * (y1 - y0) / Ny
         z = z0 + torch.arange(Nz, dtype=torch.float64) * (z1 - z0) / Nz
@@ -421,9 +471,9 @@ class PlaneCouetteFluctuation(KMM):
         padding_factor=(1.0, 1.5, 1.5),
         perturbation_amplitude: float = 0.05,
         timestepper=None,
-        time_integrator: str | None = "SBDF3",
-        nonlinear_form: str = "rotational",
-        coefficient_path: str = "optimized",
+        time_integrator: str | None = None,
+        nonlinear_form: str = "gradient",
+        coefficient_path: str = "transform",
         solve_batching: str = "batched",
         precision: str = "fp64",
         device="cuda",

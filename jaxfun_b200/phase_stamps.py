@@ -48,7 +48,7 @@ def main(argv=None) -> int:
     dom = ((-1.0, 1.0), (0.0, 4.0 * math.pi), (0.0, 2.0 * math.pi))
     dev = torch.device("cuda", 0)
     g = PlaneCouetteFluctuation(N=grid, domain=dom, Re=1000.0, dt=0.01, precision=a.precision,
-                                device=dev)
+                                device=dev, time_integrator="SBDF3", nonlinear_form="rotational")
     f = couette_perturbation_fields(grid, dom)
     f = scale_to_energy(f, g.diagnostics(g.state_from_physical(f))["Epert"], 1e-4)
     g.solve(g.state_from_physical(f), 5)

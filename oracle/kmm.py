@@ -878,6 +878,8 @@ class KMMState:
     solution_old: tuple | None = None
     solution_older: tuple | None = None
     history_steps: float = 0.0
+    have_old: float = 0.0  # CNAB2: nonlinear_old holds N(u^(n-1))
+    previous_dt: float = 0.0
 
 
 class KMMOracle:
@@ -901,7 +903,7 @@ class KMMOracle:
         self.dt = float(dt)
         self.family = family.upper()[0]
         self.padding_factor = tuple(float(p) for p in padding_factor)
-        if time_integrator not in ("SBDF3", "IMEXRK3", "IMEXRK222"):
+        if time_integrator not in ("SBDF3", "IMEXRK3", "IMEXRK222", "CNAB2"):
             raise ValueError(time_integrator)
         self.time_integrator = time_integrator
         self.nonlinear_form = nonlinear_form
@@ -954,6 +956,8 @@ class KMMOracle:
                 factors((IMEXRK3_A[rk] + IMEXRK3_B[rk]) * self.dt / 2.0)
                 for rk in range(3)
             ]
+        elif self.time_integrator == "CNAB2":
+            self.steady = factors(0.5 * self.dt)  # channelflow_kmm.py:267-274
         else:
             self.steady = factors(self.dt * IMEXRK222_A[1][1])
 
@@ -1221,9 +1225,32 @@ class KMMOracle:
             g_stage = g
         return replace(state, u=u_stage, g=g_stage)
 
+    def step_cnab2(self, state: KMMState) -> KMMState:
+        """channelflow_kmm.py:1071-1121: Crank-Nicolson on the linear terms,
+        the nonlinear term extrapolated by ``variable_ab2_extrapolate``
+        (integrators/cnab2.py:211-240) with r = dt / previous_dt, or taken
+        as is on the first step (have_old = 0)."""
+        dt = self.dt
+        cur_n = self.nonlinear_rhs(self.convection(state.u))
+        if state.have_old and state.nonlinear_old is not None:
+            r = dt / state.previous_dt
+            ext = tuple((1.0 + 0.5 * r) * c - 0.5 * r * p
+                        for c, p in zip(cur_n, state.nonlinear_old, strict=True))
+        else:
+            ext = cur_n
+        p = self.primary(state)
+        mass = self.mass_rows(p)
+        lin = (self.Lu.matvec(p[0]), self.Lg.matvec(p[1]), self.L00 @ p[2], self.L00 @ p[3])
+        rhs = [m + 0.5 * dt * ell + dt * n for m, ell, n in zip(mass, lin, ext, strict=True)]
+        u0, g, v00, w00 = self._solve_all(self.steady, *rhs)
+        return replace(state, u=self.reconstruct(u0, g, v00, w00), g=g, nonlinear_old=cur_n,
+                       have_old=1.0, previous_dt=dt)
+
     def step(self, state: KMMState) -> KMMState:
         if self.time_integrator == "SBDF3":
             return self.step_sbdf3(state)
+        if self.time_integrator == "CNAB2":
+            return self.step_cnab2(state)
         if self.time_integrator == "IMEXRK3":
             return self.step_imexrk3(state, self.startup)
         return self.step_imexrk222(state)

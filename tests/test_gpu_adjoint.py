@@ -40,7 +40,8 @@ def fd_check(solver, x0, d, steps, eps=1e-6, checkpoint=4):
 
 @pytest.mark.parametrize("N, steps", [((17, 16, 16), 8), ((33, 32, 32), 12)])
 def test_gradient_matches_central_fd_divergence_free(cuda, N, steps):
-    s = PlaneCouetteFluctuation(N=N, Re=400.0, dt=0.01, perturbation_amplitude=0.1, device=cuda)
+    s = PlaneCouetteFluctuation(N=N, Re=400.0, dt=0.01, perturbation_amplitude=0.1, device=cuda,
+                                time_integrator="SBDF3", nonlinear_form="rotational")
     x0 = ms._primary(s.initial_state())
     for seed in (200, 203):
         d = scaled_to(direction(s, seed), x0)
@@ -52,7 +53,7 @@ def test_gradient_matches_central_fd_per_leaf(cuda):
     """Each leaf on its own: u1, u2 and g enter the first nonlinear term and
     the means independently of the primary state."""
     s = PlaneCouetteFluctuation(N=(17, 16, 16), Re=400.0, dt=0.01, perturbation_amplitude=0.1,
-                                device=cuda)
+                                device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     x0 = ms._primary(s.initial_state())
     full = direction(s, 210)
     z = lambda t: torch.zeros_like(t)  # noqa: E731
@@ -72,7 +73,7 @@ def test_gradient_matches_central_fd_per_leaf(cuda):
 
 def test_checkpoint_stride_does_not_change_the_gradient(cuda):
     s = PlaneCouetteFluctuation(N=(17, 16, 16), Re=400.0, dt=0.01, perturbation_amplitude=0.1,
-                                device=cuda)
+                                device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     x0 = ms._primary(s.initial_state())
     ga, a = ms.gain_and_gradient(s, x0, 9, checkpoint=1)
     gb, b = ms.gain_and_gradient(s, x0, 9, checkpoint=4)
@@ -84,7 +85,7 @@ def test_checkpoint_stride_does_not_change_the_gradient(cuda):
 
 def test_gain_matches_the_forward_solver(cuda):
     s = PlaneCouetteFluctuation(N=(17, 16, 16), Re=400.0, dt=0.01, perturbation_amplitude=0.1,
-                                device=cuda)
+                                device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     x0 = s.initial_state()
     e0 = s.perturbation_energy(x0)
     eT = s.perturbation_energy(s.solve(x0, 7))
@@ -94,7 +95,7 @@ def test_gain_matches_the_forward_solver(cuda):
 
 def test_energy_tangent_projection_and_autograd(cuda):
     s = PlaneCouetteFluctuation(N=(17, 16, 16), Re=400.0, dt=0.01, perturbation_amplitude=0.1,
-                                device=cuda)
+                                device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     x0 = ms._primary(s.initial_state())
     # the energy gradient is exact: E is quadratic, so FD is exact up to round-off
     d = scaled_to(direction(s, 220), x0)
@@ -117,7 +118,7 @@ def test_energy_tangent_projection_and_autograd(cuda):
 
 def test_ascent_increases_gain_at_fixed_energy(cuda):
     s = PlaneCouetteFluctuation(N=(17, 16, 16), Re=400.0, dt=0.01, perturbation_amplitude=0.1,
-                                device=cuda)
+                                device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     x0 = s.initial_state()
     final, hist = ms.minimal_seed_ascent(s, x0, target_energy=1e-4, steps=10, iterations=3,
                                          step_size=0.5)

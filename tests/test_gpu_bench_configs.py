@@ -53,7 +53,8 @@ def test_reference_hydro_benchmark_golden_on_gpu(cuda):
     s = spec["solver"]
     g = PlaneCouetteFluctuation(N=tuple(s["N"]), Re=s["Re"], dt=s["dt"],
                                 perturbation_amplitude=s["perturbation_amplitude"],
-                                padding_factor=tuple(s["padding_factor"]), device=cuda)
+                                padding_factor=tuple(s["padding_factor"]), device=cuda,
+                                time_integrator="SBDF3", nonlinear_form="rotational")
     st = g.solve(g.initial_state(), spec["steps"])
     d = g.diagnostics(st)
     for key in ("Epert", "Etot", "wall_shear_top", "wall_shear_bot", "u_top", "u_bot",
@@ -78,9 +79,11 @@ def bench_workload(cuda):
     """The benchmark's seeded 65x64x64 field, projected by the GPU and by the
     oracle from the same physical samples."""
     N = (65, 64, 64)
-    g64 = PlaneCouetteFluctuation(N=N, domain=DOMAIN, Re=1000.0, dt=0.01, device=cuda)
+    g64 = PlaneCouetteFluctuation(N=N, domain=DOMAIN, Re=1000.0, dt=0.01, device=cuda,
+                                  time_integrator="SBDF3", nonlinear_form="rotational")
     g32 = PlaneCouetteFluctuation(N=N, domain=DOMAIN, Re=1000.0, dt=0.01, precision="mixed",
-                                  device=cuda)
+                                  device=cuda,
+                                  time_integrator="SBDF3", nonlinear_form="rotational")
     o = PlaneCouetteOracle(N=N, domain=DOMAIN, Re=1000.0, dt=0.01)
     f = couette_perturbation_fields(N, DOMAIN)
     f = scale_to_energy(f, g64.diagnostics(g64.state_from_physical(f))["Epert"], 1e-4)
@@ -119,7 +122,8 @@ def test_large_grids_both_forms_against_oracle(cuda, N):
     for precision, tol in (("fp64", 1e-12), ("mixed", 2e-7)):
         g = PlaneCouetteFluctuation(N=N, domain=DOMAIN, Re=1000.0, dt=0.01,
                                     perturbation_amplitude=0.02, precision=precision,
-                                    device=cuda)
+                                    device=cuda,
+                                    time_integrator="SBDF3", nonlinear_form="rotational")
         gs = g.solve(g._ensure_history(to_dev(st, cuda)), 3)
         for x, y in zip((*gs.u, gs.g), (*ref.u, ref.g), strict=True):
             assert rel(x, y) < tol, precision
@@ -132,7 +136,7 @@ def test_nonfinite_state_raises_floating_point_error(cuda, precision):
     reports it and ``solve`` raises FloatingPointError (the reference's runner
     raises it for a non-finite state, production/oracles.py:3257-3261)."""
     g = PlaneCouetteFluctuation(N=(33, 32, 32), Re=400.0, dt=1e-3, precision=precision,
-                                device=cuda)
+                                device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     st = g.initial_state()
     u0 = st.u[0].cpu()
     u0[5, 3, 2] = complex(float("nan"), 0.0)

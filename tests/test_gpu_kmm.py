@@ -30,7 +30,8 @@ def to_dev(st, dev):
 
 def pair(N, Re=600.0, dt=0.01, amp=0.05, dev="cuda"):
     o = PlaneCouetteOracle(N=N, Re=Re, dt=dt, perturbation_amplitude=amp)
-    g = PlaneCouetteFluctuation(N=N, Re=Re, dt=dt, perturbation_amplitude=amp, device=dev)
+    g = PlaneCouetteFluctuation(N=N, Re=Re, dt=dt, perturbation_amplitude=amp, device=dev,
+                                time_integrator="SBDF3", nonlinear_form="rotational")
     return o, g
 
 
@@ -67,7 +68,8 @@ def test_steps_match_oracle(cuda, N):
 def test_against_committed_golden_fixture(cuda):
     fx = np.load(os.path.join(HERE, "golden", "pcf_17x16x16.npz"))
     g = PlaneCouetteFluctuation(N=(17, 16, 16), Re=600.0, dt=0.01,
-                                perturbation_amplitude=0.05, device=cuda)
+                                perturbation_amplitude=0.05, device=cuda,
+                                time_integrator="SBDF3", nonlinear_form="rotational")
     gs = g.initial_state()
     done = 0
     for n in (0, 3, 10):
@@ -114,7 +116,7 @@ def test_full_size_properties(cuda):
     runs are bitwise identical, walls keep U = +-1."""
     N = (65, 64, 64)
     g = PlaneCouetteFluctuation(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02,
-                                device=cuda)
+                                device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     s0 = g.initial_state()
     a = g.solve(s0, 60)
     b = g.solve(s0, 60)
@@ -133,7 +135,8 @@ def test_full_size_properties(cuda):
 
 
 def test_solve_rejects_cpu_tensors(cuda):
-    g = PlaneCouetteFluctuation(N=(17, 16, 16), device=cuda)
+    g = PlaneCouetteFluctuation(N=(17, 16, 16), device=cuda,
+                                time_integrator="SBDF3", nonlinear_form="rotational")
     st = g.zero_state()
     bad = KMMState(u=tuple(t.cpu() for t in st.u), g=st.g.cpu())
     with pytest.raises(ValueError):
@@ -161,10 +164,10 @@ def test_tensor_core_and_warp_pencil_kernels_agree(cuda, N, monkeypatch):
     """The tensor-core pencil stage (folded operators) and the warp-per-pencil
     stage (recurrences) are two evaluations of the same step."""
     g1 = PlaneCouetteFluctuation(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02,
-                                 device=cuda)
+                                 device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     monkeypatch.setenv("JFB200_PENCIL", "warp")
     g2 = PlaneCouetteFluctuation(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02,
-                                 device=cuda)
+                                 device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     s0 = g1.initial_state()
     a, b = g1.solve(s0, 12), g2.solve(s0, 12)
     for x, y in zip((*a.u, a.g), (*b.u, b.g), strict=True):
@@ -176,11 +179,11 @@ def test_fused_and_split_periodic_transforms_agree(cuda, N, monkeypatch):
     """The one-launch plane transforms (CTA pair per x-plane) and the three
     separate transform launches give the same steps."""
     g1 = PlaneCouetteFluctuation(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02,
-                                 device=cuda)
+                                 device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     assert g1.info().launches_per_step == 2
     monkeypatch.setenv("JFB200_TRANSFORMS", "split")
     g2 = PlaneCouetteFluctuation(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02,
-                                 device=cuda)
+                                 device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     assert g2.info().launches_per_step == 4
     s0 = g1.initial_state()
     a, b = g1.solve(s0, 12), g2.solve(s0, 12)
@@ -192,10 +195,13 @@ def test_plans_of_different_sizes_and_precisions_coexist(cuda):
     """Building a smaller or mixed-precision plan after a larger one must not
     break the larger plan's launches (kernel attributes are process-wide)."""
     big = PlaneCouetteFluctuation(N=(65, 64, 64), Re=400.0, dt=1e-3, perturbation_amplitude=0.02,
-                                  device=cuda)
+                                  device=cuda,
+                                  time_integrator="SBDF3", nonlinear_form="rotational")
     ref = big.solve(big.initial_state(), 3)
-    PlaneCouetteFluctuation(N=(33, 32, 32), precision="mixed", device=cuda)
-    PlaneCouetteFluctuation(N=(17, 16, 16), device=cuda)
+    PlaneCouetteFluctuation(N=(33, 32, 32), precision="mixed", device=cuda,
+                            time_integrator="SBDF3", nonlinear_form="rotational")
+    PlaneCouetteFluctuation(N=(17, 16, 16), device=cuda,
+                            time_integrator="SBDF3", nonlinear_form="rotational")
     again = big.solve(big.initial_state(), 3)
     for x, y in zip((*again.u, again.g), (*ref.u, ref.g), strict=True):
         assert torch.equal(x, y)
@@ -206,9 +212,11 @@ def _seeded_pair(N, cuda):
 
     from jaxfun_b200.workloads import couette_perturbation_fields, scale_to_energy
     dom = ((-1.0, 1.0), (0.0, 4.0 * math.pi), (0.0, 2.0 * math.pi))
-    g64 = PlaneCouetteFluctuation(N=N, domain=dom, Re=1000.0, dt=0.01, device=cuda)
+    g64 = PlaneCouetteFluctuation(N=N, domain=dom, Re=1000.0, dt=0.01, device=cuda,
+                                  time_integrator="SBDF3", nonlinear_form="rotational")
     g32 = PlaneCouetteFluctuation(N=N, domain=dom, Re=1000.0, dt=0.01, precision="mixed",
-                                  device=cuda)
+                                  device=cuda,
+                                  time_integrator="SBDF3", nonlinear_form="rotational")
     f = couette_perturbation_fields(N, dom)
     f = scale_to_energy(f, g64.diagnostics(g64.state_from_physical(f))["Epert"], 1e-4)
     return g64, g32, g64.state_from_physical(f), g32.state_from_physical(f)
@@ -234,7 +242,8 @@ def test_mixed_form_tracks_fp64(cuda):
 def test_mixed_form_against_oracle(cuda, N):
     o = PlaneCouetteOracle(N=N, Re=400.0, dt=1e-3, perturbation_amplitude=0.05)
     g = PlaneCouetteFluctuation(N=N, Re=400.0, dt=1e-3, perturbation_amplitude=0.05,
-                                precision="mixed", device=cuda)
+                                precision="mixed", device=cuda,
+                                time_integrator="SBDF3", nonlinear_form="rotational")
     st, gs = o.solve(o.initial_state(), 6), g.solve(g.initial_state(), 6)
     for a, b in zip((*gs.u, gs.g), (*st.u, st.g), strict=True):
         assert rel(a, b) < 1e-7
@@ -248,7 +257,8 @@ def test_wide_wall_normal_grids_match_oracle(cuda, N, precision):
     mixed form is held to its complex64 transform round-off."""
     o = PlaneCouetteOracle(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02)
     g = PlaneCouetteFluctuation(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02,
-                                precision=precision, device=cuda)
+                                precision=precision, device=cuda,
+                                time_integrator="SBDF3", nonlinear_form="rotational")
     st = o.initial_state()
     gs = g._ensure_history(to_dev(st, cuda))
     for _ in range(4):
@@ -267,7 +277,7 @@ def test_tensor_core_velocity_products_track_dmma(cuda, N, monkeypatch):
     round the fields to complex64; the FP32 accumulation leaves the state
     after 12 steps within 5e-8 (measured 1.6e-8 at 65x64x64)."""
     kw = dict(N=N, Re=1000.0, dt=0.01, perturbation_amplitude=0.02, precision="mixed",
-              device=cuda)
+              device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     g2 = PlaneCouetteFluctuation(**kw)
     monkeypatch.setenv("JFB200_TC", "1")
     g1 = PlaneCouetteFluctuation(**kw)
@@ -282,7 +292,8 @@ def test_autotune_selects_a_variant_and_keeps_the_state(cuda, tmp_path, monkeypa
     loaded state: the state is unchanged afterwards, the chosen variant is
     active and accepted by the plan, and a second call reads the cache."""
     monkeypatch.setenv("JFB200_AUTOTUNE_CACHE", str(tmp_path / "autotune.json"))
-    kw = dict(N=(33, 32, 32), Re=1000.0, dt=0.01, perturbation_amplitude=0.02, device=cuda)
+    kw = dict(N=(33, 32, 32), Re=1000.0, dt=0.01, perturbation_amplitude=0.02, device=cuda,
+              time_integrator="SBDF3", nonlinear_form="rotational")
     ref_solver = PlaneCouetteFluctuation(**kw)
     s0 = ref_solver.initial_state()
     ref = ref_solver.solve(s0, 6)
@@ -310,7 +321,8 @@ def test_one_step_integrators_match_oracle(cuda, integrator, N, precision):
     stage (97), the mixed form at 1e-7.  The history fields pass through."""
     kw = dict(N=N, Re=400.0, dt=1e-3, perturbation_amplitude=0.05, time_integrator=integrator)
     o = PlaneCouetteOracle(**kw)
-    g = PlaneCouetteFluctuation(precision=precision, device=cuda, **kw)
+    g = PlaneCouetteFluctuation(precision=precision, device=cuda, nonlinear_form="rotational",
+                                **kw)
     st = o.initial_state()
     gs = g._ensure_history(to_dev(st, cuda))
     st, gs = o.solve(st, 5), g.solve(gs, 5)

@@ -211,7 +211,8 @@ def test_ensemble_of_uneven_members_equals_separate_runs(cuda):
         return [PlaneCouetteMHD(N=(17, 16, 16), dt=1e-3, magnetic_amplitude=0.1, device=cuda),
                 PlaneCouetteMHD(N=(25, 16, 16), dt=1e-3, magnetic_amplitude=0.1, device=cuda),
                 PlaneCouetteMHD(N=(33, 16, 16), dt=1e-3, magnetic_amplitude=0.1, device=cuda),
-                PlaneCouetteFluctuation(N=(33, 16, 16), dt=1e-3, device=cuda)]
+                PlaneCouetteFluctuation(N=(33, 16, 16), dt=1e-3, device=cuda,
+                                        time_integrator="SBDF3", nonlinear_form="rotational")]
 
     sep = members()
     ref = [m.solve(m.initial_state(), 7) for m in sep]

@@ -75,7 +75,7 @@ def test_tps_ops_match_space_methods(cuda):
 
 def test_kmm_gain_op_backward_is_the_adjoint(cuda):
     s = PlaneCouetteFluctuation(N=(17, 16, 16), Re=400.0, dt=0.01, perturbation_amplitude=0.1,
-                                device=cuda)
+                                device=cuda, time_integrator="SBDF3", nonlinear_form="rotational")
     x0 = s.initial_state()
     h = torch_ops.register_solver(s)
     try:

@@ -12,9 +12,8 @@ from jaxfun_b200.kmm import KMM, PlaneCouetteFluctuation
 
 
 @pytest.mark.parametrize("kw", [
-    {"time_integrator": "CNAB2"},
-    {"nonlinear_form": "gradient"},
-    {"family": "L"},
+    {"dpdy": 0.1},
+    {"nonlinear_form": "gradient", "precision": "mixed"},
     {"padding_factor": (1.5, 1.5, 1.5)},
 ])
 def test_unsupported_options_are_rejected_before_any_device_work(kw):
@@ -24,6 +23,7 @@ def test_unsupported_options_are_rejected_before_any_device_work(kw):
 
 @pytest.mark.parametrize("kw, exc", [
     ({"nonlinear_form": "skew"}, ValueError),
+    ({"family": "J"}, ValueError),
     ({"coefficient_path": "fast"}, ValueError),
     ({"time_integrator": "RK4"}, ValueError),
 ])

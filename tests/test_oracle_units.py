@@ -1,6 +1,8 @@
 """Unit checks of the oracle's building blocks against independent NumPy
 computations (CPU only)."""
 
+from dataclasses import replace
+
 import numpy as np
 import pytest
 
@@ -153,3 +155,49 @@ def test_mhd_field_stays_solenoidal_and_couples():
     h = ok.PlaneCouetteOracle(**kw)
     sh = h.solve(h.initial_state(), 5)
     assert np.linalg.norm(st.flow.u[0] - sh.u[0]) > 1e-8 * np.linalg.norm(sh.u[0])
+
+
+@pytest.mark.parametrize("family", ["C", "L"])
+def test_cnab2_laminar_state_and_form_agreement(family):
+    """The reference's CNAB2 property test on the oracle
+    (tests/couette/test_pcf_fluctuations_jax.py:104-136): the laminar state
+    stays zero under the rotational form, the two forms' nonlinear rows Ng
+    agree, and one rotational step matches one gradient step."""
+    kw = dict(N=(13, 12, 12), family=family, dt=1.0e-4, padding_factor=(1.0, 1.5, 1.5),
+              perturbation_amplitude=0.02, time_integrator="CNAB2")
+    grad = ok.PlaneCouetteOracle(nonlinear_form="gradient", **kw)
+    rot = ok.PlaneCouetteOracle(nonlinear_form="rotational", **kw)
+    zero = rot.state_from_physical(tuple(np.zeros(rot.counts) for _ in range(3)))
+    lam = rot.step(zero)
+    for v in (*lam.u, lam.g):
+        assert np.abs(v).max() <= 2.0e-13
+    s0 = grad.initial_state()
+    rg = grad.nonlinear_rhs(grad.convection(s0.u))
+    rr = rot.nonlinear_rhs(rot.convection(s0.u))
+    np.testing.assert_allclose(rr[1], rg[1], rtol=2.0e-11, atol=2.0e-12)
+    a, b = grad.step(s0), rot.step(s0)
+    for x, y in zip((*b.u, b.g), (*a.u, a.g), strict=True):
+        np.testing.assert_allclose(x, y, rtol=2.0e-7, atol=2.0e-10)
+    assert b.have_old == 1.0 and b.previous_dt == 1.0e-4
+
+
+def test_cnab2_second_order_in_time():
+    """Step-doubling order gate of the CNAB2 flow step (the reference's
+    temporal-order gates, tests/couette/test_pcf_mri_cnab2_order_jax.py and
+    tests/couette/test_pcf_sbdf3_jax.py:223-246, from a KMM-consistent
+    initial state): the differences of runs at dt, dt/2, dt/4 to a common
+    time shrink about fourfold."""
+    T = 0.04
+
+    def run(dt):
+        s = ok.PlaneCouetteOracle(N=(13, 12, 12), Re=100.0, dt=dt, time_integrator="CNAB2",
+                                  perturbation_amplitude=0.2, nonlinear_form="rotational")
+        st = s.initial_state()
+        means = (np.real(st.u[1][:, 0, 0]), np.real(st.u[2][:, 0, 0]))
+        st = replace(st, u=s.reconstruct(st.u[0], st.g, *means))
+        st = s.solve(st, int(round(T / dt)))
+        return np.concatenate([st.u[0].ravel(), st.g.ravel(), st.u[1].ravel()])
+
+    a, b, c = run(0.005), run(0.0025), run(0.00125)
+    ratio = np.linalg.norm(a - b) / np.linalg.norm(b - c)
+    assert 3.0 < ratio < 5.0
