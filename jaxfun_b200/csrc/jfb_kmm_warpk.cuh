@@ -436,6 +436,26 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
     // third product with zero)
     auto z_rows = [&](int ya, bool hasb) {
       T nrm[2][3][PZ];
+      // both rows' spectra (six fields, half of them in the peer CTA) are
+      // read before the first transform: the peer reads overlap
+      cpx<T> A[2][3][QK], B[2][3][QK];
+#pragma unroll
+      for (int rb = 0; rb < 2; ++rb) {
+        const int y = rank * MH + ya + rb;
+#pragma unroll
+        for (int pr = 0; pr < 3; ++pr)
+#pragma unroll
+          for (int q = 0; q < QK; ++q) {
+            const int kz = 32 * q + lane;
+            A[rb][pr][q] = B[rb][pr][q] = cmk(T(0), T(0));
+            if (kz < Kz && (rb == 0 || hasb)) {
+              const int own = kz >= KH, cl = kz - own * KH;
+              const cpx<T>* base = (own == rank) ? Ys : Ypeer;
+              A[rb][pr][q] = base[((size_t)(2 * pr) * MY + y) * LDZ + cl];
+              B[rb][pr][q] = base[((size_t)(2 * pr + 1) * MY + y) * LDZ + cl];
+            }
+          }
+      }
 #pragma unroll
       for (int rb = 0; rb < 2; ++rb) {
         if (rb == 1 && !hasb) {
@@ -443,23 +463,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
           for (int r = 0; r < PZ; ++r) nrm[1][0][r] = nrm[1][1][r] = nrm[1][2][r] = T(0);
           break;
         }
-        const int y = rank * MH + ya + rb;
         cpx<T> ph[3][PZ];
 #pragma unroll
         for (int pr = 0; pr < 3; ++pr) {
-          cpx<T> A[QK], B[QK];
-#pragma unroll
-          for (int q = 0; q < QK; ++q) {
-            const int kz = 32 * q + lane;
-            A[q] = B[q] = cmk(T(0), T(0));
-            if (kz < Kz) {
-              const int own = kz >= KH, cl = kz - own * KH;
-              const cpx<T>* base = (own == rank) ? Ys : Ypeer;
-              A[q] = base[((size_t)(2 * pr) * MY + y) * LDZ + cl];
-              B[q] = base[((size_t)(2 * pr + 1) * MY + y) * LDZ + cl];
-            }
-          }
-          build_packed<PZ, QK, T>(A, B, Kz, lane, ph[pr]);
+          build_packed<PZ, QK, T>(A[rb][pr], B[rb][pr], Kz, lane, ph[pr]);
           warp_fft_inverse<PZ, T>(ph[pr], w, lane);
         }
 #pragma unroll
@@ -514,20 +521,33 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
     WarpTw<PY, T> w;
     load_warp_tw<PY, T>(w, twy, lane);
     const T scale = T(1.0 / MY);
-    for (int t = warp; t < 3 * KH; t += NW) {
+    // every column of this warp (at most three: 3 KH <= 48 columns over 16
+    // warps) is read before the first transform, so that the peer-CTA reads
+    // of all of them are in flight together
+    constexpr int TW = (3 * 16 + NW - 1) / NW;
+    cpx<T> v[TW][PY];
+#pragma unroll
+    for (int i = 0; i < TW; ++i) {
+      const int t = warp + i * NW;
+      if (t >= 3 * KH) break;
       const int f = t / KH, cl = t % KH, kz = rank * KH + cl;
-      cpx<T> v[PY];
 #pragma unroll
       for (int n1 = 0; n1 < PY; ++n1) {
         const int y = n1 + PY * br;
         const int own = y / MH, yl = y - own * MH;
         const cpx<T>* base = (own == rank) ? Hs : Hpeer;
-        v[n1] = base[((size_t)f * MH + yl) * Kz + (swz ? (kz ^ (yl & 7)) : kz)];
+        v[i][n1] = base[((size_t)f * MH + yl) * Kz + (swz ? (kz ^ (yl & 7)) : kz)];
       }
-      warp_fft_forward<PY, T>(v, w, lane);
+    }
+#pragma unroll
+    for (int i = 0; i < TW; ++i) {
+      const int t = warp + i * NW;
+      if (t >= 3 * KH) break;
+      const int f = t / KH, cl = t % KH;
+      warp_fft_forward<PY, T>(v[i], w, lane);
       cpx<T>* col = Ys + (size_t)f * MY * LDZ + cl;
 #pragma unroll
-      for (int k1 = 0; k1 < PY; ++k1) col[(size_t)(32 * k1 + lane) * LDZ] = scale * v[k1];
+      for (int k1 = 0; k1 < PY; ++k1) col[(size_t)(32 * k1 + lane) * LDZ] = scale * v[i][k1];
     }
     __syncthreads();
     JFB_STAMP(1, 5);

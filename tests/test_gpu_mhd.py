@@ -234,7 +234,7 @@ def test_batched_ensemble_of_uneven_mhd_members_equals_separate_runs(cuda, monke
     over that size's members' tiles, the sizes on parallel graph branches),
     or as five launches over all members (JFB200_ENSEMBLE=batched); either
     result is bitwise that of separate runs, and that of the
-    one-stream-per-member graph."""
+    one-stream-per-member graph (five launches per member)."""
     from jaxfun_b200.mhd import Ensemble
 
     def members():
@@ -246,7 +246,7 @@ def test_batched_ensemble_of_uneven_mhd_members_equals_separate_runs(cuda, monke
     ref = [m.solve(m.initial_state(), 7) for m in sep]
     outs = []
     for mode, batched, launches in ((None, True, 15), ("batched", True, 5),
-                                    ("streams", False, 4)):
+                                    ("streams", False, 20)):
         if mode is None:
             monkeypatch.delenv("JFB200_ENSEMBLE", raising=False)
         else:
