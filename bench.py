@@ -69,6 +69,8 @@ def parse_args(argv=None):
     p.add_argument("--ensemble-members", type=int, default=32)
     p.add_argument("--no-helmholtz", action="store_true",
                    help="skip the 2-D Helmholtz block")
+    p.add_argument("--no-default-form", action="store_true",
+                   help="skip the gradient-form (the reference's default) timing block")
     p.add_argument("--no-sizes", action="store_true",
                    help="skip the 97^3 / 129^3 mixed-vs-FP64 block")
     p.add_argument("--no-autotune", action="store_true",
@@ -601,90 +603,121 @@ def main(argv=None):
         """The batched MHD ensemble workload: --ensemble-members members with
         wall-normal sizes cycling 33, 49, 65 x 64 x 64 Fourier modes, Re = Rm
         = 1000, imposed field B0 = 0.1 e_z, base flow U_b = x, seeded
-        divergence-free perturbations of u and b (energies 1e-4 each), FP64;
-        one CUDA graph per ensemble step."""
+        divergence-free perturbations of u and b (energies 1e-4 each); one
+        CUDA graph per ensemble step.  The headline form is the mixed one
+        (complex64 periodic transforms, FP64 solves); the FP64 form is timed
+        beside it, and the two forms' per-field distance after the timed
+        steps is reported."""
         from jaxfun_b200.mhd import Ensemble, MHDState, PlaneCouetteMRIShearpy
 
         sizes = (33, 49, 65)
-        members, states = [], []
-        for m in range(args.ensemble_members):
-            N = (sizes[m % 3], grid[1], grid[2])
-            sv = PlaneCouetteMRIShearpy(N=N, domain=domain(), Re=RE, Rm=RE, omega=0.0,
-                                        shear_rate=-1.0, background_b=(0.0, 0.0, 0.1),
-                                        dt=DT, device=dev)
-            fu = couette_perturbation_fields(N, domain(), seeds=(100 + m, 1100 + m))
-            e_u = sv.diagnostics(sv.state_from_physical(fu))["Epert"]
-            flow = sv.state_from_physical(scale_to_energy(fu, e_u, ENERGY))
-            fa = couette_perturbation_fields(N, domain(), seeds=(2100 + m, 3100 + m))
-            A = sv._A_state_from_physical(fa)
-            e_b = sv.diagnostics(MHDState(flow=flow, A=A))["Emag"]
-            A = tuple(a * math.sqrt(ENERGY / e_b) for a in A)
-            members.append(sv)
-            states.append(MHDState(flow=flow, A=A))
-        ens = Ensemble(members)
-        ens.load(states)
-        ens.advance_resident(2 + max(3, args.warmup))
-        torch.cuda.synchronize(dev)
         K = max(10, min(args.steps, 100))
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        ens.advance_resident(K)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        ms_step = e0.elapsed_time(e1) / K
-        launches = ens.launches_per_step
-        diags = [m.diagnostics(m._fetch_mhd(2.0)) for m in members[:3]]
+        warm = 2 + max(3, args.warmup)
+        states = []
 
-        def other_form(mode):
-            """The same members with JFB200_ENSEMBLE=mode: ms per ensemble step."""
-            os.environ["JFB200_ENSEMBLE"] = mode
+        def build(precision):
+            members = []
+            for m in range(args.ensemble_members):
+                N = (sizes[m % 3], grid[1], grid[2])
+                sv = PlaneCouetteMRIShearpy(N=N, domain=domain(), Re=RE, Rm=RE, omega=0.0,
+                                            shear_rate=-1.0, background_b=(0.0, 0.0, 0.1),
+                                            dt=DT, precision=precision, device=dev)
+                if len(states) <= m:
+                    fu = couette_perturbation_fields(N, domain(), seeds=(100 + m, 1100 + m))
+                    e_u = sv.diagnostics(sv.state_from_physical(fu))["Epert"]
+                    flow = sv.state_from_physical(scale_to_energy(fu, e_u, ENERGY))
+                    fa = couette_perturbation_fields(N, domain(), seeds=(2100 + m, 3100 + m))
+                    A = sv._A_state_from_physical(fa)
+                    e_b = sv.diagnostics(MHDState(flow=flow, A=A))["Emag"]
+                    A = tuple(a * math.sqrt(ENERGY / e_b) for a in A)
+                    states.append(MHDState(flow=flow, A=A))
+                members.append(sv)
+            return members
+
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def timed(members, mode=None):
+            """ms per ensemble step of the members (JFB200_ENSEMBLE=mode if
+            given), after the same warm-up from the same states."""
+            if mode is not None:
+                os.environ["JFB200_ENSEMBLE"] = mode
             try:
-                ens_o = Ensemble(members)
+                ens = Ensemble(members)
             finally:
-                del os.environ["JFB200_ENSEMBLE"]
-            ens_o.load(states)
-            ens_o.advance_resident(2 + max(3, args.warmup))
+                os.environ.pop("JFB200_ENSEMBLE", None)
+            ens.load(states)
+            ens.advance_resident(warm)
             torch.cuda.synchronize(dev)
             e0.record(stream)
-            ens_o.advance_resident(K)
+            ens.advance_resident(K)
             e1.record(stream)
             torch.cuda.synchronize(dev)
-            return {"ms_per_ensemble_step": e0.elapsed_time(e1) / K,
-                    "gpu_launches_per_step": ens_o.launches_per_step}
+            return ens, e0.elapsed_time(e1) / K
 
+        mixed = build("mixed")
+        fp64 = build("fp64")
+        ens, ms_step = timed(mixed)
+        launches = ens.launches_per_step
+        # the two forms after the same warm + K steps from the same states
+        s32 = [m._fetch_mhd(2.0) for m in mixed[:3]]
+        ens64, ms64 = timed(fp64)
+        s64 = [m._fetch_mhd(2.0) for m in fp64[:3]]
+        dist = {}
+        for a, b, n in zip(s32, s64, sizes, strict=True):
+            fa = (*a.flow.u, a.flow.g, *a.A)
+            fb = (*b.flow.u, b.flow.g, *b.A)
+            names = ("u0", "u1", "u2", "g", "Ax", "Ay", "Az")
+            dist[f"N={n}"] = {k: float((x - y).norm() / y.norm())
+                              for k, x, y in zip(names, fa, fb, strict=True)}
+        diags = [m.diagnostics(s) for m, s in zip(mixed[:3], s32, strict=True)]
         # the other forms: every member on its own stream (the form of plans
         # that cannot batch) and all members in one group
         others = {}
         if ens.batched:
-            others = {"one_stream_per_member": other_form("streams"),
-                      "one_group": other_form("batched")}
-        # stage model of one MHD member step (FP64): (91 E_s + 36 E_m) x 16 B
-        step_bytes = 0
-        for m in members:
+            others = {"one_stream_per_member": {"ms_per_ensemble_step": timed(mixed, "streams")[1]},
+                      "one_group": {"ms_per_ensemble_step": timed(mixed, "batched")[1]},
+                      "fp64_one_stream_per_member": {
+                          "ms_per_ensemble_step": timed(fp64, "streams")[1]}}
+        # stage model of one MHD member step: 91 E_s + 36 E_m complex values;
+        # FP64 16 B each, mixed: the 36 E_s and 36 E_m values of the transform
+        # arrays (X, Y, HZ, HX) at 8 B, the rest at 16 B
+        bytes64 = bytes32 = 0
+        for m in mixed:
             nx, ny, nz = m.N
             H = nz // 2 + 1
-            step_bytes += (91 * nx * ny * H + 36 * nx * m.info().my * H) * 16
+            Es, Em = nx * ny * H, nx * m.info().my * H
+            bytes64 += (91 * Es + 36 * Em) * 16
+            bytes32 += 1168 * Es + 288 * Em
         peak, peak_kind = measured_peak()
-        achieved = step_bytes / (ms_step * 1e-3) / 1e9
+
+        def roof(b, ms):
+            a = b / (ms * 1e-3) / 1e9
+            return {"bound": "hbm", "achieved": a, "peak": peak, "unit": "GB/s",
+                    "frac": a / peak, "peak_kind": f"of {peak_kind}",
+                    "algorithmic_bytes_per_ensemble_step": b}
+
         return {
-            "workload": f"{len(members)} MHD members, N cycling {sizes} x {grid[1]} x {grid[2]}, "
+            "workload": f"{len(mixed)} MHD members, N cycling {sizes} x {grid[1]} x {grid[2]}, "
                         "Re = Rm = 1000, B0 = 0.1 e_z, u and b perturbation energies 1e-4",
-            "members": len(members),
-            "dtype": "f64",
+            "members": len(mixed),
+            "form": "mixed: complex64 periodic transforms and products, FP64 operators, "
+                    "solves and state",
             "ms_per_ensemble_step": ms_step,
-            "member_steps_per_s": len(members) * 1000.0 / ms_step,
+            "member_steps_per_s": len(mixed) * 1000.0 / ms_step,
             "steps": K,
             "gpu_launches_per_step": launches,
+            "roofline": roof(bytes32, ms_step),
+            "fp64": {"ms_per_ensemble_step": ms64,
+                     "member_steps_per_s": len(fp64) * 1000.0 / ms64,
+                     "roofline": roof(bytes64, ms64)},
+            "mixed_vs_fp64_rel_l2": {"after_steps": warm + K, "members": dist},
             "other_forms": others,
             "launch": ("one CUDA graph per ensemble step: five launches per wall-normal size, "
                        "one per stage over that size's members' tiles, the sizes on parallel "
                        "branches" if ens.batched else
                        "one CUDA graph per ensemble step, one stream per member"),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": f"of {peak_kind}",
-                         "algorithmic_bytes_per_ensemble_step": step_bytes},
             "l2": "not flushed: the ensemble's state exceeds L2",
-            "device_bytes": sum(m.info().device_bytes for m in members),
+            "device_bytes": sum(m.info().device_bytes for m in mixed),
             "sample_diagnostics": [{k: d[k] for k in ("Epert", "Emag", "divB_L2")} for d in diags],
         }
 
@@ -765,6 +798,32 @@ def main(argv=None):
                           "(throughput over all host cores)"}
         return out
 
+    def default_form_block():
+        """The reference's production default on the same workload: the
+        gradient nonlinear form u . grad u (FP64) with each time integrator
+        the production runner accepts; ms per step (graph replay, CUDA events,
+        L2 not flushed) and the kernels per step."""
+        out = {}
+        f0 = couette_perturbation_fields(grid, domain())
+        for integ in ("SBDF3", "CNAB2", "IMEXRK222", "IMEXRK3"):
+            sv = PlaneCouetteFluctuation(N=grid, domain=domain(), Re=RE, dt=DT, device=dev,
+                                         time_integrator=integ, nonlinear_form="gradient")
+            e0 = sv.diagnostics(sv.state_from_physical(f0))["Epert"]
+            st = sv.solve(sv.state_from_physical(scale_to_energy(f0, e0, ENERGY)), 5)
+            torch.cuda.synchronize(dev)
+            K = 20
+            e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0_.record(stream)
+            sv.advance_resident(K)
+            e1_.record(stream)
+            torch.cuda.synchronize(dev)
+            stages = {"SBDF3": 1, "CNAB2": 1, "IMEXRK222": 2, "IMEXRK3": 3}[integ]
+            out[integ] = {"ms_per_step": e0_.elapsed_time(e1_) / K,
+                          "implicit_stages_per_step": stages}
+            del sv, st
+        out["form"] = "gradient, FP64 (warp-per-pencil stage, split periodic transforms)"
+        return out
+
     def sizes_block():
         """The same Couette workload at 97^3 and 129^3 (wall-normal points x
         Fourier modes): steady steps/s of both forms (graph replay, CUDA
@@ -830,6 +889,8 @@ def main(argv=None):
     ensb = ensemble_block() if (rank == 0 and world == 1 and not args.no_ensemble) else None
     helm = helmholtz_block() if (rank == 0 and world == 1 and not args.no_helmholtz) else None
     sizes = sizes_block() if (rank == 0 and world == 1 and not args.no_sizes) else None
+    dform = (default_form_block()
+             if (rank == 0 and world == 1 and not args.no_default_form) else None)
 
     if rank != 0:
         if world > 1:
@@ -874,6 +935,8 @@ def main(argv=None):
         line["helmholtz2d"] = helm
     if sizes is not None:
         line["larger_grids"] = sizes
+    if dform is not None:
+        line["reference_default_form"] = dform
     if world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         rate, n = cpu_oracle_rate(fields, grid, args.cpu_seconds, threads)

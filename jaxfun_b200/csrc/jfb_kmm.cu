@@ -271,7 +271,7 @@ struct jfb_kmm_plan {
   // MHD (vector potential A, three Dirichlet components per level)
   bool mhd = false;
   double eta = 0.0;
-  jfb::MhdPhys mphys = {0.0, 0.0, 0.0, 0.0};
+  jfb::MhdPhys mphys = {0.0, 0.0, 0.0, 0.0, 0.0};
   jfb::MhdOps mops;
   double *sa_steady = nullptr, *sa_startup[3] = {nullptr, nullptr, nullptr};
   jfb::c64 *AR[3], *NA[3], *NAst;
@@ -621,6 +621,17 @@ template <> struct Tx<float> {
 };
 template <typename T> static cpx<T>* buf(void* p) { return reinterpret_cast<cpx<T>*>(p); }
 
+// Field f of the step's x-physical array X (complex64 in the mixed form).
+static c64* x_field(const jfb_kmm_plan* pl, int f) {
+  const size_t e = (size_t)f * pl->d.Nx * pl->d.P;
+  return pl->mixed ? reinterpret_cast<c64*>(reinterpret_cast<c32*>(pl->X) + e) : pl->X + e;
+}
+// Field f of the nonlinear array HX (complex64 in the mixed form).
+static c64* hx_field(const jfb_kmm_plan* pl, int f) {
+  const size_t e = (size_t)f * pl->d.Nx * pl->d.P;
+  return pl->mixed ? reinterpret_cast<c64*>(reinterpret_cast<c32*>(pl->HX) + e) : pl->HX + e;
+}
+
 // nb / nf: fields transformed backward / forward (6 / 3 for the flow step,
 // 12 / 6 for the coupled MHD step)
 template <int P, typename T>
@@ -712,8 +723,22 @@ static int launch_transforms_t(jfb_kmm_plan* pl, cudaStream_t s) {
     }
     JFB_CHECK_LAUNCH();
     if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[2], s));
-    const int zb = ceil_div((int64_t)d.Nx * d.My, kZRows);
-    z_grad_kernel<<<zb, 256, pl->smem_zg, s>>>(pl->ops, pl->d, pl->fz, pl->twz, pl->Y, pl->HZ);
+    if (pl->pz) {  // warp-shuffle z transforms (Mz = 32 P, Kz <= 64)
+      const int blocks = ceil_div(ceil_div((int64_t)d.Nx * d.My, 2), 8);
+      switch (pl->pz * 10 + pl->qk) {
+#define JFB_ZG(P, Q)                                                                     \
+  case P * 10 + Q:                                                                       \
+    z_grad_warp_kernel<P, Q><<<blocks, 256, 0, s>>>(pl->ops, pl->d, pl->twz, pl->Y, pl->HZ); \
+    break;
+        JFB_ZG(2, 1) JFB_ZG(2, 2) JFB_ZG(3, 1) JFB_ZG(3, 2)
+        JFB_ZG(4, 1) JFB_ZG(4, 2) JFB_ZG(6, 1) JFB_ZG(6, 2)
+#undef JFB_ZG
+        default: break;
+      }
+    } else {
+      const int zb = ceil_div((int64_t)d.Nx * d.My, kZRows);
+      z_grad_kernel<<<zb, 256, pl->smem_zg, s>>>(pl->ops, pl->d, pl->fz, pl->twz, pl->Y, pl->HZ);
+    }
     JFB_CHECK_LAUNCH();
     if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[3], s));
     if (pl->py) {
@@ -765,28 +790,33 @@ static int launch_transforms_t(jfb_kmm_plan* pl, cudaStream_t s) {
 }
 
 // The coupled MHD step: twelve fields (u, omega, b, j) backward in y, the z
-// stage with the Lorentz force and the EMF, six fields (n, emf) forward in y.
+// stage with the Lorentz force and the EMF, six fields (n, emf) forward in y;
+// complex64 in the mixed form (tdims: the flow's base-flow terms are added in
+// FP64 by the pencil stage).
+template <typename T>
 static int launch_transforms_mhd(jfb_kmm_plan* pl, cudaStream_t s) {
-  const Dims& d = pl->d;
+  const Dims d = tdims<T>(pl);
+  const size_t smy = pl->smem_y / sizeof(c64) * sizeof(cpx<T>);
   if (pl->py) {  // warp-shuffle transforms along y (My = 32 P)
-    launch_y_warp_any<double>(pl, s, true, 12, 6);
+    launch_y_warp_any<T>(pl, s, true, 12, 6);
   } else {
     dim3 gy(d.Nx, 12, d.Kz / pl->KC);
-    y_backward_kernel<double><<<gy, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->X, pl->Y);
+    y_backward_kernel<T><<<gy, 256, smy, s>>>(d, pl->fy, pl->KC, Tx<T>::twy(pl), buf<T>(pl->X),
+                                              buf<T>(pl->Y));
   }
   JFB_CHECK_LAUNCH();
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[2], s));
   const int zb = ceil_div((int64_t)d.Nx * d.My, kZRows);
-  z_cross_mhd_kernel<<<zb, 256, pl->smem_zm, s>>>(pl->ops, d, pl->mphys, pl->fz, pl->twz, pl->Y,
-                                                  pl->HZ);
+  z_cross_mhd_kernel<T><<<zb, 256, pl->smem_zm / sizeof(c64) * sizeof(cpx<T>), s>>>(
+      pl->ops, d, pl->mphys, pl->fz, Tx<T>::twz(pl), buf<T>(pl->Y), buf<T>(pl->HZ));
   JFB_CHECK_LAUNCH();
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[3], s));
   if (pl->py) {
-    launch_y_warp_any<double>(pl, s, false, 12, 6);
+    launch_y_warp_any<T>(pl, s, false, 12, 6);
   } else {
     dim3 gf(d.Nx, 6, d.Kz / pl->KC);
-    y_forward_kernel<double><<<gf, 256, pl->smem_y, s>>>(d, pl->fy, pl->KC, pl->twy, pl->HZ,
-                                                         pl->HX, pl->ops.xphys);
+    y_forward_kernel<T><<<gf, 256, smy, s>>>(d, pl->fy, pl->KC, Tx<T>::twy(pl), buf<T>(pl->HZ),
+                                             buf<T>(pl->HX), pl->ops.xphys);
   }
   JFB_CHECK_LAUNCH();
   if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[4], s));
@@ -794,7 +824,8 @@ static int launch_transforms_mhd(jfb_kmm_plan* pl, cudaStream_t s) {
 }
 
 static int launch_transforms(jfb_kmm_plan* pl, cudaStream_t s) {
-  if (pl->mhd) return launch_transforms_mhd(pl, s);
+  if (pl->mhd)
+    return pl->mixed ? launch_transforms_mhd<float>(pl, s) : launch_transforms_mhd<double>(pl, s);
   return pl->mixed ? launch_transforms_t<float>(pl, s) : launch_transforms_t<double>(pl, s);
 }
 
@@ -808,6 +839,10 @@ static int launch_mhd(jfb_kmm_plan* pl, const MhdArgs& a0, cudaStream_t s) {
   const int blocks = (pl->d.Ny / 2) * ceil_div(pl->d.Kz, 8);
   MhdArgs a = a0;
   a.status = pl->status;
+  // mixed form: the step's EMF and b, j at the nodes are complex64
+  a.x32 = (pl->mixed && a.mode != kMhdFromPhys) ? 1 : 0;
+  a.uw_b0z = pl->mphys.uw_emf * pl->mphys.b0z;
+  a.uw_b0x = pl->mphys.uw_emf * pl->mphys.b0x;
   mhd_a_kernel<<<blocks, kMhdThreads, pl->smem_mhd, s>>>(pl->d, pl->ops, pl->mops, a);
   JFB_CHECK_LAUNCH();
   return JFB_OK;
@@ -818,11 +853,12 @@ static int mhd_fields(jfb_kmm_plan* pl, int c, cudaStream_t s) {
   MhdArgs m = blank_mhd();
   m.mode = kMhdFields;
   m.Aa = pl->AR[c];
-  m.XB = pl->X + (size_t)6 * pl->d.Nx * pl->d.P;
+  m.XB = x_field(pl, 6);
   return launch_mhd(pl, m, s);
 }
 
 static inline int slot(int64_t m) { return (int)(((m % 3) + 3) % 3); }
+
 
 // u1, u2 of the current state into U1S/U2S (reconstruction).
 static int ensure_explicit(jfb_kmm_plan* pl, cudaStream_t s) {
@@ -902,7 +938,7 @@ static void steady_args(jfb_kmm_plan* pl, int64_t m, StageArgs& a, MhdArgs& mm) 
   mm = blank_mhd();
   if (pl->mhd) {
     mm.mode = kMhdStep;
-    mm.HXA = pl->HX + (size_t)3 * pl->d.Nx * pl->d.P;
+    mm.HXA = hx_field(pl, 3);
     mm.c0 = a.c0;
     mm.c1 = a.c1;
     mm.c2 = a.c2;
@@ -918,7 +954,7 @@ static void steady_args(jfb_kmm_plan* pl, int64_t m, StageArgs& a, MhdArgs& mm) 
     mm.sa = pl->sa_steady;
     mm.sa_rec = pl->sg_rec;
     mm.A_out = pl->AR[nw];
-    mm.XB = pl->X + (size_t)6 * pl->d.Nx * pl->d.P;
+    mm.XB = x_field(pl, 6);
     mm.status = pl->status;
   }
 }
@@ -990,7 +1026,7 @@ static int startup_step(jfb_kmm_plan* pl, cudaStream_t s, c64* const* rec = null
     if (pl->mhd) {
       MhdArgs m = blank_mhd();
       m.mode = kMhdStep;
-      m.HXA = pl->HX + (size_t)3 * pl->d.Nx * pl->d.P;
+      m.HXA = hx_field(pl, 3);
       m.c0 = 1.0;
       m.slin = a.cL * pl->eta;
       m.d0 = kRK3A[rk];
@@ -1003,7 +1039,7 @@ static int startup_step(jfb_kmm_plan* pl, cudaStream_t s, c64* const* rec = null
       m.sa = pl->sa_startup[rk];
       m.sa_rec = pl->sg_rec;
       m.A_out = pl->AR[nw];
-      m.XB = pl->X + (size_t)6 * pl->d.Nx * pl->d.P;
+      m.XB = x_field(pl, 6);
       if ((st = launch_mhd(pl, m, s))) return st;
     }
     if (rec && rk < 2) {
@@ -1164,7 +1200,7 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   pl->mhd = mhd != nullptr;
   if (mhd) {
     pl->eta = mhd->eta;
-    pl->mphys = MhdPhys{mhd->b0[0], mhd->b0[1], mhd->b0[2], 2.0 * mhd->omega};
+    pl->mphys = MhdPhys{mhd->b0[0], mhd->b0[1], mhd->b0[2], 2.0 * mhd->omega, cfg->u_wall};
   }
   int st = JFB_OK;
   auto fail = [&](int code) {
@@ -1252,7 +1288,8 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
       return fail(JFB_ERR_ARG);
     }
     if (allow_smem((const void*)mhd_a_kernel) != cudaSuccess ||
-        allow_smem((const void*)z_cross_mhd_kernel) != cudaSuccess) {
+        allow_smem((const void*)z_cross_mhd_kernel<double>) != cudaSuccess ||
+        allow_smem((const void*)z_cross_mhd_kernel<float>) != cudaSuccess) {
       set_error("cannot configure the MHD kernels");
       return fail(JFB_ERR_CUDA);
     }
@@ -1394,15 +1431,14 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
     G.oVel = G.oGO + round4(nDo);
     G.oMean = G.rows * kGLd;
     G.oMid = G.oMean + 2 * N + 6 * d.nD;
-    const size_t smem = ((size_t)G.oMid + 5 * 2 * kGW) * sizeof(double);
+    const size_t smem = ((size_t)G.oMid + (d.grad ? 6 : 5) * 2 * kGW) * sizeof(double);
     const char* env = std::getenv("JFB200_PENCIL");
     const bool want = !(env && std::string(env) == "warp");
-    // the tensor-core stage writes the rotational form's fields (u, omega)
-    pl->gemm = smem <= 227 * 1024 && (d.nD + 1) / 2 <= kMaxM && Jl <= kMaxM && !d.grad;
+    pl->gemm = smem <= 227 * 1024 && (d.nD + 1) / 2 <= kMaxM && Jl <= kMaxM;
     GemmHost gh;
     if (pl->gemm) {
       std::string err;
-      if (!build_gemm_operators(pl->hop, gh, err)) {
+      if (!build_gemm_operators(pl->hop, gh, err, d.grad)) {
         set_error(err);
         return fail(JFB_ERR_ARG);
       }
@@ -1655,7 +1691,6 @@ extern "C" int jfb_mhd_create(const jfb_kmm_config* cfg, const jfb_mhd_params* p
   JFB_REQUIRE(std::isfinite(prm->omega) && std::isfinite(prm->b0[0]) &&
                   std::isfinite(prm->b0[1]) && std::isfinite(prm->b0[2]),
               "omega and b0 must be finite");
-  JFB_REQUIRE(cfg->precision == JFB_PRECISION_FP64, "the MHD step runs in FP64 only");
   return create_plan(cfg, prm, out);
 }
 
@@ -2101,8 +2136,16 @@ extern "C" int jfb_mhd_convection(jfb_kmm_plan* pl, void* h0, void* h1, void* h2
   for (int half = 0; half < 2; ++half) {
     StageArgs a = blank_args();
     a.mode = kHOnly;
-    a.HX = pl->HX + (size_t)half * 3 * d.Nx * d.P;
+    a.HX = hx_field(pl, 3 * half);
     a.Hd_out = pl->HD;
+    // mixed form: complex64 nonlinear fields; the flow's base-flow terms are
+    // added in FP64 from the x-physical u, omega (the EMF's are in HX)
+    a.x32 = pl->mixed ? 1 : 0;
+    a.Xlin = (pl->mixed && half == 0) ? reinterpret_cast<const c32*>(pl->X) : nullptr;
+    if (half == 1) {  // the EMF's U_b e_y x B0 (mean mode; the step adds it in the A stage)
+      a.emf_b0z = pl->mphys.uw_emf * pl->mphys.b0z;
+      a.emf_b0x = pl->mphys.uw_emf * pl->mphys.b0x;
+    }
     if ((st = launch_pencil(pl, a, s))) return st;
     for (int f = 0; f < 3; ++f)
       to_full_kernel<<<512, 256, 0, s>>>(pl->HD + (size_t)f * d.nD * d.P, d.nD, d.Ny, d.Nz,
@@ -2963,20 +3006,33 @@ static bool ensemble_batchable(const jfb_ensemble* e) {
   if (env && std::string(env) == "streams") return false;
   if (e->m.size() > (size_t)kEnsMax) return false;
   for (const jfb_kmm_plan* pl : e->m)
-    if (!pl->mhd || !pl->gemm || pl->py == 0 || pl->py != e->m[0]->py || pl->mixed) return false;
+    if (!pl->mhd || !pl->gemm || pl->py == 0 || pl->py != e->m[0]->py ||
+        pl->mixed != e->m[0]->mixed)
+      return false;
   return true;
 }
 
-template <int P>
+template <int P, typename F>
 static cudaError_t ens_y_launch(const EnsGroup& G, const EnsMember* tab, bool backward,
                                 cudaStream_t s) {
   const int stage = backward ? 2 : 4;
   const int blocks = G.htiles.first[stage][G.htiles.nm];
   if (backward)
-    ens_y_backward_kernel<P><<<blocks, 256, G.smem[2], s>>>(tab, G.tiles);
+    ens_y_backward_kernel<P, F><<<blocks, 256, G.smem[2], s>>>(tab, G.tiles);
   else
-    ens_y_forward_kernel<P><<<blocks, 256, G.smem[4], s>>>(tab, G.tiles);
+    ens_y_forward_kernel<P, F><<<blocks, 256, G.smem[4], s>>>(tab, G.tiles);
   return cudaGetLastError();
+}
+
+template <typename F>
+static cudaError_t ens_y_any(int py, const EnsGroup& G, const EnsMember* tab, bool backward,
+                             cudaStream_t s) {
+  switch (py) {
+    case 2: return ens_y_launch<2, F>(G, tab, backward, s);
+    case 3: return ens_y_launch<3, F>(G, tab, backward, s);
+    case 4: return ens_y_launch<4, F>(G, tab, backward, s);
+    default: return ens_y_launch<6, F>(G, tab, backward, s);
+  }
 }
 
 // The five launches of one group's steady step with ring-phase table `tab`.
@@ -2987,23 +3043,16 @@ static int ensemble_group_step(const jfb_ensemble* e, const EnsGroup& G, const E
   JFB_CHECK_LAUNCH();
   ens_mhd_a_kernel<<<T.first[1][T.nm], kMhdThreads, G.smem[1], s>>>(tab, G.tiles);
   JFB_CHECK_LAUNCH();
-  cudaError_t ce;
-  switch (e->py) {
-    case 2: ce = ens_y_launch<2>(G, tab, true, s); break;
-    case 3: ce = ens_y_launch<3>(G, tab, true, s); break;
-    case 4: ce = ens_y_launch<4>(G, tab, true, s); break;
-    default: ce = ens_y_launch<6>(G, tab, true, s); break;
-  }
-  JFB_CHECK_CUDA(ce);
-  ens_z_cross_kernel<<<T.first[3][T.nm], 256, G.smem[3], s>>>(tab, G.tiles);
+  const bool f32 = e->m[0]->mixed;
+  JFB_CHECK_CUDA(f32 ? ens_y_any<float>(e->py, G, tab, true, s)
+                     : ens_y_any<double>(e->py, G, tab, true, s));
+  if (f32)
+    ens_z_cross_kernel<float><<<T.first[3][T.nm], 256, G.smem[3], s>>>(tab, G.tiles);
+  else
+    ens_z_cross_kernel<double><<<T.first[3][T.nm], 256, G.smem[3], s>>>(tab, G.tiles);
   JFB_CHECK_LAUNCH();
-  switch (e->py) {
-    case 2: ce = ens_y_launch<2>(G, tab, false, s); break;
-    case 3: ce = ens_y_launch<3>(G, tab, false, s); break;
-    case 4: ce = ens_y_launch<4>(G, tab, false, s); break;
-    default: ce = ens_y_launch<6>(G, tab, false, s); break;
-  }
-  JFB_CHECK_CUDA(ce);
+  JFB_CHECK_CUDA(f32 ? ens_y_any<float>(e->py, G, tab, false, s)
+                     : ens_y_any<double>(e->py, G, tab, false, s));
   return JFB_OK;
 }
 
@@ -3019,15 +3068,19 @@ static int ensemble_table(jfb_ensemble* e, EnsGroup& G, int k) {
     EnsMember& x = h[i];
     std::memset(&x, 0, sizeof(x));
     x.d = pl->d;
+    x.dT = pl->mixed ? tdims<float>(pl) : pl->d;
     x.o = pl->ops;
     x.G = pl->gops;
     x.ga = gemm_args(pl, a);
     x.M = pl->mops;
     x.ma = mm;
+    x.ma.x32 = pl->mixed ? 1 : 0;
+    x.ma.uw_b0z = pl->mphys.uw_emf * pl->mphys.b0z;
+    x.ma.uw_b0x = pl->mphys.uw_emf * pl->mphys.b0x;
     x.ph = pl->mphys;
     x.fz = pl->fz;
-    x.twy = pl->twy;
-    x.twz = pl->twz;
+    x.twy = pl->mixed ? (const void*)pl->twy32 : (const void*)pl->twy;
+    x.twz = pl->mixed ? (const void*)pl->twz32 : (const void*)pl->twz;
     x.X = pl->X;
     x.Y = pl->Y;
     x.HZ = pl->HZ;
@@ -3141,12 +3194,16 @@ extern "C" int jfb_ensemble_create(jfb_kmm_plan* const* plans, int32_t n, jfb_en
       if ((err = cudaMemcpy(G.tiles, &T, sizeof(EnsTiles), cudaMemcpyHostToDevice)) != cudaSuccess)
         return fail(err);
     }
+#define JFB_ENS_Y(F)                                                                     \
+  (const void*)ens_y_backward_kernel<2, F>, (const void*)ens_y_forward_kernel<2, F>,     \
+      (const void*)ens_y_backward_kernel<3, F>, (const void*)ens_y_forward_kernel<3, F>, \
+      (const void*)ens_y_backward_kernel<4, F>, (const void*)ens_y_forward_kernel<4, F>, \
+      (const void*)ens_y_backward_kernel<6, F>, (const void*)ens_y_forward_kernel<6, F>
     const void* fns[] = {(const void*)ens_pencil_kernel, (const void*)ens_mhd_a_kernel,
-                         (const void*)ens_z_cross_kernel,
-                         (const void*)ens_y_backward_kernel<2>, (const void*)ens_y_forward_kernel<2>,
-                         (const void*)ens_y_backward_kernel<3>, (const void*)ens_y_forward_kernel<3>,
-                         (const void*)ens_y_backward_kernel<4>, (const void*)ens_y_forward_kernel<4>,
-                         (const void*)ens_y_backward_kernel<6>, (const void*)ens_y_forward_kernel<6>};
+                         (const void*)ens_z_cross_kernel<double>,
+                         (const void*)ens_z_cross_kernel<float>, JFB_ENS_Y(double),
+                         JFB_ENS_Y(float)};
+#undef JFB_ENS_Y
     for (const void* f : fns)
       if ((err = allow_smem(f)) != cudaSuccess) return fail(err);
   }

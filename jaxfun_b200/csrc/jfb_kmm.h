@@ -40,9 +40,11 @@ struct HostOperators {
 //   Nu/Ng right-hand sides   gNuE, gNuO, gNgE, gNgO   (physical -> coefficient)
 //   mass rows of Su / Sg     gMuE, gMuO, gMgE, gMgO   (coefficient -> coefficient)
 //   velocity / vorticity     gA0Ee ... gB1Oo          (coefficient -> physical)
+//   gradient form: d/dx u0   gA1Oe, gA1Eo (A1 = V D S_B^T; empty otherwise)
 enum GemmSub {
   gNuE, gNuO, gNgE, gNgO, gMuE, gMuO, gMgE, gMgO,
   gA0Ee, gP2Ee, gP1Oe, gP1Eo, gA0Oo, gP2Oo, gB1Ee, gB2Oe, gB2Eo, gB1Oo,
+  gA1Oe, gA1Eo,
   gNumSub
 };
 
@@ -54,7 +56,7 @@ struct GemmHost {
   std::vector<double> R3;     // S_D Q (nD x N): mean-flow nonlinear rows
   std::vector<double> X2D;    // (T_i, phi_j'')_w of the Dirichlet basis (nD x nD)
   // middle Gauss node of an odd N: rows of A0 (even cols), P2 (even), P1 (odd),
-  // B1 (even), B2 (odd), each padded to mid_stride
+  // B1 (even), B2 (odd), A1 (odd; gradient form), each padded to mid_stride
   std::vector<double> mid;
   int mid_stride = 0;
   // MHD: x-physical values (N x nD, row-major) of a Dirichlet-basis field and
@@ -113,7 +115,8 @@ std::vector<double> x_map_matrix(const XBasis& xb, int map, int k, int* rows, in
 Stencil make_stencil(int N, bool biharmonic, int family = 0);
 // Builds GemmHost from the 1-D operators; returns false (with a message) if a
 // parity property the split relies on does not hold.
-bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& err);
+bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& err,
+                          bool gradient = false);
 void build_host_operators(const jfb_kmm_config& cfg, HostOperators& op);
 void mode_coefficients(const HostOperators& op, const jfb_kmm_config& cfg, int ky,
                        int kz, double gamma, bool biharmonic, double out[3]);

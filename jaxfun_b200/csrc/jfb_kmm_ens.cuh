@@ -19,9 +19,13 @@ namespace jfb {
 
 constexpr int kEnsMax = 64;  // members of a batched ensemble
 
-// One member's arguments of the five stages of a steady step.
+// One member's arguments of the five stages of a steady step.  The
+// transform buffers and twiddles are complex128 (FP64 form) or complex64
+// (mixed form: the stage kernels' T = float); dT are the dimensions handed
+// to the periodic-axis stages (the mixed form leaves the flow's base flow
+// out of them).
 struct __align__(16) EnsMember {
-  Dims d;
+  Dims d, dT;
   DevOps o;
   GemmOps G;
   GemmStageArgs ga;
@@ -29,8 +33,8 @@ struct __align__(16) EnsMember {
   MhdArgs ma;
   MhdPhys ph;
   FFTPlan fz;
-  const c64 *twy, *twz;
-  c64 *X, *Y, *HZ, *HX;
+  const void *twy, *twz;
+  void *X, *Y, *HZ, *HX;
   const double* xb;
   int KCw, chunks;
 };
@@ -77,32 +81,39 @@ __global__ void __launch_bounds__(kMhdThreads, 1)
 }
 
 // twelve fields (u, omega, b, j) inverse along y: tile = (x-plane, field, kz chunk)
-template <int P>
+template <int P, typename F>
 __global__ void __launch_bounds__(256)
     ens_y_backward_kernel(const EnsMember* __restrict__ tab, const EnsTiles* __restrict__ T) {
   const int m = ens_member(T, 2, blockIdx.x);
   const EnsMember& e = ens_args(tab, m);
   const int t = blockIdx.x - T->first[2][m];
   const int zc = t % e.chunks, f = (t / e.chunks) % 12, j = t / (e.chunks * 12);
-  y_backward_warp_body<P, double>(e.d, e.KCw, e.twy, e.X, e.Y, j, f, zc);
+  y_backward_warp_body<P, F>(e.dT, e.KCw, static_cast<const cpx<F>*>(e.twy),
+                             static_cast<const cpx<F>*>(e.X), static_cast<cpx<F>*>(e.Y), j, f,
+                             zc);
 }
 
+template <typename F>
 __global__ void __launch_bounds__(256)
     ens_z_cross_kernel(const EnsMember* __restrict__ tab, const EnsTiles* __restrict__ T) {
   const int m = ens_member(T, 3, blockIdx.x);
   const EnsMember& e = ens_args(tab, m);
-  z_cross_mhd_body(e.o, e.d, e.ph, e.fz, e.twz, e.Y, e.HZ, blockIdx.x - T->first[3][m]);
+  z_cross_mhd_body<F>(e.o, e.dT, e.ph, e.fz, static_cast<const cpx<F>*>(e.twz),
+                      static_cast<const cpx<F>*>(e.Y), static_cast<cpx<F>*>(e.HZ),
+                      blockIdx.x - T->first[3][m]);
 }
 
 // six fields (n, emf) forward along y
-template <int P>
+template <int P, typename F>
 __global__ void __launch_bounds__(256)
     ens_y_forward_kernel(const EnsMember* __restrict__ tab, const EnsTiles* __restrict__ T) {
   const int m = ens_member(T, 4, blockIdx.x);
   const EnsMember& e = ens_args(tab, m);
   const int t = blockIdx.x - T->first[4][m];
   const int zc = t % e.chunks, f = (t / e.chunks) % 6, j = t / (e.chunks * 6);
-  y_forward_warp_body<P, double>(e.d, e.KCw, e.twy, e.HZ, e.HX, e.xb, j, f, zc);
+  y_forward_warp_body<P, F>(e.dT, e.KCw, static_cast<const cpx<F>*>(e.twy),
+                            static_cast<const cpx<F>*>(e.HZ), static_cast<cpx<F>*>(e.HX), e.xb,
+                            j, f, zc);
 }
 
 }  // namespace jfb

@@ -267,6 +267,32 @@ __device__ __forceinline__ void velocity_fields(double ky, double kz, c64 av, c6
   }
 }
 
+// Gradient form: u, d/dx u and d/dy u = i ky u (f[0..8]) of one pencil from
+// the symmetric or antisymmetric halves of A0 u0, A1 u0, P1 u0, P2 u0, B1 g,
+// B2 g (d/dx u1, d/dx u2 are the terms of omega that velocity_fields forms
+// from P2 u0, B2 g); for ky = kz = 0 the g slot carries the mean flow v + i w.
+__device__ __forceinline__ void gradient_fields(double ky, double kz, c64 av, c64 a1, c64 b1,
+                                                c64 b2, c64 c1, c64 c2, c64 (&f)[9]) {
+  const double k2 = ky * ky + kz * kz;
+  f[0] = av;
+  f[3] = a1;
+  if (k2 == 0.0) {
+    f[1] = cmk(c1.re, 0.0);
+    f[2] = cmk(c1.im, 0.0);
+    f[4] = cmk(c2.re, 0.0);
+    f[5] = cmk(c2.im, 0.0);
+  } else {
+    const double inv = 1.0 / k2;
+    f[1] = mul_i((ky * inv) * b1 + (kz * inv) * c1);
+    f[2] = mul_i((kz * inv) * b1 - (ky * inv) * c1);
+    f[4] = mul_i((ky * inv) * b2 + (kz * inv) * c2);
+    f[5] = mul_i((kz * inv) * b2 - (ky * inv) * c2);
+  }
+  f[6] = mul_i(ky * f[0]);
+  f[7] = mul_i(ky * f[1]);
+  f[8] = mul_i(ky * f[2]);
+}
+
 // Forward elimination with the unit lower factor of one parity class, in
 // place on y[r * stride] (r < m): y_r -= L[i, i-2] y_{r-1} + L[i, i-4] y_{r-2},
 // i = 2 r + par; the multipliers (rec[2 i], rec[2 i + 1]) are loaded eight
@@ -397,11 +423,12 @@ __device__ void mean_flow(const Dims& d, const DevOps& o, const GemmOps& G,
 }
 
 // One value of the middle-node products (odd N): operator op = e / 32 of
-// (A0, P2 | u0 even; P1 | u0 odd; B1 | g even; B2 | g odd), column e % 32.
+// (A0, P2 | u0 even; P1 | u0 odd; B1 | g even; B2 | g odd; A1 | u0 odd,
+// gradient form only), column e % 32.
 __device__ __forceinline__ double mid_dot(const GemmOps& G, const double* sm, int e) {
   const int col = e % (2 * kGW), op = e / (2 * kGW);
-  const int oB = (op <= 1) ? G.oUE : (op == 2) ? G.oUO : (op == 3) ? G.oGE : G.oGO;
-  const int K = (op <= 1) ? G.nBe : (op == 2) ? G.nBo : (op == 3) ? G.nDe : G.nDo;
+  const int oB = (op <= 1) ? G.oUE : (op == 2 || op == 5) ? G.oUO : (op == 3) ? G.oGE : G.oGO;
+  const int K = (op <= 1) ? G.nBe : (op == 2 || op == 5) ? G.nBo : (op == 3) ? G.nDe : G.nDo;
   const double* row = G.mid + op * G.mid_stride;
   double s = 0.0;
   for (int k = 0; k < K; ++k) s += __ldg(row + k) * sm[(size_t)(oB + k) * kGLd + col];
@@ -414,13 +441,21 @@ __device__ __forceinline__ void mid_store(const Dims& d, const GemmStageArgs& a,
                                           int w, int N, int Jl, size_t P) {
   if (s_p[w] < 0) return;
   auto val = [&](int op) { return cmk(md[op * 2 * kGW + 2 * w], md[op * 2 * kGW + 2 * w + 1]); };
-  c64 f[6];
-  velocity_fields(s_ky[w], s_kz[w], val(0), val(2), val(1), val(3), val(4), f);
-#pragma unroll
-  for (int q = 0; q < 6; ++q) {
+  auto put = [&](int q, const c64 v) {
     const size_t e = (size_t)q * N * P + (size_t)Jl * P + s_p[w];
-    if (a.x32) reinterpret_cast<c32*>(a.X)[e] = cmk((float)f[q].re, (float)f[q].im);
-    else a.X[e] = f[q];
+    if (a.x32) reinterpret_cast<c32*>(a.X)[e] = cmk((float)v.re, (float)v.im);
+    else a.X[e] = v;
+  };
+  if (d.grad) {
+    c64 f[9];
+    gradient_fields(s_ky[w], s_kz[w], val(0), val(5), val(2), val(1), val(3), val(4), f);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) put(q, f[q]);
+  } else {
+    c64 f[6];
+    velocity_fields(s_ky[w], s_kz[w], val(0), val(2), val(1), val(3), val(4), f);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) put(q, f[q]);
   }
 }
 
@@ -871,7 +906,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
     // middle Gauss node (odd N) while the velocity operators arrive: one FP64
     // dot product per (operator, pencil, re/im)
     __syncthreads();
-    if (tid < 5 * 2 * kGW) sm[G.oMid + tid] = mid_dot(G, sm, tid);
+    if (tid < (d.grad ? 6 : 5) * 2 * kGW) sm[G.oMid + tid] = mid_dot(G, sm, tid);
   }
   const bool staged = mbar_wait_bounded(&s_bar, 0, G.status, kStatusWaitTimeout);
   // a timed-out copy leaves the velocity operators incomplete: skip D (the
@@ -980,10 +1015,11 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
     const double* vs = sm + (size_t)G.oVel * kGLd - G.sub[gA0Ee].off + lane;
     for (int task = warp; task < 4 * MTv; task += kGWarps) {
       const int jt = task >> 2, ncol0 = (task & 3) * 8;
-      // accumulators: 0 aE, 1 b1E, 2 b2E, 3 c1E, 4 c2E, 5 aO, 6 b1O, 7 b2O, 8 c1O, 9 c2O
-      double acc[10][2];
+      // accumulators: 0 aE, 1 b1E, 2 b2E, 3 c1E, 4 c2E, 5 aO, 6 b1O, 7 b2O, 8 c1O, 9 c2O,
+      // gradient form: 10 a1O (A1 u0 even), 11 a1E (A1 u0 odd)
+      double acc[12][2];
 #pragma unroll
-      for (int q = 0; q < 10; ++q) acc[q][0] = acc[q][1] = 0.0;
+      for (int q = 0; q < 12; ++q) acc[q][0] = acc[q][1] = 0.0;
       auto group3 = [&](int oB, int s0, int s1, int s2, int q0, int q1, int q2) {
         const double* __restrict__ Bs = sm + (size_t)oB * kGLd + t4 * kGLd + ncol0 + g;
         const SubDesc d0 = G.sub[s0], d1 = G.sub[s1], d2 = G.sub[s2];
@@ -1014,22 +1050,28 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
       group3(G.oUO, gP1Eo, gA0Oo, gP2Oo, 1, 5, 7);
       group2(G.oGE, gB1Ee, gB2Oe, 3, 9);
       group2(G.oGO, gB2Eo, gB1Oo, 4, 8);
+      if (d.grad) {  // d/dx u0: A1 on the even and odd coefficient halves
+        auto group1 = [&](int oB, int s0, int q0) {
+          const double* __restrict__ Bs = sm + (size_t)oB * kGLd + t4 * kGLd + ncol0 + g;
+          const SubDesc d0 = G.sub[s0];
+          const double* A0 = vs + d0.off + jt * d0.kt * 32;
+#pragma unroll 4
+          for (int kt = 0; kt < d0.kt; ++kt)
+            dmma_8x8x4(acc[q0][0], acc[q0][1], A0[kt * 32], Bs[kt * 4 * kGLd]);
+        };
+        group1(G.oUE, gA1Oe, 10);
+        group1(G.oUO, gA1Eo, 11);
+      }
       // epilogue: six fields at x_j and x_{N-1-j}, j < Jl
       const int j = jt * 8 + g;
       const int w = (ncol0 >> 1) + t4;
       const int p = s_p[w];
       if (j < Jl && p >= 0) {
         const int jm = N - 1 - j;
-        c64 fe[6], fo[6];
-        velocity_fields(s_ky[w], s_kz[w], cmk(acc[0][0], acc[0][1]), cmk(acc[1][0], acc[1][1]),
-                        cmk(acc[2][0], acc[2][1]), cmk(acc[3][0], acc[3][1]),
-                        cmk(acc[4][0], acc[4][1]), fe);
-        velocity_fields(s_ky[w], s_kz[w], cmk(acc[5][0], acc[5][1]), cmk(acc[6][0], acc[6][1]),
-                        cmk(acc[7][0], acc[7][1]), cmk(acc[8][0], acc[8][1]),
-                        cmk(acc[9][0], acc[9][1]), fo);
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          const c64 vp = fe[q] + fo[q], vm = fe[q] - fo[q];
+        auto cv = [&](int q) { return cmk(acc[q][0], acc[q][1]); };
+        // field q at x_j and x_{N-1-j} from its symmetric and antisymmetric halves
+        auto put = [&](int q, const c64 fe, const c64 fo) {
+          const c64 vp = fe + fo, vm = fe - fo;
           const size_t e = (size_t)q * N * P + p;
           if (a.x32) {
             c32* X = reinterpret_cast<c32*>(a.X) + e;
@@ -1040,6 +1082,19 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
             X[(size_t)j * P] = vp;
             X[(size_t)jm * P] = vm;
           }
+        };
+        if (d.grad) {
+          c64 fe[9], fo[9];
+          gradient_fields(s_ky[w], s_kz[w], cv(0), cv(11), cv(1), cv(2), cv(3), cv(4), fe);
+          gradient_fields(s_ky[w], s_kz[w], cv(5), cv(10), cv(6), cv(7), cv(8), cv(9), fo);
+#pragma unroll
+          for (int q = 0; q < 9; ++q) put(q, fe[q], fo[q]);
+        } else {
+          c64 fe[6], fo[6];
+          velocity_fields(s_ky[w], s_kz[w], cv(0), cv(1), cv(2), cv(3), cv(4), fe);
+          velocity_fields(s_ky[w], s_kz[w], cv(5), cv(6), cv(7), cv(8), cv(9), fo);
+#pragma unroll
+          for (int q = 0; q < 6; ++q) put(q, fe[q], fo[q]);
         }
       }
     }

@@ -87,6 +87,9 @@ struct StageArgs {
   int x32;  // HX (read, step modes) and X (written by the x-backward) hold complex64
   const c32* Xlin;  // mixed form: u, omega of HX's state; FP64 base-flow terms added here
   int* status;      // plan status word: kStatusNonFinite when a solved value is not finite
+  // MHD EMF rows (kHOnly): U_wall B0z, U_wall B0x of the term U_b e_y x B0,
+  // added to the (0, 0) mode of components 0 and 2 (the z stage leaves it out)
+  double emf_b0z, emf_b0x;
 };
 
 __host__ __device__ inline int packed_rec_size(int n) {
@@ -743,6 +746,11 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
           v = cmk((double)h.re, (double)h.im);
         } else {
           v = a.HX[e];
+        }
+        if ((a.emf_b0z != 0.0 || a.emf_b0x != 0.0) && p0 + w == 0) {
+          const int f = fi / d.Nx, j = fi % d.Nx;
+          if (f == 0) v.re += a.emf_b0z * o.xphys[j];
+          else if (f == 2) v.re -= a.emf_b0x * o.xphys[j];
         }
         if (a.Xlin && a.mode != kFromPhys) {
           // base-flow terms of the rotational product in FP64 (the complex64

@@ -54,6 +54,7 @@ enum MhdMode { kMhdStep = 0, kMhdFields = 1, kMhdFromPhys = 2 };
 struct MhdPhys {
   double b0x, b0y, b0z;
   double two_omega;
+  double uw_emf;  // U_wall of the base flow in the EMF (U_b = uw_emf x)
 };
 
 struct MhdArgs {
@@ -68,6 +69,11 @@ struct MhdArgs {
   c64* A_out;
   c64* XB;  // b, j at the x nodes: 6 x [Nx][P] (null: not wanted)
   int* status;  // plan status word (kStatusNonFinite)
+  int x32;      // mixed form: HXA (the EMF) is read and XB written as complex64
+  // U_b e_y x B0 = x (U_wall B0z, 0, -U_wall B0x): a function of x alone, so
+  // only the (ky, kz) = (0, 0) mode of the EMF; added here in FP64 (the z
+  // stage leaves it out, so that no O(1) constant enters the transforms)
+  double uw_b0z, uw_b0x;
 };
 
 constexpr int kMhdThreads = 512;
@@ -122,7 +128,22 @@ __device__ __forceinline__ void mhd_a_body(const Dims& d, const DevOps& o, const
     for (int e = tid; e < 3 * N * kMhdW; e += kMhdThreads) {
       const int w = e % kMhdW, cj = e / kMhdW;  // cj = c N + j
       const int p = s_p[w];
-      HS[e] = (p >= 0) ? a.HXA[(size_t)cj * P + p] : cmk(0.0, 0.0);
+      c64 v = cmk(0.0, 0.0);
+      if (p >= 0) {
+        if (a.x32) {
+          const c32 h = reinterpret_cast<const c32*>(a.HXA)[(size_t)cj * P + p];
+          v = cmk((double)h.re, (double)h.im);
+        } else {
+          v = a.HXA[(size_t)cj * P + p];
+        }
+        if (p == 0 && a.mode == kMhdStep) {
+          const int c = cj / N;
+          const double x = o.xphys[cj - c * N];
+          if (c == 0) v.re += a.uw_b0z * x;
+          else if (c == 2) v.re -= a.uw_b0x * x;
+        }
+      }
+      HS[e] = v;
     }
     __syncthreads();
     // 1. scalar products S_D Q v of the three x profiles (mirror sums), and
@@ -304,9 +325,17 @@ __device__ __forceinline__ void mhd_a_body(const Dims& d, const DevOps& o, const
     }
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-      c64* X = a.XB + (size_t)f * N * P + p;
-      X[(size_t)j * P] = S[f] + A[f];
-      if (jm != j) X[(size_t)jm * P] = S[f] - A[f];
+      const size_t e0 = (size_t)f * N * P + p;
+      const c64 vj = S[f] + A[f], vm = S[f] - A[f];
+      if (a.x32) {
+        c32* X = reinterpret_cast<c32*>(a.XB) + e0;
+        X[(size_t)j * P] = cmk((float)vj.re, (float)vj.im);
+        if (jm != j) X[(size_t)jm * P] = cmk((float)vm.re, (float)vm.im);
+      } else {
+        c64* X = a.XB + e0;
+        X[(size_t)j * P] = vj;
+        if (jm != j) X[(size_t)jm * P] = vm;
+      }
     }
   }
 }
@@ -320,24 +349,33 @@ __global__ void __launch_bounds__(kMhdThreads, 1)
 // ---------------------------------------------------------------------------
 // z stage of the coupled step, per group of kZRows (x, y) rows: twelve half
 // spectra (u, omega, b, j) -> six packed complex inverse FFTs, the products
-//   n = -(u_t x omega_t) - j x b,   emf = (u + U_b e_y) x b
+//   n = -(u_t x omega_t) - j x (b + B0) - 2 Omega e_z x u,
+//   emf = (u + U_b e_y) x (b + B0)
 // (_mhd_convection, pcf_mhd_jax.py:339-357; the flow part in the split form
-// of rotational_product, whose constant base-flow term the y stage adds; b
-// includes the imposed field and n the Coriolis term of MhdPhys), then three
-// packed forward transforms: HZ fields (n_x, n_y, n_z, e_x, e_y, e_z).
+// of rotational_product, whose constant base-flow term the y stage adds;
+// B0 the imposed field and Omega the rotation of MhdPhys,
+// pcf_mhd_mri_shearpy_jax.py:149-176), then three packed forward
+// transforms: HZ fields (n_x, n_y, n_z, e_x, e_y, e_z).  The products are
+// expanded so that no O(1) value (B0, U_b) is added to a perturbation value
+// before a product: in FP32 (the mixed form) every term keeps the
+// perturbation's digits.  The EMF's term U_b e_y x B0, a function of x
+// alone, is left to mhd_a_kernel (FP64, mean pencil).  In the mixed form the
+// flow's base-flow terms are left out here too (d.uwall = 0; the pencil
+// stage adds them in FP64), the EMF's U_b e_y x b is not (ph.uw_emf).
 // ---------------------------------------------------------------------------
 // The z stage of rows [bid kZRows, (bid + 1) kZRows) (the kernel below, or
 // one member's rows of the ensemble kernel).
+template <typename T>
 __device__ __forceinline__ void z_cross_mhd_body(const DevOps& o, const Dims& d,
                                                  const MhdPhys& ph, const FFTPlan& plan,
-                                                 const c64* __restrict__ tw,
-                                                 const c64* __restrict__ Y,
-                                                 c64* __restrict__ HZ, const int bid) {
+                                                 const cpx<T>* __restrict__ tw,
+                                                 const cpx<T>* __restrict__ Y,
+                                                 cpx<T>* __restrict__ HZ, const int bid) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int NC = kZRows * 6;   // packed input columns
   constexpr int NCf = kZRows * 3;  // packed output columns
-  c64* A = reinterpret_cast<c64*>(smem_raw);
-  c64* B = A + d.Mz * NC;
+  cpx<T>* A = reinterpret_cast<cpx<T>*>(smem_raw);
+  cpx<T>* B = A + d.Mz * NC;
   const int row0 = bid * kZRows;  // row = j * My + y
   const int nrows = d.Nx * d.My;
   const size_t plane = (size_t)d.Nx * d.My * d.Kz;
@@ -346,55 +384,55 @@ __device__ __forceinline__ void z_cross_mhd_body(const DevOps& o, const Dims& d,
     const int k = idx % d.Mz, c = idx / d.Mz;
     const int rl = c / 6, pr = c % 6;
     const int row = row0 + rl;
-    c64 z = cmk(0.0, 0.0);
+    cpx<T> z = cmk(T(0), T(0));
     if (row < nrows) {
-      const c64* fa = Y + (size_t)(2 * pr) * plane + (size_t)row * d.Kz;
-      const c64* fb = Y + (size_t)(2 * pr + 1) * plane + (size_t)row * d.Kz;
+      const cpx<T>* fa = Y + (size_t)(2 * pr) * plane + (size_t)row * d.Kz;
+      const cpx<T>* fb = Y + (size_t)(2 * pr + 1) * plane + (size_t)row * d.Kz;
       if (k == 0) {
         z = cmk(fa[0].re, fb[0].re);
       } else if (k < d.Kz) {
-        const c64 xa = fa[k], xb = fb[k];
+        const cpx<T> xa = fa[k], xb = fb[k];
         z = cmk(xa.re - xb.im, xa.im + xb.re);
       } else if (k > d.Mz - d.Kz) {
         const int kk = d.Mz - k;
-        const c64 xa = fa[kk], xb = fb[kk];  // conj(xa) + i conj(xb)
+        const cpx<T> xa = fa[kk], xb = fb[kk];  // conj(xa) + i conj(xb)
         z = cmk(xa.re + xb.im, -xa.im + xb.re);
       }
     }
     A[k * NC + c] = z;
   }
   __syncthreads();
-  c64* phys = fft_columns<double>(A, B, plan, NC, NC, tw, +1);
-  c64* other = (phys == A) ? B : A;
+  cpx<T>* phys = fft_columns<T>(A, B, plan, NC, NC, tw, +1);
+  cpx<T>* other = (phys == A) ? B : A;
+  const T bx = T(ph.b0x), by = T(ph.b0y), bz = T(ph.b0z), tw2 = T(ph.two_omega);
   for (int idx = threadIdx.x; idx < d.Mz * kZRows; idx += blockDim.x) {
     const int rl = idx % kZRows, n = idx / kZRows;
     const int row = row0 + rl;
     const int j = (row < nrows) ? row / d.My : 0;
-    const c64* z = phys + n * NC + rl * 6;
-    const double u0 = z[0].re, u1 = z[0].im, u2 = z[1].re;
-    const double w0 = z[1].im, w1 = z[2].re, w2 = z[2].im;
-    const double b0 = z[3].re + ph.b0x, b1 = z[3].im + ph.b0y, b2 = z[4].re + ph.b0z;
-    const double j0 = z[4].im, j1 = z[5].re, j2 = z[5].im;
-    const double ub = d.uwall * o.xphys[j];
-    double n0, n1, n2;
-    rotational_product(u0, u1, u2, w0, w1, w2, ub, d.uwall, n0, n1, n2);
-    n0 -= ph.two_omega * u1;
-    n1 += ph.two_omega * u0;
-    n0 -= j1 * b2 - j2 * b1;
-    n1 -= j2 * b0 - j0 * b2;
-    n2 -= j0 * b1 - j1 * b0;
-    const double v1 = u1 + ub;
-    const double e0 = v1 * b2 - u2 * b1;
-    const double e1 = u2 * b0 - u0 * b2;
-    const double e2 = u0 * b1 - v1 * b0;
-    c64* out = other + n * NCf + rl * 3;
+    const cpx<T>* z = phys + n * NC + rl * 6;
+    const T u0 = z[0].re, u1 = z[0].im, u2 = z[1].re;
+    const T w0 = z[1].im, w1 = z[2].re, w2 = z[2].im;
+    const T b0 = z[3].re, b1 = z[3].im, b2 = z[4].re;
+    const T j0 = z[4].im, j1 = z[5].re, j2 = z[5].im;
+    const T ub = T(d.uwall * o.xphys[j]), ue = T(ph.uw_emf * o.xphys[j]);
+    T n0, n1, n2;
+    rotational_product(u0, u1, u2, w0, w1, w2, ub, T(d.uwall), n0, n1, n2);
+    n0 -= tw2 * u1;
+    n1 += tw2 * u0;
+    n0 -= (j1 * b2 - j2 * b1) + (j1 * bz - j2 * by);
+    n1 -= (j2 * b0 - j0 * b2) + (j2 * bx - j0 * bz);
+    n2 -= (j0 * b1 - j1 * b0) + (j0 * by - j1 * bx);
+    const T e0 = (u1 * b2 - u2 * b1) + (u1 * bz - u2 * by) + ue * b2;
+    const T e1 = (u2 * b0 - u0 * b2) + (u2 * bx - u0 * bz);
+    const T e2 = (u0 * b1 - u1 * b0) + (u0 * by - u1 * bx) - ue * b0;
+    cpx<T>* out = other + n * NCf + rl * 3;
     out[0] = cmk(n0, n1);
     out[1] = cmk(n2, e0);
     out[2] = cmk(e1, e2);
   }
   __syncthreads();
-  c64* spec = fft_columns<double>(other, phys, plan, NCf, NCf, tw, -1);
-  const double scale = 1.0 / d.Mz;
+  cpx<T>* spec = fft_columns<T>(other, phys, plan, NCf, NCf, tw, -1);
+  const T scale = T(1.0 / d.Mz), h = T(0.5);
   for (int idx = threadIdx.x; idx < d.Kz * kZRows * 6; idx += blockDim.x) {
     const int k = idx % d.Kz;
     const int rf = idx / d.Kz;
@@ -402,21 +440,23 @@ __device__ __forceinline__ void z_cross_mhd_body(const DevOps& o, const Dims& d,
     const int row = row0 + rl;
     if (row >= nrows) continue;
     const int col = rl * 3 + f / 2;
-    const c64 Zk = spec[k * NCf + col];
-    const c64 Zm = spec[((d.Mz - k) % d.Mz) * NCf + col];
+    const cpx<T> Zk = spec[k * NCf + col];
+    const cpx<T> Zm = spec[((d.Mz - k) % d.Mz) * NCf + col];
     // x + i y packed: X_k = (Z_k + conj Z_-k)/2, Y_k = (Z_k - conj Z_-k)/(2i)
-    c64 v;
-    if ((f & 1) == 0) v = cmk(0.5 * (Zk.re + Zm.re), 0.5 * (Zk.im - Zm.im));
-    else v = cmk(0.5 * (Zk.im + Zm.im), -0.5 * (Zk.re - Zm.re));
+    cpx<T> v;
+    if ((f & 1) == 0) v = cmk(h * (Zk.re + Zm.re), h * (Zk.im - Zm.im));
+    else v = cmk(h * (Zk.im + Zm.im), -h * (Zk.re - Zm.re));
     HZ[(size_t)f * plane + (size_t)row * d.Kz + k] = scale * v;
   }
 }
 
+template <typename T>
 __global__ void __launch_bounds__(256)
     z_cross_mhd_kernel(const __grid_constant__ DevOps o, const __grid_constant__ Dims d,
                        const __grid_constant__ MhdPhys ph, const __grid_constant__ FFTPlan plan,
-                       const c64* __restrict__ tw, const c64* __restrict__ Y, c64* __restrict__ HZ) {
-  z_cross_mhd_body(o, d, ph, plan, tw, Y, HZ, blockIdx.x);
+                       const cpx<T>* __restrict__ tw, const cpx<T>* __restrict__ Y,
+                       cpx<T>* __restrict__ HZ) {
+  z_cross_mhd_body<T>(o, d, ph, plan, tw, Y, HZ, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------

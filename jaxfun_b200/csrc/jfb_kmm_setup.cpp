@@ -398,7 +398,8 @@ bool cols_mirror(const LMat& M, int sign_even_col) {
 }
 }  // namespace
 
-bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& err) {
+bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& err,
+                          bool gradient) {
   const int N = op.N, nB = op.nB, nD = op.nD;
   const LD pi = std::acos(-1.0L);
   const LD dfx = op.dfx;
@@ -447,13 +448,14 @@ bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& er
   const LMat B2 = mul(mul(V, D), SDt);
   const LMat P1 = mul(B1, F);
   const LMat P2 = mul(B2, F);
+  const LMat A1 = mul(mul(V, D), SBt);  // d/dx of a TB field at the nodes (gradient form)
   const LMat K0 = from_dense(op.XB0, nB, nB), K2 = from_dense(op.XB2, nB, nB),
              K4 = from_dense(op.XB4, nB, nB);
   const LMat X0D = from_dense(op.XD0, nD, nD), X2D = from_dense(op.XD2, nD, nD);
 
   if (!rows_mirror(R0, +1) || !rows_mirror(R1, -1) || !rows_mirror(R2, +1) || !rows_mirror(R3, +1) ||
       !cols_mirror(A0, +1) || !cols_mirror(B1, +1) || !cols_mirror(B2, -1) ||
-      !cols_mirror(P1, -1) || !cols_mirror(P2, +1)) {
+      !cols_mirror(P1, -1) || !cols_mirror(P2, +1) || (gradient && !cols_mirror(A1, -1))) {
     err = "x-operators lack the mirror parity of the Gauss nodes";
     return false;
   }
@@ -541,8 +543,12 @@ bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& er
   add(gB2Oe, Jl, nDe, ph(B2, 0));
   add(gB2Eo, Jl, nDo, ph(B2, 1));
   add(gB1Oo, Jl, nDo, ph(B1, 1));
+  // gradient form: d/dx u0 at the nodes (an even coefficient gives the
+  // antisymmetric half); empty sub-matrices otherwise
+  add(gA1Oe, gradient ? Jl : 0, gradient ? nBe : 0, ph(A1, 0));
+  add(gA1Eo, gradient ? Jl : 0, gradient ? nBo : 0, ph(A1, 1));
   gh.mid_stride = std::max(std::max(nBe, nBo), std::max(nDe, nDo));
-  gh.mid.assign((size_t)5 * gh.mid_stride, 0.0);
+  gh.mid.assign((size_t)6 * gh.mid_stride, 0.0);
   if (N % 2 == 1) {
     const int j = Jl;
     for (int k = 0; k < nBe; ++k) {
@@ -552,6 +558,8 @@ bool build_gemm_operators(const HostOperators& op, GemmHost& gh, std::string& er
     for (int k = 0; k < nBo; ++k) gh.mid[2 * gh.mid_stride + k] = (double)P1(j, 2 * k + 1);
     for (int k = 0; k < nDe; ++k) gh.mid[3 * gh.mid_stride + k] = (double)B1(j, 2 * k);
     for (int k = 0; k < nDo; ++k) gh.mid[4 * gh.mid_stride + k] = (double)B2(j, 2 * k + 1);
+    if (gradient)
+      for (int k = 0; k < nBo; ++k) gh.mid[5 * gh.mid_stride + k] = (double)A1(j, 2 * k + 1);
   }
 
   {

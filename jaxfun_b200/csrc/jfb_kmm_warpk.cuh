@@ -267,6 +267,95 @@ __global__ void __launch_bounds__(256) z_cross_warp_kernel(DevOps o, Dims d,
 }
 
 // ---------------------------------------------------------------------------
+// z_grad: the gradient form's z stage (z_grad_kernel) with warp-shuffle
+// transforms, FP64, one warp per pair of (x, y) rows.  Per row, the twelve
+// real fields u_i, d/dx u_i, d/dy u_i (Y fields 0..8) and d/dz u_i = i kz u_i
+// (formed here) go through six packed inverse transforms; the three products
+// n_i = u . grad u_i + U_b d/dy u_i (+ u_0 dU_b/dx for i = 1) of the row
+// pair go through three packed forward transforms.
+// ---------------------------------------------------------------------------
+template <int P, int QK>
+__global__ void __launch_bounds__(256) z_grad_warp_kernel(DevOps o, Dims d,
+                                                          const c64* __restrict__ tw,
+                                                          const c64* __restrict__ Y,
+                                                          c64* __restrict__ HZ) {
+  const int lane = threadIdx.x & 31;
+  const int pair = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int nrows = d.Nx * d.My;
+  const int rowa = 2 * pair;
+  if (rowa >= nrows) return;
+  const bool hasb = rowa + 1 < nrows;
+  WarpTw<P, double> w;
+  load_warp_tw<P, double>(w, tw, lane);
+  const size_t plane = (size_t)d.Nx * d.My * d.Kz;
+  double nrm[2][3][P];
+#pragma unroll
+  for (int rb = 0; rb < 2; ++rb) {
+    const int row = rowa + rb;
+    const bool ok = rb == 0 || hasb;
+    // virtual real field v of the row at spectral index k: Y field v (v < 9)
+    // or i kz times Y field v - 9
+    auto spec = [&](int v, int k) -> c64 {
+      if (!ok || k >= d.Kz) return cmk(0.0, 0.0);
+      const c64 x = Y[(size_t)(v < 9 ? v : v - 9) * plane + (size_t)row * d.Kz + k];
+      return v < 9 ? x : mul_i((k * d.dfz) * x);
+    };
+    c64 ph[6][P];
+#pragma unroll
+    for (int pr = 0; pr < 6; ++pr) {
+      c64 A[QK], B[QK];
+#pragma unroll
+      for (int q = 0; q < QK; ++q) {
+        A[q] = spec(2 * pr, 32 * q + lane);
+        B[q] = spec(2 * pr + 1, 32 * q + lane);
+      }
+      build_packed<P, QK, double>(A, B, d.Kz, lane, ph[pr]);
+      warp_fft_inverse<P, double>(ph[pr], w, lane);
+    }
+    const int j = (ok ? row : rowa) / d.My;
+    const double ub = d.uwall * o.xphys[j];
+#pragma unroll
+    for (int r = 0; r < P; ++r) {
+      const double u0 = ph[0][r].re, u1 = ph[0][r].im, u2 = ph[1][r].re;
+      const double x0 = ph[1][r].im, x1 = ph[2][r].re, x2 = ph[2][r].im;  // d/dx
+      const double y0 = ph[3][r].re, y1 = ph[3][r].im, y2 = ph[4][r].re;  // d/dy
+      const double z0 = ph[4][r].im, z1 = ph[5][r].re, z2 = ph[5][r].im;  // d/dz
+      nrm[rb][0][r] = (u0 * x0 + u1 * y0 + u2 * z0) + ub * y0;
+      nrm[rb][1][r] = ((u0 * x1 + u1 * y1 + u2 * z1) + ub * y1) + u0 * d.uwall;
+      nrm[rb][2][r] = (u0 * x2 + u1 * y2 + u2 * z2) + ub * y2;
+    }
+  }
+  c64 F0[P], F1[P], F2[P];
+#pragma unroll
+  for (int r = 0; r < P; ++r) {
+    F0[r] = cmk(nrm[0][0][r], nrm[0][1][r]);
+    F1[r] = cmk(nrm[1][0][r], nrm[1][1][r]);
+    F2[r] = cmk(nrm[0][2][r], nrm[1][2][r]);
+  }
+  warp_fft_forward<P, double>(F0, w, lane);
+  warp_fft_forward<P, double>(F1, w, lane);
+  warp_fft_forward<P, double>(F2, w, lane);
+  c64 xa0[QK], xa1[QK], xb0[QK], xb1[QK], x2a[QK], x2b[QK];
+  unpack_pair<P, QK, double>(F0, lane, xa0, xa1);
+  unpack_pair<P, QK, double>(F1, lane, xb0, xb1);
+  unpack_pair<P, QK, double>(F2, lane, x2a, x2b);
+  const double scale = 1.0 / (32 * P);
+#pragma unroll
+  for (int q = 0; q < QK; ++q) {
+    const int k = 32 * q + lane;
+    if (k >= d.Kz) continue;
+    HZ[(size_t)0 * plane + (size_t)rowa * d.Kz + k] = scale * xa0[q];
+    HZ[(size_t)1 * plane + (size_t)rowa * d.Kz + k] = scale * xa1[q];
+    HZ[(size_t)2 * plane + (size_t)rowa * d.Kz + k] = scale * x2a[q];
+    if (hasb) {
+      HZ[(size_t)0 * plane + (size_t)(rowa + 1) * d.Kz + k] = scale * xb0[q];
+      HZ[(size_t)1 * plane + (size_t)(rowa + 1) * d.Kz + k] = scale * xb1[q];
+      HZ[(size_t)2 * plane + (size_t)(rowa + 1) * d.Kz + k] = scale * x2b[q];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // z_forward_real: three real fields (Nx, Ny, Nz) -> half spectra along z,
 // scaled 1/Nz.  One warp per pair of rows.
 // ---------------------------------------------------------------------------
@@ -436,26 +525,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
     // third product with zero)
     auto z_rows = [&](int ya, bool hasb) {
       T nrm[2][3][PZ];
-      // both rows' spectra (six fields, half of them in the peer CTA) are
-      // read before the first transform: the peer reads overlap
-      cpx<T> A[2][3][QK], B[2][3][QK];
-#pragma unroll
-      for (int rb = 0; rb < 2; ++rb) {
-        const int y = rank * MH + ya + rb;
-#pragma unroll
-        for (int pr = 0; pr < 3; ++pr)
-#pragma unroll
-          for (int q = 0; q < QK; ++q) {
-            const int kz = 32 * q + lane;
-            A[rb][pr][q] = B[rb][pr][q] = cmk(T(0), T(0));
-            if (kz < Kz && (rb == 0 || hasb)) {
-              const int own = kz >= KH, cl = kz - own * KH;
-              const cpx<T>* base = (own == rank) ? Ys : Ypeer;
-              A[rb][pr][q] = base[((size_t)(2 * pr) * MY + y) * LDZ + cl];
-              B[rb][pr][q] = base[((size_t)(2 * pr + 1) * MY + y) * LDZ + cl];
-            }
-          }
-      }
 #pragma unroll
       for (int rb = 0; rb < 2; ++rb) {
         if (rb == 1 && !hasb) {
@@ -463,10 +532,23 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
           for (int r = 0; r < PZ; ++r) nrm[1][0][r] = nrm[1][1][r] = nrm[1][2][r] = T(0);
           break;
         }
+        const int y = rank * MH + ya + rb;
         cpx<T> ph[3][PZ];
 #pragma unroll
         for (int pr = 0; pr < 3; ++pr) {
-          build_packed<PZ, QK, T>(A[rb][pr], B[rb][pr], Kz, lane, ph[pr]);
+          cpx<T> A[QK], B[QK];
+#pragma unroll
+          for (int q = 0; q < QK; ++q) {
+            const int kz = 32 * q + lane;
+            A[q] = B[q] = cmk(T(0), T(0));
+            if (kz < Kz) {
+              const int own = kz >= KH, cl = kz - own * KH;
+              const cpx<T>* base = (own == rank) ? Ys : Ypeer;
+              A[q] = base[((size_t)(2 * pr) * MY + y) * LDZ + cl];
+              B[q] = base[((size_t)(2 * pr + 1) * MY + y) * LDZ + cl];
+            }
+          }
+          build_packed<PZ, QK, T>(A, B, Kz, lane, ph[pr]);
           warp_fft_inverse<PZ, T>(ph[pr], w, lane);
         }
 #pragma unroll
@@ -521,33 +603,20 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPlaneThreads, 1)
     WarpTw<PY, T> w;
     load_warp_tw<PY, T>(w, twy, lane);
     const T scale = T(1.0 / MY);
-    // every column of this warp (at most three: 3 KH <= 48 columns over 16
-    // warps) is read before the first transform, so that the peer-CTA reads
-    // of all of them are in flight together
-    constexpr int TW = (3 * 16 + NW - 1) / NW;
-    cpx<T> v[TW][PY];
-#pragma unroll
-    for (int i = 0; i < TW; ++i) {
-      const int t = warp + i * NW;
-      if (t >= 3 * KH) break;
+    for (int t = warp; t < 3 * KH; t += NW) {
       const int f = t / KH, cl = t % KH, kz = rank * KH + cl;
+      cpx<T> v[PY];
 #pragma unroll
       for (int n1 = 0; n1 < PY; ++n1) {
         const int y = n1 + PY * br;
         const int own = y / MH, yl = y - own * MH;
         const cpx<T>* base = (own == rank) ? Hs : Hpeer;
-        v[i][n1] = base[((size_t)f * MH + yl) * Kz + (swz ? (kz ^ (yl & 7)) : kz)];
+        v[n1] = base[((size_t)f * MH + yl) * Kz + (swz ? (kz ^ (yl & 7)) : kz)];
       }
-    }
-#pragma unroll
-    for (int i = 0; i < TW; ++i) {
-      const int t = warp + i * NW;
-      if (t >= 3 * KH) break;
-      const int f = t / KH, cl = t % KH;
-      warp_fft_forward<PY, T>(v[i], w, lane);
+      warp_fft_forward<PY, T>(v, w, lane);
       cpx<T>* col = Ys + (size_t)f * MY * LDZ + cl;
 #pragma unroll
-      for (int k1 = 0; k1 < PY; ++k1) col[(size_t)(32 * k1 + lane) * LDZ] = scale * v[i][k1];
+      for (int k1 = 0; k1 < PY; ++k1) col[(size_t)(32 * k1 + lane) * LDZ] = scale * v[k1];
     }
     __syncthreads();
     JFB_STAMP(1, 5);

@@ -36,7 +36,10 @@ class MHDState:
 class PlaneCouetteMHD(PlaneCouetteFluctuation):
     """Plane Couette MHD with A as the evolved magnetic unknown
     (pcf_mhd_jax.py:69-790).  GPU path: SBDF3 with IMEXRK3 startup,
-    rotational nonlinear form, Chebyshev family, FP64."""
+    rotational nonlinear form, Chebyshev family; ``precision`` "fp64", or
+    "mixed" (complex64 periodic transforms and products of u, omega, b, j
+    with the flow's base-flow terms added in FP64; FP64 operators, solves and
+    state)."""
 
     DIAGNOSTIC_NAMES = PlaneCouetteFluctuation.DIAGNOSTIC_NAMES + ("divB_L2", "Emag")
 
@@ -56,6 +59,7 @@ class PlaneCouetteMHD(PlaneCouetteFluctuation):
         nonlinear_form: str = "rotational",
         coefficient_path: str = "transform",
         solve_batching: str = "batched",
+        precision: str = "fp64",
         device="cuda",
     ) -> None:
         self.Rm = float(Re if Rm is None else Rm)
@@ -74,7 +78,7 @@ class PlaneCouetteMHD(PlaneCouetteFluctuation):
             nonlinear_form=nonlinear_form,
             coefficient_path=coefficient_path,
             solve_batching=solve_batching,
-            precision="fp64",
+            precision=precision,
             device=device,
         )
 
@@ -251,6 +255,7 @@ class PlaneCouetteMRIShearpy(PlaneCouetteMHD):
         nonlinear_form: str = "rotational",
         coefficient_path: str = "transform",
         solve_batching: str = "batched",
+        precision: str = "fp64",
         device="cuda",
     ) -> None:
         from .kmm import KMM
@@ -271,7 +276,7 @@ class PlaneCouetteMRIShearpy(PlaneCouetteMHD):
             self, N=N, domain=domain, nu=1.0 / self.Re, dt=dt, family=family,
             padding_factor=padding_factor, time_integrator=time_integrator,
             nonlinear_form=nonlinear_form, coefficient_path=coefficient_path,
-            solve_batching=solve_batching, precision="fp64", device=device,
+            solve_batching=solve_batching, precision=precision, device=device,
             _u_wall=-self.shear_rate,
         )
         self.dUb_dx = -self.shear_rate

@@ -80,13 +80,13 @@ def test_mhd_argument_errors_are_reported_without_a_gpu():
     lib = _lib.load()
     cfg = _lib.KMMConfig()
     cfg.nx, cfg.ny, cfg.nz = 17, 16, 16
-    cfg.precision = _lib.JFB_PRECISION_MIXED
+    cfg.nonlinear_form = _lib.JFB_NONLINEAR_GRADIENT
     h = ctypes.c_void_p()
     prm = _lib.MHDParams()
     prm.eta = 1.0 / 400.0
     assert lib.jfb_mhd_create(ctypes.byref(cfg), ctypes.byref(prm), ctypes.byref(h)) == _lib.JFB_ERR_ARG
-    assert b"FP64" in lib.jfb_last_error()
-    cfg.precision = _lib.JFB_PRECISION_FP64
+    assert b"rotational" in lib.jfb_last_error()
+    cfg.nonlinear_form = _lib.JFB_NONLINEAR_ROTATIONAL
     prm.eta = -1.0
     assert lib.jfb_mhd_create(ctypes.byref(cfg), ctypes.byref(prm), ctypes.byref(h)) == _lib.JFB_ERR_ARG
     assert b"eta" in lib.jfb_last_error()

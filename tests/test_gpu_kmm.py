@@ -331,3 +331,38 @@ def test_one_step_integrators_match_oracle(cuda, integrator, N, precision):
         assert rel(a, b) < tol
     assert gs.history_steps == 0.0
     assert all(float(t.abs().max()) == 0.0 for t in gs.nonlinear_old)
+
+
+def test_set_state_keeps_the_nonnegative_kz_half_of_a_full_complex_state(cuda):
+    """Boundary semantics of the half-spectrum storage: a full complex state
+    that is not the spectrum of a real field (the reference keeps such states
+    as given) is loaded as its kz >= 0 columns; reading it back gives those
+    columns unchanged (the Nyquist row ky = -Ny/2 zero, as the reference
+    masks it), the kz < 0 columns as the conjugate mirror c(-ky, -kz) =
+    conj(c(ky, kz)) and the Nyquist column kz = -Nz/2 zero."""
+    g = PlaneCouetteFluctuation(N=(17, 16, 16), Re=400.0, dt=1e-3, device=cuda,
+                                time_integrator="SBDF3", nonlinear_form="rotational")
+    rng = np.random.default_rng(7)
+
+    def noise(shape):
+        return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+    Nx, Ny, Nz = g.N
+    u = (noise((Nx - 4, Ny, Nz)), noise((Nx - 2, Ny, Nz)), noise((Nx - 2, Ny, Nz)))
+    gg = noise((Nx - 2, Ny, Nz))
+    st = KMMState(u=tuple(torch.from_numpy(a).to(cuda) for a in u),
+                  g=torch.from_numpy(gg).to(cuda))
+    out = g.solve(st, 0)
+
+    def expected(a):
+        e = np.zeros_like(a)
+        Kz = Nz // 2
+        e[:, :, :Kz] = a[:, :, :Kz]
+        e[:, Ny // 2, :Kz] = 0.0
+        for kz in range(Kz + 1, Nz):
+            for ky in range(Ny):
+                e[:, ky, kz] = np.conj(e[:, (Ny - ky) % Ny, Nz - kz])
+        return e
+
+    assert np.array_equal(out.u[0].cpu().numpy(), expected(u[0]))
+    assert np.array_equal(out.g.cpu().numpy(), expected(gg))

@@ -201,6 +201,28 @@ def test_rotating_shear_variant_matches_oracle(cuda):
         assert abs(dg[k] - do[k]) <= 1e-12 * max(1.0, abs(do[k])), k
 
 
+@pytest.mark.parametrize("precision, tol", [("fp64", 1e-12), ("mixed", 5e-6)])
+def test_rotating_shear_convection_matches_oracle(cuda, precision, tol):
+    """H and HA of a rotating-shear state with an imposed field (the EMF's
+    U_b e_y x B0 term reaches only the mean mode, which the A stage adds in
+    FP64)."""
+    from jaxfun_b200.mhd import PlaneCouetteMRIShearpy
+    from oracle.kmm import PlaneCouetteMRIOracle
+
+    kw = dict(N=(17, 16, 16), Re=400.0, Rm=250.0, omega=0.5, shear_rate=1.5,
+              background_b=(0.01, 0.02, 0.1), dt=1e-3, magnetic_amplitude=0.2)
+    o = PlaneCouetteMRIOracle(**kw)
+    g = PlaneCouetteMRIShearpy(device=cuda, precision=precision, **kw)
+    st = o.solve(o.initial_state(), 2)
+    H, HA = g.convection(to_dev(st, cuda))
+    Ho, HAo = o.mhd_convection(st)
+    for a, b in zip(H, Ho, strict=True):
+        assert rel(a, b) < tol
+    sc = max(np.linalg.norm(h) for h in HAo)
+    for a, b in zip(HA, HAo, strict=True):
+        assert rel(a, b, floor=sc) < tol
+
+
 def test_ensemble_of_uneven_members_equals_separate_runs(cuda):
     """Members of uneven wall-normal size (and a flow-only member) advanced
     as one graph per step give bitwise the results of separate runs."""
@@ -225,6 +247,66 @@ def test_ensemble_of_uneven_members_equals_separate_runs(cuda):
         else:
             la, lb = (*a.u, a.g), (*b.u, b.g)
         for x, y in zip(la, lb, strict=True):
+            assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize("N", [(17, 16, 16), (33, 32, 32), (65, 64, 64)])
+def test_mixed_form_tracks_the_oracle(cuda, N):
+    """Mixed MHD form: complex64 periodic transforms and products of u,
+    omega, b, j (the flow's base-flow terms added in FP64 by the pencil
+    stage), FP64 operators, solves and state.  Against the FP64 oracle after
+    two startup and six steady steps: every field within 5e-8 relative L2
+    (measured <= 1.1e-8)."""
+    kw = dict(N=N, Re=400.0, dt=1e-3, perturbation_amplitude=0.05, magnetic_amplitude=0.2)
+    o = PlaneCouetteMHDOracle(**kw)
+    g = PlaneCouetteMHD(device=cuda, precision="mixed", **kw)
+    st = o.initial_state()
+    gs = g.solve(to_dev(st, cuda), 8)
+    st = o.solve(st, 8)
+    for a, b in zip((*gs.flow.u, gs.flow.g), (*st.flow.u, st.flow.g), strict=True):
+        assert rel(a, b) < 5e-8
+    sc = a_scale(st.A)
+    for a, b in zip(gs.A, st.A, strict=True):
+        assert rel(a, b, floor=sc) < 5e-8
+
+
+def test_mixed_rotating_shear_variant_tracks_the_oracle(cuda):
+    """The rotating-shear variant (imposed B0, Coriolis, eta != nu) in the
+    mixed form: within 2e-8 of the oracle after six steps (measured 5e-9)."""
+    from jaxfun_b200.mhd import PlaneCouetteMRIShearpy
+    from oracle.kmm import PlaneCouetteMRIOracle
+
+    kw = dict(N=(33, 32, 32), Re=400.0, Rm=250.0, omega=0.5, shear_rate=1.5,
+              background_b=(0.01, 0.02, 0.1), dt=1e-3, magnetic_amplitude=0.2)
+    o = PlaneCouetteMRIOracle(**kw)
+    g = PlaneCouetteMRIShearpy(device=cuda, precision="mixed", **kw)
+    st = o.initial_state()
+    gs = g.solve(to_dev(st, cuda), 6)
+    st = o.solve(st, 6)
+    for a, b in zip((*gs.flow.u, gs.flow.g), (*st.flow.u, st.flow.g), strict=True):
+        assert rel(a, b) < 2e-8
+    sc = a_scale(st.A)
+    for a, b in zip(gs.A, st.A, strict=True):
+        assert rel(a, b, floor=sc) < 2e-8
+
+
+def test_mixed_batched_ensemble_equals_separate_runs(cuda):
+    """Mixed-form members of uneven wall-normal size: the batched stages
+    (complex64 transform stages) give each member bitwise its own plan's
+    result."""
+    from jaxfun_b200.mhd import Ensemble
+
+    def members():
+        return [PlaneCouetteMHD(N=(n, 64, 64), dt=1e-3, magnetic_amplitude=0.1,
+                                precision="mixed", device=cuda) for n in (33, 17, 25, 33)]
+
+    ref = [m.solve(m.initial_state(), 7) for m in members()]
+    ms = members()
+    ens = Ensemble(ms)
+    assert ens.batched and ens.launches_per_step == 15
+    out = ens.solve([m.initial_state() for m in ms], 7)
+    for a, b in zip(out, ref, strict=True):
+        for x, y in zip((*a.flow.u, a.flow.g, *a.A), (*b.flow.u, b.flow.g, *b.A), strict=True):
             assert torch.equal(x, y)
 
 

@@ -76,3 +76,26 @@ def test_noalloc_rejects_batches_beyond_its_fixed_capacity(cuda):
                                           stream_of(band))
     assert st == _lib.JFB_ERR_ARG
     assert b"JFB_NOALLOC_LU_MAX_BATCH" in lib.jfb_last_error()
+
+
+def test_noalloc_call_leaves_device_memory_unchanged(cuda):
+    """The entry point's defining property: after a first call (which may
+    load the library's kernels and with them the fixed status array), further
+    calls take no device memory; the free memory the driver reports is the
+    same before and after them."""
+    lib = _lib.load()
+    p, q, n = 4, 12, 41
+    bands = [random_bands(seed, p=p, q=q, n=n, device=cuda) for seed in (4, 5, 6)]
+    first = ctypes.c_int32(-7)
+    st = lib.jfb_banded_lu_factor_noalloc(bands[0].data_ptr(), bands[0].shape[0], p, q, n,
+                                          ctypes.byref(first), stream_of(bands[0]))
+    assert st == _lib.JFB_OK
+    torch.cuda.synchronize(cuda)
+    free0, _ = torch.cuda.mem_get_info(cuda)
+    for b in bands[1:]:
+        st = lib.jfb_banded_lu_factor_noalloc(b.data_ptr(), b.shape[0], p, q, n,
+                                              ctypes.byref(first), stream_of(b))
+        assert st == _lib.JFB_OK and first.value == -1
+    torch.cuda.synchronize(cuda)
+    free1, _ = torch.cuda.mem_get_info(cuda)
+    assert free1 == free0
