@@ -821,7 +821,8 @@ def main(argv=None):
             out[integ] = {"ms_per_step": e0_.elapsed_time(e1_) / K,
                           "implicit_stages_per_step": stages}
             del sv, st
-        out["form"] = "gradient, FP64 (warp-per-pencil stage, split periodic transforms)"
+        out["form"] = ("gradient, FP64 (tensor-core pencil stage where the tiling fits, split "
+                       "periodic transforms with the warp-shuffle gradient z stage)")
         return out
 
     def sizes_block():

@@ -692,7 +692,7 @@ static void launch_zfwd_warp(jfb_kmm_plan* pl, const double* u0, const double* u
 template <int PY, int PZ, typename T>
 static cudaError_t launch_plane(jfb_kmm_plan* pl, cudaStream_t s) {
   return launch_ex(pl->pdl, plane_cross_kernel<PY, PZ, 1, T>, dim3(2 * pl->d.Nx),
-                   dim3(kPlaneThreads), plane_smem_bytes(pl->d.My, pl->d.Kz, sizeof(cpx<T>)),
+                   dim3(plane_threads<T>()), plane_smem_bytes(pl->d.My, pl->d.Kz, sizeof(cpx<T>)),
                    s, pl->ops, tdims<T>(pl), Tx<T>::twy(pl), Tx<T>::twz(pl),
                    (const cpx<T>*)buf<T>(pl->X), buf<T>(pl->HX));
 }
@@ -3166,8 +3166,12 @@ extern "C" int jfb_ensemble_create(jfb_kmm_plan* const* plans, int32_t n, jfb_en
     for (int i = 0; i < n; ++i) idx[i] = i;
     std::stable_sort(idx.begin(), idx.end(),
                      [&](int a, int b) { return e->m[a]->d.Nx > e->m[b]->d.Nx; });
+    // JFB200_ENSEMBLE_GROUP=k: at most k members per group (more groups on
+    // parallel branches, so that stages of different kinds overlap)
+    const char* genv = std::getenv("JFB200_ENSEMBLE_GROUP");
+    const int gmax = genv ? std::max(1, std::atoi(genv)) : n;
     for (int i : idx) {
-      if (e->groups.empty() ||
+      if (e->groups.empty() || (int)e->groups.back().order.size() >= gmax ||
           (!single && e->m[e->groups.back().order.back()]->d.Nx != e->m[i]->d.Nx))
         e->groups.emplace_back();
       e->groups.back().order.push_back(i);
