@@ -427,13 +427,16 @@ __global__ void __launch_bounds__(256) z_forward_real_warp_kernel(
 #ifndef JFB_PLANE_THREADS_F64
 #define JFB_PLANE_THREADS_F64 384
 #endif
-// threads per CTA of the plane kernel: sixteen warps in FP32; twelve in
-// FP64, whose complex128 z stage wants more registers per thread (measured at
-// 65x64x64: 53.6 us per CTA against 58.5 us with sixteen warps, 54.6 us with
-// eight)
+// threads per CTA of the plane kernel: twelve warps, whose registers (up to
+// 168 per thread) suit the z stage better than sixteen warps at 128 (measured
+// at 65x64x64, per CTA: FP64 53.6 us against 58.5 us with sixteen warps and
+// 54.6 us with eight; FP32 26.4 us against 27.5 us with sixteen)
+#ifndef JFB_PLANE_THREADS_F32
+#define JFB_PLANE_THREADS_F32 384
+#endif
 template <typename T>
 __host__ __device__ constexpr int plane_threads() {
-  return sizeof(T) == 8 ? JFB_PLANE_THREADS_F64 : 512;
+  return sizeof(T) == 8 ? JFB_PLANE_THREADS_F64 : JFB_PLANE_THREADS_F32;
 }
 
 __host__ __device__ inline size_t plane_smem_bytes(int My, int Kz, size_t elem) {
