@@ -801,13 +801,15 @@ def main(argv=None):
     def default_form_block():
         """The reference's production default on the same workload: the
         gradient nonlinear form u . grad u (FP64) with each time integrator
-        the production runner accepts; ms per step (graph replay, CUDA events,
-        L2 not flushed) and the kernels per step."""
+        the production runner accepts, and its mixed form with SBDF3; ms per
+        step (graph replay, CUDA events, L2 not flushed)."""
         out = {}
         f0 = couette_perturbation_fields(grid, domain())
-        for integ in ("SBDF3", "CNAB2", "IMEXRK222", "IMEXRK3"):
+        for integ, prec in (("SBDF3", "fp64"), ("CNAB2", "fp64"), ("IMEXRK222", "fp64"),
+                            ("IMEXRK3", "fp64"), ("SBDF3", "mixed")):
             sv = PlaneCouetteFluctuation(N=grid, domain=domain(), Re=RE, dt=DT, device=dev,
-                                         time_integrator=integ, nonlinear_form="gradient")
+                                         time_integrator=integ, nonlinear_form="gradient",
+                                         precision=prec)
             e0 = sv.diagnostics(sv.state_from_physical(f0))["Epert"]
             st = sv.solve(sv.state_from_physical(scale_to_energy(f0, e0, ENERGY)), 5)
             torch.cuda.synchronize(dev)
@@ -818,11 +820,12 @@ def main(argv=None):
             e1_.record(stream)
             torch.cuda.synchronize(dev)
             stages = {"SBDF3": 1, "CNAB2": 1, "IMEXRK222": 2, "IMEXRK3": 3}[integ]
-            out[integ] = {"ms_per_step": e0_.elapsed_time(e1_) / K,
-                          "implicit_stages_per_step": stages}
+            out[integ if prec == "fp64" else f"{integ}_mixed"] = {
+                "ms_per_step": e0_.elapsed_time(e1_) / K, "implicit_stages_per_step": stages}
             del sv, st
-        out["form"] = ("gradient, FP64 (tensor-core pencil stage where the tiling fits, split "
-                       "periodic transforms with the warp-shuffle gradient z stage)")
+        out["form"] = ("gradient, FP64 (and SBDF3_mixed: complex64 transforms; tensor-core "
+                       "pencil stage where the tiling fits, split periodic transforms with the "
+                       "warp-shuffle gradient z stage)")
         return out
 
     def sizes_block():

@@ -114,8 +114,8 @@ int jfb_wavenumber_solve(const double* L, const int64_t* L_offsets, int64_t n_L,
 /* Constructor arguments of KMM / PlaneCouetteFluctuationJax
  * (examples/channelflow_kmm.py:107-230, examples/pcf_fluctuations_jax.py:35-75)
  * restricted to the hot path: Chebyshev or Legendre family, x unpadded, the
- * rotational or gradient nonlinear form (gradient: FP64 precision), the time
- * integrators above (MHD plans and the adjoint: SBDF3, Chebyshev, rotational).
+ * rotational or gradient nonlinear form, the time integrators above (MHD
+ * plans: SBDF3, Chebyshev, rotational; the adjoint: also FP64).
  * u_wall = 0 gives the plain KMM channel (no base flow). */
 typedef struct jfb_kmm_config {
   int32_t nx, ny, nz;     /* N = (wall-normal orthogonal size, Fourier y, z) */

@@ -712,8 +712,10 @@ static int launch_transforms_t(jfb_kmm_plan* pl, cudaStream_t s) {
     return JFB_OK;
   }
   if (d.grad) {
-    // gradient form (FP64): u_i, d/dx u_i, d/dy u_i backward in y, the
-    // twelve-field z stage, n_i forward in y (no constant base-flow term)
+    // gradient form: u_i, d/dx u_i, d/dy u_i backward in y, the
+    // twelve-field z stage, n_i forward in y (no constant base-flow term;
+    // complex64 in the mixed form, whose base-flow terms the pencil stage
+    // adds in FP64)
     if (pl->py) {
       launch_y_warp_any<T>(pl, s, true, 9);
     } else {
@@ -728,7 +730,8 @@ static int launch_transforms_t(jfb_kmm_plan* pl, cudaStream_t s) {
       switch (pl->pz * 10 + pl->qk) {
 #define JFB_ZG(P, Q)                                                                     \
   case P * 10 + Q:                                                                       \
-    z_grad_warp_kernel<P, Q><<<blocks, 256, 0, s>>>(pl->ops, pl->d, pl->twz, pl->Y, pl->HZ); \
+    z_grad_warp_kernel<P, Q, T><<<blocks, 256, 0, s>>>(pl->ops, d, Tx<T>::twz(pl),              \
+                                                        buf<T>(pl->Y), buf<T>(pl->HZ));         \
     break;
         JFB_ZG(2, 1) JFB_ZG(2, 2) JFB_ZG(3, 1) JFB_ZG(3, 2)
         JFB_ZG(4, 1) JFB_ZG(4, 2) JFB_ZG(6, 1) JFB_ZG(6, 2)
@@ -737,7 +740,8 @@ static int launch_transforms_t(jfb_kmm_plan* pl, cudaStream_t s) {
       }
     } else {
       const int zb = ceil_div((int64_t)d.Nx * d.My, kZRows);
-      z_grad_kernel<<<zb, 256, pl->smem_zg, s>>>(pl->ops, pl->d, pl->fz, pl->twz, pl->Y, pl->HZ);
+      z_grad_kernel<T><<<zb, 256, pl->smem_zg / sizeof(c64) * sizeof(cpx<T>), s>>>(
+          pl->ops, d, pl->fz, Tx<T>::twz(pl), buf<T>(pl->Y), buf<T>(pl->HZ));
     }
     JFB_CHECK_LAUNCH();
     if (pl->timing_events) JFB_CHECK_CUDA(cudaEventRecord(pl->timing_events[3], s));
@@ -1177,9 +1181,6 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   JFB_REQUIRE(cfg->nonlinear_form == JFB_NONLINEAR_ROTATIONAL ||
                   cfg->nonlinear_form == JFB_NONLINEAR_GRADIENT,
               "nonlinear_form must be JFB_NONLINEAR_ROTATIONAL or JFB_NONLINEAR_GRADIENT");
-  JFB_REQUIRE(cfg->nonlinear_form == JFB_NONLINEAR_ROTATIONAL ||
-                  cfg->precision == JFB_PRECISION_FP64,
-              "the gradient nonlinear form runs in FP64 precision");
   JFB_REQUIRE(!mhd || (cfg->family == JFB_FAMILY_CHEBYSHEV &&
                        cfg->nonlinear_form == JFB_NONLINEAR_ROTATIONAL),
               "the MHD step is Chebyshev / rotational only");
@@ -1269,7 +1270,9 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
   // gradient form: nine fields backward in y (u_i, d/dx u_i, d/dy u_i), the
   // twelve-field z stage z_grad_kernel (shared-memory transforms)
   pl->smem_zg = (size_t)2 * d.Mz * kZRows * 6 * sizeof(c64);
-  if (d.grad && (pl->smem_zg > 227 * 1024 || allow_smem((const void*)z_grad_kernel) != cudaSuccess)) {
+  if (d.grad && (pl->smem_zg > 227 * 1024 ||
+                 allow_smem((const void*)z_grad_kernel<double>) != cudaSuccess ||
+                 allow_smem((const void*)z_grad_kernel<float>) != cudaSuccess)) {
     set_error("grid too large for the gradient-form z stage");
     return fail(JFB_ERR_ARG);
   }

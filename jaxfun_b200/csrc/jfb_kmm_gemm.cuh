@@ -132,6 +132,17 @@ __device__ __forceinline__ void add_base_flow_terms(const c32 (&x)[4], bool mean
   if (mean) h[0].re -= ub * uw;
 }
 
+// Gradient form (pcf_fluctuations_jax.py:99-106): U_b d/dy u_i and
+// u_0 dU_b/dx e_y at one x node, from x = (u0, d/dy u0, d/dy u1, d/dy u2)
+// (X fields 0, 6, 7, 8).
+__device__ __forceinline__ void add_base_convection_terms(const c32 (&x)[4], double ub, double uw,
+                                                          c64 (&h)[3]) {
+  auto c = [&](int k) { return cmk((double)x[k].re, (double)x[k].im); };
+  h[0] = h[0] + ub * c(1);
+  h[1] = (h[1] + ub * c(2)) + uw * c(0);
+  h[2] = h[2] + ub * c(3);
+}
+
 __host__ __device__ inline int round4(int x) { return (x + 3) & ~3; }
 
 // Read-only (non-coherent) load of one complex value.
@@ -540,7 +551,9 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
   // (row i -> i / 2), likewise g.  Column = pencil (8 +ky then 8 -ky).
   const bool has_b = (a.c1 != 0.0), has_c = (a.c2 != 0.0);
   const int sides = (kyi == 0) ? 1 : 2;
-  c32 xl[2][2][4];  // mixed form: (u0, u1, omega0, omega2) at rows j, N-1-j of two items
+  // mixed form: (u0, u1, omega0, omega2), gradient form (u0, d/dy u0..2), at
+  // rows j, N-1-j of two items
+  c32 xl[2][2][4];
   {
     const int lv = 1 + has_b + has_c;
     const int nrow = 3 * N + (d.nB + d.nD) * lv;
@@ -592,7 +605,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
         const int j = idx / kGW, w = idx % kGW, p = s_p[w];
         if (p < 0) continue;
         const int rows[2] = {j, N - 1 - j};
-        const int fs[4] = {0, 1, 3, 5};
+        const int fs[4] = {0, d.grad ? 6 : 1, d.grad ? 7 : 3, d.grad ? 8 : 5};
 #pragma unroll
         for (int s2 = 0; s2 < 2; ++s2)
 #pragma unroll
@@ -634,8 +647,13 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
     }
     if (a.Xlin && ok) {
       const bool mean = s_p[w] == 0;
-      add_base_flow_terms(xl[it][0], mean, d.uwall * o.xphys[j], d.uwall, h[0]);
-      if (jm != j) add_base_flow_terms(xl[it][1], mean, d.uwall * o.xphys[jm], d.uwall, h[1]);
+      if (d.grad) {
+        add_base_convection_terms(xl[it][0], d.uwall * o.xphys[j], d.uwall, h[0]);
+        if (jm != j) add_base_convection_terms(xl[it][1], d.uwall * o.xphys[jm], d.uwall, h[1]);
+      } else {
+        add_base_flow_terms(xl[it][0], mean, d.uwall * o.xphys[j], d.uwall, h[0]);
+        if (jm != j) add_base_flow_terms(xl[it][1], mean, d.uwall * o.xphys[jm], d.uwall, h[1]);
+      }
     }
     if (mean_cta && w == 0) {
       mean[j] = h[0][1].re;

@@ -761,7 +761,11 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
             const c32 x = a.Xlin[((size_t)g * d.Nx + j) * P + p0 + w];
             return cmk((double)x.re, (double)x.im);
           };
-          if (f == 0) {
+          if (d.grad) {  // U_b d/dy u_i (+ u_0 dU_b/dx e_y), pcf_fluctuations_jax.py:99-106
+            if (f == 0) v = v + ub * ld(6);
+            else if (f == 1) v = (v + ub * ld(7)) + uw * ld(0);
+            else v = v + ub * ld(8);
+          } else if (f == 0) {
             v = v - uw * ld(1) - ub * ld(5);
             if (p0 + w == 0) v.re -= ub * uw;
           } else if (f == 1) {
@@ -1222,67 +1226,70 @@ __global__ void __launch_bounds__(256) z_cross_kernel(DevOps o, Dims d, FFTPlan 
 // inverse transform, give
 //   n_i = u_0 d/dx u_i + u_1 d/dy u_i + u_2 d/dz u_i + U_b d/dy u_i
 //         (+ u_0 dU_b/dx for i = 1),
-// forward transformed two per complex transform (n2 alone).
+// forward transformed two per complex transform (n2 alone).  In complex64
+// (the mixed form) d.uwall = 0: the base-flow terms, linear in the
+// perturbation, are added in FP64 by the pencil stage.
 // ---------------------------------------------------------------------------
+template <typename T>
 __global__ void __launch_bounds__(256) z_grad_kernel(DevOps o, Dims d, FFTPlan plan,
-                                                     const c64* __restrict__ tw,
-                                                     const c64* __restrict__ Y,
-                                                     c64* __restrict__ HZ) {
+                                                     const cpx<T>* __restrict__ tw,
+                                                     const cpx<T>* __restrict__ Y,
+                                                     cpx<T>* __restrict__ HZ) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int NC = kZRows * 6;   // packed input columns
   constexpr int NCf = kZRows * 2;  // packed output columns: (n0 + i n1), (n2 + i 0)
-  c64* A = reinterpret_cast<c64*>(smem_raw);
-  c64* B = A + d.Mz * NC;
+  cpx<T>* A = reinterpret_cast<cpx<T>*>(smem_raw);
+  cpx<T>* B = A + d.Mz * NC;
   const int row0 = blockIdx.x * kZRows;  // row = j * My + y
   const int nrows = d.Nx * d.My;
   const size_t plane = (size_t)d.Nx * d.My * d.Kz;
   // virtual real field v: v < 9 is Y field v, v >= 9 is i kz (Y field v - 9)
-  auto spec = [&](int v, int row, int k) -> c64 {
-    const c64 x = Y[(size_t)(v < 9 ? v : v - 9) * plane + (size_t)row * d.Kz + k];
-    return v < 9 ? x : mul_i((k * d.dfz) * x);
+  auto spec = [&](int v, int row, int k) -> cpx<T> {
+    const cpx<T> x = Y[(size_t)(v < 9 ? v : v - 9) * plane + (size_t)row * d.Kz + k];
+    return v < 9 ? x : mul_i(T(k * d.dfz) * x);
   };
   for (int idx = threadIdx.x; idx < d.Mz * NC; idx += blockDim.x) {
     const int k = idx % d.Mz, c = idx / d.Mz;
     const int rl = c / 6, pr = c % 6;
     const int row = row0 + rl;
-    c64 z = cmk(0.0, 0.0);
+    cpx<T> z = cmk(T(0), T(0));
     if (row < nrows) {
       if (k == 0) {
         z = cmk(spec(2 * pr, row, 0).re, spec(2 * pr + 1, row, 0).re);
       } else if (k < d.Kz) {
-        const c64 xa = spec(2 * pr, row, k), xb = spec(2 * pr + 1, row, k);
+        const cpx<T> xa = spec(2 * pr, row, k), xb = spec(2 * pr + 1, row, k);
         z = cmk(xa.re - xb.im, xa.im + xb.re);
       } else if (k > d.Mz - d.Kz) {
         const int kk = d.Mz - k;
-        const c64 xa = spec(2 * pr, row, kk), xb = spec(2 * pr + 1, row, kk);
+        const cpx<T> xa = spec(2 * pr, row, kk), xb = spec(2 * pr + 1, row, kk);
         z = cmk(xa.re + xb.im, -xa.im + xb.re);  // conj(xa) + i conj(xb)
       }
     }
     A[k * NC + c] = z;
   }
   __syncthreads();
-  c64* phys = fft_columns<double>(A, B, plan, NC, NC, tw, +1);
-  c64* other = (phys == A) ? B : A;
+  cpx<T>* phys = fft_columns<T>(A, B, plan, NC, NC, tw, +1);
+  cpx<T>* other = (phys == A) ? B : A;
   for (int idx = threadIdx.x; idx < d.Mz * kZRows; idx += blockDim.x) {
     const int rl = idx % kZRows, n = idx / kZRows;
     const int row = row0 + rl;
     const int j = (row < nrows) ? row / d.My : 0;
-    const c64* z = phys + n * NC + rl * 6;
-    const double u0 = z[0].re, u1 = z[0].im, u2 = z[1].re;
-    const double x0 = z[1].im, x1 = z[2].re, x2 = z[2].im;  // d/dx
-    const double y0 = z[3].re, y1 = z[3].im, y2 = z[4].re;  // d/dy
-    const double z0 = z[4].im, z1 = z[5].re, z2 = z[5].im;  // d/dz
-    const double ub = d.uwall * o.xphys[j];
-    const double n0 = (u0 * x0 + u1 * y0 + u2 * z0) + ub * y0;
-    const double n1 = ((u0 * x1 + u1 * y1 + u2 * z1) + ub * y1) + u0 * d.uwall;
-    const double n2 = (u0 * x2 + u1 * y2 + u2 * z2) + ub * y2;
-    c64* out = other + n * NCf + rl * 2;
+    const cpx<T>* z = phys + n * NC + rl * 6;
+    const T u0 = z[0].re, u1 = z[0].im, u2 = z[1].re;
+    const T x0 = z[1].im, x1 = z[2].re, x2 = z[2].im;  // d/dx
+    const T y0 = z[3].re, y1 = z[3].im, y2 = z[4].re;  // d/dy
+    const T z0 = z[4].im, z1 = z[5].re, z2 = z[5].im;  // d/dz
+    const T ub = T(d.uwall * o.xphys[j]), uw = T(d.uwall);
+    const T n0 = (u0 * x0 + u1 * y0 + u2 * z0) + ub * y0;
+    const T n1 = ((u0 * x1 + u1 * y1 + u2 * z1) + ub * y1) + u0 * uw;
+    const T n2 = (u0 * x2 + u1 * y2 + u2 * z2) + ub * y2;
+    cpx<T>* out = other + n * NCf + rl * 2;
     out[0] = cmk(n0, n1);
-    out[1] = cmk(n2, 0.0);
+    out[1] = cmk(n2, T(0));
   }
   __syncthreads();
-  c64* res = fft_columns<double>(other, phys, plan, NCf, NCf, tw, -1);
-  const double scale = 1.0 / d.Mz;
+  cpx<T>* res = fft_columns<T>(other, phys, plan, NCf, NCf, tw, -1);
+  const T scale = T(1.0 / d.Mz), h = T(0.5);
   for (int idx = threadIdx.x; idx < d.Kz * kZRows * 3; idx += blockDim.x) {
     const int k = idx % d.Kz;
     const int rf = idx / d.Kz;
@@ -1290,12 +1297,12 @@ __global__ void __launch_bounds__(256) z_grad_kernel(DevOps o, Dims d, FFTPlan p
     const int row = row0 + rl;
     if (row >= nrows) continue;
     const int col = rl * 2 + f / 2;
-    const c64 Zk = res[k * NCf + col];
-    const c64 Zm = res[((d.Mz - k) % d.Mz) * NCf + col];
+    const cpx<T> Zk = res[k * NCf + col];
+    const cpx<T> Zm = res[((d.Mz - k) % d.Mz) * NCf + col];
     // x + i y packed: X_k = (Z_k + conj Z_-k)/2, Y_k = (Z_k - conj Z_-k)/(2i)
-    c64 v;
-    if ((f & 1) == 0) v = cmk(0.5 * (Zk.re + Zm.re), 0.5 * (Zk.im - Zm.im));
-    else v = cmk(0.5 * (Zk.im + Zm.im), -0.5 * (Zk.re - Zm.re));
+    cpx<T> v;
+    if ((f & 1) == 0) v = cmk(h * (Zk.re + Zm.re), h * (Zk.im - Zm.im));
+    else v = cmk(h * (Zk.im + Zm.im), -h * (Zk.re - Zm.re));
     HZ[(size_t)f * plane + (size_t)row * d.Kz + k] = scale * v;
   }
 }

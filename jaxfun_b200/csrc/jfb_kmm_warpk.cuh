@@ -268,78 +268,78 @@ __global__ void __launch_bounds__(256) z_cross_warp_kernel(DevOps o, Dims d,
 
 // ---------------------------------------------------------------------------
 // z_grad: the gradient form's z stage (z_grad_kernel) with warp-shuffle
-// transforms, FP64, one warp per pair of (x, y) rows.  Per row, the twelve
+// transforms, one warp per pair of (x, y) rows.  Per row, the twelve
 // real fields u_i, d/dx u_i, d/dy u_i (Y fields 0..8) and d/dz u_i = i kz u_i
 // (formed here) go through six packed inverse transforms; the three products
 // n_i = u . grad u_i + U_b d/dy u_i (+ u_0 dU_b/dx for i = 1) of the row
 // pair go through three packed forward transforms.
 // ---------------------------------------------------------------------------
-template <int P, int QK>
+template <int P, int QK, typename T>
 __global__ void __launch_bounds__(256) z_grad_warp_kernel(DevOps o, Dims d,
-                                                          const c64* __restrict__ tw,
-                                                          const c64* __restrict__ Y,
-                                                          c64* __restrict__ HZ) {
+                                                          const cpx<T>* __restrict__ tw,
+                                                          const cpx<T>* __restrict__ Y,
+                                                          cpx<T>* __restrict__ HZ) {
   const int lane = threadIdx.x & 31;
   const int pair = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   const int nrows = d.Nx * d.My;
   const int rowa = 2 * pair;
   if (rowa >= nrows) return;
   const bool hasb = rowa + 1 < nrows;
-  WarpTw<P, double> w;
-  load_warp_tw<P, double>(w, tw, lane);
+  WarpTw<P, T> w;
+  load_warp_tw<P, T>(w, tw, lane);
   const size_t plane = (size_t)d.Nx * d.My * d.Kz;
-  double nrm[2][3][P];
+  T nrm[2][3][P];
 #pragma unroll
   for (int rb = 0; rb < 2; ++rb) {
     const int row = rowa + rb;
     const bool ok = rb == 0 || hasb;
     // virtual real field v of the row at spectral index k: Y field v (v < 9)
     // or i kz times Y field v - 9
-    auto spec = [&](int v, int k) -> c64 {
-      if (!ok || k >= d.Kz) return cmk(0.0, 0.0);
-      const c64 x = Y[(size_t)(v < 9 ? v : v - 9) * plane + (size_t)row * d.Kz + k];
-      return v < 9 ? x : mul_i((k * d.dfz) * x);
+    auto spec = [&](int v, int k) -> cpx<T> {
+      if (!ok || k >= d.Kz) return cmk(T(0), T(0));
+      const cpx<T> x = Y[(size_t)(v < 9 ? v : v - 9) * plane + (size_t)row * d.Kz + k];
+      return v < 9 ? x : mul_i(T(k * d.dfz) * x);
     };
-    c64 ph[6][P];
+    cpx<T> ph[6][P];
 #pragma unroll
     for (int pr = 0; pr < 6; ++pr) {
-      c64 A[QK], B[QK];
+      cpx<T> A[QK], B[QK];
 #pragma unroll
       for (int q = 0; q < QK; ++q) {
         A[q] = spec(2 * pr, 32 * q + lane);
         B[q] = spec(2 * pr + 1, 32 * q + lane);
       }
-      build_packed<P, QK, double>(A, B, d.Kz, lane, ph[pr]);
-      warp_fft_inverse<P, double>(ph[pr], w, lane);
+      build_packed<P, QK, T>(A, B, d.Kz, lane, ph[pr]);
+      warp_fft_inverse<P, T>(ph[pr], w, lane);
     }
     const int j = (ok ? row : rowa) / d.My;
-    const double ub = d.uwall * o.xphys[j];
+    const T ub = T(d.uwall * o.xphys[j]), uw = T(d.uwall);
 #pragma unroll
     for (int r = 0; r < P; ++r) {
-      const double u0 = ph[0][r].re, u1 = ph[0][r].im, u2 = ph[1][r].re;
-      const double x0 = ph[1][r].im, x1 = ph[2][r].re, x2 = ph[2][r].im;  // d/dx
-      const double y0 = ph[3][r].re, y1 = ph[3][r].im, y2 = ph[4][r].re;  // d/dy
-      const double z0 = ph[4][r].im, z1 = ph[5][r].re, z2 = ph[5][r].im;  // d/dz
+      const T u0 = ph[0][r].re, u1 = ph[0][r].im, u2 = ph[1][r].re;
+      const T x0 = ph[1][r].im, x1 = ph[2][r].re, x2 = ph[2][r].im;  // d/dx
+      const T y0 = ph[3][r].re, y1 = ph[3][r].im, y2 = ph[4][r].re;  // d/dy
+      const T z0 = ph[4][r].im, z1 = ph[5][r].re, z2 = ph[5][r].im;  // d/dz
       nrm[rb][0][r] = (u0 * x0 + u1 * y0 + u2 * z0) + ub * y0;
-      nrm[rb][1][r] = ((u0 * x1 + u1 * y1 + u2 * z1) + ub * y1) + u0 * d.uwall;
+      nrm[rb][1][r] = ((u0 * x1 + u1 * y1 + u2 * z1) + ub * y1) + u0 * uw;
       nrm[rb][2][r] = (u0 * x2 + u1 * y2 + u2 * z2) + ub * y2;
     }
   }
-  c64 F0[P], F1[P], F2[P];
+  cpx<T> F0[P], F1[P], F2[P];
 #pragma unroll
   for (int r = 0; r < P; ++r) {
     F0[r] = cmk(nrm[0][0][r], nrm[0][1][r]);
     F1[r] = cmk(nrm[1][0][r], nrm[1][1][r]);
     F2[r] = cmk(nrm[0][2][r], nrm[1][2][r]);
   }
-  warp_fft_forward<P, double>(F0, w, lane);
-  warp_fft_forward<P, double>(F1, w, lane);
-  warp_fft_forward<P, double>(F2, w, lane);
-  c64 xa0[QK], xa1[QK], xb0[QK], xb1[QK], x2a[QK], x2b[QK];
-  unpack_pair<P, QK, double>(F0, lane, xa0, xa1);
-  unpack_pair<P, QK, double>(F1, lane, xb0, xb1);
-  unpack_pair<P, QK, double>(F2, lane, x2a, x2b);
-  const double scale = 1.0 / (32 * P);
+  warp_fft_forward<P, T>(F0, w, lane);
+  warp_fft_forward<P, T>(F1, w, lane);
+  warp_fft_forward<P, T>(F2, w, lane);
+  cpx<T> xa0[QK], xa1[QK], xb0[QK], xb1[QK], x2a[QK], x2b[QK];
+  unpack_pair<P, QK, T>(F0, lane, xa0, xa1);
+  unpack_pair<P, QK, T>(F1, lane, xb0, xb1);
+  unpack_pair<P, QK, T>(F2, lane, x2a, x2b);
+  const T scale = T(1.0 / (32 * P));
 #pragma unroll
   for (int q = 0; q < QK; ++q) {
     const int k = 32 * q + lane;

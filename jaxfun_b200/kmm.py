@@ -56,8 +56,8 @@ class KMM:
     Same constructor defaults as the reference: gradient nonlinear form,
     ``time_integrator=None`` meaning IMEXRK222, the "transform" coefficient
     path.  Supported on the GPU path: Chebyshev or Legendre family,
-    wall-normal axis unpadded, the gradient form ``u . grad u`` (FP64
-    precision) or the rotational form ``-(u x omega)`` (FP64 or mixed); time
+    wall-normal axis unpadded, the gradient form ``u . grad u`` or the
+    rotational form ``-(u x omega)``, each in FP64 or mixed precision; time
     integrators SBDF3 (IMEXRK3 startup), IMEXRK3, IMEXRK222 (the one-step
     integrators keep no history: the state's history fields pass through
     unchanged, as in the reference's ``KMM.step``) and CNAB2 with the
@@ -112,16 +112,14 @@ class KMM:
         unsupported = []
         if time_integrator not in _GPU_STEPPERS:
             unsupported.append(f"time_integrator={time_integrator!r}")
-        if self.nonlinear_form == "gradient" and precision != "fp64":
-            unsupported.append(f"nonlinear_form='gradient' with precision={precision!r}")
         if self.padding_factor[0] != 1.0:
             unsupported.append("wall-normal padding")
         if float(dpdy) != 0.0:
             unsupported.append("dpdy != 0")
         if unsupported:
             raise NotImplementedError(
-                "the B200 step supports SBDF3, IMEXRK3 or IMEXRK222 / gradient (FP64) or "
-                "rotational / unpadded x only; requested " + ", ".join(unsupported)
+                "the B200 step supports SBDF3, IMEXRK3, IMEXRK222 or CNAB2 / unpadded x "
+                "only; requested " + ", ".join(unsupported)
             )
         self.time_integrator = time_integrator
         self.family = fam

@@ -13,7 +13,6 @@ from jaxfun_b200.kmm import KMM, PlaneCouetteFluctuation
 
 @pytest.mark.parametrize("kw", [
     {"dpdy": 0.1},
-    {"nonlinear_form": "gradient", "precision": "mixed"},
     {"padding_factor": (1.5, 1.5, 1.5)},
 ])
 def test_unsupported_options_are_rejected_before_any_device_work(kw):
@@ -103,3 +102,49 @@ def test_minimal_seed_ascent_rejects_bad_options():
             ms._check_ascent_options(**args)
     assert ms._check_ascent_options(4, 2, 0.5, 0.5, 1e-8) == (4, 2)
     assert list(ms._TrialSteps(1.0, 0.5, 0.2)) == [1.0, 0.5, 0.25]
+
+
+def test_checkpoint_payload_round_trip_keeps_every_history_level():
+    """The production runner's payload layout (production/oracles.py:
+    3872-3945, 327-420) for a flow state with SBDF3 / CNAB2 history and an
+    MHD state: the restored state has the same arrays and scalars."""
+    import torch
+
+    from jaxfun_b200.checkpoint import (FLOW_KIND, MHD_KIND, checkpoint_payload,
+                                        state_from_checkpoint_payload)
+    from jaxfun_b200.kmm import KMMState
+    from jaxfun_b200.mhd import MHDState
+
+    g = torch.Generator().manual_seed(3)
+
+    def arr(*shape):
+        return torch.randn(*shape, 2, generator=g, dtype=torch.float64).contiguous()
+
+    def lv():
+        return (arr(5, 4, 4), arr(7, 4, 4), arr(7), arr(7))
+
+    flow = KMMState(u=(arr(5, 4, 4), arr(7, 4, 4), arr(7, 4, 4)), g=arr(7, 4, 4),
+                    nonlinear_old=lv(), nonlinear_older=lv(), solution_old=lv(),
+                    solution_older=lv(), history_steps=2.0, have_old=1.0, previous_dt=0.01)
+    back = state_from_checkpoint_payload(checkpoint_payload(flow), state_kind=FLOW_KIND)
+    for name in ("u", "nonlinear_old", "nonlinear_older", "solution_old", "solution_older"):
+        for a, b in zip(getattr(flow, name), getattr(back, name), strict=True):
+            assert torch.equal(a, b)
+    assert torch.equal(flow.g, back.g)
+    assert (back.history_steps, back.have_old, back.previous_dt) == (2.0, 1.0, 0.01)
+
+    cnab = KMMState(u=flow.u, g=flow.g, nonlinear_old=lv(), have_old=1.0, previous_dt=0.01)
+    pl = checkpoint_payload(cnab)
+    assert "solution_old" not in pl and pl["have_old"] == 1.0
+    back = state_from_checkpoint_payload(pl, state_kind=FLOW_KIND)
+    assert back.solution_old is None and back.nonlinear_older is None
+
+    mhd = MHDState(flow=flow, A=(arr(7, 4, 4),) * 3, nonlinear_A_old=(arr(7, 4, 4),) * 3,
+                   A_old=(arr(7, 4, 4),) * 3)
+    pl = checkpoint_payload(mhd)
+    assert "flow_u" in pl and "flow_history_steps" in pl and "A_older" not in pl
+    back = state_from_checkpoint_payload(pl, state_kind=MHD_KIND)
+    assert torch.equal(back.A[0], mhd.A[0]) and back.A_older is None
+    assert torch.equal(back.flow.solution_older[1], flow.solution_older[1])
+    with pytest.raises(ValueError):
+        state_from_checkpoint_payload(pl, state_kind="axisymmetric_tc_hydro")
