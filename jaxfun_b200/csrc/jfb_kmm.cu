@@ -1507,7 +1507,8 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
                           oTA + kTcImgA <= oTB &&
                           oTB + kTcImgB <= (size_t)G.rows * kGLd * sizeof(double) &&
                           (size_t)10 * 32 * kTcStagePitch * sizeof(float) <= (size_t)kTcImgA;
-      if (pl->mixed && tc_fit) {
+      // (rotational form only: the tcgen05 epilogue forms u and omega)
+      if (pl->mixed && tc_fit && !d.grad) {
         std::vector<unsigned char> img(kTcImgA, 0);
         auto bf16_bits = [](float f) -> uint16_t {  // round to nearest even
           uint32_t u;

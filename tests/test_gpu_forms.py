@@ -165,3 +165,13 @@ def test_cnab2_rotational_keeps_laminar_state_and_matches_gradient_step(cuda, fa
     rs = rotational.step(rotational.initial_state())
     for a, b in zip((*rs.u, rs.g), (*gs.u, gs.g), strict=True):
         assert torch.allclose(a, b, rtol=2.0e-7, atol=2.0e-10)
+
+
+def test_mixed_gradient_form_has_no_tensor_core_velocity_variant(cuda, monkeypatch):
+    """The tcgen05 velocity products form the rotational fields only: a
+    gradient-form plan does not offer them, even when JFB200_TC asks."""
+    monkeypatch.setenv("JFB200_TC", "1")
+    g = PlaneCouetteFluctuation(N=(33, 32, 32), Re=400.0, dt=1e-3, precision="mixed",
+                                nonlinear_form="gradient", time_integrator="SBDF3", device=cuda)
+    v = g.variant()
+    assert v["available"]["tc_velocity"] == 0 and v["current"]["tc_velocity"] == 0
