@@ -175,3 +175,46 @@ def test_mixed_gradient_form_has_no_tensor_core_velocity_variant(cuda, monkeypat
                                 nonlinear_form="gradient", time_integrator="SBDF3", device=cuda)
     v = g.variant()
     assert v["available"]["tc_velocity"] == 0 and v["current"]["tc_velocity"] == 0
+
+
+@pytest.mark.parametrize("family", ["C", "L"])
+@pytest.mark.parametrize("integrator", ["IMEXRK222", "CNAB2", "SBDF3"])
+def test_smallest_grids_without_dealiasing_match_oracle(cuda, family, integrator):
+    """The reference's small test grids (9, 4, 4) with padding (1, 1, 1):
+    two-point Fourier half spectra and four-point transforms, gradient form,
+    against the oracle after three steps."""
+    kw = dict(family=family, nonlinear_form="gradient", time_integrator=integrator,
+              padding_factor=(1.0, 1.0, 1.0))
+    o = PlaneCouetteOracle(N=(9, 4, 4), Re=200.0, dt=1e-3, perturbation_amplitude=0.05, **kw)
+    g = PlaneCouetteFluctuation(N=(9, 4, 4), Re=200.0, dt=1e-3, perturbation_amplitude=0.05,
+                                device=cuda, **kw)
+    st = o.initial_state()
+    gs = g.solve(g._ensure_history(to_dev(st, cuda)), 3)
+    st = o.solve(st, 3)
+    for a, b in zip((*gs.u, gs.g), (*st.u, st.g), strict=True):
+        assert rel(a, b) < 1e-12
+
+
+def test_imaginary_mean_flow_input_steps_to_a_real_mean(cuda):
+    """The reference's mean-mode test (tests/couette/test_pcf_fluctuations_jax.py:
+    198-215): imaginary parts added to the (0, 0) modes of u1, u2 leave no
+    imaginary part in the stepped mean flow."""
+    g = PlaneCouetteFluctuation(N=(9, 4, 4), Re=200.0, dt=1e-3, padding_factor=(1.0, 1.0, 1.0),
+                                device=cuda)
+    s0 = g.initial_state()
+    u1, u2 = s0.u[1].clone(), s0.u[2].clone()
+    im = 1e-4j * torch.linspace(1.0, 2.0, u1.shape[0], dtype=torch.float64, device=cuda)
+    u1[:, 0, 0] += im
+    u2[:, 0, 0] += 2.0 * im
+    s1 = g.step(KMMState(u=(s0.u[0], u1, u2), g=s0.g))
+    assert float(s1.u[1][:, 0, 0].imag.abs().max()) < 1e-12
+    assert float(s1.u[2][:, 0, 0].imag.abs().max()) < 1e-12
+
+
+def test_zero_state_stays_zero(cuda):
+    """tests/couette/test_pcf_fluctuations_jax.py:191-196: a step of the
+    zero fluctuation (Legendre, default gradient form and integrator)."""
+    g = PlaneCouetteFluctuation(N=(9, 8, 8), family="L", dt=1.0e-3, device=cuda)
+    st = g.step(g.zero_state())
+    for t in (*st.u, st.g):
+        assert float(t.abs().max()) <= 1.0e-7
