@@ -219,10 +219,51 @@ __device__ __noinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, i
 // acc[nt] += A(rows of one 8-row tile) * B(Bs rows, columns 8 nt ..), k tiles
 // [kb, ke) with ke - kb <= KMAX; A fragments are loaded in chunks of 8 k tiles,
 // the next chunk in flight while the current one is multiplied.
+// The rolled form of the products (JFB_GEMM_COMPACT = 1) is the default:
+// its smaller code cut phase B from 12.6 to 9.9 us per CTA at 65x64x64 (the
+// unrolled form stalled on instruction fetch).
+#ifndef JFB_VEL_UNROLL
+#define JFB_VEL_UNROLL 1
+#endif
+constexpr int kVelUnroll = JFB_VEL_UNROLL;  // k tiles per unrolled step of the velocity products
+#ifndef JFB_GEMM_COMPACT
+#define JFB_GEMM_COMPACT 1
+#endif
 template <int NT, int KMAX>
 __device__ __forceinline__ void gemm_acc(const double* __restrict__ A, int kb, int ke,
                                          const double* __restrict__ Bs, int lane,
                                          double (&acc)[NT][2]) {
+#if JFB_GEMM_COMPACT
+  // rolled form: two chunk buffers, the next chunk loading while the current
+  // one is multiplied (smaller code than the unrolled form below)
+  constexpr int CH = 8;
+  const int g = lane >> 2, t4 = lane & 3;
+  const double* __restrict__ b = Bs + t4 * kGLd + g;
+  double a0[CH], a1[CH];
+  auto load = [&](double (&af)[CH], int k0) {
+#pragma unroll
+    for (int k = 0; k < CH; ++k) af[k] = (k0 + k < ke) ? __ldg(A + (k0 + k) * 32 + lane) : 0.0;
+  };
+  auto mul = [&](const double (&af)[CH], int k0) {
+#pragma unroll
+    for (int k = 0; k < CH; ++k)
+      if (k0 + k < ke) {
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+          dmma_8x8x4(acc[nt][0], acc[nt][1], af[k], b[(k0 + k) * 4 * kGLd + nt * 8]);
+      }
+  };
+  if (kb >= ke) return;
+  load(a0, kb);
+#pragma unroll 1
+  for (int k0 = kb; k0 < ke; k0 += 2 * CH) {
+    if (k0 + CH < ke) load(a1, k0 + CH);
+    mul(a0, k0);
+    if (k0 + CH >= ke) break;
+    if (k0 + 2 * CH < ke) load(a0, k0 + 2 * CH);
+    mul(a1, k0 + CH);
+  }
+#else
   constexpr int CH = 8, NC = (KMAX + CH - 1) / CH;
   const int g = lane >> 2, t4 = lane & 3;
   const double* __restrict__ b = Bs + t4 * kGLd + g;
@@ -248,6 +289,7 @@ __device__ __forceinline__ void gemm_acc(const double* __restrict__ A, int kb, i
       }
     }
   }
+#endif
 }
 
 __device__ __forceinline__ int2 sub_krange(const GemmOps& G, int id, int mt) {
@@ -1044,7 +1086,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
         const double* A0 = vs + d0.off + jt * d0.kt * 32;
         const double* A1 = vs + d1.off + jt * d1.kt * 32;
         const double* A2 = vs + d2.off + jt * d2.kt * 32;
-#pragma unroll 4
+#pragma unroll kVelUnroll
         for (int kt = 0; kt < d0.kt; ++kt) {
           const double b = Bs[kt * 4 * kGLd];
           dmma_8x8x4(acc[q0][0], acc[q0][1], A0[kt * 32], b);
@@ -1057,7 +1099,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
         const SubDesc d0 = G.sub[s0], d1 = G.sub[s1];
         const double* A0 = vs + d0.off + jt * d0.kt * 32;
         const double* A1 = vs + d1.off + jt * d1.kt * 32;
-#pragma unroll 4
+#pragma unroll kVelUnroll
         for (int kt = 0; kt < d0.kt; ++kt) {
           const double b = Bs[kt * 4 * kGLd];
           dmma_8x8x4(acc[q0][0], acc[q0][1], A0[kt * 32], b);

@@ -105,7 +105,25 @@ __host__ __device__ inline int packed_rec_size(int n) {
 // Chebyshev (fam 0): d_n = sum_{m > n, m - n odd} 2 m c_m, d_0 halved
 // (Chebyshev.py:319-353); Legendre (fam 1): d_n = (2n + 1) sum_{m > n, m - n
 // odd} c_m (Legendre.py:195-227).
-__device__ void chebder_warp(const c64* c, c64* d, int L, double scale, int lane, int fam) {
+// Warp-level helpers of the warp-per-pencil stage: inlined, or (with
+// JFB_WARP_HELPERS_NOINLINE) one shared copy each, for a smaller kernel.
+#ifndef JFB_WARP_HELPERS_NOINLINE
+#define JFB_WARP_HELPERS_NOINLINE 0
+#endif
+#if JFB_WARP_HELPERS_NOINLINE
+#define JFB_WARP_HELPER __noinline__
+#else
+#define JFB_WARP_HELPER __forceinline__
+#endif
+#ifndef JFB_CHEBDER_NOINLINE
+#define JFB_CHEBDER_NOINLINE 0
+#endif
+#if JFB_CHEBDER_NOINLINE
+__device__ __noinline__
+#else
+__device__
+#endif
+void chebder_warp(const c64* c, c64* d, int L, double scale, int lane, int fam) {
   const int K = (L + 31) / 32;
   const int lo = lane * K, hi = min(L, lo + K);
   c64 se = cmk(0.0, 0.0), so = cmk(0.0, 0.0);
@@ -141,7 +159,7 @@ __device__ void chebder_warp(const c64* c, c64* d, int L, double scale, int lane
 }
 
 // out = S_B^T a  (length Nx from nB)
-__device__ __forceinline__ void apply_SBT(const DevOps& o, const Dims& d, const c64* a,
+__device__ JFB_WARP_HELPER void apply_SBT(const DevOps& o, const Dims& d, const c64* a,
                                           c64* out, int lane) {
   for (int n = lane; n < d.Nx; n += 32) {
     c64 v = cmk(0.0, 0.0);
@@ -153,7 +171,7 @@ __device__ __forceinline__ void apply_SBT(const DevOps& o, const Dims& d, const 
   __syncwarp();
 }
 // out = S_D^T a  (length Nx from nD)
-__device__ __forceinline__ void apply_SDT(const Dims& d, const c64* a, c64* out, int lane) {
+__device__ JFB_WARP_HELPER void apply_SDT(const Dims& d, const c64* a, c64* out, int lane) {
   for (int n = lane; n < d.Nx; n += 32) {
     c64 v = cmk(0.0, 0.0);
     if (n < d.nD) v = a[n];
@@ -163,7 +181,7 @@ __device__ __forceinline__ void apply_SDT(const Dims& d, const c64* a, c64* out,
   __syncwarp();
 }
 // out[i] = scale * (S_B (ns .* c))[i]   (length nB)
-__device__ __forceinline__ void apply_SB_ns(const DevOps& o, const Dims& d, const c64* c,
+__device__ JFB_WARP_HELPER void apply_SB_ns(const DevOps& o, const Dims& d, const c64* c,
                                             c64* out, double scale, int lane) {
   for (int i = lane; i < d.nB; i += 32) {
     c64 v = (o.sB0[i] * o.ns[i]) * c[i];
@@ -174,7 +192,7 @@ __device__ __forceinline__ void apply_SB_ns(const DevOps& o, const Dims& d, cons
   __syncwarp();
 }
 // out[i] = scale * (S_D (ns .* c))[i]   (length nD)
-__device__ __forceinline__ void apply_SD_ns(const DevOps& o, const Dims& d, const c64* c,
+__device__ JFB_WARP_HELPER void apply_SD_ns(const DevOps& o, const Dims& d, const c64* c,
                                             c64* out, double scale, int lane) {
   for (int i = lane; i < d.nD; i += 32) {
     const c64 v = o.ns[i] * c[i] - o.ns[i + 2] * c[i + 2];
@@ -308,7 +326,7 @@ __device__ __forceinline__ void packed_solve_warp(const double* __restrict__ rec
 // Rows i = lane + 32 t of one pencil (n <= 128: the host limits Nx to 129),
 // all global loads of the warp issued before the arithmetic.
 // out[i] = c0 x[i] + c1 y[i] + c2 z[i]  (the y, z terms only when c1, c2 != 0)
-__device__ __forceinline__ void comb_rows(c64* out, const c64* x, const c64* y, const c64* z,
+__device__ JFB_WARP_HELPER void comb_rows(c64* out, const c64* x, const c64* y, const c64* z,
                                           double c0, double c1, double c2, int n, size_t P,
                                           int p, int lane) {
   c64 vx[4], vy[4], vz[4];
@@ -335,7 +353,7 @@ __device__ __forceinline__ void comb_rows(c64* out, const c64* x, const c64* y, 
   }
 }
 // acc[i] = mass[i] + dt (d0 acc[i] + d1 q1[i] + d2 q2[i])  (q terms when d1, d2 != 0)
-__device__ __forceinline__ void rhs_rows(c64* acc, const c64* mass, const c64* q1,
+__device__ JFB_WARP_HELPER void rhs_rows(c64* acc, const c64* mass, const c64* q1,
                                          const c64* q2, double d0, double d1, double d2,
                                          double dt, int n, size_t P, int p, int lane) {
   c64 v1[4], v2[4];
