@@ -115,8 +115,11 @@ __host__ __device__ inline int packed_rec_size(int n) {
 #else
 #define JFB_WARP_HELPER __forceinline__
 #endif
+// chebder_warp has one shared copy (sixteen call sites): the smaller
+// warp-per-pencil kernel took 474 instead of 514 us per launch at 97x96x96
+// (the other helpers not inlined as well: 527 us)
 #ifndef JFB_CHEBDER_NOINLINE
-#define JFB_CHEBDER_NOINLINE 0
+#define JFB_CHEBDER_NOINLINE 1
 #endif
 #if JFB_CHEBDER_NOINLINE
 __device__ __noinline__
@@ -383,7 +386,23 @@ __device__ JFB_WARP_HELPER void rhs_rows(c64* acc, const c64* mass, const c64* q
 // and g (TD, in A4) form uo0 = S_B^T u0 (-> A5), f = P_TD(d/dx uo0),
 // u1 = i(ky f + kz g)/k^2 (-> A0), u2 = i(kz f - ky g)/k^2 (-> A1); the
 // ky = kz = 0 pencil takes the real mean-flow vectors (v00, w00) from vw.
-__device__ void reconstruct_warp(const DevOps& o, const Dims& d, const c64* A3,
+#ifndef JFB_CTA_DMMA_NOINLINE
+#define JFB_CTA_DMMA_NOINLINE 0
+#endif
+#if JFB_CTA_DMMA_NOINLINE
+#define JFB_CTA_DMMA_INLINE __noinline__
+#else
+#define JFB_CTA_DMMA_INLINE __forceinline__
+#endif
+#ifndef JFB_RECON_NOINLINE
+#define JFB_RECON_NOINLINE 0
+#endif
+#if JFB_RECON_NOINLINE
+__device__ __noinline__
+#else
+__device__
+#endif
+void reconstruct_warp(const DevOps& o, const Dims& d, const c64* A3,
                                  const c64* A4, const c64* vw, bool mean_pencil,
                                  double kyp, double kzp, c64* A0, c64* A1, c64* A2,
                                  c64* A5, int lane) {
@@ -573,7 +592,7 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 // Output: out[(f N + j) ldo + w].  A warp's unit of work is one 8-row tile of
 // the operator against up to kDmmaGroup column tiles: each operator fragment
 // (read from L2, shared by all CTAs) is loaded once per unit.
-__device__ __forceinline__ void cta_backward_dmma(const double* __restrict__ VE,
+__device__ JFB_CTA_DMMA_INLINE void cta_backward_dmma(const double* __restrict__ VE,
                                                   const double* __restrict__ VO, int N,
                                                   int NF, const double* Bs, c64* out,
                                                   int ldo) {
@@ -639,7 +658,7 @@ __device__ __forceinline__ void cta_backward_dmma(const double* __restrict__ VE,
 // floor(N/2) rows) sit in shared memory as rows of kLDF doubles, column
 // c = (w NF + f) 2 + re/im.  Output: out[(f N + n) kLDW + w].  Units of
 // work as in cta_backward_dmma.
-__device__ __forceinline__ void cta_forward_dmma(const double* __restrict__ QE,
+__device__ JFB_CTA_DMMA_INLINE void cta_forward_dmma(const double* __restrict__ QE,
                                                  const double* __restrict__ QO, int N, int NF,
                                                  const double* Se, const double* So, c64* out) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
