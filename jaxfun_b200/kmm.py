@@ -18,6 +18,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .cadence import Cadence, run_with_cadence
 
 _STEPPERS = {"IMEXRK222", "IMEXRK3", "CNAB2", "SBDF3"}
 _GPU_STEPPERS = {"SBDF3": _lib.JFB_INTEGRATOR_SBDF3, "IMEXRK3": _lib.JFB_INTEGRATOR_IMEXRK3,
@@ -317,6 +318,20 @@ class KMM:
             self._current = out
         self.check()
         return out
+
+    def solve_with_cadence(self, state, steps: int, cadence: Cadence, *, block_size: int = 1,
+                           on_diagnostics=None, on_snapshot=None, on_checkpoint=None,
+                           should_stop=None, t0: float = 0.0, tstep0: int = 0):
+        """``solve`` in blocks with host callbacks at the cadence boundaries
+        (channelflow_kmm.py:1264-1289; contract in ``jaxfun_b200.cadence``);
+        the diagnostics passed to ``on_diagnostics`` are ``self.diagnostics``
+        of the state at the boundary."""
+        return run_with_cadence(
+            self.solve, state, steps=steps, dt=self.dt, cadence=cadence,
+            block_size=block_size, diagnostics=self.diagnostics,
+            on_diagnostics=on_diagnostics, on_snapshot=on_snapshot,
+            on_checkpoint=on_checkpoint, should_stop=should_stop, t0=t0, tstep0=tstep0,
+        )
 
     def check(self) -> None:
         """Read and clear the plan's device status word (synchronises the
