@@ -35,7 +35,14 @@ namespace jfb {
 
 constexpr int kGW = 16;         // pencils per CTA
 constexpr int kGLd = 36;        // doubles per shared row: 2 kGW + 4
-constexpr int kGThreads = 512;  // 16 warps
+// Threads per CTA (a multiple of 128, at least 384: the tcgen05 epilogue
+// reads TMEM with twelve warps).  Twelve warps at up to 168 registers took
+// 47.7 us per CTA at 65x64x64, sixteen at 128 registers 43.7 us.
+#ifndef JFB_GEMM_THREADS
+#define JFB_GEMM_THREADS 512
+#endif
+constexpr int kGThreads = JFB_GEMM_THREADS;
+static_assert(kGThreads % 128 == 0 && kGThreads >= 384, "pencil_gemm_kernel thread count");
 constexpr int kGWarps = kGThreads / 32;
 
 struct SubDesc {
@@ -1049,7 +1056,8 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
     __syncthreads();
     JFB_STAMP(0, 13);
     if (!skip_epi) {
-      const int j = tid >> 4, w = tid & 15;
+      for (int e = tid; e < 32 * kGW; e += kGThreads) {
+      const int j = e >> 4, w = e & 15;
       const int p = s_p[w];
       if (j < Jl && p >= 0) {
         auto val = [&](int slot) {
@@ -1067,6 +1075,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
           X[(size_t)j * P] = cmk((float)vp.re, (float)vp.im);
           X[(size_t)jm * P] = cmk((float)vm.re, (float)vm.im);
         }
+      }
       }
       if (Jh > Jl && tid < kGW) mid_store(d, a, sm + G.oMid, s_p, s_ky, s_kz, tid, N, Jl, P);
     }
