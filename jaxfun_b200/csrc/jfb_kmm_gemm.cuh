@@ -38,6 +38,11 @@ constexpr int kGLd = 36;        // doubles per shared row: 2 kGW + 4
 // Threads per CTA (a multiple of 128, at least 384: the tcgen05 epilogue
 // reads TMEM with twelve warps).  Twelve warps at up to 168 registers took
 // 47.7 us per CTA at 65x64x64, sixteen at 128 registers 43.7 us.
+// Base-flow samples of the mixed form loaded before the staging copies are
+// issued (1) or while they fly (0).
+#ifndef JFB_XLIN_EARLY
+#define JFB_XLIN_EARLY 0
+#endif
 #ifndef JFB_GEMM_THREADS
 #define JFB_GEMM_THREADS 512
 #endif
@@ -604,6 +609,25 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
   // rows j, N-1-j of two items
   c32 xl[2][2][4];
   {
+    // mixed form: this thread's base-flow samples (before the copies are
+    // issued with JFB_XLIN_EARLY, else while they fly)
+    auto load_xlin = [&]() {
+      if (!a.Xlin) return;
+#pragma unroll
+      for (int it = 0; it < 2; ++it) {
+        const int idx = tid + it * kGThreads;
+        if (idx >= Jh * kGW) continue;
+        const int j = idx / kGW, w = idx % kGW, p = s_p[w];
+        if (p < 0) continue;
+        const int rows[2] = {j, N - 1 - j};
+        const int fs[4] = {0, d.grad ? 6 : 1, d.grad ? 7 : 3, d.grad ? 8 : 5};
+#pragma unroll
+        for (int s2 = 0; s2 < 2; ++s2)
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            xl[it][s2][k] = a.Xlin[((size_t)fs[k] * N + rows[s2]) * P + p];
+      }
+    };
     const int lv = 1 + has_b + has_c;
     const int nrow = 3 * N + (d.nB + d.nD) * lv;
     // one half-warp per row (lane & 15 = pencil column), so that the row's
@@ -612,6 +636,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
     const int side = c >> 3, kz = c & 7;  // nkz <= 8 columns per side
     const bool col_ok = side < sides && kz < nkz;
     const size_t so = (size_t)(side ? d.Ny - kyi : kyi) * d.Kz + kz0 + kz;
+    if (JFB_XLIN_EARLY) load_xlin();
     for (int r = hw; r < nrow; r += kGThreads / 16) {
       if (!col_ok) continue;
       const c64* src;
@@ -645,23 +670,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
       }
       cp_async16(rowc + (size_t)dst_row * LC + side * 8 + kz, src + so);
     }
-    // mixed form: this thread's base-flow samples, loaded while the copies fly
-    if (a.Xlin) {
-#pragma unroll
-      for (int it = 0; it < 2; ++it) {
-        const int idx = tid + it * kGThreads;
-        if (idx >= Jh * kGW) continue;
-        const int j = idx / kGW, w = idx % kGW, p = s_p[w];
-        if (p < 0) continue;
-        const int rows[2] = {j, N - 1 - j};
-        const int fs[4] = {0, d.grad ? 6 : 1, d.grad ? 7 : 3, d.grad ? 8 : 5};
-#pragma unroll
-        for (int s2 = 0; s2 < 2; ++s2)
-#pragma unroll
-          for (int k = 0; k < 4; ++k)
-            xl[it][s2][k] = a.Xlin[((size_t)fs[k] * N + rows[s2]) * P + p];
-      }
-    }
+    if (!JFB_XLIN_EARLY) load_xlin();
     cp_async_commit();
     cp_async_wait_all();
   }
@@ -1056,7 +1065,11 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
     __syncthreads();
     JFB_STAMP(0, 13);
     if (!skip_epi) {
-      for (int e = tid; e < 32 * kGW; e += kGThreads) {
+      constexpr int kEpiIters = (32 * kGW + kGThreads - 1) / kGThreads;
+#pragma unroll
+      for (int it = 0; it < kEpiIters; ++it) {
+      const int e = tid + it * kGThreads;
+      if (e >= 32 * kGW) break;
       const int j = e >> 4, w = e & 15;
       const int p = s_p[w];
       if (j < Jl && p >= 0) {
