@@ -19,6 +19,10 @@ through ``jfb_kmm_timed_steps`` gives per-kernel times (events around every
 launch); reports the per-kernel roofline of the dominant kernel, the
 back-to-back CUDA-graph throughput, an end-to-end figure through the public
 ``solve`` API with pinned host buffers, and the CPU oracle on the host cores.
+Further blocks (each with a --no-... switch): the adjoint and minimal-seed
+ascent, the MHD ensemble, the 2-D Helmholtz solve, the linear-stability tools
+(growth-rate map and optimal-growth scan), the larger grids and the
+reference's default (gradient) form with its integrators.
 
 Reference arm (--impl reference): the reference (JAX) cannot be installed
 here, so the reference's CPU algorithm is timed through the NumPy/SciPy
@@ -69,6 +73,8 @@ def parse_args(argv=None):
     p.add_argument("--ensemble-members", type=int, default=32)
     p.add_argument("--no-helmholtz", action="store_true",
                    help="skip the 2-D Helmholtz block")
+    p.add_argument("--no-linear", action="store_true",
+                   help="skip the linear-stability / transient-growth block")
     p.add_argument("--no-default-form", action="store_true",
                    help="skip the gradient-form (the reference's default) timing block")
     p.add_argument("--no-sizes", action="store_true",
@@ -886,12 +892,73 @@ def main(argv=None):
             out[f"{n}x{n - 1}x{n - 1}"] = rec
         return out
 
+    def linear_block():
+        """Plane-Couette linear stability at Re 1000 on the KMM Legendre
+        operators: the leading growth rate of an 8 x 8 (ky, kz) map at nx 64
+        (one batched assembly, shift-inverted solve and eigenvalue call), and
+        the optimal growth G(t) at 40 times for (ky, kz) = (0, 1.66) at nx 80
+        (one batched matrix exponential); CUDA events around each.  CPU
+        baseline: the oracle's restatement of the reference's collocation
+        operator with QZ, per mode, on the host."""
+        import numpy as np
+
+        from jaxfun_b200.linear import PlaneCouetteLinear
+
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def timed(fn, reps=3):
+            fn()
+            torch.cuda.synchronize(dev)
+            e0.record(stream)
+            for _ in range(reps):
+                r = fn()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            return r, e0.elapsed_time(e1) / reps
+
+        pcf = PlaneCouetteLinear.couette(nx=64, Re=1000.0, device=dev)
+        ky, kz = torch.meshgrid(torch.linspace(0.0, 3.0, 8), torch.linspace(0.25, 3.0, 8),
+                                indexing="ij")
+        rates, ms_map = timed(lambda: pcf.growth_rates(ky, kz), reps=2)
+        scan = PlaneCouetteLinear.couette(nx=80, Re=1000.0, device=dev)
+        times = np.linspace(120.0, 160.0, 40)
+        G, ms_scan = timed(lambda: scan.optimal_growth(0.0, 1.66, times).reshape(-1))
+        i = int(G.argmax())
+        out = {
+            "workload": "plane Couette, Re 1000: leading growth rate over an 8 x 8 (ky, kz) map "
+                        "at nx 64; optimal growth at 40 times in [120, 160] for (0, 1.66) at nx 80",
+            "growth_rate_map": {"modes": 64, "nx": 64, "ms": ms_map,
+                                "max_growth_rate": float(rates.max())},
+            "optimal_growth_scan": {"nx": 80, "times": 40, "ms": ms_scan,
+                                    "gmax": float(G[i]), "t_opt": float(times[i])},
+        }
+        if not args.no_cpu_baseline:
+            import time as _time
+
+            from oracle.linear import PlaneCouetteLinearOracle
+            orc = PlaneCouetteLinearOracle.couette(nx=64, Re=1000.0)
+            t0 = _time.perf_counter()
+            for kyv, kzv in ((1.0, 1.0), (2.0, 0.5)):
+                orc.growth_rate(kyv, kzv)
+            per_mode = (_time.perf_counter() - t0) / 2
+            orc80 = PlaneCouetteLinearOracle.couette(nx=80, Re=1000.0)
+            t0 = _time.perf_counter()
+            orc80.nonmodal_growth(0.0, 1.66, times)
+            scan_s = _time.perf_counter() - t0
+            out["cpu_baseline"] = {
+                "kind": "port", "cores": host_threads(),
+                "growth_rate_map_ms": per_mode * 64 * 1e3, "optimal_growth_scan_ms": scan_s * 1e3,
+                "sample": "2 modes of the map timed and scaled to 64; the full 40-time scan "
+                          "(scipy QZ and SVD, default LAPACK threads)"}
+        return out
+
     forms = ("mixed", "fp64") if args.precision == "both" else (args.precision,)
     results = {p: measure(p) for p in forms}
     err = mixed_error() if "mixed" in forms and rank == 0 else None
     adj = adjoint_block() if (rank == 0 and world == 1 and not args.no_adjoint) else None
     ensb = ensemble_block() if (rank == 0 and world == 1 and not args.no_ensemble) else None
     helm = helmholtz_block() if (rank == 0 and world == 1 and not args.no_helmholtz) else None
+    lin = linear_block() if (rank == 0 and world == 1 and not args.no_linear) else None
     sizes = sizes_block() if (rank == 0 and world == 1 and not args.no_sizes) else None
     dform = (default_form_block()
              if (rank == 0 and world == 1 and not args.no_default_form) else None)
@@ -937,6 +1004,8 @@ def main(argv=None):
         line["mhd_ensemble"] = ensb
     if helm is not None:
         line["helmholtz2d"] = helm
+    if lin is not None:
+        line["linear_stability"] = lin
     if sizes is not None:
         line["larger_grids"] = sizes
     if dform is not None:
