@@ -26,6 +26,13 @@ constexpr int kLDW = kNW + 1;  // padded pencil stride in shared memory
 constexpr int kMaxNR = 2;      // rows per lane in the register solves (n <= 128)
 constexpr int kSolveChunk = 16;  // back-substitution columns per prefetch
 constexpr int kLoadBatch = 4;    // staged loads per thread in flight
+// Mixed form, warp-per-pencil stage: the FP64 base-flow terms in a separate
+// branch-free pass over the sample points (1) or per loaded H value (0).
+// The pass took the 97x96x96 stage from 474 to 458 us, 129x128x128 from
+// 1173 to 1132 us (events around the launch, steady SBDF3 step).
+#ifndef JFB_WARP_XLIN_PASS
+#define JFB_WARP_XLIN_PASS 1
+#endif
 
 struct DevOps {
   const double* Q;   // [n][j] scalar-product quadrature (Nx x Nx)
@@ -789,7 +796,7 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
           if (f == 0) v.re += a.emf_b0z * o.xphys[j];
           else if (f == 2) v.re -= a.emf_b0x * o.xphys[j];
         }
-        if (a.Xlin && a.mode != kFromPhys) {
+        if (!JFB_WARP_XLIN_PASS && a.Xlin && a.mode != kFromPhys) {
           // base-flow terms of the rotational product in FP64 (the complex64
           // transforms carry -(u' x omega') only)
           const int f = fi / d.Nx, j = fi % d.Nx;
@@ -829,6 +836,53 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
       }
     }
     __syncthreads();
+    if (JFB_WARP_XLIN_PASS && a.Xlin && a.mode != kFromPhys && !nyq) {
+      // mixed form: the base-flow terms in FP64 (the complex64 transforms
+      // carry the perturbation products only), one pass per sample point
+      // (j, pencil) with its four complex64 velocity samples loaded without
+      // branches, kLoadBatch points per thread in flight; the same sums in
+      // the same order as a per-field update of the loaded H values
+      const int npt = d.Nx * kNW;
+      const int g1 = d.grad ? 6 : 1, g2 = d.grad ? 7 : 3, g3 = d.grad ? 8 : 5;
+      for (int i0 = threadIdx.x; i0 < npt; i0 += kLoadBatch * blockDim.x) {
+        c64 x[kLoadBatch][4];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+          const int idx = i0 + u * blockDim.x;
+          const int w = idx % kNW, j = idx / kNW;
+          const bool ok = idx < npt && w < nvalid;
+          const int gs[4] = {0, g1, g2, g3};
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            c32 v = {0.f, 0.f};
+            if (ok) v = a.Xlin[((size_t)gs[k] * d.Nx + j) * P + p0 + w];
+            x[u][k] = cmk((double)v.re, (double)v.im);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+          const int idx = i0 + u * blockDim.x;
+          const int w = idx % kNW, j = idx / kNW;
+          if (idx >= npt || w >= nvalid) continue;
+          const double uw = d.uwall, ub = d.uwall * o.xphys[j];
+          c64* h0 = R1 + (size_t)j * kLDW + w;
+          c64* h1 = h0 + (size_t)d.Nx * kLDW;
+          c64* h2 = h1 + (size_t)d.Nx * kLDW;
+          if (d.grad) {  // U_b d/dy u_i (+ u_0 dU_b/dx e_y), pcf_fluctuations_jax.py:99-106
+            *h0 = *h0 + ub * x[u][1];
+            *h1 = (*h1 + ub * x[u][2]) + uw * x[u][0];
+            *h2 = *h2 + ub * x[u][3];
+          } else {  // x = (u0, u1, omega0, omega2)
+            c64 v = *h0 - uw * x[u][1] - ub * x[u][3];
+            if (p0 + w == 0) v.re -= ub * uw;
+            *h0 = v;
+            *h1 = *h1 + uw * x[u][0];
+            *h2 = *h2 + ub * x[u][2];
+          }
+        }
+      }
+      __syncthreads();
+    }
     // mirror sums / differences of the samples as B-operand rows in ARR
     // (free until the per-pencil work starts)
     {
