@@ -39,8 +39,15 @@ factor of Q, which needs no eigenvectors.  The eigenvector route of
 ``transient_growth_from_eigs`` (the reference's) serves ``n_modes``
 truncations.
 
-Not built: the MHD operator (``mhd=True``: induction equation, imposed field,
-the four magnetic wall conditions).
+MHD (``mhd=True``, ``shearpy``): the induction equation with an imposed
+field (0, by, bz), the magnetic multiplier of div b = 0 and the four
+magnetic wall conditions (conducting, dirichlet, pseudo_vacuum, insulating)
+are wall rows of a descriptor pencil; here that operator keeps the
+reference's primitive-variable Chebyshev-Lobatto form (eight blocks of nx
+values), assembled for a batch of modes on the device, with the same
+shift-inverted eigen-solve (a singular M maps to infinite eigenvalues, which
+the finite cap removes) and the reference's modal route for the transient
+growth in the kinetic, magnetic or total energy.
 """
 
 from __future__ import annotations
@@ -271,6 +278,29 @@ def legendre_kmm_matrices(nx: int) -> dict[str, np.ndarray]:
     }
 
 
+def cheb_lobatto(n: int):
+    """Chebyshev-Lobatto points x_j = cos(pi j / (n-1)) (x_0 = +1), the
+    collocation first-derivative matrix (diagonal from the negative row sums)
+    and its square, and the Clenshaw-Curtis weights (Trefethen, Spectral
+    Methods in MATLAB, cheb and clencurt)."""
+    n = int(n)
+    if n < 4:
+        raise ValueError("nx must be at least 4")
+    N = n - 1
+    j = np.arange(n)
+    theta = np.pi * j / N
+    x = np.cos(theta)
+    c = np.where((j == 0) | (j == N), 2.0, 1.0) * np.where(j % 2 == 0, 1.0, -1.0)
+    D = np.outer(c, 1.0 / c) / (x[:, None] - x[None, :] + np.eye(n))
+    D -= np.diag(D.sum(axis=1))
+    s = np.ones(n)
+    for k in range(1, N // 2 + 1):
+        s -= (1.0 if 2 * k == N else 2.0) * np.cos(2 * k * theta) / (4.0 * k * k - 1.0)
+    w = 2.0 * s / N
+    w[0] = w[-1] = 1.0 / (N * N - 1.0) if N % 2 == 0 else 1.0 / (N * N)
+    return x, D, D @ D, w
+
+
 class PlaneCouetteLinear:
     """Plane-Couette linear operator on the KMM unknowns (u, g), batched
     over wavenumbers (examples/pcf_linear_jax.py:69-397, hydrodynamic part).
@@ -279,21 +309,25 @@ class PlaneCouetteLinear:
     spanwise; base flow U(x) = Uoffset + Uprime x along y, rotation
     ``omega`` about z.  ``ky``/``kz`` arguments accept scalars or arrays
     (broadcast together) wherever a batch makes sense.  Eigenvectors are
-    coefficient vectors [u (nx - 4); g (nx - 2)], not collocation values."""
+    coefficient vectors [u (nx - 4); g (nx - 2)] of the hydrodynamic
+    operator, and collocation values of (u_x, u_y, u_z, p, b_x, b_y, b_z,
+    phi) for the MHD operator (``mhd=True``)."""
 
     def __init__(self, nx=64, nu=1.0e-3, eta=1.0e-3, Uprime=1.0, Uoffset=0.0, omega=0.0,
                  by=0.0, bz=0.0, mhd=False, magnetic_bc="conducting", device="cuda"):
         if magnetic_bc not in _MAGNETIC_BCS:
             raise ValueError("magnetic_bc must be 'conducting', 'dirichlet', 'pseudo_vacuum' "
                              "or 'insulating'")
-        if mhd:
-            raise NotImplementedError(
-                "the MHD linear operator (induction equation, imposed field, magnetic wall "
-                "conditions) is not built on the B200 operators; hydrodynamic operator only")
         self.nx, self.nu, self.eta = int(nx), float(nu), float(eta)
         self.Uprime, self.Uoffset, self.omega = float(Uprime), float(Uoffset), float(omega)
-        self.by, self.bz, self.mhd, self.magnetic_bc = float(by), float(bz), False, magnetic_bc
+        self.by, self.bz, self.mhd, self.magnetic_bc = float(by), float(bz), bool(mhd), magnetic_bc
         self.device = torch.device(device)
+        if self.mhd:
+            x, D, D2, w = cheb_lobatto(self.nx)
+            self._c = {k: torch.as_tensor(v, dtype=torch.complex128, device=self.device)
+                       for k, v in (("x", x), ("D", D), ("D2", D2), ("w", w))}
+            self.n = 8 * self.nx
+            return
         self.nB, self.nD = self.nx - 4, self.nx - 2
         self.n = self.nB + self.nD
         mats = legendre_kmm_matrices(self.nx)
@@ -310,8 +344,7 @@ class PlaneCouetteLinear:
     @classmethod
     def shearpy(cls, nx=64, Re=1000.0, Rm=1000.0, shear_rate=1.0, omega=2.0 / 3.0, by=0.0,
                 bz=0.025, velocity_scale=1.0, **kw):
-        """The rotating-shear MHD configuration (pcf_linear_jax.py:154-178);
-        raises ``NotImplementedError`` (MHD operator not built)."""
+        """The rotating-shear MHD configuration (pcf_linear_jax.py:154-178)."""
         return cls(nx=nx, nu=float(velocity_scale) / float(Re), eta=float(velocity_scale) / float(Rm),
                    Uprime=-float(shear_rate), Uoffset=0.0, omega=float(omega), by=by, bz=bz,
                    mhd=True, **kw)
@@ -325,9 +358,99 @@ class PlaneCouetteLinear:
             raise ValueError("at least one of ky or kz must be non-zero")
         return ky.reshape(-1), kz.reshape(-1), ky.shape
 
+    def _collocation_batch(self, ky, kz):
+        """MHD descriptor pencil (B, 8 nx, 8 nx): blocks (u_x, u_y, u_z, p,
+        b_x, b_y, b_z, phi) of collocation values, momentum with the Lorentz
+        force of the imposed field, induction with the shear of b_x into b_y,
+        continuity and div b = 0 through the multipliers p and phi, the wall
+        rows of the velocity (no slip) and of the chosen magnetic condition
+        (pcf_linear_jax.py:204-348)."""
+        c, n = self._c, self.nx
+        B = ky.numel()
+        cx = lambda v: v.to(torch.complex128)[:, None, None]  # noqa: E731
+        iky, ikz = 1j * cx(ky), 1j * cx(kz)
+        k2 = cx(ky * ky + kz * kz)
+        I = torch.eye(n, dtype=torch.complex128, device=self.device)
+        D, D2 = c["D"], c["D2"]
+        U = torch.diag(self.Uoffset + self.Uprime * c["x"])
+        lap = D2 - k2 * I
+        adv = -iky * U
+        ikB = 1j * cx(ky * self.by + kz * self.bz)
+        L = torch.zeros(B, 8 * n, 8 * n, dtype=torch.complex128, device=self.device)
+        M = torch.zeros_like(L)
+
+        def blk(A, r, col, v):
+            A[:, r * n:(r + 1) * n, col * n:(col + 1) * n] += v
+
+        for f in range(3):
+            blk(L, f, f, adv + self.nu * lap)
+            blk(M, f, f, I)
+            blk(L, f, 4 + f, ikB * I)            # Lorentz force of the imposed field
+            blk(L, 4 + f, f, ikB * I)            # induction by the imposed field
+            blk(L, 4 + f, 4 + f, adv + self.eta * lap)
+            blk(M, 4 + f, 4 + f, I)
+        blk(L, 0, 3, -D)
+        blk(L, 1, 3, -iky * I)
+        blk(L, 2, 3, -ikz * I)
+        blk(L, 1, 0, (-self.Uprime - 2.0 * self.omega) * I)
+        blk(L, 0, 1, 2.0 * self.omega * I)
+        blk(L, 3, 0, D)
+        blk(L, 3, 1, iky * I)
+        blk(L, 3, 2, ikz * I)
+        blk(L, 5, 4, self.Uprime * I)
+        blk(L, 4, 7, -D)
+        blk(L, 5, 7, -iky * I)
+        blk(L, 6, 7, -ikz * I)
+        blk(L, 7, 4, D)
+        blk(L, 7, 5, iky * I)
+        blk(L, 7, 6, ikz * I)
+        walls = (0, n - 1)
+        rows = [f * n + wl for f in range(3) for wl in walls]
+        bc = self.magnetic_bc
+        if bc == "dirichlet":
+            rows += [f * n + wl for f in (4, 5, 6) for wl in walls]
+        elif bc == "conducting":
+            rows += [f * n + wl for f in (4, 5, 6) for wl in walls]
+        else:  # pseudo_vacuum, insulating: phi pinned at the walls
+            rows += [f * n + wl for f in (4, 5, 6, 7) for wl in walls]
+        L[:, rows, :] = 0.0
+        M[:, rows, :] = 0.0
+        for f in range(3):
+            for wl in walls:
+                L[:, f * n + wl, f * n + wl] = 1.0
+        bx, byb, bzb, phi = 4 * n, 5 * n, 6 * n, 7 * n
+        if bc == "dirichlet":
+            for b0 in (bx, byb, bzb):
+                for wl in walls:
+                    L[:, b0 + wl, b0 + wl] = 1.0
+        elif bc == "conducting":
+            for wl in walls:
+                L[:, bx + wl, bx + wl] = 1.0
+                L[:, byb + wl, byb:byb + n] = D[wl]
+                L[:, bzb + wl, bzb:bzb + n] = D[wl]
+        elif bc == "pseudo_vacuum":
+            for wl in walls:
+                L[:, phi + wl, phi + wl] = 1.0
+                L[:, bx + wl, bx:bx + n] = D[wl]
+                L[:, byb + wl, byb + wl] = 1.0
+                L[:, bzb + wl, bzb + wl] = 1.0
+        else:  # insulating: exterior potential field exp(-k |x|) matched at each wall
+            k = torch.sqrt(ky * ky + kz * kz).to(torch.complex128)
+            for wl, sgn in ((0, 1.0), (n - 1, -1.0)):
+                L[:, phi + wl, phi + wl] = 1.0
+                L[:, bx + wl, bx:bx + n] = D[wl]
+                L[:, bx + wl, bx + wl] += sgn * k
+                L[:, byb + wl, byb + wl] = 1.0
+                L[:, byb + wl, bx + wl] = sgn * 1j * ky.to(torch.complex128) / k
+                L[:, bzb + wl, bzb + wl] = 1.0
+                L[:, bzb + wl, bx + wl] = sgn * 1j * kz.to(torch.complex128) / k
+        return L, M
+
     def assemble_batch(self, ky, kz):
         """(L, M) of shape (B, n, n) for the flattened broadcast of ky, kz."""
         ky, kz, _ = self._wavenumbers(ky, kz)
+        if self.mhd:
+            return self._collocation_batch(ky, kz)
         m, nB = self._m, self.nB
         c = lambda v: v.to(torch.complex128)[:, None, None]  # noqa: E731
         k2 = c(ky * ky + kz * kz)
@@ -352,13 +475,22 @@ class PlaneCouetteLinear:
         return L[0], M[0]
 
     def energy_matrix_batch(self, ky, kz, kind="total"):
-        """Kinetic-energy metric Q (B, n, n): q^H Q q = int |u_x|^2 + |u_y|^2
-        + |u_z|^2 dx for the mode's coefficients q = [u; g]."""
+        """Energy metric Q (B, n, n).  Hydrodynamic operator: q^H Q q =
+        int |u_x|^2 + |u_y|^2 + |u_z|^2 dx for the coefficients q = [u; g];
+        MHD operator: Clenshaw-Curtis weights on the velocity ("kinetic"),
+        field ("magnetic") or both ("total") blocks."""
         if kind not in ("total", "kinetic", "magnetic"):
             raise ValueError("kind must be 'total', 'kinetic', or 'magnetic'")
-        if kind == "magnetic":
+        if kind == "magnetic" and not self.mhd:
             raise ValueError("magnetic energy norm requires mhd=True")
         ky, kz, _ = self._wavenumbers(ky, kz)
+        if self.mhd:  # Clenshaw-Curtis weights on the velocity and/or field blocks
+            n = self.nx
+            Q = torch.zeros(self.n, self.n, dtype=torch.complex128, device=self.device)
+            blocks = ([0, 1, 2] if kind != "magnetic" else []) + ([4, 5, 6] if kind != "kinetic" else [])
+            for f in blocks:
+                Q[f * n:(f + 1) * n, f * n:(f + 1) * n] = torch.diag(self._c["w"])
+            return Q.expand(ky.numel(), self.n, self.n)
         k2 = (ky * ky + kz * kz).to(torch.complex128)[:, None, None]
         m, nB = self._m, self.nB
         Q = torch.zeros(ky.numel(), self.n, self.n, dtype=torch.complex128, device=self.device)
@@ -383,7 +515,7 @@ class PlaneCouetteLinear:
         w, V = _keep_finite(w, V, finite_cap)
         o = _growth_sort(w)
         w, V = w[o], V[:, o]
-        Q = self.energy_matrix(ky=ky, kz=kz)
+        Q = self.energy_matrix("total", ky=ky, kz=kz)
         scale = float(torch.linalg.matrix_norm(Q, ord=2))
         energy = torch.einsum("im,im->m", V.conj(), Q @ V).real
         keep = torch.nonzero(energy > math.sqrt(np.finfo(float).eps) * scale
@@ -401,8 +533,15 @@ class PlaneCouetteLinear:
         """Leading growth rate of every mode of the broadcast (ky, kz) grid,
         one batched solve and eigenvalue call; shape of the broadcast."""
         _, _, shape = self._wavenumbers(ky, kz)
-        w, _ = _pencil_eig(*self.assemble_batch(ky, kz), vectors=False)
-        ok = torch.isfinite(w.real) & (w.abs() < finite_cap)
+        w, V = _pencil_eig(*self.assemble_batch(ky, kz), vectors=self.mhd)
+        ok = torch.isfinite(w.real) & torch.isfinite(w.imag) & (w.abs() < finite_cap)
+        if self.mhd:
+            # descriptor pencil: only eigenvectors with energy are modes
+            # (multiplier directions carry none), as in ``eigs``
+            Q = self.energy_matrix_batch(ky, kz)
+            scale = torch.linalg.matrix_norm(Q[:1], ord=2).reshape(())
+            energy = torch.einsum("bim,bim->bm", V.conj(), Q @ V).real
+            ok &= energy > math.sqrt(np.finfo(float).eps) * scale * (V.abs() ** 2).sum(1)
         re = torch.where(ok, w.real, torch.full_like(w.real, -math.inf))
         return re.max(dim=-1).values.reshape(shape)
 
@@ -413,6 +552,12 @@ class PlaneCouetteLinear:
         A = M^-1 L, Q = R^H R; one batched matrix exponential over
         (mode, time).  Shape (*broadcast, T)."""
         _, _, shape = self._wavenumbers(ky, kz)
+        if self.mhd:  # descriptor pencil: the modal route, one mode at a time
+            kyf, kzf, _ = self._wavenumbers(ky, kz)
+            t = parse_times(times)
+            G = [[r["gain"] for r in self.nonmodal_growth(float(a), float(b), t)]
+                 for a, b in zip(kyf.tolist(), kzf.tolist(), strict=True)]
+            return torch.tensor(G, dtype=torch.float64, device=self.device).reshape(*shape, len(t))
         tt = torch.as_tensor(parse_times(times), dtype=torch.float64, device=self.device)
         A = self._operator(ky, kz)                                            # (B, n, n)
         R = torch.linalg.cholesky(self.energy_matrix_batch(ky, kz)).mH        # Q = R^H R
@@ -423,22 +568,26 @@ class PlaneCouetteLinear:
     def nonmodal_growth(self, ky, kz, times, n_modes=None, finite_cap=NONMODAL_FINITE_CAP,
                         energy="total"):
         """Optimal transient growth rows ``{"t", "gain", "amplification"}``
-        (pcf_linear_jax.py:385-396).  All modes: the propagator of
-        ``optimal_growth``; ``n_modes``: the leading eigenvectors through
-        ``transient_growth_from_eigs``."""
+        (pcf_linear_jax.py:385-396).  Hydrodynamic operator, all modes: the
+        propagator of ``optimal_growth``; ``n_modes`` or the MHD operator:
+        the leading (all finite) eigenvectors through
+        ``transient_growth_from_eigs`` in the ``energy`` norm ("kinetic",
+        "magnetic" or "total")."""
         Q = self.energy_matrix(energy, ky=ky, kz=kz)
         t = parse_times(times)
-        if n_modes is None:
+        if n_modes is None and not self.mhd:
             gains = self.optimal_growth(float(ky), float(kz), t).reshape(-1).cpu().numpy()
             return _growth_rows(t, gains)
         w, V = _pencil_eig(*self.assemble(ky, kz))
         w, V = _keep_finite(w, V, finite_cap)
-        o = _growth_sort(w)[: int(n_modes)]
+        o = _growth_sort(w)
+        if n_modes is not None:
+            o = o[: int(n_modes)]
         return transient_growth_from_eigs(w[o], V[:, o], Q, t)
 
 
 def main(argv=None) -> int:
-    """Command line of pcf_linear_jax.py:399-460 (hydrodynamic options)."""
+    """Command line of pcf_linear_jax.py:399-460."""
     import argparse
 
     p = argparse.ArgumentParser(description="Plane-Couette linear/non-modal analysis (B200)")
@@ -449,11 +598,23 @@ def main(argv=None) -> int:
     p.add_argument("--nonmodal", action="store_true")
     p.add_argument("--times", type=str, default="1,5,10,20")
     p.add_argument("--n-modes", type=int, default=None)
+    p.add_argument("--Rm", type=float, default=None)
+    p.add_argument("--mhd", action="store_true")
+    p.add_argument("--shearpy", action="store_true")
+    p.add_argument("--by", type=float, default=0.0)
+    p.add_argument("--bz", type=float, default=0.025)
+    p.add_argument("--magnetic-bc", choices=list(_MAGNETIC_BCS), default="conducting")
+    p.add_argument("--energy", choices=["total", "kinetic", "magnetic"], default="total")
     a = p.parse_args(argv)
-    solver = PlaneCouetteLinear.couette(nx=a.nx, Re=a.Re)
+    if a.shearpy:
+        solver = PlaneCouetteLinear.shearpy(nx=a.nx, Re=a.Re, Rm=a.Rm or a.Re, by=a.by, bz=a.bz,
+                                            magnetic_bc=a.magnetic_bc)
+    else:
+        solver = PlaneCouetteLinear.couette(nx=a.nx, Re=a.Re, Rm=a.Rm, mhd=a.mhd, by=a.by,
+                                            bz=a.bz, magnetic_bc=a.magnetic_bc)
     if a.nonmodal:
         print_transient_growth(solver.nonmodal_growth(a.ky, a.kz, parse_times(a.times),
-                                                      n_modes=a.n_modes))
+                                                      n_modes=a.n_modes, energy=a.energy))
     else:
         w, _ = solver.eigs(a.ky, a.kz, n_return=8)
         print_eigenvalues(w)

@@ -1,19 +1,21 @@
 """NumPy/SciPy restatement of the reference's plane-Couette linear-stability
-tools (test oracle).
+tools, hydrodynamic and MHD (test oracle).
 
 TEST INFRASTRUCTURE ONLY — imported by ``tests/``; never by the product
 package.
 
-Restates, for the hydrodynamic operator (``mhd=False``):
+Restates:
 
 * ``src/jaxfun/la/eig.py:12-125,145-242`` — growth ordering, finite and
   physical eigensystems of a pencil ``L q = s M q``, optimal transient growth
   from a modal basis in an energy metric;
 * ``examples/pcf_linear_jax.py:29-66,69-397`` — the primitive-variable
-  (u_x, u_y, u_z, p) Chebyshev-Lobatto collocation operator of plane Couette
-  flow with base flow ``U(x) = Uoffset + Uprime x`` along y and a rotation
-  ``omega`` about z, velocity walls as identity rows with zero mass (their
-  eigenvalues lie at infinity and are filtered).
+  (u_x, u_y, u_z, p [, b_x, b_y, b_z, phi]) Chebyshev-Lobatto collocation
+  operator of plane Couette flow with base flow ``U(x) = Uoffset + Uprime x``
+  along y, a rotation ``omega`` about z and, with ``mhd=True``, an imposed
+  field (0, by, bz) and the four magnetic wall conditions; wall conditions
+  are rows with zero mass (their eigenvalues lie at infinity and are
+  filtered).
 
 Pinned against the reference's recorded outputs of these tools
 (``couette/couette_linear_benchmarks.md``, in
@@ -155,38 +157,56 @@ def cheb_lobatto(n: int):
 
 
 class PlaneCouetteLinearOracle:
-    """pcf_linear_jax.py:69-397 for ``mhd=False``: blocks (u_x, u_y, u_z, p),
+    """pcf_linear_jax.py:69-397: blocks (u_x, u_y, u_z, p) and, with
+    ``mhd=True``, (b_x, b_y, b_z, phi) (phi: the multiplier of div b = 0),
     each ``nx`` collocation values."""
 
-    def __init__(self, nx=64, nu=1.0e-3, Uprime=1.0, Uoffset=0.0, omega=0.0):
-        self.nx, self.nu = int(nx), float(nu)
+    BCS = ("conducting", "dirichlet", "pseudo_vacuum", "insulating")
+
+    def __init__(self, nx=64, nu=1.0e-3, eta=1.0e-3, Uprime=1.0, Uoffset=0.0, omega=0.0,
+                 by=0.0, bz=0.0, mhd=False, magnetic_bc="conducting"):
+        if magnetic_bc not in self.BCS:
+            raise ValueError("magnetic_bc must be 'conducting', 'dirichlet', 'pseudo_vacuum' "
+                             "or 'insulating'")
+        self.nx, self.nu, self.eta = int(nx), float(nu), float(eta)
         self.Uprime, self.Uoffset, self.omega = float(Uprime), float(Uoffset), float(omega)
+        self.by, self.bz, self.mhd, self.magnetic_bc = float(by), float(bz), bool(mhd), magnetic_bc
         self.x, self.D, self.D2, self.weights = cheb_lobatto(self.nx)
+        self.nb = 8 if self.mhd else 4
 
     @classmethod
-    def couette(cls, nx=64, Re=400.0, U_wall=1.0, **kw):
-        """pcf_linear_jax.py:141-152 (hydro)."""
-        return cls(nx=nx, nu=float(U_wall) / float(Re), Uprime=float(U_wall), **kw)
+    def couette(cls, nx=64, Re=400.0, Rm=None, U_wall=1.0, mhd=False, **kw):
+        """pcf_linear_jax.py:141-152."""
+        Rm = Re if Rm is None else Rm
+        return cls(nx=nx, nu=float(U_wall) / float(Re), eta=float(U_wall) / float(Rm),
+                   Uprime=float(U_wall), mhd=mhd, **kw)
+
+    @classmethod
+    def shearpy(cls, nx=64, Re=1000.0, Rm=1000.0, shear_rate=1.0, omega=2.0 / 3.0, by=0.0,
+                bz=0.025, velocity_scale=1.0, **kw):
+        """pcf_linear_jax.py:154-178."""
+        return cls(nx=nx, nu=float(velocity_scale) / float(Re), eta=float(velocity_scale) / float(Rm),
+                   Uprime=-float(shear_rate), omega=float(omega), by=by, bz=bz, mhd=True, **kw)
 
     def assemble(self, ky, kz):
-        """pcf_linear_jax.py:292-348 (hydro) with the wall rows of
-        pcf_linear_jax.py:204-210."""
+        """pcf_linear_jax.py:292-348 with the wall rows of
+        pcf_linear_jax.py:204-290."""
         ky, kz = float(ky), float(kz)
         k2 = ky * ky + kz * kz
         if k2 <= 0.0:
             raise ValueError("at least one of ky or kz must be non-zero")
-        n = self.nx
+        n, nb = self.nx, self.nb
         I = np.eye(n, dtype=complex)
-        L = np.zeros((4 * n, 4 * n), dtype=complex)
+        L = np.zeros((nb * n, nb * n), dtype=complex)
         M = np.zeros_like(L)
 
         def blk(A, r, c, v):
             A[r * n:(r + 1) * n, c * n:(c + 1) * n] += v
 
-        U = self.Uoffset + self.Uprime * self.x
-        diffusion_advection = self.nu * (self.D2 - k2 * I) - 1j * ky * np.diag(U)
+        lap = self.D2 - k2 * I
+        adv = -1j * ky * np.diag(self.Uoffset + self.Uprime * self.x)
         for c in range(3):
-            blk(L, c, c, diffusion_advection)
+            blk(L, c, c, adv + self.nu * lap)
             blk(M, c, c, I)
         # pressure gradient, shear and rotation, continuity
         blk(L, 0, 3, -self.D)
@@ -197,26 +217,83 @@ class PlaneCouetteLinearOracle:
         blk(L, 3, 0, self.D)
         blk(L, 3, 1, 1j * ky * I)
         blk(L, 3, 2, 1j * kz * I)
+        if self.mhd:
+            # Lorentz force and induction by the imposed field, shear of b_x
+            # into b_y, the magnetic multiplier and div b = 0
+            ikB = 1j * (ky * self.by + kz * self.bz)
+            for c in range(3):
+                blk(L, c, 4 + c, ikB * I)
+                blk(L, 4 + c, c, ikB * I)
+                blk(L, 4 + c, 4 + c, adv + self.eta * lap)
+                blk(M, 4 + c, 4 + c, I)
+            blk(L, 5, 4, self.Uprime * I)
+            blk(L, 4, 7, -self.D)
+            blk(L, 5, 7, -1j * ky * I)
+            blk(L, 6, 7, -1j * kz * I)
+            blk(L, 7, 4, self.D)
+            blk(L, 7, 5, 1j * ky * I)
+            blk(L, 7, 6, 1j * kz * I)
+
+        def row(r, entries):
+            L[r, :] = 0.0
+            M[r, :] = 0.0
+            for cols, vals in entries:
+                L[r, cols] = vals
+
+        walls = (0, n - 1)
         for c in range(3):
-            for wall in (0, n - 1):
-                r = c * n + wall
-                L[r, :] = 0.0
-                M[r, :] = 0.0
-                L[r, r] = 1.0
+            for wall in walls:
+                row(c * n + wall, [(c * n + wall, 1.0)])
+        if self.mhd:
+            bx, by_, bz_, phi = 4 * n, 5 * n, 6 * n, 7 * n
+            bc = self.magnetic_bc
+            if bc == "insulating":
+                k = float(np.hypot(ky, kz))
+                for wall, sgn in ((0, 1.0), (n - 1, -1.0)):
+                    row(phi + wall, [(phi + wall, 1.0)])
+                    robin = self.D[wall, :].astype(complex).copy()
+                    robin[wall] += sgn * k
+                    row(bx + wall, [(slice(bx, bx + n), robin)])
+                    row(by_ + wall, [(by_ + wall, 1.0), (bx + wall, sgn * 1j * ky / k)])
+                    row(bz_ + wall, [(bz_ + wall, 1.0), (bx + wall, sgn * 1j * kz / k)])
+            elif bc == "dirichlet":
+                for b0 in (bx, by_, bz_):
+                    for wall in walls:
+                        row(b0 + wall, [(b0 + wall, 1.0)])
+            elif bc == "pseudo_vacuum":
+                for wall in walls:
+                    row(phi + wall, [(phi + wall, 1.0)])
+                    row(bx + wall, [(slice(bx, bx + n), self.D[wall, :])])
+                    row(by_ + wall, [(by_ + wall, 1.0)])
+                    row(bz_ + wall, [(bz_ + wall, 1.0)])
+            else:  # conducting
+                for wall in walls:
+                    row(bx + wall, [(bx + wall, 1.0)])
+                    row(by_ + wall, [(slice(by_, by_ + n), self.D[wall, :])])
+                    row(bz_ + wall, [(slice(bz_, bz_ + n), self.D[wall, :])])
         return L, M
 
-    def energy_matrix(self):
-        """pcf_linear_jax.py:350-373 (kinetic = total for hydro)."""
+    def energy_matrix(self, kind="total"):
+        """pcf_linear_jax.py:350-373."""
+        if kind not in ("total", "kinetic", "magnetic"):
+            raise ValueError("kind must be 'total', 'kinetic', or 'magnetic'")
+        if kind == "magnetic" and not self.mhd:
+            raise ValueError("magnetic energy norm requires mhd=True")
         n = self.nx
-        Q = np.zeros((4 * n, 4 * n), dtype=complex)
-        for c in range(3):
+        Q = np.zeros((self.nb * n, self.nb * n), dtype=complex)
+        blocks = []
+        if kind in ("total", "kinetic"):
+            blocks += [0, 1, 2]
+        if self.mhd and kind in ("total", "magnetic"):
+            blocks += [4, 5, 6]
+        for c in blocks:
             Q[c * n:(c + 1) * n, c * n:(c + 1) * n] = np.diag(self.weights)
         return Q
 
     def eigs(self, ky, kz, n_return=8, finite_cap=NONMODAL_FINITE_CAP):
         """pcf_linear_jax.py:375-379."""
         L, M = self.assemble(ky, kz)
-        return physical_eigensystem(L, M, self.energy_matrix(), finite_cap=finite_cap,
+        return physical_eigensystem(L, M, self.energy_matrix("total"), finite_cap=finite_cap,
                                     n_return=n_return)
 
     def growth_rate(self, ky, kz):
@@ -224,7 +301,8 @@ class PlaneCouetteLinearOracle:
         w, _ = self.eigs(ky, kz, n_return=1)
         return float(w[0].real) if len(w) else float("nan")
 
-    def nonmodal_growth(self, ky, kz, times, n_modes=None, finite_cap=NONMODAL_FINITE_CAP):
-        """pcf_linear_jax.py:385-396 (kinetic energy norm)."""
+    def nonmodal_growth(self, ky, kz, times, n_modes=None, finite_cap=NONMODAL_FINITE_CAP,
+                        energy="total"):
+        """pcf_linear_jax.py:385-396."""
         w, V = finite_eigensystem(*self.assemble(ky, kz), finite_cap=finite_cap, n_return=n_modes)
-        return transient_growth_from_eigs(w, V, self.energy_matrix(), times)
+        return transient_growth_from_eigs(w, V, self.energy_matrix(energy), times)

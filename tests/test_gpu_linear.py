@@ -161,3 +161,50 @@ def test_options_and_errors(cuda):
         # parts to rounding) is not defined
         for v in a.cpu().numpy():
             assert np.abs(b - v).min() <= 1e-8 * abs(v)
+
+
+# -- the MHD operator (collocation descriptor pencil) --------------------------
+
+def test_mhd_energy_norms_and_imposed_field_sweep(cuda):
+    g = GOLD["mhd_energy_norms_re500_nx48"]
+    T = [g["t"]]
+    mhd = jl.PlaneCouetteLinear.couette(nx=g["nx"], Re=g["Re"], Rm=g["Rm"], mhd=True, device=cuda)
+    b0 = g["B0_zero"]
+    # kinetic: the recorded value differs from the hydro one at 9e-9 (truncation-sensitive)
+    assert mhd.nonmodal_growth(g["ky"], g["kz"], T, energy="kinetic")[0]["gain"] == pytest.approx(
+        b0["kinetic"], rel=1e-6)
+    for kind in ("magnetic", "total"):
+        got = mhd.nonmodal_growth(g["ky"], g["kz"], T, energy=kind)[0]["gain"]
+        assert got == pytest.approx(b0[kind], rel=1e-8), kind
+    for bz, want in g["bz_sweep_total"][1:]:
+        m = jl.PlaneCouetteLinear.couette(nx=g["nx"], Re=g["Re"], Rm=g["Rm"], mhd=True, bz=bz,
+                                          device=cuda)
+        assert m.nonmodal_growth(g["ky"], g["kz"], T)[0]["gain"] == pytest.approx(want, rel=5e-7)
+
+
+def test_shearpy_mri_growth_rate(cuda):
+    g = GOLD["shearpy_mri_lead_eigenvalue"]
+    kz = math.sqrt(15.0 / 16.0) * g["omega"] / g["bz"]
+    for nx, want in g["lead"]:
+        lin = jl.PlaneCouetteLinear.shearpy(nx=nx, Re=g["Re"], Rm=g["Rm"], shear_rate=g["shear_rate"],
+                                            omega=g["omega"], by=g["by"], bz=g["bz"], device=cuda)
+        w, V = lin.eigs(0.0, kz, n_return=3)
+        assert abs(complex(w[0]) - want) <= 1e-10 and V.shape == (8 * nx, 3)
+        assert lin.growth_rate(0.0, kz) == pytest.approx(want, abs=1e-10)
+
+
+@pytest.mark.parametrize("bc", ["conducting", "dirichlet", "pseudo_vacuum", "insulating"])
+def test_magnetic_wall_conditions_match_the_oracle(cuda, bc):
+    kw = dict(nx=24, Re=200.0, Rm=200.0, mhd=True, bz=0.05, magnetic_bc=bc)
+    lin = jl.PlaneCouetteLinear.couette(device=cuda, **kw)
+    orc = ol.PlaneCouetteLinearOracle.couette(**kw)
+    ky, kz = torch.tensor([1.0, 0.5]), torch.tensor([1.0, 2.0])
+    rates = lin.growth_rates(ky, kz).cpu()
+    for i in range(2):
+        want = orc.growth_rate(float(ky[i]), float(kz[i]))
+        assert float(rates[i]) == pytest.approx(want, rel=1e-9)
+    a = lin.nonmodal_growth(1.0, 1.0, [5.0, 20.0])
+    b = orc.nonmodal_growth(1.0, 1.0, [5.0, 20.0])
+    assert [r["gain"] for r in a] == pytest.approx([r["gain"] for r in b], rel=1e-6)
+    G = lin.optimal_growth(ky, kz, [5.0, 20.0]).cpu()
+    assert G.shape == (2, 2) and float(G[0, 1]) == pytest.approx(a[1]["gain"], rel=1e-12)

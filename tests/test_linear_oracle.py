@@ -119,9 +119,60 @@ def test_legendre_kmm_basis_matrices():
 
 
 def test_operator_options_rejected_before_device_work():
-    with pytest.raises(NotImplementedError, match="MHD"):
-        PlaneCouetteLinear.couette(nx=16, Re=100.0, mhd=True, device="meta")
-    with pytest.raises(NotImplementedError, match="MHD"):
-        PlaneCouetteLinear.shearpy(nx=16, device="meta")
     with pytest.raises(ValueError, match="magnetic_bc"):
         PlaneCouetteLinear(nx=16, magnetic_bc="vacuum", device="meta")
+    hydro = PlaneCouetteLinear.couette(nx=16, Re=100.0, device="meta")
+    with pytest.raises(ValueError, match="mhd=True"):
+        hydro.energy_matrix("magnetic", ky=1.0, kz=1.0)
+    with pytest.raises(ValueError, match="kind"):
+        hydro.energy_matrix("enstrophy", ky=1.0, kz=1.0)
+    mhd = PlaneCouetteLinear.shearpy(nx=16, device="meta")
+    assert mhd.mhd and mhd.n == 8 * 16 and mhd.Uprime == -1.0
+    with pytest.raises(ValueError, match="nx"):
+        PlaneCouetteLinear.couette(nx=3, mhd=True, device="meta")
+
+
+def test_product_collocation_matrices_match_the_oracle():
+    """The MHD operator's Chebyshev-Lobatto points, derivative matrix and
+    Clenshaw-Curtis weights (host arrays) against the oracle's."""
+    from jaxfun_b200.linear import cheb_lobatto
+
+    for n in (5, 8, 33):
+        for a, b in zip(cheb_lobatto(n), ol.cheb_lobatto(n), strict=True):
+            assert np.allclose(a, b, rtol=1e-13, atol=1e-12)
+    x, D, D2, w = cheb_lobatto(17)
+    assert abs(w.sum() - 2.0) < 1e-14
+    assert np.allclose(D @ x ** 3, 3 * x ** 2, atol=1e-11)
+
+
+def test_oracle_mhd_energy_norms():
+    g = GOLD["mhd_energy_norms_re500_nx48"]
+    T = [g["t"]]
+    mhd = ol.PlaneCouetteLinearOracle.couette(nx=g["nx"], Re=g["Re"], Rm=g["Rm"], mhd=True)
+    for kind in ("kinetic", "magnetic", "total"):
+        got = mhd.nonmodal_growth(g["ky"], g["kz"], T, energy=kind)[0]["gain"]
+        assert got == pytest.approx(g["B0_zero"][kind], rel=1e-7), kind
+    for bz, want in g["bz_sweep_total"][1:]:
+        m = ol.PlaneCouetteLinearOracle.couette(nx=g["nx"], Re=g["Re"], Rm=g["Rm"], mhd=True, bz=bz)
+        assert m.nonmodal_growth(g["ky"], g["kz"], T)[0]["gain"] == pytest.approx(want, rel=5e-7)
+
+
+def test_oracle_shearpy_mri_growth_rate():
+    g = GOLD["shearpy_mri_lead_eigenvalue"]
+    kz = math.sqrt(15.0 / 16.0) * g["omega"] / g["bz"]
+    for nx, want in g["lead"][:2]:
+        lin = ol.PlaneCouetteLinearOracle.shearpy(nx=nx, Re=g["Re"], Rm=g["Rm"],
+                                                  shear_rate=g["shear_rate"], omega=g["omega"],
+                                                  by=g["by"], bz=g["bz"])
+        w, _ = lin.eigs(0.0, kz, n_return=3)
+        assert abs(w[0] - want) <= 1e-10
+
+
+def test_oracle_magnetic_wall_conditions_are_stable():
+    """Every wall condition gives a finite, decaying leading mode for a
+    weak imposed field at moderate Re (smoke check of the wall rows)."""
+    for bc in ol.PlaneCouetteLinearOracle.BCS:
+        m = ol.PlaneCouetteLinearOracle.couette(nx=24, Re=200.0, Rm=200.0, mhd=True, bz=0.05,
+                                                magnetic_bc=bc)
+        r = m.growth_rate(1.0, 1.0)
+        assert math.isfinite(r) and r < 0.0, bc
