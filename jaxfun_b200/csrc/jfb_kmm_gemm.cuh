@@ -527,9 +527,15 @@ __device__ __forceinline__ void mid_store(const Dims& d, const GemmStageArgs& a,
 
 // The pencil stage of one tile `bid` of `nbid` (the kernel below, or one
 // member's tile of the ensemble kernel in jfb_kmm_ens.cuh).
+// kTC = false compiles the body without the tcgen05 velocity products (the
+// default kernel: a smaller instruction footprint, 78.7 -> 77.4 us per
+// mixed step at 65x64x64); kTC = true keeps them behind the plan's runtime
+// flag G.tc.
+template <bool kTC>
 __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o, const GemmOps& G,
                                                  const GemmStageArgs& a, const int bid,
                                                  const int nbid) {
+  const bool use_tc = kTC && G.tc;
   extern __shared__ __align__(128) double sm[];
   __shared__ int s_p[kGW], s_mode[kGW];
   __shared__ double s_ky[kGW], s_kz[kGW];
@@ -586,14 +592,14 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
     prefetch_l2(a.s00inv, (size_t)d.nD * d.nD * sizeof(double));
     if (sl != 0.0) prefetch_l2(G.X2D, (size_t)d.nD * d.nD * sizeof(double));
   }
-  if (G.tc && warp == 3) {  // 128 TMEM columns: the three 32-column accumulators
+  if (use_tc && warp == 3) {  // 128 TMEM columns: the three 32-column accumulators
     __syncwarp();
     tc_alloc(&s_tmem, 128);
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = G.tc ? s_tmem : 0u;
+  const uint32_t tmem = use_tc ? s_tmem : 0u;
   // everything above reads only constant operators and factor records; the
   // arrays below are produced (HX) or still read (X) by the previous kernel
   pdl_wait();
@@ -863,7 +869,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
   // stage the velocity operators (tail of the operator copy) into dead rows
   if (tid == 0) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    if (G.tc) {  // split-BF16 velocity operators in the tcgen05 operand layout
+    if (use_tc) {  // split-BF16 velocity operators in the tcgen05 operand layout
       mbar_arrive_expect(&s_bar, (uint32_t)kTcImgA);
       bulk_g2s(reinterpret_cast<unsigned char*>(sm) + G.oTA, G.vimg, (uint32_t)kTcImgA, &s_bar);
     } else {
@@ -979,7 +985,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
     for (int i = tid; i < d.nD; i += kGThreads)
       rowc[(((i & 1) ? G.oGO : G.oGE) + (i >> 1)) * LC + 0] = m_x[i];
   }
-  if (Jh > Jl && !G.tc) {
+  if (Jh > Jl && !use_tc) {
     // middle Gauss node (odd N) while the velocity operators arrive: one FP64
     // dot product per (operator, pencil, re/im)
     __syncthreads();
@@ -992,7 +998,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
   JFB_STAMP(0, 7);
 
   // ------------------------------------------------------------------ D --
-  if (!skip_d && G.tc) {
+  if (!skip_d && use_tc) {
     unsigned char* smb = reinterpret_cast<unsigned char*>(sm);
     // state operand: FP64 coefficient rows -> three BF16 parts, K-major
     // (row n = pencil column: 2 w + re/im, k = coefficient row of the half)
@@ -1183,9 +1189,9 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
     }
   }
   JFB_STAMP(0, 8);
-  if (Jh > Jl && !skip_d && !G.tc && tid < kGW)  // products formed in C3
+  if (Jh > Jl && !skip_d && !use_tc && tid < kGW)  // products formed in C3
     mid_store(d, a, sm + G.oMid, s_p, s_ky, s_kz, tid, N, Jl, P);
-  if (G.tc) {  // free the TMEM columns (every tcgen05 load has completed)
+  if (use_tc) {  // free the TMEM columns (every tcgen05 load has completed)
     tc_fence_before();
     __syncthreads();
     if (warp == 3) {
@@ -1196,10 +1202,11 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
   JFB_STAMP(0, 9);
 }
 
+template <bool kTC>
 __global__ void __launch_bounds__(kGThreads, 1)
     pencil_gemm_kernel(const __grid_constant__ Dims d, const __grid_constant__ DevOps o,
                        const __grid_constant__ GemmOps G, const __grid_constant__ GemmStageArgs a) {
-  pencil_gemm_body(d, o, G, a, blockIdx.x, gridDim.x);
+  pencil_gemm_body<kTC>(d, o, G, a, blockIdx.x, gridDim.x);
 }
 
 }  // namespace jfb
