@@ -588,12 +588,12 @@ static int launch_implicit(jfb_kmm_plan* pl, const StageArgs& a, cudaStream_t s)
   }
   const GemmStageArgs g = gemm_args(pl, a);
   const int blocks = (pl->d.Ny / 2) * ceil_div(pl->d.Kz, 8);
-  if (pl->gops.tc)
-    JFB_CHECK_CUDA(launch_ex(pl->pdl, pencil_gemm_kernel<true>, dim3(blocks), dim3(kGThreads),
-                             pl->smem_gemm, s, pl->d, pl->ops, pl->gops, g));
-  else
-    JFB_CHECK_CUDA(launch_ex(pl->pdl, pencil_gemm_kernel<false>, dim3(blocks), dim3(kGThreads),
-                             pl->smem_gemm, s, pl->d, pl->ops, pl->gops, g));
+  // the tcgen05 variant exists for the rotational form only
+  auto* k = pl->gops.tc ? pencil_gemm_kernel<true, 0>
+            : pl->d.grad ? pencil_gemm_kernel<false, 1>
+                         : pencil_gemm_kernel<false, 0>;
+  JFB_CHECK_CUDA(launch_ex(pl->pdl, k, dim3(blocks), dim3(kGThreads), pl->smem_gemm, s, pl->d,
+                           pl->ops, pl->gops, g));
   return JFB_OK;
 }
 
@@ -1496,8 +1496,9 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
       G.kt_mg_lin[0] = ceil_div(nDe, 4);
       G.kt_mg_lin[1] = ceil_div(nDo, 4);
       pl->smem_gemm = smem;
-      JFB_CHECK_CUDA(allow_smem((const void*)pencil_gemm_kernel<false>));
-      JFB_CHECK_CUDA(allow_smem((const void*)pencil_gemm_kernel<true>));
+      JFB_CHECK_CUDA(allow_smem((const void*)pencil_gemm_kernel<false, 0>));
+      JFB_CHECK_CUDA(allow_smem((const void*)pencil_gemm_kernel<false, 1>));
+      JFB_CHECK_CUDA(allow_smem((const void*)pencil_gemm_kernel<true, 0>));
       // mixed form, JFB200_TC=1: the velocity products on the tcgen05
       // tensor cores (split-BF16 operands, FP32 accumulation) when the
       // halves fit the 32-row quarters / 32-deep K blocks and the images fit

@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
     ens_pencil_kernel(const EnsMember* __restrict__ tab, const EnsTiles* __restrict__ T) {
   const int m = ens_member(T, 0, blockIdx.x);
   const EnsMember& e = ens_args(tab, m);
-  pencil_gemm_body<true>(e.d, e.o, e.G, e.ga, blockIdx.x - T->first[0][m],
+  pencil_gemm_body<true, 2>(e.d, e.o, e.G, e.ga, blockIdx.x - T->first[0][m],
                    T->first[0][m + 1] - T->first[0][m]);
 }
 

@@ -502,7 +502,7 @@ __device__ __forceinline__ double mid_dot(const GemmOps& G, const double* sm, in
 }
 
 // u, omega at the middle node of pencil w from the products md[].
-__device__ __forceinline__ void mid_store(const Dims& d, const GemmStageArgs& a, const double* md,
+__device__ __forceinline__ void mid_store(const bool grad, const GemmStageArgs& a, const double* md,
                                           const int* s_p, const double* s_ky, const double* s_kz,
                                           int w, int N, int Jl, size_t P) {
   if (s_p[w] < 0) return;
@@ -512,7 +512,7 @@ __device__ __forceinline__ void mid_store(const Dims& d, const GemmStageArgs& a,
     if (a.x32) reinterpret_cast<c32*>(a.X)[e] = cmk((float)v.re, (float)v.im);
     else a.X[e] = v;
   };
-  if (d.grad) {
+  if (grad) {
     c64 f[9];
     gradient_fields(s_ky[w], s_kz[w], val(0), val(5), val(2), val(1), val(3), val(4), f);
 #pragma unroll
@@ -530,12 +530,14 @@ __device__ __forceinline__ void mid_store(const Dims& d, const GemmStageArgs& a,
 // kTC = false compiles the body without the tcgen05 velocity products (the
 // default kernel: a smaller instruction footprint, 78.7 -> 77.4 us per
 // mixed step at 65x64x64); kTC = true keeps them behind the plan's runtime
-// flag G.tc.
-template <bool kTC>
+// flag G.tc.  kForm: 0 rotational, 1 gradient (each without the other's
+// code), 2 the plan's runtime flag d.grad.
+template <bool kTC, int kForm>
 __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o, const GemmOps& G,
                                                  const GemmStageArgs& a, const int bid,
                                                  const int nbid) {
   const bool use_tc = kTC && G.tc;
+  const bool grad = kForm == 2 ? d.grad != 0 : kForm == 1;
   extern __shared__ __align__(128) double sm[];
   __shared__ int s_p[kGW], s_mode[kGW];
   __shared__ double s_ky[kGW], s_kz[kGW];
@@ -627,7 +629,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
         const int j = idx / kGW, w = idx % kGW, p = s_p[w];
         if (p < 0) continue;
         const int rows[2] = {j, N - 1 - j};
-        const int fs[4] = {0, d.grad ? 6 : 1, d.grad ? 7 : 3, d.grad ? 8 : 5};
+        const int fs[4] = {0, grad ? 6 : 1, grad ? 7 : 3, grad ? 8 : 5};
 #pragma unroll
         for (int s2 = 0; s2 < 2; ++s2)
 #pragma unroll
@@ -712,7 +714,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
     }
     if (a.Xlin && ok) {
       const bool mean = s_p[w] == 0;
-      if (d.grad) {
+      if (grad) {
         add_base_convection_terms(xl[it][0], d.uwall * o.xphys[j], d.uwall, h[0]);
         if (jm != j) add_base_convection_terms(xl[it][1], d.uwall * o.xphys[jm], d.uwall, h[1]);
       } else {
@@ -989,7 +991,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
     // middle Gauss node (odd N) while the velocity operators arrive: one FP64
     // dot product per (operator, pencil, re/im)
     __syncthreads();
-    if (tid < (d.grad ? 6 : 5) * 2 * kGW) sm[G.oMid + tid] = mid_dot(G, sm, tid);
+    if (tid < (grad ? 6 : 5) * 2 * kGW) sm[G.oMid + tid] = mid_dot(G, sm, tid);
   }
   const bool staged = mbar_wait_bounded(&s_bar, 0, G.status, kStatusWaitTimeout);
   // a timed-out copy leaves the velocity operators incomplete: skip D (the
@@ -1097,7 +1099,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
         }
       }
       }
-      if (Jh > Jl && tid < kGW) mid_store(d, a, sm + G.oMid, s_p, s_ky, s_kz, tid, N, Jl, P);
+      if (Jh > Jl && tid < kGW) mid_store(grad, a, sm + G.oMid, s_p, s_ky, s_kz, tid, N, Jl, P);
     }
   } else if (!skip_d) {
     const int MTv = G.sub[gA0Ee].mt;
@@ -1139,7 +1141,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
       group3(G.oUO, gP1Eo, gA0Oo, gP2Oo, 1, 5, 7);
       group2(G.oGE, gB1Ee, gB2Oe, 3, 9);
       group2(G.oGO, gB2Eo, gB1Oo, 4, 8);
-      if (d.grad) {  // d/dx u0: A1 on the even and odd coefficient halves
+      if (grad) {  // d/dx u0: A1 on the even and odd coefficient halves
         auto group1 = [&](int oB, int s0, int q0) {
           const double* __restrict__ Bs = sm + (size_t)oB * kGLd + t4 * kGLd + ncol0 + g;
           const SubDesc d0 = G.sub[s0];
@@ -1172,7 +1174,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
             X[(size_t)jm * P] = vm;
           }
         };
-        if (d.grad) {
+        if (grad) {
           c64 fe[9], fo[9];
           gradient_fields(s_ky[w], s_kz[w], cv(0), cv(11), cv(1), cv(2), cv(3), cv(4), fe);
           gradient_fields(s_ky[w], s_kz[w], cv(5), cv(10), cv(6), cv(7), cv(8), cv(9), fo);
@@ -1190,7 +1192,7 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
   }
   JFB_STAMP(0, 8);
   if (Jh > Jl && !skip_d && !use_tc && tid < kGW)  // products formed in C3
-    mid_store(d, a, sm + G.oMid, s_p, s_ky, s_kz, tid, N, Jl, P);
+    mid_store(grad, a, sm + G.oMid, s_p, s_ky, s_kz, tid, N, Jl, P);
   if (use_tc) {  // free the TMEM columns (every tcgen05 load has completed)
     tc_fence_before();
     __syncthreads();
@@ -1202,11 +1204,11 @@ __device__ __forceinline__ void pencil_gemm_body(const Dims& d, const DevOps& o,
   JFB_STAMP(0, 9);
 }
 
-template <bool kTC>
+template <bool kTC, int kForm>
 __global__ void __launch_bounds__(kGThreads, 1)
     pencil_gemm_kernel(const __grid_constant__ Dims d, const __grid_constant__ DevOps o,
                        const __grid_constant__ GemmOps G, const __grid_constant__ GemmStageArgs a) {
-  pencil_gemm_body<kTC>(d, o, G, a, blockIdx.x, gridDim.x);
+  pencil_gemm_body<kTC, kForm>(d, o, G, a, blockIdx.x, gridDim.x);
 }
 
 }  // namespace jfb
