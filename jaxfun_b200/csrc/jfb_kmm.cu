@@ -525,10 +525,10 @@ static int launch_pencil(jfb_kmm_plan* pl, const StageArgs& a0, cudaStream_t s) 
   const int blocks = pl->d.Ny * pl->d.nKb;
   StageArgs a = a0;
   a.status = pl->status;
-  if (pl->d.nD <= 64)
-    pencil_stage_kernel<1><<<blocks, kNW * 32, pl->smem_pencil, s>>>(pl->ops, pl->d, a);
-  else
-    pencil_stage_kernel<2><<<blocks, kNW * 32, pl->smem_pencil, s>>>(pl->ops, pl->d, a);
+  // one instantiation per register-row count and nonlinear form
+  auto* k = pl->d.nD <= 64 ? (pl->d.grad ? pencil_stage_kernel<1, 1> : pencil_stage_kernel<1, 0>)
+                           : (pl->d.grad ? pencil_stage_kernel<2, 1> : pencil_stage_kernel<2, 0>);
+  k<<<blocks, kNW * 32, pl->smem_pencil, s>>>(pl->ops, pl->d, a);
   JFB_CHECK_LAUNCH();
   return JFB_OK;
 }
@@ -1320,8 +1320,10 @@ static int create_plan(const jfb_kmm_config* cfg, const jfb_mhd_params* mhd,
     set_error("grid too large for the shared-memory tiling");
     return fail(JFB_ERR_ARG);
   }
-  allow_smem((const void*)pencil_stage_kernel<1>);
-  allow_smem((const void*)pencil_stage_kernel<2>);
+  allow_smem((const void*)pencil_stage_kernel<1, 0>);
+  allow_smem((const void*)pencil_stage_kernel<2, 0>);
+  allow_smem((const void*)pencil_stage_kernel<1, 1>);
+  allow_smem((const void*)pencil_stage_kernel<2, 1>);
   for (const void* fn : {(const void*)y_backward_kernel<double>, (const void*)y_forward_kernel<double>,
                          (const void*)y_backward_kernel<float>, (const void*)y_forward_kernel<float>})
     allow_smem(fn);

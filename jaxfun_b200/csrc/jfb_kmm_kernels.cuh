@@ -724,8 +724,10 @@ __device__ JFB_CTA_DMMA_INLINE void cta_forward_dmma(const double* __restrict__ 
 // ---------------------------------------------------------------------------
 // pencil_stage: see file header.  Block = kNW warps, one pencil per warp.
 // ---------------------------------------------------------------------------
-template <int NR>
+// kForm: 0 rotational, 1 gradient (each compiled without the other's code).
+template <int NR, int kForm>
 __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, StageArgs a) {
+  const bool grad = kForm == 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   c64* R1 = reinterpret_cast<c64*>(smem_raw);  // 6 * Nx * kLDW
   c64* ARR = R1 + 6 * d.Nx * kLDW;              // kNW * 6 * Nx
@@ -805,7 +807,7 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
             const c32 x = a.Xlin[((size_t)g * d.Nx + j) * P + p0 + w];
             return cmk((double)x.re, (double)x.im);
           };
-          if (d.grad) {  // U_b d/dy u_i (+ u_0 dU_b/dx e_y), pcf_fluctuations_jax.py:99-106
+          if (grad) {  // U_b d/dy u_i (+ u_0 dU_b/dx e_y), pcf_fluctuations_jax.py:99-106
             if (f == 0) v = v + ub * ld(6);
             else if (f == 1) v = (v + ub * ld(7)) + uw * ld(0);
             else v = v + ub * ld(8);
@@ -843,7 +845,7 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
       // branches, kLoadBatch points per thread in flight; the same sums in
       // the same order as a per-field update of the loaded H values
       const int npt = d.Nx * kNW;
-      const int g1 = d.grad ? 6 : 1, g2 = d.grad ? 7 : 3, g3 = d.grad ? 8 : 5;
+      const int g1 = grad ? 6 : 1, g2 = grad ? 7 : 3, g3 = grad ? 8 : 5;
       for (int i0 = threadIdx.x; i0 < npt; i0 += kLoadBatch * blockDim.x) {
         c64 x[kLoadBatch][4];
 #pragma unroll
@@ -868,7 +870,7 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
           c64* h0 = R1 + (size_t)j * kLDW + w;
           c64* h1 = h0 + (size_t)d.Nx * kLDW;
           c64* h2 = h1 + (size_t)d.Nx * kLDW;
-          if (d.grad) {  // U_b d/dy u_i (+ u_0 dU_b/dx e_y), pcf_fluctuations_jax.py:99-106
+          if (grad) {  // U_b d/dy u_i (+ u_0 dU_b/dx e_y), pcf_fluctuations_jax.py:99-106
             *h0 = *h0 + ub * x[u][1];
             *h1 = (*h1 + ub * x[u][2]) + uw * x[u][0];
             *h2 = *h2 + ub * x[u][3];
@@ -1126,7 +1128,7 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
     apply_SDT(d, A1, A3, lane);
     chebder_warp(A3, A4, d.Nx, d.dfx, lane, d.family);  // A4 = D uo2
     chebder_warp(A2, A0, d.Nx, d.dfx, lane, d.family);  // A0 = D uo1
-    if (d.grad) {
+    if (grad) {
       // gradient form: the x-derivatives of the three components
       // (channelflow_kmm.py:716-740); the y / z derivatives are wavenumber
       // weights applied on the way to the periodic transforms
@@ -1155,7 +1157,7 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
     const int n = idx % d.Nx, wf = idx / d.Nx;
     const int w = wf / 6, f = wf % 6;
     const int arr = (f == 0) ? 5 : (f == 1) ? 2 : (f == 2) ? 3 : (f == 3) ? 1
-                    : (f == 4) ? (d.grad ? 0 : 4) : (d.grad ? 4 : 0);
+                    : (f == 4) ? (grad ? 0 : 4) : (grad ? 4 : 0);
     const c64 v = ARR[(w * 6 + arr) * d.Nx + n];
     *reinterpret_cast<double2*>(Bs + (size_t)n * kLDB + 2 * wf) = make_double2(v.re, v.im);
   }
@@ -1169,7 +1171,7 @@ __global__ void __launch_bounds__(256, 1) pencil_stage_kernel(DevOps o, Dims d, 
       const c64 v = ARR[fi * kNW + w];
       if (a.x32) reinterpret_cast<c32*>(a.X)[e] = cmk((float)v.re, (float)v.im);
       else a.X[e] = v;
-      if (d.grad && fi < 3 * d.Nx) {
+      if (grad && fi < 3 * d.Nx) {
         // fields 6..8: d/dy u_i = i ky u_i (the CTA's pencils share ky)
         const c64 dy = mul_i(kyp * v);
         const size_t ey = (size_t)(6 * d.Nx + fi) * P + p0 + w;
