@@ -176,3 +176,22 @@ def test_oracle_magnetic_wall_conditions_are_stable():
                                                 magnetic_bc=bc)
         r = m.growth_rate(1.0, 1.0)
         assert math.isfinite(r) and r < 0.0, bc
+
+
+def test_growth_order_and_finite_filter_match_the_oracle():
+    """Ordering by descending real part, ties by descending imaginary part
+    (la/eig.py:12-19), and the finite-cap filter, on index arrays only."""
+    import torch
+
+    from jaxfun_b200.linear import _growth_sort, _keep_finite
+
+    rng = np.random.default_rng(7)
+    re = rng.integers(-3, 3, 40).astype(float)          # many equal real parts
+    im = rng.integers(-2, 3, 40).astype(float)
+    w = re + 1j * im
+    got = _growth_sort(torch.as_tensor(w)).numpy()
+    want = ol.growth_order(w)
+    assert np.array_equal(w[got], w[want])
+    v = torch.tensor([1.0 + 0j, complex(math.inf, 0), 5e6 + 0j, -2.0 + 1j, complex(0, math.nan)])
+    kept, _ = _keep_finite(v, None, 1e6)
+    assert kept.tolist() == [1.0 + 0j, -2.0 + 1j]
