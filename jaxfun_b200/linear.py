@@ -407,12 +407,10 @@ class PlaneCouetteLinear:
         walls = (0, n - 1)
         rows = [f * n + wl for f in range(3) for wl in walls]
         bc = self.magnetic_bc
-        if bc == "dirichlet":
-            rows += [f * n + wl for f in (4, 5, 6) for wl in walls]
-        elif bc == "conducting":
-            rows += [f * n + wl for f in (4, 5, 6) for wl in walls]
-        else:  # pseudo_vacuum, insulating: phi pinned at the walls
-            rows += [f * n + wl for f in (4, 5, 6, 7) for wl in walls]
+        # the field's wall rows; pseudo_vacuum and insulating also pin phi
+        # there (div b = 0 at the wall follows from their other rows)
+        pinned = (4, 5, 6) if bc in ("dirichlet", "conducting") else (4, 5, 6, 7)
+        rows += [f * n + wl for f in pinned for wl in walls]
         L[:, rows, :] = 0.0
         M[:, rows, :] = 0.0
         for f in range(3):
